@@ -1,0 +1,853 @@
+/*
+ * FP64 CPU oracle for the BINDER hot path -- TEST INFRASTRUCTURE ONLY (see binder_oracle.h).
+ *
+ * Every function restates one piece of the reference CPU backend (ste93ste/BINDER) and cites the
+ * file:line it follows.  Compiled with -ffp-contract=off so that expression-by-expression FP64
+ * evaluation order (and therefore the Jacobian determinants) matches the reference bit for bit.
+ */
+#include "binder_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PI_D 3.14159265358979323846
+
+static int g_threads = 0;
+void orc_set_threads(int n) { g_threads = n; }
+int orc_get_threads(void) {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Philox4x32-10, as published by Salmon et al. (SC'11): 10 rounds of the 4x32 bijection with  */
+/* the multipliers M0 = 0xD2511F53, M1 = 0xCD9E8D57 and the Weyl key increments 0x9E3779B9,    */
+/* 0xBB67AE85.  The CUDA path uses the identical function so draws agree exactly.             */
+/* ------------------------------------------------------------------------------------------ */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * (uint64_t)c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * (uint64_t)c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static inline void philox_draw(uint64_t seed, uint32_t index, uint32_t sweep, uint32_t tag,
+                               uint32_t chain, uint32_t out[4]) {
+    const uint32_t ctr[4] = {index, sweep, tag, chain};
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    orc_philox4x32_10(ctr, key, out);
+}
+
+/* uniform in (0,1) with 23 random bits: exactly representable in float and double */
+static inline double u01_f24(uint32_t x) { return ((double)(x >> 9) + 0.5) * (1.0 / 8388608.0); }
+/* uniform in (0,1) with 32 random bits (double) */
+static inline double u01_d32(uint32_t x) { return ((double)x + 0.5) * (1.0 / 4294967296.0); }
+
+/* ------------------------------------------------------------------------------------------ */
+/* cubic B-spline weights for offsets -1, 0, 1, 2 at fraction d in [0,1)                       */
+/* BINDER/src/cpu/Spline.cpp:44-73                                                             */
+/* ------------------------------------------------------------------------------------------ */
+void orc_spline3(double d, double w[4]) {
+    const double d2 = d * d, d3 = d2 * d;
+    const double e = 1.0 - d, e2 = e * e, e3 = e2 * e;
+    w[0] = e3 / 6.0;
+    w[1] = 2.0 / 3.0 - d2 + d3 * 0.5;
+    w[2] = 2.0 / 3.0 - e2 + e3 * 0.5;
+    w[3] = d3 / 6.0;
+}
+
+/* moving-image bin at a node; outside the moving grid the likelihood uses row 0
+ * (BINDER/src/cpu/MILikelihood.cpp:46-48, :92-93) */
+static inline int node_bin(const int *v, int x, int y, int z, int nxn, int nyn, int nzn) {
+    if (x < 0 || y < 0 || z < 0 || x >= nxn || y >= nyn || z >= nzn) return 0;
+    return v[((long)x * nyn + y) * nzn + z];
+}
+
+typedef struct {
+    double w[64];
+    int kbin[64];
+    int node[64][3];
+    int n;
+    double S;
+} neigh_t;
+
+/* weights B(y_j - d_i) * theta[v_j, u_i] for the 4x4x4 (3D) or 4x4 (2D) neighbourhood,
+ * Registration.cpp:219-272 */
+static void neighbourhood(const double *di, int ui, const int *v, const double *theta, int is2D,
+                          int nxn, int nyn, int nzn, int L, neigh_t *nb) {
+    double bx[4], by[4], bz[4] = {1.0, 1.0, 1.0, 1.0};
+    const int ix = (int)floor(di[0]), iy = (int)floor(di[1]);
+    const int iz = is2D ? 0 : (int)floor(di[2]);
+    orc_spline3(di[0] - floor(di[0]), bx);
+    orc_spline3(di[1] - floor(di[1]), by);
+    if (!is2D) orc_spline3(di[2] - floor(di[2]), bz);
+    const int ZZ = is2D ? 1 : 4;
+    int j = 0;
+    double S = 0.0;
+    for (int a = 0; a < 4; ++a) {
+        const int X = ix + a - 1;
+        for (int b = 0; b < 4; ++b) {
+            const int Y = iy + b - 1;
+            const double bxy = bx[a] * by[b];
+            for (int c = 0; c < ZZ; ++c) {
+                const int Z = is2D ? 0 : iz + c - 1;
+                const int k = node_bin(v, X, Y, Z, nxn, nyn, nzn);
+                const double w = bxy * bz[c] * theta[(long)k * L + ui];
+                nb->w[j] = w;
+                nb->kbin[j] = k;
+                nb->node[j][0] = X; nb->node[j][1] = Y; nb->node[j][2] = Z;
+                S += w;
+                ++j;
+            }
+        }
+    }
+    nb->n = j;
+    nb->S = S;
+}
+
+/* Registration.cpp:122-165 (E-step loop) and :219-330 (per voxel, sample == false) */
+double orc_estep(const double *d, const int *u, const int *v, const double *theta,
+                 int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L,
+                 double *dream, double *hist, long long *degenerate) {
+    const int is2D = (nz == 1);
+    const int N = is2D ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    const int T = orc_get_threads();
+    double *hist_t = (double *)calloc((size_t)T * K * L, sizeof(double));
+    double mll = 0.0;
+    long long deg = 0;
+#pragma omp parallel num_threads(T) reduction(+ : mll, deg)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        double *h = hist_t + (size_t)tid * K * L;
+        neigh_t nb;
+#pragma omp for schedule(static)
+        for (long i = 0; i < V; ++i) {
+            const double *di = d + i * N;
+            neighbourhood(di, u[i], v, theta, is2D, nxn, nyn, nzn, L, &nb);
+            double *dr = dream + i * N;
+            if (!(nb.S > 0.0)) {
+                for (int n = 0; n < N; ++n) dr[n] = floor(di[n]);
+                deg += 1;
+                continue;
+            }
+            mll += -log(nb.S);
+            double acc[3] = {0.0, 0.0, 0.0};
+            for (int j = 0; j < nb.n; ++j) {
+                const double p = nb.w[j] / nb.S;
+                h[(long)nb.kbin[j] * L + u[i]] += p;
+                for (int n = 0; n < N; ++n) acc[n] += p * (double)nb.node[j][n];
+            }
+            for (int n = 0; n < N; ++n) dr[n] = acc[n];
+        }
+    }
+    memset(hist, 0, sizeof(double) * K * L);
+    for (int t = 0; t < T; ++t)
+        for (long q = 0; q < (long)K * L; ++q) hist[q] += hist_t[(size_t)t * K * L + q];
+    free(hist_t);
+    if (degenerate) *degenerate = deg;
+    return mll;
+}
+
+/* Registration.cpp:278-307 (sample == true): categorical draw over the neighbourhood.
+ * The draw is t = u * S and the first neighbour whose running sum reaches t is taken, which is
+ * the reference's normalised-CDF test (random_number <= cumulative_probability). */
+double orc_estep_sample(const double *d, const int *u, const int *v, const double *theta,
+                        int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L,
+                        uint64_t seed, uint32_t sweep, uint32_t chain,
+                        double *dream, double *hist) {
+    const int is2D = (nz == 1);
+    const int N = is2D ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    const int T = orc_get_threads();
+    double *hist_t = (double *)calloc((size_t)T * K * L, sizeof(double));
+    double mll = 0.0;
+#pragma omp parallel num_threads(T) reduction(+ : mll)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        double *h = hist_t + (size_t)tid * K * L;
+        neigh_t nb;
+#pragma omp for schedule(static)
+        for (long i = 0; i < V; ++i) {
+            const double *di = d + i * N;
+            neighbourhood(di, u[i], v, theta, is2D, nxn, nyn, nzn, L, &nb);
+            double *dr = dream + i * N;
+            if (!(nb.S > 0.0)) {
+                for (int n = 0; n < N; ++n) dr[n] = floor(di[n]);
+                continue;
+            }
+            mll += -log(nb.S);
+            uint32_t r[4];
+            philox_draw(seed, (uint32_t)i, sweep, 1u, chain, r);
+            const double t = u01_f24(r[0]) * nb.S;
+            double cdf = 0.0;
+            int pick = nb.n - 1;
+            for (int j = 0; j < nb.n; ++j) {
+                cdf += nb.w[j];
+                if (cdf >= t) { pick = j; break; }
+            }
+            h[(long)nb.kbin[pick] * L + u[i]] += 1.0;
+            for (int n = 0; n < N; ++n) dr[n] = (double)nb.node[pick][n];
+        }
+    }
+    memset(hist, 0, sizeof(double) * K * L);
+    for (int t = 0; t < T; ++t)
+        for (long q = 0; q < (long)K * L; ++q) hist[q] += hist_t[(size_t)t * K * L + q];
+    free(hist_t);
+    return mll;
+}
+
+/* MILikelihood.cpp:71-86: theta <- (hist + alpha - 1) / row sum */
+void orc_theta_map(double *th, int K, int L, double alpha) {
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int l = 0; l < L; ++l) s += th[k * L + l] + alpha - 1.0;
+        for (int l = 0; l < L; ++l) th[k * L + l] = (th[k * L + l] + alpha - 1.0) / s;
+    }
+}
+
+/* MILikelihood.cpp:33-39 and :183-206: sum_k -log Dir(theta_k; alpha) */
+double orc_dirichlet_cost(const double *th, int K, int L, double alpha) {
+    double cost = 0.0;
+    for (int k = 0; k < K; ++k) {
+        double sum_alpha = 0.0;
+        for (int l = 0; l < L; ++l) sum_alpha += alpha;
+        double lp = lgamma(sum_alpha);
+        for (int l = 0; l < L; ++l) lp -= lgamma(alpha);
+        for (int l = 0; l < L; ++l) lp += (alpha - 1.0) * log(th[k * L + l]);
+        cost += -lp;
+    }
+    return cost;
+}
+
+/* Gamma(shape, 1) by Marsaglia & Tsang (ACM TOMS 26(3), 2000), with the shape < 1 boost
+ * Gamma(a) = Gamma(a+1) * U^(1/a).  Attempt j draws Philox ctr = {index, sweep, tag | j<<8, chain}:
+ * words 0,1 -> Box-Muller normal, word 2 -> acceptance uniform, word 3 -> boost uniform.
+ * Capped at 64 attempts (acceptance probability per attempt is > 0.95). */
+double orc_gamma_sample(double shape, uint64_t seed, uint32_t index, uint32_t sweep,
+                        uint32_t tag, uint32_t chain, int *capped) {
+    const int small = shape < 1.0;
+    const double a = small ? shape + 1.0 : shape;
+    const double dd = a - 1.0 / 3.0;
+    const double c = 1.0 / sqrt(9.0 * dd);
+    for (uint32_t att = 0; att < 64; ++att) {
+        uint32_t r[4];
+        philox_draw(seed, index, sweep, tag | (att << 8), chain, r);
+        const double u1 = u01_d32(r[0]), u2 = u01_d32(r[1]);
+        const double z = sqrt(-2.0 * log(u1)) * cos(2.0 * PI_D * u2);
+        double vv = 1.0 + c * z;
+        if (vv <= 0.0) continue;
+        vv = vv * vv * vv;
+        const double uu = u01_d32(r[2]);
+        if (uu < 1.0 - 0.0331 * (z * z) * (z * z) ||
+            log(uu) < 0.5 * z * z + dd * (1.0 - vv + log(vv))) {
+            double g = dd * vv;
+            if (small) g *= pow(u01_d32(r[3]), 1.0 / shape);
+            return g;
+        }
+    }
+    if (capped) *capped = 1;
+    return dd;
+}
+
+/* MILikelihood.cpp:132-169: theta_k ~ Dirichlet(hist_k + alpha) */
+int orc_dirichlet_sample(double *th, int K, int L, double alpha, uint64_t seed, uint32_t sweep,
+                         uint32_t chain) {
+    int capped_rows = 0;
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        int capped = 0;
+        for (int l = 0; l < L; ++l) {
+            const double g = orc_gamma_sample(th[k * L + l] + alpha, seed, (uint32_t)(k * L + l),
+                                              sweep, 4u, chain, &capped);
+            th[k * L + l] = g;
+            s += g;
+        }
+        for (int l = 0; l < L; ++l) th[k * L + l] /= s;
+        capped_rows += capped;
+    }
+    return capped_rows;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* orthonormal DCT-II (forward) / DCT-III (inverse) along each axis, as the FFTW REDFT10/01   */
+/* plans with the scaling of BINDER/src/cpu/DCT.cpp:83-175                                     */
+/* ------------------------------------------------------------------------------------------ */
+static double *dct_matrix(int n) {
+    double *C = (double *)malloc(sizeof(double) * n * n);
+    for (int k = 0; k < n; ++k) {
+        const double s = (k == 0) ? sqrt(1.0 / n) : sqrt(2.0 / n);
+        for (int j = 0; j < n; ++j) {
+            const long m = ((long)(2 * j + 1) * k) % (4L * n);
+            C[k * n + j] = s * cos(PI_D * (double)m / (2.0 * n));
+        }
+    }
+    return C;
+}
+
+/* y[.., k, ..] = sum_j M[k][j] x[.., j, ..] along an axis of length n with stride s */
+static void apply_axis(const double *M, int n, int transpose, double *data, long outer, long s) {
+    const int T = orc_get_threads();
+#pragma omp parallel num_threads(T)
+    {
+        double *in = (double *)malloc(sizeof(double) * n);
+#pragma omp for schedule(static)
+        for (long o = 0; o < outer * s; ++o) {
+            const long b = (o / s) * (long)n * s + (o % s);
+            for (int j = 0; j < n; ++j) in[j] = data[b + (long)j * s];
+            for (int k = 0; k < n; ++k) {
+                double acc = 0.0;
+                if (!transpose)
+                    for (int j = 0; j < n; ++j) acc += M[k * n + j] * in[j];
+                else
+                    for (int j = 0; j < n; ++j) acc += M[j * n + k] * in[j];
+                data[b + (long)k * s] = acc;
+            }
+        }
+        free(in);
+    }
+}
+
+void orc_dct3(const double *in, double *out, int nx, int ny, int nz, int inverse) {
+    const long V = (long)nx * ny * nz;
+    if (out != in) memcpy(out, in, sizeof(double) * V);
+    double *Cx = dct_matrix(nx), *Cy = dct_matrix(ny), *Cz = dct_matrix(nz);
+    apply_axis(Cz, nz, inverse, out, (long)nx * ny, 1);
+    apply_axis(Cy, ny, inverse, out, nx, nz);
+    apply_axis(Cx, nx, inverse, out, 1, (long)ny * nz);
+    free(Cx); free(Cy); free(Cz);
+}
+
+/* Box-Muller normal pair from one Philox draw (23-bit uniforms, same as the CUDA path) */
+static inline void normal_pair(uint64_t seed, uint32_t index, uint32_t sweep, uint32_t tag,
+                               uint32_t chain, double *z0, double *z1) {
+    uint32_t r[4];
+    philox_draw(seed, index, sweep, tag, chain, r);
+    const double u1 = u01_f24(r[0]), u2 = u01_f24(r[1]);
+    const double rr = sqrt(-2.0 * log(u1));
+    *z0 = rr * cos(2.0 * PI_D * u2);
+    *z1 = rr * sin(2.0 * PI_D * u2);
+}
+
+/* NonLinearTransformation.cpp:58-76 (constrain_transformation), :79-126 (sample_transformation),
+ * :128-137 (fill_in_data), :151-171 (raw regulariser), :173-188 (update_final_locations),
+ * :190-223 (smooth), :344-364 + :433-451 (noise std and draws). */
+double orc_smooth(const double *dream, const double *voxel_pos, const double *D,
+                  const double gamma[3], double sigma, int nx, int ny, int nz, double *final_out,
+                  int add_noise, uint64_t seed, uint32_t sweep, uint32_t chain,
+                  const double rho[3], const double eta[3], double *raw_reg) {
+    const int N = (nz == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    double *buf = (double *)malloc(sizeof(double) * V);
+    double *noise = NULL;
+    if (add_noise) {
+        noise = (double *)malloc(sizeof(double) * V * 3);
+        for (long i = 0; i < V; ++i) {
+            double z0, z1, z2, z3;
+            normal_pair(seed, (uint32_t)i, sweep, 2u, chain, &z0, &z1);
+            normal_pair(seed, (uint32_t)i, sweep, 3u, chain, &z2, &z3);
+            noise[i * 3 + 0] = z0; noise[i * 3 + 1] = z1; noise[i * 3 + 2] = z2;
+        }
+    }
+    const double ss2 = sigma * sigma;
+    const double rho_p = rho ? rho[0] * rho[1] * rho[2] : 0.0;
+    double cost = 0.0, raw = 0.0;
+    for (int n = 0; n < N; ++n) {
+        for (long i = 0; i < V; ++i) buf[i] = dream[i * N + n] - voxel_pos[i * N + n];
+        orc_dct3(buf, buf, nx, ny, nz, 0);
+        for (long i = 0; i < V; ++i) {
+            double c = buf[i] * (1.0 / (1.0 + gamma[n] * ss2 * D[i]));
+            if (add_noise) c += noise[i * 3 + n] * sqrt(ss2 / (1.0 + gamma[n] * ss2 * D[i]));
+            if (add_noise && raw_reg) raw += eta[n] * eta[n] * rho_p * D[i] * c * c;
+            cost += 0.5 * gamma[n] * D[i] * c * c;
+            buf[i] = c;
+        }
+        orc_dct3(buf, buf, nx, ny, nz, 1);
+        for (long i = 0; i < V; ++i) final_out[i * N + n] = buf[i] + voxel_pos[i * N + n];
+    }
+    if (raw_reg) *raw_reg = raw;
+    free(buf);
+    free(noise);
+    return cost;
+}
+
+/* Registration.cpp:122-217 */
+int orc_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
+           double *theta, double alpha, const double *D, const double gamma[3], double sigma,
+           int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L,
+           double non_zero_voxels, int max_iter, double convergence_th, int update_theta,
+           orc_iter_stats *stats) {
+    const int N = (nz == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    double *dream = (double *)malloc(sizeof(double) * V * N);
+    double *hist = (double *)malloc(sizeof(double) * K * L);
+    double mlp_old = 1e100;
+    int it = 0;
+    while (it < max_iter) {
+        const double mll = orc_estep(final_locations, u, v, theta, nx, ny, nz, nxn, nyn, nzn, K, L,
+                                     dream, hist, NULL);
+        if (update_theta) {
+            memcpy(theta, hist, sizeof(double) * K * L);
+            orc_theta_map(theta, K, L, alpha);
+        }
+        const double lpl = orc_dirichlet_cost(theta, K, L, alpha);
+        const double lpt = orc_smooth(dream, voxel_pos, D, gamma, sigma, nx, ny, nz,
+                                      final_locations, 0, 0, 0, 0, NULL, NULL, NULL);
+        const double mlp = mll + lpt + lpl;
+        if (stats) {
+            stats[it].mll = mll;
+            stats[it].log_prior_likelihood = lpl;
+            stats[it].log_prior_transformation = lpt;
+            stats[it].mlp = mlp;
+        }
+        ++it;
+        if ((mlp_old - mlp) / non_zero_voxels < convergence_th) break;
+        mlp_old = mlp;
+    }
+    free(dream);
+    free(hist);
+    return it;
+}
+
+/* Registration.cpp:515-642 with NonLinearTransformation.cpp:79-126 for block 3 */
+int orc_sampler(double *final_locations, double *dream, const double *voxel_pos, const int *u,
+                const int *v, double *theta, double alpha, const double *D, double gamma[3],
+                double sigma, const double rho[3], const double eta[3],
+                int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L,
+                uint64_t seed, uint32_t chain, int N_b, int N_s, int sample_gamma,
+                int sample_gamma_every, int sample_posteriors, int sample_likelihood_parameters,
+                int sample_transformation_parameters, double *mean_out, double *cov_out) {
+    const int N = (nz == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    double *hist = (double *)calloc((size_t)K * L, sizeof(double));
+    double *M2 = (double *)calloc((size_t)V * N * N, sizeof(double));
+    memset(mean_out, 0, sizeof(double) * V * N);
+    const double alpha_0 = 1.0, beta_0 = 10000.0; /* NonLinearTransformation.cpp:41-42 */
+    int capped = 0;
+    for (int sweep = 0; sweep < N_b + N_s; ++sweep) {
+        if (sample_posteriors)
+            orc_estep_sample(final_locations, u, v, theta, nx, ny, nz, nxn, nyn, nzn, K, L, seed,
+                             (uint32_t)sweep, chain, dream, hist);
+        if (sample_likelihood_parameters) {
+            memcpy(theta, hist, sizeof(double) * K * L);
+            capped += orc_dirichlet_sample(theta, K, L, alpha, seed, (uint32_t)sweep, chain);
+        }
+        if (sample_transformation_parameters) {
+            const int sg = sample_gamma && (sweep % sample_gamma_every == 0);
+            double raw = 0.0;
+            orc_smooth(dream, voxel_pos, D, gamma, sigma, nx, ny, nz, final_locations, 1, seed,
+                       (uint32_t)sweep, chain, rho, eta, sg ? &raw : NULL);
+            if (sg) {
+                const double a_post = alpha_0 + 0.5 * (double)(N * V);
+                const double b_post = beta_0 + 0.5 * (double)V * raw;
+                int c = 0;
+                const double nu = orc_gamma_sample(a_post, seed, 0u, (uint32_t)sweep, 5u, chain, &c) /
+                                  b_post;
+                capped += c;
+                const double rp = rho[0] * rho[1] * rho[2];
+                for (int n = 0; n < 3; ++n) gamma[n] = nu * rp * eta[n] * eta[n] * (double)V;
+            }
+        }
+        if (sweep >= N_b) {
+            const double inv_n = 1.0 / ((double)(sweep - N_b) + 1.0);
+            for (long i = 0; i < V; ++i) {
+                double d1[3], d2[3];
+                for (int n = 0; n < N; ++n) {
+                    const double val = final_locations[i * N + n];
+                    const double m_old = mean_out[i * N + n];
+                    d1[n] = val - m_old;
+                    const double m_new = m_old + d1[n] * inv_n;
+                    mean_out[i * N + n] = m_new;
+                    d2[n] = val - m_new;
+                }
+                for (int r = 0; r < N; ++r)
+                    for (int c = 0; c < N; ++c) M2[i * N * N + r * N + c] += d1[r] * d2[c];
+            }
+        }
+    }
+    const double inv = 1.0 / (double)(N_s - 1);
+    for (long q = 0; q < V * N * N; ++q) cov_out[q] = M2[q] * inv;
+    free(hist);
+    free(M2);
+    return capped;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Jacobian determinants                                                                       */
+/* ------------------------------------------------------------------------------------------ */
+/* cofactor expansion along the first row, the grouping the reference writes out
+ * (BINDER/src/cpu/utils.cpp:156-160 and topology_correction_3D.cpp:286-288) */
+static inline double det3(double a00, double a01, double a02, double a10, double a11, double a12,
+                          double a20, double a21, double a22) {
+    return a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) +
+           a02 * (a10 * a21 - a11 * a20);
+}
+
+/* BINDER/src/cpu/utils.cpp:100-345: mean over the valid ones of the 8 one-sided corner
+ * determinants at every voxel; corners visited in the order fff, bff, fbf, ffb, bbf, bfb, fbb,
+ * bbb (f = forward difference along that axis, b = backward). */
+void orc_jacobian3d(const double *f, int nx, int ny, int nz, double vx, double vy, double vz,
+                    double *J) {
+    static const int dirs[8][3] = {{1, 1, 1},  {-1, 1, 1},  {1, -1, 1},  {1, 1, -1},
+                                   {-1, -1, 1}, {-1, 1, -1}, {1, -1, -1}, {-1, -1, -1}};
+    const double vol = 1.0 / (vx * vy * vz);
+    const int T = orc_get_threads();
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const long p = ((long)x * ny + y) * nz + z;
+                const double *w0 = f + p * 3;
+                double tot = 0.0;
+                int valid = 0;
+                for (int c = 0; c < 8; ++c) {
+                    const int sx = dirs[c][0], sy = dirs[c][1], sz = dirs[c][2];
+                    if ((sx > 0 && x >= nx - 1) || (sx < 0 && x <= 0)) continue;
+                    if ((sy > 0 && y >= ny - 1) || (sy < 0 && y <= 0)) continue;
+                    if ((sz > 0 && z >= nz - 1) || (sz < 0 && z <= 0)) continue;
+                    const double *px = f + (p + (long)sx * ny * nz) * 3;
+                    const double *py = f + (p + (long)sy * nz) * 3;
+                    const double *pz = f + (p + sz) * 3;
+                    double col[3][3]; /* col[axis][component] */
+                    for (int m = 0; m < 3; ++m) {
+                        col[0][m] = sx > 0 ? px[m] - w0[m] : w0[m] - px[m];
+                        col[1][m] = sy > 0 ? py[m] - w0[m] : w0[m] - py[m];
+                        col[2][m] = sz > 0 ? pz[m] - w0[m] : w0[m] - pz[m];
+                    }
+                    const double Jc = det3(col[0][0], col[1][0], col[2][0], col[0][1], col[1][1],
+                                           col[2][1], col[0][2], col[1][2], col[2][2]) * vol;
+                    tot += Jc;
+                    valid++;
+                }
+                J[p] = valid > 0 ? tot / valid : 1.0;
+            }
+}
+
+/* BINDER/src/cpu/utils.cpp:10-98: mean over the valid ones of the 4 one-sided corner
+ * determinants (ff, bf, fb, bb) */
+void orc_jacobian2d(const double *f, int nx, int ny, double vx, double vy, double *J) {
+    static const int dirs[4][2] = {{1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+    const double vol = 1.0 / (vx * vy);
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y) {
+            const long p = (long)x * ny + y;
+            const double *w0 = f + p * 2;
+            double tot = 0.0;
+            int valid = 0;
+            for (int c = 0; c < 4; ++c) {
+                const int sx = dirs[c][0], sy = dirs[c][1];
+                if ((sx > 0 && x >= nx - 1) || (sx < 0 && x <= 0)) continue;
+                if ((sy > 0 && y >= ny - 1) || (sy < 0 && y <= 0)) continue;
+                const double *px = f + (p + (long)sx * ny) * 2;
+                const double *py = f + (p + sy) * 2;
+                const double ax0 = sx > 0 ? px[0] - w0[0] : w0[0] - px[0];
+                const double ax1 = sx > 0 ? px[1] - w0[1] : w0[1] - px[1];
+                const double ay0 = sy > 0 ? py[0] - w0[0] : w0[0] - py[0];
+                const double ay1 = sy > 0 ? py[1] - w0[1] : w0[1] - py[1];
+                tot += (ax0 * ay1 - ay0 * ax1) * vol;
+                valid++;
+            }
+            J[p] = valid > 0 ? tot / valid : 1.0;
+        }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* topology correction (BINDER/src/cpu/topology_correction_3D.cpp)                             */
+/* ------------------------------------------------------------------------------------------ */
+/* :488-607: the 8 corner Jacobians of every cell (x..x+1, y..y+1, z..z+1), stored in the order
+ * of the cell vertices 000, 100, 010, 001, 011, 101, 110, 111; each uses the three cell edges
+ * through its vertex (hi - lo). */
+void orc_corner_jacobians3d(const double *pos, int nx, int ny, int nz, const double vs[3],
+                            double e1, double e2, double *Jc, int *n_below, int *n_above) {
+    static const int vert[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                   {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
+    const double vol = 1.0 / (vs[0] * vs[1] * vs[2]);
+    long nb = 0, na = 0;
+    const int T = orc_get_threads();
+#pragma omp parallel for num_threads(T) schedule(static) reduction(+ : nb, na)
+    for (int x = 0; x < nx - 1; ++x)
+        for (int y = 0; y < ny - 1; ++y)
+            for (int z = 0; z < nz - 1; ++z) {
+                const long cell = ((long)x * (ny - 1) + y) * (nz - 1) + z;
+                for (int c = 0; c < 8; ++c) {
+                    const int cx = vert[c][0], cy = vert[c][1], cz = vert[c][2];
+                    const double *w = pos + (((long)(x + cx) * ny + (y + cy)) * nz + (z + cz)) * 3;
+                    /* neighbours across each edge through the vertex */
+                    const double *wx = pos + (((long)(x + 1 - cx) * ny + (y + cy)) * nz + (z + cz)) * 3;
+                    const double *wy = pos + (((long)(x + cx) * ny + (y + 1 - cy)) * nz + (z + cz)) * 3;
+                    const double *wz = pos + (((long)(x + cx) * ny + (y + cy)) * nz + (z + 1 - cz)) * 3;
+                    double col[3][3];
+                    for (int m = 0; m < 3; ++m) {
+                        col[0][m] = cx ? w[m] - wx[m] : wx[m] - w[m];
+                        col[1][m] = cy ? w[m] - wy[m] : wy[m] - w[m];
+                        col[2][m] = cz ? w[m] - wz[m] : wz[m] - w[m];
+                    }
+                    double j = det3(col[0][0], col[1][0], col[2][0], col[0][1], col[1][1], col[2][1],
+                                    col[0][2], col[1][2], col[2][2]);
+                    j *= vol;
+                    Jc[cell * 8 + c] = j;
+                    if (j < e1) nb++;
+                    if (j > e2) na++;
+                }
+            }
+    if (n_below) *n_below = (int)nb;
+    if (n_above) *n_above = (int)na;
+}
+
+/* :172-245: forward differences with periodic wrap, grad[p][n1*3+n2] = d pos_n1 / d axis_n2 / vs[n1] */
+void orc_gradients3d(const double *pos, int nx, int ny, int nz, const double vs[3], double *g) {
+    const int T = orc_get_threads();
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const long p = ((long)x * ny + y) * nz + z;
+                const int x2 = (x + 1 > nx - 1) ? x + 1 - nx : x + 1;
+                const int y2 = (y + 1 > ny - 1) ? y + 1 - ny : y + 1;
+                const int z2 = (z + 1 > nz - 1) ? z + 1 - nz : z + 1;
+                const long px = ((long)x2 * ny + y) * nz + z;
+                const long py = ((long)x * ny + y2) * nz + z;
+                const long pz = ((long)x * ny + y) * nz + z2;
+                for (int n1 = 0; n1 < 3; ++n1) {
+                    g[p * 9 + n1 * 3 + 0] = (pos[px * 3 + n1] - pos[p * 3 + n1]) / vs[n1];
+                    g[p * 9 + n1 * 3 + 1] = (pos[py * 3 + n1] - pos[p * 3 + n1]) / vs[n1];
+                    g[p * 9 + n1 * 3 + 2] = (pos[pz * 3 + n1] - pos[p * 3 + n1]) / vs[n1];
+                }
+            }
+}
+
+/* :247-332 and :452-486: in lexicographic cell order, every flagged corner's gradient matrix is
+ * blended toward the identity in steps of 0.1 until its determinant lies in [e1, e2], then one
+ * more step is applied and written back.  The blending loop is capped at 11 steps (alpha = 1
+ * gives the identity); returns the number of corners that hit the cap. */
+int orc_limit_gradients3d(double *g, const double *Jc, int nx, int ny, int nz, double e1,
+                          double e2) {
+    static const int vert[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                   {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
+    int capped = 0;
+    for (int x = 0; x < nx - 1; ++x)
+        for (int y = 0; y < ny - 1; ++y)
+            for (int z = 0; z < nz - 1; ++z)
+                for (int c = 0; c < 8; ++c) {
+                    const long cell = ((long)x * (ny - 1) + y) * (nz - 1) + z;
+                    const double jv = Jc[cell * 8 + c];
+                    if (!(jv < e1 || jv > e2)) continue;
+                    /* column n2 is the forward difference stored at the vertex minus its n2 bit */
+                    long gp[3];
+                    for (int n2 = 0; n2 < 3; ++n2) {
+                        int o[3] = {vert[c][0], vert[c][1], vert[c][2]};
+                        o[n2] = 0;
+                        gp[n2] = ((long)(x + o[0]) * ny + (y + o[1])) * nz + (z + o[2]);
+                    }
+                    double J[3][3];
+                    for (int n1 = 0; n1 < 3; ++n1)
+                        for (int n2 = 0; n2 < 3; ++n2) J[n1][n2] = g[gp[n2] * 9 + n1 * 3 + n2];
+                    double alpha = 0.0;
+                    double det = det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0],
+                                      J[2][1], J[2][2]);
+                    int steps = 0;
+                    while (det > e2 || det < e1) {
+                        if (++steps > 11) { capped++; break; }
+                        alpha += 0.1;
+                        if (alpha > 1.0) alpha = 1.0;
+                        double Jn[3][3];
+                        for (int n1 = 0; n1 < 3; ++n1)
+                            for (int n2 = 0; n2 < 3; ++n2)
+                                Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                        det = det3(Jn[0][0], Jn[0][1], Jn[0][2], Jn[1][0], Jn[1][1], Jn[1][2],
+                                   Jn[2][0], Jn[2][1], Jn[2][2]);
+                    }
+                    alpha += 0.1;
+                    if (alpha > 1.0) alpha = 1.0;
+                    for (int n1 = 0; n1 < 3; ++n1)
+                        for (int n2 = 0; n2 < 3; ++n2)
+                            g[gp[n2] * 9 + n1 * 3 + n2] =
+                                (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                }
+    return capped;
+}
+
+/* complex DFT along one axis (FFTW sign convention: forward e^{-2 pi i jk/n}, unnormalised) */
+static void dft_axis(double *re, double *im, int n, long outer, long s, int sign) {
+    double *cs = (double *)malloc(sizeof(double) * n), *sn = (double *)malloc(sizeof(double) * n);
+    for (int m = 0; m < n; ++m) {
+        cs[m] = cos(2.0 * PI_D * m / n);
+        sn[m] = sin(2.0 * PI_D * m / n);
+    }
+    const int T = orc_get_threads();
+#pragma omp parallel num_threads(T)
+    {
+        double *ir = (double *)malloc(sizeof(double) * n), *ii = (double *)malloc(sizeof(double) * n);
+#pragma omp for schedule(static)
+        for (long o = 0; o < outer * s; ++o) {
+            const long b = (o / s) * (long)n * s + (o % s);
+            for (int j = 0; j < n; ++j) { ir[j] = re[b + j * s]; ii[j] = im[b + j * s]; }
+            for (int k = 0; k < n; ++k) {
+                double ar = 0.0, ai = 0.0;
+                for (int j = 0; j < n; ++j) {
+                    const int m = (int)(((long)j * k) % n);
+                    const double c = cs[m], sgn_s = sign * sn[m];
+                    ar += ir[j] * c - ii[j] * sgn_s;
+                    ai += ir[j] * sgn_s + ii[j] * c;
+                }
+                re[b + k * s] = ar;
+                im[b + k * s] = ai;
+            }
+        }
+        free(ir); free(ii);
+    }
+    free(cs); free(sn);
+}
+
+static void dft3(double *re, double *im, int nx, int ny, int nz, int sign) {
+    dft_axis(re, im, nz, (long)nx * ny, 1, sign);
+    dft_axis(re, im, ny, nx, nz, sign);
+    dft_axis(re, im, nx, 1, (long)ny * nz, sign);
+}
+
+/* :361-449: periodic Poisson integration of each component's gradient field, then rescale by
+ * the voxel size and restore the mean */
+void orc_integrate3d(double *pos, const double *g, int nx, int ny, int nz, const double vs[3],
+                     const double mean[3]) {
+    const long V = (long)nx * ny * nz;
+    double *re[3], *im[3];
+    for (int a = 0; a < 3; ++a) {
+        re[a] = (double *)malloc(sizeof(double) * V);
+        im[a] = (double *)malloc(sizeof(double) * V);
+    }
+    for (int n = 0; n < 3; ++n) {
+        for (int a = 0; a < 3; ++a) {
+            for (long p = 0; p < V; ++p) { re[a][p] = g[p * 9 + n * 3 + a]; im[a][p] = 0.0; }
+            dft3(re[a], im[a], nx, ny, nz, -1);
+        }
+        for (int x = 0; x < nx; ++x) {
+            const double cx = cos(2.0 * PI_D * x / (nx * 1.0)), sx = sin(2.0 * PI_D * x / (nx * 1.0));
+            for (int y = 0; y < ny; ++y) {
+                const double cy = cos(2.0 * PI_D * y / (ny * 1.0)), sy = sin(2.0 * PI_D * y / (ny * 1.0));
+                for (int z = 0; z < nz; ++z) {
+                    const double cz = cos(2.0 * PI_D * z / (nz * 1.0)), sz = sin(2.0 * PI_D * z / (nz * 1.0));
+                    const long p = ((long)x * ny + y) * nz + z;
+                    const double nrm = 6.0 - 2.0 * cz - 2.0 * cx - 2.0 * cy;
+                    if (fabs(nrm) > 1e-10) {
+                        const double dr = re[0][p] * (cx - 1) + im[0][p] * sx + re[1][p] * (cy - 1) +
+                                          im[1][p] * sy + re[2][p] * (cz - 1) + im[2][p] * sz;
+                        const double di = im[0][p] * (cx - 1) - re[0][p] * sx + im[1][p] * (cy - 1) -
+                                          re[1][p] * sy + im[2][p] * (cz - 1) - re[2][p] * sz;
+                        re[0][p] = dr / nrm;
+                        im[0][p] = di / nrm;
+                    } else {
+                        re[0][p] = 0.0;
+                        im[0][p] = 0.0;
+                    }
+                }
+            }
+        }
+        dft3(re[0], im[0], nx, ny, nz, +1);
+        for (long p = 0; p < V; ++p) pos[p * 3 + n] = re[0][p] / (nx * ny * nz * 1.0);
+    }
+    for (long p = 0; p < V; ++p)
+        for (int n = 0; n < 3; ++n) {
+            pos[p * 3 + n] *= vs[n];
+            pos[p * 3 + n] += mean[n];
+        }
+    for (int a = 0; a < 3; ++a) { free(re[a]); free(im[a]); }
+}
+
+static void minmax(const double *J, long V, double *mn, double *mx) {
+    double a = J[0], b = J[0];
+    for (long i = 1; i < V; ++i) {
+        if (J[i] < a) a = J[i];
+        if (J[i] > b) b = J[i];
+    }
+    *mn = a;
+    *mx = b;
+}
+
+/* :17-143 */
+int orc_topology3d(double *field, double e1, double e2, int max_outer, int max_inner,
+                   const double vs[3], int nx, int ny, int nz) {
+    const long V = (long)nx * ny * nz;
+    for (long p = 0; p < V; ++p)
+        for (int n = 0; n < 3; ++n) field[p * 3 + n] *= vs[n];
+    double *J = (double *)malloc(sizeof(double) * V);
+    orc_jacobian3d(field, nx, ny, nz, vs[0], vs[1], vs[2], J);
+    double jmin, jmax;
+    minmax(J, V, &jmin, &jmax);
+    int outer = 0;
+    if (!(jmin >= e1 && jmax <= e2)) {
+        const long cells = (long)(nx - 1) * (ny - 1) * (nz - 1);
+        double *Jc = (double *)malloc(sizeof(double) * (cells > 0 ? cells : 1) * 8);
+        double *g = (double *)malloc(sizeof(double) * V * 9);
+        while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+            int nb = 0, na = 0;
+            orc_corner_jacobians3d(field, nx, ny, nz, vs, e1, e2, Jc, &nb, &na);
+            int inner = 0;
+            while ((nb > 0 || na > 0) && inner < max_inner) {
+                orc_gradients3d(field, nx, ny, nz, vs, g);
+                orc_limit_gradients3d(g, Jc, nx, ny, nz, e1, e2);
+                double mean[3] = {0.0, 0.0, 0.0};
+                for (long p = 0; p < V; ++p)
+                    for (int n = 0; n < 3; ++n) mean[n] += field[p * 3 + n];
+                for (int n = 0; n < 3; ++n) mean[n] = mean[n] / (nx * ny * nz);
+                orc_integrate3d(field, g, nx, ny, nz, vs, mean);
+                orc_corner_jacobians3d(field, nx, ny, nz, vs, e1, e2, Jc, &nb, &na);
+                inner++;
+            }
+            orc_jacobian3d(field, nx, ny, nz, vs[0], vs[1], vs[2], J);
+            minmax(J, V, &jmin, &jmax);
+            outer++;
+        }
+        free(Jc);
+        free(g);
+    }
+    for (long p = 0; p < V; ++p)
+        for (int n = 0; n < 3; ++n) field[p * 3 + n] /= vs[n];
+    free(J);
+    return outer;
+}
+
+/* MI of the joint distribution given by a (soft) joint histogram */
+double orc_mutual_information(const double *h, int K, int L) {
+    double tot = 0.0;
+    for (long q = 0; q < (long)K * L; ++q) tot += h[q];
+    if (!(tot > 0.0)) return 0.0;
+    double *pk = (double *)calloc(K, sizeof(double)), *pl = (double *)calloc(L, sizeof(double));
+    for (int k = 0; k < K; ++k)
+        for (int l = 0; l < L; ++l) {
+            pk[k] += h[k * L + l] / tot;
+            pl[l] += h[k * L + l] / tot;
+        }
+    double mi = 0.0;
+    for (int k = 0; k < K; ++k)
+        for (int l = 0; l < L; ++l) {
+            const double p = h[k * L + l] / tot;
+            if (p > 0.0) mi += p * log(p / (pk[k] * pl[l]));
+        }
+    free(pk);
+    free(pl);
+    return mi;
+}

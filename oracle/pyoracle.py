@@ -1,0 +1,280 @@
+"""ctypes front end of the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle.so`` (the FP64 restatement in binder_oracle.c) and, when present,
+``oracle/_ref/libbinder_ref.so`` (the reference's own CPU sources built by oracle/Makefile).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs may import this module; the
+product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libbinder_ref.so")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+
+
+def build() -> None:
+    """Build the checkers in place (the reference build only where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+class _IterStats(C.Structure):
+    _fields_ = [("mll", C.c_double), ("log_prior_likelihood", C.c_double),
+                ("log_prior_transformation", C.c_double), ("mlp", C.c_double)]
+
+
+def _load_oracle():
+    if not os.path.exists(ORACLE_SO):
+        build()
+    lib = C.CDLL(ORACLE_SO)
+    i, d, ll, u64, u32 = C.c_int, C.c_double, C.c_longlong, C.c_uint64, C.c_uint32
+    lib.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+    lib.orc_spline3.argtypes = [d, _dp]
+    lib.orc_estep.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [_dp, _dp, C.POINTER(ll)]
+    lib.orc_estep.restype = d
+    lib.orc_estep_sample.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [u64, u32, u32, _dp, _dp]
+    lib.orc_estep_sample.restype = d
+    lib.orc_theta_map.argtypes = [_dp, i, i, d]
+    lib.orc_dirichlet_cost.argtypes = [_dp, i, i, d]
+    lib.orc_dirichlet_cost.restype = d
+    lib.orc_dirichlet_sample.argtypes = [_dp, i, i, d, u64, u32, u32]
+    lib.orc_dirichlet_sample.restype = i
+    lib.orc_gamma_sample.argtypes = [d, u64, u32, u32, u32, u32, C.POINTER(i)]
+    lib.orc_gamma_sample.restype = d
+    lib.orc_dct3.argtypes = [_dp, _dp, i, i, i, i]
+    lib.orc_smooth.argtypes = [_dp, _dp, _dp, _dp, d, i, i, i, _dp, i, u64, u32, u32,
+                               C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_smooth.restype = d
+    lib.orc_em.argtypes = [_dp, _dp, _ip, _ip, _dp, d, _dp, _dp, d] + [i] * 8 + \
+        [d, i, d, i, C.c_void_p]
+    lib.orc_em.restype = i
+    lib.orc_sampler.argtypes = [_dp, _dp, _dp, _ip, _ip, _dp, d, _dp, _dp, d, _dp, _dp] + \
+        [i] * 8 + [u64, u32, i, i, i, i, i, i, i, _dp, _dp]
+    lib.orc_sampler.restype = i
+    lib.orc_jacobian3d.argtypes = [_dp, i, i, i, d, d, d, _dp]
+    lib.orc_jacobian2d.argtypes = [_dp, i, i, d, d, _dp]
+    lib.orc_corner_jacobians3d.argtypes = [_dp, i, i, i, _dp, d, d, _dp, C.POINTER(i),
+                                           C.POINTER(i)]
+    lib.orc_gradients3d.argtypes = [_dp, i, i, i, _dp, _dp]
+    lib.orc_limit_gradients3d.argtypes = [_dp, _dp, i, i, i, d, d]
+    lib.orc_limit_gradients3d.restype = i
+    lib.orc_integrate3d.argtypes = [_dp, _dp, i, i, i, _dp, _dp]
+    lib.orc_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i]
+    lib.orc_topology3d.restype = i
+    lib.orc_mutual_information.argtypes = [_dp, i, i]
+    lib.orc_mutual_information.restype = d
+    lib.orc_set_threads.argtypes = [i]
+    lib.orc_get_threads.restype = i
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = _load_oracle()
+    return _LIB
+
+
+def ref_lib():
+    """The reference's own CPU sources (None when the prebuilt library is absent)."""
+    if not os.path.exists(REF_SO):
+        return None
+    r = C.CDLL(REF_SO)
+    i, d = C.c_int, C.c_double
+    r.ref_spline.argtypes = [i, d, _dp]
+    r.ref_jacobian3d.argtypes = [_dp, i, i, i, d, d, d, _dp]
+    r.ref_jacobian2d.argtypes = [_dp, i, i, d, d, _dp]
+    r.ref_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i, _dp]
+    r.ref_smooth_deformation.argtypes = [_dp, _dp, _dp, _dp, i, i, i, d, d, _dp, _dp]
+    r.ref_smooth_deformation.restype = d
+    r.ref_mi_update.argtypes = [d, _dp, _dp, i, i, _dp]
+    r.ref_mi_update.restype = d
+    r.ref_dirichlet_cost.argtypes = [d, _dp, i, i]
+    r.ref_dirichlet_cost.restype = d
+    return r
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _c32i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def philox(ctr, key):
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32_10(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
+    return out
+
+
+def spline3(d: float):
+    w = np.zeros(4)
+    lib().orc_spline3(float(d), w)
+    return w
+
+
+def estep(d, u, v, theta, vshape, nshape, K, L):
+    """EM E-step. Returns (mll, dream[V*N], hist[K*L], degenerate)."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    dream = np.zeros(nx * ny * nz * N)
+    hist = np.zeros(K * L)
+    deg = C.c_longlong(0)
+    mll = lib().orc_estep(_c64(d).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                          _c64(theta).ravel(), nx, ny, nz, *nshape, K, L, dream, hist,
+                          C.byref(deg))
+    return mll, dream, hist, deg.value
+
+
+def estep_sample(d, u, v, theta, vshape, nshape, K, L, seed, sweep, chain=0):
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    dream = np.zeros(nx * ny * nz * N)
+    hist = np.zeros(K * L)
+    mll = lib().orc_estep_sample(_c64(d).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                                 _c64(theta).ravel(), nx, ny, nz, *nshape, K, L, seed, sweep,
+                                 chain, dream, hist)
+    return mll, dream, hist
+
+
+def theta_map(hist, K, L, alpha):
+    th = _c64(hist).ravel().copy()
+    lib().orc_theta_map(th, K, L, float(alpha))
+    return th
+
+
+def dirichlet_cost(theta, K, L, alpha):
+    return lib().orc_dirichlet_cost(_c64(theta).ravel(), K, L, float(alpha))
+
+
+def dirichlet_sample(hist, K, L, alpha, seed, sweep, chain=0):
+    th = _c64(hist).ravel().copy()
+    capped = lib().orc_dirichlet_sample(th, K, L, float(alpha), seed, sweep, chain)
+    return th, capped
+
+
+def gamma_sample(shape, seed, index, sweep, tag, chain=0):
+    c = C.c_int(0)
+    g = lib().orc_gamma_sample(float(shape), seed, index, sweep, tag, chain, C.byref(c))
+    return g, c.value
+
+
+def dct3(x, inverse=False):
+    x = _c64(x)
+    out = np.zeros_like(x)
+    nx, ny, nz = x.shape
+    lib().orc_dct3(x.ravel(), out.ravel() if False else out.reshape(-1), nx, ny, nz, int(inverse))
+    return out
+
+
+def smooth(dream, voxel_pos, D, gamma, sigma, shape, noise=None, rho=None, eta=None,
+           want_raw=False):
+    """DCT-prior M-step. noise = (seed, sweep, chain) adds the sampling noise.
+    Returns (cost, final[V*N]) or (cost, final, raw_reg) when want_raw."""
+    nx, ny, nz = shape
+    N = 2 if nz == 1 else 3
+    out = np.zeros(nx * ny * nz * N)
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    raw = C.c_double(0.0)
+    rho_a = _c64(rho if rho is not None else [1, 1, 1])
+    eta_a = _c64(eta if eta is not None else [1, 1, 1])
+    seed, sweep, chain = noise if noise is not None else (0, 0, 0)
+    cost = lib().orc_smooth(_c64(dream).ravel(), _c64(voxel_pos).ravel(), _c64(D).ravel(), g,
+                            float(sigma), nx, ny, nz, out, int(noise is not None), seed, sweep,
+                            chain, rho_a.ctypes.data, eta_a.ctypes.data,
+                            C.addressof(raw) if want_raw else None)
+    if want_raw:
+        return cost, out, raw.value
+    return cost, out
+
+
+def em(final_locations, voxel_pos, u, v, theta, alpha, D, gamma, sigma, vshape, nshape, K, L,
+       non_zero_voxels, max_iter, convergence_th, update_theta=True):
+    """Full EM. Returns (iterations, final[V*N], theta[K*L], stats[iters, 4])."""
+    fl = _c64(final_locations).ravel().copy()
+    th = _c64(theta).ravel().copy()
+    stats = (_IterStats * max(1, max_iter))()
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    it = lib().orc_em(fl, _c64(voxel_pos).ravel(), _c32i(u).ravel(), _c32i(v).ravel(), th,
+                      float(alpha), _c64(D).ravel(), g, float(sigma), *vshape, *nshape, K, L,
+                      float(non_zero_voxels), int(max_iter), float(convergence_th),
+                      int(update_theta), C.addressof(stats))
+    st = np.array([[s.mll, s.log_prior_likelihood, s.log_prior_transformation, s.mlp]
+                   for s in stats[:it]])
+    return it, fl, th, st
+
+
+def sampler(final_locations, dream, voxel_pos, u, v, theta, alpha, D, gamma, sigma, rho, eta,
+            vshape, nshape, K, L, seed, N_b, N_s, sample_gamma=0, sample_gamma_every=1,
+            sample_posteriors=1, sample_likelihood_parameters=1,
+            sample_transformation_parameters=1, chain=0):
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    V = nx * ny * nz
+    fl = _c64(final_locations).ravel().copy()
+    dr = _c64(dream).ravel().copy()
+    th = _c64(theta).ravel().copy()
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    mean = np.zeros(V * N)
+    cov = np.zeros(V * N * N)
+    capped = lib().orc_sampler(fl, dr, _c64(voxel_pos).ravel(), _c32i(u).ravel(),
+                               _c32i(v).ravel(), th, float(alpha), _c64(D).ravel(), g,
+                               float(sigma), _c64(rho), _c64(eta), nx, ny, nz, *nshape, K, L,
+                               seed, chain, N_b, N_s, sample_gamma, sample_gamma_every,
+                               sample_posteriors, sample_likelihood_parameters,
+                               sample_transformation_parameters, mean, cov)
+    return mean, cov, fl, th, g, capped
+
+
+def jacobian3d(field, shape, vs=(1.0, 1.0, 1.0)):
+    nx, ny, nz = shape
+    J = np.zeros(nx * ny * nz)
+    lib().orc_jacobian3d(_c64(field).ravel(), nx, ny, nz, *map(float, vs), J)
+    return J
+
+
+def jacobian2d(field, shape, vs=(1.0, 1.0)):
+    nx, ny = shape
+    J = np.zeros(nx * ny)
+    lib().orc_jacobian2d(_c64(field).ravel(), nx, ny, *map(float, vs), J)
+    return J
+
+
+def corner_jacobians3d(pos, shape, vs, e1, e2):
+    nx, ny, nz = shape
+    Jc = np.zeros(max(1, (nx - 1) * (ny - 1) * (nz - 1)) * 8)
+    nb, na = C.c_int(0), C.c_int(0)
+    lib().orc_corner_jacobians3d(_c64(pos).ravel(), nx, ny, nz, _c64(vs), float(e1), float(e2),
+                                 Jc, C.byref(nb), C.byref(na))
+    return Jc, nb.value, na.value
+
+
+def topology3d(field, e1, e2, max_outer, max_inner, vs, shape):
+    f = _c64(field).ravel().copy()
+    outer = lib().orc_topology3d(f, float(e1), float(e2), int(max_outer), int(max_inner),
+                                 _c64(vs), *shape)
+    return f, outer
+
+
+def mutual_information(hist, K, L):
+    return lib().orc_mutual_information(_c64(hist).ravel(), K, L)

@@ -1,0 +1,79 @@
+// extern "C" entry points over the reference's own CPU classes, compiled from the unmodified
+// reference sources into oracle/_ref/libbinder_ref.so (test infrastructure: a checker only).
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "MILikelihood.h"
+#include "NonLinearTransformation.h"
+#include "Spline.h"
+#include "topology_correction_3D.h"
+#include "utils.h"
+
+extern "C" {
+
+// Spline::spline (BINDER/src/cpu/Spline.cpp:44-109)
+void ref_spline(int order, double d, double out[4]) {
+    Spline s(order, false);
+    const auto w = s.spline(d);
+    for (int i = 0; i < 4; ++i) out[i] = w[i];
+}
+
+// compute_jacobian_determinant_3D / _2D (BINDER/src/cpu/utils.cpp:10-345)
+void ref_jacobian3d(const double *field, int nx, int ny, int nz, double vx, double vy, double vz,
+                    double *J) {
+    const auto r = compute_jacobian_determinant_3D(field, nx, ny, nz, vx, vy, vz);
+    std::memcpy(J, r.data(), sizeof(double) * r.size());
+}
+
+void ref_jacobian2d(const double *field, int nx, int ny, double vx, double vy, double *J) {
+    const auto r = compute_jacobian_determinant_2D(field, nx, ny, vx, vy);
+    std::memcpy(J, r.data(), sizeof(double) * r.size());
+}
+
+// topology_correction_3D::correct_topology (BINDER/src/cpu/topology_correction_3D.cpp:17-143)
+void ref_topology3d(const double *field, double e1, double e2, int max_outer, int max_inner,
+                    const double *vs, int nx, int ny, int nz, double *out) {
+    topology_correction_3D tc;
+    const double *r = tc.correct_topology(field, e1, e2, max_outer, max_inner, 1, vs, nx, ny, nz);
+    std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * nz * 3);
+}
+
+// NonLinearTransformation::smooth_deformation (BINDER/src/cpu/NonLinearTransformation.cpp:226-278)
+double ref_smooth_deformation(const double gamma[3], const double rho[3], const double eta[3],
+                              const double *D, int nx, int ny, int nz, double sigma, double offset,
+                              const double *field, double *out) {
+    NonLinearTransformation t(gamma[0], gamma[1], gamma[2], rho[0], rho[1], rho[2], eta[0], eta[1],
+                              eta[2], D, nx, ny, nz, 1, sigma, offset);
+    auto [cost, ptr] = t.smooth_deformation(field);
+    const int N = nz == 1 ? 2 : 3;
+    std::memcpy(out, ptr, sizeof(double) * (size_t)nx * ny * nz * N);
+    delete[] ptr;
+    return cost;
+}
+
+// MILikelihood::update_parameters and compute_cost (BINDER/src/cpu/MILikelihood.cpp:33-124):
+// the histogram is fed through accumulate_info with a 1-D node grid of K nodes (node k has bin k)
+// and L voxels (voxel l has bin l).
+double ref_mi_update(double alpha, const double *theta_in, const double *hist, int K, int L,
+                     double *theta_out) {
+    std::vector<int> nodes(K), voxels(L);
+    for (int k = 0; k < K; ++k) nodes[k] = k;
+    for (int l = 0; l < L; ++l) voxels[l] = l;
+    MILikelihood mi(alpha, theta_in, 1, nodes.data(), voxels.data(), K, L, K, 1, 1, L, 1, 1);
+    mi.initialize_parameters();
+    for (int k = 0; k < K; ++k)
+        for (int l = 0; l < L; ++l) mi.accumulate_info(0, l, k, 0, 0, hist[k * L + l]);
+    mi.update_parameters();
+    const auto th = mi.get_parameters();
+    std::memcpy(theta_out, th.data(), sizeof(double) * K * L);
+    return mi.compute_cost();
+}
+
+double ref_dirichlet_cost(double alpha, const double *theta, int K, int L) {
+    std::vector<int> nodes(K, 0), voxels(L, 0);
+    MILikelihood mi(alpha, theta, 1, nodes.data(), voxels.data(), K, L, K, 1, 1, L, 1, 1);
+    return mi.compute_cost();
+}
+
+}  // extern "C"
