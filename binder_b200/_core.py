@@ -1,0 +1,236 @@
+"""Drop-in mirror of the reference's ``BINDER._core`` extension module on the B200 engine.
+
+Same classes, method names, keyword names and argument meaning as the pybind11 bindings of the
+reference (ste93ste/BINDER, BINDER/src/gpu/bindings.cpp:14-289, plus the CPU-only
+``compute_jacobian_determinant_3D`` of BINDER/src/cpu/bindings.cpp:564-593), so the reference's
+``FastRegistration`` and CLI can import this module in place of ``BINDER._core``.  Inputs of any
+float dtype are accepted (the CUDA backend force-casts to float32, the CPU backend to float64);
+positions and theta are computed in FP32, Welford moments, Jacobians and topology correction in
+FP64.  Errors raise ``BinderError`` (a RuntimeError), as the reference's std::runtime_error does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import BinderError, check, lib
+
+backend = "b200"
+has_topology_correction = True
+
+__all__ = ["backend", "has_topology_correction", "Registration", "NonLinearTransformation",
+           "topology_correction_3D", "compute_jacobian_determinant_3D", "BinderError"]
+
+
+def _f32(a, n=None, name="array"):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))
+    if n is not None and a.size != n:
+        raise ValueError(f"{name} has {a.size} elements, expected {n}")
+    return a
+
+
+def _f64(a, n=None, name="array"):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+    if n is not None and a.size != n:
+        raise ValueError(f"{name} has {a.size} elements, expected {n}")
+    return a
+
+
+def _i32(a, n=None, name="array"):
+    a = np.asarray(a)
+    if a.dtype.kind == "f":
+        a = a.astype(np.int32)  # pybind11 forcecast truncates float bins the same way
+    a = np.ascontiguousarray(a.astype(np.int32, copy=False).reshape(-1))
+    if n is not None and a.size != n:
+        raise ValueError(f"{name} has {a.size} elements, expected {n}")
+    return a
+
+
+class Registration:
+    """``_core.Registration`` (gpu/bindings.cpp:17-157)."""
+
+    def __init__(self, final_locations, threads, voxel_pos, node_pos, Nx_v, Ny_v, Nz_v, Nx_n,
+                 Ny_n, Nz_n, spline_order, non_zero_voxels):
+        self._h = C.c_void_p()
+        self._shape = (int(Nx_v), int(Ny_v), int(Nz_v))
+        self._nshape = (int(Nx_n), int(Ny_n), int(Nz_n))
+        V = int(Nx_v) * int(Ny_v) * int(Nz_v)
+        N = 2 if int(Nz_v) == 1 else 3
+        fl = _f32(final_locations, V * N, "final_locations")
+        vp = _f32(voxel_pos, V * N, "voxel_pos")
+        check(lib().binder_registration_create(C.byref(self._h), fl, int(threads), vp, None,
+                                               int(Nx_v), int(Ny_v), int(Nz_v), int(Nx_n),
+                                               int(Ny_n), int(Nz_n), int(spline_order),
+                                               float(non_zero_voxels)))
+        self._V = V
+        self._K = self._L = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().binder_registration_destroy(h)
+            self._h = C.c_void_p()
+
+    # -- set-up ------------------------------------------------------------------------------
+    def setMILikelihood(self, alpha, theta, K, L, threads, binned_nodes, binned_voxels):
+        K, L = int(K), int(L)
+        Vn = int(np.prod(self._nshape))
+        check(lib().binder_registration_set_mi_likelihood(
+            self._h, float(alpha), _f32(theta, K * L, "theta"), K, L, int(threads),
+            _i32(binned_nodes, Vn, "binned_nodes"), _i32(binned_voxels, self._V, "binned_voxels")))
+        self._K, self._L = K, L
+
+    def setNonLinearTransformation(self, gamma_x, gamma_y, gamma_z, voxels_size_x, voxels_size_y,
+                                   voxels_size_z, nodes_size_x, nodes_size_y, nodes_size_z, D):
+        check(lib().binder_registration_set_nonlinear_transformation(
+            self._h, float(gamma_x), float(gamma_y), float(gamma_z), float(voxels_size_x),
+            float(voxels_size_y), float(voxels_size_z), float(nodes_size_x), float(nodes_size_y),
+            float(nodes_size_z), _f32(D, self._V, "D")))
+
+    # -- hot path ----------------------------------------------------------------------------
+    def EM(self, max_EM_iterations, convergence_th, update_likelihood_parameters, debug):
+        it = C.c_int(0)
+        check(lib().binder_registration_em(self._h, int(max_EM_iterations), float(convergence_th),
+                                           int(update_likelihood_parameters), int(debug),
+                                           C.byref(it)))
+        return it.value
+
+    def sampler(self, seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
+                sample_likelihood_parameters, sample_transformation_parameters):
+        mean = np.zeros(self._V * 3, np.float64)
+        cov = np.zeros(self._V * 9, np.float64)
+        check(lib().binder_registration_sampler(
+            self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(N_b), int(N_s), int(sample_gamma),
+            int(sample_gamma_every), int(sample_posteriors), int(sample_likelihood_parameters),
+            int(sample_transformation_parameters), mean, cov))
+        return mean.reshape(*self._shape, 3), cov.reshape(*self._shape, 3, 3)
+
+    # -- getters / setters -------------------------------------------------------------------
+    def get_final_locations_as_numpy_array(self):
+        out = np.zeros(self._V * 3, np.float32)
+        check(lib().binder_registration_get_final_locations(self._h, out))
+        return out.reshape(*self._shape, 3)
+
+    def get_final_locations(self):
+        return self.get_final_locations_as_numpy_array().reshape(-1)
+
+    def get_dream_locations(self):
+        out = np.zeros(self._V * 3, np.float32)
+        check(lib().binder_registration_get_dream_locations(self._h, out))
+        return out
+
+    def set_dream_locations(self, dream_locations):
+        check(lib().binder_registration_set_dream_locations(
+            self._h, _f32(dream_locations, self._V * 3, "dream_locations")))
+
+    def get_likelihood_parameters(self):
+        if self._K is None:
+            raise BinderError(4, "setMILikelihood has not been called")
+        out = np.zeros(self._K * self._L, np.float32)
+        check(lib().binder_registration_get_likelihood_parameters(self._h, out))
+        return out
+
+    def get_shape(self):
+        out = np.zeros(4, np.int32)
+        check(lib().binder_registration_get_shape(self._h, out))
+        return [int(v) for v in out]
+
+    # -- additions (no reference counterpart) ------------------------------------------------
+    def iteration_stats(self, max_n=1 << 20):
+        """[n, 4] FP64 (mll, Dirichlet prior, deformation prior, min-log-posterior) per EM step."""
+        cap = max(1, int(max_n))
+        buf = np.zeros(cap * 4, np.float64)
+        n = C.c_int(0)
+        check(lib().binder_registration_get_iteration_stats(self._h, buf, cap, C.byref(n)))
+        return buf[: n.value * 4].reshape(n.value, 4)
+
+    def state(self):
+        g = np.zeros(3, np.float64)
+        nu = C.c_double(0)
+        deg = C.c_ulonglong(0)
+        fl = C.c_uint(0)
+        check(lib().binder_registration_get_state(self._h, g, C.byref(nu), C.byref(deg),
+                                                  C.byref(fl)))
+        return {"gamma": g, "nu": nu.value, "degenerate": deg.value, "flags": fl.value}
+
+    def last_elapsed_ms(self):
+        ms = C.c_double(0)
+        check(lib().binder_registration_last_elapsed_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def set_chain(self, chain):
+        check(lib().binder_registration_set_chain(self._h, int(chain)))
+
+
+class NonLinearTransformation:
+    """``_core.NonLinearTransformation`` (gpu/bindings.cpp:160-255)."""
+
+    def __init__(self, gamma_x, gamma_y, gamma_z, voxels_size_x, voxels_size_y, voxels_size_z,
+                 nodes_size_x, nodes_size_y, nodes_size_z, D, Nx_v, Ny_v, Nz_v, threads,
+                 sigma_spline, spline_offset):
+        self._h = C.c_void_p()
+        self._shape = (int(Nx_v), int(Ny_v), int(Nz_v))
+        self._V = int(np.prod(self._shape))
+        check(lib().binder_transform_create(
+            C.byref(self._h), float(gamma_x), float(gamma_y), float(gamma_z),
+            float(voxels_size_x), float(voxels_size_y), float(voxels_size_z), float(nodes_size_x),
+            float(nodes_size_y), float(nodes_size_z), _f32(D, self._V, "D"), int(Nx_v), int(Ny_v),
+            int(Nz_v), int(threads), float(sigma_spline), float(spline_offset)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().binder_transform_destroy(h)
+            self._h = C.c_void_p()
+
+    def get_shape(self):
+        out = np.zeros(4, np.int32)
+        check(lib().binder_transform_get_shape(self._h, out))
+        return [int(v) for v in out]
+
+    def smooth_deformation(self, deformation):
+        out = np.zeros(self._V * 3, np.float32)
+        cost = C.c_double(0)
+        check(lib().binder_transform_smooth_deformation(
+            self._h, _f32(deformation, self._V * 3, "deformation"), out, C.byref(cost)))
+        return cost.value, out.reshape(*self._shape, 3)
+
+    def sampleDeformationField(self, deformationField, number_of_samples):
+        n = int(number_of_samples)
+        out = np.zeros(max(n, 0) * self._V * 3, np.float32)
+        check(lib().binder_transform_sample_deformation_field(
+            self._h, _f32(deformationField, self._V * 3, "deformationField"), n, out))
+        return out.reshape(n, *self._shape, 3)
+
+
+class topology_correction_3D:
+    """``_core.topology_correction_3D`` (gpu/bindings.cpp:259-287); FP64 throughout."""
+
+    def __init__(self):
+        self.last_stats = None
+
+    def correct_topology(self, h_init, e1, e2, max_outer_it, max_it, threads, voxel_sizes, Nx_v,
+                         Ny_v, Nz_v):
+        V = int(Nx_v) * int(Ny_v) * int(Nz_v)
+        field = _f64(h_init, V * 3, "h_init")
+        out = np.zeros(V * 3, np.float64)
+        stats = np.zeros(6, np.int64)
+        check(lib().binder_topology_correct_3d(
+            field, float(e1), float(e2), int(max_outer_it), int(max_it), int(threads),
+            _f64(voxel_sizes, 3, "voxel_sizes"), int(Nx_v), int(Ny_v), int(Nz_v), out,
+            stats.ctypes.data))
+        self.last_stats = dict(zip(["outer_iterations", "inner_iterations", "below_e1_before",
+                                    "below_e1_after", "above_e2_before", "above_e2_after"],
+                                   stats.tolist()))
+        return out.reshape(int(Nx_v), int(Ny_v), int(Nz_v), 3)
+
+
+def compute_jacobian_determinant_3D(field, Nx, Ny, Nz, voxel_size_x, voxel_size_y, voxel_size_z):
+    """``_core.compute_jacobian_determinant_3D`` (cpu/bindings.cpp:564-593), FP64 on the GPU."""
+    V = int(Nx) * int(Ny) * int(Nz)
+    J = np.zeros(V, np.float64)
+    check(lib().binder_jacobian_determinant_3d(_f64(field, V * 3, "field"), int(Nx), int(Ny),
+                                               int(Nz), float(voxel_size_x), float(voxel_size_y),
+                                               float(voxel_size_z), J))
+    return J.reshape(int(Nx), int(Ny), int(Nz))

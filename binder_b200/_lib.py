@@ -1,0 +1,106 @@
+"""Loader for ``libbinder_b200.so`` (the sm_100a engine behind the C ABI in include/binder_b200.h).
+
+There is no fallback: if the library is missing or cannot be loaded, importing the package's
+compute entry points raises ImportError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libbinder_b200.so")
+
+STATUS_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "unsupported", 4: "not ready",
+                5: "device fault"}
+
+# every entry point declared in include/binder_b200.h
+EXPORTS = [
+    "binder_last_error", "binder_backend", "binder_has_topology_correction",
+    "binder_registration_create", "binder_registration_destroy",
+    "binder_registration_set_mi_likelihood", "binder_registration_set_nonlinear_transformation",
+    "binder_registration_em", "binder_registration_sampler",
+    "binder_registration_get_final_locations", "binder_registration_get_dream_locations",
+    "binder_registration_set_dream_locations", "binder_registration_get_likelihood_parameters",
+    "binder_registration_get_shape", "binder_registration_get_iteration_stats",
+    "binder_registration_get_state", "binder_registration_last_elapsed_ms",
+    "binder_registration_set_stream", "binder_registration_set_chain",
+    "binder_transform_create", "binder_transform_destroy",
+    "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
+    "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
+]
+
+
+class BinderError(RuntimeError):
+    """A non-zero status from the C ABI (the reference raises std::runtime_error here)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"binder_b200 {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64 = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_P = C.c_void_p
+_i, _d, _u32, _u64 = C.c_int, C.c_double, C.c_uint32, C.c_uint64
+
+
+def _declare(lib):
+    lib.binder_last_error.restype = C.c_char_p
+    lib.binder_backend.restype = C.c_char_p
+    lib.binder_has_topology_correction.restype = _i
+    sig = {
+        "binder_registration_create": [C.POINTER(_P), _f32, _i, _f32, _P] + [_i] * 7 + [_d],
+        "binder_registration_destroy": [_P],
+        "binder_registration_set_mi_likelihood": [_P, _d, _f32, _i, _i, _i, _i32, _i32],
+        "binder_registration_set_nonlinear_transformation": [_P] + [_d] * 9 + [_f32],
+        "binder_registration_em": [_P, _i, _d, _i, _i, C.POINTER(_i)],
+        "binder_registration_sampler": [_P, _u64, _i, _i, _i, _i, _i, _i, _i, _f64, _f64],
+        "binder_registration_get_final_locations": [_P, _f32],
+        "binder_registration_get_dream_locations": [_P, _f32],
+        "binder_registration_set_dream_locations": [_P, _f32],
+        "binder_registration_get_likelihood_parameters": [_P, _f32],
+        "binder_registration_get_shape": [_P, _i32],
+        "binder_registration_get_iteration_stats": [_P, _f64, _i, C.POINTER(_i)],
+        "binder_registration_get_state": [_P, _f64, C.POINTER(_d), C.POINTER(C.c_ulonglong),
+                                          C.POINTER(C.c_uint)],
+        "binder_registration_last_elapsed_ms": [_P, C.POINTER(_d)],
+        "binder_registration_set_stream": [_P, _P],
+        "binder_registration_set_chain": [_P, _u32],
+        "binder_transform_create": [C.POINTER(_P)] + [_d] * 9 + [_f32, _i, _i, _i, _i, _d, _d],
+        "binder_transform_destroy": [_P],
+        "binder_transform_smooth_deformation": [_P, _f32, _f32, C.POINTER(_d)],
+        "binder_transform_sample_deformation_field": [_P, _f32, _i, _f32],
+        "binder_transform_get_shape": [_P, _i32],
+        "binder_jacobian_determinant_3d": [_f64, _i, _i, _i, _d, _d, _d, _f64],
+        "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _i
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    """The loaded C library (ImportError when it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m binder_b200.build` "
+                "(the package has no CPU fallback)")
+        _LIB = _declare(C.CDLL(LIB_PATH))
+    return _LIB
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise BinderError(status, lib().binder_last_error().decode(errors="replace"))

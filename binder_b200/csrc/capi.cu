@@ -1,0 +1,317 @@
+// extern "C" boundary: status codes instead of exceptions, thread-local error text.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/binder_b200.h"
+#include "engine.cuh"
+
+struct binder_registration {
+    binder::Registration *impl;
+};
+struct binder_transform {
+    binder::PriorTransform *impl;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F &&f) {
+    try {
+        g_err.clear();
+        f();
+        return BINDER_STATUS_OK;
+    } catch (const binder::Error &e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g_err = "host allocation failed";
+        return BINDER_STATUS_CUDA_ERROR;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return BINDER_STATUS_CUDA_ERROR;
+    } catch (...) {
+        g_err = "unknown error";
+        return BINDER_STATUS_CUDA_ERROR;
+    }
+}
+
+#define NEED(p)                                                                              \
+    do {                                                                                     \
+        if (!(p)) throw binder::Error(BINDER_STATUS_INVALID_ARGUMENT, #p " must not be NULL"); \
+    } while (0)
+}  // namespace
+
+extern "C" {
+
+const char *binder_last_error(void) { return g_err.c_str(); }
+const char *binder_backend(void) { return "b200"; }
+int binder_has_topology_correction(void) { return 1; }
+
+int binder_registration_create(binder_registration **out, const float *final_locations,
+                               int threads, const float *voxel_pos, const float *node_pos,
+                               int Nx_v, int Ny_v, int Nz_v, int Nx_n, int Ny_n, int Nz_n,
+                               int spline_order, double non_zero_voxels) {
+    (void)threads;
+    (void)node_pos;
+    return guard([&] {
+        NEED(out);
+        NEED(final_locations);
+        NEED(voxel_pos);
+        *out = nullptr;
+        auto *impl = new binder::Registration(final_locations, voxel_pos, Nx_v, Ny_v, Nz_v, Nx_n,
+                                              Ny_n, Nz_n, spline_order, non_zero_voxels);
+        *out = new binder_registration{impl};
+    });
+}
+
+int binder_registration_destroy(binder_registration *h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->impl;
+        delete h;
+    });
+}
+
+int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, const float *theta,
+                                          int K, int L, int threads, const int32_t *binned_nodes,
+                                          const int32_t *binned_voxels) {
+    (void)threads;
+    return guard([&] {
+        NEED(h);
+        NEED(theta);
+        NEED(binned_nodes);
+        NEED(binned_voxels);
+        h->impl->set_mi_likelihood(alpha, theta, K, L, binned_nodes, binned_voxels);
+    });
+}
+
+int binder_registration_set_nonlinear_transformation(binder_registration *h, double gamma_x,
+                                                     double gamma_y, double gamma_z,
+                                                     double voxels_size_x, double voxels_size_y,
+                                                     double voxels_size_z, double nodes_size_x,
+                                                     double nodes_size_y, double nodes_size_z,
+                                                     const float *D) {
+    return guard([&] {
+        NEED(h);
+        NEED(D);
+        const double g[3] = {gamma_x, gamma_y, gamma_z};
+        const double rho[3] = {voxels_size_x, voxels_size_y, voxels_size_z};
+        const double eta[3] = {nodes_size_x, nodes_size_y, nodes_size_z};
+        h->impl->set_nonlinear_transformation(g, rho, eta, D);
+    });
+}
+
+int binder_registration_em(binder_registration *h, int max_iterations, double convergence_th,
+                           int update_likelihood_parameters, int debug, int *iterations_out) {
+    return guard([&] {
+        NEED(h);
+        const int it = h->impl->em(max_iterations, convergence_th, update_likelihood_parameters, debug);
+        if (iterations_out) *iterations_out = it;
+    });
+}
+
+int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, int N_s,
+                                int sample_gamma, int sample_gamma_every, int sample_posteriors,
+                                int sample_likelihood_parameters,
+                                int sample_transformation_parameters, double *mean_out,
+                                double *cov_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(mean_out);
+        NEED(cov_out);
+        h->impl->sampler(seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
+                         sample_likelihood_parameters, sample_transformation_parameters, mean_out,
+                         cov_out);
+    });
+}
+
+int binder_registration_get_final_locations(const binder_registration *h, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_final_locations(out);
+    });
+}
+
+int binder_registration_get_dream_locations(const binder_registration *h, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_dream_locations(out);
+    });
+}
+
+int binder_registration_set_dream_locations(binder_registration *h, const float *in) {
+    return guard([&] {
+        NEED(h);
+        NEED(in);
+        h->impl->set_dream_locations(in);
+    });
+}
+
+int binder_registration_get_likelihood_parameters(const binder_registration *h, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_likelihood_parameters(out);
+    });
+}
+
+int binder_registration_get_shape(const binder_registration *h, int out[4]) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_shape(out);
+    });
+}
+
+int binder_registration_get_iteration_stats(const binder_registration *h, double *out, int max_n,
+                                            int *n_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        const int n = h->impl->get_iteration_stats(out, max_n);
+        if (n_out) *n_out = n;
+    });
+}
+
+int binder_registration_get_state(const binder_registration *h, double gamma_out[3],
+                                  double *nu_out, unsigned long long *degenerate_out,
+                                  unsigned *flags_out) {
+    return guard([&] {
+        NEED(h);
+        h->impl->get_state(gamma_out, nu_out, degenerate_out, flags_out);
+    });
+}
+
+int binder_registration_last_elapsed_ms(const binder_registration *h, double *ms_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(ms_out);
+        *ms_out = h->impl->last_elapsed_ms();
+    });
+}
+
+int binder_registration_set_stream(binder_registration *h, void *cuda_stream) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_stream(reinterpret_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int binder_registration_set_chain(binder_registration *h, uint32_t chain) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_chain(chain);
+    });
+}
+
+int binder_transform_create(binder_transform **out, double gamma_x, double gamma_y,
+                            double gamma_z, double voxels_size_x, double voxels_size_y,
+                            double voxels_size_z, double nodes_size_x, double nodes_size_y,
+                            double nodes_size_z, const float *D, int Nx_v, int Ny_v, int Nz_v,
+                            int threads, double sigma_spline, double spline_offset) {
+    (void)threads;
+    (void)spline_offset;
+    return guard([&] {
+        NEED(out);
+        NEED(D);
+        *out = nullptr;
+        const double g[3] = {gamma_x, gamma_y, gamma_z};
+        const double rho[3] = {voxels_size_x, voxels_size_y, voxels_size_z};
+        const double eta[3] = {nodes_size_x, nodes_size_y, nodes_size_z};
+        auto *impl = new binder::PriorTransform(g, rho, eta, D, Nx_v, Ny_v, Nz_v, sigma_spline);
+        *out = new binder_transform{impl};
+    });
+}
+
+int binder_transform_destroy(binder_transform *h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->impl;
+        delete h;
+    });
+}
+
+int binder_transform_smooth_deformation(binder_transform *h, const float *field, float *out,
+                                        double *log_prior_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(field);
+        NEED(out);
+        const double c = h->impl->smooth(field, out);
+        if (log_prior_out) *log_prior_out = c;
+    });
+}
+
+int binder_transform_sample_deformation_field(binder_transform *h, const float *field,
+                                              int number_of_samples, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(field);
+        NEED(out);
+        h->impl->sample(field, number_of_samples, out);
+    });
+}
+
+int binder_transform_get_shape(const binder_transform *h, int out[4]) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_shape(out);
+    });
+}
+
+int binder_jacobian_determinant_3d(const double *field, int Nx, int Ny, int Nz, double voxel_size_x,
+                                   double voxel_size_y, double voxel_size_z, double *J_out) {
+    return guard([&] {
+        NEED(field);
+        NEED(J_out);
+        BINDER_CHECK(Nx > 0 && Ny > 0 && Nz > 0, "dimensions must be positive");
+        const long V = (long)Nx * Ny * Nz;
+        double *df = nullptr, *dj = nullptr;
+        BINDER_CUDA(cudaMalloc(&df, sizeof(double) * V * 3));
+        try {
+            BINDER_CUDA(cudaMalloc(&dj, sizeof(double) * V));
+            BINDER_CUDA(cudaMemcpy(df, field, sizeof(double) * V * 3, cudaMemcpyHostToDevice));
+            const double vs[3] = {voxel_size_x, voxel_size_y, voxel_size_z};
+            binder::jacobian3d_device(df, Nx, Ny, Nz, vs, dj, 0);
+            BINDER_CUDA(cudaMemcpy(J_out, dj, sizeof(double) * V, cudaMemcpyDeviceToHost));
+        } catch (...) {
+            cudaFree(df);
+            cudaFree(dj);
+            throw;
+        }
+        cudaFree(df);
+        cudaFree(dj);
+    });
+}
+
+int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
+                               int max_it, int threads, const double voxel_sizes[3], int Nx,
+                               int Ny, int Nz, double *out, long long *stats_out) {
+    (void)threads;
+    return guard([&] {
+        NEED(field);
+        NEED(voxel_sizes);
+        NEED(out);
+        BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
+                     "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
+        const long V = (long)Nx * Ny * Nz;
+        if (out != field) std::memcpy(out, field, sizeof(double) * V * 3);
+        const auto r = binder::topology_correct_3d(out, e1, e2, max_outer_it, max_it, voxel_sizes,
+                                                   Nx, Ny, Nz, 0);
+        if (stats_out) {
+            stats_out[0] = r.outer_iterations;
+            stats_out[1] = r.inner_iterations;
+            stats_out[2] = r.below_before;
+            stats_out[3] = r.below_after;
+            stats_out[4] = r.above_before;
+            stats_out[5] = r.above_after;
+        }
+    });
+}
+
+}  // extern "C"

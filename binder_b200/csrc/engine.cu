@@ -1,0 +1,612 @@
+// Registration / sampling engines: device buffers, CUDA-graph-captured iteration chunks and the
+// device-side convergence test of the EM loop (BINDER/src/cpu/Registration.cpp:122-217,
+// :515-642; BINDER/src/gpu/Registration.cu:839-1026).
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace binder {
+
+namespace {
+
+template <typename T>
+T *dalloc(size_t n) {
+    T *p = nullptr;
+    if (n) BINDER_CUDA(cudaMalloc(&p, n * sizeof(T)));
+    return p;
+}
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+bool verbose() {
+    const char *v = std::getenv("BINDER_B200_VERBOSE");
+    return v && v[0] && v[0] != '0';
+}
+
+// the B-spline prior's standard deviation for cubic splines, sqrt(9 / (8 pi))
+// (BINDER/src/cpu/Spline.cpp:22)
+constexpr double kSigmaCubic2 = 9.0 / (8.0 * 3.14159265358979323846);
+
+struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~Graph() {
+        if (e) cudaGraphExecDestroy(e);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+}  // namespace
+
+void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa) {
+    soa.resize((size_t)V * N);
+    for (long i = 0; i < V; ++i)
+        for (int n = 0; n < N; ++n) soa[(size_t)n * V + i] = aos[i * N + n];
+}
+
+void soa_to_aos(const float *soa, long V, int N, float *aos) {
+    for (long i = 0; i < V; ++i)
+        for (int n = 0; n < N; ++n) aos[i * N + n] = soa[(size_t)n * V + i];
+}
+
+// ------------------------------------------------------------------------------------------
+void DctSet::init(int nx, int ny, int nz) {
+    const int dims[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        const int m = dims[a];
+        n[a] = m;
+        std::vector<double> C((size_t)m * m);
+        dct2_matrix(m, C.data());
+        std::vector<float> F((size_t)m * m), I((size_t)m * m);
+        for (int k = 0; k < m; ++k)
+            for (int j = 0; j < m; ++j) {
+                F[(size_t)k * m + j] = (float)C[(size_t)k * m + j];
+                I[(size_t)j * m + k] = (float)C[(size_t)k * m + j];
+            }
+        fwd[a] = dalloc<float>((size_t)m * m);
+        inv[a] = dalloc<float>((size_t)m * m);
+        BINDER_CUDA(cudaMemcpy(fwd[a], F.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
+        BINDER_CUDA(cudaMemcpy(inv[a], I.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
+    }
+}
+
+void DctSet::release() {
+    for (int a = 0; a < 3; ++a) {
+        dfree(fwd[a]);
+        dfree(inv[a]);
+    }
+}
+
+void MStep::init(int x, int y, int z) {
+    nx = x; ny = y; nz = z;
+    V = (long)x * y * z;
+    dct.init(x, y, z);
+    t1 = dalloc<float>((size_t)V * 3);
+    t2 = dalloc<float>((size_t)V * 3);
+}
+
+void MStep::release() {
+    dct.release();
+    dfree(t1);
+    dfree(t2);
+}
+
+void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
+                    double sigma2, int sample, int want_raw, int every, uint64_t seed,
+                    uint32_t chain, double rho_p, const double eta2[3], const int *skip,
+                    cudaStream_t s) {
+    AxisArgs<float> a{};
+    a.comp_stride = V;
+    a.st = st;
+    a.skip = skip;
+    a.ny = ny;
+    a.nz = nz;
+    // forward DCT-II along z, y
+    a.in = r; a.out = t1; a.M = dct.fwd[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+    launch_axis_pass(a, kEpiNone, 3, s);
+    a.in = t1; a.out = t2; a.M = dct.fwd[1]; a.n = ny; a.outer = nx; a.s = nz;
+    launch_axis_pass(a, kEpiNone, 3, s);
+    // x: forward, prior scaling (+ noise, costs), inverse
+    a.in = t2; a.out = t1; a.M = dct.fwd[0]; a.M2 = dct.inv[0]; a.n = nx; a.outer = 1;
+    a.s = (long)ny * nz;
+    a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
+    a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
+    for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
+    launch_axis_pass(a, kEpiSpectral, 3, s);
+    // inverse DCT-III along y, z; the last pass adds the voxel positions
+    a.in = t1; a.out = t2; a.M = dct.inv[1]; a.M2 = nullptr; a.n = ny; a.outer = nx; a.s = nz;
+    launch_axis_pass(a, kEpiNone, 3, s);
+    a.in = t2; a.out = d; a.M = dct.inv[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+    a.xpos = xpos;
+    launch_axis_pass(a, kEpiPositions, 3, s);
+}
+
+// ------------------------------------------------------------------------------------------
+Registration::Registration(const float *final_locations, const float *voxel_pos, int nx, int ny,
+                           int nz, int nxn, int nyn, int nzn, int spline_order,
+                           double non_zero_voxels)
+    : nx_(nx), ny_(ny), nz_(nz), nxn_(nxn), nyn_(nyn), nzn_(nzn) {
+    BINDER_CHECK(nx > 0 && ny > 0 && nz > 0 && nxn > 0 && nyn > 0 && nzn > 0,
+                 "grid dimensions must be positive");
+    if (nz == 1)
+        throw Error(kUnsupported, "2D registration (Nz_v == 1) is not built on the GPU path");
+    if (spline_order != 3)
+        throw Error(kUnsupported, "only cubic B-splines (spline_order = 3) are built");
+    BINDER_CHECK((long)nx * ny * nz < (1L << 31), "volume too large");
+    N_ = 3;
+    V_ = (long)nx * ny * nz;
+    Vn_ = (long)nxn * nyn * nzn;
+    nzv_ = non_zero_voxels;
+    BINDER_CUDA(cudaStreamCreate(&own_stream_));
+    stream_ = own_stream_;
+    d_ = dalloc<float>((size_t)V_ * 3);
+    r_ = dalloc<float>((size_t)V_ * 3);
+    st_ = dalloc<DevState>(1);
+    BINDER_CUDA(cudaMemset(st_, 0, sizeof(DevState)));
+    std::vector<float> soa;
+    aos_to_soa(final_locations, V_, 3, soa);
+    BINDER_CUDA(cudaMemcpy(d_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    // the identity voxel grid (the common case) is recomputed in the kernels instead of read
+    bool identity = true;
+    for (long i = 0; i < V_ && identity; ++i) {
+        const float e[3] = {(float)(i / ((long)ny * nz)), (float)((i / nz) % ny), (float)(i % nz)};
+        for (int n = 0; n < 3; ++n) identity &= (voxel_pos[i * 3 + n] == e[n]);
+    }
+    if (!identity) {
+        aos_to_soa(voxel_pos, V_, 3, soa);
+        x_ = dalloc<float>((size_t)V_ * 3);
+        BINDER_CUDA(cudaMemcpy(x_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    }
+    std::vector<float> zeros((size_t)V_ * 3, 0.0f);
+    set_dream_locations(zeros.data());
+    mstep_.init(nx, ny, nz);
+}
+
+Registration::~Registration() {
+    cudaDeviceSynchronize();
+    if (own_stream_) cudaStreamDestroy(own_stream_);
+    dfree(d_); dfree(x_); dfree(r_); dfree(D_); dfree(theta_); dfree(hist_); dfree(hcnt_);
+    dfree(u_); dfree(vpad_); dfree(mean_); dfree(m2_); dfree(stats_); dfree(st_);
+    mstep_.release();
+}
+
+void Registration::set_mi_likelihood(double alpha, const float *theta, int K, int L,
+                                     const int *binned_nodes, const int *binned_voxels) {
+    BINDER_CHECK(K >= 1 && K <= 256 && L >= 1 && L <= 256,
+                 "numbers of bins K and L must be in [1, 256]");
+    BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
+    std::vector<uint8_t> u((size_t)V_);
+    for (long i = 0; i < V_; ++i) {
+        const int b = binned_voxels[i];
+        if (b < 0 || b >= L)
+            throw Error(kInvalidArgument, "binned_voxels value " + std::to_string(b) +
+                                              " outside [0, L) at voxel " + std::to_string(i));
+        u[i] = (uint8_t)b;
+    }
+    P_ = 8;
+    PZ_ = 8;
+    pyn_ = nyn_ + 2 * P_;
+    zp_ = ((nzn_ + 2 * PZ_ + 3) / 4) * 4 + 4;
+    const size_t padded = (size_t)(nxn_ + 2 * P_) * pyn_ * zp_;
+    std::vector<uint8_t> vp(padded, 0);
+    for (int x = 0; x < nxn_; ++x)
+        for (int y = 0; y < nyn_; ++y)
+            for (int z = 0; z < nzn_; ++z) {
+                const long j = ((long)x * nyn_ + y) * nzn_ + z;
+                const int b = binned_nodes[j];
+                if (b < 0 || b >= K)
+                    throw Error(kInvalidArgument, "binned_nodes value " + std::to_string(b) +
+                                                      " outside [0, K) at node " + std::to_string(j));
+                vp[((size_t)(x + P_) * pyn_ + (y + P_)) * zp_ + (z + PZ_)] = (uint8_t)b;
+            }
+    dfree(u_); dfree(vpad_); dfree(theta_); dfree(hist_); dfree(hcnt_);
+    u_ = dalloc<uint8_t>((size_t)V_);
+    vpad_ = dalloc<uint8_t>(padded);
+    theta_ = dalloc<float>((size_t)K * L);
+    hist_ = dalloc<float>((size_t)K * L);
+    hcnt_ = dalloc<unsigned>((size_t)K * L);
+    BINDER_CUDA(cudaMemcpy(u_, u.data(), V_, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpy(vpad_, vp.data(), padded, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpy(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemset(hist_, 0, sizeof(float) * K * L));
+    BINDER_CUDA(cudaMemset(hcnt_, 0, sizeof(unsigned) * K * L));
+    K_ = K;
+    L_ = L;
+    alpha_ = alpha;
+    egrid_e_ = estep_grid(false, K, L, V_);
+    egrid_s_ = estep_grid(true, K, L, V_);
+    have_mi_ = true;
+}
+
+void Registration::set_nonlinear_transformation(const double gamma[3], const double rho[3],
+                                                const double eta[3], const float *D) {
+    for (int n = 0; n < 3; ++n) {
+        gamma0_[n] = gamma[n];
+        rho_[n] = rho[n];
+        eta_[n] = eta[n];
+    }
+    dfree(D_);
+    D_ = dalloc<float>((size_t)V_);
+    BINDER_CUDA(cudaMemcpy(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice));
+    sigma2_ = kSigmaCubic2;
+    have_tr_ = true;
+}
+
+void Registration::require_ready() const {
+    if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
+}
+
+void Registration::reset_state(bool for_sampler) {
+    DevState h{};
+    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    h.mll = h.lp_lik = h.lp_tr = h.raw_reg = 0.0;
+    h.mlp_old = 1e100;
+    for (int n = 0; n < 3; ++n) h.gamma[n] = gamma0_[n];
+    const double rp = rho_[0] * rho_[1] * rho_[2];
+    h.nu = gamma0_[0] / (rp * eta_[0] * eta_[0] * (double)V_);  // NonLinearTransformation.cpp:43
+    h.degenerate = 0;
+    h.done = 0;
+    h.iter = 0;
+    h.flags = 0;
+    h.sweep = 0;
+    (void)for_sampler;
+    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+}
+
+void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
+    EStepArgs e{};
+    e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_; e.hist = hist_;
+    e.hcnt = hcnt_; e.st = st_; e.skip = &st_->done; e.V = V_;
+    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
+    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
+    e.seed = seed_; e.chain = chain_;
+    launch_estep(e, false, egrid_e_, stream_);
+    launch_theta_update(theta_, hist_, K_, L_, alpha_, update, st_, stream_);
+    const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+    mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
+                   rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, stream_);
+    launch_em_finish(st_, stats_, max_iter, th, nzv_, stream_);
+}
+
+int Registration::em(int max_iterations, double convergence_th, int update, int debug) {
+    require_ready();
+    if (max_iterations <= 0) return 0;
+    if (stats_cap_ < max_iterations) {
+        dfree(stats_);
+        stats_ = dalloc<double>((size_t)max_iterations * 4);
+        stats_cap_ = max_iterations;
+    }
+    BINDER_CUDA(cudaMemset(stats_, 0, sizeof(double) * 4 * max_iterations));
+    reset_state(false);
+    BINDER_CUDA(cudaDeviceSynchronize());
+
+    cudaEvent_t t0, t1;
+    BINDER_CUDA(cudaEventCreate(&t0));
+    BINDER_CUDA(cudaEventCreate(&t1));
+    const int chunk = max_iterations < 8 ? max_iterations : 8;
+    Graph graph;
+    BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    try {
+        for (int c = 0; c < chunk; ++c) enqueue_em_iteration(max_iterations, convergence_th, update);
+    } catch (...) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(stream_, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    BINDER_CUDA(cudaStreamEndCapture(stream_, &graph.g));
+    BINDER_CUDA(cudaGraphInstantiate(&graph.e, graph.g, 0));
+
+    BINDER_CUDA(cudaEventRecord(t0, stream_));
+    DevState h{};
+    int launched = 0;
+    while (true) {
+        BINDER_CUDA(cudaGraphLaunch(graph.e, stream_));
+        launched += chunk;
+        BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+        BINDER_CUDA(cudaStreamSynchronize(stream_));
+        if (h.done || launched >= max_iterations) break;
+    }
+    BINDER_CUDA(cudaEventRecord(t1, stream_));
+    BINDER_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    last_ms_ = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    iters_done_ = h.iter;
+    if (debug || verbose()) {
+        std::vector<double> s((size_t)h.iter * 4);
+        if (h.iter)
+            BINDER_CUDA(cudaMemcpy(s.data(), stats_, sizeof(double) * 4 * h.iter,
+                                   cudaMemcpyDeviceToHost));
+        for (int it = 0; it < h.iter; ++it)
+            std::printf("Iteration %d: mll %.8f  prior(theta) %.8f  prior(T) %.8f  mlp %.8f  "
+                        "mlp/voxel %.8f\n",
+                        it + 1, s[it * 4 + 0], s[it * 4 + 1], s[it * 4 + 2], s[it * 4 + 3],
+                        s[it * 4 + 3] / nzv_);
+        std::printf("EM: %d iterations in %.3f ms\n", h.iter, ms);
+    }
+    return h.iter;
+}
+
+void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
+                           int sample_gamma_every, int sample_posteriors,
+                           int sample_likelihood_parameters, int sample_transformation_parameters,
+                           double *mean_out, double *cov_out) {
+    if (sample_posteriors || sample_likelihood_parameters) {
+        if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    }
+    if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
+    BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
+    BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
+    seed_ = seed;
+    dfree(mean_);
+    dfree(m2_);
+    mean_ = dalloc<double>((size_t)V_ * 3);
+    m2_ = dalloc<double>((size_t)V_ * 6);
+    BINDER_CUDA(cudaMemset(mean_, 0, sizeof(double) * V_ * 3));
+    BINDER_CUDA(cudaMemset(m2_, 0, sizeof(double) * V_ * 6));
+    reset_state(true);
+    const int total = N_b + N_s;
+    if (total > 0) {
+        const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+        const double rho_p = rho_[0] * rho_[1] * rho_[2];
+        const int every = sample_gamma_every < 1 ? 1 : sample_gamma_every;
+        const int chunk = total < 16 ? total : 16;
+        BINDER_CUDA(cudaDeviceSynchronize());
+        Graph graph;
+        BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+        try {
+            for (int c = 0; c < chunk; ++c) {
+                if (sample_posteriors) {
+                    EStepArgs e{};
+                    e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_;
+                    e.hist = hist_; e.hcnt = hcnt_; e.st = st_; e.skip = &st_->done; e.V = V_;
+                    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
+                    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
+                    e.seed = seed_; e.chain = chain_;
+                    launch_estep(e, true, egrid_s_, stream_);
+                }
+                if (sample_likelihood_parameters)
+                    launch_dirichlet_sample(theta_, hcnt_, K_, L_, alpha_, seed_, chain_, st_,
+                                            stream_);
+                if (sample_transformation_parameters) {
+                    mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 1, sample_gamma, every, seed_,
+                                   chain_, rho_p, eta2, &st_->done, stream_);
+                    if (sample_gamma)
+                        launch_nu_sample(st_, sample_gamma, every, N_, V_, rho_p, eta2, seed_,
+                                         chain_, stream_);
+                }
+                launch_sweep_end(d_, mean_, m2_, V_, N_b, total, st_, stream_);
+            }
+        } catch (...) {
+            cudaGraph_t g;
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        BINDER_CUDA(cudaStreamEndCapture(stream_, &graph.g));
+        BINDER_CUDA(cudaGraphInstantiate(&graph.e, graph.g, 0));
+        cudaEvent_t t0, t1;
+        BINDER_CUDA(cudaEventCreate(&t0));
+        BINDER_CUDA(cudaEventCreate(&t1));
+        BINDER_CUDA(cudaEventRecord(t0, stream_));
+        for (int done = 0; done < total; done += chunk) BINDER_CUDA(cudaGraphLaunch(graph.e, stream_));
+        BINDER_CUDA(cudaEventRecord(t1, stream_));
+        BINDER_CUDA(cudaEventSynchronize(t1));
+        float ms = 0.0f;
+        BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+        last_ms_ = ms;
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (verbose()) std::printf("sampler: %d sweeps in %.3f ms\n", total, ms);
+    }
+    DevState h{};
+    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    for (int n = 0; n < 3; ++n) gamma0_[n] = h.gamma[n];  // the prior keeps sampled gammas
+    std::vector<double> mean((size_t)V_ * 3), m2((size_t)V_ * 6);
+    BINDER_CUDA(cudaMemcpy(mean.data(), mean_, sizeof(double) * V_ * 3, cudaMemcpyDeviceToHost));
+    BINDER_CUDA(cudaMemcpy(m2.data(), m2_, sizeof(double) * V_ * 6, cudaMemcpyDeviceToHost));
+    const double inv = 1.0 / (double)(N_s - 1);
+    static const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (long i = 0; i < V_; ++i) {
+        for (int n = 0; n < 3; ++n) mean_out[i * 3 + n] = mean[(size_t)n * V_ + i];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                cov_out[i * 9 + r * 3 + c] = m2[(size_t)sym[r][c] * V_ + i] * inv;
+    }
+}
+
+void Registration::get_final_locations(float *out) const {
+    std::vector<float> soa((size_t)V_ * 3);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpy(soa.data(), d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
+    soa_to_aos(soa.data(), V_, 3, out);
+}
+
+void Registration::set_final_locations(const float *in) {
+    std::vector<float> soa;
+    aos_to_soa(in, V_, 3, soa);
+    BINDER_CUDA(cudaMemcpy(d_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+}
+
+void Registration::get_dream_locations(float *out) const {
+    std::vector<float> r((size_t)V_ * 3), x;
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpy(r.data(), r_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
+    if (x_) {
+        x.resize((size_t)V_ * 3);
+        BINDER_CUDA(cudaMemcpy(x.data(), x_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
+    }
+    for (long i = 0; i < V_; ++i) {
+        const float e[3] = {(float)(i / ((long)ny_ * nz_)), (float)((i / nz_) % ny_), (float)(i % nz_)};
+        for (int n = 0; n < 3; ++n)
+            out[i * 3 + n] = r[(size_t)n * V_ + i] + (x_ ? x[(size_t)n * V_ + i] : e[n]);
+    }
+}
+
+void Registration::set_dream_locations(const float *in) {
+    std::vector<float> soa((size_t)V_ * 3), x;
+    if (x_) {
+        x.resize((size_t)V_ * 3);
+        BINDER_CUDA(cudaMemcpy(x.data(), x_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
+    }
+    for (long i = 0; i < V_; ++i) {
+        const float e[3] = {(float)(i / ((long)ny_ * nz_)), (float)((i / nz_) % ny_), (float)(i % nz_)};
+        for (int n = 0; n < 3; ++n)
+            soa[(size_t)n * V_ + i] = in[i * 3 + n] - (x_ ? x[(size_t)n * V_ + i] : e[n]);
+    }
+    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+}
+
+void Registration::get_likelihood_parameters(float *out) const {
+    if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpy(out, theta_, sizeof(float) * K_ * L_, cudaMemcpyDeviceToHost));
+}
+
+void Registration::get_shape(int out[4]) const {
+    out[0] = nx_; out[1] = ny_; out[2] = nz_; out[3] = N_;
+}
+
+int Registration::get_iteration_stats(double *out, int max_n) const {
+    const int n = iters_done_ < max_n ? iters_done_ : max_n;
+    if (n > 0 && stats_)
+        BINDER_CUDA(cudaMemcpy(out, stats_, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+    return n;
+}
+
+void Registration::get_state(double *gamma_out, double *nu_out, unsigned long long *degenerate,
+                             unsigned *flags) const {
+    DevState h{};
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    if (gamma_out)
+        for (int n = 0; n < 3; ++n) gamma_out[n] = h.gamma[n];
+    if (nu_out) *nu_out = h.nu;
+    if (degenerate) *degenerate = h.degenerate;
+    if (flags) *flags = h.flags;
+}
+
+// ------------------------------------------------------------------------------------------
+PriorTransform::PriorTransform(const double gamma[3], const double rho[3], const double eta[3],
+                               const float *D, int nx, int ny, int nz, double sigma_spline)
+    : nx_(nx), ny_(ny), nz_(nz) {
+    BINDER_CHECK(nx > 0 && ny > 0 && nz > 0, "grid dimensions must be positive");
+    if (nz == 1)
+        throw Error(kUnsupported, "2D prior transformation (Nz_v == 1) is not built on the GPU path");
+    V_ = (long)nx * ny * nz;
+    for (int n = 0; n < 3; ++n) {
+        gamma_[n] = gamma[n];
+        rho_[n] = rho[n];
+        eta_[n] = eta[n];
+    }
+    sigma2_ = sigma_spline * sigma_spline;
+    BINDER_CUDA(cudaStreamCreate(&own_stream_));
+    stream_ = own_stream_;
+    D_ = dalloc<float>((size_t)V_);
+    BINDER_CUDA(cudaMemcpy(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice));
+    r_ = dalloc<float>((size_t)V_ * 3);
+    d_ = dalloc<float>((size_t)V_ * 3);
+    zeros_ = dalloc<float>((size_t)V_ * 3);
+    BINDER_CUDA(cudaMemset(zeros_, 0, sizeof(float) * V_ * 3));
+    st_ = dalloc<DevState>(1);
+    BINDER_CUDA(cudaMemset(st_, 0, sizeof(DevState)));
+    mstep_.init(nx, ny, nz);
+}
+
+PriorTransform::~PriorTransform() {
+    cudaDeviceSynchronize();
+    if (own_stream_) cudaStreamDestroy(own_stream_);
+    dfree(D_); dfree(r_); dfree(d_); dfree(zeros_); dfree(chunk_); dfree(st_);
+    mstep_.release();
+}
+
+// BINDER/src/cpu/NonLinearTransformation.cpp:226-278: voxel positions are zero, so the result
+// is the smoothed field itself
+double PriorTransform::smooth(const float *field, float *out) {
+    std::vector<float> soa;
+    aos_to_soa(field, V_, 3, soa);
+    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    DevState h{};
+    for (int n = 0; n < 3; ++n) h.gamma[n] = gamma_[n];
+    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+    const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+    mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 0, 0, 1, seed_, 0,
+                   rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    BINDER_CUDA(cudaMemcpy(soa.data(), d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
+    soa_to_aos(soa.data(), V_, 3, out);
+    return h.lp_tr;
+}
+
+// NonLinearTransformation.cpp:280-341: independent prior samples around the given field.  The
+// Philox sweep counter continues across calls, so repeated calls give fresh samples.
+void PriorTransform::sample(const float *field, int n, float *out) {
+    BINDER_CHECK(n >= 0, "number_of_samples must be non-negative");
+    if (n == 0) return;
+    std::vector<float> soa;
+    aos_to_soa(field, V_, 3, soa);
+    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    DevState h{};
+    for (int c = 0; c < 3; ++c) h.gamma[c] = gamma_[c];
+    h.sweep = sweep_;
+    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+    const int B = n < 64 ? n : 64;
+    dfree(chunk_);
+    chunk_ = dalloc<float>((size_t)B * V_ * 3);
+    const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+    const double rho_p = rho_[0] * rho_[1] * rho_[2];
+    auto capture = [&](int count, Graph &g) {
+        BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+        try {
+            for (int j = 0; j < count; ++j) {
+                mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 1, 0, 1, seed_, 0, rho_p, eta2,
+                               nullptr, stream_);
+                BINDER_CUDA(cudaMemcpyAsync(chunk_ + (size_t)j * V_ * 3, d_, sizeof(float) * V_ * 3,
+                                            cudaMemcpyDeviceToDevice, stream_));
+                launch_sweep_advance(st_, 0x7fffffff, stream_);
+            }
+        } catch (...) {
+            cudaGraph_t gg;
+            cudaStreamEndCapture(stream_, &gg);
+            if (gg) cudaGraphDestroy(gg);
+            throw;
+        }
+        BINDER_CUDA(cudaStreamEndCapture(stream_, &g.g));
+        BINDER_CUDA(cudaGraphInstantiate(&g.e, g.g, 0));
+    };
+    BINDER_CUDA(cudaDeviceSynchronize());
+    Graph full, tail;
+    capture(B, full);
+    const int rem = n % B;
+    if (rem) capture(rem, tail);
+    std::vector<float> host((size_t)B * V_ * 3);
+    int done = 0;
+    while (done < n) {
+        const int cnt = (n - done) >= B ? B : rem;
+        BINDER_CUDA(cudaGraphLaunch(cnt == B ? full.e : tail.e, stream_));
+        BINDER_CUDA(cudaMemcpyAsync(host.data(), chunk_, sizeof(float) * (size_t)cnt * V_ * 3,
+                                    cudaMemcpyDeviceToHost, stream_));
+        BINDER_CUDA(cudaStreamSynchronize(stream_));
+        for (int j = 0; j < cnt; ++j)
+            soa_to_aos(host.data() + (size_t)j * V_ * 3, V_, 3, out + (size_t)(done + j) * V_ * 3);
+        done += cnt;
+    }
+    sweep_ += n;
+}
+
+void PriorTransform::get_shape(int out[4]) const {
+    out[0] = nx_; out[1] = ny_; out[2] = nz_; out[3] = 3;
+}
+
+}  // namespace binder

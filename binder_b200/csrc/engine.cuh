@@ -1,0 +1,124 @@
+// Registration and prior-transformation engines behind the C-ABI (one object per image pair).
+#pragma once
+
+#include <vector>
+
+#include "estep.cuh"
+#include "topology.cuh"
+
+namespace binder {
+
+// device DCT matrices of one grid (forward C and inverse C^T per axis)
+struct DctSet {
+    int n[3] = {0, 0, 0};
+    float *fwd[3] = {nullptr, nullptr, nullptr};
+    float *inv[3] = {nullptr, nullptr, nullptr};
+    void init(int nx, int ny, int nz);
+    void release();
+};
+
+// The DCT-prior M-step of BINDER/src/cpu/NonLinearTransformation.cpp:58-126 on SoA buffers:
+// out = IDCT( DCT(r) / (1 + gamma sigma^2 D) [+ noise] ) + x, costs into st.
+struct MStep {
+    int nx = 0, ny = 0, nz = 0;
+    long V = 0;
+    DctSet dct;
+    float *t1 = nullptr, *t2 = nullptr;
+    void init(int nx, int ny, int nz);
+    void release();
+    void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
+                 double sigma2, int sample, int want_raw, int every, uint64_t seed, uint32_t chain,
+                 double rho_p, const double eta2[3], const int *skip, cudaStream_t s);
+};
+
+class Registration {
+  public:
+    Registration(const float *final_locations, const float *voxel_pos, int nx, int ny, int nz,
+                 int nxn, int nyn, int nzn, int spline_order, double non_zero_voxels);
+    ~Registration();
+
+    void set_mi_likelihood(double alpha, const float *theta, int K, int L, const int *binned_nodes,
+                           const int *binned_voxels);
+    void set_nonlinear_transformation(const double gamma[3], const double rho[3],
+                                      const double eta[3], const float *D);
+    int em(int max_iterations, double convergence_th, int update_likelihood_parameters, int debug);
+    void sampler(uint64_t seed, int N_b, int N_s, int sample_gamma, int sample_gamma_every,
+                 int sample_posteriors, int sample_likelihood_parameters,
+                 int sample_transformation_parameters, double *mean_out, double *cov_out);
+
+    void get_final_locations(float *out) const;      // AoS [V][3]
+    void set_final_locations(const float *in);
+    void get_dream_locations(float *out) const;      // AoS [V][3]
+    void set_dream_locations(const float *in);
+    void get_likelihood_parameters(float *out) const;  // [K*L]
+    void get_shape(int out[4]) const;
+    int get_iteration_stats(double *out, int max_n) const;  // [n][4]: mll, lp_lik, lp_tr, mlp
+    void get_state(double *gamma_out, double *nu_out, unsigned long long *degenerate,
+                   unsigned *flags) const;
+    void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+    void set_chain(uint32_t c) { chain_ = c; }
+    double last_elapsed_ms() const { return last_ms_; }
+
+    int K() const { return K_; }
+    int L() const { return L_; }
+
+  private:
+    void enqueue_em_iteration(int max_iter, double th, int update);
+    void reset_state(bool for_sampler);
+    void require_ready() const;
+
+    int nx_, ny_, nz_, nxn_, nyn_, nzn_, N_;
+    long V_, Vn_;
+    double nzv_;
+    cudaStream_t stream_ = 0, own_stream_ = 0;  // a blocking stream: ordered after legacy-stream copies
+    uint32_t chain_ = 0;
+    // device buffers
+    float *d_ = nullptr, *x_ = nullptr, *r_ = nullptr, *D_ = nullptr, *theta_ = nullptr,
+          *hist_ = nullptr;
+    unsigned *hcnt_ = nullptr;
+    uint8_t *u_ = nullptr, *vpad_ = nullptr;
+    double *mean_ = nullptr, *m2_ = nullptr, *stats_ = nullptr;
+    int stats_cap_ = 0;
+    DevState *st_ = nullptr;
+    MStep mstep_;
+    // likelihood / prior parameters
+    bool have_mi_ = false, have_tr_ = false;
+    int K_ = 0, L_ = 0;
+    double alpha_ = 2.0;
+    double gamma0_[3] = {0, 0, 0}, rho_[3] = {1, 1, 1}, eta_[3] = {1, 1, 1};
+    double sigma2_ = 0.0;
+    int P_ = 8, PZ_ = 8, pyn_ = 0, zp_ = 0;
+    int egrid_e_ = 0, egrid_s_ = 0;
+    uint64_t seed_ = 12345;
+    int iters_done_ = 0;
+    double last_ms_ = 0.0;
+};
+
+// _core.NonLinearTransformation: smoothing and prior sampling of a displacement field
+class PriorTransform {
+  public:
+    PriorTransform(const double gamma[3], const double rho[3], const double eta[3], const float *D,
+                   int nx, int ny, int nz, double sigma_spline);
+    ~PriorTransform();
+    double smooth(const float *field_aos, float *out_aos);
+    void sample(const float *field_aos, int n, float *out_aos);
+    void get_shape(int out[4]) const;
+    void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+
+  private:
+    int nx_, ny_, nz_;
+    long V_;
+    double gamma_[3], rho_[3], eta_[3], sigma2_;
+    float *D_ = nullptr, *r_ = nullptr, *d_ = nullptr, *zeros_ = nullptr, *chunk_ = nullptr;
+    DevState *st_ = nullptr;
+    MStep mstep_;
+    cudaStream_t stream_ = 0, own_stream_ = 0;
+    uint64_t seed_ = 1234;
+    int sweep_ = 0;
+};
+
+// helpers shared with the C-ABI
+void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa);
+void soa_to_aos(const float *soa, long V, int N, float *aos);
+
+}  // namespace binder

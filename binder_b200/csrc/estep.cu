@@ -1,0 +1,458 @@
+// E-step kernels (EM soft assignment and Gibbs categorical draw), theta updates, Dirichlet and
+// gamma-prior sampling, EM bookkeeping and FP64 Welford moments.
+#include <cmath>
+
+#include "estep.cuh"
+
+namespace binder {
+
+namespace {
+
+constexpr int kEThreads = 256;
+
+// cubic B-spline weights for node offsets -1, 0, 1, 2 at fraction t in [0,1)
+// (BINDER/src/cpu/Spline.cpp:44-73; Registration.cu:20-31 evaluates the same polynomial)
+__device__ __forceinline__ void bspline3(float t, float w[4]) {
+    const float t2 = t * t, t3 = t2 * t;
+    const float e = 1.0f - t, e2 = e * e, e3 = e2 * e;
+    w[0] = e3 * (1.0f / 6.0f);
+    w[1] = (2.0f / 3.0f) - t2 + 0.5f * t3;
+    w[2] = (2.0f / 3.0f) - e2 + 0.5f * e3;
+    w[3] = t3 * (1.0f / 6.0f);
+}
+
+// 64 moving-image bins of the 4x4x4 neighbourhood, packed 4 per word along z.  Fast path: two
+// aligned 32-bit loads per (x, y) row from the zero-padded bin volume and a funnel shift; the
+// padding is bin 0, which is the reference's value for nodes outside the moving grid
+// (MILikelihood.cpp:46-48).  Slow path (neighbourhood leaves the padded volume): per-node test.
+__device__ __forceinline__ void gather_bins(const EStepArgs &a, int ix, int iy, int iz,
+                                            uint32_t pk[16]) {
+    const int zz0 = iz - 1 + a.PZ;
+    const bool fast = (ix - 1 + a.P >= 0) && (ix + 2 + a.P < a.nxn + 2 * a.P) &&
+                      (iy - 1 + a.P >= 0) && (iy + 2 + a.P < a.nyn + 2 * a.P) && (zz0 >= 0) &&
+                      ((zz0 >> 2) + 2 <= (a.zp >> 2));
+    if (fast) {
+        const int w = zz0 >> 2, sh = (zz0 & 3) * 8;
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t *row = reinterpret_cast<const uint32_t *>(
+                    a.vpad + ((long)(ix - 1 + p + a.P) * a.pyn + (iy - 1 + q + a.P)) * a.zp);
+                const uint32_t lo = __ldg(row + w), hi = __ldg(row + w + 1);
+                pk[p * 4 + q] = __funnelshift_r(lo, hi, sh);
+            }
+    } else {
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint32_t word = 0;
+                const int X = ix - 1 + p, Y = iy - 1 + q;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int Z = iz - 1 + c;
+                    uint32_t b = 0;
+                    if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn)
+                        b = a.vpad[((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp + (Z + a.PZ)];
+                    word |= b << (8 * c);
+                }
+                pk[p * 4 + q] = word;
+            }
+    }
+}
+
+__device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int comp) {
+    if (a.x) return a.x[comp * a.V + i];
+    const long yz = (long)a.ny * a.nz;
+    return comp == 0 ? (float)(i / yz) : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
+}
+
+// BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
+// histogram kept in shared memory and neighbouring equal bins combined before the atomics.
+template <bool SAMPLE>
+__global__ void __launch_bounds__(kEThreads) estep_kernel(const EStepArgs a) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) float sm[];
+    const int KL = a.K * a.L;
+    float *th = sm;
+    float *hs = sm + KL;                                 // EM histogram
+    unsigned *hc = reinterpret_cast<unsigned *>(sm + KL);  // Gibbs counts
+    __shared__ double red[32];
+    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+        th[q] = a.theta[q];
+        if (SAMPLE) hc[q] = 0u; else hs[q] = 0.0f;
+    }
+    __syncthreads();
+
+    const uint32_t sweep = SAMPLE ? (uint32_t)a.st->sweep : 0u;
+    double mll = 0.0;
+    unsigned long long deg = 0;
+    const float *d0 = a.d, *d1 = a.d + a.V, *d2 = a.d + 2 * a.V;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.V;
+         i += (long)gridDim.x * blockDim.x) {
+        const float px = d0[i], py = d1[i], pz = d2[i];
+        const float x0 = voxel_coord(a, i, 0), x1 = voxel_coord(a, i, 1), x2 = voxel_coord(a, i, 2);
+        // positions far outside any grid (or non-finite) are degenerate: keep them as they are
+        if (!(fabsf(px) < 1.0e6f && fabsf(py) < 1.0e6f && fabsf(pz) < 1.0e6f)) {
+            a.r[i] = px - x0; a.r[a.V + i] = py - x1; a.r[2 * a.V + i] = pz - x2;
+            ++deg;
+            continue;
+        }
+        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+        float bx[4], by[4], bz[4];
+        bspline3(px - fx, bx);
+        bspline3(py - fy, by);
+        bspline3(pz - fz, bz);
+        uint32_t pk[16];
+        gather_bins(a, ix, iy, iz, pk);
+        const float *thc = th + a.u[i];  // theta column of this voxel's bin: thc[k * L]
+        const int L = a.L;
+
+        // pass 1: normaliser and the posterior-weighted node offsets
+        float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float bxy = __fmul_rn(bx[p], by[q]);
+                const uint32_t word = pk[p * 4 + q];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int k = (word >> (8 * c)) & 0xff;
+                    const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
+                    S = __fadd_rn(S, w);
+                    Sx = fmaf((float)(p - 1), w, Sx);
+                    Sy = fmaf((float)(q - 1), w, Sy);
+                    Sz = fmaf((float)(c - 1), w, Sz);
+                }
+            }
+        if (!(S > 0.0f)) {
+            a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
+            ++deg;
+            continue;
+        }
+        if (!SAMPLE) {
+            const float inv = 1.0f / S;
+            mll -= log((double)S);
+            a.r[i] = (fx + Sx * inv) - x0;
+            a.r[a.V + i] = (fy + Sy * inv) - x1;
+            a.r[2 * a.V + i] = (fz + Sz * inv) - x2;
+            // pass 2: normalised posteriors into the histogram column u_i, runs of equal bins
+            // combined in a register before each shared-memory atomic
+            const int ui = a.u[i];
+            int ck = -1;
+            float cacc = 0.0f;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float bxy = __fmul_rn(bx[p], by[q]);
+                    const uint32_t word = pk[p * 4 + q];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int k = (word >> (8 * c)) & 0xff;
+                        const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]) * inv;
+                        if (k == ck) {
+                            cacc += w;
+                        } else {
+                            if (ck >= 0) atomicAdd(&hs[ck * L + ui], cacc);
+                            ck = k;
+                            cacc = w;
+                        }
+                    }
+                }
+            atomicAdd(&hs[ck * L + ui], cacc);
+        } else {
+            // categorical draw: first neighbour whose running sum reaches u * S
+            const u32x4 rr = philox_draw(a.seed, (uint32_t)i, sweep, 1u, a.chain);
+            const float t = u01_f24(rr.x) * S;
+            float cdf = 0.0f;
+            int pick = -1, kp = 0;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float bxy = __fmul_rn(bx[p], by[q]);
+                    const uint32_t word = pk[p * 4 + q];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int k = (word >> (8 * c)) & 0xff;
+                        const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
+                        cdf = __fadd_rn(cdf, w);
+                        if (pick < 0 && cdf >= t) {
+                            pick = p * 16 + q * 4 + c;
+                            kp = k;
+                        }
+                    }
+                }
+            if (pick < 0) {  // unreachable (cdf ends at S >= t); keep the last neighbour
+                pick = 63;
+                kp = (pk[15] >> 24) & 0xff;
+            }
+            atomicAdd(&hc[kp * L + a.u[i]], 1u);
+            a.r[i] = (fx + (float)(pick / 16 - 1)) - x0;
+            a.r[a.V + i] = (fy + (float)((pick / 4) % 4 - 1)) - x1;
+            a.r[2 * a.V + i] = (fz + (float)(pick % 4 - 1)) - x2;
+        }
+    }
+
+    // merge: histogram entries this CTA touched, and the FP64 mll / degenerate partials
+    __syncthreads();
+    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+        if (SAMPLE) {
+            const unsigned v = hc[q];
+            if (v) atomicAdd(&a.hcnt[q], v);
+        } else {
+            const float v = hs[q];
+            if (v != 0.0f) atomicAdd(&a.hist[q], v);
+        }
+    }
+    const double m = block_sum(mll, red);
+    if (threadIdx.x == 0 && !SAMPLE) atomicAdd(&a.st->mll, m);
+    const double dg = block_sum((double)deg, red);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+}
+
+// MILikelihood.cpp:71-86 (update) and :33-39, :183-206 (cost), one CTA
+__global__ void theta_update_kernel(float *theta, float *hist, int K, int L, double alpha,
+                                    int update, DevState *st) {
+    if (st->done) return;
+    __shared__ double rowlp[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double lp_total = 0.0;
+    // the log-normaliser terms are the same for every row: lgamma(sum alpha) - L lgamma(alpha)
+    double sum_alpha = 0.0;
+    for (int l = 0; l < L; ++l) sum_alpha += alpha;
+    double lnorm = lgamma(sum_alpha);
+    const double lga = lgamma(alpha);
+    for (int l = 0; l < L; ++l) lnorm -= lga;
+    for (int k = wid; k < K; k += nw) {
+        if (update) {
+            double s = 0.0;
+            for (int l = lane; l < L; l += 32) s += (double)hist[k * L + l] + alpha - 1.0;
+            s = warp_sum(s);
+            for (int l = lane; l < L; l += 32)
+                theta[k * L + l] = (float)(((double)hist[k * L + l] + alpha - 1.0) / s);
+            __syncwarp();
+        }
+        double sl = 0.0;
+        for (int l = lane; l < L; l += 32) sl += (alpha - 1.0) * log((double)theta[k * L + l]);
+        sl = warp_sum(sl);
+        if (lane == 0) lp_total += -(lnorm + sl);
+    }
+    __syncthreads();  // every row has been read before the histogram is cleared
+    for (int q = threadIdx.x; q < K * L; q += blockDim.x) hist[q] = 0.0f;
+    if (lane == 0) rowlp[wid] = lp_total;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < nw; ++w) t += rowlp[w];
+        st->lp_lik = t;
+    }
+}
+
+// Gamma(shape, 1) by Marsaglia & Tsang (ACM TOMS 26(3), 2000) in FP64, with the shape < 1 boost;
+// attempt j uses Philox ctr = {index, sweep, tag | j << 8, chain}: words 0,1 Box-Muller normal,
+// word 2 acceptance uniform, word 3 boost uniform.  At most 64 attempts; *capped set beyond.
+__device__ double gamma_mt(double shape, uint64_t seed, uint32_t index, uint32_t sweep,
+                           uint32_t tag, uint32_t chain, bool *capped) {
+    const bool small = shape < 1.0;
+    const double a = small ? shape + 1.0 : shape;
+    const double dd = a - 1.0 / 3.0;
+    const double c = 1.0 / sqrt(9.0 * dd);
+    for (uint32_t att = 0; att < 64; ++att) {
+        const u32x4 r = philox_draw(seed, index, sweep, tag | (att << 8), chain);
+        const double u1 = u01_d32(r.x), u2 = u01_d32(r.y);
+        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        double v = 1.0 + c * z;
+        if (v <= 0.0) continue;
+        v = v * v * v;
+        const double uu = u01_d32(r.z);
+        if (uu < 1.0 - 0.0331 * (z * z) * (z * z) || log(uu) < 0.5 * z * z + dd * (1.0 - v + log(v))) {
+            double g = dd * v;
+            if (small) g *= pow(u01_d32(r.w), 1.0 / shape);
+            return g;
+        }
+    }
+    *capped = true;
+    return dd;
+}
+
+// MILikelihood.cpp:132-169 (Registration.cu:426-442 on the GPU): one CTA per row k
+__global__ void dirichlet_sample_kernel(float *theta, unsigned *hcnt, int K, int L, double alpha,
+                                        uint64_t seed, uint32_t chain, DevState *st) {
+    if (st->done) return;
+    __shared__ double red[32];
+    const int k = blockIdx.x;
+    const uint32_t sweep = (uint32_t)st->sweep;
+    double g = 0.0;
+    bool capped = false;
+    const int l = threadIdx.x;
+    if (l < L) {
+        const double shape = (double)hcnt[k * L + l] + alpha;
+        g = gamma_mt(shape, seed, (uint32_t)(k * L + l), sweep, 4u, chain, &capped);
+        hcnt[k * L + l] = 0u;
+    }
+    const double s = block_sum(g, red);
+    __shared__ double tot;
+    if (threadIdx.x == 0) tot = s;
+    __syncthreads();
+    if (l < L) theta[k * L + l] = (float)(g / tot);
+    if (capped) atomicOr(&st->flags, (unsigned)kFlagGammaCapped);
+}
+
+// NonLinearTransformation.cpp:115-124 and :140-148
+__global__ void nu_sample_kernel(DevState *st, int sample_gamma, int every, int N, long V,
+                                 double rho_p, double e0, double e1, double e2, uint64_t seed,
+                                 uint32_t chain) {
+    if (st->done) return;
+    const int sweep = st->sweep;
+    if (sample_gamma && (sweep % every == 0)) {
+        const double alpha_0 = 1.0, beta_0 = 10000.0;
+        const double a_post = alpha_0 + 0.5 * (double)N * (double)V;
+        const double b_post = beta_0 + 0.5 * (double)V * st->raw_reg;
+        bool capped = false;
+        const double nu = gamma_mt(a_post, seed, 0u, (uint32_t)sweep, 5u, chain, &capped) / b_post;
+        if (capped) st->flags |= kFlagGammaCapped;
+        st->nu = nu;
+        st->gamma[0] = nu * rho_p * e0 * (double)V;
+        st->gamma[1] = nu * rho_p * e1 * (double)V;
+        st->gamma[2] = nu * rho_p * e2 * (double)V;
+    }
+    st->raw_reg = 0.0;
+}
+
+// Registration.cpp:195-214
+__global__ void em_finish_kernel(DevState *st, double *stats, int max_iter, double th, double nzv) {
+    if (st->done) return;
+    const double mlp = st->mll + st->lp_tr + st->lp_lik;
+    const int it = st->iter;
+    if (it < max_iter) {
+        stats[it * 4 + 0] = st->mll;
+        stats[it * 4 + 1] = st->lp_lik;
+        stats[it * 4 + 2] = st->lp_tr;
+        stats[it * 4 + 3] = mlp;
+    }
+    if (!isfinite(mlp)) st->flags |= kFlagNonFinite;
+    st->iter = it + 1;
+    if ((st->mlp_old - mlp) / nzv < th || it + 1 >= max_iter) st->done = 1;
+    st->mlp_old = mlp;
+    st->mll = 0.0;
+    st->lp_tr = 0.0;
+}
+
+// Registration.cpp:593-623 in FP64 with the symmetric M2 (xx, xy, xz, yy, yz, zz)
+__global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long V, int N_b,
+                                 DevState *st) {
+    if (st->done) return;
+    const int sweep = st->sweep;
+    if (sweep >= N_b) {
+        const double inv_n = 1.0 / ((double)(sweep - N_b) + 1.0);
+        for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
+             i += (long)gridDim.x * blockDim.x) {
+            double d1[3], d2[3];
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                const double val = (double)d[n * V + i];
+                const double mo = mean[n * V + i];
+                d1[n] = val - mo;
+                const double mn = mo + d1[n] * inv_n;
+                mean[n * V + i] = mn;
+                d2[n] = val - mn;
+            }
+            m2[0 * V + i] += d1[0] * d2[0];
+            m2[1 * V + i] += d1[0] * d2[1];
+            m2[2 * V + i] += d1[0] * d2[2];
+            m2[3 * V + i] += d1[1] * d2[1];
+            m2[4 * V + i] += d1[1] * d2[2];
+            m2[5 * V + i] += d1[2] * d2[2];
+        }
+    }
+}
+
+__global__ void sweep_advance_kernel(DevState *st, int total) {
+    if (st->done) return;
+    st->sweep += 1;
+    if (st->sweep >= total) st->done = 1;
+}
+
+}  // namespace
+
+int estep_grid(bool sample, int K, int L, long V) {
+    int dev = 0, sms = 148, per_sm = 1;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem = (size_t)2 * K * L * sizeof(float);
+    if (sample) {
+        BINDER_CUDA(cudaFuncSetAttribute(estep_kernel<true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estep_kernel<true>,
+                                                                  kEThreads, smem));
+    } else {
+        BINDER_CUDA(cudaFuncSetAttribute(estep_kernel<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estep_kernel<false>,
+                                                                  kEThreads, smem));
+    }
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const long need = (V + kEThreads - 1) / kEThreads;
+    long g = (long)sms * per_sm;
+    if (need < g) g = need < 1 ? 1 : need;
+    return (int)g;
+}
+
+void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s) {
+    const size_t smem = (size_t)2 * a.K * a.L * sizeof(float);
+    if (sample)
+        estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
+    else
+        estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, int update,
+                         DevState *st, cudaStream_t s) {
+    theta_update_kernel<<<1, 1024, 0, s>>>(theta, hist, K, L, alpha, update, st);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_dirichlet_sample(float *theta, unsigned *hcnt, int K, int L, double alpha,
+                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s) {
+    const int threads = ((L + 31) / 32) * 32;
+    dirichlet_sample_kernel<<<K, threads, 0, s>>>(theta, hcnt, K, L, alpha, seed, chain, st);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, double rho_p,
+                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s) {
+    nu_sample_kernel<<<1, 1, 0, s>>>(st, sample_gamma, every, N, V, rho_p, eta2[0], eta2[1],
+                                     eta2[2], seed, chain);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_em_finish(DevState *st, double *stats, int max_iter, double th, double nzv,
+                      cudaStream_t s) {
+    em_finish_kernel<<<1, 1, 0, s>>>(st, stats, max_iter, th, nzv);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N_b, int total,
+                      DevState *st, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    long need = (V + 255) / 256;
+    const long g = need < (long)sms * 8 ? (need < 1 ? 1 : need) : (long)sms * 8;
+    sweep_end_kernel<<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    BINDER_CUDA(cudaGetLastError());
+    launch_sweep_advance(st, total, s);
+}
+
+void launch_sweep_advance(DevState *st, int total, cudaStream_t s) {
+    sweep_advance_kernel<<<1, 1, 0, s>>>(st, total);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+}  // namespace binder

@@ -1,0 +1,52 @@
+// E-step (EM and Gibbs), theta updates, prior-precision sampling, Welford moments.
+#pragma once
+
+#include "transform.cuh"
+
+namespace binder {
+
+struct EStepArgs {
+    const float *d;   // positions, SoA [3][V] (node-grid coordinates)
+    float *r;         // out: dream location minus voxel position, SoA [3][V]
+    const float *x;   // voxel positions SoA [3][V], or null for the identity grid
+    const uint8_t *u;     // fixed-image bins [V]
+    const uint8_t *vpad;  // moving-image bins, zero-padded [nxn+2P][nyn+2P][zp bytes]
+    const float *theta;   // [K*L]
+    float *hist;          // EM: soft joint histogram [K*L] (accumulated)
+    unsigned *hcnt;       // Gibbs: joint counts [K*L] (accumulated)
+    DevState *st;
+    const int *skip;
+    long V;
+    int nx, ny, nz;
+    int nxn, nyn, nzn;
+    int P, PZ, pyn, zp;
+    int K, L;
+    uint64_t seed;
+    uint32_t chain;
+};
+
+void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
+int estep_grid(bool sample, int K, int L, long V);
+
+// theta <- (hist + alpha - 1)/rowsum (if update), Dirichlet prior cost into st->lp_lik,
+// hist zeroed for the next iteration.  One CTA.
+void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, int update,
+                         DevState *st, cudaStream_t s);
+// theta_k ~ Dirichlet(counts_k + alpha) with Philox gammas (tag 4, sweep = st->sweep); counts zeroed
+void launch_dirichlet_sample(float *theta, unsigned *hcnt, int K, int L, double alpha,
+                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s);
+// nu ~ Gamma(alpha0 + N V/2, beta0 + V/2 raw) when sample_gamma and sweep % every == 0;
+// gammas refreshed from nu.  Also resets raw_reg.
+void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, double rho_p,
+                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s);
+// EM bookkeeping: min-log-posterior, per-iteration stats, convergence flag
+void launch_em_finish(DevState *st, double *stats, int max_iter, double th, double nzv,
+                      cudaStream_t s);
+// Welford mean / symmetric M2 update in FP64 when sweep >= N_b, then sweep += 1 (done once
+// sweep reaches `total`)
+void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N_b, int total,
+                      DevState *st, cudaStream_t s);
+// sweep += 1 (done once sweep reaches `total`)
+void launch_sweep_advance(DevState *st, int total, cudaStream_t s);
+
+}  // namespace binder

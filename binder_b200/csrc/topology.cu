@@ -1,0 +1,515 @@
+// Jacobian determinants and topology correction in FP64.
+//
+// This file is compiled with -fmad=false: every determinant is evaluated with the reference's
+// expression grouping and without fused multiply-adds, so the per-voxel Jacobians (and therefore
+// the negative / out-of-range counts and the set of corners the limiter touches) equal the
+// reference CPU backend's bit for bit on the same FP64 input.
+#include <cmath>
+#include <vector>
+
+#include "topology.cuh"
+#include "transform.cuh"
+
+namespace binder {
+
+namespace {
+
+// cofactor expansion along the first row with the reference's grouping
+// (BINDER/src/cpu/utils.cpp:156-160, topology_correction_3D.cpp:286-288)
+__device__ __forceinline__ double det3(double a00, double a01, double a02, double a10, double a11,
+                                       double a12, double a20, double a21, double a22) {
+    return a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) +
+           a02 * (a10 * a21 - a11 * a20);
+}
+
+__device__ __forceinline__ unsigned long long ordered(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+double unordered(unsigned long long o) {
+    const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+    double v;
+    memcpy(&v, &b, sizeof(v));
+    return v;
+}
+
+struct Red {
+    unsigned long long mn, mx;
+    unsigned long long below, above, negative;
+    double sum[3];
+    int count;  // flagged cells (limiter list length)
+    int pad;
+};
+
+// BINDER/src/cpu/utils.cpp:100-345.  Element (p, m) of the field is f[p*ps + m*cs].
+__global__ void jacobian_kernel(const double *f, long ps, long cs, int nx, int ny, int nz,
+                                double vol, double *J, double e1, double e2, Red *red) {
+    const long V = (long)nx * ny * nz;
+    const long yz = (long)ny * nz;
+    // corner order of the reference: fff, bff, fbf, ffb, bbf, bfb, fbb, bbb
+    const int dir[8][3] = {{1, 1, 1},  {-1, 1, 1},  {1, -1, 1},  {1, 1, -1},
+                           {-1, -1, 1}, {-1, 1, -1}, {1, -1, -1}, {-1, -1, -1}};
+    double lmin = 1e300, lmax = -1e300;
+    unsigned long long lb = 0, la = 0, ln = 0;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / yz), y = (int)((p / nz) % ny), z = (int)(p % nz);
+        double w0[3];
+        for (int m = 0; m < 3; ++m) w0[m] = f[p * ps + m * cs];
+        double tot = 0.0;
+        int valid = 0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int sx = dir[c][0], sy = dir[c][1], sz = dir[c][2];
+            if ((sx > 0 && x >= nx - 1) || (sx < 0 && x <= 0)) continue;
+            if ((sy > 0 && y >= ny - 1) || (sy < 0 && y <= 0)) continue;
+            if ((sz > 0 && z >= nz - 1) || (sz < 0 && z <= 0)) continue;
+            const long qx = p + sx * yz, qy = p + sy * nz, qz = p + sz;
+            double col[3][3];  // [axis][component]
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const double ax = f[qx * ps + m * cs], ay = f[qy * ps + m * cs],
+                             az = f[qz * ps + m * cs];
+                col[0][m] = sx > 0 ? ax - w0[m] : w0[m] - ax;
+                col[1][m] = sy > 0 ? ay - w0[m] : w0[m] - ay;
+                col[2][m] = sz > 0 ? az - w0[m] : w0[m] - az;
+            }
+            const double jc = det3(col[0][0], col[1][0], col[2][0], col[0][1], col[1][1], col[2][1],
+                                   col[0][2], col[1][2], col[2][2]) * vol;
+            tot += jc;
+            valid++;
+        }
+        const double jv = valid > 0 ? tot / valid : 1.0;
+        if (J) J[p] = jv;
+        lmin = fmin(lmin, jv);
+        lmax = fmax(lmax, jv);
+        lb += jv < e1;
+        la += jv > e2;
+        ln += jv < 0.0;
+    }
+    if (red) {
+        // warp-level first, then one atomic per warp
+        for (int o = 16; o > 0; o >>= 1) {
+            lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+            lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+            lb += __shfl_xor_sync(0xffffffffu, lb, o);
+            la += __shfl_xor_sync(0xffffffffu, la, o);
+            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&red->mn, ordered(lmin));
+            atomicMax(&red->mx, ordered(lmax));
+            if (lb) atomicAdd(&red->below, lb);
+            if (la) atomicAdd(&red->above, la);
+            if (ln) atomicAdd(&red->negative, ln);
+        }
+    }
+}
+
+// topology_correction_3D.cpp:488-607: the 8 vertex Jacobians of every cell, in the vertex order
+// 000, 100, 010, 001, 011, 101, 110, 111, each from the three cell edges through its vertex.
+// Positions are SoA [3][V].
+__global__ void corner_kernel(const double *pos, int nx, int ny, int nz, double vol, double e1,
+                              double e2, double *Jc, Red *red) {
+    const long V = (long)nx * ny * nz;
+    const long cy = ny - 1, cz = nz - 1;
+    const long cells = (long)(nx - 1) * cy * cz;
+    const int vert[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                            {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
+    unsigned long long lb = 0, la = 0;
+    for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < cells;
+         cell += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(cell / (cy * cz)), y = (int)((cell / cz) % cy), z = (int)(cell % cz);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int vx = vert[c][0], vy = vert[c][1], vz = vert[c][2];
+            const long pw = ((long)(x + vx) * ny + (y + vy)) * nz + (z + vz);
+            const long pxn = ((long)(x + 1 - vx) * ny + (y + vy)) * nz + (z + vz);
+            const long pyn = ((long)(x + vx) * ny + (y + 1 - vy)) * nz + (z + vz);
+            const long pzn = ((long)(x + vx) * ny + (y + vy)) * nz + (z + 1 - vz);
+            double col[3][3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const double w = pos[m * V + pw];
+                const double a = pos[m * V + pxn], b = pos[m * V + pyn], d = pos[m * V + pzn];
+                col[0][m] = vx ? w - a : a - w;
+                col[1][m] = vy ? w - b : b - w;
+                col[2][m] = vz ? w - d : d - w;
+            }
+            double j = det3(col[0][0], col[1][0], col[2][0], col[0][1], col[1][1], col[2][1],
+                            col[0][2], col[1][2], col[2][2]);
+            j *= vol;
+            Jc[cell * 8 + c] = j;
+            lb += j < e1;
+            la += j > e2;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lb += __shfl_xor_sync(0xffffffffu, lb, o);
+        la += __shfl_xor_sync(0xffffffffu, la, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (lb) atomicAdd(&red->below, lb);
+        if (la) atomicAdd(&red->above, la);
+    }
+}
+
+// topology_correction_3D.cpp:172-245: periodic forward differences, g[(n1*3+n2)][p] =
+// (pos_n1(p + e_n2) - pos_n1(p)) / vs[n1]
+__global__ void gradient_kernel(const double *pos, int nx, int ny, int nz, double v0, double v1,
+                                double v2, double *g) {
+    const long V = (long)nx * ny * nz;
+    const double vs[3] = {v0, v1, v2};
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / ((long)ny * nz)), y = (int)((p / nz) % ny), z = (int)(p % nz);
+        const int x2 = x + 1 > nx - 1 ? x + 1 - nx : x + 1;
+        const int y2 = y + 1 > ny - 1 ? y + 1 - ny : y + 1;
+        const int z2 = z + 1 > nz - 1 ? z + 1 - nz : z + 1;
+        const long px = ((long)x2 * ny + y) * nz + z, py = ((long)x * ny + y2) * nz + z,
+                   pz = ((long)x * ny + y) * nz + z2;
+#pragma unroll
+        for (int n1 = 0; n1 < 3; ++n1) {
+            const double c = pos[n1 * V + p];
+            g[(n1 * 3 + 0) * V + p] = (pos[n1 * V + px] - c) / vs[n1];
+            g[(n1 * 3 + 1) * V + p] = (pos[n1 * V + py] - c) / vs[n1];
+            g[(n1 * 3 + 2) * V + p] = (pos[n1 * V + pz] - c) / vs[n1];
+        }
+    }
+}
+
+__global__ void flag_cells_kernel(const double *Jc, int nx, int ny, int nz, double e1, double e2,
+                                  int *list, Red *red) {
+    const long cells = (long)(nx - 1) * (ny - 1) * (nz - 1);
+    for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < cells;
+         cell += (long)gridDim.x * blockDim.x) {
+        bool any = false;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const double j = Jc[cell * 8 + c];
+            any |= (j < e1 || j > e2);
+        }
+        if (any) list[atomicAdd(&red->count, 1)] = (int)cell;
+    }
+}
+
+// topology_correction_3D.cpp:247-332.  The reference visits cells in lexicographic order and a
+// cell's 8 corners in order; a cell reads and writes gradients only inside its 2x2x2 footprint,
+// so two cells interact only if they differ by at most 1 along every axis.  Level 4x + 2y + z
+// orders every such pair exactly as the lexicographic walk does and never puts two of them on
+// the same level, so processing levels in increasing order (cells of one level in parallel)
+// reproduces the sequential result exactly.  One CTA; levels are separated by __syncthreads.
+__global__ void __launch_bounds__(1024) limiter_kernel(const int *list, int *sorted, const double *Jc,
+                                                       double *g, int nx, int ny, int nz,
+                                                       double e1, double e2, int nlev, Red *red,
+                                                       unsigned *flags) {
+    extern __shared__ int sh[];
+    int *off = sh;             // nlev + 1
+    int *cur = sh + nlev + 1;  // nlev
+    const long V = (long)nx * ny * nz;
+    const long cy = ny - 1, cz = nz - 1;
+    const int n = red->count;
+    for (int l = threadIdx.x; l < nlev + 1; l += blockDim.x) off[l] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const long cell = list[q];
+        const int x = (int)(cell / (cy * cz)), y = (int)((cell / cz) % cy), z = (int)(cell % cz);
+        atomicAdd(&off[4 * x + 2 * y + z + 1], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int l = 0; l < nlev; ++l) off[l + 1] += off[l];
+    __syncthreads();
+    for (int l = threadIdx.x; l < nlev; l += blockDim.x) cur[l] = off[l];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const long cell = list[q];
+        const int x = (int)(cell / (cy * cz)), y = (int)((cell / cz) % cy), z = (int)(cell % cz);
+        sorted[atomicAdd(&cur[4 * x + 2 * y + z], 1)] = (int)cell;
+    }
+    __syncthreads();
+    const int vert[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                            {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {1, 1, 1}};
+    bool capped = false;
+    for (int l = 0; l < nlev; ++l) {
+        const int beg = off[l], end = off[l + 1];
+        if (beg == end) continue;  // uniform: every thread reads the same shared value
+        for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+            const long cell = sorted[q];
+            const int x = (int)(cell / (cy * cz)), y = (int)((cell / cz) % cy), z = (int)(cell % cz);
+            for (int c = 0; c < 8; ++c) {
+                const double jv = Jc[cell * 8 + c];
+                if (!(jv < e1 || jv > e2)) continue;
+                long gp[3];
+                for (int n2 = 0; n2 < 3; ++n2) {
+                    int o[3] = {vert[c][0], vert[c][1], vert[c][2]};
+                    o[n2] = 0;
+                    gp[n2] = ((long)(x + o[0]) * ny + (y + o[1])) * nz + (z + o[2]);
+                }
+                double J[3][3];
+                for (int n1 = 0; n1 < 3; ++n1)
+                    for (int n2 = 0; n2 < 3; ++n2) J[n1][n2] = g[(n1 * 3 + n2) * V + gp[n2]];
+                double alpha = 0.0;
+                double det = det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0],
+                                  J[2][1], J[2][2]);
+                int steps = 0;
+                while (det > e2 || det < e1) {
+                    if (++steps > 11) {  // alpha == 1 (identity) already tried: [e1, e2] misses 1
+                        capped = true;
+                        break;
+                    }
+                    alpha += 0.1;
+                    if (alpha > 1.0) alpha = 1.0;
+                    double Jn[3][3];
+                    for (int n1 = 0; n1 < 3; ++n1)
+                        for (int n2 = 0; n2 < 3; ++n2)
+                            Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                    det = det3(Jn[0][0], Jn[0][1], Jn[0][2], Jn[1][0], Jn[1][1], Jn[1][2], Jn[2][0],
+                               Jn[2][1], Jn[2][2]);
+                }
+                alpha += 0.1;
+                if (alpha > 1.0) alpha = 1.0;
+                for (int n1 = 0; n1 < 3; ++n1)
+                    for (int n2 = 0; n2 < 3; ++n2)
+                        g[(n1 * 3 + n2) * V + gp[n2]] =
+                            (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+            }
+        }
+        __syncthreads();
+    }
+    if (capped) atomicOr(flags, (unsigned)kFlagLimiterCapped);
+}
+
+// backward-difference divergence (periodic) of each component's gradient row; the reference's
+// Fourier factor (e^{-i theta} - 1) applied to the gradient spectra is minus its transform
+__global__ void divergence_kernel(const double *g, int nx, int ny, int nz, double *div) {
+    const long V = (long)nx * ny * nz;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / ((long)ny * nz)), y = (int)((p / nz) % ny), z = (int)(p % nz);
+        const int xm = x == 0 ? nx - 1 : x - 1, ym = y == 0 ? ny - 1 : y - 1,
+                  zm = z == 0 ? nz - 1 : z - 1;
+        const long px = ((long)xm * ny + y) * nz + z, py = ((long)x * ny + ym) * nz + z,
+                   pz = ((long)x * ny + y) * nz + zm;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            const double *gx = g + (n * 3 + 0) * V, *gy = g + (n * 3 + 1) * V,
+                         *gz = g + (n * 3 + 2) * V;
+            div[n * V + p] = (gx[p] - gx[px]) + (gy[p] - gy[py]) + (gz[p] - gz[pz]);
+        }
+    }
+}
+
+__global__ void sum_kernel(const double *pos, long V, Red *red) {
+    double s[3] = {0.0, 0.0, 0.0};
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x)
+        for (int n = 0; n < 3; ++n) s[n] += pos[n * V + p];
+    for (int n = 0; n < 3; ++n) {
+        double v = warp_sum(s[n]);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&red->sum[n], v);
+    }
+}
+
+// AoS grid-unit field -> SoA physical (scale) and back
+__global__ void aos_to_soa_kernel(const double *aos, long V, double s0, double s1, double s2,
+                                  double *soa) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        soa[p] = aos[p * 3 + 0] * s0;
+        soa[V + p] = aos[p * 3 + 1] * s1;
+        soa[2 * V + p] = aos[p * 3 + 2] * s2;
+    }
+}
+__global__ void soa_to_aos_kernel(const double *soa, long V, double s0, double s1, double s2,
+                                  double *aos) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        aos[p * 3 + 0] = soa[p] / s0;
+        aos[p * 3 + 1] = soa[V + p] / s1;
+        aos[p * 3 + 2] = soa[2 * V + p] / s2;
+    }
+}
+
+int grid_for(long work) {
+    int dev = 0, sms = 148;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long need = (work + 255) / 256;
+    const long cap = (long)sms * 8;
+    return (int)(need < 1 ? 1 : (need < cap ? need : cap));
+}
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    explicit DBuf(size_t n) {
+        if (n) BINDER_CUDA(cudaMalloc(&p, n * sizeof(T)));
+    }
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+};
+
+void reset_red(Red *r, cudaStream_t s) {
+    Red h{};
+    h.mn = ~0ull;
+    h.mx = 0ull;
+    BINDER_CUDA(cudaMemcpyAsync(r, &h, sizeof(Red), cudaMemcpyHostToDevice, s));
+}
+
+Red read_red(const Red *r, cudaStream_t s) {
+    Red h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, r, sizeof(Red), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+}  // namespace
+
+void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const double vs[3],
+                       double *J, cudaStream_t s) {
+    const long V = (long)nx * ny * nz;
+    jacobian_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, 3, 1, nx, ny, nz,
+                                                1.0 / (vs[0] * vs[1] * vs[2]), J, 0.0, 0.0, nullptr);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_outer,
+                                   int max_inner, const double vs[3], int nx, int ny, int nz,
+                                   cudaStream_t s) {
+    BINDER_CHECK(nx >= 2 && ny >= 2 && nz >= 2, "topology correction needs at least 2 voxels per axis");
+    BINDER_CHECK(nx <= 256 && ny <= 256 && nz <= 256, "topology correction supports axes up to 256");
+    BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
+    const long V = (long)nx * ny * nz;
+    const long cells = (long)(nx - 1) * (ny - 1) * (nz - 1);
+    const double vol = 1.0 / (vs[0] * vs[1] * vs[2]);
+    TopologyResult res{};
+
+    DBuf<double> aos(V * 3), pos(V * 3), grad(V * 9), jc(cells * 8), div(V * 3), t1(V * 3),
+        t2(V * 3);
+    DBuf<int> list(cells), sorted(cells);
+    DBuf<Red> red(1);
+    DBuf<unsigned> flags(1);
+    BINDER_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned), s));
+    BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
+    aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, vs[0], vs[1], vs[2], pos.p);
+
+    // Hartley matrices and cosine tables for the periodic Poisson solve
+    const int dims[3] = {nx, ny, nz};
+    std::vector<DBuf<double> *> mats, coss;
+    for (int a = 0; a < 3; ++a) {
+        const int n = dims[a];
+        std::vector<double> H((size_t)n * n), cs(n);
+        hartley_matrix(n, H.data());
+        const double pi = 3.14159265358979323846;
+        for (int k = 0; k < n; ++k) cs[k] = std::cos(2.0 * pi * k / (n * 1.0));
+        mats.push_back(new DBuf<double>((size_t)n * n));
+        coss.push_back(new DBuf<double>(n));
+        BINDER_CUDA(cudaMemcpyAsync(mats.back()->p, H.data(), sizeof(double) * n * n,
+                                    cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemcpyAsync(coss.back()->p, cs.data(), sizeof(double) * n,
+                                    cudaMemcpyHostToDevice, s));
+    }
+    struct Cleanup {
+        std::vector<DBuf<double> *> &a, &b;
+        ~Cleanup() {
+            for (auto *p : a) delete p;
+            for (auto *p : b) delete p;
+        }
+    } cleanup{mats, coss};
+
+    auto jac_stats = [&]() {
+        reset_red(red.p, s);
+        jacobian_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, 1, V, nx, ny, nz, vol, nullptr, e1, e2,
+                                                    red.p);
+        BINDER_CUDA(cudaGetLastError());
+        return read_red(red.p, s);
+    };
+    auto corners = [&]() {
+        reset_red(red.p, s);
+        corner_kernel<<<grid_for(cells), 256, 0, s>>>(pos.p, nx, ny, nz, vol, e1, e2, jc.p, red.p);
+        BINDER_CUDA(cudaGetLastError());
+        return read_red(red.p, s);
+    };
+
+    Red r = jac_stats();
+    double jmin = unordered(r.mn), jmax = unordered(r.mx);
+    res.below_before = (long long)r.below;
+    res.above_before = (long long)r.above;
+    const int nlev = 4 * (nx - 2) + 2 * (ny - 2) + (nz - 2) + 1;
+    const size_t lim_smem = sizeof(int) * (2 * (size_t)nlev + 1);
+    BINDER_CUDA(cudaFuncSetAttribute(limiter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)lim_smem));
+    int outer = 0;
+    while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+        Red c = corners();
+        int inner = 0;
+        while ((c.below > 0 || c.above > 0) && inner < max_inner) {
+            gradient_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, nx, ny, nz, vs[0], vs[1], vs[2],
+                                                        grad.p);
+            reset_red(red.p, s);
+            flag_cells_kernel<<<grid_for(cells), 256, 0, s>>>(jc.p, nx, ny, nz, e1, e2, list.p,
+                                                              red.p);
+            limiter_kernel<<<1, 1024, lim_smem, s>>>(list.p, sorted.p, jc.p, grad.p, nx, ny, nz,
+                                                     e1, e2, nlev, red.p, flags.p);
+            BINDER_CUDA(cudaGetLastError());
+            sum_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, V, red.p);
+            divergence_kernel<<<grid_for(V), 256, 0, s>>>(grad.p, nx, ny, nz, div.p);
+            BINDER_CUDA(cudaGetLastError());
+            Red sr = read_red(red.p, s);
+            double mean[3];
+            for (int n = 0; n < 3; ++n) mean[n] = sr.sum[n] / (nx * ny * nz);
+
+            // u = -(1/V) H (H div / lambda), separable Hartley passes z, y, [x fused], y, z
+            AxisArgs<double> a{};
+            a.comp_stride = V;
+            a.ny = ny;
+            a.nz = nz;
+            a.cos_x = coss[0]->p;
+            a.cos_y = coss[1]->p;
+            a.cos_z = coss[2]->p;
+            // z forward
+            a.in = div.p; a.out = t1.p; a.M = mats[2]->p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+            launch_axis_pass(a, kEpiNone, 3, s);
+            // y forward
+            a.in = t1.p; a.out = t2.p; a.M = mats[1]->p; a.n = ny; a.outer = nx; a.s = nz;
+            launch_axis_pass(a, kEpiNone, 3, s);
+            // x forward, -1/(lambda V), x inverse
+            a.in = t2.p; a.out = t1.p; a.M = mats[0]->p; a.M2 = mats[0]->p; a.n = nx; a.outer = 1;
+            a.s = (long)ny * nz;
+            launch_axis_pass(a, kEpiPoisson, 3, s);
+            // y inverse
+            a.in = t1.p; a.out = t2.p; a.M = mats[1]->p; a.n = ny; a.outer = nx; a.s = nz;
+            launch_axis_pass(a, kEpiNone, 3, s);
+            // z inverse -> physical positions u * vs + mean
+            a.in = t2.p; a.out = pos.p; a.M = mats[2]->p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+            for (int n = 0; n < 3; ++n) {
+                a.out_scale[n] = vs[n];
+                a.out_offset[n] = mean[n];
+            }
+            launch_axis_pass(a, kEpiTopoOut, 3, s);
+            c = corners();
+            inner++;
+            res.inner_iterations++;
+        }
+        r = jac_stats();
+        jmin = unordered(r.mn);
+        jmax = unordered(r.mx);
+        outer++;
+    }
+    res.outer_iterations = outer;
+    r = jac_stats();
+    res.below_after = (long long)r.below;
+    res.above_after = (long long)r.above;
+    soa_to_aos_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, V, vs[0], vs[1], vs[2], aos.p);
+    BINDER_CUDA(cudaGetLastError());
+    BINDER_CUDA(cudaMemcpyAsync(host, aos.p, sizeof(double) * V * 3, cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaMemcpyAsync(&res.flags, flags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    return res;
+}
+
+}  // namespace binder

@@ -1,0 +1,29 @@
+// Jacobian determinants and topology correction (FP64), BINDER/src/cpu/utils.cpp:100-345 and
+// BINDER/src/cpu/topology_correction_3D.cpp:17-607.
+#pragma once
+
+#include "common.cuh"
+
+namespace binder {
+
+struct JacStats {
+    double jmin, jmax;
+    long long below, above, negative;
+};
+
+// averaged 8-corner Jacobian of an AoS [V][3] field (FP64) -> J [V]
+void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const double vs[3],
+                       double *J, cudaStream_t s);
+
+// full correction on a host AoS field in grid units (in place)
+struct TopologyResult {
+    int outer_iterations;
+    int inner_iterations;
+    long long below_before, above_before, below_after, above_after;
+    unsigned flags;
+};
+TopologyResult topology_correct_3d(double *field_aos_host, double e1, double e2, int max_outer,
+                                   int max_inner, const double vs[3], int nx, int ny, int nz,
+                                   cudaStream_t s);
+
+}  // namespace binder

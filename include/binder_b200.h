@@ -1,0 +1,156 @@
+/*
+ * binder_b200 -- C ABI of the B200 (sm_100a) engine for BINDER's registration and Gibbs-sampling
+ * hot path.
+ *
+ * Every entry point replaces one method of the reference's pybind11 module `BINDER._core`
+ * (ste93ste/BINDER, BINDER/src/gpu/bindings.cpp for the CUDA backend, BINDER/src/cpu/bindings.cpp
+ * for the CPU backend); the citation beside each declaration names the binding it stands in for.
+ * Conventions:
+ *   - plain host pointers and sizes; the library copies inputs and writes caller-owned outputs
+ *     (the reference CPU backend instead keeps pointers into caller arrays);
+ *   - position fields are [Nx][Ny][Nz][3] C-order, components interleaved; bins are int32;
+ *     theta is [K][L] row-major (K = moving/node bins, L = fixed/voxel bins);
+ *   - every function returns 0 on success or a BINDER_STATUS_* code; binder_last_error() then
+ *     holds a message (thread-local).  Nothing here throws across the boundary.
+ * All work runs on the calling thread's current CUDA device, on a stream owned by the object.
+ */
+#ifndef BINDER_B200_H
+#define BINDER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BINDER_STATUS_OK 0
+#define BINDER_STATUS_INVALID_ARGUMENT 1
+#define BINDER_STATUS_CUDA_ERROR 2
+#define BINDER_STATUS_UNSUPPORTED 3
+#define BINDER_STATUS_NOT_READY 4
+#define BINDER_STATUS_DEVICE_FAULT 5
+
+/* device status bits reported by binder_registration_get_state */
+#define BINDER_FLAG_GAMMA_CAPPED 1u   /* a Marsaglia-Tsang gamma sampler hit its attempt cap */
+#define BINDER_FLAG_LIMITER_CAPPED 2u /* a topology limiter blend loop hit its step cap */
+#define BINDER_FLAG_NON_FINITE 4u     /* the min-log-posterior became non-finite */
+
+typedef struct binder_registration binder_registration;
+typedef struct binder_transform binder_transform;
+
+/* last error message of this thread ("" when none) */
+const char *binder_last_error(void);
+/* "b200" -- stands in for `_core.backend` ("cuda" / "cpu"), bindings.cpp:16 (gpu), :20 (cpu) */
+const char *binder_backend(void);
+/* 1: topology correction is built -- `_core.has_topology_correction`, probed at
+ * BINDER/FastRegistration.py:118-119 */
+int binder_has_topology_correction(void);
+
+/* ---- _core.Registration -------------------------------------------------------------------- */
+
+/* Registration(final_locations, threads, voxel_pos, node_pos, Nx_v, Ny_v, Nz_v, Nx_n, Ny_n, Nz_n,
+ *              spline_order, non_zero_voxels)                    gpu/bindings.cpp:18-47
+ * final_locations, voxel_pos, node_pos: [Nx_v*Ny_v*Nz_v*3] floats.  `threads` is accepted for
+ * interface parity and unused.  node_pos may be NULL (the reference never reads it). */
+int binder_registration_create(binder_registration **out, const float *final_locations,
+                               int threads, const float *voxel_pos, const float *node_pos,
+                               int Nx_v, int Ny_v, int Nz_v, int Nx_n, int Ny_n, int Nz_n,
+                               int spline_order, double non_zero_voxels);
+int binder_registration_destroy(binder_registration *h);
+
+/* setMILikelihood(alpha, theta, K, L, threads, binned_nodes, binned_voxels)   gpu/bindings.cpp:49-70
+ * theta [K*L]; binned_nodes [Nx_n*Ny_n*Nz_n] in [0, K); binned_voxels [Nx_v*Ny_v*Nz_v] in [0, L) */
+int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, const float *theta,
+                                          int K, int L, int threads, const int32_t *binned_nodes,
+                                          const int32_t *binned_voxels);
+
+/* setNonLinearTransformation(gamma_x..z, voxels_size_x..z, nodes_size_x..z, D)
+ *                                                               gpu/bindings.cpp:72-95; D [V] */
+int binder_registration_set_nonlinear_transformation(binder_registration *h, double gamma_x,
+                                                     double gamma_y, double gamma_z,
+                                                     double voxels_size_x, double voxels_size_y,
+                                                     double voxels_size_z, double nodes_size_x,
+                                                     double nodes_size_y, double nodes_size_z,
+                                                     const float *D);
+
+/* EM(max_EM_iterations, convergence_th, update_likelihood_parameters, debug)
+ *                                                               gpu/bindings.cpp:99-103
+ * *iterations_out (optional) receives the number of EM iterations run. */
+int binder_registration_em(binder_registration *h, int max_iterations, double convergence_th,
+                           int update_likelihood_parameters, int debug, int *iterations_out);
+
+/* sampler(seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
+ *         sample_likelihood_parameters, sample_transformation_parameters) -> (mean, cov)
+ *                                                               gpu/bindings.cpp:105-131
+ * mean_out [V*3] and cov_out [V*3*3] (M2 / (N_s - 1)) in FP64 (FP64 Welford accumulators). */
+int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, int N_s,
+                                int sample_gamma, int sample_gamma_every, int sample_posteriors,
+                                int sample_likelihood_parameters,
+                                int sample_transformation_parameters, double *mean_out,
+                                double *cov_out);
+
+/* get_final_locations_as_numpy_array() -> [Nx,Ny,Nz,3]          gpu/bindings.cpp:142-157 */
+int binder_registration_get_final_locations(const binder_registration *h, float *out);
+/* get_dream_locations() / set_dream_locations(arr)              gpu/bindings.cpp:133-140 */
+int binder_registration_get_dream_locations(const binder_registration *h, float *out);
+int binder_registration_set_dream_locations(binder_registration *h, const float *in);
+/* get_likelihood_parameters() -> K*L                            gpu/bindings.cpp:97 */
+int binder_registration_get_likelihood_parameters(const binder_registration *h, float *out);
+/* get_shape() -> (Nx, Ny, Nz, N)                                cpu/bindings.cpp:294 */
+int binder_registration_get_shape(const binder_registration *h, int out[4]);
+
+/* Per-iteration statistics of the last EM call, [n][4] = (min-log-likelihood, Dirichlet prior,
+ * deformation prior, min-log-posterior) in FP64 -- the values the reference prints at
+ * Registration.cpp:197-202.  Returns n (<= max_n) through *n_out. */
+int binder_registration_get_iteration_stats(const binder_registration *h, double *out, int max_n,
+                                            int *n_out);
+/* current gammas, nu, degenerate-voxel count and BINDER_FLAG_* bits; any pointer may be NULL */
+int binder_registration_get_state(const binder_registration *h, double gamma_out[3],
+                                  double *nu_out, unsigned long long *degenerate_out,
+                                  unsigned *flags_out);
+/* device time of the last EM / sampler call in milliseconds */
+int binder_registration_last_elapsed_ms(const binder_registration *h, double *ms_out);
+/* run the object's work on a caller stream (a cudaStream_t; NULL restores the object's own) */
+int binder_registration_set_stream(binder_registration *h, void *cuda_stream);
+/* Philox chain index, so independent chains with one seed draw disjoint streams */
+int binder_registration_set_chain(binder_registration *h, uint32_t chain);
+
+/* ---- _core.NonLinearTransformation --------------------------------------------------------- */
+
+/* NonLinearTransformation(gamma_x..z, voxels_size_x..z, nodes_size_x..z, D, Nx_v, Ny_v, Nz_v,
+ *                         threads, sigma_spline, spline_offset)   gpu/bindings.cpp:160-198 */
+int binder_transform_create(binder_transform **out, double gamma_x, double gamma_y,
+                            double gamma_z, double voxels_size_x, double voxels_size_y,
+                            double voxels_size_z, double nodes_size_x, double nodes_size_y,
+                            double nodes_size_z, const float *D, int Nx_v, int Ny_v, int Nz_v,
+                            int threads, double sigma_spline, double spline_offset);
+int binder_transform_destroy(binder_transform *h);
+/* smooth_deformation(field) -> (log_prior_deformation, field')  gpu/bindings.cpp:201-224 */
+int binder_transform_smooth_deformation(binder_transform *h, const float *field, float *out,
+                                        double *log_prior_out);
+/* sampleDeformationField(field, n) -> [n, Nx, Ny, Nz, 3]        gpu/bindings.cpp:226-255 */
+int binder_transform_sample_deformation_field(binder_transform *h, const float *field,
+                                              int number_of_samples, float *out);
+int binder_transform_get_shape(const binder_transform *h, int out[4]);
+
+/* ---- Jacobian determinant and topology correction ----------------------------------------- */
+
+/* compute_jacobian_determinant_3D(field, Nx, Ny, Nz, vx, vy, vz) -> [Nx,Ny,Nz]
+ *                                                               cpu/bindings.cpp:564-593
+ * FP64 in and out; evaluated on the GPU with the reference's arithmetic (bit-identical). */
+int binder_jacobian_determinant_3d(const double *field, int Nx, int Ny, int Nz, double voxel_size_x,
+                                   double voxel_size_y, double voxel_size_z, double *J_out);
+
+/* topology_correction_3D().correct_topology(h, e1, e2, max_outer_it, max_it, threads,
+ *                                           voxel_sizes, Nx, Ny, Nz) -> [Nx,Ny,Nz,3]
+ *                                                               gpu/bindings.cpp:259-287
+ * FP64 throughout.  stats_out (optional, 6 values): outer iterations, inner iterations,
+ * voxels with J < e1 before and after, voxels with J > e2 before and after. */
+int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
+                               int max_it, int threads, const double voxel_sizes[3], int Nx,
+                               int Ny, int Nz, double *out, long long *stats_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BINDER_B200_H */

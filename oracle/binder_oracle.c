@@ -395,6 +395,19 @@ double orc_smooth(const double *dream, const double *voxel_pos, const double *D,
     return cost;
 }
 
+/* NonLinearTransformation.cpp:280-341 */
+void orc_sample_field(const double *field, const double *D, const double gamma[3], double sigma,
+                      int nx, int ny, int nz, int n, uint64_t seed, uint32_t sweep0,
+                      double *out) {
+    const int N = (nz == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    double *zeros = (double *)calloc((size_t)V * N, sizeof(double));
+    for (int s = 0; s < n; ++s)
+        orc_smooth(field, zeros, D, gamma, sigma, nx, ny, nz, out + (size_t)s * V * N, 1, seed,
+                   sweep0 + (uint32_t)s, 0, NULL, NULL, NULL);
+    free(zeros);
+}
+
 /* Registration.cpp:122-217 */
 int orc_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
            double *theta, double alpha, const double *D, const double gamma[3], double sigma,

@@ -73,6 +73,13 @@ double orc_smooth(const double *dream, const double *voxel_pos, const double *D,
                   int add_noise, uint64_t seed, uint32_t sweep, uint32_t chain,
                   const double rho[3], const double eta[3], double *raw_reg);
 
+/* ---- prior sampling of a field: BINDER/src/cpu/NonLinearTransformation.cpp:280-341 ------------
+ * n samples of IDCT(DCT(field)/(1+gamma sigma^2 D) + noise) with zero voxel positions, sample s
+ * using sweep index sweep0 + s.  out [n*V*N]. */
+void orc_sample_field(const double *field, const double *D, const double gamma[3], double sigma,
+                      int nx, int ny, int nz, int n, uint64_t seed, uint32_t sweep0,
+                      double *out);
+
 /* ---- EM driver: BINDER/src/cpu/Registration.cpp:122-217 -------------------------------------- */
 typedef struct {
     double mll, log_prior_likelihood, log_prior_transformation, mlp;

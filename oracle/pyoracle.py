@@ -54,6 +54,7 @@ def _load_oracle():
     lib.orc_smooth.argtypes = [_dp, _dp, _dp, _dp, d, i, i, i, _dp, i, u64, u32, u32,
                                C.c_void_p, C.c_void_p, C.c_void_p]
     lib.orc_smooth.restype = d
+    lib.orc_sample_field.argtypes = [_dp, _dp, _dp, d, i, i, i, i, u64, u32, _dp]
     lib.orc_em.argtypes = [_dp, _dp, _ip, _ip, _dp, d, _dp, _dp, d] + [i] * 8 + \
         [d, i, d, i, C.c_void_p]
     lib.orc_em.restype = i
@@ -180,7 +181,7 @@ def dct3(x, inverse=False):
     x = _c64(x)
     out = np.zeros_like(x)
     nx, ny, nz = x.shape
-    lib().orc_dct3(x.ravel(), out.ravel() if False else out.reshape(-1), nx, ny, nz, int(inverse))
+    lib().orc_dct3(x.reshape(-1), out.reshape(-1), nx, ny, nz, int(inverse))
     return out
 
 
@@ -204,6 +205,17 @@ def smooth(dream, voxel_pos, D, gamma, sigma, shape, noise=None, rho=None, eta=N
     if want_raw:
         return cost, out, raw.value
     return cost, out
+
+
+def sample_field(field, D, gamma, sigma, shape, n, seed=1234, sweep0=0):
+    nx, ny, nz = shape
+    N = 2 if nz == 1 else 3
+    out = np.zeros(n * nx * ny * nz * N)
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    lib().orc_sample_field(_c64(field).ravel(), _c64(D).ravel(), g, float(sigma), nx, ny, nz,
+                           int(n), seed, sweep0, out)
+    return out.reshape(n, nx, ny, nz, N)
 
 
 def em(final_locations, voxel_pos, u, v, theta, alpha, D, gamma, sigma, vshape, nshape, K, L,

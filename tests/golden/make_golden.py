@@ -1,0 +1,93 @@
+"""Generate the golden fixtures in this directory from the reference's own CPU sources.
+
+The reference's Spline.cpp, MILikelihood.cpp, utils.cpp, DCT.cpp, FFT.cpp,
+NonLinearTransformation.cpp and topology_correction_3D.cpp are compiled unmodified by
+oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in
+oracle/ref_shim).  This script feeds them seeded inputs and stores inputs and outputs as small
+.npz files, so the parity tests are pinned to the reference even where its sources are absent.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle  # noqa: E402
+
+
+def grid(shape):
+    return np.stack(np.indices(shape), -1).astype(np.float64)
+
+
+def main():
+    R = pyoracle.ref_lib()
+    if R is None:
+        pyoracle.build()
+        R = pyoracle.ref_lib()
+    assert R is not None, "oracle/_ref/libbinder_ref.so could not be built"
+    rng = np.random.default_rng(20260101)
+
+    # spline weights, orders 1-3 (Spline.cpp:44-109)
+    ds = np.concatenate([[0.0, 0.5, 1.0 - 1e-12], rng.random(13)])
+    W = np.zeros((3, ds.size, 4))
+    for o in (1, 2, 3):
+        for i, d in enumerate(ds):
+            w = np.zeros(4)
+            R.ref_spline(o, float(d), w)
+            W[o - 1, i] = w
+    np.savez(os.path.join(HERE, "spline_ref.npz"), d=ds, weights=W)
+
+    # Jacobian determinant (utils.cpp:100-345): smooth field with folds, anisotropic voxels
+    shape = (9, 11, 10)
+    f = grid(shape) + rng.normal(0, 0.45, shape + (3,))
+    vs = np.array([1.1, 0.9, 1.3])
+    J = np.zeros(np.prod(shape))
+    R.ref_jacobian3d(f.ravel(), *shape, *vs, J)
+    np.savez(os.path.join(HERE, "jacobian_ref.npz"), field=f, shape=shape, vs=vs, J=J)
+
+    # topology correction (topology_correction_3D.cpp:17-143)
+    cases = {}
+    for k, (shape, sig, vs) in enumerate([((8, 9, 10), 0.45, (1.0, 1.2, 0.9)),
+                                         ((12, 10, 11), 0.55, (1.0, 1.0, 1.0))]):
+        f = grid(shape) + rng.normal(0, sig, shape + (3,))
+        out = np.zeros(f.size)
+        R.ref_topology3d(f.ravel(), 0.01, 100.0, 10, 10, np.asarray(vs, float), *shape, out)
+        cases[f"field{k}"] = f
+        cases[f"shape{k}"] = np.array(shape)
+        cases[f"vs{k}"] = np.array(vs, float)
+        cases[f"out{k}"] = out.reshape(f.shape)
+    np.savez(os.path.join(HERE, "topology_ref.npz"), e1=0.01, e2=100.0, max_outer=10,
+             max_inner=10, **cases)
+
+    # DCT smoothing + prior cost (NonLinearTransformation.cpp:226-278)
+    shape = (11, 20, 7)
+    field = rng.standard_normal(shape + (3,))
+    from binder_b200.utils import initialize_fourier_domain_smoothing
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).ravel()
+    gamma = np.array([5.0, 3.0, 7.0])
+    one = np.ones(3)
+    out = np.zeros(field.size)
+    cost = R.ref_smooth_deformation(gamma, one, one, D, *shape, 1.0, 0.0, field.ravel(), out)
+    np.savez(os.path.join(HERE, "smoothing_ref.npz"), field=field, D=D, gamma=gamma, sigma=1.0,
+             out=out.reshape(field.shape), cost=cost)
+
+    # MI parameter update and Dirichlet cost (MILikelihood.cpp:33-124)
+    K, L = 16, 12
+    hist = rng.random((K, L)) * 50.0
+    th0 = np.full((K, L), 1.0 / L)
+    th = np.zeros(K * L)
+    cost = R.ref_mi_update(2.0, th0.ravel(), hist.ravel(), K, L, th)
+    np.savez(os.path.join(HERE, "mi_ref.npz"), hist=hist, alpha=2.0, theta=th.reshape(K, L),
+             cost=cost)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

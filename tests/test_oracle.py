@@ -1,0 +1,136 @@
+"""The FP64 oracle against the reference's own outputs (golden fixtures from its compiled CPU
+sources), published known-answer vectors, and the analytic checks of the reference's tests."""
+import numpy as np
+import pytest
+from scipy import fft as sfft
+
+from conftest import golden
+
+
+# Random123 known-answer vectors for philox4x32-10 (Salmon et al., SC'11 distribution)
+PHILOX_KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+    ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+    ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+     [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(oracle, ctr, key, want):
+    assert list(oracle.philox(ctr, key)) == want
+
+
+def test_spline_matches_reference(oracle):
+    g = golden("spline_ref.npz")
+    for d, w in zip(g["d"], g["weights"][2]):
+        np.testing.assert_allclose(oracle.spline3(d), w, rtol=0, atol=1e-15)
+    # partition of unity (tests/cpu/test_check_spline.py)
+    for d in np.linspace(0, 1, 17, endpoint=False):
+        assert abs(oracle.spline3(d).sum() - 1.0) < 1e-14
+
+
+def test_jacobian_bit_exact_vs_reference(oracle):
+    g = golden("jacobian_ref.npz")
+    J = oracle.jacobian3d(g["field"], tuple(g["shape"]), g["vs"])
+    assert np.array_equal(J, g["J"])
+    assert (J < 0).sum() > 0  # the fixture has folds
+
+
+def test_topology_matches_reference(oracle):
+    g = golden("topology_ref.npz")
+    for k in range(2):
+        shape = tuple(int(s) for s in g[f"shape{k}"])
+        out, outer = oracle.topology3d(g[f"field{k}"], g["e1"], g["e2"], 10, 10, g[f"vs{k}"], shape)
+        ref = g[f"out{k}"].ravel()
+        np.testing.assert_allclose(out, ref, rtol=0, atol=1e-9)
+        Jo = oracle.jacobian3d(out, shape)
+        Jr = oracle.jacobian3d(ref, shape)
+        assert np.array_equal(Jo < 0.01, Jr < 0.01)
+        assert (oracle.jacobian3d(g[f"field{k}"], shape) < 0).sum() > 0
+
+
+def test_smoothing_matches_reference(oracle):
+    g = golden("smoothing_ref.npz")
+    shape = g["field"].shape[:3]
+    zeros = np.zeros_like(g["field"])
+    cost, out = oracle.smooth(g["field"], zeros, g["D"], g["gamma"], float(g["sigma"]), shape)
+    np.testing.assert_allclose(out.reshape(g["out"].shape), g["out"], rtol=0, atol=1e-12)
+    assert cost == pytest.approx(float(g["cost"]), rel=1e-12)
+
+
+def test_dct_is_scipy_ortho(oracle):
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((5, 8, 7))
+    np.testing.assert_allclose(oracle.dct3(x), sfft.dctn(x, norm="ortho"), atol=1e-12)
+    np.testing.assert_allclose(oracle.dct3(oracle.dct3(x), inverse=True), x, atol=1e-12)
+
+
+def test_smoothing_equals_mirrored_dft(oracle):
+    """tests/gpu/test_smoothing_and_log_cost.py: DCT smoothing equals a DFT of the mirrored
+    signal with the full eigenvalue matrix, and the prior cost agrees (restated)."""
+    from binder_b200.utils import initialize_fourier_domain_smoothing
+    rng = np.random.default_rng(7)
+    shape = (11, 20, 7)
+    gamma = 5.0
+    field = rng.standard_normal(shape + (3,))
+    D, Dfull = initialize_fourier_domain_smoothing(shape, True, 2, 3, return_full_matrix=True)
+    cost, out = oracle.smooth(field, np.zeros_like(field), D, [gamma] * 3, 1.0, shape)
+    out = out.reshape(field.shape)
+    cost_fft = 0.0
+    for n in range(3):
+        m = field[..., n]
+        for ax in range(3):
+            m = np.concatenate([m, np.flip(m, axis=ax)], axis=ax)
+        C = np.fft.fftn(m) / m.size / (1 + gamma * Dfull)
+        cost_fft += 0.5 * gamma * m.size * np.sum(Dfull * np.abs(C) ** 2) / 8
+        t = np.fft.ifftn(C).real * m.size
+        np.testing.assert_allclose(t[:shape[0], :shape[1], :shape[2]], out[..., n], atol=1e-10)
+    assert cost == pytest.approx(cost_fft, rel=1e-9)
+
+
+def test_mi_update_matches_reference(oracle):
+    g = golden("mi_ref.npz")
+    K, L = g["hist"].shape
+    th = oracle.theta_map(g["hist"], K, L, float(g["alpha"]))
+    np.testing.assert_allclose(th.reshape(K, L), g["theta"], rtol=1e-15, atol=0)
+    assert oracle.dirichlet_cost(th, K, L, float(g["alpha"])) == pytest.approx(float(g["cost"]),
+                                                                               rel=1e-13)
+
+
+def _prior_covariance(shape, gamma, sigma, order):
+    """sigma^2 (I + gamma sigma^2 Gamma)^-1 with Neumann finite differences
+    (tests/gpu/test_sampling_DCT_3D.py), in Fortran voxel order."""
+    Nx, Ny, Nz = shape
+
+    def d1(n):
+        G = np.diag(np.ones(n)) - np.diag(np.ones(n - 1), -1)
+        return G[1:, :]
+
+    gp = gamma * sigma ** 2
+    N = Nx * Ny * Nz
+    if order == 1:
+        Gr = np.kron(np.eye(Nz), np.kron(np.eye(Ny), d1(Nx)))
+        Gc = np.kron(np.eye(Nz), np.kron(d1(Ny), np.eye(Nx)))
+        Gd = np.kron(d1(Nz), np.kron(np.eye(Nx), np.eye(Ny)))
+        A = np.eye(N) + gp * (Gr.T @ Gr + Gc.T @ Gc + Gd.T @ Gd)
+    else:
+        G2 = [d1(n).T @ d1(n) for n in (Nx, Ny, Nz)]
+        G = np.kron(np.eye(Nz), np.kron(np.eye(Ny), G2[0])) + \
+            np.kron(np.eye(Nz), np.kron(G2[1], np.eye(Nx))) + \
+            np.kron(G2[2], np.kron(np.eye(Nx), np.eye(Ny)))
+        A = np.eye(N) + gp * G.T @ G
+    return sigma ** 2 * np.linalg.inv(A)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_prior_sampling_covariance(oracle, order):
+    """tests/gpu/test_sampling_DCT_3D.py restated on the oracle's prior sampler (1e5 samples)."""
+    from binder_b200.utils import initialize_fourier_domain_smoothing
+    shape, gamma, sigma = (3, 5, 4), 5.0, 0.34
+    cov = _prior_covariance(shape, gamma, sigma, order)
+    D = initialize_fourier_domain_smoothing(shape, True, order, 3)
+    s = oracle.sample_field(np.zeros(shape + (3,)), D, [gamma] * 3, sigma, shape, 100000, seed=99)
+    x = s[..., 0].reshape(-1, np.prod(shape), order="F")
+    emp = x.T @ x / x.shape[0]
+    np.testing.assert_allclose(emp, cov, rtol=1e-3, atol=1e-3)
