@@ -162,6 +162,33 @@ class Registration:
     def set_chain(self, chain):
         check(lib().binder_registration_set_chain(self._h, int(chain)))
 
+    def stream(self):
+        """The object's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
+        p = C.c_void_p()
+        check(lib().binder_registration_get_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def profile_stage(self, stage, n=10):
+        """Average ms of one launch of stage 0 (E-step), 1 (M-step) or 2 (theta update), timed
+        with CUDA events; leaves positions unspecified (call reset() afterwards)."""
+        ms = C.c_double(0)
+        check(lib().binder_registration_profile_stage(self._h, int(stage), int(n), C.byref(ms)))
+        return ms.value
+
+    def reset(self):
+        """Restore creation-time positions and theta on the device (no host transfer)."""
+        check(lib().binder_registration_reset(self._h))
+
+    def correct_topology(self, e1, e2, max_outer_it, max_it, voxel_sizes):
+        """Topology correction of this object's positions on the device, in place (replaces the
+        host round trip of FastRegistration.py:527-546).  Returns the iteration / count stats."""
+        stats = np.zeros(6, np.int64)
+        check(lib().binder_registration_correct_topology(
+            self._h, float(e1), float(e2), int(max_outer_it), int(max_it),
+            _f64(voxel_sizes, 3, "voxel_sizes"), stats.ctypes.data))
+        return dict(zip(["outer_iterations", "inner_iterations", "below_e1_before",
+                         "below_e1_after", "above_e2_before", "above_e2_after"], stats.tolist()))
+
 
 class NonLinearTransformation:
     """``_core.NonLinearTransformation`` (gpu/bindings.cpp:160-255)."""
@@ -224,6 +251,11 @@ class topology_correction_3D:
                                     "below_e1_after", "above_e2_before", "above_e2_after"],
                                    stats.tolist()))
         return out.reshape(int(Nx_v), int(Ny_v), int(Nz_v), 3)
+
+
+def kernel_launch_count():
+    """Kernels launched by the library in this process (graph replays count every node)."""
+    return int(lib().binder_kernel_launch_count())
 
 
 def compute_jacobian_determinant_3D(field, Nx, Ny, Nz, voxel_size_x, voxel_size_y, voxel_size_z):

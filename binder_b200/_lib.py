@@ -27,6 +27,9 @@ EXPORTS = [
     "binder_registration_get_shape", "binder_registration_get_iteration_stats",
     "binder_registration_get_state", "binder_registration_last_elapsed_ms",
     "binder_registration_set_stream", "binder_registration_set_chain",
+    "binder_registration_reset", "binder_registration_correct_topology",
+    "binder_kernel_launch_count", "binder_registration_get_stream",
+    "binder_registration_profile_stage",
     "binder_transform_create", "binder_transform_destroy",
     "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
     "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
@@ -53,6 +56,7 @@ def _declare(lib):
     lib.binder_last_error.restype = C.c_char_p
     lib.binder_backend.restype = C.c_char_p
     lib.binder_has_topology_correction.restype = _i
+    lib.binder_kernel_launch_count.restype = C.c_longlong
     sig = {
         "binder_registration_create": [C.POINTER(_P), _f32, _i, _f32, _P] + [_i] * 7 + [_d],
         "binder_registration_destroy": [_P],
@@ -71,6 +75,10 @@ def _declare(lib):
         "binder_registration_last_elapsed_ms": [_P, C.POINTER(_d)],
         "binder_registration_set_stream": [_P, _P],
         "binder_registration_set_chain": [_P, _u32],
+        "binder_registration_reset": [_P],
+        "binder_registration_get_stream": [_P, C.POINTER(_P)],
+        "binder_registration_profile_stage": [_P, _i, _i, C.POINTER(_d)],
+        "binder_registration_correct_topology": [_P, _d, _d, _i, _i, _f64, _P],
         "binder_transform_create": [C.POINTER(_P)] + [_d] * 9 + [_f32, _i, _i, _i, _i, _d, _d],
         "binder_transform_destroy": [_P],
         "binder_transform_smooth_deformation": [_P, _f32, _f32, C.POINTER(_d)],

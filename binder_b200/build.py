@@ -36,6 +36,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(ROOT, "include", "binder_b200.h"))
     hdr_time = _newest(headers)
+    src_time = max(hdr_time, _newest([os.path.join(CSRC, s) for s in SOURCES]))
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= src_time:
+        return LIB  # up to date (objects may be absent where only the library was shipped)
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)

@@ -208,6 +208,49 @@ int binder_registration_set_chain(binder_registration *h, uint32_t chain) {
     });
 }
 
+int binder_registration_reset(binder_registration *h) {
+    return guard([&] {
+        NEED(h);
+        h->impl->reset();
+    });
+}
+
+int binder_registration_correct_topology(binder_registration *h, double e1, double e2,
+                                         int max_outer_it, int max_it,
+                                         const double voxel_sizes[3], long long *stats_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(voxel_sizes);
+        const auto r = h->impl->correct_topology(e1, e2, max_outer_it, max_it, voxel_sizes);
+        if (stats_out) {
+            stats_out[0] = r.outer_iterations;
+            stats_out[1] = r.inner_iterations;
+            stats_out[2] = r.below_before;
+            stats_out[3] = r.below_after;
+            stats_out[4] = r.above_before;
+            stats_out[5] = r.above_after;
+        }
+    });
+}
+
+int binder_registration_get_stream(const binder_registration *h, void **stream_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(stream_out);
+        *stream_out = reinterpret_cast<void *>(h->impl->stream());
+    });
+}
+
+int binder_registration_profile_stage(binder_registration *h, int stage, int n, double *avg_ms_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(avg_ms_out);
+        *avg_ms_out = h->impl->profile_stage(stage, n);
+    });
+}
+
+long long binder_kernel_launch_count(void) { return binder::launch_counter(); }
+
 int binder_transform_create(binder_transform **out, double gamma_x, double gamma_y,
                             double gamma_z, double voxels_size_x, double voxels_size_y,
                             double voxels_size_z, double nodes_size_x, double nodes_size_y,

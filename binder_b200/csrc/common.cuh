@@ -125,4 +125,8 @@ __device__ __forceinline__ T block_sum(T v, T *scratch) {
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// process-wide count of kernels this library has launched (graph replays count every node)
+long long &launch_counter();
+inline void count_launch(long long n = 1) { launch_counter() += n; }
+
 }  // namespace binder

@@ -42,7 +42,39 @@ struct Graph {
     }
 };
 
+// Capture `enqueue` into `graph` on stream s.  Kernels counted while capturing are taken back out
+// of the launch counter and returned, so each replay can add them again.
+template <typename F>
+long long capture_graph(cudaStream_t s, Graph &graph, F &&enqueue) {
+    const long long before = launch_counter();
+    BINDER_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    try {
+        enqueue();
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        launch_counter() = before;
+        throw;
+    }
+    BINDER_CUDA(cudaStreamEndCapture(s, &graph.g));
+    BINDER_CUDA(cudaGraphInstantiate(&graph.e, graph.g, 0));
+    const long long captured = launch_counter() - before;
+    launch_counter() = before;
+    return captured;
+}
+
+void replay(const Graph &graph, long long kernels, cudaStream_t s) {
+    BINDER_CUDA(cudaGraphLaunch(graph.e, s));
+    count_launch(kernels);
+}
+
 }  // namespace
+
+long long &launch_counter() {
+    static long long counter = 0;
+    return counter;
+}
 
 void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa) {
     soa.resize((size_t)V * N);
@@ -163,6 +195,8 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
         x_ = dalloc<float>((size_t)V_ * 3);
         BINDER_CUDA(cudaMemcpy(x_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
     }
+    d0_ = dalloc<float>((size_t)V_ * 3);
+    BINDER_CUDA(cudaMemcpy(d0_, d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice));
     std::vector<float> zeros((size_t)V_ * 3, 0.0f);
     set_dream_locations(zeros.data());
     mstep_.init(nx, ny, nz);
@@ -173,6 +207,8 @@ Registration::~Registration() {
     if (own_stream_) cudaStreamDestroy(own_stream_);
     dfree(d_); dfree(x_); dfree(r_); dfree(D_); dfree(theta_); dfree(hist_); dfree(hcnt_);
     dfree(u_); dfree(vpad_); dfree(mean_); dfree(m2_); dfree(stats_); dfree(st_);
+    dfree(d0_); dfree(theta0_);
+    delete topo_;
     mstep_.release();
 }
 
@@ -205,8 +241,9 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
                                                       " outside [0, K) at node " + std::to_string(j));
                 vp[((size_t)(x + P_) * pyn_ + (y + P_)) * zp_ + (z + PZ_)] = (uint8_t)b;
             }
-    dfree(u_); dfree(vpad_); dfree(theta_); dfree(hist_); dfree(hcnt_);
+    dfree(u_); dfree(vpad_); dfree(theta_); dfree(hist_); dfree(hcnt_); dfree(theta0_);
     u_ = dalloc<uint8_t>((size_t)V_);
+    theta0_ = dalloc<float>((size_t)K * L);
     vpad_ = dalloc<uint8_t>(padded);
     theta_ = dalloc<float>((size_t)K * L);
     hist_ = dalloc<float>((size_t)K * L);
@@ -214,6 +251,7 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     BINDER_CUDA(cudaMemcpy(u_, u.data(), V_, cudaMemcpyHostToDevice));
     BINDER_CUDA(cudaMemcpy(vpad_, vp.data(), padded, cudaMemcpyHostToDevice));
     BINDER_CUDA(cudaMemcpy(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpy(theta0_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice));
     BINDER_CUDA(cudaMemset(hist_, 0, sizeof(float) * K * L));
     BINDER_CUDA(cudaMemset(hcnt_, 0, sizeof(unsigned) * K * L));
     K_ = K;
@@ -292,23 +330,15 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
     BINDER_CUDA(cudaEventCreate(&t1));
     const int chunk = max_iterations < 8 ? max_iterations : 8;
     Graph graph;
-    BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
-    try {
+    const long long kernels = capture_graph(stream_, graph, [&] {
         for (int c = 0; c < chunk; ++c) enqueue_em_iteration(max_iterations, convergence_th, update);
-    } catch (...) {
-        cudaGraph_t g;
-        cudaStreamEndCapture(stream_, &g);
-        if (g) cudaGraphDestroy(g);
-        throw;
-    }
-    BINDER_CUDA(cudaStreamEndCapture(stream_, &graph.g));
-    BINDER_CUDA(cudaGraphInstantiate(&graph.e, graph.g, 0));
+    });
 
     BINDER_CUDA(cudaEventRecord(t0, stream_));
     DevState h{};
     int launched = 0;
     while (true) {
-        BINDER_CUDA(cudaGraphLaunch(graph.e, stream_));
+        replay(graph, kernels, stream_);
         launched += chunk;
         BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));
@@ -363,8 +393,7 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
         const int chunk = total < 16 ? total : 16;
         BINDER_CUDA(cudaDeviceSynchronize());
         Graph graph;
-        BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
-        try {
+        const long long kernels = capture_graph(stream_, graph, [&] {
             for (int c = 0; c < chunk; ++c) {
                 if (sample_posteriors) {
                     EStepArgs e{};
@@ -387,19 +416,12 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
                 }
                 launch_sweep_end(d_, mean_, m2_, V_, N_b, total, st_, stream_);
             }
-        } catch (...) {
-            cudaGraph_t g;
-            cudaStreamEndCapture(stream_, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-        }
-        BINDER_CUDA(cudaStreamEndCapture(stream_, &graph.g));
-        BINDER_CUDA(cudaGraphInstantiate(&graph.e, graph.g, 0));
+        });
         cudaEvent_t t0, t1;
         BINDER_CUDA(cudaEventCreate(&t0));
         BINDER_CUDA(cudaEventCreate(&t1));
         BINDER_CUDA(cudaEventRecord(t0, stream_));
-        for (int done = 0; done < total; done += chunk) BINDER_CUDA(cudaGraphLaunch(graph.e, stream_));
+        for (int done = 0; done < total; done += chunk) replay(graph, kernels, stream_);
         BINDER_CUDA(cudaEventRecord(t1, stream_));
         BINDER_CUDA(cudaEventSynchronize(t1));
         float ms = 0.0f;
@@ -423,6 +445,66 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
             for (int c = 0; c < 3; ++c)
                 cov_out[i * 9 + r * 3 + c] = m2[(size_t)sym[r][c] * V_ + i] * inv;
     }
+}
+
+double Registration::profile_stage(int stage, int n) {
+    require_ready();
+    BINDER_CHECK(stage >= 0 && stage <= 2, "stage must be 0 (E-step), 1 (M-step) or 2 (theta)");
+    BINDER_CHECK(n >= 1, "n must be >= 1");
+    reset_state(false);
+    EStepArgs e{};
+    e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_; e.hist = hist_;
+    e.hcnt = hcnt_; e.st = st_; e.skip = nullptr; e.V = V_;
+    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
+    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
+    e.seed = seed_; e.chain = chain_;
+    const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+    auto one = [&] {
+        if (stage == 0) launch_estep(e, false, egrid_e_, stream_);
+        else if (stage == 1)
+            mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
+                           rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
+        else launch_theta_update(theta_, hist_, K_, L_, alpha_, 1, st_, stream_);
+    };
+    one();  // warm-up
+    cudaEvent_t t0, t1;
+    BINDER_CUDA(cudaEventCreate(&t0));
+    BINDER_CUDA(cudaEventCreate(&t1));
+    BINDER_CUDA(cudaEventRecord(t0, stream_));
+    for (int i = 0; i < n; ++i) one();
+    BINDER_CUDA(cudaEventRecord(t1, stream_));
+    BINDER_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    return ms / n;
+}
+
+void Registration::reset() {
+    BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice, stream_));
+    if (have_mi_) {
+        BINDER_CUDA(cudaMemcpyAsync(theta_, theta0_, sizeof(float) * K_ * L_,
+                                    cudaMemcpyDeviceToDevice, stream_));
+        BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
+        BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K_ * L_, stream_));
+    }
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    reset_state(false);
+}
+
+TopologyResult Registration::correct_topology(double e1, double e2, int max_outer, int max_inner,
+                                              const double vs[3]) {
+    BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
+                 "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
+    if (!topo_) topo_ = new TopologyWorkspace(nx_, ny_, nz_);
+    topo_->load_float_grid(d_, vs, stream_);
+    TopologyResult r = topo_->run(e1, e2, max_outer, max_inner, vs, stream_);
+    topo_->store_float_grid(d_, vs, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    return r;
 }
 
 void Registration::get_final_locations(float *out) const {
@@ -566,35 +648,26 @@ void PriorTransform::sample(const float *field, int n, float *out) {
     chunk_ = dalloc<float>((size_t)B * V_ * 3);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     const double rho_p = rho_[0] * rho_[1] * rho_[2];
-    auto capture = [&](int count, Graph &g) {
-        BINDER_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
-        try {
-            for (int j = 0; j < count; ++j) {
-                mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 1, 0, 1, seed_, 0, rho_p, eta2,
-                               nullptr, stream_);
-                BINDER_CUDA(cudaMemcpyAsync(chunk_ + (size_t)j * V_ * 3, d_, sizeof(float) * V_ * 3,
-                                            cudaMemcpyDeviceToDevice, stream_));
-                launch_sweep_advance(st_, 0x7fffffff, stream_);
-            }
-        } catch (...) {
-            cudaGraph_t gg;
-            cudaStreamEndCapture(stream_, &gg);
-            if (gg) cudaGraphDestroy(gg);
-            throw;
+    auto enqueue = [&](int count) {
+        for (int j = 0; j < count; ++j) {
+            mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 1, 0, 1, seed_, 0, rho_p, eta2,
+                           nullptr, stream_);
+            BINDER_CUDA(cudaMemcpyAsync(chunk_ + (size_t)j * V_ * 3, d_, sizeof(float) * V_ * 3,
+                                        cudaMemcpyDeviceToDevice, stream_));
+            launch_sweep_advance(st_, 0x7fffffff, stream_);
         }
-        BINDER_CUDA(cudaStreamEndCapture(stream_, &g.g));
-        BINDER_CUDA(cudaGraphInstantiate(&g.e, g.g, 0));
     };
     BINDER_CUDA(cudaDeviceSynchronize());
     Graph full, tail;
-    capture(B, full);
+    const long long k_full = capture_graph(stream_, full, [&] { enqueue(B); });
     const int rem = n % B;
-    if (rem) capture(rem, tail);
+    long long k_tail = 0;
+    if (rem) k_tail = capture_graph(stream_, tail, [&] { enqueue(rem); });
     std::vector<float> host((size_t)B * V_ * 3);
     int done = 0;
     while (done < n) {
         const int cnt = (n - done) >= B ? B : rem;
-        BINDER_CUDA(cudaGraphLaunch(cnt == B ? full.e : tail.e, stream_));
+        if (cnt == B) replay(full, k_full, stream_); else replay(tail, k_tail, stream_);
         BINDER_CUDA(cudaMemcpyAsync(host.data(), chunk_, sizeof(float) * (size_t)cnt * V_ * 3,
                                     cudaMemcpyDeviceToHost, stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));

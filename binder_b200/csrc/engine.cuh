@@ -46,6 +46,13 @@ class Registration {
                  int sample_posteriors, int sample_likelihood_parameters,
                  int sample_transformation_parameters, double *mean_out, double *cov_out);
 
+    // restore the positions given at construction, the theta given to set_mi_likelihood and a
+    // fresh device state (device-to-device, no host transfer)
+    void reset();
+    // topology correction of the object's own positions on the device (FP64), in place
+    TopologyResult correct_topology(double e1, double e2, int max_outer, int max_inner,
+                                    const double vs[3]);
+
     void get_final_locations(float *out) const;      // AoS [V][3]
     void set_final_locations(const float *in);
     void get_dream_locations(float *out) const;      // AoS [V][3]
@@ -58,6 +65,9 @@ class Registration {
     void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
     void set_chain(uint32_t c) { chain_ = c; }
     double last_elapsed_ms() const { return last_ms_; }
+    cudaStream_t stream() const { return stream_; }
+    // average ms per launch of stage 0 (E-step), 1 (M-step) or 2 (theta update), n eager launches
+    double profile_stage(int stage, int n);
 
     int K() const { return K_; }
     int L() const { return L_; }
@@ -74,7 +84,8 @@ class Registration {
     uint32_t chain_ = 0;
     // device buffers
     float *d_ = nullptr, *x_ = nullptr, *r_ = nullptr, *D_ = nullptr, *theta_ = nullptr,
-          *hist_ = nullptr;
+          *hist_ = nullptr, *d0_ = nullptr, *theta0_ = nullptr;
+    TopologyWorkspace *topo_ = nullptr;
     unsigned *hcnt_ = nullptr;
     uint8_t *u_ = nullptr, *vpad_ = nullptr;
     double *mean_ = nullptr, *m2_ = nullptr, *stats_ = nullptr;

@@ -406,35 +406,35 @@ int estep_grid(bool sample, int K, int L, long V) {
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s) {
     const size_t smem = (size_t)2 * a.K * a.L * sizeof(float);
     if (sample)
-        estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
+        count_launch(), estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
     else
-        estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
+        count_launch(), estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, int update,
                          DevState *st, cudaStream_t s) {
-    theta_update_kernel<<<1, 1024, 0, s>>>(theta, hist, K, L, alpha, update, st);
+    count_launch(), theta_update_kernel<<<1, 1024, 0, s>>>(theta, hist, K, L, alpha, update, st);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void launch_dirichlet_sample(float *theta, unsigned *hcnt, int K, int L, double alpha,
                              uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s) {
     const int threads = ((L + 31) / 32) * 32;
-    dirichlet_sample_kernel<<<K, threads, 0, s>>>(theta, hcnt, K, L, alpha, seed, chain, st);
+    count_launch(), dirichlet_sample_kernel<<<K, threads, 0, s>>>(theta, hcnt, K, L, alpha, seed, chain, st);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, double rho_p,
                       const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s) {
-    nu_sample_kernel<<<1, 1, 0, s>>>(st, sample_gamma, every, N, V, rho_p, eta2[0], eta2[1],
+    count_launch(), nu_sample_kernel<<<1, 1, 0, s>>>(st, sample_gamma, every, N, V, rho_p, eta2[0], eta2[1],
                                      eta2[2], seed, chain);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void launch_em_finish(DevState *st, double *stats, int max_iter, double th, double nzv,
                       cudaStream_t s) {
-    em_finish_kernel<<<1, 1, 0, s>>>(st, stats, max_iter, th, nzv);
+    count_launch(), em_finish_kernel<<<1, 1, 0, s>>>(st, stats, max_iter, th, nzv);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -445,13 +445,13 @@ void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N_b,
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     long need = (V + 255) / 256;
     const long g = need < (long)sms * 8 ? (need < 1 ? 1 : need) : (long)sms * 8;
-    sweep_end_kernel<<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    count_launch(), sweep_end_kernel<<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
     BINDER_CUDA(cudaGetLastError());
     launch_sweep_advance(st, total, s);
 }
 
 void launch_sweep_advance(DevState *st, int total, cudaStream_t s) {
-    sweep_advance_kernel<<<1, 1, 0, s>>>(st, total);
+    count_launch(), sweep_advance_kernel<<<1, 1, 0, s>>>(st, total);
     BINDER_CUDA(cudaGetLastError());
 }
 

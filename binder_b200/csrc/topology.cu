@@ -372,67 +372,91 @@ Red read_red(const Red *r, cudaStream_t s) {
 void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const double vs[3],
                        double *J, cudaStream_t s) {
     const long V = (long)nx * ny * nz;
-    jacobian_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, 3, 1, nx, ny, nz,
+    count_launch(), jacobian_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, 3, 1, nx, ny, nz,
                                                 1.0 / (vs[0] * vs[1] * vs[2]), J, 0.0, 0.0, nullptr);
     BINDER_CUDA(cudaGetLastError());
 }
 
-TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_outer,
-                                   int max_inner, const double vs[3], int nx, int ny, int nz,
-                                   cudaStream_t s) {
+namespace {
+__global__ void float_soa_to_physical_kernel(const float *d, long V, double s0, double s1, double s2,
+                                             double *pos) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        pos[p] = (double)d[p] * s0;
+        pos[V + p] = (double)d[V + p] * s1;
+        pos[2 * V + p] = (double)d[2 * V + p] * s2;
+    }
+}
+__global__ void physical_to_float_soa_kernel(const double *pos, long V, double s0, double s1,
+                                             double s2, float *d) {
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        d[p] = (float)(pos[p] / s0);
+        d[V + p] = (float)(pos[V + p] / s1);
+        d[2 * V + p] = (float)(pos[2 * V + p] / s2);
+    }
+}
+}  // namespace
+
+struct TopologyWorkspace::Impl {
+    int nx, ny, nz;
+    long V, cells;
+    DBuf<double> pos, grad, jc, div, t1, t2;
+    DBuf<int> list, sorted;
+    DBuf<Red> red;
+    DBuf<unsigned> flags;
+    DBuf<double> H[3], cs[3];
+    Impl(int x, int y, int z)
+        : nx(x), ny(y), nz(z), V((long)x * y * z), cells((long)(x - 1) * (y - 1) * (z - 1)),
+          pos(V * 3), grad(V * 9), jc(cells * 8), div(V * 3), t1(V * 3), t2(V * 3), list(cells),
+          sorted(cells), red(1), flags(1),
+          H{DBuf<double>((size_t)x * x), DBuf<double>((size_t)y * y), DBuf<double>((size_t)z * z)},
+          cs{DBuf<double>(x), DBuf<double>(y), DBuf<double>(z)} {
+        const int dims[3] = {x, y, z};
+        const double pi = 3.14159265358979323846;
+        for (int a = 0; a < 3; ++a) {
+            const int n = dims[a];
+            std::vector<double> M((size_t)n * n), c(n);
+            hartley_matrix(n, M.data());
+            for (int k = 0; k < n; ++k) c[k] = std::cos(2.0 * pi * k / (n * 1.0));
+            BINDER_CUDA(cudaMemcpy(H[a].p, M.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
+            BINDER_CUDA(cudaMemcpy(cs[a].p, c.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        }
+    }
+};
+
+TopologyWorkspace::TopologyWorkspace(int nx, int ny, int nz) {
     BINDER_CHECK(nx >= 2 && ny >= 2 && nz >= 2, "topology correction needs at least 2 voxels per axis");
     BINDER_CHECK(nx <= 256 && ny <= 256 && nz <= 256, "topology correction supports axes up to 256");
+    impl_ = new Impl(nx, ny, nz);
+}
+TopologyWorkspace::~TopologyWorkspace() { delete impl_; }
+double *TopologyWorkspace::positions() { return impl_->pos.p; }
+
+// BINDER/src/cpu/topology_correction_3D.cpp:17-143 on the workspace's SoA physical positions
+TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int max_inner,
+                                      const double vs[3], cudaStream_t s) {
     BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
-    const long V = (long)nx * ny * nz;
-    const long cells = (long)(nx - 1) * (ny - 1) * (nz - 1);
+    Impl &w = *impl_;
+    const int nx = w.nx, ny = w.ny, nz = w.nz;
+    const long V = w.V, cells = w.cells;
     const double vol = 1.0 / (vs[0] * vs[1] * vs[2]);
     TopologyResult res{};
-
-    DBuf<double> aos(V * 3), pos(V * 3), grad(V * 9), jc(cells * 8), div(V * 3), t1(V * 3),
-        t2(V * 3);
-    DBuf<int> list(cells), sorted(cells);
-    DBuf<Red> red(1);
-    DBuf<unsigned> flags(1);
-    BINDER_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(unsigned), s));
-    BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
-    aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, vs[0], vs[1], vs[2], pos.p);
-
-    // Hartley matrices and cosine tables for the periodic Poisson solve
-    const int dims[3] = {nx, ny, nz};
-    std::vector<DBuf<double> *> mats, coss;
-    for (int a = 0; a < 3; ++a) {
-        const int n = dims[a];
-        std::vector<double> H((size_t)n * n), cs(n);
-        hartley_matrix(n, H.data());
-        const double pi = 3.14159265358979323846;
-        for (int k = 0; k < n; ++k) cs[k] = std::cos(2.0 * pi * k / (n * 1.0));
-        mats.push_back(new DBuf<double>((size_t)n * n));
-        coss.push_back(new DBuf<double>(n));
-        BINDER_CUDA(cudaMemcpyAsync(mats.back()->p, H.data(), sizeof(double) * n * n,
-                                    cudaMemcpyHostToDevice, s));
-        BINDER_CUDA(cudaMemcpyAsync(coss.back()->p, cs.data(), sizeof(double) * n,
-                                    cudaMemcpyHostToDevice, s));
-    }
-    struct Cleanup {
-        std::vector<DBuf<double> *> &a, &b;
-        ~Cleanup() {
-            for (auto *p : a) delete p;
-            for (auto *p : b) delete p;
-        }
-    } cleanup{mats, coss};
+    BINDER_CUDA(cudaMemsetAsync(w.flags.p, 0, sizeof(unsigned), s));
 
     auto jac_stats = [&]() {
-        reset_red(red.p, s);
-        jacobian_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, 1, V, nx, ny, nz, vol, nullptr, e1, e2,
-                                                    red.p);
+        reset_red(w.red.p, s);
+        count_launch(), jacobian_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, 1, V, nx, ny, nz, vol, nullptr, e1, e2,
+                                                    w.red.p);
         BINDER_CUDA(cudaGetLastError());
-        return read_red(red.p, s);
+        return read_red(w.red.p, s);
     };
     auto corners = [&]() {
-        reset_red(red.p, s);
-        corner_kernel<<<grid_for(cells), 256, 0, s>>>(pos.p, nx, ny, nz, vol, e1, e2, jc.p, red.p);
+        reset_red(w.red.p, s);
+        count_launch(), corner_kernel<<<grid_for(cells), 256, 0, s>>>(w.pos.p, nx, ny, nz, vol, e1, e2, w.jc.p,
+                                                      w.red.p);
         BINDER_CUDA(cudaGetLastError());
-        return read_red(red.p, s);
+        return read_red(w.red.p, s);
     };
 
     Red r = jac_stats();
@@ -448,44 +472,41 @@ TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_o
         Red c = corners();
         int inner = 0;
         while ((c.below > 0 || c.above > 0) && inner < max_inner) {
-            gradient_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, nx, ny, nz, vs[0], vs[1], vs[2],
-                                                        grad.p);
-            reset_red(red.p, s);
-            flag_cells_kernel<<<grid_for(cells), 256, 0, s>>>(jc.p, nx, ny, nz, e1, e2, list.p,
-                                                              red.p);
-            limiter_kernel<<<1, 1024, lim_smem, s>>>(list.p, sorted.p, jc.p, grad.p, nx, ny, nz,
-                                                     e1, e2, nlev, red.p, flags.p);
+            count_launch(), gradient_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, nx, ny, nz, vs[0], vs[1], vs[2],
+                                                        w.grad.p);
+            reset_red(w.red.p, s);
+            count_launch(), flag_cells_kernel<<<grid_for(cells), 256, 0, s>>>(w.jc.p, nx, ny, nz, e1, e2, w.list.p,
+                                                              w.red.p);
+            count_launch(), limiter_kernel<<<1, 1024, lim_smem, s>>>(w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny,
+                                                     nz, e1, e2, nlev, w.red.p, w.flags.p);
             BINDER_CUDA(cudaGetLastError());
-            sum_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, V, red.p);
-            divergence_kernel<<<grid_for(V), 256, 0, s>>>(grad.p, nx, ny, nz, div.p);
+            count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, w.red.p);
+            count_launch(), divergence_kernel<<<grid_for(V), 256, 0, s>>>(w.grad.p, nx, ny, nz, w.div.p);
             BINDER_CUDA(cudaGetLastError());
-            Red sr = read_red(red.p, s);
+            Red sr = read_red(w.red.p, s);
             double mean[3];
             for (int n = 0; n < 3; ++n) mean[n] = sr.sum[n] / (nx * ny * nz);
 
-            // u = -(1/V) H (H div / lambda), separable Hartley passes z, y, [x fused], y, z
+            // u = -(1/V) H (H div / lambda): separable Hartley passes z, y, [x fused], y, z
             AxisArgs<double> a{};
             a.comp_stride = V;
             a.ny = ny;
             a.nz = nz;
-            a.cos_x = coss[0]->p;
-            a.cos_y = coss[1]->p;
-            a.cos_z = coss[2]->p;
-            // z forward
-            a.in = div.p; a.out = t1.p; a.M = mats[2]->p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+            a.cos_x = w.cs[0].p;
+            a.cos_y = w.cs[1].p;
+            a.cos_z = w.cs[2].p;
+            a.in = w.div.p; a.out = w.t1.p; a.M = w.H[2].p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
             launch_axis_pass(a, kEpiNone, 3, s);
-            // y forward
-            a.in = t1.p; a.out = t2.p; a.M = mats[1]->p; a.n = ny; a.outer = nx; a.s = nz;
+            a.in = w.t1.p; a.out = w.t2.p; a.M = w.H[1].p; a.n = ny; a.outer = nx; a.s = nz;
             launch_axis_pass(a, kEpiNone, 3, s);
-            // x forward, -1/(lambda V), x inverse
-            a.in = t2.p; a.out = t1.p; a.M = mats[0]->p; a.M2 = mats[0]->p; a.n = nx; a.outer = 1;
+            a.in = w.t2.p; a.out = w.t1.p; a.M = w.H[0].p; a.M2 = w.H[0].p; a.n = nx; a.outer = 1;
             a.s = (long)ny * nz;
             launch_axis_pass(a, kEpiPoisson, 3, s);
-            // y inverse
-            a.in = t1.p; a.out = t2.p; a.M = mats[1]->p; a.n = ny; a.outer = nx; a.s = nz;
+            a.in = w.t1.p; a.out = w.t2.p; a.M = w.H[1].p; a.M2 = nullptr; a.n = ny; a.outer = nx;
+            a.s = nz;
             launch_axis_pass(a, kEpiNone, 3, s);
-            // z inverse -> physical positions u * vs + mean
-            a.in = t2.p; a.out = pos.p; a.M = mats[2]->p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+            // last pass: physical positions u * vs + mean
+            a.in = w.t2.p; a.out = w.pos.p; a.M = w.H[2].p; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
             for (int n = 0; n < 3; ++n) {
                 a.out_scale[n] = vs[n];
                 a.out_offset[n] = mean[n];
@@ -504,10 +525,37 @@ TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_o
     r = jac_stats();
     res.below_after = (long long)r.below;
     res.above_after = (long long)r.above;
-    soa_to_aos_kernel<<<grid_for(V), 256, 0, s>>>(pos.p, V, vs[0], vs[1], vs[2], aos.p);
+    BINDER_CUDA(cudaMemcpyAsync(&res.flags, w.flags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    return res;
+}
+
+void TopologyWorkspace::load_float_grid(const float *d_soa, const double vs[3], cudaStream_t s) {
+    count_launch(), float_soa_to_physical_kernel<<<grid_for(impl_->V), 256, 0, s>>>(d_soa, impl_->V, vs[0], vs[1],
+                                                                    vs[2], impl_->pos.p);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void TopologyWorkspace::store_float_grid(float *d_soa, const double vs[3], cudaStream_t s) {
+    count_launch(), physical_to_float_soa_kernel<<<grid_for(impl_->V), 256, 0, s>>>(impl_->pos.p, impl_->V, vs[0],
+                                                                    vs[1], vs[2], d_soa);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_outer,
+                                   int max_inner, const double vs[3], int nx, int ny, int nz,
+                                   cudaStream_t s) {
+    BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
+    TopologyWorkspace ws(nx, ny, nz);
+    const long V = (long)nx * ny * nz;
+    DBuf<double> aos(V * 3);
+    BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
+    count_launch(), aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, vs[0], vs[1], vs[2], ws.positions());
+    BINDER_CUDA(cudaGetLastError());
+    TopologyResult res = ws.run(e1, e2, max_outer, max_inner, vs, s);
+    count_launch(), soa_to_aos_kernel<<<grid_for(V), 256, 0, s>>>(ws.positions(), V, vs[0], vs[1], vs[2], aos.p);
     BINDER_CUDA(cudaGetLastError());
     BINDER_CUDA(cudaMemcpyAsync(host, aos.p, sizeof(double) * V * 3, cudaMemcpyDeviceToHost, s));
-    BINDER_CUDA(cudaMemcpyAsync(&res.flags, flags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     BINDER_CUDA(cudaStreamSynchronize(s));
     return res;
 }

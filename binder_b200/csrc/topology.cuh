@@ -26,4 +26,24 @@ TopologyResult topology_correct_3d(double *field_aos_host, double e1, double e2,
                                    int max_inner, const double vs[3], int nx, int ny, int nz,
                                    cudaStream_t s);
 
+// Device buffers of the correction for one grid (positions, gradients, corner Jacobians, Poisson
+// work space), reusable across calls.  Positions are SoA [3][V] in physical units.
+class TopologyWorkspace {
+  public:
+    TopologyWorkspace(int nx, int ny, int nz);
+    ~TopologyWorkspace();
+    TopologyWorkspace(const TopologyWorkspace &) = delete;
+    TopologyWorkspace &operator=(const TopologyWorkspace &) = delete;
+    double *positions();
+    // grid-unit FP32 SoA field <-> the workspace's FP64 physical positions
+    void load_float_grid(const float *d_soa, const double vs[3], cudaStream_t s);
+    void store_float_grid(float *d_soa, const double vs[3], cudaStream_t s);
+    TopologyResult run(double e1, double e2, int max_outer, int max_inner, const double vs[3],
+                       cudaStream_t s);
+
+  private:
+    struct Impl;
+    Impl *impl_;
+};
+
 }  // namespace binder

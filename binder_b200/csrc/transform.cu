@@ -253,7 +253,7 @@ void launch_r(const AxisArgs<T> &a, int ncomp, cudaStream_t stream) {
     const long gx = contig ? (a.outer + TC - 1) / TC : a.outer * ((a.s + TC - 1) / TC);
     BINDER_CHECK(gx < (1L << 31), "transform grid too large");
     dim3 grid((unsigned)gx, 1, (unsigned)ncomp);
-    axis_kernel<T, R, MODE><<<grid, kThreads, smem, stream>>>(a);
+    count_launch(), axis_kernel<T, R, MODE><<<grid, kThreads, smem, stream>>>(a);
     BINDER_CUDA(cudaGetLastError());
 }
 

@@ -115,6 +115,32 @@ int binder_registration_set_stream(binder_registration *h, void *cuda_stream);
 /* Philox chain index, so independent chains with one seed draw disjoint streams */
 int binder_registration_set_chain(binder_registration *h, uint32_t chain);
 
+/* No counterpart in the reference: restore the positions given at creation, the theta given to
+ * set_mi_likelihood and a fresh iteration state, device to device (re-runs without host I/O). */
+int binder_registration_reset(binder_registration *h);
+
+/* Topology correction of the object's own current positions, on the device, in place.  Same
+ * algorithm and arguments as binder_topology_correct_3d below; it replaces the round trip
+ * get_final_locations -> topology_correction_3D().correct_topology -> next Registration that
+ * BINDER/FastRegistration.py:515,527-546 performs.  stats_out as for binder_topology_correct_3d. */
+int binder_registration_correct_topology(binder_registration *h, double e1, double e2,
+                                         int max_outer_it, int max_it,
+                                         const double voxel_sizes[3], long long *stats_out);
+
+/* No counterpart in the reference: the cudaStream_t the object's work runs on (for events). */
+int binder_registration_get_stream(const binder_registration *h, void **stream_out);
+
+/* No counterpart in the reference: average device time in ms of one launch of a pipeline stage,
+ * timed with CUDA events over `n` back-to-back eager launches on the object's stream.
+ * stage 0 = EM E-step kernel, 1 = DCT-prior M-step (all passes), 2 = theta update.  The object's
+ * positions, dream locations and histogram are left unspecified: call binder_registration_reset
+ * before further use. */
+int binder_registration_profile_stage(binder_registration *h, int stage, int n, double *avg_ms_out);
+
+/* No counterpart in the reference: number of kernels this library has launched in this process
+ * (each replay of a captured CUDA graph counts all of its kernels). */
+long long binder_kernel_launch_count(void);
+
 /* ---- _core.NonLinearTransformation --------------------------------------------------------- */
 
 /* NonLinearTransformation(gamma_x..z, voxels_size_x..z, nodes_size_x..z, D, Nx_v, Ny_v, Nz_v,

@@ -14,7 +14,8 @@ HEADER = os.path.join(ROOT, "include", "binder_b200.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(binder_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char \*)\s*(binder_\w+)\s*\(",
+                                 text, re.M)))
 
 
 def test_header_lists_all_python_bindings():

@@ -52,13 +52,14 @@ def test_one_em_iteration_matches_oracle(core, oracle):
     mll, dream, hist, deg = oracle.estep(d0, c["u"], c["v"], c["theta"].astype(np.float64), shape,
                                          shape, K, L)
     theta = oracle.theta_map(hist, K, L, 2.0)
-    lpl = oracle.dirichlet_cost(theta.astype(np.float32), K, L, 2.0)
     lpt, final = oracle.smooth(dream, c["grid"], c["D"], c["gamma"], SIGMA_CUBIC, shape)
     assert deg == 0
     np.testing.assert_allclose(dream_g, dream, rtol=0, atol=5e-5)       # FP32 E-step
     np.testing.assert_allclose(theta_g, theta, rtol=1e-4, atol=1e-7)    # FP32 histogram
     assert st[0] == pytest.approx(mll, rel=1e-6)                        # FP64 log-sum of FP32 S
-    assert st[1] == pytest.approx(lpl, rel=1e-9)                        # FP64 Dirichlet cost
+    # FP64 Dirichlet cost of the GPU's own FP32 theta; vs the oracle's theta within FP32 round-off
+    assert st[1] == pytest.approx(oracle.dirichlet_cost(theta_g, K, L, 2.0), rel=1e-12)
+    assert st[1] == pytest.approx(oracle.dirichlet_cost(theta, K, L, 2.0), rel=1e-6)
     assert st[2] == pytest.approx(lpt, rel=2e-4)                        # FP32 DCT prior cost
     np.testing.assert_allclose(final_g, final, rtol=0, atol=2e-4)      # FP32 DCT M-step
 
