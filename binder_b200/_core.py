@@ -162,6 +162,10 @@ class Registration:
     def set_chain(self, chain):
         check(lib().binder_registration_set_chain(self._h, int(chain)))
 
+    def set_precision(self, precision):
+        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32."""
+        check(lib().binder_registration_set_precision(self._h, int(precision)))
+
     def stream(self):
         """The object's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
         p = C.c_void_p()
@@ -215,6 +219,10 @@ class NonLinearTransformation:
         out = np.zeros(4, np.int32)
         check(lib().binder_transform_get_shape(self._h, out))
         return [int(v) for v in out]
+
+    def set_precision(self, precision):
+        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32."""
+        check(lib().binder_transform_set_precision(self._h, int(precision)))
 
     def smooth_deformation(self, deformation):
         out = np.zeros(self._V * 3, np.float32)

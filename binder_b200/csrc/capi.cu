@@ -233,6 +233,20 @@ int binder_registration_correct_topology(binder_registration *h, double e1, doub
     });
 }
 
+int binder_registration_set_precision(binder_registration *h, int precision) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_precision(precision);
+    });
+}
+
+int binder_transform_set_precision(binder_transform *h, int precision) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_precision(precision);
+    });
+}
+
 int binder_registration_get_stream(const binder_registration *h, void **stream_out) {
     return guard([&] {
         NEED(h);

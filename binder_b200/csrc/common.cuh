@@ -45,6 +45,7 @@ enum DeviceFlag : unsigned {
     kFlagGammaCapped = 1u << 0,    // a Marsaglia-Tsang sampler reached its attempt cap
     kFlagLimiterCapped = 1u << 1,  // a gradient-limiter blend loop reached its step cap
     kFlagNonFinite = 1u << 2,      // a reduction produced a non-finite value
+    kFlagTensorTimeout = 1u << 3,  // a tensor-core pass gave up waiting on its MMA barrier
 };
 
 // ------------------------------------------------------------------------------------------

@@ -103,6 +103,11 @@ void DctSet::init(int nx, int ny, int nz) {
             }
         fwd[a] = dalloc<float>((size_t)m * m);
         inv[a] = dalloc<float>((size_t)m * m);
+        std::vector<double> CT((size_t)m * m);
+        for (int k = 0; k < m; ++k)
+            for (int j = 0; j < m; ++j) CT[(size_t)j * m + k] = C[(size_t)k * m + j];
+        ufwd[a].init(C.data(), m);
+        uinv[a].init(CT.data(), m);
         BINDER_CUDA(cudaMemcpy(fwd[a], F.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
         BINDER_CUDA(cudaMemcpy(inv[a], I.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
     }
@@ -112,6 +117,8 @@ void DctSet::release() {
     for (int a = 0; a < 3; ++a) {
         dfree(fwd[a]);
         dfree(inv[a]);
+        ufwd[a].release();
+        uinv[a].release();
     }
 }
 
@@ -121,6 +128,13 @@ void MStep::init(int x, int y, int z) {
     dct.init(x, y, z);
     t1 = dalloc<float>((size_t)V * 3);
     t2 = dalloc<float>((size_t)V * 3);
+    precision = default_precision();
+}
+
+int default_precision() {
+    const char *e = std::getenv("BINDER_B200_PRECISION");
+    if (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == 0) return e[0] - '0';
+    return kPrecTF32x3;
 }
 
 void MStep::release() {
@@ -139,24 +153,34 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     a.skip = skip;
     a.ny = ny;
     a.nz = nz;
-    // forward DCT-II along z, y
-    a.in = r; a.out = t1; a.M = dct.fwd[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
-    launch_axis_pass(a, kEpiNone, 3, s);
-    a.in = t1; a.out = t2; a.M = dct.fwd[1]; a.n = ny; a.outer = nx; a.s = nz;
-    launch_axis_pass(a, kEpiNone, 3, s);
-    // x: forward, prior scaling (+ noise, costs), inverse
-    a.in = t2; a.out = t1; a.M = dct.fwd[0]; a.M2 = dct.inv[0]; a.n = nx; a.outer = 1;
-    a.s = (long)ny * nz;
     a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
     a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
-    launch_axis_pass(a, kEpiSpectral, 3, s);
+    const bool tc = precision != kPrecFP32Simt;
+    const int planes = precision == kPrecTF32 ? 1 : 2;
+    auto pass = [&](int axis, bool inverse, int mode) {
+        if (tc)
+            launch_axis_pass_tc(a, inverse ? dct.uinv[axis] : dct.ufwd[axis],
+                                mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, 3, planes,
+                                s);
+        else
+            launch_axis_pass(a, mode, 3, s);
+    };
+    // forward DCT-II along z, y
+    a.in = r; a.out = t1; a.M = dct.fwd[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+    pass(2, false, kEpiNone);
+    a.in = t1; a.out = t2; a.M = dct.fwd[1]; a.n = ny; a.outer = nx; a.s = nz;
+    pass(1, false, kEpiNone);
+    // x: forward, prior scaling (+ noise, costs), inverse
+    a.in = t2; a.out = t1; a.M = dct.fwd[0]; a.M2 = dct.inv[0]; a.n = nx; a.outer = 1;
+    a.s = (long)ny * nz;
+    pass(0, false, kEpiSpectral);
     // inverse DCT-III along y, z; the last pass adds the voxel positions
     a.in = t1; a.out = t2; a.M = dct.inv[1]; a.M2 = nullptr; a.n = ny; a.outer = nx; a.s = nz;
-    launch_axis_pass(a, kEpiNone, 3, s);
+    pass(1, true, kEpiNone);
     a.in = t2; a.out = d; a.M = dct.inv[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
     a.xpos = xpos;
-    launch_axis_pass(a, kEpiPositions, 3, s);
+    pass(2, true, kEpiPositions);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -481,6 +505,16 @@ double Registration::profile_stage(int stage, int n) {
     BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
     return ms / n;
+}
+
+void Registration::set_precision(int p) {
+    BINDER_CHECK(p >= 0 && p <= 2, "precision must be 0 (FP32), 1 (3xTF32) or 2 (TF32)");
+    mstep_.precision = p;
+}
+
+void PriorTransform::set_precision(int p) {
+    BINDER_CHECK(p >= 0 && p <= 2, "precision must be 0 (FP32), 1 (3xTF32) or 2 (TF32)");
+    mstep_.precision = p;
 }
 
 void Registration::reset() {

@@ -5,6 +5,7 @@
 
 #include "estep.cuh"
 #include "topology.cuh"
+#include "umma_transform.cuh"
 
 namespace binder {
 
@@ -13,6 +14,7 @@ struct DctSet {
     int n[3] = {0, 0, 0};
     float *fwd[3] = {nullptr, nullptr, nullptr};
     float *inv[3] = {nullptr, nullptr, nullptr};
+    UmmaMatrix ufwd[3], uinv[3];  // the same matrices preformatted for the tensor cores
     void init(int nx, int ny, int nz);
     void release();
 };
@@ -24,6 +26,7 @@ struct MStep {
     long V = 0;
     DctSet dct;
     float *t1 = nullptr, *t2 = nullptr;
+    int precision = kPrecFP32Simt;  // TransformPrecision
     void init(int nx, int ny, int nz);
     void release();
     void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
@@ -64,6 +67,7 @@ class Registration {
                    unsigned *flags) const;
     void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
     void set_chain(uint32_t c) { chain_ = c; }
+    void set_precision(int p);
     double last_elapsed_ms() const { return last_ms_; }
     cudaStream_t stream() const { return stream_; }
     // average ms per launch of stage 0 (E-step), 1 (M-step) or 2 (theta update), n eager launches
@@ -115,6 +119,7 @@ class PriorTransform {
     void sample(const float *field_aos, int n, float *out_aos);
     void get_shape(int out[4]) const;
     void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
+    void set_precision(int p);
 
   private:
     int nx_, ny_, nz_;
@@ -127,6 +132,9 @@ class PriorTransform {
     uint64_t seed_ = 1234;
     int sweep_ = 0;
 };
+
+// default transform precision: BINDER_B200_PRECISION (0 FP32 SIMT, 1 3xTF32, 2 TF32) or 3xTF32
+int default_precision();
 
 // helpers shared with the C-ABI
 void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa);

@@ -68,10 +68,116 @@ __device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int com
     return comp == 0 ? (float)(i / yz) : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
 }
 
+constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
+
+// EM E-step for K <= 64 (BINDER/src/cpu/Registration.cpp:219-330, sample == false), one pass over
+// the 64 neighbours.  The posterior mass of a voxel is collected per moving bin k in a private
+// shared-memory column hk[k][thread] (bank = thread % 32, so never a conflict and never an
+// atomic), with a 64-bit mask of the bins touched; once the normaliser S is known the touched bins
+// are flushed as hist[k][u] += hk[k] / S -- one shared atomic per distinct bin instead of one per
+// neighbour.  theta is staged transposed (thT[u][k]) so lanes that share a fixed-image bin read
+// consecutive banks.
+__global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStepArgs a) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) float sm[];
+    const int K = a.K, L = a.L, KL = K * L;
+    float *thT = sm;            // [L][K]
+    float *hs = sm + KL;        // [K][L] CTA histogram
+    float *hk = sm + 2 * KL;    // [K][kEThreads] per-thread bin masses
+    __shared__ double red[32];
+    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+        const int k = q / L, l = q - k * L;
+        thT[l * K + k] = a.theta[q];
+        hs[q] = 0.0f;
+    }
+    for (int q = threadIdx.x; q < K * kEThreads; q += blockDim.x) hk[q] = 0.0f;
+    __syncthreads();
+
+    float *my = hk + threadIdx.x;  // my[k * kEThreads]
+    double mll = 0.0;
+    unsigned long long deg = 0;
+    const float *d0 = a.d, *d1 = a.d + a.V, *d2 = a.d + 2 * a.V;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.V;
+         i += (long)gridDim.x * blockDim.x) {
+        const float px = d0[i], py = d1[i], pz = d2[i];
+        const float x0 = voxel_coord(a, i, 0), x1 = voxel_coord(a, i, 1), x2 = voxel_coord(a, i, 2);
+        if (!(fabsf(px) < 1.0e6f && fabsf(py) < 1.0e6f && fabsf(pz) < 1.0e6f)) {
+            a.r[i] = px - x0; a.r[a.V + i] = py - x1; a.r[2 * a.V + i] = pz - x2;
+            ++deg;
+            continue;
+        }
+        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+        float bx[4], by[4], bz[4];
+        bspline3(px - fx, bx);
+        bspline3(py - fy, by);
+        bspline3(pz - fz, bz);
+        uint32_t pk[16];
+        gather_bins(a, ix, iy, iz, pk);
+        const int ui = a.u[i];
+        const float *thu = thT + ui * K;
+        float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
+        unsigned long long mask = 0ull;
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float bxy = bx[p] * by[q];
+                const uint32_t word = pk[p * 4 + q];
+                float r0 = 0.0f, rz = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int k = (word >> (8 * c)) & 0xff;
+                    const float w = (bxy * bz[c]) * thu[k];
+                    r0 += w;
+                    rz = fmaf((float)(c - 1), w, rz);
+                    my[k * kEThreads] += w;
+                    mask |= 1ull << k;
+                }
+                S += r0;
+                Sx = fmaf((float)(p - 1), r0, Sx);
+                Sy = fmaf((float)(q - 1), r0, Sy);
+                Sz += rz;
+            }
+        if (!(S > 0.0f)) {
+            while (mask) {
+                const int k = __ffsll((long long)mask) - 1;
+                mask &= mask - 1;
+                my[k * kEThreads] = 0.0f;
+            }
+            a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
+            ++deg;
+            continue;
+        }
+        const float inv = 1.0f / S;
+        mll -= log((double)S);
+        a.r[i] = (fx + Sx * inv) - x0;
+        a.r[a.V + i] = (fy + Sy * inv) - x1;
+        a.r[2 * a.V + i] = (fz + Sz * inv) - x2;
+        float *hcol = hs + ui;  // hcol[k * L]
+        while (mask) {
+            const int k = __ffsll((long long)mask) - 1;
+            mask &= mask - 1;
+            atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
+            my[k * kEThreads] = 0.0f;
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+        const float v = hs[q];
+        if (v != 0.0f) atomicAdd(&a.hist[q], v);
+    }
+    const double m = block_sum(mll, red);
+    if (threadIdx.x == 0) atomicAdd(&a.st->mll, m);
+    const double dg = block_sum((double)deg, red);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+}
+
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
-// histogram kept in shared memory and neighbouring equal bins combined before the atomics.
+// histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
+// for the Gibbs draw and for EM with K > 64.
 template <bool SAMPLE>
-__global__ void __launch_bounds__(kEThreads) estep_kernel(const EStepArgs a) {
+__global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int KL = a.K * a.L;
@@ -380,22 +486,23 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 
 }  // namespace
 
+namespace {
+size_t estep_smem(bool sample, int K, int L) {
+    if (!sample && K <= kSmallK) return (size_t)(2 * K * L + K * kEThreads) * sizeof(float);
+    return (size_t)2 * K * L * sizeof(float);
+}
+}  // namespace
+
 int estep_grid(bool sample, int K, int L, long V) {
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = (size_t)2 * K * L * sizeof(float);
-    if (sample) {
-        BINDER_CUDA(cudaFuncSetAttribute(estep_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estep_kernel<true>,
-                                                                  kEThreads, smem));
-    } else {
-        BINDER_CUDA(cudaFuncSetAttribute(estep_kernel<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, estep_kernel<false>,
-                                                                  kEThreads, smem));
-    }
+    const size_t smem = estep_smem(sample, K, L);
+    const void *fn = sample ? (const void *)estep_kernel<true>
+                            : (K <= kSmallK ? (const void *)estep_em_fast_kernel
+                                            : (const void *)estep_kernel<false>);
+    BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kEThreads, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const long need = (V + kEThreads - 1) / kEThreads;
     long g = (long)sms * per_sm;
@@ -404,9 +511,11 @@ int estep_grid(bool sample, int K, int L, long V) {
 }
 
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s) {
-    const size_t smem = (size_t)2 * a.K * a.L * sizeof(float);
+    const size_t smem = estep_smem(sample, a.K, a.L);
     if (sample)
         count_launch(), estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
+    else if (a.K <= kSmallK)
+        count_launch(), estep_em_fast_kernel<<<grid, kEThreads, smem, s>>>(a);
     else
         count_launch(), estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
     BINDER_CUDA(cudaGetLastError());

@@ -1,0 +1,401 @@
+// Tensor-core (tcgen05 / TMEM) version of the separable transform passes of transform.cu.
+//
+// One CTA (4 warps) owns a tile of 128 lines of one component.  The pass is the GEMM
+//   D[line][k] = sum_j X[line][j] * M[k][j]      (M = the n x n transform, rows = outputs)
+// with A = the 128 x n data tile and B = M, both K-major in shared memory in the canonical
+// no-swizzle layout (8-row x 16-byte core matrices), streamed in K chunks of 32 through a
+// two-stage pipeline, accumulated in TMEM by tcgen05.mma (M = 128, N = n padded to 16).
+// Precision: TF32 operands (one plane), or "3xTF32" -- hi/lo TF32 planes and the three products
+// hi*hi + hi*lo + lo*hi, which keeps FP32-level accuracy -- always with FP32 accumulation.
+// The x-axis pass of the DCT prior is fused: forward GEMM into TMEM columns [0, Npad), the prior
+// scaling / noise / costs applied while TMEM chunks are re-staged as the A operand of the inverse
+// GEMM, which accumulates into TMEM columns [Npad, 2 Npad).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "transform.cuh"
+#include "umma.cuh"
+#include "umma_transform.cuh"
+
+namespace binder {
+
+namespace {
+
+constexpr int kLines = 128;           // UMMA M
+constexpr int kKC = 32;               // K elements per pipeline chunk
+constexpr int kAPlane = kLines * kKC;  // floats per A plane per stage
+constexpr uint64_t kWaitLimit = 2000000000ull;  // 2 s of wall time per barrier wait
+
+struct UArgs {
+    const float *in;
+    float *out;
+    long V;
+    int n, Npad, nkc;
+    long outer, s;
+    const float *B1, *B2;  // preformatted [nkc][2 planes][Npad * 32]
+    // spectral epilogue
+    const float *D;
+    DevState *st;
+    double sigma2;
+    int sample, want_raw, every;
+    uint64_t seed;
+    uint32_t chain;
+    double rho_p;
+    double eta2[3];
+    // positions epilogue
+    const float *xpos;
+    int ny, nz;
+    const int *skip;
+};
+
+__device__ __forceinline__ float prior_normal_tc(uint64_t seed, uint32_t i, uint32_t sweep,
+                                                 uint32_t chain, int comp) {
+    const u32x4 r = philox_draw(seed, i, sweep, comp < 2 ? 2u : 3u, chain);
+    const float u1 = u01_f24(r.x), u2 = u01_f24(r.y);
+    const float rad = sqrtf(-2.0f * logf(u1));
+    float sn, cs;
+    sincospif(2.0f * u2, &sn, &cs);
+    return comp == 1 ? rad * sn : rad * cs;
+}
+
+// one 16-byte slot of the K-major A plane: rows `line`, K elements 4q .. 4q+3 of the chunk
+__device__ __forceinline__ int a_slot(int line, int q) {
+    return q * 512 + (line >> 3) * 32 + (line & 7) * 4;
+}
+
+template <int PLANES>
+__device__ __forceinline__ void store_split(float *plane0, int off, float4 v) {
+    float4 hi = make_float4(umma::to_tf32(v.x), umma::to_tf32(v.y), umma::to_tf32(v.z),
+                            umma::to_tf32(v.w));
+    *reinterpret_cast<float4 *>(plane0 + off) = hi;
+    if (PLANES == 2) {
+        float4 lo = make_float4(umma::to_tf32(v.x - hi.x), umma::to_tf32(v.y - hi.y),
+                                umma::to_tf32(v.z - hi.z), umma::to_tf32(v.w - hi.w));
+        *reinterpret_cast<float4 *>(plane0 + kAPlane + off) = lo;
+    }
+}
+
+template <int MODE, int PLANES>
+__global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int Npad = a.Npad, n = a.n;
+    float *As = reinterpret_cast<float *>(smem_raw);              // [2 stages][PLANES][kAPlane]
+    float *Bs = As + 2 * PLANES * kAPlane;                        // [2 stages][PLANES][Npad*32]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * PLANES * Npad * kKC);  // [3]
+    uint32_t *holder = reinterpret_cast<uint32_t *>(mbar + 3);
+    int *s_err = reinterpret_cast<int *>(holder + 1);
+    __shared__ double red[32];
+
+    const bool fused = (MODE == kEpiSpectral);
+    const uint32_t want = fused ? 2u * Npad : (uint32_t)Npad;
+    uint32_t ncols = 32;
+    while (ncols < want) ncols <<= 1;
+
+    if (warp == 0) umma::tmem_alloc(holder, ncols);
+    if (tid == 0) {
+        umma::mbar_init(&mbar[0], 1);
+        umma::mbar_init(&mbar[1], 1);
+        umma::mbar_init(&mbar[2], 1);
+        *s_err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *holder;
+
+    const int comp = blockIdx.z;
+    const float *in = a.in + comp * a.V;
+    float *out = a.out + comp * a.V;
+    const long nlines = a.outer * a.s;
+    const long l0 = (long)blockIdx.x * kLines;
+    const bool contig = (a.s == 1);
+    // this thread's line (TMEM lane == tile row == tid)
+    const long lg = l0 + tid;
+    const bool valid = lg < nlines;
+    const long o = valid ? lg / a.s : 0, t = valid ? lg - o * a.s : 0;
+    const long lbase = o * (long)n * a.s + t;  // element (line, j) at lbase + j * s
+    const uint32_t idesc = umma::instr_desc(kLines, Npad, umma::kFmtTF32);
+    const uint32_t bplane = (uint32_t)Npad * kKC;  // floats per B plane
+
+    uint32_t chunk = 0;  // running chunk counter over both GEMMs: stage = chunk & 1
+    double part_cost = 0.0, part_raw = 0.0;
+    const uint32_t sweep = (MODE == kEpiSpectral && a.sample) ? (uint32_t)a.st->sweep : 0u;
+    const bool want_raw = (MODE == kEpiSpectral) && a.want_raw && (a.st->sweep % a.every == 0);
+    const double gamma = (MODE == kEpiSpectral) ? a.st->gamma[comp] : 0.0;
+    const float gs2 = (float)(gamma * a.sigma2);
+
+    // ---- one GEMM: accumulate into TMEM columns [col_off, col_off + Npad) ----------------------
+    auto gemm = [&](const float *Bg, uint32_t col_off, int src) {
+        for (int kc = 0; kc < a.nkc; ++kc) {
+            const uint32_t c = chunk++;
+            const int stage = c & 1;
+            if (c >= 2 && !umma::mbar_wait(&mbar[stage], ((c >> 1) - 1) & 1, kWaitLimit))
+                atomicOr(s_err, 1);
+            __syncthreads();
+            if (*s_err) return;
+            float *Ap = As + stage * PLANES * kAPlane;
+            float *Bp = Bs + stage * PLANES * bplane;
+            // A operand
+            if (src == 0) {
+                if (contig) {
+                    // rows of n contiguous floats: 8 lines x 4 float4 per warp instruction
+                    const int lane = tid & 31, r = lane & 7, h = lane >> 3;
+                    for (int it = warp; it < 32; it += 4) {
+                        const int line = (it >> 1) * 8 + r, q = (it & 1) * 4 + h;
+                        const long g = l0 + line;
+                        const int j0 = kc * kKC + q * 4;
+                        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (g < nlines) {
+                            const float *p = in + g * n + j0;
+                            if ((n & 3) == 0 && j0 + 3 < n) {
+                                v = __ldg(reinterpret_cast<const float4 *>(p));
+                            } else {
+                                v.x = j0 < n ? __ldg(p) : 0.f;
+                                v.y = j0 + 1 < n ? __ldg(p + 1) : 0.f;
+                                v.z = j0 + 2 < n ? __ldg(p + 2) : 0.f;
+                                v.w = j0 + 3 < n ? __ldg(p + 3) : 0.f;
+                            }
+                        }
+                        store_split<PLANES>(Ap, a_slot(line, q), v);
+                    }
+                } else {
+                    // strided axis: lanes are consecutive lines -> coalesced along t
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int j0 = kc * kKC + q * 4;
+                        float4 v;
+                        v.x = (valid && j0 < n) ? __ldg(in + lbase + (long)j0 * a.s) : 0.f;
+                        v.y = (valid && j0 + 1 < n) ? __ldg(in + lbase + (long)(j0 + 1) * a.s) : 0.f;
+                        v.z = (valid && j0 + 2 < n) ? __ldg(in + lbase + (long)(j0 + 2) * a.s) : 0.f;
+                        v.w = (valid && j0 + 3 < n) ? __ldg(in + lbase + (long)(j0 + 3) * a.s) : 0.f;
+                        store_split<PLANES>(Ap, a_slot(tid, q), v);
+                    }
+                }
+            } else {
+                // fused x pass: forward coefficients of this chunk from TMEM, prior scaling,
+                // noise and costs, re-staged as the A operand of the inverse GEMM
+                float v[32];
+                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kc * kKC), v);
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = kc * kKC + m;
+                    float c = 0.0f;
+                    if (valid && k < n) {
+                        const long i = (long)k * a.s + t;
+                        const float Dv = __ldg(a.D + i);
+                        const float f = 1.0f / (1.0f + gs2 * Dv);
+                        c = v[m] * f;
+                        if (a.sample)
+                            c += sqrtf((float)a.sigma2 * f) *
+                                 prior_normal_tc(a.seed, (uint32_t)i, sweep, a.chain, comp);
+                        const double c2 = (double)c * (double)c;
+                        part_cost += 0.5 * gamma * (double)Dv * c2;
+                        if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)Dv * c2;
+                    }
+                    v[m] = c;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    store_split<PLANES>(Ap, a_slot(tid, q),
+                                        make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+            }
+            // B operand: the preformatted chunk, copied as-is
+            {
+                const float4 *srcb = reinterpret_cast<const float4 *>(Bg + (size_t)kc * 2 * bplane);
+                float4 *dstb = reinterpret_cast<float4 *>(Bp);
+                const int nv = PLANES * (int)bplane / 4;
+                for (int qv = tid; qv < nv; qv += 128) dstb[qv] = __ldg(srcb + qv);
+            }
+            umma::fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                umma::fence_after_sync();
+                const uint32_t abase = umma::smem_u32(Ap), bbase = umma::smem_u32(Bp);
+#pragma unroll
+                for (int ks = 0; ks < kKC / 8; ++ks) {
+                    const uint32_t ao = (uint32_t)ks * 2u * 2048u;
+                    const uint32_t bo = (uint32_t)ks * 2u * (uint32_t)Npad * 16u;
+                    const uint64_t ahi = umma::smem_desc(abase + ao, 2048u, 128u);
+                    const uint64_t bhi = umma::smem_desc(bbase + bo, (uint32_t)Npad * 16u, 128u);
+                    umma::mma_tf32(tmem + col_off, ahi, bhi, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+                    if (PLANES == 2) {
+                        const uint64_t alo = umma::smem_desc(abase + kAPlane * 4u + ao, 2048u, 128u);
+                        const uint64_t blo =
+                            umma::smem_desc(bbase + bplane * 4u + bo, (uint32_t)Npad * 16u, 128u);
+                        umma::mma_tf32(tmem + col_off, ahi, blo, idesc, 1u);
+                        umma::mma_tf32(tmem + col_off, alo, bhi, idesc, 1u);
+                    }
+                }
+                umma::commit(&mbar[stage]);
+            }
+        }
+        // wait for the whole accumulation
+        const uint32_t last = chunk - 1;
+        if (!umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitLimit)) atomicOr(s_err, 1);
+        __syncthreads();
+        umma::fence_after_sync();
+    };
+
+    gemm(a.B1, 0u, 0);
+    uint32_t acc_col = 0;
+    if (fused && !*s_err) {
+        gemm(a.B2, (uint32_t)Npad, 1);
+        acc_col = (uint32_t)Npad;
+    }
+
+    if (!*s_err) {
+        // ---- epilogue: 32 TMEM columns at a time -------------------------------------------
+        const int nchunks = (n + 31) / 32;
+        for (int cc = 0; cc < nchunks; ++cc) {
+            float v[32];
+            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + acc_col + (uint32_t)(cc * 32), v);
+            if (!valid) continue;
+            if (contig) {
+                float *dst = out + lg * n;
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = cc * 32 + m;
+                    if (k < n) {
+                        float val = v[m];
+                        if (MODE == kEpiPositions) {
+                            const long i = lg * n + k;
+                            float xv;
+                            if (a.xpos) {
+                                xv = __ldg(a.xpos + comp * a.V + i);
+                            } else {
+                                const long yz = (long)a.ny * a.nz;
+                                xv = comp == 0 ? (float)(i / yz)
+                                               : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
+                            }
+                            val += xv;
+                        }
+                        dst[k] = val;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = cc * 32 + m;
+                    if (k < n) out[lbase + (long)k * a.s] = v[m];
+                }
+            }
+        }
+    }
+
+    if (MODE == kEpiSpectral) {
+        const double sc = block_sum(part_cost, red);
+        if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
+        if (a.want_raw) {
+            const double sr = block_sum(part_raw, red);
+            if (tid == 0) atomicAdd(&a.st->raw_reg, sr);
+        }
+    }
+
+    // ---- teardown: after an error, drain every tcgen05 op still in flight (bounded) -------------
+    if (*s_err) {
+        if (tid == 0) {
+            umma::commit(&mbar[2]);
+            umma::mbar_wait(&mbar[2], 0, kWaitLimit);
+            if (a.st) atomicOr(&a.st->flags, (unsigned)kFlagTensorTimeout);
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
+float tf32_rna_host(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) {
+        u += 0x1000u;
+        u &= 0xFFFFE000u;
+    }
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+template <int MODE, int PLANES>
+void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
+    const size_t need = (size_t)(2 * PLANES * kAPlane + 2 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
+    const uint32_t want = MODE == kEpiSpectral ? 2u * a.Npad : (uint32_t)a.Npad;
+    uint32_t ncols = 32;
+    while (ncols < want) ncols <<= 1;
+    // a CTA that takes all 512 TMEM columns must be alone on its SM
+    const size_t smem = (ncols == 512 && need < 120 * 1024) ? 120 * 1024 : need;
+    BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
+    BINDER_CUDA(cudaFuncSetAttribute(umma_axis_kernel<MODE, PLANES>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long tiles = (a.outer * a.s + kLines - 1) / kLines;
+    BINDER_CHECK(tiles < (1L << 31), "transform grid too large");
+    dim3 grid((unsigned)tiles, 1, (unsigned)ncomp);
+    count_launch(), umma_axis_kernel<MODE, PLANES><<<grid, 128, smem, s>>>(a);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+void UmmaMatrix::init(const double *M, int n_) {
+    n = n_;
+    Npad = ((n + 15) / 16) * 16;
+    nkc = (n + kKC - 1) / kKC;
+    const size_t plane = (size_t)Npad * kKC;
+    std::vector<float> host((size_t)nkc * 2 * plane, 0.0f);
+    for (int kc = 0; kc < nkc; ++kc)
+        for (int k = 0; k < n; ++k)
+            for (int jj = 0; jj < kKC; ++jj) {
+                const int j = kc * kKC + jj;
+                if (j >= n) continue;
+                const float v = (float)M[(size_t)k * n + j];
+                const float hi = tf32_rna_host(v);
+                const float lo = tf32_rna_host(v - hi);
+                const size_t off = (size_t)(jj / 4) * (Npad * 4) + (k / 8) * 32 + (k % 8) * 4 + (jj % 4);
+                host[(size_t)kc * 2 * plane + off] = hi;
+                host[(size_t)kc * 2 * plane + plane + off] = lo;
+            }
+    BINDER_CUDA(cudaMalloc(&dev, host.size() * sizeof(float)));
+    BINDER_CUDA(cudaMemcpy(dev, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+}
+
+void UmmaMatrix::release() {
+    if (dev) cudaFree(dev);
+    dev = nullptr;
+}
+
+void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const UmmaMatrix *M2,
+                         int mode, int ncomp, int planes, cudaStream_t s) {
+    BINDER_CHECK(b.n == M1.n, "matrix / axis length mismatch");
+    BINDER_CHECK(planes == 1 || planes == 2, "planes must be 1 (TF32) or 2 (3xTF32)");
+    UArgs a{};
+    a.in = b.in; a.out = b.out; a.V = b.comp_stride; a.n = b.n; a.Npad = M1.Npad; a.nkc = M1.nkc;
+    a.outer = b.outer; a.s = b.s; a.B1 = M1.dev; a.B2 = M2 ? M2->dev : nullptr;
+    a.D = b.D; a.st = b.st; a.sigma2 = b.sigma2; a.sample = b.sample; a.want_raw = b.want_raw;
+    a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
+    for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
+    a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.skip = b.skip;
+#define BINDER_UMMA_CASE(MODE)                                                    \
+    case MODE:                                                                    \
+        if (planes == 2) launch_umma<MODE, 2>(a, ncomp, s);                       \
+        else launch_umma<MODE, 1>(a, ncomp, s);                                   \
+        break;
+    switch (mode) {
+        BINDER_UMMA_CASE(kEpiNone)
+        BINDER_UMMA_CASE(kEpiPositions)
+        case kEpiSpectral:
+            BINDER_CHECK(M2 && M2->n == b.n, "fused pass needs the inverse matrix");
+            BINDER_CHECK(b.outer == 1, "fused prior pass runs on the outermost axis");
+            if (planes == 2) launch_umma<kEpiSpectral, 2>(a, ncomp, s);
+            else launch_umma<kEpiSpectral, 1>(a, ncomp, s);
+            break;
+        default: BINDER_CHECK(false, "unsupported epilogue on the tensor-core path");
+    }
+#undef BINDER_UMMA_CASE
+}
+
+}  // namespace binder

@@ -1,0 +1,28 @@
+// Tensor-core (tcgen05) separable transform passes -- see umma_transform.cu.
+#pragma once
+
+#include "transform.cuh"
+
+namespace binder {
+
+// An n x n transform matrix preformatted for the UMMA B operand: K chunks of 32, each a hi and a
+// lo TF32 plane in the canonical no-swizzle K-major layout, rows padded to a multiple of 16.
+struct UmmaMatrix {
+    int n = 0, Npad = 0, nkc = 0;
+    float *dev = nullptr;
+    void init(const double *M, int n);
+    void release();
+};
+
+// precision of the DCT passes
+enum TransformPrecision : int {
+    kPrecFP32Simt = 0,   // FP32 FMA (CUDA cores)
+    kPrecTF32x3 = 1,     // tensor cores, 3xTF32 split: FP32-level accuracy
+    kPrecTF32 = 2,       // tensor cores, one TF32 product
+};
+
+// One pass on the tensor cores: modes kEpiNone, kEpiPositions, kEpiSpectral (M2 = inverse).
+void launch_axis_pass_tc(const AxisArgs<float> &a, const UmmaMatrix &M1, const UmmaMatrix *M2,
+                         int mode, int ncomp, int planes, cudaStream_t s);
+
+}  // namespace binder

@@ -127,6 +127,17 @@ int binder_registration_correct_topology(binder_registration *h, double e1, doub
                                          int max_outer_it, int max_it,
                                          const double voxel_sizes[3], long long *stats_out);
 
+/* No counterpart in the reference (its GPU backend is FP32 cuFFT only): arithmetic of the DCT
+ * passes.  BINDER_PRECISION_FP32 = FP32 FMA on the CUDA cores; _TF32X3 = tensor cores (tcgen05)
+ * with hi/lo TF32 operand splitting, FP32-level accuracy; _TF32 = one TF32 tensor-core product
+ * (about 1e-3 relative error per pass).  All accumulate in FP32.  The default comes from the
+ * BINDER_B200_PRECISION environment variable (0, 1 or 2), else TF32X3. */
+#define BINDER_PRECISION_FP32 0
+#define BINDER_PRECISION_TF32X3 1
+#define BINDER_PRECISION_TF32 2
+int binder_registration_set_precision(binder_registration *h, int precision);
+int binder_transform_set_precision(binder_transform *h, int precision);
+
 /* No counterpart in the reference: the cudaStream_t the object's work runs on (for events). */
 int binder_registration_get_stream(const binder_registration *h, void **stream_out);
 
