@@ -19,12 +19,11 @@
 #include "umma_transform.cuh"
 
 namespace binder {
-
 namespace {
 
-constexpr int kLines = 128;           // UMMA M
-constexpr int kKC = 32;               // K elements per pipeline chunk
-constexpr int kAPlane = kLines * kKC;  // floats per A plane per stage
+constexpr int kLines = 128;            // UMMA M
+constexpr int kKC = 16;                // K elements per pipeline chunk
+constexpr int kAPlane = kLines * kKC;  // floats per A plane per stage (8 KB)
 constexpr uint64_t kWaitLimit = 2000000000ull;  // 2 s of wall time per barrier wait
 
 struct UArgs {
@@ -33,7 +32,7 @@ struct UArgs {
     long V;
     int n, Npad, nkc;
     long outer, s;
-    const float *B1, *B2;  // preformatted [nkc][2 planes][Npad * 32]
+    const float *B1, *B2;  // preformatted [nkc][2 planes][Npad * kKC]
     // spectral epilogue
     const float *D;
     DevState *st;
@@ -59,32 +58,39 @@ __device__ __forceinline__ float prior_normal_tc(uint64_t seed, uint32_t i, uint
     return comp == 1 ? rad * sn : rad * cs;
 }
 
-// one 16-byte slot of the K-major A plane: rows `line`, K elements 4q .. 4q+3 of the chunk
+// 16-byte slot of the K-major A plane holding row `line`, K elements 4q .. 4q+3 of the chunk:
+// 16-byte K columns 2 KB apart (LBO), 8-row groups 128 B apart (SBO), rows 16 B apart
 __device__ __forceinline__ int a_slot(int line, int q) {
     return q * 512 + (line >> 3) * 32 + (line & 7) * 4;
 }
 
 template <int PLANES>
 __device__ __forceinline__ void store_split(float *plane0, int off, float4 v) {
-    float4 hi = make_float4(umma::to_tf32(v.x), umma::to_tf32(v.y), umma::to_tf32(v.z),
-                            umma::to_tf32(v.w));
+    const float4 hi = make_float4(umma::to_tf32(v.x), umma::to_tf32(v.y), umma::to_tf32(v.z),
+                                  umma::to_tf32(v.w));
     *reinterpret_cast<float4 *>(plane0 + off) = hi;
     if (PLANES == 2) {
-        float4 lo = make_float4(umma::to_tf32(v.x - hi.x), umma::to_tf32(v.y - hi.y),
-                                umma::to_tf32(v.z - hi.z), umma::to_tf32(v.w - hi.w));
+        const float4 lo = make_float4(umma::to_tf32(v.x - hi.x), umma::to_tf32(v.y - hi.y),
+                                      umma::to_tf32(v.z - hi.z), umma::to_tf32(v.w - hi.w));
         *reinterpret_cast<float4 *>(plane0 + kAPlane + off) = lo;
     }
 }
 
+// A chunk for this thread: contiguous axis -> 4 float4 of 4 lines; strided -> its own line
+struct AChunk {
+    float4 v[4];
+};
+
 template <int MODE, int PLANES>
-__global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
+__global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int Npad = a.Npad, n = a.n;
-    float *As = reinterpret_cast<float *>(smem_raw);              // [2 stages][PLANES][kAPlane]
-    float *Bs = As + 2 * PLANES * kAPlane;                        // [2 stages][PLANES][Npad*32]
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * PLANES * Npad * kKC);  // [3]
+    const uint32_t bplane = (uint32_t)Npad * kKC;  // floats per B plane
+    float *As = reinterpret_cast<float *>(smem_raw);   // [2 stages][PLANES][kAPlane]
+    float *Bs = As + 2 * PLANES * kAPlane;             // [2 stages][PLANES][bplane]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * PLANES * bplane);  // [3]
     uint32_t *holder = reinterpret_cast<uint32_t *>(mbar + 3);
     int *s_err = reinterpret_cast<int *>(holder + 1);
     __shared__ double red[32];
@@ -106,6 +112,7 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *holder;
+    const uint32_t tlane = (uint32_t)(warp * 32) << 16;
 
     const int comp = blockIdx.z;
     const float *in = a.in + comp * a.V;
@@ -119,7 +126,8 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
     const long o = valid ? lg / a.s : 0, t = valid ? lg - o * a.s : 0;
     const long lbase = o * (long)n * a.s + t;  // element (line, j) at lbase + j * s
     const uint32_t idesc = umma::instr_desc(kLines, Npad, umma::kFmtTF32);
-    const uint32_t bplane = (uint32_t)Npad * kKC;  // floats per B plane
+    // contiguous-axis load mapping: 8 lines x 4 float4 per warp instruction
+    const int cr = lane & 7, cq = lane >> 3;
 
     uint32_t chunk = 0;  // running chunk counter over both GEMMs: stage = chunk & 1
     double part_cost = 0.0, part_raw = 0.0;
@@ -128,8 +136,54 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
     const double gamma = (MODE == kEpiSpectral) ? a.st->gamma[comp] : 0.0;
     const float gs2 = (float)(gamma * a.sigma2);
 
-    // ---- one GEMM: accumulate into TMEM columns [col_off, col_off + Npad) ----------------------
+    auto load_global = [&](int kc, AChunk &r) {
+        if (contig) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int line = (warp + 4 * i) * 8 + cr;
+                const long g = l0 + line;
+                const int j0 = kc * kKC + cq * 4;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (g < nlines) {
+                    const float *p = in + g * n + j0;
+                    if ((n & 3) == 0 && j0 + 3 < n) {
+                        v = __ldg(reinterpret_cast<const float4 *>(p));
+                    } else {
+                        v.x = j0 < n ? __ldg(p) : 0.f;
+                        v.y = j0 + 1 < n ? __ldg(p + 1) : 0.f;
+                        v.z = j0 + 2 < n ? __ldg(p + 2) : 0.f;
+                        v.w = j0 + 3 < n ? __ldg(p + 3) : 0.f;
+                    }
+                }
+                r.v[i] = v;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j0 = kc * kKC + q * 4;
+                float4 v;
+                v.x = (valid && j0 < n) ? __ldg(in + lbase + (long)j0 * a.s) : 0.f;
+                v.y = (valid && j0 + 1 < n) ? __ldg(in + lbase + (long)(j0 + 1) * a.s) : 0.f;
+                v.z = (valid && j0 + 2 < n) ? __ldg(in + lbase + (long)(j0 + 2) * a.s) : 0.f;
+                v.w = (valid && j0 + 3 < n) ? __ldg(in + lbase + (long)(j0 + 3) * a.s) : 0.f;
+                r.v[q] = v;
+            }
+        }
+    };
+    auto store_global_chunk = [&](const AChunk &r, float *Ap) {
+        if (contig) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) store_split<PLANES>(Ap, a_slot((warp + 4 * i) * 8 + cr, cq), r.v[i]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) store_split<PLANES>(Ap, a_slot(tid, q), r.v[q]);
+        }
+    };
+
+    // ---- one GEMM into TMEM columns [col_off, col_off + Npad); src 0 = global, 1 = TMEM acc0 ----
     auto gemm = [&](const float *Bg, uint32_t col_off, int src) {
+        AChunk pre;
+        if (src == 0) load_global(0, pre);
         for (int kc = 0; kc < a.nkc; ++kc) {
             const uint32_t c = chunk++;
             const int stage = c & 1;
@@ -139,77 +193,46 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
             if (*s_err) return;
             float *Ap = As + stage * PLANES * kAPlane;
             float *Bp = Bs + stage * PLANES * bplane;
+            // B operand: the preformatted chunk, asynchronously
+            {
+                const float *srcb = Bg + (size_t)kc * 2 * bplane;
+                const int nv = PLANES * (int)bplane / 4;
+                for (int qv = tid; qv < nv; qv += 128) umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
+                umma::cp_async_commit();
+            }
             // A operand
             if (src == 0) {
-                if (contig) {
-                    // rows of n contiguous floats: 8 lines x 4 float4 per warp instruction
-                    const int lane = tid & 31, r = lane & 7, h = lane >> 3;
-                    for (int it = warp; it < 32; it += 4) {
-                        const int line = (it >> 1) * 8 + r, q = (it & 1) * 4 + h;
-                        const long g = l0 + line;
-                        const int j0 = kc * kKC + q * 4;
-                        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (g < nlines) {
-                            const float *p = in + g * n + j0;
-                            if ((n & 3) == 0 && j0 + 3 < n) {
-                                v = __ldg(reinterpret_cast<const float4 *>(p));
-                            } else {
-                                v.x = j0 < n ? __ldg(p) : 0.f;
-                                v.y = j0 + 1 < n ? __ldg(p + 1) : 0.f;
-                                v.z = j0 + 2 < n ? __ldg(p + 2) : 0.f;
-                                v.w = j0 + 3 < n ? __ldg(p + 3) : 0.f;
-                            }
-                        }
-                        store_split<PLANES>(Ap, a_slot(line, q), v);
-                    }
-                } else {
-                    // strided axis: lanes are consecutive lines -> coalesced along t
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int j0 = kc * kKC + q * 4;
-                        float4 v;
-                        v.x = (valid && j0 < n) ? __ldg(in + lbase + (long)j0 * a.s) : 0.f;
-                        v.y = (valid && j0 + 1 < n) ? __ldg(in + lbase + (long)(j0 + 1) * a.s) : 0.f;
-                        v.z = (valid && j0 + 2 < n) ? __ldg(in + lbase + (long)(j0 + 2) * a.s) : 0.f;
-                        v.w = (valid && j0 + 3 < n) ? __ldg(in + lbase + (long)(j0 + 3) * a.s) : 0.f;
-                        store_split<PLANES>(Ap, a_slot(tid, q), v);
-                    }
-                }
+                store_global_chunk(pre, Ap);
+                if (kc + 1 < a.nkc) load_global(kc + 1, pre);  // in flight during this chunk's MMAs
             } else {
                 // fused x pass: forward coefficients of this chunk from TMEM, prior scaling,
                 // noise and costs, re-staged as the A operand of the inverse GEMM
-                float v[32];
-                umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(kc * kKC), v);
+                float v[16];
+                umma::tmem_ld16(tmem + tlane + (uint32_t)(kc * kKC), v);
 #pragma unroll
-                for (int m = 0; m < 32; ++m) {
+                for (int m = 0; m < 16; ++m) {
                     const int k = kc * kKC + m;
-                    float c = 0.0f;
+                    float cval = 0.0f;
                     if (valid && k < n) {
                         const long i = (long)k * a.s + t;
                         const float Dv = __ldg(a.D + i);
                         const float f = 1.0f / (1.0f + gs2 * Dv);
-                        c = v[m] * f;
+                        cval = v[m] * f;
                         if (a.sample)
-                            c += sqrtf((float)a.sigma2 * f) *
-                                 prior_normal_tc(a.seed, (uint32_t)i, sweep, a.chain, comp);
-                        const double c2 = (double)c * (double)c;
+                            cval += sqrtf((float)a.sigma2 * f) *
+                                    prior_normal_tc(a.seed, (uint32_t)i, sweep, a.chain, comp);
+                        const double c2 = (double)cval * (double)cval;
                         part_cost += 0.5 * gamma * (double)Dv * c2;
                         if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)Dv * c2;
                     }
-                    v[m] = c;
+                    v[m] = cval;
                 }
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
+                for (int q = 0; q < 4; ++q)
                     store_split<PLANES>(Ap, a_slot(tid, q),
                                         make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
             }
-            // B operand: the preformatted chunk, copied as-is
-            {
-                const float4 *srcb = reinterpret_cast<const float4 *>(Bg + (size_t)kc * 2 * bplane);
-                float4 *dstb = reinterpret_cast<float4 *>(Bp);
-                const int nv = PLANES * (int)bplane / 4;
-                for (int qv = tid; qv < nv; qv += 128) dstb[qv] = __ldg(srcb + qv);
-            }
+            umma::cp_async_wait_all();
             umma::fence_proxy_async_smem();
             __syncthreads();
             if (tid == 0) {
@@ -252,7 +275,7 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
         const int nchunks = (n + 31) / 32;
         for (int cc = 0; cc < nchunks; ++cc) {
             float v[32];
-            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + acc_col + (uint32_t)(cc * 32), v);
+            umma::tmem_ld32(tmem + tlane + acc_col + (uint32_t)(cc * 32), v);
             if (!valid) continue;
             if (contig) {
                 float *dst = out + lg * n;
@@ -297,6 +320,7 @@ __global__ void __launch_bounds__(128, 1) umma_axis_kernel(const UArgs a) {
 
     // ---- teardown: after an error, drain every tcgen05 op still in flight (bounded) -------------
     if (*s_err) {
+        umma::cp_async_wait_all();
         if (tid == 0) {
             umma::commit(&mbar[2]);
             umma::mbar_wait(&mbar[2], 0, kWaitLimit);
@@ -326,8 +350,12 @@ void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
     const uint32_t want = MODE == kEpiSpectral ? 2u * a.Npad : (uint32_t)a.Npad;
     uint32_t ncols = 32;
     while (ncols < want) ncols <<= 1;
-    // a CTA that takes all 512 TMEM columns must be alone on its SM
-    const size_t smem = (ncols == 512 && need < 120 * 1024) ? 120 * 1024 : need;
+    // never let more CTAs share an SM than its 512 TMEM columns can hold at once (a surplus CTA
+    // would only wait inside tcgen05.alloc): pad the shared-memory request accordingly
+    const size_t per_sm = 228 * 1024;
+    const size_t max_ctas = 512 / ncols;
+    const size_t floor_smem = per_sm / (max_ctas + 1) + 1024;
+    const size_t smem = need > floor_smem ? need : floor_smem;
     BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
     BINDER_CUDA(cudaFuncSetAttribute(umma_axis_kernel<MODE, PLANES>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
