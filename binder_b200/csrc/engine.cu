@@ -171,14 +171,26 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     pass(2, false, kEpiNone);
     a.in = t1; a.out = t2; a.M = dct.fwd[1]; a.n = ny; a.outer = nx; a.s = nz;
     pass(1, false, kEpiNone);
-    // x: forward, prior scaling (+ noise, costs), inverse
+    // x: forward, prior scaling (+ noise, costs), inverse.  The CUDA-core path fuses the three in
+    // one pass; the tensor-core path stores the scaled coefficients and runs the inverse as its
+    // own pass, so neither needs more than half of an SM's TMEM (two CTAs per SM).
     a.in = t2; a.out = t1; a.M = dct.fwd[0]; a.M2 = dct.inv[0]; a.n = nx; a.outer = 1;
     a.s = (long)ny * nz;
-    pass(0, false, kEpiSpectral);
+    const float *yin = t1;
+    float *yout = t2;
+    if (tc) {
+        pass(0, false, kEpiSpectralOut);
+        a.in = t1; a.out = t2; a.M2 = nullptr;
+        pass(0, true, kEpiNone);
+        yin = t2;
+        yout = t1;
+    } else {
+        pass(0, false, kEpiSpectral);
+    }
     // inverse DCT-III along y, z; the last pass adds the voxel positions
-    a.in = t1; a.out = t2; a.M = dct.inv[1]; a.M2 = nullptr; a.n = ny; a.outer = nx; a.s = nz;
+    a.in = yin; a.out = yout; a.M = dct.inv[1]; a.M2 = nullptr; a.n = ny; a.outer = nx; a.s = nz;
     pass(1, true, kEpiNone);
-    a.in = t2; a.out = d; a.M = dct.inv[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
+    a.in = yout; a.out = d; a.M = dct.inv[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
     a.xpos = xpos;
     pass(2, true, kEpiPositions);
 }

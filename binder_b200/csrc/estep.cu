@@ -81,13 +81,14 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStep
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
-    float *thT = sm;            // [L][K]
-    float *hs = sm + KL;        // [K][L] CTA histogram
-    float *hk = sm + 2 * KL;    // [K][kEThreads] per-thread bin masses
+    const int KP = K + 1;       // padded row: lanes with different u_i spread over banks
+    float *thT = sm;            // [L][K + 1]
+    float *hs = sm + L * KP;    // [K][L] CTA histogram
+    float *hk = hs + KL;        // [K][kEThreads] per-thread bin masses
     __shared__ double red[32];
     for (int q = threadIdx.x; q < KL; q += blockDim.x) {
         const int k = q / L, l = q - k * L;
-        thT[l * K + k] = a.theta[q];
+        thT[l * KP + k] = a.theta[q];
         hs[q] = 0.0f;
     }
     for (int q = threadIdx.x; q < K * kEThreads; q += blockDim.x) hk[q] = 0.0f;
@@ -115,9 +116,10 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStep
         uint32_t pk[16];
         gather_bins(a, ix, iy, iz, pk);
         const int ui = a.u[i];
-        const float *thu = thT + ui * K;
+        const float *thu = thT + ui * KP;
         float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
-        unsigned long long mask = 0ull;
+        // bins touched, as two 32-bit masks (cheaper than one 64-bit shift per node)
+        uint32_t mlo = 0u, mhi = 0u;
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
@@ -132,35 +134,39 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStep
                     r0 += w;
                     rz = fmaf((float)(c - 1), w, rz);
                     my[k * kEThreads] += w;
-                    mask |= 1ull << k;
+                    const uint32_t bit = 1u << (k & 31);
+                    mlo |= (k < 32) ? bit : 0u;
+                    mhi |= (k < 32) ? 0u : bit;
                 }
                 S += r0;
                 Sx = fmaf((float)(p - 1), r0, Sx);
                 Sy = fmaf((float)(q - 1), r0, Sy);
                 Sz += rz;
             }
-        if (!(S > 0.0f)) {
-            while (mask) {
-                const int k = __ffsll((long long)mask) - 1;
-                mask &= mask - 1;
-                my[k * kEThreads] = 0.0f;
-            }
+        const bool ok = S > 0.0f;
+        const float inv = ok ? 1.0f / S : 0.0f;
+        float *hcol = hs + ui;  // hcol[k * L]
+        while (mlo) {
+            const int k = __ffs((int)mlo) - 1;
+            mlo &= mlo - 1;
+            if (ok) atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
+            my[k * kEThreads] = 0.0f;
+        }
+        while (mhi) {
+            const int k = 32 + __ffs((int)mhi) - 1;
+            mhi &= mhi - 1;
+            if (ok) atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
+            my[k * kEThreads] = 0.0f;
+        }
+        if (!ok) {
             a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
             ++deg;
             continue;
         }
-        const float inv = 1.0f / S;
-        mll -= log((double)S);
+        mll -= (double)logf(S);  // FP32 log, FP64 accumulation
         a.r[i] = (fx + Sx * inv) - x0;
         a.r[a.V + i] = (fy + Sy * inv) - x1;
         a.r[2 * a.V + i] = (fz + Sz * inv) - x2;
-        float *hcol = hs + ui;  // hcol[k * L]
-        while (mask) {
-            const int k = __ffsll((long long)mask) - 1;
-            mask &= mask - 1;
-            atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
-            my[k * kEThreads] = 0.0f;
-        }
     }
     __syncthreads();
     for (int q = threadIdx.x; q < KL; q += blockDim.x) {
@@ -488,7 +494,7 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 
 namespace {
 size_t estep_smem(bool sample, int K, int L) {
-    if (!sample && K <= kSmallK) return (size_t)(2 * K * L + K * kEThreads) * sizeof(float);
+    if (!sample && K <= kSmallK) return (size_t)(L * (K + 1) + K * L + K * kEThreads) * sizeof(float);
     return (size_t)2 * K * L * sizeof(float);
 }
 }  // namespace

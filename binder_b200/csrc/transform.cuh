@@ -33,6 +33,7 @@ enum EpilogueMode : int {
     kEpiPositions = 2,  // store y + x_grid (final inverse pass) into the position field
     kEpiPoisson = 3,    // fused fwd -> -1/lambda (Hartley Poisson) -> inverse (x axis)
     kEpiTopoOut = 4,    // store u * scale + mean into a physical-position field (FP64)
+    kEpiSpectralOut = 5,  // forward pass whose epilogue applies the prior scaling and stores it
 };
 
 template <typename T>

@@ -3,8 +3,9 @@
 // One CTA (4 warps) owns a tile of 128 lines of one component.  The pass is the GEMM
 //   D[line][k] = sum_j X[line][j] * M[k][j]      (M = the n x n transform, rows = outputs)
 // with A = the 128 x n data tile and B = M, both K-major in shared memory in the canonical
-// no-swizzle layout (8-row x 16-byte core matrices), streamed in K chunks of 32 through a
-// two-stage pipeline, accumulated in TMEM by tcgen05.mma (M = 128, N = n padded to 16).
+// no-swizzle layout (8-row x 16-byte core matrices), streamed in K chunks of 16 (A: registers
+// prefetched one chunk ahead into a 2-stage ring; B: cp.async into a 3-slot ring one chunk ahead),
+// accumulated in TMEM by tcgen05.mma (M = 128, N = n padded to 16).
 // Precision: TF32 operands (one plane), or "3xTF32" -- hi/lo TF32 planes and the three products
 // hi*hi + hi*lo + lo*hi, which keeps FP32-level accuracy -- always with FP32 accumulation.
 // The x-axis pass of the DCT prior is fused: forward GEMM into TMEM columns [0, Npad), the prior
@@ -48,8 +49,10 @@ struct UArgs {
     const int *skip;
 };
 
-__device__ __forceinline__ float prior_normal_tc(uint64_t seed, uint32_t i, uint32_t sweep,
-                                                 uint32_t chain, int comp) {
+// out of line: the epilogue loops are unrolled, and an inlined Philox + Box-Muller per element
+// would bloat them (instruction-cache misses) even in EM, where the branch is never taken
+__device__ __noinline__ float prior_normal_tc(uint64_t seed, uint32_t i, uint32_t sweep,
+                                              uint32_t chain, int comp) {
     const u32x4 r = philox_draw(seed, i, sweep, comp < 2 ? 2u : 3u, chain);
     const float u1 = u01_f24(r.x), u2 = u01_f24(r.y);
     const float rad = sqrtf(-2.0f * logf(u1));
@@ -89,8 +92,8 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     const int Npad = a.Npad, n = a.n;
     const uint32_t bplane = (uint32_t)Npad * kKC;  // floats per B plane
     float *As = reinterpret_cast<float *>(smem_raw);   // [2 stages][PLANES][kAPlane]
-    float *Bs = As + 2 * PLANES * kAPlane;             // [2 stages][PLANES][bplane]
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 2 * PLANES * bplane);  // [3]
+    float *Bs = As + 2 * PLANES * kAPlane;             // [3 slots][PLANES][bplane]
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(Bs + 3 * PLANES * bplane);  // [3]
     uint32_t *holder = reinterpret_cast<uint32_t *>(mbar + 3);
     int *s_err = reinterpret_cast<int *>(holder + 1);
     __shared__ double red[32];
@@ -131,9 +134,9 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
 
     uint32_t chunk = 0;  // running chunk counter over both GEMMs: stage = chunk & 1
     double part_cost = 0.0, part_raw = 0.0;
-    const uint32_t sweep = (MODE == kEpiSpectral && a.sample) ? (uint32_t)a.st->sweep : 0u;
-    const bool want_raw = (MODE == kEpiSpectral) && a.want_raw && (a.st->sweep % a.every == 0);
-    const double gamma = (MODE == kEpiSpectral) ? a.st->gamma[comp] : 0.0;
+    const uint32_t sweep = ((MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.sample) ? (uint32_t)a.st->sweep : 0u;
+    const bool want_raw = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.want_raw && (a.st->sweep % a.every == 0);
+    const double gamma = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) ? a.st->gamma[comp] : 0.0;
     const float gs2 = (float)(gamma * a.sigma2);
 
     auto load_global = [&](int kc, AChunk &r) {
@@ -181,25 +184,43 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     };
 
     // ---- one GEMM into TMEM columns [col_off, col_off + Npad); src 0 = global, 1 = TMEM acc0 ----
+    // A ring of 2 stages, B ring of 3: the B chunk for c+1 is requested (cp.async) as soon as the
+    // MMAs of chunk c-2 are known complete, so its L2 latency overlaps chunk c.
+    auto issue_b = [&](const float *Bg, int kc, uint32_t c) {
+        if (kc < a.nkc) {
+            const float *srcb = Bg + (size_t)kc * 2 * bplane;
+            float *Bp = Bs + (c % 3) * PLANES * bplane;
+            const int nv = PLANES * (int)bplane / 4;
+            for (int qv = tid; qv < nv; qv += 128) umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
+        }
+        umma::cp_async_commit();  // possibly empty: keeps one group per chunk
+    };
     auto gemm = [&](const float *Bg, uint32_t col_off, int src) {
         AChunk pre;
+        float dpre[16];
         if (src == 0) load_global(0, pre);
+        auto load_d = [&](int kc) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int k = kc * kKC + m;
+                dpre[m] = (valid && k < n) ? __ldg(a.D + (long)k * a.s + t) : 0.0f;
+            }
+        };
+        if (src == 1) load_d(0);
+        issue_b(Bg, 0, chunk);
         for (int kc = 0; kc < a.nkc; ++kc) {
             const uint32_t c = chunk++;
             const int stage = c & 1;
             if (c >= 2 && !umma::mbar_wait(&mbar[stage], ((c >> 1) - 1) & 1, kWaitLimit))
                 atomicOr(s_err, 1);
             __syncthreads();
-            if (*s_err) return;
-            float *Ap = As + stage * PLANES * kAPlane;
-            float *Bp = Bs + stage * PLANES * bplane;
-            // B operand: the preformatted chunk, asynchronously
-            {
-                const float *srcb = Bg + (size_t)kc * 2 * bplane;
-                const int nv = PLANES * (int)bplane / 4;
-                for (int qv = tid; qv < nv; qv += 128) umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
-                umma::cp_async_commit();
+            if (*s_err) {
+                umma::cp_async_wait_all();
+                return;
             }
+            issue_b(Bg, kc + 1, c + 1);  // its ring slot was last read by chunk c - 2
+            float *Ap = As + stage * PLANES * kAPlane;
+            float *Bp = Bs + (c % 3) * PLANES * bplane;
             // A operand
             if (src == 0) {
                 store_global_chunk(pre, Ap);
@@ -209,30 +230,32 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                 // noise and costs, re-staged as the A operand of the inverse GEMM
                 float v[16];
                 umma::tmem_ld16(tmem + tlane + (uint32_t)(kc * kKC), v);
+                float ccost = 0.0f;
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int k = kc * kKC + m;
                     float cval = 0.0f;
                     if (valid && k < n) {
-                        const long i = (long)k * a.s + t;
-                        const float Dv = __ldg(a.D + i);
-                        const float f = 1.0f / (1.0f + gs2 * Dv);
+                        const float Dv = dpre[m];
+                        const float f = __frcp_rn(fmaf(gs2, Dv, 1.0f));
                         cval = v[m] * f;
                         if (a.sample)
                             cval += sqrtf((float)a.sigma2 * f) *
-                                    prior_normal_tc(a.seed, (uint32_t)i, sweep, a.chain, comp);
-                        const double c2 = (double)cval * (double)cval;
-                        part_cost += 0.5 * gamma * (double)Dv * c2;
-                        if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)Dv * c2;
+                                    prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
+                                                    a.chain, comp);
+                        ccost += Dv * cval * cval;
                     }
                     v[m] = cval;
                 }
+                part_cost += 0.5 * gamma * (double)ccost;
+                if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)ccost;
+                if (kc + 1 < a.nkc) load_d(kc + 1);
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     store_split<PLANES>(Ap, a_slot(tid, q),
                                         make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
             }
-            umma::cp_async_wait_all();
+            asm volatile("cp.async.wait_group 1;" ::: "memory");  // B chunk c has landed
             umma::fence_proxy_async_smem();
             __syncthreads();
             if (tid == 0) {
@@ -256,6 +279,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                 umma::commit(&mbar[stage]);
             }
         }
+        umma::cp_async_wait_all();  // the trailing (empty) group
         // wait for the whole accumulation
         const uint32_t last = chunk - 1;
         if (!umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitLimit)) atomicOr(s_err, 1);
@@ -273,43 +297,93 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     if (!*s_err) {
         // ---- epilogue: 32 TMEM columns at a time -------------------------------------------
         const int nchunks = (n + 31) / 32;
-        for (int cc = 0; cc < nchunks; ++cc) {
-            float v[32];
-            umma::tmem_ld32(tmem + tlane + acc_col + (uint32_t)(cc * 32), v);
-            if (!valid) continue;
-            if (contig) {
-                float *dst = out + lg * n;
+        if (contig) {
+            // each warp stages its 32 lines x 32 columns in shared memory (row pitch 33, no bank
+            // conflicts) and writes them back as coalesced 128-byte rows; the pipeline buffers
+            // are free once the accumulation has completed
+            float *stg = reinterpret_cast<float *>(smem_raw) + warp * 32 * 33;
+            // positions pass (z axis): row g = x * ny + y; each lane owns the coordinate of row
+            // `lane` of this warp and the row loop broadcasts it
+            float rowc = 0.0f;
+            if (MODE == kEpiPositions && !a.xpos) {
+                const int gi = (int)(l0 + warp * 32 + lane);
+                rowc = comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny);
+            }
+            for (int cc = 0; cc < nchunks; ++cc) {
+                float v[32];
+                umma::tmem_ld32(tmem + tlane + acc_col + (uint32_t)(cc * 32), v);
+#pragma unroll
+                for (int m = 0; m < 32; ++m) stg[lane * 33 + m] = v[m];
+                __syncwarp();
+                const int k = cc * 32 + lane;
+#pragma unroll 4
+                for (int r = 0; r < 32; ++r) {
+                    const long g = l0 + warp * 32 + r;
+                    const float rc = __shfl_sync(0xffffffffu, rowc, r);
+                    if (g < nlines && k < n) {
+                        float val = stg[r * 33 + lane];
+                        if (MODE == kEpiPositions)
+                            val += a.xpos ? __ldg(a.xpos + comp * a.V + g * n + k)
+                                          : (comp == 2 ? (float)k : rc);
+                        out[g * n + k] = val;
+                    }
+                }
+                __syncwarp();
+            }
+        } else {
+            // prior eigenvalues of coefficient (k, t) at flat index k * s + t, one 32-chunk ahead
+            // in registers: loaded beside the stores to `out` they would be serialised behind them
+            float dnext[32];
+            auto load_dchunk = [&](int cc) {
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = cc * 32 + m;
+                    dnext[m] = (valid && k < n) ? __ldg(a.D + (long)k * a.s + t) : 0.0f;
+                }
+            };
+            if (MODE == kEpiSpectralOut) load_dchunk(0);
+            for (int cc = 0; cc < nchunks; ++cc) {
+                float v[32], dcur[32];
+                umma::tmem_ld32(tmem + tlane + acc_col + (uint32_t)(cc * 32), v);
+                if (MODE == kEpiSpectralOut) {
+#pragma unroll
+                    for (int m = 0; m < 32; ++m) dcur[m] = dnext[m];
+                    if (cc + 1 < nchunks) load_dchunk(cc + 1);
+                }
+                if (!valid) continue;
+                // prior costs of this chunk: FP32 partial sums over 32 coefficients, FP64 across
+                float ccost = 0.0f, craw = 0.0f;
+                float *op = out + lbase;
 #pragma unroll
                 for (int m = 0; m < 32; ++m) {
                     const int k = cc * 32 + m;
                     if (k < n) {
                         float val = v[m];
-                        if (MODE == kEpiPositions) {
-                            const long i = lg * n + k;
-                            float xv;
-                            if (a.xpos) {
-                                xv = __ldg(a.xpos + comp * a.V + i);
-                            } else {
-                                const long yz = (long)a.ny * a.nz;
-                                xv = comp == 0 ? (float)(i / yz)
-                                               : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
-                            }
-                            val += xv;
+                        if (MODE == kEpiSpectralOut) {
+                            // forward x pass: coefficient (k, t) has flat index k * s + t
+                            const float Dv = dcur[m];
+                            const float f = __frcp_rn(fmaf(gs2, Dv, 1.0f));
+                            val *= f;
+                            if (a.sample)
+                                val += sqrtf((float)a.sigma2 * f) *
+                                       prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
+                                                       a.chain, comp);
+                            const float dv2 = Dv * val * val;
+                            ccost += dv2;
+                            craw += dv2;
                         }
-                        dst[k] = val;
+                        op[(long)k * a.s] = val;
                     }
                 }
-            } else {
-#pragma unroll
-                for (int m = 0; m < 32; ++m) {
-                    const int k = cc * 32 + m;
-                    if (k < n) out[lbase + (long)k * a.s] = v[m];
+                if (MODE == kEpiSpectralOut) {
+                    part_cost += 0.5 * gamma * (double)ccost;
+                    if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)craw;
                 }
             }
         }
     }
 
-    if (MODE == kEpiSpectral) {
+    if (MODE == kEpiSpectral || MODE == kEpiSpectralOut) {
         const double sc = block_sum(part_cost, red);
         if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
         if (a.want_raw) {
@@ -346,7 +420,9 @@ float tf32_rna_host(float x) {
 
 template <int MODE, int PLANES>
 void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
-    const size_t need = (size_t)(2 * PLANES * kAPlane + 2 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
+    size_t need = (size_t)(2 * PLANES * kAPlane + 3 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
+    const size_t staging = (size_t)4 * 32 * 33 * sizeof(float) + 64;  // contiguous-axis epilogue
+    if (need < staging) need = staging;
     const uint32_t want = MODE == kEpiSpectral ? 2u * a.Npad : (uint32_t)a.Npad;
     uint32_t ncols = 32;
     while (ncols < want) ncols <<= 1;
@@ -415,6 +491,11 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     switch (mode) {
         BINDER_UMMA_CASE(kEpiNone)
         BINDER_UMMA_CASE(kEpiPositions)
+        case kEpiSpectralOut:
+            BINDER_CHECK(b.outer == 1, "prior scaling runs on the outermost axis");
+            if (planes == 2) launch_umma<kEpiSpectralOut, 2>(a, ncomp, s);
+            else launch_umma<kEpiSpectralOut, 1>(a, ncomp, s);
+            break;
         case kEpiSpectral:
             BINDER_CHECK(M2 && M2->n == b.n, "fused pass needs the inverse matrix");
             BINDER_CHECK(b.outer == 1, "fused prior pass runs on the outermost axis");
