@@ -78,13 +78,8 @@ def dist_setup(n_gpus):
 
 
 def max_over_ranks(x, dist):
-    if dist is None:
-        return x
-    import torch
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from binder_b200.replicas import max_over_ranks as mor
+    return mor(x, dist)
 
 
 def barrier(dist):
@@ -137,8 +132,9 @@ class Clocks(threading.Thread):
 
 def make_inputs(rank):
     from binder_b200 import phantoms
+    from binder_b200.replicas import unit_seed
     from binder_b200.utils import initialize_fourier_domain_smoothing
-    pair = phantoms.make_pair(SHAPE, SEED + rank, bins=BINS)
+    pair = phantoms.make_pair(SHAPE, unit_seed(SEED, rank), bins=BINS)  # one pair per rank
     V = int(np.prod(SHAPE))
     grid = phantoms.identity_positions(SHAPE).astype(np.float32)
     D = initialize_fourier_domain_smoothing(SHAPE, True, 2, 3).astype(np.float32)
