@@ -34,6 +34,7 @@ EXPORTS = [
     "binder_transform_create", "binder_transform_destroy",
     "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
     "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
+    "binder_jacobian_determinant_3d_noalloc", "binder_jacobian_noalloc_max_voxels",
 ]
 
 
@@ -58,6 +59,7 @@ def _declare(lib):
     lib.binder_backend.restype = C.c_char_p
     lib.binder_has_topology_correction.restype = _i
     lib.binder_kernel_launch_count.restype = C.c_longlong
+    lib.binder_jacobian_noalloc_max_voxels.restype = C.c_longlong
     sig = {
         "binder_registration_create": [C.POINTER(_P), _f32, _i, _f32, _P] + [_i] * 7 + [_d],
         "binder_registration_destroy": [_P],
@@ -88,6 +90,8 @@ def _declare(lib):
         "binder_transform_sample_deformation_field": [_P, _f32, _i, _f32],
         "binder_transform_get_shape": [_P, _i32],
         "binder_jacobian_determinant_3d": [_f64, _i, _i, _i, _d, _d, _d, _f64],
+        "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
+                                                   C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],
     }
     for name, args in sig.items():

@@ -346,6 +346,26 @@ int binder_jacobian_determinant_3d(const double *field, int Nx, int Ny, int Nz, 
     });
 }
 
+int binder_jacobian_determinant_3d_noalloc(const double *field, int Nx, int Ny, int Nz,
+                                           double voxel_size_x, double voxel_size_y,
+                                           double voxel_size_z, double *J_out,
+                                           double minmax_out[2], long long *negative_out) {
+    return guard([&] {
+        NEED(field);
+        NEED(J_out);
+        const double vs[3] = {voxel_size_x, voxel_size_y, voxel_size_z};
+        binder::JacStats st{};
+        binder::jacobian3d_noalloc(field, Nx, Ny, Nz, vs, J_out, &st);
+        if (minmax_out) {
+            minmax_out[0] = st.jmin;
+            minmax_out[1] = st.jmax;
+        }
+        if (negative_out) *negative_out = st.negative;
+    });
+}
+
+long long binder_jacobian_noalloc_max_voxels(void) { return binder::kJacobianNoAllocMaxVoxels; }
+
 int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
                                int max_it, int threads, const double voxel_sizes[3], int Nx,
                                int Ny, int Nz, double *out, long long *stats_out) {

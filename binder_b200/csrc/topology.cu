@@ -5,6 +5,7 @@
 // the negative / out-of-range counts and the set of corners the limiter touches) equal the
 // reference CPU backend's bit for bit on the same FP64 input.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "topology.cuh"
@@ -375,6 +376,82 @@ void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const do
     count_launch(), jacobian_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, 3, 1, nx, ny, nz,
                                                 1.0 / (vs[0] * vs[1] * vs[2]), J, 0.0, 0.0, nullptr);
     BINDER_CUDA(cudaGetLastError());
+}
+
+// ---- Jacobian through a fixed device scratch array ------------------------------------------
+// Some callers cannot afford cudaMalloc / cudaFree on every call: a framework whose caching
+// allocator already holds most of the GPU's memory (a fresh cudaMalloc then fails even though the
+// framework has room), or a loop that keeps other streams busy and cannot take the device-wide
+// synchronisation cudaFree implies.  This variant stages the field, the determinants and the
+// summary record in one array that is part of the library's device image, sized for grids of up
+// to kJacobianNoAllocMaxVoxels voxels (16 MiB in all), so a call allocates nothing.
+namespace {
+constexpr size_t kNoAllocHeader = 256;  // the reduction record, padded
+static_assert(sizeof(Red) <= kNoAllocHeader, "reduction record does not fit its slot");
+// [Red | field: 3 * max doubles | J: max doubles]
+static __device__ __align__(256) unsigned char
+    g_jacobian_scratch[kNoAllocHeader + 4 * sizeof(double) * kJacobianNoAllocMaxVoxels];
+constexpr int kNoAllocMaxDevices = 64;
+
+// address of the scratch array on the current device, looked up once per device (with that
+// device current) and kept; the lock guards only this table, not the scratch itself
+unsigned char *jacobian_scratch_address() {
+    static std::mutex mu;
+    static unsigned char *addr[kNoAllocMaxDevices] = {};
+    int dev = -1;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CHECK(dev >= 0 && dev < kNoAllocMaxDevices, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        BINDER_CUDA(cudaGetSymbolAddress(&p, g_jacobian_scratch));
+        addr[dev] = static_cast<unsigned char *>(p);
+    }
+    return addr[dev];
+}
+
+// the record's starting values: min/max as empty ordered keys, counts zero
+__global__ void clear_red_kernel(Red *r) {
+    r->mn = ~0ull;
+    r->mx = 0ull;
+    r->below = r->above = r->negative = 0ull;
+    r->sum[0] = r->sum[1] = r->sum[2] = 0.0;
+    r->count = 0;
+    r->pad = 0;
+}
+}  // namespace
+
+void jacobian3d_noalloc(const double *field_host, int nx, int ny, int nz, const double vs[3],
+                        double *J_host, JacStats *stats) {
+    BINDER_CHECK(nx > 0 && ny > 0 && nz > 0, "dimensions must be positive");
+    const long V = (long)nx * ny * nz;
+    if (V > kJacobianNoAllocMaxVoxels)
+        throw Error(kInvalidArgument,
+                    "grid of " + std::to_string(V) + " voxels exceeds the no-allocation limit of " +
+                        std::to_string(kJacobianNoAllocMaxVoxels) + " voxels");
+    unsigned char *base = jacobian_scratch_address();
+    Red *red = reinterpret_cast<Red *>(base);
+    double *df = reinterpret_cast<double *>(base + kNoAllocHeader);
+    double *dj = df + 3 * kJacobianNoAllocMaxVoxels;
+    const cudaStream_t s = 0;
+    count_launch(), clear_red_kernel<<<1, 1, 0, s>>>(red);
+    BINDER_CUDA(cudaGetLastError());
+    BINDER_CUDA(cudaMemcpyAsync(df, field_host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
+    // e1 = e2 = 0: `below` and `above` count J < 0 and J > 0
+    count_launch(), jacobian_kernel<<<grid_for(V), 256, 0, s>>>(
+        df, 3, 1, nx, ny, nz, 1.0 / (vs[0] * vs[1] * vs[2]), dj, 0.0, 0.0, red);
+    BINDER_CUDA(cudaGetLastError());
+    BINDER_CUDA(cudaMemcpyAsync(J_host, dj, sizeof(double) * V, cudaMemcpyDeviceToHost, s));
+    Red h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, red, sizeof(Red), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->jmin = unordered(h.mn);
+        stats->jmax = unordered(h.mx);
+        stats->below = (long long)h.below;
+        stats->above = (long long)h.above;
+        stats->negative = (long long)h.negative;
+    }
 }
 
 namespace {

@@ -15,6 +15,15 @@ struct JacStats {
 void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const double vs[3],
                        double *J, cudaStream_t s);
 
+// The same determinants from a host AoS field into host J, staged through a fixed array in the
+// library's device image instead of allocated buffers (grids up to kJacobianNoAllocMaxVoxels).
+// Runs on the legacy default stream of the current device and returns when J is on the host.
+// Calls that overlap in time on one device share the array and race.  stats may be NULL; its
+// `below` / `above` count J < 0 / J > 0.
+constexpr long kJacobianNoAllocMaxVoxels = 1L << 19;
+void jacobian3d_noalloc(const double *field_host, int nx, int ny, int nz, const double vs[3],
+                        double *J_host, JacStats *stats);
+
 // full correction on a host AoS field in grid units (in place)
 struct TopologyResult {
     int outer_iterations;

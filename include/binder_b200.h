@@ -178,6 +178,29 @@ int binder_transform_get_shape(const binder_transform *h, int out[4]);
 int binder_jacobian_determinant_3d(const double *field, int Nx, int Ny, int Nz, double voxel_size_x,
                                    double voxel_size_y, double voxel_size_z, double *J_out);
 
+/* No counterpart in the reference: binder_jacobian_determinant_3d without any device allocation.
+ * The call above allocates device buffers for the field and the determinants (cudaMalloc) and
+ * frees them (cudaFree) every time.  Some callers cannot do that: a framework whose caching
+ * allocator already holds most of the GPU's memory gets out-of-memory from a fresh cudaMalloc
+ * even though its own pool has room, and a caller that keeps other streams busy cannot afford the
+ * device-wide synchronisation cudaFree implies.  This variant stages the field, the determinants
+ * and its summary in one fixed array inside the library's device image (16 MiB), so it handles
+ * grids of at most binder_jacobian_noalloc_max_voxels() voxels (524288; e.g. 80x80x80) and
+ * rejects larger ones with BINDER_STATUS_INVALID_ARGUMENT.  The summary is reset on every call.
+ *   - The first call on each device looks up the array's device address (with that device
+ *     current) and keeps it; make that first call before any stream capture begins.
+ *   - Work runs on the legacy default stream of the calling thread's current device; the call
+ *     returns when J_out is filled.
+ *   - Calls that overlap in time on the same device share the array and race: serialise them.
+ * J_out as for binder_jacobian_determinant_3d (bit-identical values).  minmax_out (optional, 2
+ * values) receives min and max of J; negative_out (optional) the number of voxels with J < 0. */
+int binder_jacobian_determinant_3d_noalloc(const double *field, int Nx, int Ny, int Nz,
+                                           double voxel_size_x, double voxel_size_y,
+                                           double voxel_size_z, double *J_out,
+                                           double minmax_out[2], long long *negative_out);
+/* largest voxel count binder_jacobian_determinant_3d_noalloc accepts */
+long long binder_jacobian_noalloc_max_voxels(void);
+
 /* topology_correction_3D().correct_topology(h, e1, e2, max_outer_it, max_it, threads,
  *                                           voxel_sizes, Nx, Ny, Nz) -> [Nx,Ny,Nz,3]
  *                                                               gpu/bindings.cpp:259-287
