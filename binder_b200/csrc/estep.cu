@@ -62,6 +62,31 @@ __device__ __forceinline__ void gather_bins(const EStepArgs &a, int ix, int iy, 
     }
 }
 
+// word (p, q) of gather_bins alone: bins of nodes (ix-1+p, iy-1+q, iz-1 .. iz+2)
+__device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int iy, int iz, int p,
+                                                int q) {
+    const int zz0 = iz - 1 + a.PZ;
+    const int X = ix - 1 + p, Y = iy - 1 + q;
+    const bool fast = (X + a.P >= 0) && (X + a.P < a.nxn + 2 * a.P) && (Y + a.P >= 0) &&
+                      (Y + a.P < a.nyn + 2 * a.P) && (zz0 >= 0) && ((zz0 >> 2) + 2 <= (a.zp >> 2));
+    if (fast) {
+        const uint32_t *rowp = reinterpret_cast<const uint32_t *>(
+            a.vpad + ((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp);
+        const int w = zz0 >> 2, sh = (zz0 & 3) * 8;
+        return __funnelshift_r(__ldg(rowp + w), __ldg(rowp + w + 1), sh);
+    }
+    uint32_t word = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int Z = iz - 1 + c;
+        uint32_t b = 0;
+        if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn)
+            b = a.vpad[((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp + (Z + a.PZ)];
+        word |= b << (8 * c);
+    }
+    return word;
+}
+
 __device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int comp) {
     if (a.x) return a.x[comp * a.V + i];
     const long yz = (long)a.ny * a.nz;
@@ -69,41 +94,56 @@ __device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int com
 }
 
 constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
+constexpr int kFastThreads = 256;
 
 // EM E-step for K <= 64 (BINDER/src/cpu/Registration.cpp:219-330, sample == false), one pass over
 // the 64 neighbours.  The posterior mass of a voxel is collected per moving bin k in a private
 // shared-memory column hk[k][thread] (bank = thread % 32, so never a conflict and never an
-// atomic), with a 64-bit mask of the bins touched; once the normaliser S is known the touched bins
-// are flushed as hist[k][u] += hk[k] / S -- one shared atomic per distinct bin instead of one per
-// neighbour.  theta is staged transposed (thT[u][k]) so lanes that share a fixed-image bin read
-// consecutive banks.
-__global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStepArgs a) {
+// atomic), while the smallest and largest bin touched are tracked; once the normaliser S is known
+// the columns in [kmin, kmax] that hold mass are flushed as hist[k][u] += hk[k] / S -- one shared
+// atomic per distinct bin instead of one per neighbour (the bin range of a 4x4x4 neighbourhood is
+// a handful of bins in smooth images).  theta is staged transposed (thT[u][k]) so lanes that share
+// a fixed-image bin read consecutive banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
+// host).
+template <int TPB>
+__global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
     const int KP = K + 1;       // padded row: lanes with different u_i spread over banks
     float *thT = sm;            // [L][K + 1]
     float *hs = sm + L * KP;    // [K][L] CTA histogram
-    float *hk = hs + KL;        // [K][kEThreads] per-thread bin masses
+    float *hk = hs + KL;        // [K][TPB] per-thread bin masses
     __shared__ double red[32];
-    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+    for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L, l = q - k * L;
         thT[l * KP + k] = a.theta[q];
         hs[q] = 0.0f;
     }
-    for (int q = threadIdx.x; q < K * kEThreads; q += blockDim.x) hk[q] = 0.0f;
+    for (int q = threadIdx.x; q < K * TPB; q += TPB) hk[q] = 0.0f;
     __syncthreads();
 
-    float *my = hk + threadIdx.x;  // my[k * kEThreads]
+    float *my = hk + threadIdx.x;  // my[k * TPB]
     double mll = 0.0;
-    unsigned long long deg = 0;
-    const float *d0 = a.d, *d1 = a.d + a.V, *d2 = a.d + 2 * a.V;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.V;
-         i += (long)gridDim.x * blockDim.x) {
+    unsigned deg = 0;
+    // unsigned: i + stride stays below 2^32 for any V < 2^31
+    const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
+    const float *d0 = a.d, *d1 = a.d + V, *d2 = a.d + 2 * (size_t)V;
+    float *r0p = a.r, *r1p = a.r + V, *r2p = a.r + 2 * (size_t)V;
+    for (unsigned i = blockIdx.x * TPB + threadIdx.x; i < V; i += gridDim.x * TPB) {
         const float px = d0[i], py = d1[i], pz = d2[i];
-        const float x0 = voxel_coord(a, i, 0), x1 = voxel_coord(a, i, 1), x2 = voxel_coord(a, i, 2);
+        float x0, x1, x2;
+        if (a.x) {
+            x0 = a.x[i]; x1 = a.x[V + i]; x2 = a.x[2 * (size_t)V + i];
+        } else {
+            const unsigned row = i / nz;
+            x2 = (float)(i - row * nz);
+            const unsigned xi = row / ny;
+            x1 = (float)(row - xi * ny);
+            x0 = (float)xi;
+        }
         if (!(fabsf(px) < 1.0e6f && fabsf(py) < 1.0e6f && fabsf(pz) < 1.0e6f)) {
-            a.r[i] = px - x0; a.r[a.V + i] = py - x1; a.r[2 * a.V + i] = pz - x2;
+            r0p[i] = px - x0; r1p[i] = py - x1; r2p[i] = pz - x2;
             ++deg;
             continue;
         }
@@ -118,58 +158,51 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_em_fast_kernel(const EStep
         const int ui = a.u[i];
         const float *thu = thT + ui * KP;
         float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
-        // bins touched, as two 32-bit masks (cheaper than one 64-bit shift per node)
-        uint32_t mlo = 0u, mhi = 0u;
+        int kmin = 255, kmax = 0;
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float bxy = bx[p] * by[q];
                 const uint32_t word = pk[p * 4 + q];
-                float r0 = 0.0f, rz = 0.0f;
+                float rs = 0.0f, rz = 0.0f;
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const int k = (word >> (8 * c)) & 0xff;
                     const float w = (bxy * bz[c]) * thu[k];
-                    r0 += w;
+                    rs += w;
                     rz = fmaf((float)(c - 1), w, rz);
-                    my[k * kEThreads] += w;
-                    const uint32_t bit = 1u << (k & 31);
-                    mlo |= (k < 32) ? bit : 0u;
-                    mhi |= (k < 32) ? 0u : bit;
+                    my[k * TPB] += w;
+                    kmin = min(kmin, k);
+                    kmax = max(kmax, k);
                 }
-                S += r0;
-                Sx = fmaf((float)(p - 1), r0, Sx);
-                Sy = fmaf((float)(q - 1), r0, Sy);
+                S += rs;
+                Sx = fmaf((float)(p - 1), rs, Sx);
+                Sy = fmaf((float)(q - 1), rs, Sy);
                 Sz += rz;
             }
         const bool ok = S > 0.0f;
         const float inv = ok ? 1.0f / S : 0.0f;
         float *hcol = hs + ui;  // hcol[k * L]
-        while (mlo) {
-            const int k = __ffs((int)mlo) - 1;
-            mlo &= mlo - 1;
-            if (ok) atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
-            my[k * kEThreads] = 0.0f;
-        }
-        while (mhi) {
-            const int k = 32 + __ffs((int)mhi) - 1;
-            mhi &= mhi - 1;
-            if (ok) atomicAdd(&hcol[k * L], my[k * kEThreads] * inv);
-            my[k * kEThreads] = 0.0f;
+        for (int k = kmin; k <= kmax; ++k) {
+            const float m = my[k * TPB];
+            if (m != 0.0f) {
+                if (ok) atomicAdd(&hcol[k * L], m * inv);
+                my[k * TPB] = 0.0f;
+            }
         }
         if (!ok) {
-            a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
+            r0p[i] = fx - x0; r1p[i] = fy - x1; r2p[i] = fz - x2;
             ++deg;
             continue;
         }
         mll -= (double)logf(S);  // FP32 log, FP64 accumulation
-        a.r[i] = (fx + Sx * inv) - x0;
-        a.r[a.V + i] = (fy + Sy * inv) - x1;
-        a.r[2 * a.V + i] = (fz + Sz * inv) - x2;
+        r0p[i] = (fx + Sx * inv) - x0;
+        r1p[i] = (fy + Sy * inv) - x1;
+        r2p[i] = (fz + Sz * inv) - x2;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < KL; q += blockDim.x) {
+    for (int q = threadIdx.x; q < KL; q += TPB) {
         const float v = hs[q];
         if (v != 0.0f) atomicAdd(&a.hist[q], v);
     }
@@ -190,6 +223,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
     float *th = sm;
     float *hs = sm + KL;                                 // EM histogram
     unsigned *hc = reinterpret_cast<unsigned *>(sm + KL);  // Gibbs counts
+    float *cps = sm + 2 * KL + threadIdx.x;  // Gibbs: cdf at the end of node row r, cps[r * kEThreads]
     __shared__ double red[32];
     for (int q = threadIdx.x; q < KL; q += blockDim.x) {
         th[q] = a.theta[q];
@@ -239,6 +273,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
                     Sy = fmaf((float)(q - 1), w, Sy);
                     Sz = fmaf((float)(c - 1), w, Sz);
                 }
+                if (SAMPLE) cps[(p * 4 + q) * kEThreads] = S;
             }
         if (!(S > 0.0f)) {
             a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
@@ -277,31 +312,41 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
                 }
             atomicAdd(&hs[ck * L + ui], cacc);
         } else {
-            // categorical draw: first neighbour whose running sum reaches u * S
+            // categorical draw: first neighbour whose running sum reaches u * S.  The running sum
+            // is the same sequence of FP32 additions as S above and never decreases (w >= 0), so
+            // the first node row whose end value reaches the target holds the pick; only that
+            // row's four nodes are summed again, from the previous row's end value.
             const u32x4 rr = philox_draw(a.seed, (uint32_t)i, sweep, 1u, a.chain);
             const float t = u01_f24(rr.x) * S;
+            int row = 15;
             float cdf = 0.0f;
+            for (int r = 0; r < 16; ++r) {
+                const float e = cps[r * kEThreads];
+                if (e >= t) {
+                    row = r;
+                    break;
+                }
+                cdf = e;
+            }
+            const int p = row >> 2, q = row & 3;
+            const float bxp = p == 0 ? bx[0] : (p == 1 ? bx[1] : (p == 2 ? bx[2] : bx[3]));
+            const float byq = q == 0 ? by[0] : (q == 1 ? by[1] : (q == 2 ? by[2] : by[3]));
+            const float bxy = __fmul_rn(bxp, byq);
+            const uint32_t word = gather_word(a, ix, iy, iz, p, q);
             int pick = -1, kp = 0;
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float bxy = __fmul_rn(bx[p], by[q]);
-                    const uint32_t word = pk[p * 4 + q];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const int k = (word >> (8 * c)) & 0xff;
-                        const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
-                        cdf = __fadd_rn(cdf, w);
-                        if (pick < 0 && cdf >= t) {
-                            pick = p * 16 + q * 4 + c;
-                            kp = k;
-                        }
-                    }
+            for (int c = 0; c < 4; ++c) {
+                const int k = (word >> (8 * c)) & 0xff;
+                const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
+                cdf = __fadd_rn(cdf, w);
+                if (pick < 0 && cdf >= t) {
+                    pick = row * 4 + c;
+                    kp = k;
                 }
+            }
             if (pick < 0) {  // unreachable (cdf ends at S >= t); keep the last neighbour
                 pick = 63;
-                kp = (pk[15] >> 24) & 0xff;
+                kp = (gather_word(a, ix, iy, iz, 3, 3) >> 24) & 0xff;
             }
             atomicAdd(&hc[kp * L + a.u[i]], 1u);
             a.r[i] = (fx + (float)(pick / 16 - 1)) - x0;
@@ -494,8 +539,8 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 
 namespace {
 size_t estep_smem(bool sample, int K, int L) {
-    if (!sample && K <= kSmallK) return (size_t)(L * (K + 1) + K * L + K * kEThreads) * sizeof(float);
-    return (size_t)2 * K * L * sizeof(float);
+    if (!sample && K <= kSmallK) return (size_t)(L * (K + 1) + K * L + K * kFastThreads) * sizeof(float);
+    return (size_t)(2 * K * L + (sample ? 16 * kEThreads : 0)) * sizeof(float);
 }
 }  // namespace
 
@@ -505,12 +550,13 @@ int estep_grid(bool sample, int K, int L, long V) {
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t smem = estep_smem(sample, K, L);
     const void *fn = sample ? (const void *)estep_kernel<true>
-                            : (K <= kSmallK ? (const void *)estep_em_fast_kernel
+                            : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads>
                                             : (const void *)estep_kernel<false>);
+    const int tpb = (!sample && K <= kSmallK) ? kFastThreads : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kEThreads, smem));
+    BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tpb, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
-    const long need = (V + kEThreads - 1) / kEThreads;
+    const long need = (V + tpb - 1) / tpb;
     long g = (long)sms * per_sm;
     if (need < g) g = need < 1 ? 1 : need;
     return (int)g;
@@ -521,7 +567,7 @@ void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s) {
     if (sample)
         count_launch(), estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
     else if (a.K <= kSmallK)
-        count_launch(), estep_em_fast_kernel<<<grid, kEThreads, smem, s>>>(a);
+        count_launch(), estep_em_fast_kernel<kFastThreads><<<grid, kFastThreads, smem, s>>>(a);
     else
         count_launch(), estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
     BINDER_CUDA(cudaGetLastError());
