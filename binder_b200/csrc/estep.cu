@@ -93,6 +93,9 @@ __device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int com
     return comp == 0 ? (float)(i / yz) : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
 }
 
+// row pitch (floats) of the transposed theta table: >= K and 9 banks apart row to row
+__host__ __device__ constexpr int theta_pitch(int K) { return K + ((9 - K % 32) + 32) % 32; }
+
 constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
 constexpr int kFastThreads = 256;
 
@@ -102,23 +105,28 @@ constexpr int kFastThreads = 256;
 // atomic), while the smallest and largest bin touched are tracked; once the normaliser S is known
 // the columns in [kmin, kmax] that hold mass are flushed as hist[k][u] += hk[k] / S -- one shared
 // atomic per distinct bin instead of one per neighbour (the bin range of a 4x4x4 neighbourhood is
-// a handful of bins in smooth images).  theta is staged transposed (thT[u][k]) so lanes that share
-// a fixed-image bin read consecutive banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
+// a handful of bins in smooth images).  The CTA histogram is 32-bit fixed point (scale a.hscale,
+// chosen by the host so that a cell cannot overflow: each voxel adds at most 1 to a cell), which
+// makes every flush a native integer shared atomic, and is converted to FP32 once per CTA.  Each
+// contribution is rounded to within 0.5 / hscale (4e-6 at 2^17); FP32 accumulation of the same
+// sums would round each addition relative to the running sum instead.  theta is staged
+// transposed (thT[u][k]) with a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ
+// by small amounts read different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
 // host).
 template <int TPB>
 __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
-    const int KP = K + 1;       // padded row: lanes with different u_i spread over banks
-    float *thT = sm;            // [L][K + 1]
-    float *hs = sm + L * KP;    // [K][L] CTA histogram
-    float *hk = hs + KL;        // [K][TPB] per-thread bin masses
+    const int KP = theta_pitch(K);
+    float *thT = sm;                                             // [L][KP]
+    unsigned *hs = reinterpret_cast<unsigned *>(sm + L * KP);    // [K][L] CTA histogram (fixed)
+    float *hk = sm + L * KP + KL;                                // [K][TPB] per-thread bin masses
     __shared__ double red[32];
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L, l = q - k * L;
         thT[l * KP + k] = a.theta[q];
-        hs[q] = 0.0f;
+        hs[q] = 0u;
     }
     for (int q = threadIdx.x; q < K * TPB; q += TPB) hk[q] = 0.0f;
     __syncthreads();
@@ -183,11 +191,12 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
             }
         const bool ok = S > 0.0f;
         const float inv = ok ? 1.0f / S : 0.0f;
-        float *hcol = hs + ui;  // hcol[k * L]
+        const float invs = inv * a.hscale;
+        unsigned *hcol = hs + ui;  // hcol[k * L]
         for (int k = kmin; k <= kmax; ++k) {
             const float m = my[k * TPB];
             if (m != 0.0f) {
-                if (ok) atomicAdd(&hcol[k * L], m * inv);
+                if (ok) atomicAdd(&hcol[k * L], __float2uint_rn(m * invs));
                 my[k * TPB] = 0.0f;
             }
         }
@@ -203,8 +212,8 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
     }
     __syncthreads();
     for (int q = threadIdx.x; q < KL; q += TPB) {
-        const float v = hs[q];
-        if (v != 0.0f) atomicAdd(&a.hist[q], v);
+        const unsigned v = hs[q];
+        if (v) atomicAdd(&a.hist[q], (float)v * a.hinv);
     }
     const double m = block_sum(mll, red);
     if (threadIdx.x == 0) atomicAdd(&a.st->mll, m);
@@ -539,7 +548,7 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 
 namespace {
 size_t estep_smem(bool sample, int K, int L) {
-    if (!sample && K <= kSmallK) return (size_t)(L * (K + 1) + K * L + K * kFastThreads) * sizeof(float);
+    if (!sample && K <= kSmallK) return (size_t)(L * theta_pitch(K) + K * L + K * kFastThreads) * sizeof(float);
     return (size_t)(2 * K * L + (sample ? 16 * kEThreads : 0)) * sizeof(float);
 }
 }  // namespace
@@ -562,8 +571,18 @@ int estep_grid(bool sample, int K, int L, long V) {
     return (int)g;
 }
 
-void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s) {
-    const size_t smem = estep_smem(sample, a.K, a.L);
+void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) {
+    const size_t smem = estep_smem(sample, args.K, args.L);
+    EStepArgs a = args;
+    // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
+    // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a
+    // cell, fit in 32 bits
+    const long per_cta = ((a.V + (long)grid * kFastThreads - 1) / ((long)grid * kFastThreads)) *
+                         kFastThreads;
+    int e = 30;
+    while (e > 0 && (double)per_cta * (std::ldexp(1.0, e) + 1.0) >= 4294967295.0) --e;
+    a.hscale = (float)std::ldexp(1.0, e);
+    a.hinv = (float)std::ldexp(1.0, -e);
     if (sample)
         count_launch(), estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
     else if (a.K <= kSmallK)

@@ -23,6 +23,8 @@ struct EStepArgs {
     int K, L;
     uint64_t seed;
     uint32_t chain;
+    // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
+    float hscale, hinv;
 };
 
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
