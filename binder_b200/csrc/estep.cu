@@ -93,11 +93,64 @@ __device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int com
     return comp == 0 ? (float)(i / yz) : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
 }
 
-// row pitch (floats) of the transposed theta table: >= K and 9 banks apart row to row
+// row pitch (floats) of the shared theta / histogram tables: >= n and 9 banks apart row to row
 __host__ __device__ constexpr int theta_pitch(int K) { return K + ((9 - K % 32) + 32) % 32; }
 
 constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
 constexpr int kFastThreads = 256;
+
+// The 64-node pass of one EM voxel: weights w = bx[p] by[q] bz[c] theta[k] added to the
+// thread's private bin column col[k * TPB], their sum S, their first moments along each axis
+// (node offset -1 .. 2 times w) and the range of bins touched.  theta and the column are disjoint
+// regions of shared memory; the __restrict__ qualifiers let the compiler hoist the theta loads of
+// later nodes above earlier column updates.  Products and sums run on paired FP32 lanes (nodes
+// c = 0,1 and c = 2,3 of each packed word).
+template <int TPB>
+__device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
+                                              float *__restrict__ col, const uint32_t (&pk)[16],
+                                              const float (&bx)[4], const float (&by)[4],
+                                              const float (&bz)[4], float &S, float &Sx, float &Sy,
+                                              float &Sz, int &kmin, int &kmax) {
+    const float2 bz01 = make_float2(bz[0], bz[1]), bz23 = make_float2(bz[2], bz[3]);
+    const float2 m1 = make_float2(-1.0f, -1.0f), p2 = make_float2(2.0f, 2.0f);
+    float2 a01 = make_float2(0.f, 0.f), a23 = a01;  // sum of w
+    float2 x01 = a01, x23 = a01;                    // sum of (p - 1) w
+    float2 y01 = a01, y23 = a01;                    // sum of (q - 1) w
+    int lo = 255, hi = 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float bxy = bx[p] * by[q];
+            const float2 bb = make_float2(bxy, bxy);
+            const float2 b01 = __fmul2_rn(bb, bz01), b23 = __fmul2_rn(bb, bz23);
+            const uint32_t word = pk[p * 4 + q];
+            const int k0 = word & 0xff, k1 = (word >> 8) & 0xff, k2 = (word >> 16) & 0xff,
+                      k3 = word >> 24;
+            const float2 w01 = __fmul2_rn(b01, make_float2(thu[k0], thu[k1]));
+            const float2 w23 = __fmul2_rn(b23, make_float2(thu[k2], thu[k3]));
+            col[k0 * TPB] += w01.x;
+            col[k1 * TPB] += w01.y;
+            col[k2 * TPB] += w23.x;
+            col[k3 * TPB] += w23.y;
+            a01 = __fadd2_rn(a01, w01);
+            a23 = __fadd2_rn(a23, w23);
+            if (p == 0) { x01 = __ffma2_rn(m1, w01, x01); x23 = __ffma2_rn(m1, w23, x23); }
+            if (p == 2) { x01 = __fadd2_rn(x01, w01); x23 = __fadd2_rn(x23, w23); }
+            if (p == 3) { x01 = __ffma2_rn(p2, w01, x01); x23 = __ffma2_rn(p2, w23, x23); }
+            if (q == 0) { y01 = __ffma2_rn(m1, w01, y01); y23 = __ffma2_rn(m1, w23, y23); }
+            if (q == 2) { y01 = __fadd2_rn(y01, w01); y23 = __fadd2_rn(y23, w23); }
+            if (q == 3) { y01 = __ffma2_rn(p2, w01, y01); y23 = __ffma2_rn(p2, w23, y23); }
+            lo = min(min(lo, min(k0, k1)), min(k2, k3));
+            hi = max(max(hi, max(k0, k1)), max(k2, k3));
+        }
+    S = (a01.x + a01.y) + (a23.x + a23.y);
+    Sx = (x01.x + x01.y) + (x23.x + x23.y);
+    Sy = (y01.x + y01.y) + (y23.x + y23.y);
+    Sz = (a23.x - a01.x) + 2.0f * a23.y;  // offsets -1, 0, 1, 2 along z
+    kmin = lo;
+    kmax = hi;
+}
 
 // EM E-step for K <= 64 (BINDER/src/cpu/Registration.cpp:219-330, sample == false), one pass over
 // the 64 neighbours.  The posterior mass of a voxel is collected per moving bin k in a private
@@ -110,23 +163,23 @@ constexpr int kFastThreads = 256;
 // makes every flush a native integer shared atomic, and is converted to FP32 once per CTA.  Each
 // contribution is rounded to within 0.5 / hscale (4e-6 at 2^17); FP32 accumulation of the same
 // sums would round each addition relative to the running sum instead.  theta is staged
-// transposed (thT[u][k]) with a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ
-// by small amounts read different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
+// transposed (thT[u][k]); it and the histogram use a row pitch of 9 (mod 32) banks, so lanes
+// whose (u, k) pairs differ by small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
 // host).
 template <int TPB>
 __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
-    const int KP = theta_pitch(K);
+    const int KP = theta_pitch(K), LP = theta_pitch(L);
     float *thT = sm;                                             // [L][KP]
-    unsigned *hs = reinterpret_cast<unsigned *>(sm + L * KP);    // [K][L] CTA histogram (fixed)
-    float *hk = sm + L * KP + KL;                                // [K][TPB] per-thread bin masses
+    unsigned *hs = reinterpret_cast<unsigned *>(sm + L * KP);    // [K][LP] CTA histogram (fixed)
+    float *hk = sm + L * KP + K * LP;                            // [K][TPB] per-thread bin masses
     __shared__ double red[32];
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L, l = q - k * L;
         thT[l * KP + k] = a.theta[q];
-        hs[q] = 0u;
+        hs[k * LP + l] = 0u;
     }
     for (int q = threadIdx.x; q < K * TPB; q += TPB) hk[q] = 0.0f;
     __syncthreads();
@@ -164,39 +217,17 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
         uint32_t pk[16];
         gather_bins(a, ix, iy, iz, pk);
         const int ui = a.u[i];
-        const float *thu = thT + ui * KP;
-        float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
-        int kmin = 255, kmax = 0;
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float bxy = bx[p] * by[q];
-                const uint32_t word = pk[p * 4 + q];
-                float rs = 0.0f, rz = 0.0f;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const int k = (word >> (8 * c)) & 0xff;
-                    const float w = (bxy * bz[c]) * thu[k];
-                    rs += w;
-                    rz = fmaf((float)(c - 1), w, rz);
-                    my[k * TPB] += w;
-                    kmin = min(kmin, k);
-                    kmax = max(kmax, k);
-                }
-                S += rs;
-                Sx = fmaf((float)(p - 1), rs, Sx);
-                Sy = fmaf((float)(q - 1), rs, Sy);
-                Sz += rz;
-            }
+        float S, Sx, Sy, Sz;
+        int kmin, kmax;
+        em_accumulate<TPB>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin, kmax);
         const bool ok = S > 0.0f;
         const float inv = ok ? 1.0f / S : 0.0f;
         const float invs = inv * a.hscale;
-        unsigned *hcol = hs + ui;  // hcol[k * L]
+        unsigned *hcol = hs + ui;  // hcol[k * LP]
         for (int k = kmin; k <= kmax; ++k) {
             const float m = my[k * TPB];
             if (m != 0.0f) {
-                if (ok) atomicAdd(&hcol[k * L], __float2uint_rn(m * invs));
+                if (ok) atomicAdd(&hcol[k * LP], __float2uint_rn(m * invs));
                 my[k * TPB] = 0.0f;
             }
         }
@@ -212,7 +243,8 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
     }
     __syncthreads();
     for (int q = threadIdx.x; q < KL; q += TPB) {
-        const unsigned v = hs[q];
+        const int k = q / L;
+        const unsigned v = hs[k * LP + (q - k * L)];
         if (v) atomicAdd(&a.hist[q], (float)v * a.hinv);
     }
     const double m = block_sum(mll, red);
@@ -548,7 +580,8 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 
 namespace {
 size_t estep_smem(bool sample, int K, int L) {
-    if (!sample && K <= kSmallK) return (size_t)(L * theta_pitch(K) + K * L + K * kFastThreads) * sizeof(float);
+    if (!sample && K <= kSmallK)
+        return (size_t)(L * theta_pitch(K) + K * theta_pitch(L) + K * kFastThreads) * sizeof(float);
     return (size_t)(2 * K * L + (sample ? 16 * kEThreads : 0)) * sizeof(float);
 }
 }  // namespace
