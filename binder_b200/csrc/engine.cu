@@ -7,21 +7,20 @@
 #include <cstring>
 
 #include "engine.cuh"
+#include "layout.cuh"
 
 namespace binder {
 
 namespace {
 
+// device buffers come from the stream-ordered pool (layout.cuh)
 template <typename T>
-T *dalloc(size_t n) {
-    T *p = nullptr;
-    if (n) BINDER_CUDA(cudaMalloc(&p, n * sizeof(T)));
-    return p;
+T *dalloc(size_t n, cudaStream_t s) {
+    return dev_alloc_n<T>(n, s);
 }
 template <typename T>
-void dfree(T *&p) {
-    if (p) cudaFree(p);
-    p = nullptr;
+void dfree(T *&p, cudaStream_t s) {
+    dev_free_p(p, s);
 }
 
 bool verbose() {
@@ -69,26 +68,25 @@ void replay(const Graph &graph, long long kernels, cudaStream_t s) {
     count_launch(kernels);
 }
 
+GridDims dims_of(int nx, int ny, int nz) { return GridDims{nx, ny, nz}; }
+
 }  // namespace
+
+void EmGraphCache::clear() {
+    if (e) cudaGraphExecDestroy(e);
+    if (g) cudaGraphDestroy(g);
+    e = nullptr;
+    g = nullptr;
+    kernels = 0;
+}
 
 long long &launch_counter() {
     static long long counter = 0;
     return counter;
 }
 
-void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa) {
-    soa.resize((size_t)V * N);
-    for (long i = 0; i < V; ++i)
-        for (int n = 0; n < N; ++n) soa[(size_t)n * V + i] = aos[i * N + n];
-}
-
-void soa_to_aos(const float *soa, long V, int N, float *aos) {
-    for (long i = 0; i < V; ++i)
-        for (int n = 0; n < N; ++n) aos[i * N + n] = soa[(size_t)n * V + i];
-}
-
 // ------------------------------------------------------------------------------------------
-void DctSet::init(int nx, int ny, int nz) {
+void DctSet::init(int nx, int ny, int nz, cudaStream_t s) {
     const int dims[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
         const int m = dims[a];
@@ -101,33 +99,36 @@ void DctSet::init(int nx, int ny, int nz) {
                 F[(size_t)k * m + j] = (float)C[(size_t)k * m + j];
                 I[(size_t)j * m + k] = (float)C[(size_t)k * m + j];
             }
-        fwd[a] = dalloc<float>((size_t)m * m);
-        inv[a] = dalloc<float>((size_t)m * m);
+        fwd[a] = dalloc<float>((size_t)m * m, s);
+        inv[a] = dalloc<float>((size_t)m * m, s);
         std::vector<double> CT((size_t)m * m);
         for (int k = 0; k < m; ++k)
             for (int j = 0; j < m; ++j) CT[(size_t)j * m + k] = C[(size_t)k * m + j];
-        ufwd[a].init(C.data(), m);
-        uinv[a].init(CT.data(), m);
-        BINDER_CUDA(cudaMemcpy(fwd[a], F.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
-        BINDER_CUDA(cudaMemcpy(inv[a], I.data(), sizeof(float) * m * m, cudaMemcpyHostToDevice));
+        ufwd[a].init(C.data(), m, s);
+        uinv[a].init(CT.data(), m, s);
+        BINDER_CUDA(cudaMemcpyAsync(fwd[a], F.data(), sizeof(float) * m * m,
+                                    cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemcpyAsync(inv[a], I.data(), sizeof(float) * m * m,
+                                    cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaStreamSynchronize(s));  // F and I go out of scope
     }
 }
 
-void DctSet::release() {
+void DctSet::release(cudaStream_t s) {
     for (int a = 0; a < 3; ++a) {
-        dfree(fwd[a]);
-        dfree(inv[a]);
-        ufwd[a].release();
-        uinv[a].release();
+        dfree(fwd[a], s);
+        dfree(inv[a], s);
+        ufwd[a].release(s);
+        uinv[a].release(s);
     }
 }
 
-void MStep::init(int x, int y, int z) {
+void MStep::init(int x, int y, int z, cudaStream_t s) {
     nx = x; ny = y; nz = z;
     V = (long)x * y * z;
-    dct.init(x, y, z);
-    t1 = dalloc<float>((size_t)V * 3);
-    t2 = dalloc<float>((size_t)V * 3);
+    dct.init(x, y, z, s);
+    t1 = dalloc<float>((size_t)V * 3, s);
+    t2 = dalloc<float>((size_t)V * 3, s);
     precision = default_precision();
 }
 
@@ -137,10 +138,10 @@ int default_precision() {
     return kPrecTF32x3;
 }
 
-void MStep::release() {
-    dct.release();
-    dfree(t1);
-    dfree(t2);
+void MStep::release(cudaStream_t s) {
+    dct.release(s);
+    dfree(t1, s);
+    dfree(t2, s);
 }
 
 void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
@@ -213,39 +214,51 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
     nzv_ = non_zero_voxels;
     BINDER_CUDA(cudaStreamCreate(&own_stream_));
     stream_ = own_stream_;
-    d_ = dalloc<float>((size_t)V_ * 3);
-    r_ = dalloc<float>((size_t)V_ * 3);
-    st_ = dalloc<DevState>(1);
-    BINDER_CUDA(cudaMemset(st_, 0, sizeof(DevState)));
-    std::vector<float> soa;
-    aos_to_soa(final_locations, V_, 3, soa);
-    BINDER_CUDA(cudaMemcpy(d_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    const cudaStream_t s = own_stream_;
+    const GridDims g = dims_of(nx, ny, nz);
+    d_ = dalloc<float>((size_t)V_ * 3, s);
+    r_ = dalloc<float>((size_t)V_ * 3, s);
+    d0_ = dalloc<float>((size_t)V_ * 3, s);
+    st_ = dalloc<DevState>(1, s);
+    BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
+    // the caller's AoS arrays go to the device as they are (r_ is the staging buffer) and are
+    // rearranged there
+    BINDER_CUDA(cudaMemcpyAsync(r_, final_locations, sizeof(float) * V_ * 3,
+                                cudaMemcpyHostToDevice, s));
+    launch_aos_to_soa(r_, d_, V_, s);
+    BINDER_CUDA(cudaMemcpyAsync(d0_, d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice, s));
     // the identity voxel grid (the common case) is recomputed in the kernels instead of read
-    bool identity = true;
-    for (long i = 0; i < V_ && identity; ++i) {
-        const float e[3] = {(float)(i / ((long)ny * nz)), (float)((i / nz) % ny), (float)(i % nz)};
-        for (int n = 0; n < 3; ++n) identity &= (voxel_pos[i * 3 + n] == e[n]);
+    if (voxel_pos != final_locations)
+        BINDER_CUDA(cudaMemcpyAsync(r_, voxel_pos, sizeof(float) * V_ * 3,
+                                    cudaMemcpyHostToDevice, s));
+    launch_identity_check(r_, g, &st_->flags, s);
+    unsigned mismatch = 0;
+    BINDER_CUDA(cudaMemcpyAsync(&mismatch, &st_->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    if (mismatch) {
+        x_ = dalloc<float>((size_t)V_ * 3, s);
+        launch_aos_to_soa(r_, x_, V_, s);
     }
-    if (!identity) {
-        aos_to_soa(voxel_pos, V_, 3, soa);
-        x_ = dalloc<float>((size_t)V_ * 3);
-        BINDER_CUDA(cudaMemcpy(x_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
-    }
-    d0_ = dalloc<float>((size_t)V_ * 3);
-    BINDER_CUDA(cudaMemcpy(d0_, d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice));
-    std::vector<float> zeros((size_t)V_ * 3, 0.0f);
-    set_dream_locations(zeros.data());
-    mstep_.init(nx, ny, nz);
+    BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
+    // dream locations start at zero: r = 0 - x
+    launch_aos_minus_to_soa(nullptr, x_, g, r_, s);
+    mstep_.init(nx, ny, nz, s);
+    BINDER_CUDA(cudaStreamSynchronize(s));
 }
 
 Registration::~Registration() {
-    cudaDeviceSynchronize();
-    if (own_stream_) cudaStreamDestroy(own_stream_);
-    dfree(d_); dfree(x_); dfree(r_); dfree(D_); dfree(theta_); dfree(hist_); dfree(hcnt_);
-    dfree(u_); dfree(vpad_); dfree(mean_); dfree(m2_); dfree(stats_); dfree(st_);
-    dfree(d0_); dfree(theta0_);
+    // nothing of this object may still run when its buffers go back to the pool
+    if (stream_ != own_stream_) cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(own_stream_);
+    em_graph_.clear();
+    const cudaStream_t s = own_stream_;
+    dfree(d_, s); dfree(x_, s); dfree(r_, s); dfree(D_, s); dfree(theta_, s); dfree(hist_, s);
+    dfree(hcnt_, s); dfree(u_, s); dfree(vpad_, s); dfree(mean_, s); dfree(m2_, s);
+    dfree(stats_, s); dfree(st_, s); dfree(d0_, s); dfree(theta0_, s);
     delete topo_;
-    mstep_.release();
+    mstep_.release(s);
+    cudaStreamSynchronize(s);  // the frees complete, so the next object can reuse the memory
+    cudaStreamDestroy(s);
 }
 
 void Registration::set_mi_likelihood(double alpha, const float *theta, int K, int L,
@@ -253,43 +266,50 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     BINDER_CHECK(K >= 1 && K <= 256 && L >= 1 && L <= 256,
                  "numbers of bins K and L must be in [1, 256]");
     BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
-    std::vector<uint8_t> u((size_t)V_);
-    for (long i = 0; i < V_; ++i) {
-        const int b = binned_voxels[i];
-        if (b < 0 || b >= L)
-            throw Error(kInvalidArgument, "binned_voxels value " + std::to_string(b) +
-                                              " outside [0, L) at voxel " + std::to_string(i));
-        u[i] = (uint8_t)b;
-    }
+    BINDER_CUDA(cudaStreamSynchronize(stream_));  // buffers below may be in use
+    em_graph_.clear();
+    const cudaStream_t s = own_stream_;
     P_ = 8;
     PZ_ = 8;
     pyn_ = nyn_ + 2 * P_;
     zp_ = ((nzn_ + 2 * PZ_ + 3) / 4) * 4 + 4;
     const size_t padded = (size_t)(nxn_ + 2 * P_) * pyn_ * zp_;
-    std::vector<uint8_t> vp(padded, 0);
-    for (int x = 0; x < nxn_; ++x)
-        for (int y = 0; y < nyn_; ++y)
-            for (int z = 0; z < nzn_; ++z) {
-                const long j = ((long)x * nyn_ + y) * nzn_ + z;
-                const int b = binned_nodes[j];
-                if (b < 0 || b >= K)
-                    throw Error(kInvalidArgument, "binned_nodes value " + std::to_string(b) +
-                                                      " outside [0, K) at node " + std::to_string(j));
-                vp[((size_t)(x + P_) * pyn_ + (y + P_)) * zp_ + (z + PZ_)] = (uint8_t)b;
-            }
-    dfree(u_); dfree(vpad_); dfree(theta_); dfree(hist_); dfree(hcnt_); dfree(theta0_);
-    u_ = dalloc<uint8_t>((size_t)V_);
-    theta0_ = dalloc<float>((size_t)K * L);
-    vpad_ = dalloc<uint8_t>(padded);
-    theta_ = dalloc<float>((size_t)K * L);
-    hist_ = dalloc<float>((size_t)K * L);
-    hcnt_ = dalloc<unsigned>((size_t)K * L);
-    BINDER_CUDA(cudaMemcpy(u_, u.data(), V_, cudaMemcpyHostToDevice));
-    BINDER_CUDA(cudaMemcpy(vpad_, vp.data(), padded, cudaMemcpyHostToDevice));
-    BINDER_CUDA(cudaMemcpy(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice));
-    BINDER_CUDA(cudaMemcpy(theta0_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice));
-    BINDER_CUDA(cudaMemset(hist_, 0, sizeof(float) * K * L));
-    BINDER_CUDA(cudaMemset(hcnt_, 0, sizeof(unsigned) * K * L));
+    dfree(u_, s); dfree(vpad_, s); dfree(theta_, s); dfree(hist_, s); dfree(hcnt_, s);
+    dfree(theta0_, s);
+    u_ = dalloc<uint8_t>((size_t)V_, s);
+    theta0_ = dalloc<float>((size_t)K * L, s);
+    vpad_ = dalloc<uint8_t>(padded, s);
+    theta_ = dalloc<float>((size_t)K * L, s);
+    hist_ = dalloc<float>((size_t)K * L, s);
+    hcnt_ = dalloc<unsigned>((size_t)K * L, s);
+    // int32 bins to the device as they are, narrowed to bytes (and range-checked) there
+    int *bins = dalloc<int>((size_t)(V_ + Vn_), s);
+    unsigned long long *bad = dalloc<unsigned long long>(2, s);
+    BINDER_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(unsigned long long), s));
+    BINDER_CUDA(cudaMemcpyAsync(bins, binned_voxels, sizeof(int) * V_, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(bins + V_, binned_nodes, sizeof(int) * Vn_,
+                                cudaMemcpyHostToDevice, s));
+    launch_bins_to_u8(bins, V_, L, u_, bad, s);
+    BINDER_CUDA(cudaMemsetAsync(vpad_, 0, padded, s));
+    launch_bins_to_padded(bins + V_, nxn_, nyn_, nzn_, K, vpad_, P_, PZ_, pyn_, zp_, bad + 1, s);
+    BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * K * L, cudaMemcpyDeviceToDevice, s));
+    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K * L, s));
+    BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K * L, s));
+    unsigned long long hbad[2];
+    BINDER_CUDA(cudaMemcpyAsync(hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    dfree(bad, s);
+    dfree(bins, s);
+    if (hbad[0] != ~0ull || hbad[1] != ~0ull) {
+        have_mi_ = false;
+        if (hbad[0] != ~0ull)
+            throw Error(kInvalidArgument, "binned_voxels value " +
+                                              std::to_string(binned_voxels[hbad[0]]) +
+                                              " outside [0, L) at voxel " + std::to_string(hbad[0]));
+        throw Error(kInvalidArgument, "binned_nodes value " + std::to_string(binned_nodes[hbad[1]]) +
+                                          " outside [0, K) at node " + std::to_string(hbad[1]));
+    }
     K_ = K;
     L_ = L;
     alpha_ = alpha;
@@ -305,9 +325,12 @@ void Registration::set_nonlinear_transformation(const double gamma[3], const dou
         rho_[n] = rho[n];
         eta_[n] = eta[n];
     }
-    dfree(D_);
-    D_ = dalloc<float>((size_t)V_);
-    BINDER_CUDA(cudaMemcpy(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    em_graph_.clear();
+    dfree(D_, own_stream_);
+    D_ = dalloc<float>((size_t)V_, own_stream_);
+    BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice, own_stream_));
+    BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     sigma2_ = kSigmaCubic2;
     have_tr_ = true;
 }
@@ -319,7 +342,8 @@ void Registration::require_ready() const {
 
 void Registration::reset_state(bool for_sampler) {
     DevState h{};
-    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
     h.mll = h.lp_lik = h.lp_tr = h.raw_reg = 0.0;
     h.mlp_old = 1e100;
     for (int n = 0; n < 3; ++n) h.gamma[n] = gamma0_[n];
@@ -331,7 +355,8 @@ void Registration::reset_state(bool for_sampler) {
     h.flags = 0;
     h.sweep = 0;
     (void)for_sampler;
-    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));  // `h` goes out of scope
 }
 
 void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
@@ -353,28 +378,48 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
     require_ready();
     if (max_iterations <= 0) return 0;
     if (stats_cap_ < max_iterations) {
-        dfree(stats_);
-        stats_ = dalloc<double>((size_t)max_iterations * 4);
+        BINDER_CUDA(cudaStreamSynchronize(stream_));
+        dfree(stats_, own_stream_);
+        stats_ = dalloc<double>((size_t)max_iterations * 4, own_stream_);
         stats_cap_ = max_iterations;
+        BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     }
-    BINDER_CUDA(cudaMemset(stats_, 0, sizeof(double) * 4 * max_iterations));
+    BINDER_CUDA(cudaMemsetAsync(stats_, 0, sizeof(double) * 4 * max_iterations, stream_));
     reset_state(false);
-    BINDER_CUDA(cudaDeviceSynchronize());
 
     cudaEvent_t t0, t1;
     BINDER_CUDA(cudaEventCreate(&t0));
     BINDER_CUDA(cudaEventCreate(&t1));
     const int chunk = max_iterations < 8 ? max_iterations : 8;
-    Graph graph;
-    const long long kernels = capture_graph(stream_, graph, [&] {
-        for (int c = 0; c < chunk; ++c) enqueue_em_iteration(max_iterations, convergence_th, update);
-    });
+    // the captured chunk is kept for the next call with the same parameters and buffers
+    EmGraphCache &gc = em_graph_;
+    if (!gc.e || gc.chunk != chunk || gc.max_iter != max_iterations || gc.update != update ||
+        gc.th != convergence_th || gc.stream != stream_ || gc.stats != stats_) {
+        gc.clear();
+        Graph graph;
+        gc.kernels = capture_graph(stream_, graph, [&] {
+            for (int c = 0; c < chunk; ++c)
+                enqueue_em_iteration(max_iterations, convergence_th, update);
+        });
+        gc.g = graph.g;
+        gc.e = graph.e;
+        graph.g = nullptr;
+        graph.e = nullptr;
+        gc.chunk = chunk;
+        gc.max_iter = max_iterations;
+        gc.update = update;
+        gc.th = convergence_th;
+        gc.stream = stream_;
+        gc.stats = stats_;
+    }
+    const long long kernels = gc.kernels;
 
     BINDER_CUDA(cudaEventRecord(t0, stream_));
     DevState h{};
     int launched = 0;
     while (true) {
-        replay(graph, kernels, stream_);
+        BINDER_CUDA(cudaGraphLaunch(gc.e, stream_));
+        count_launch(kernels);
         launched += chunk;
         BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));
@@ -390,9 +435,11 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
     iters_done_ = h.iter;
     if (debug || verbose()) {
         std::vector<double> s((size_t)h.iter * 4);
-        if (h.iter)
-            BINDER_CUDA(cudaMemcpy(s.data(), stats_, sizeof(double) * 4 * h.iter,
-                                   cudaMemcpyDeviceToHost));
+        if (h.iter) {
+            BINDER_CUDA(cudaMemcpyAsync(s.data(), stats_, sizeof(double) * 4 * h.iter,
+                                        cudaMemcpyDeviceToHost, stream_));
+            BINDER_CUDA(cudaStreamSynchronize(stream_));
+        }
         for (int it = 0; it < h.iter; ++it)
             std::printf("Iteration %d: mll %.8f  prior(theta) %.8f  prior(T) %.8f  mlp %.8f  "
                         "mlp/voxel %.8f\n",
@@ -414,12 +461,15 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
     BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
     seed_ = seed;
-    dfree(mean_);
-    dfree(m2_);
-    mean_ = dalloc<double>((size_t)V_ * 3);
-    m2_ = dalloc<double>((size_t)V_ * 6);
-    BINDER_CUDA(cudaMemset(mean_, 0, sizeof(double) * V_ * 3));
-    BINDER_CUDA(cudaMemset(m2_, 0, sizeof(double) * V_ * 6));
+    em_graph_.clear();
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    if (!mean_) {
+        mean_ = dalloc<double>((size_t)V_ * 3, own_stream_);
+        m2_ = dalloc<double>((size_t)V_ * 6, own_stream_);
+        BINDER_CUDA(cudaStreamSynchronize(own_stream_));
+    }
+    BINDER_CUDA(cudaMemsetAsync(mean_, 0, sizeof(double) * V_ * 3, stream_));
+    BINDER_CUDA(cudaMemsetAsync(m2_, 0, sizeof(double) * V_ * 6, stream_));
     reset_state(true);
     const int total = N_b + N_s;
     if (total > 0) {
@@ -427,7 +477,6 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
         const double rho_p = rho_[0] * rho_[1] * rho_[2];
         const int every = sample_gamma_every < 1 ? 1 : sample_gamma_every;
         const int chunk = total < 16 ? total : 16;
-        BINDER_CUDA(cudaDeviceSynchronize());
         Graph graph;
         const long long kernels = capture_graph(stream_, graph, [&] {
             for (int c = 0; c < chunk; ++c) {
@@ -468,19 +517,19 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
         if (verbose()) std::printf("sampler: %d sweeps in %.3f ms\n", total, ms);
     }
     DevState h{};
-    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
+    BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+    // moments rearranged to AoS on the device, then one transfer each
+    double *mean_aos = dalloc<double>((size_t)V_ * 3, stream_);
+    double *cov_aos = dalloc<double>((size_t)V_ * 9, stream_);
+    launch_moments_to_aos(mean_, m2_, V_, 1.0 / (double)(N_s - 1), mean_aos, cov_aos, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(mean_out, mean_aos, sizeof(double) * V_ * 3,
+                                cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaMemcpyAsync(cov_out, cov_aos, sizeof(double) * V_ * 9,
+                                cudaMemcpyDeviceToHost, stream_));
+    dfree(mean_aos, stream_);
+    dfree(cov_aos, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
     for (int n = 0; n < 3; ++n) gamma0_[n] = h.gamma[n];  // the prior keeps sampled gammas
-    std::vector<double> mean((size_t)V_ * 3), m2((size_t)V_ * 6);
-    BINDER_CUDA(cudaMemcpy(mean.data(), mean_, sizeof(double) * V_ * 3, cudaMemcpyDeviceToHost));
-    BINDER_CUDA(cudaMemcpy(m2.data(), m2_, sizeof(double) * V_ * 6, cudaMemcpyDeviceToHost));
-    const double inv = 1.0 / (double)(N_s - 1);
-    static const int sym[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-    for (long i = 0; i < V_; ++i) {
-        for (int n = 0; n < 3; ++n) mean_out[i * 3 + n] = mean[(size_t)n * V_ + i];
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c)
-                cov_out[i * 9 + r * 3 + c] = m2[(size_t)sym[r][c] * V_ + i] * inv;
-    }
 }
 
 double Registration::profile_stage(int stage, int n) {
@@ -522,6 +571,17 @@ double Registration::profile_stage(int stage, int n) {
 void Registration::set_precision(int p) {
     BINDER_CHECK(p >= 0 && p <= 2, "precision must be 0 (FP32), 1 (3xTF32) or 2 (TF32)");
     mstep_.precision = p;
+    em_graph_.clear();
+}
+
+void Registration::set_stream(cudaStream_t s) {
+    stream_ = s ? s : own_stream_;
+    em_graph_.clear();
+}
+
+void Registration::set_chain(uint32_t c) {
+    chain_ = c;
+    em_graph_.clear();
 }
 
 void PriorTransform::set_precision(int p) {
@@ -545,7 +605,7 @@ TopologyResult Registration::correct_topology(double e1, double e2, int max_oute
                                               const double vs[3]) {
     BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
                  "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
-    if (!topo_) topo_ = new TopologyWorkspace(nx_, ny_, nz_);
+    if (!topo_) topo_ = new TopologyWorkspace(nx_, ny_, nz_, own_stream_);
     topo_->load_float_grid(d_, vs, stream_);
     TopologyResult r = topo_->run(e1, e2, max_outer, max_inner, vs, stream_);
     topo_->store_float_grid(d_, vs, stream_);
@@ -553,52 +613,41 @@ TopologyResult Registration::correct_topology(double e1, double e2, int max_oute
     return r;
 }
 
+// AoS host arrays <-> device state, rearranged on the device with the M-step's scratch t1 (idle
+// between calls) as the staging buffer
 void Registration::get_final_locations(float *out) const {
-    std::vector<float> soa((size_t)V_ * 3);
+    launch_soa_to_aos(d_, mstep_.t1, V_, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+                                stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpy(soa.data(), d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
-    soa_to_aos(soa.data(), V_, 3, out);
 }
 
 void Registration::set_final_locations(const float *in) {
-    std::vector<float> soa;
-    aos_to_soa(in, V_, 3, soa);
-    BINDER_CUDA(cudaMemcpy(d_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * 3, cudaMemcpyHostToDevice,
+                                stream_));
+    launch_aos_to_soa(mstep_.t1, d_, V_, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Registration::get_dream_locations(float *out) const {
-    std::vector<float> r((size_t)V_ * 3), x;
+    launch_soa_to_aos_plus(r_, x_, dims_of(nx_, ny_, nz_), mstep_.t1, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+                                stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpy(r.data(), r_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
-    if (x_) {
-        x.resize((size_t)V_ * 3);
-        BINDER_CUDA(cudaMemcpy(x.data(), x_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
-    }
-    for (long i = 0; i < V_; ++i) {
-        const float e[3] = {(float)(i / ((long)ny_ * nz_)), (float)((i / nz_) % ny_), (float)(i % nz_)};
-        for (int n = 0; n < 3; ++n)
-            out[i * 3 + n] = r[(size_t)n * V_ + i] + (x_ ? x[(size_t)n * V_ + i] : e[n]);
-    }
 }
 
 void Registration::set_dream_locations(const float *in) {
-    std::vector<float> soa((size_t)V_ * 3), x;
-    if (x_) {
-        x.resize((size_t)V_ * 3);
-        BINDER_CUDA(cudaMemcpy(x.data(), x_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
-    }
-    for (long i = 0; i < V_; ++i) {
-        const float e[3] = {(float)(i / ((long)ny_ * nz_)), (float)((i / nz_) % ny_), (float)(i % nz_)};
-        for (int n = 0; n < 3; ++n)
-            soa[(size_t)n * V_ + i] = in[i * 3 + n] - (x_ ? x[(size_t)n * V_ + i] : e[n]);
-    }
-    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * 3, cudaMemcpyHostToDevice,
+                                stream_));
+    launch_aos_minus_to_soa(mstep_.t1, x_, dims_of(nx_, ny_, nz_), r_, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Registration::get_likelihood_parameters(float *out) const {
     if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    BINDER_CUDA(cudaMemcpyAsync(out, theta_, sizeof(float) * K_ * L_, cudaMemcpyDeviceToHost,
+                                stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpy(out, theta_, sizeof(float) * K_ * L_, cudaMemcpyDeviceToHost));
 }
 
 void Registration::get_shape(int out[4]) const {
@@ -607,16 +656,19 @@ void Registration::get_shape(int out[4]) const {
 
 int Registration::get_iteration_stats(double *out, int max_n) const {
     const int n = iters_done_ < max_n ? iters_done_ : max_n;
-    if (n > 0 && stats_)
-        BINDER_CUDA(cudaMemcpy(out, stats_, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+    if (n > 0 && stats_) {
+        BINDER_CUDA(cudaMemcpyAsync(out, stats_, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost,
+                                    stream_));
+        BINDER_CUDA(cudaStreamSynchronize(stream_));
+    }
     return n;
 }
 
 void Registration::get_state(double *gamma_out, double *nu_out, unsigned long long *degenerate,
                              unsigned *flags) const {
     DevState h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
     if (gamma_out)
         for (int n = 0; n < 3; ++n) gamma_out[n] = h.gamma[n];
     if (nu_out) *nu_out = h.nu;
@@ -640,40 +692,46 @@ PriorTransform::PriorTransform(const double gamma[3], const double rho[3], const
     sigma2_ = sigma_spline * sigma_spline;
     BINDER_CUDA(cudaStreamCreate(&own_stream_));
     stream_ = own_stream_;
-    D_ = dalloc<float>((size_t)V_);
-    BINDER_CUDA(cudaMemcpy(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice));
-    r_ = dalloc<float>((size_t)V_ * 3);
-    d_ = dalloc<float>((size_t)V_ * 3);
-    zeros_ = dalloc<float>((size_t)V_ * 3);
-    BINDER_CUDA(cudaMemset(zeros_, 0, sizeof(float) * V_ * 3));
-    st_ = dalloc<DevState>(1);
-    BINDER_CUDA(cudaMemset(st_, 0, sizeof(DevState)));
-    mstep_.init(nx, ny, nz);
+    const cudaStream_t s = own_stream_;
+    D_ = dalloc<float>((size_t)V_, s);
+    BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice, s));
+    r_ = dalloc<float>((size_t)V_ * 3, s);
+    d_ = dalloc<float>((size_t)V_ * 3, s);
+    zeros_ = dalloc<float>((size_t)V_ * 3, s);
+    BINDER_CUDA(cudaMemsetAsync(zeros_, 0, sizeof(float) * V_ * 3, s));
+    st_ = dalloc<DevState>(1, s);
+    BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
+    mstep_.init(nx, ny, nz, s);
+    BINDER_CUDA(cudaStreamSynchronize(s));
 }
 
 PriorTransform::~PriorTransform() {
-    cudaDeviceSynchronize();
-    if (own_stream_) cudaStreamDestroy(own_stream_);
-    dfree(D_); dfree(r_); dfree(d_); dfree(zeros_); dfree(chunk_); dfree(st_);
-    mstep_.release();
+    if (stream_ != own_stream_) cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(own_stream_);
+    const cudaStream_t s = own_stream_;
+    dfree(D_, s); dfree(r_, s); dfree(d_, s); dfree(zeros_, s); dfree(chunk_, s); dfree(st_, s);
+    mstep_.release(s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
 }
 
 // BINDER/src/cpu/NonLinearTransformation.cpp:226-278: voxel positions are zero, so the result
 // is the smoothed field itself
 double PriorTransform::smooth(const float *field, float *out) {
-    std::vector<float> soa;
-    aos_to_soa(field, V_, 3, soa);
-    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * 3,
+                                cudaMemcpyHostToDevice, stream_));
+    launch_aos_to_soa(mstep_.t1, r_, V_, stream_);
     DevState h{};
     for (int n = 0; n < 3; ++n) h.gamma[n] = gamma_[n];
-    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice, stream_));
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 0, 0, 1, seed_, 0,
                    rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
+    launch_soa_to_aos(d_, mstep_.t1, V_, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+                                stream_));
+    BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpy(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost));
-    BINDER_CUDA(cudaMemcpy(soa.data(), d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost));
-    soa_to_aos(soa.data(), V_, 3, out);
     return h.lp_tr;
 }
 
@@ -682,43 +740,44 @@ double PriorTransform::smooth(const float *field, float *out) {
 void PriorTransform::sample(const float *field, int n, float *out) {
     BINDER_CHECK(n >= 0, "number_of_samples must be non-negative");
     if (n == 0) return;
-    std::vector<float> soa;
-    aos_to_soa(field, V_, 3, soa);
-    BINDER_CUDA(cudaMemcpy(r_, soa.data(), sizeof(float) * V_ * 3, cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * 3,
+                                cudaMemcpyHostToDevice, stream_));
+    launch_aos_to_soa(mstep_.t1, r_, V_, stream_);
     DevState h{};
     for (int c = 0; c < 3; ++c) h.gamma[c] = gamma_[c];
     h.sweep = sweep_;
-    BINDER_CUDA(cudaMemcpy(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice));
+    BINDER_CUDA(cudaMemcpyAsync(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice, stream_));
     const int B = n < 64 ? n : 64;
-    dfree(chunk_);
-    chunk_ = dalloc<float>((size_t)B * V_ * 3);
+    dfree(chunk_, own_stream_);
+    chunk_ = dalloc<float>((size_t)B * V_ * 3, own_stream_);
+    BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     const double rho_p = rho_[0] * rho_[1] * rho_[2];
+    // each sample is rearranged to AoS straight into the chunk, which then goes to the caller's
+    // output in one transfer
     auto enqueue = [&](int count) {
         for (int j = 0; j < count; ++j) {
             mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 1, 0, 1, seed_, 0, rho_p, eta2,
                            nullptr, stream_);
-            BINDER_CUDA(cudaMemcpyAsync(chunk_ + (size_t)j * V_ * 3, d_, sizeof(float) * V_ * 3,
-                                        cudaMemcpyDeviceToDevice, stream_));
+            launch_soa_to_aos(d_, chunk_ + (size_t)j * V_ * 3, V_, stream_);
             launch_sweep_advance(st_, 0x7fffffff, stream_);
         }
     };
-    BINDER_CUDA(cudaDeviceSynchronize());
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
     Graph full, tail;
     const long long k_full = capture_graph(stream_, full, [&] { enqueue(B); });
     const int rem = n % B;
     long long k_tail = 0;
     if (rem) k_tail = capture_graph(stream_, tail, [&] { enqueue(rem); });
-    std::vector<float> host((size_t)B * V_ * 3);
     int done = 0;
     while (done < n) {
         const int cnt = (n - done) >= B ? B : rem;
         if (cnt == B) replay(full, k_full, stream_); else replay(tail, k_tail, stream_);
-        BINDER_CUDA(cudaMemcpyAsync(host.data(), chunk_, sizeof(float) * (size_t)cnt * V_ * 3,
-                                    cudaMemcpyDeviceToHost, stream_));
+        BINDER_CUDA(cudaMemcpyAsync(out + (size_t)done * V_ * 3, chunk_,
+                                    sizeof(float) * (size_t)cnt * V_ * 3, cudaMemcpyDeviceToHost,
+                                    stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));
-        for (int j = 0; j < cnt; ++j)
-            soa_to_aos(host.data() + (size_t)j * V_ * 3, V_, 3, out + (size_t)(done + j) * V_ * 3);
         done += cnt;
     }
     sweep_ += n;

@@ -15,8 +15,8 @@ struct DctSet {
     float *fwd[3] = {nullptr, nullptr, nullptr};
     float *inv[3] = {nullptr, nullptr, nullptr};
     UmmaMatrix ufwd[3], uinv[3];  // the same matrices preformatted for the tensor cores
-    void init(int nx, int ny, int nz);
-    void release();
+    void init(int nx, int ny, int nz, cudaStream_t s);
+    void release(cudaStream_t s);
 };
 
 // The DCT-prior M-step of BINDER/src/cpu/NonLinearTransformation.cpp:58-126 on SoA buffers:
@@ -27,11 +27,25 @@ struct MStep {
     DctSet dct;
     float *t1 = nullptr, *t2 = nullptr;
     int precision = kPrecFP32Simt;  // TransformPrecision
-    void init(int nx, int ny, int nz);
-    void release();
+    // buffers from the stream-ordered pool on stream s
+    void init(int nx, int ny, int nz, cudaStream_t s);
+    void release(cudaStream_t s);
     void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
                  double sigma2, int sample, int want_raw, int every, uint64_t seed, uint32_t chain,
                  double rho_p, const double eta2[3], const int *skip, cudaStream_t s);
+};
+
+// A captured chunk of EM iterations, replayed by later EM calls while the parameters it was
+// captured with (and every buffer it names) stay the same; the setters that change either clear it.
+struct EmGraphCache {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    long long kernels = 0;
+    int chunk = 0, max_iter = 0, update = 0;
+    double th = 0.0;
+    cudaStream_t stream = nullptr;
+    const double *stats = nullptr;
+    void clear();
 };
 
 class Registration {
@@ -65,8 +79,8 @@ class Registration {
     int get_iteration_stats(double *out, int max_n) const;  // [n][4]: mll, lp_lik, lp_tr, mlp
     void get_state(double *gamma_out, double *nu_out, unsigned long long *degenerate,
                    unsigned *flags) const;
-    void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
-    void set_chain(uint32_t c) { chain_ = c; }
+    void set_stream(cudaStream_t s);
+    void set_chain(uint32_t c);
     void set_precision(int p);
     double last_elapsed_ms() const { return last_ms_; }
     cudaStream_t stream() const { return stream_; }
@@ -84,7 +98,9 @@ class Registration {
     int nx_, ny_, nz_, nxn_, nyn_, nzn_, N_;
     long V_, Vn_;
     double nzv_;
-    cudaStream_t stream_ = 0, own_stream_ = 0;  // a blocking stream: ordered after legacy-stream copies
+    // own_stream_ owns the buffers (pool allocations and frees); stream_ (own_stream_ unless the
+    // caller set one) carries the copies and kernels
+    cudaStream_t stream_ = 0, own_stream_ = 0;
     uint32_t chain_ = 0;
     // device buffers
     float *d_ = nullptr, *x_ = nullptr, *r_ = nullptr, *D_ = nullptr, *theta_ = nullptr,
@@ -96,6 +112,7 @@ class Registration {
     int stats_cap_ = 0;
     DevState *st_ = nullptr;
     MStep mstep_;
+    EmGraphCache em_graph_;
     // likelihood / prior parameters
     bool have_mi_ = false, have_tr_ = false;
     int K_ = 0, L_ = 0;
@@ -136,8 +153,5 @@ class PriorTransform {
 // default transform precision: BINDER_B200_PRECISION (0 FP32 SIMT, 1 3xTF32, 2 TF32) or 3xTF32
 int default_precision();
 
-// helpers shared with the C-ABI
-void aos_to_soa(const float *aos, long V, int N, std::vector<float> &soa);
-void soa_to_aos(const float *soa, long V, int N, float *aos);
 
 }  // namespace binder

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <vector>
 
+#include "layout.cuh"
 #include "topology.cuh"
 #include "transform.cuh"
 
@@ -341,15 +342,13 @@ int grid_for(long work) {
     return (int)(need < 1 ? 1 : (need < cap ? need : cap));
 }
 
+// device buffer from the stream-ordered pool, released on the stream it was allocated on
 template <typename T>
 struct DBuf {
     T *p = nullptr;
-    explicit DBuf(size_t n) {
-        if (n) BINDER_CUDA(cudaMalloc(&p, n * sizeof(T)));
-    }
-    ~DBuf() {
-        if (p) cudaFree(p);
-    }
+    cudaStream_t s = 0;
+    DBuf(size_t n, cudaStream_t stream) : s(stream) { p = dev_alloc_n<T>(n, s); }
+    ~DBuf() { dev_free(p, s); }
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
 };
@@ -483,12 +482,13 @@ struct TopologyWorkspace::Impl {
     DBuf<Red> red;
     DBuf<unsigned> flags;
     DBuf<double> H[3], cs[3];
-    Impl(int x, int y, int z)
+    Impl(int x, int y, int z, cudaStream_t st)
         : nx(x), ny(y), nz(z), V((long)x * y * z), cells((long)(x - 1) * (y - 1) * (z - 1)),
-          pos(V * 3), grad(V * 9), jc(cells * 8), div(V * 3), t1(V * 3), t2(V * 3), list(cells),
-          sorted(cells), red(1), flags(1),
-          H{DBuf<double>((size_t)x * x), DBuf<double>((size_t)y * y), DBuf<double>((size_t)z * z)},
-          cs{DBuf<double>(x), DBuf<double>(y), DBuf<double>(z)} {
+          pos(V * 3, st), grad(V * 9, st), jc(cells * 8, st), div(V * 3, st), t1(V * 3, st),
+          t2(V * 3, st), list(cells, st), sorted(cells, st), red(1, st), flags(1, st),
+          H{DBuf<double>((size_t)x * x, st), DBuf<double>((size_t)y * y, st),
+            DBuf<double>((size_t)z * z, st)},
+          cs{DBuf<double>(x, st), DBuf<double>(y, st), DBuf<double>(z, st)} {
         const int dims[3] = {x, y, z};
         const double pi = 3.14159265358979323846;
         for (int a = 0; a < 3; ++a) {
@@ -496,16 +496,19 @@ struct TopologyWorkspace::Impl {
             std::vector<double> M((size_t)n * n), c(n);
             hartley_matrix(n, M.data());
             for (int k = 0; k < n; ++k) c[k] = std::cos(2.0 * pi * k / (n * 1.0));
-            BINDER_CUDA(cudaMemcpy(H[a].p, M.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
-            BINDER_CUDA(cudaMemcpy(cs[a].p, c.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+            BINDER_CUDA(cudaMemcpyAsync(H[a].p, M.data(), sizeof(double) * n * n,
+                                        cudaMemcpyHostToDevice, st));
+            BINDER_CUDA(cudaMemcpyAsync(cs[a].p, c.data(), sizeof(double) * n,
+                                        cudaMemcpyHostToDevice, st));
+            BINDER_CUDA(cudaStreamSynchronize(st));  // the host tables go out of scope
         }
     }
 };
 
-TopologyWorkspace::TopologyWorkspace(int nx, int ny, int nz) {
+TopologyWorkspace::TopologyWorkspace(int nx, int ny, int nz, cudaStream_t s) {
     BINDER_CHECK(nx >= 2 && ny >= 2 && nz >= 2, "topology correction needs at least 2 voxels per axis");
     BINDER_CHECK(nx <= 256 && ny <= 256 && nz <= 256, "topology correction supports axes up to 256");
-    impl_ = new Impl(nx, ny, nz);
+    impl_ = new Impl(nx, ny, nz, s);
 }
 TopologyWorkspace::~TopologyWorkspace() { delete impl_; }
 double *TopologyWorkspace::positions() { return impl_->pos.p; }
@@ -623,9 +626,9 @@ TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_o
                                    int max_inner, const double vs[3], int nx, int ny, int nz,
                                    cudaStream_t s) {
     BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
-    TopologyWorkspace ws(nx, ny, nz);
+    TopologyWorkspace ws(nx, ny, nz, s);
     const long V = (long)nx * ny * nz;
-    DBuf<double> aos(V * 3);
+    DBuf<double> aos(V * 3, s);
     BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
     count_launch(), aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, vs[0], vs[1], vs[2], ws.positions());
     BINDER_CUDA(cudaGetLastError());

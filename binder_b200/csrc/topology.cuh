@@ -36,10 +36,11 @@ TopologyResult topology_correct_3d(double *field_aos_host, double e1, double e2,
                                    cudaStream_t s);
 
 // Device buffers of the correction for one grid (positions, gradients, corner Jacobians, Poisson
-// work space), reusable across calls.  Positions are SoA [3][V] in physical units.
+// work space), reusable across calls.  Positions are SoA [3][V] in physical units.  The buffers
+// come from the stream-ordered pool on stream `s`, which must outlive the workspace.
 class TopologyWorkspace {
   public:
-    TopologyWorkspace(int nx, int ny, int nz);
+    TopologyWorkspace(int nx, int ny, int nz, cudaStream_t s);
     ~TopologyWorkspace();
     TopologyWorkspace(const TopologyWorkspace &) = delete;
     TopologyWorkspace &operator=(const TopologyWorkspace &) = delete;

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <vector>
 
+#include "layout.cuh"
 #include "transform.cuh"
 #include "umma.cuh"
 #include "umma_transform.cuh"
@@ -445,7 +446,7 @@ void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-void UmmaMatrix::init(const double *M, int n_) {
+void UmmaMatrix::init(const double *M, int n_, cudaStream_t s) {
     n = n_;
     Npad = ((n + 15) / 16) * 16;
     nkc = (n + kKC - 1) / kKC;
@@ -463,14 +464,13 @@ void UmmaMatrix::init(const double *M, int n_) {
                 host[(size_t)kc * 2 * plane + off] = hi;
                 host[(size_t)kc * 2 * plane + plane + off] = lo;
             }
-    BINDER_CUDA(cudaMalloc(&dev, host.size() * sizeof(float)));
-    BINDER_CUDA(cudaMemcpy(dev, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice));
+    dev = dev_alloc_n<float>(host.size(), s);
+    BINDER_CUDA(cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));  // `host` goes out of scope
 }
 
-void UmmaMatrix::release() {
-    if (dev) cudaFree(dev);
-    dev = nullptr;
-}
+void UmmaMatrix::release(cudaStream_t s) { dev_free_p(dev, s); }
 
 void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const UmmaMatrix *M2,
                          int mode, int ncomp, int planes, cudaStream_t s) {

@@ -5,13 +5,14 @@
 
 namespace binder {
 
-// An n x n transform matrix preformatted for the UMMA B operand: K chunks of 32, each a hi and a
+// An n x n transform matrix preformatted for the UMMA B operand: K chunks of 16, each a hi and a
 // lo TF32 plane in the canonical no-swizzle K-major layout, rows padded to a multiple of 16.
 struct UmmaMatrix {
     int n = 0, Npad = 0, nkc = 0;
     float *dev = nullptr;
-    void init(const double *M, int n);
-    void release();
+    // device copy from the stream-ordered pool on stream s (synchronised before returning)
+    void init(const double *M, int n, cudaStream_t s);
+    void release(cudaStream_t s);
 };
 
 // precision of the DCT passes
