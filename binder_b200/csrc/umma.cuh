@@ -1,5 +1,6 @@
 // Thin inline-PTX wrappers for the sm_100a tensor-core path: tcgen05 UMMA issue, TMEM allocation
-// and loads, mbarriers.  Only single-CTA (cta_group::1) forms; no cluster multicast anywhere.
+// and loads, mbarriers.  Only single-CTA (cta_group::1) forms, each CTA reading its own shared
+// memory and this GPU's global memory.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -160,11 +161,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64
     }
 }
 
-// round-to-nearest (ties away) FP32 -> TF32, the low 13 bits cleared
+// round-to-nearest (ties away from zero) FP32 -> TF32, the low 13 bits cleared: adding half of
+// the dropped range to the sign-magnitude bit pattern carries into the kept mantissa exactly when
+// the dropped part is >= one half.  Inf and NaN pass through unchanged (a NaN must stay a NaN for
+// the non-finite checks downstream).  Integer ALU work (full rate), where cvt.rna.tf32.f32 would
+// occupy the conversion pipe at a quarter of that rate.
 __device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    const uint32_t u = __float_as_uint(x);
+    return (u & 0x7f800000u) == 0x7f800000u ? x : __uint_as_float((u + 0x1000u) & 0xFFFFE000u);
 }
 
 }  // namespace umma

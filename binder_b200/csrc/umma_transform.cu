@@ -212,8 +212,9 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
         for (int kc = 0; kc < a.nkc; ++kc) {
             const uint32_t c = chunk++;
             const int stage = c & 1;
-            if (c >= 2 && !umma::mbar_wait(&mbar[stage], ((c >> 1) - 1) & 1, kWaitLimit))
-                atomicOr(s_err, 1);
+            // one thread waits for the MMAs that last read this stage; the rest wait at the barrier
+            if (tid == 0 && c >= 2 && !umma::mbar_wait(&mbar[stage], ((c >> 1) - 1) & 1, kWaitLimit))
+                *s_err = 1;
             __syncthreads();
             if (*s_err) {
                 umma::cp_async_wait_all();
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
         umma::cp_async_wait_all();  // the trailing (empty) group
         // wait for the whole accumulation
         const uint32_t last = chunk - 1;
-        if (!umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitLimit)) atomicOr(s_err, 1);
+        if (tid == 0 && !umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kWaitLimit)) *s_err = 1;
         __syncthreads();
         umma::fence_after_sync();
     };
