@@ -46,6 +46,72 @@ ALPHA = 2.0
 ESTEP_BYTES_PER_VOXEL = 26.0
 
 
+GIBBS_SHAPE = (96, 96, 96)
+GIBBS_CHAINS = 32
+GIBBS_BURN, GIBBS_SAMPLES = 20, 80  # sweeps per chain in the timed window
+GIBBS_SEED = 1000
+
+
+def run_gibbs(core, rank, chains, dist):
+    """Gibbs sweeps/s: `chains` chains of GIBBS_BURN + GIBBS_SAMPLES sweeps on a 96^3 MI pair
+    (64 bins) after 10 EM iterations, one Registration, Philox chain index = chain number.  The
+    device time of each sampler call (CUDA events on the engine stream) is summed; e2e adds the
+    FP64 mean / covariance read-back of every call."""
+    from binder_b200 import phantoms
+    from binder_b200.replicas import unit_seed
+    from binder_b200.utils import initialize_fourier_domain_smoothing
+    shape = GIBBS_SHAPE
+    V = int(np.prod(shape))
+    pair = phantoms.make_pair(shape, unit_seed(GIBBS_SEED, rank), bins=BINS)
+    grid = phantoms.identity_positions(shape).astype(np.float32)
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
+    g = GAMMA_INIT * V
+    reg = core.Registration(grid, 1, grid, grid, *shape, *shape, 3, float(np.count_nonzero(pair.u)))
+    reg.setNonLinearTransformation(g, g, g, 1, 1, 1, 1, 1, 1, D)
+    reg.setMILikelihood(ALPHA, np.full((BINS, BINS), 1.0 / BINS, np.float32), BINS, BINS, 1,
+                        pair.v, pair.u)
+    reg.EM(10, -1e300, 1, 0)
+    reg.sampler(GIBBS_SEED, 2, 3, 1, 1, 1, 1, 1)  # warm-up
+    barrier(dist)
+    dev_ms = 0.0
+    t0 = time.perf_counter()
+    for c in range(chains):
+        reg.set_chain(c)
+        reg.sampler(unit_seed(GIBBS_SEED, c), GIBBS_BURN, GIBBS_SAMPLES, 1, 1, 1, 1, 1)
+        dev_ms += reg.last_elapsed_ms()
+    wall = time.perf_counter() - t0
+    dev_ms = max_over_ranks(dev_ms, dist)
+    wall = max_over_ranks(wall, dist)
+    world = dist.get_world_size() if dist is not None else 1
+    sweeps = world * chains * (GIBBS_BURN + GIBBS_SAMPLES)
+    cpu = cpu_gibbs(pair, grid, D, g) if rank == 0 else None
+    return {"metric": f"Gibbs sweeps/s (96x96x96 MI pair, 64 bins, {chains} chains x "
+                      f"{GIBBS_BURN + GIBBS_SAMPLES} sweeps, all sampling switches on)",
+            "value": sweeps / (dev_ms / 1e3), "unit": "sweeps/s", "higher_is_better": True,
+            "ms_per_sweep": dev_ms / (chains * (GIBBS_BURN + GIBBS_SAMPLES)),
+            "e2e": {"value": sweeps / wall, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(chains * V * 12 * 8)},
+            "sample_moments": "FP64 Welford, mean [V,3] + covariance [V,3,3] per chain",
+            "cpu_baseline": cpu}
+
+
+def cpu_gibbs(pair, grid, D, g, sweeps=2):
+    """Sweeps/s of the FP64 oracle sampler (OpenMP, all host cores) on the same 96^3 pair."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    pyoracle.set_threads(threads)
+    shape = GIBBS_SHAPE
+    x = grid.astype(np.float64)
+    t0 = time.perf_counter()
+    pyoracle.sampler(x, x, x, pair.u, pair.v, np.full(BINS * BINS, 1.0 / BINS), ALPHA,
+                     D.astype(np.float64), (g, g, g), math.sqrt(9.0 / (8.0 * math.pi)),
+                     (1.0, 1.0, 1.0), (1.0, 1.0, 1.0), shape, shape, BINS, BINS, GIBBS_SEED, 0,
+                     sweeps, 1, 1, 1, 1, 1)
+    t = time.perf_counter() - t0
+    return {"value": sweeps / t, "unit": "sweeps/s", "cores": threads, "kind": "port",
+            "sample": f"{sweeps} sweeps of the 96^3 pair from the identity grid ({t:.2f} s)"}
+
+
 def metric(em_iters):
     return (f"3D registrations/s (160x192x160 MI pair, 64 bins, {em_iters} EM iterations + "
             "topology correction)")
@@ -58,6 +124,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--em-iters", type=int, default=EM_ITERS)
+    p.add_argument("--gibbs-chains", type=int, default=GIBBS_CHAINS)
     return p.parse_args()
 
 
@@ -235,6 +302,10 @@ def run_b200(args, rank, world, local, dist):
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * args.steps / e2e_s
 
+    # Gibbs sampling throughput on the 96^3 pair (every rank runs its own chains)
+    del reg
+    gibbs = run_gibbs(core, rank, args.gibbs_chains, dist)
+
     if rank != 0:
         return None
     peaks = {}
@@ -268,6 +339,7 @@ def run_b200(args, rank, world, local, dist):
                      "em_iteration": (em_ms / args.em_iters) if em_ms else None,
                      "topology_stats": topo_stats},
         "em_iterations_per_s": world * args.em_iters / ((em_ms or 1) / 1e3),
+        "gibbs": gibbs,
         "cpu_baseline": cpu_baseline(inp, args.em_iters),
     }
     return line
@@ -330,7 +402,21 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": value, "unit": "registrations/s", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "registrations/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "gibbs": reference_gibbs()}
+
+
+def reference_gibbs():
+    """Gibbs sweeps/s of the oracle sampler on the 96^3 pair (the --impl reference line)."""
+    from binder_b200 import phantoms
+    from binder_b200.utils import initialize_fourier_domain_smoothing
+    shape = GIBBS_SHAPE
+    pair = phantoms.make_pair(shape, GIBBS_SEED, bins=BINS)
+    grid = phantoms.identity_positions(shape).astype(np.float32)
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
+    cpu = cpu_gibbs(pair, grid, D, GAMMA_INIT * float(np.prod(shape)))
+    return {"metric": "Gibbs sweeps/s (96x96x96 MI pair, 64 bins)", "value": cpu["value"],
+            "unit": "sweeps/s", "cpu_baseline": cpu}
 
 
 def main():
