@@ -86,6 +86,24 @@ def main():
     cost = R.ref_mi_update(2.0, th0.ravel(), hist.ravel(), K, L, th)
     np.savez(os.path.join(HERE, "mi_ref.npz"), hist=hist, alpha=2.0, theta=th.reshape(K, L),
              cost=cost)
+
+    # 2D Jacobian determinant (utils.cpp:10-98): folds, anisotropic pixels
+    shape2 = (13, 17)
+    f2 = np.stack(np.indices(shape2), -1).astype(np.float64) + rng.normal(0, 0.45, shape2 + (2,))
+    vs2 = np.array([1.2, 0.8])
+    J2 = np.zeros(np.prod(shape2))
+    R.ref_jacobian2d(f2.ravel(), *shape2, *vs2, J2)
+    np.savez(os.path.join(HERE, "jacobian2d_ref.npz"), field=f2, shape=shape2, vs=vs2, J=J2)
+
+    # 2D DCT smoothing + prior cost (NonLinearTransformation.cpp with Nz = 1)
+    shape = (14, 23, 1)
+    field = rng.standard_normal(shape[:2] + (2,))
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 2).ravel()
+    gamma = np.array([4.0, 6.0, 0.0])
+    out = np.zeros(field.size)
+    cost = R.ref_smooth_deformation(gamma, one, one, D, *shape, 1.0, 0.0, field.ravel(), out)
+    np.savez(os.path.join(HERE, "smoothing2d_ref.npz"), field=field, D=D, gamma=gamma, sigma=1.0,
+             out=out.reshape(field.shape), cost=cost)
     print("golden fixtures written to", HERE)
 
 

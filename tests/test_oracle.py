@@ -59,6 +59,22 @@ def test_smoothing_matches_reference(oracle):
     assert cost == pytest.approx(float(g["cost"]), rel=1e-12)
 
 
+def test_jacobian2d_bit_exact_vs_reference(oracle):
+    g = golden("jacobian2d_ref.npz")
+    J = oracle.jacobian2d(g["field"], tuple(int(s) for s in g["shape"]), tuple(g["vs"]))
+    assert np.array_equal(J, g["J"])
+    assert (J < 0).sum() > 0
+
+
+def test_smoothing2d_matches_reference(oracle):
+    g = golden("smoothing2d_ref.npz")
+    shape = g["field"].shape[:2] + (1,)
+    zeros = np.zeros_like(g["field"])
+    cost, out = oracle.smooth(g["field"], zeros, g["D"], g["gamma"], float(g["sigma"]), shape)
+    np.testing.assert_allclose(out.reshape(g["out"].shape), g["out"], rtol=0, atol=1e-12)
+    assert cost == pytest.approx(float(g["cost"]), rel=1e-12)
+
+
 def test_dct_is_scipy_ortho(oracle):
     rng = np.random.default_rng(3)
     x = rng.standard_normal((5, 8, 7))
