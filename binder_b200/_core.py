@@ -20,7 +20,8 @@ backend = "b200"
 has_topology_correction = True
 
 __all__ = ["backend", "has_topology_correction", "Registration", "NonLinearTransformation",
-           "topology_correction_3D", "compute_jacobian_determinant_3D", "BinderError"]
+           "topology_correction_3D", "compute_jacobian_determinant_3D",
+           "compute_jacobian_determinant_2D", "BinderError"]
 
 
 def _f32(a, n=None, name="array"):
@@ -64,6 +65,7 @@ class Registration:
                                                int(Ny_n), int(Nz_n), int(spline_order),
                                                float(non_zero_voxels)))
         self._V = V
+        self._N = N
         self._K = self._L = None
 
     def __del__(self):
@@ -98,31 +100,32 @@ class Registration:
 
     def sampler(self, seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
                 sample_likelihood_parameters, sample_transformation_parameters):
-        mean = np.zeros(self._V * 3, np.float64)
-        cov = np.zeros(self._V * 9, np.float64)
+        N = self._N
+        mean = np.zeros(self._V * N, np.float64)
+        cov = np.zeros(self._V * N * N, np.float64)
         check(lib().binder_registration_sampler(
             self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(N_b), int(N_s), int(sample_gamma),
             int(sample_gamma_every), int(sample_posteriors), int(sample_likelihood_parameters),
             int(sample_transformation_parameters), mean, cov))
-        return mean.reshape(*self._shape, 3), cov.reshape(*self._shape, 3, 3)
+        return mean.reshape(*self._shape, N), cov.reshape(*self._shape, N, N)
 
     # -- getters / setters -------------------------------------------------------------------
     def get_final_locations_as_numpy_array(self):
-        out = np.zeros(self._V * 3, np.float32)
+        out = np.zeros(self._V * self._N, np.float32)
         check(lib().binder_registration_get_final_locations(self._h, out))
-        return out.reshape(*self._shape, 3)
+        return out.reshape(*self._shape, self._N)
 
     def get_final_locations(self):
         return self.get_final_locations_as_numpy_array().reshape(-1)
 
     def get_dream_locations(self):
-        out = np.zeros(self._V * 3, np.float32)
+        out = np.zeros(self._V * self._N, np.float32)
         check(lib().binder_registration_get_dream_locations(self._h, out))
         return out
 
     def set_dream_locations(self, dream_locations):
         check(lib().binder_registration_set_dream_locations(
-            self._h, _f32(dream_locations, self._V * 3, "dream_locations")))
+            self._h, _f32(dream_locations, self._V * self._N, "dream_locations")))
 
     def get_likelihood_parameters(self):
         if self._K is None:
@@ -203,6 +206,7 @@ class NonLinearTransformation:
         self._h = C.c_void_p()
         self._shape = (int(Nx_v), int(Ny_v), int(Nz_v))
         self._V = int(np.prod(self._shape))
+        self._N = 2 if int(Nz_v) == 1 else 3
         check(lib().binder_transform_create(
             C.byref(self._h), float(gamma_x), float(gamma_y), float(gamma_z),
             float(voxels_size_x), float(voxels_size_y), float(voxels_size_z), float(nodes_size_x),
@@ -225,18 +229,20 @@ class NonLinearTransformation:
         check(lib().binder_transform_set_precision(self._h, int(precision)))
 
     def smooth_deformation(self, deformation):
-        out = np.zeros(self._V * 3, np.float32)
+        N = self._N
+        out = np.zeros(self._V * N, np.float32)
         cost = C.c_double(0)
         check(lib().binder_transform_smooth_deformation(
-            self._h, _f32(deformation, self._V * 3, "deformation"), out, C.byref(cost)))
-        return cost.value, out.reshape(*self._shape, 3)
+            self._h, _f32(deformation, self._V * N, "deformation"), out, C.byref(cost)))
+        return cost.value, out.reshape(*self._shape, N)
 
     def sampleDeformationField(self, deformationField, number_of_samples):
         n = int(number_of_samples)
-        out = np.zeros(max(n, 0) * self._V * 3, np.float32)
+        N = self._N
+        out = np.zeros(max(n, 0) * self._V * N, np.float32)
         check(lib().binder_transform_sample_deformation_field(
-            self._h, _f32(deformationField, self._V * 3, "deformationField"), n, out))
-        return out.reshape(n, *self._shape, 3)
+            self._h, _f32(deformationField, self._V * N, "deformationField"), n, out))
+        return out.reshape(n, *self._shape, N)
 
 
 class topology_correction_3D:
@@ -274,3 +280,12 @@ def compute_jacobian_determinant_3D(field, Nx, Ny, Nz, voxel_size_x, voxel_size_
                                                int(Nz), float(voxel_size_x), float(voxel_size_y),
                                                float(voxel_size_z), J))
     return J.reshape(int(Nx), int(Ny), int(Nz))
+
+
+def compute_jacobian_determinant_2D(field, Nx, Ny, voxel_size_x, voxel_size_y):
+    """``_core.compute_jacobian_determinant_2D`` (cpu/bindings.cpp:535-560), FP64 on the GPU."""
+    V = int(Nx) * int(Ny)
+    J = np.zeros(V, np.float64)
+    check(lib().binder_jacobian_determinant_2d(_f64(field, V * 2, "field"), int(Nx), int(Ny),
+                                               float(voxel_size_x), float(voxel_size_y), J))
+    return J.reshape(int(Nx), int(Ny))

@@ -35,6 +35,7 @@ EXPORTS = [
     "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
     "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
     "binder_jacobian_determinant_3d_noalloc", "binder_jacobian_noalloc_max_voxels",
+    "binder_jacobian_determinant_2d",
 ]
 
 
@@ -90,6 +91,7 @@ def _declare(lib):
         "binder_transform_sample_deformation_field": [_P, _f32, _i, _f32],
         "binder_transform_get_shape": [_P, _i32],
         "binder_jacobian_determinant_3d": [_f64, _i, _i, _i, _d, _d, _d, _f64],
+        "binder_jacobian_determinant_2d": [_f64, _i, _i, _d, _d, _f64],
         "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],

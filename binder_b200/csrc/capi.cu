@@ -366,6 +366,16 @@ int binder_jacobian_determinant_3d_noalloc(const double *field, int Nx, int Ny, 
 
 long long binder_jacobian_noalloc_max_voxels(void) { return binder::kJacobianNoAllocMaxVoxels; }
 
+int binder_jacobian_determinant_2d(const double *field, int Nx, int Ny, double voxel_size_x,
+                                   double voxel_size_y, double *J_out) {
+    return guard([&] {
+        NEED(field);
+        NEED(J_out);
+        const double vs[2] = {voxel_size_x, voxel_size_y};
+        binder::jacobian2d(field, Nx, Ny, vs, J_out);
+    });
+}
+
 int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
                                int max_it, int threads, const double voxel_sizes[3], int Nx,
                                int Ny, int Nz, double *out, long long *stats_out) {

@@ -68,8 +68,6 @@ void replay(const Graph &graph, long long kernels, cudaStream_t s) {
     count_launch(kernels);
 }
 
-GridDims dims_of(int nx, int ny, int nz) { return GridDims{nx, ny, nz}; }
-
 }  // namespace
 
 void EmGraphCache::clear() {
@@ -91,6 +89,7 @@ void DctSet::init(int nx, int ny, int nz, cudaStream_t s) {
     for (int a = 0; a < 3; ++a) {
         const int m = dims[a];
         n[a] = m;
+        if (m < 2) continue;  // the unit z axis of a 2D image has no transform
         std::vector<double> C((size_t)m * m);
         dct2_matrix(m, C.data());
         std::vector<float> F((size_t)m * m), I((size_t)m * m);
@@ -154,6 +153,9 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     a.skip = skip;
     a.ny = ny;
     a.nz = nz;
+    const bool two_d = nz == 1;
+    const int ncomp = two_d ? 2 : 3;
+    a.dims = ncomp;
     a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
     a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
@@ -162,11 +164,31 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     auto pass = [&](int axis, bool inverse, int mode) {
         if (tc)
             launch_axis_pass_tc(a, inverse ? dct.uinv[axis] : dct.ufwd[axis],
-                                mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, 3, planes,
-                                s);
+                                mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, ncomp,
+                                planes, s);
         else
-            launch_axis_pass(a, mode, 3, s);
+            launch_axis_pass(a, mode, ncomp, s);
     };
+    if (two_d) {
+        // an nx x ny image, components (x, y): forward along y, then x with the prior scaling,
+        // inverse along x, and the inverse along y adds the pixel positions
+        a.in = r; a.out = t1; a.M = dct.fwd[1]; a.n = ny; a.outer = nx; a.s = 1;
+        pass(1, false, kEpiNone);
+        a.in = t1; a.out = t2; a.M = dct.fwd[0]; a.M2 = dct.inv[0]; a.n = nx; a.outer = 1; a.s = ny;
+        const float *yin = t2;
+        if (tc) {
+            pass(0, false, kEpiSpectralOut);
+            a.in = t2; a.out = t1; a.M2 = nullptr;
+            pass(0, true, kEpiNone);
+            yin = t1;
+        } else {
+            pass(0, false, kEpiSpectral);
+        }
+        a.in = yin; a.out = d; a.M = dct.inv[1]; a.M2 = nullptr; a.n = ny; a.outer = nx; a.s = 1;
+        a.xpos = xpos;
+        pass(1, true, kEpiPositions);
+        return;
+    }
     // forward DCT-II along z, y
     a.in = r; a.out = t1; a.M = dct.fwd[2]; a.n = nz; a.outer = (long)nx * ny; a.s = 1;
     pass(2, false, kEpiNone);
@@ -203,41 +225,39 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
     : nx_(nx), ny_(ny), nz_(nz), nxn_(nxn), nyn_(nyn), nzn_(nzn) {
     BINDER_CHECK(nx > 0 && ny > 0 && nz > 0 && nxn > 0 && nyn > 0 && nzn > 0,
                  "grid dimensions must be positive");
-    if (nz == 1)
-        throw Error(kUnsupported, "2D registration (Nz_v == 1) is not built on the GPU path");
     if (spline_order != 3)
         throw Error(kUnsupported, "only cubic B-splines (spline_order = 3) are built");
     BINDER_CHECK((long)nx * ny * nz < (1L << 31), "volume too large");
-    N_ = 3;
+    BINDER_CHECK(nz > 1 || nzn == 1, "a 2D image (Nz_v == 1) needs a 2D node grid (Nz_n == 1)");
+    N_ = nz == 1 ? 2 : 3;  // a 2D image has two displacement components
     V_ = (long)nx * ny * nz;
     Vn_ = (long)nxn * nyn * nzn;
     nzv_ = non_zero_voxels;
     BINDER_CUDA(cudaStreamCreate(&own_stream_));
     stream_ = own_stream_;
     const cudaStream_t s = own_stream_;
-    const GridDims g = dims_of(nx, ny, nz);
-    d_ = dalloc<float>((size_t)V_ * 3, s);
-    r_ = dalloc<float>((size_t)V_ * 3, s);
-    d0_ = dalloc<float>((size_t)V_ * 3, s);
+    const GridDims g = grid_dims();
+    const size_t VN = (size_t)V_ * N_;
+    d_ = dalloc<float>(VN, s);
+    r_ = dalloc<float>(VN, s);
+    d0_ = dalloc<float>(VN, s);
     st_ = dalloc<DevState>(1, s);
     BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
     // the caller's AoS arrays go to the device as they are (r_ is the staging buffer) and are
     // rearranged there
-    BINDER_CUDA(cudaMemcpyAsync(r_, final_locations, sizeof(float) * V_ * 3,
-                                cudaMemcpyHostToDevice, s));
-    launch_aos_to_soa(r_, d_, V_, s);
-    BINDER_CUDA(cudaMemcpyAsync(d0_, d_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(r_, final_locations, sizeof(float) * VN, cudaMemcpyHostToDevice, s));
+    launch_aos_to_soa(r_, d_, V_, N_, s);
+    BINDER_CUDA(cudaMemcpyAsync(d0_, d_, sizeof(float) * VN, cudaMemcpyDeviceToDevice, s));
     // the identity voxel grid (the common case) is recomputed in the kernels instead of read
     if (voxel_pos != final_locations)
-        BINDER_CUDA(cudaMemcpyAsync(r_, voxel_pos, sizeof(float) * V_ * 3,
-                                    cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemcpyAsync(r_, voxel_pos, sizeof(float) * VN, cudaMemcpyHostToDevice, s));
     launch_identity_check(r_, g, &st_->flags, s);
     unsigned mismatch = 0;
     BINDER_CUDA(cudaMemcpyAsync(&mismatch, &st_->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     BINDER_CUDA(cudaStreamSynchronize(s));
     if (mismatch) {
-        x_ = dalloc<float>((size_t)V_ * 3, s);
-        launch_aos_to_soa(r_, x_, V_, s);
+        x_ = dalloc<float>(VN, s);
+        launch_aos_to_soa(r_, x_, V_, N_, s);
     }
     BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
     // dream locations start at zero: r = 0 - x
@@ -269,11 +289,15 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     BINDER_CUDA(cudaStreamSynchronize(stream_));  // buffers below may be in use
     em_graph_.clear();
     const cudaStream_t s = own_stream_;
+    // zero-padded byte volume of the node bins, in the E-step's view (a 2D node grid nxn x nyn
+    // is the volume nxn x 1 x nyn: its y axis is the packed axis and has no padded y rows)
+    const View w = estep_view();
     P_ = 8;
     PZ_ = 8;
-    pyn_ = nyn_ + 2 * P_;
-    zp_ = ((nzn_ + 2 * PZ_ + 3) / 4) * 4 + 4;
-    const size_t padded = (size_t)(nxn_ + 2 * P_) * pyn_ * zp_;
+    const int Py = N_ == 3 ? P_ : 0;
+    pyn_ = w.nyn + 2 * Py;
+    zp_ = ((w.nzn + 2 * PZ_ + 3) / 4) * 4 + 4;
+    const size_t padded = (size_t)(w.nxn + 2 * P_) * pyn_ * zp_;
     dfree(u_, s); dfree(vpad_, s); dfree(theta_, s); dfree(hist_, s); dfree(hcnt_, s);
     dfree(theta0_, s);
     u_ = dalloc<uint8_t>((size_t)V_, s);
@@ -291,7 +315,8 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
                                 cudaMemcpyHostToDevice, s));
     launch_bins_to_u8(bins, V_, L, u_, bad, s);
     BINDER_CUDA(cudaMemsetAsync(vpad_, 0, padded, s));
-    launch_bins_to_padded(bins + V_, nxn_, nyn_, nzn_, K, vpad_, P_, PZ_, pyn_, zp_, bad + 1, s);
+    launch_bins_to_padded(bins + V_, w.nxn, w.nyn, w.nzn, K, vpad_, P_, Py, PZ_, pyn_, zp_, bad + 1,
+                          s);
     BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice, s));
     BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * K * L, cudaMemcpyDeviceToDevice, s));
     BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K * L, s));
@@ -313,8 +338,8 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     K_ = K;
     L_ = L;
     alpha_ = alpha;
-    egrid_e_ = estep_grid(false, K, L, V_);
-    egrid_s_ = estep_grid(true, K, L, V_);
+    egrid_e_ = estep_grid(false, K, L, V_, N_);
+    egrid_s_ = estep_grid(true, K, L, V_, N_);
     have_mi_ = true;
 }
 
@@ -359,14 +384,27 @@ void Registration::reset_state(bool for_sampler) {
     BINDER_CUDA(cudaStreamSynchronize(stream_));  // `h` goes out of scope
 }
 
-void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
+// grid dimensions as the E-step sees them: a 2D image nx x ny (nz = 1) is the volume nx x 1 x ny
+Registration::View Registration::estep_view() const {
+    if (N_ == 3) return View{nx_, ny_, nz_, nxn_, nyn_, nzn_};
+    return View{nx_, 1, ny_, nxn_, 1, nyn_};
+}
+
+GridDims Registration::grid_dims() const { return GridDims{nx_, ny_, nz_, N_}; }
+
+EStepArgs Registration::estep_args(const int *skip) const {
+    const View w = estep_view();
     EStepArgs e{};
     e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_; e.hist = hist_;
-    e.hcnt = hcnt_; e.st = st_; e.skip = &st_->done; e.V = V_;
-    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
-    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
+    e.hcnt = hcnt_; e.st = st_; e.skip = skip; e.V = V_;
+    e.nx = w.nx; e.ny = w.ny; e.nz = w.nz; e.nxn = w.nxn; e.nyn = w.nyn; e.nzn = w.nzn;
+    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
     e.seed = seed_; e.chain = chain_;
-    launch_estep(e, false, egrid_e_, stream_);
+    return e;
+}
+
+void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
+    launch_estep(estep_args(&st_->done), false, egrid_e_, stream_);
     launch_theta_update(theta_, hist_, K_, L_, alpha_, update, st_, stream_);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
@@ -463,13 +501,14 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     seed_ = seed;
     em_graph_.clear();
     BINDER_CUDA(cudaStreamSynchronize(stream_));
+    const int NM2 = N_ * (N_ + 1) / 2;  // upper triangle of the covariance
     if (!mean_) {
-        mean_ = dalloc<double>((size_t)V_ * 3, own_stream_);
-        m2_ = dalloc<double>((size_t)V_ * 6, own_stream_);
+        mean_ = dalloc<double>((size_t)V_ * N_, own_stream_);
+        m2_ = dalloc<double>((size_t)V_ * NM2, own_stream_);
         BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     }
-    BINDER_CUDA(cudaMemsetAsync(mean_, 0, sizeof(double) * V_ * 3, stream_));
-    BINDER_CUDA(cudaMemsetAsync(m2_, 0, sizeof(double) * V_ * 6, stream_));
+    BINDER_CUDA(cudaMemsetAsync(mean_, 0, sizeof(double) * V_ * N_, stream_));
+    BINDER_CUDA(cudaMemsetAsync(m2_, 0, sizeof(double) * V_ * NM2, stream_));
     reset_state(true);
     const int total = N_b + N_s;
     if (total > 0) {
@@ -481,13 +520,7 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
         const long long kernels = capture_graph(stream_, graph, [&] {
             for (int c = 0; c < chunk; ++c) {
                 if (sample_posteriors) {
-                    EStepArgs e{};
-                    e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_;
-                    e.hist = hist_; e.hcnt = hcnt_; e.st = st_; e.skip = &st_->done; e.V = V_;
-                    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
-                    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
-                    e.seed = seed_; e.chain = chain_;
-                    launch_estep(e, true, egrid_s_, stream_);
+                    launch_estep(estep_args(&st_->done), true, egrid_s_, stream_);
                 }
                 if (sample_likelihood_parameters)
                     launch_dirichlet_sample(theta_, hcnt_, K_, L_, alpha_, seed_, chain_, st_,
@@ -499,7 +532,7 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
                         launch_nu_sample(st_, sample_gamma, every, N_, V_, rho_p, eta2, seed_,
                                          chain_, stream_);
                 }
-                launch_sweep_end(d_, mean_, m2_, V_, N_b, total, st_, stream_);
+                launch_sweep_end(d_, mean_, m2_, V_, N_, N_b, total, st_, stream_);
             }
         });
         cudaEvent_t t0, t1;
@@ -519,12 +552,12 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     DevState h{};
     BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
     // moments rearranged to AoS on the device, then one transfer each
-    double *mean_aos = dalloc<double>((size_t)V_ * 3, stream_);
-    double *cov_aos = dalloc<double>((size_t)V_ * 9, stream_);
-    launch_moments_to_aos(mean_, m2_, V_, 1.0 / (double)(N_s - 1), mean_aos, cov_aos, stream_);
-    BINDER_CUDA(cudaMemcpyAsync(mean_out, mean_aos, sizeof(double) * V_ * 3,
+    double *mean_aos = dalloc<double>((size_t)V_ * N_, stream_);
+    double *cov_aos = dalloc<double>((size_t)V_ * N_ * N_, stream_);
+    launch_moments_to_aos(mean_, m2_, V_, N_, 1.0 / (double)(N_s - 1), mean_aos, cov_aos, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(mean_out, mean_aos, sizeof(double) * V_ * N_,
                                 cudaMemcpyDeviceToHost, stream_));
-    BINDER_CUDA(cudaMemcpyAsync(cov_out, cov_aos, sizeof(double) * V_ * 9,
+    BINDER_CUDA(cudaMemcpyAsync(cov_out, cov_aos, sizeof(double) * V_ * N_ * N_,
                                 cudaMemcpyDeviceToHost, stream_));
     dfree(mean_aos, stream_);
     dfree(cov_aos, stream_);
@@ -537,12 +570,7 @@ double Registration::profile_stage(int stage, int n) {
     BINDER_CHECK(stage >= 0 && stage <= 2, "stage must be 0 (E-step), 1 (M-step) or 2 (theta)");
     BINDER_CHECK(n >= 1, "n must be >= 1");
     reset_state(false);
-    EStepArgs e{};
-    e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_; e.hist = hist_;
-    e.hcnt = hcnt_; e.st = st_; e.skip = nullptr; e.V = V_;
-    e.nx = nx_; e.ny = ny_; e.nz = nz_; e.nxn = nxn_; e.nyn = nyn_; e.nzn = nzn_;
-    e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_;
-    e.seed = seed_; e.chain = chain_;
+    const EStepArgs e = estep_args(nullptr);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     auto one = [&] {
         if (stage == 0) launch_estep(e, false, egrid_e_, stream_);
@@ -590,7 +618,7 @@ void PriorTransform::set_precision(int p) {
 }
 
 void Registration::reset() {
-    BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * 3, cudaMemcpyDeviceToDevice, stream_));
+    BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * N_, cudaMemcpyDeviceToDevice, stream_));
     if (have_mi_) {
         BINDER_CUDA(cudaMemcpyAsync(theta_, theta0_, sizeof(float) * K_ * L_,
                                     cudaMemcpyDeviceToDevice, stream_));
@@ -605,6 +633,8 @@ TopologyResult Registration::correct_topology(double e1, double e2, int max_oute
                                               const double vs[3]) {
     BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
                  "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
+    if (N_ == 2)
+        throw Error(kUnsupported, "topology correction of a 2D registration is not built");
     if (!topo_) topo_ = new TopologyWorkspace(nx_, ny_, nz_, own_stream_);
     topo_->load_float_grid(d_, vs, stream_);
     TopologyResult r = topo_->run(e1, e2, max_outer, max_inner, vs, stream_);
@@ -616,30 +646,30 @@ TopologyResult Registration::correct_topology(double e1, double e2, int max_oute
 // AoS host arrays <-> device state, rearranged on the device with the M-step's scratch t1 (idle
 // between calls) as the staging buffer
 void Registration::get_final_locations(float *out) const {
-    launch_soa_to_aos(d_, mstep_.t1, V_, stream_);
-    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+    launch_soa_to_aos(d_, mstep_.t1, V_, N_, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * N_, cudaMemcpyDeviceToHost,
                                 stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Registration::set_final_locations(const float *in) {
-    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * 3, cudaMemcpyHostToDevice,
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * N_, cudaMemcpyHostToDevice,
                                 stream_));
-    launch_aos_to_soa(mstep_.t1, d_, V_, stream_);
+    launch_aos_to_soa(mstep_.t1, d_, V_, N_, stream_);
     BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Registration::get_dream_locations(float *out) const {
-    launch_soa_to_aos_plus(r_, x_, dims_of(nx_, ny_, nz_), mstep_.t1, stream_);
-    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+    launch_soa_to_aos_plus(r_, x_, grid_dims(), mstep_.t1, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * N_, cudaMemcpyDeviceToHost,
                                 stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Registration::set_dream_locations(const float *in) {
-    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * 3, cudaMemcpyHostToDevice,
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, in, sizeof(float) * V_ * N_, cudaMemcpyHostToDevice,
                                 stream_));
-    launch_aos_minus_to_soa(mstep_.t1, x_, dims_of(nx_, ny_, nz_), r_, stream_);
+    launch_aos_minus_to_soa(mstep_.t1, x_, grid_dims(), r_, stream_);
     BINDER_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -681,9 +711,8 @@ PriorTransform::PriorTransform(const double gamma[3], const double rho[3], const
                                const float *D, int nx, int ny, int nz, double sigma_spline)
     : nx_(nx), ny_(ny), nz_(nz) {
     BINDER_CHECK(nx > 0 && ny > 0 && nz > 0, "grid dimensions must be positive");
-    if (nz == 1)
-        throw Error(kUnsupported, "2D prior transformation (Nz_v == 1) is not built on the GPU path");
     V_ = (long)nx * ny * nz;
+    N_ = nz == 1 ? 2 : 3;
     for (int n = 0; n < 3; ++n) {
         gamma_[n] = gamma[n];
         rho_[n] = rho[n];
@@ -695,10 +724,10 @@ PriorTransform::PriorTransform(const double gamma[3], const double rho[3], const
     const cudaStream_t s = own_stream_;
     D_ = dalloc<float>((size_t)V_, s);
     BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice, s));
-    r_ = dalloc<float>((size_t)V_ * 3, s);
-    d_ = dalloc<float>((size_t)V_ * 3, s);
-    zeros_ = dalloc<float>((size_t)V_ * 3, s);
-    BINDER_CUDA(cudaMemsetAsync(zeros_, 0, sizeof(float) * V_ * 3, s));
+    r_ = dalloc<float>((size_t)V_ * N_, s);
+    d_ = dalloc<float>((size_t)V_ * N_, s);
+    zeros_ = dalloc<float>((size_t)V_ * N_, s);
+    BINDER_CUDA(cudaMemsetAsync(zeros_, 0, sizeof(float) * V_ * N_, s));
     st_ = dalloc<DevState>(1, s);
     BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
     mstep_.init(nx, ny, nz, s);
@@ -718,17 +747,17 @@ PriorTransform::~PriorTransform() {
 // BINDER/src/cpu/NonLinearTransformation.cpp:226-278: voxel positions are zero, so the result
 // is the smoothed field itself
 double PriorTransform::smooth(const float *field, float *out) {
-    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * 3,
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * N_,
                                 cudaMemcpyHostToDevice, stream_));
-    launch_aos_to_soa(mstep_.t1, r_, V_, stream_);
+    launch_aos_to_soa(mstep_.t1, r_, V_, N_, stream_);
     DevState h{};
     for (int n = 0; n < 3; ++n) h.gamma[n] = gamma_[n];
     BINDER_CUDA(cudaMemcpyAsync(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice, stream_));
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 0, 0, 1, seed_, 0,
                    rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
-    launch_soa_to_aos(d_, mstep_.t1, V_, stream_);
-    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * 3, cudaMemcpyDeviceToHost,
+    launch_soa_to_aos(d_, mstep_.t1, V_, N_, stream_);
+    BINDER_CUDA(cudaMemcpyAsync(out, mstep_.t1, sizeof(float) * V_ * N_, cudaMemcpyDeviceToHost,
                                 stream_));
     BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
@@ -741,16 +770,16 @@ void PriorTransform::sample(const float *field, int n, float *out) {
     BINDER_CHECK(n >= 0, "number_of_samples must be non-negative");
     if (n == 0) return;
     BINDER_CUDA(cudaStreamSynchronize(stream_));
-    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * 3,
+    BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * N_,
                                 cudaMemcpyHostToDevice, stream_));
-    launch_aos_to_soa(mstep_.t1, r_, V_, stream_);
+    launch_aos_to_soa(mstep_.t1, r_, V_, N_, stream_);
     DevState h{};
     for (int c = 0; c < 3; ++c) h.gamma[c] = gamma_[c];
     h.sweep = sweep_;
     BINDER_CUDA(cudaMemcpyAsync(st_, &h, sizeof(DevState), cudaMemcpyHostToDevice, stream_));
     const int B = n < 64 ? n : 64;
     dfree(chunk_, own_stream_);
-    chunk_ = dalloc<float>((size_t)B * V_ * 3, own_stream_);
+    chunk_ = dalloc<float>((size_t)B * V_ * N_, own_stream_);
     BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     const double rho_p = rho_[0] * rho_[1] * rho_[2];
@@ -760,7 +789,7 @@ void PriorTransform::sample(const float *field, int n, float *out) {
         for (int j = 0; j < count; ++j) {
             mstep_.enqueue(r_, d_, zeros_, D_, st_, sigma2_, 1, 0, 1, seed_, 0, rho_p, eta2,
                            nullptr, stream_);
-            launch_soa_to_aos(d_, chunk_ + (size_t)j * V_ * 3, V_, stream_);
+            launch_soa_to_aos(d_, chunk_ + (size_t)j * V_ * N_, V_, N_, stream_);
             launch_sweep_advance(st_, 0x7fffffff, stream_);
         }
     };
@@ -774,8 +803,8 @@ void PriorTransform::sample(const float *field, int n, float *out) {
     while (done < n) {
         const int cnt = (n - done) >= B ? B : rem;
         if (cnt == B) replay(full, k_full, stream_); else replay(tail, k_tail, stream_);
-        BINDER_CUDA(cudaMemcpyAsync(out + (size_t)done * V_ * 3, chunk_,
-                                    sizeof(float) * (size_t)cnt * V_ * 3, cudaMemcpyDeviceToHost,
+        BINDER_CUDA(cudaMemcpyAsync(out + (size_t)done * V_ * N_, chunk_,
+                                    sizeof(float) * (size_t)cnt * V_ * N_, cudaMemcpyDeviceToHost,
                                     stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));
         done += cnt;
@@ -784,7 +813,7 @@ void PriorTransform::sample(const float *field, int n, float *out) {
 }
 
 void PriorTransform::get_shape(int out[4]) const {
-    out[0] = nx_; out[1] = ny_; out[2] = nz_; out[3] = 3;
+    out[0] = nx_; out[1] = ny_; out[2] = nz_; out[3] = N_;
 }
 
 }  // namespace binder

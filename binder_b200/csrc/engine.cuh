@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "estep.cuh"
+#include "layout.cuh"
 #include "topology.cuh"
 #include "umma_transform.cuh"
 
@@ -91,6 +92,13 @@ class Registration {
     int L() const { return L_; }
 
   private:
+    // grid dimensions as the E-step sees them (a 2D image nx x ny is the volume nx x 1 x ny)
+    struct View {
+        int nx, ny, nz, nxn, nyn, nzn;
+    };
+    View estep_view() const;
+    GridDims grid_dims() const;
+    EStepArgs estep_args(const int *skip) const;
     void enqueue_em_iteration(int max_iter, double th, int update);
     void reset_state(bool for_sampler);
     void require_ready() const;
@@ -141,6 +149,7 @@ class PriorTransform {
   private:
     int nx_, ny_, nz_;
     long V_;
+    int N_ = 3;  // displacement components (2 for an image)
     double gamma_[3], rho_[3], eta_[3], sigma2_;
     float *D_ = nullptr, *r_ = nullptr, *d_ = nullptr, *zeros_ = nullptr, *chunk_ = nullptr;
     DevState *st_ = nullptr;

@@ -21,57 +21,67 @@ __device__ __forceinline__ void bspline3(float t, float w[4]) {
     w[3] = t3 * (1.0f / 6.0f);
 }
 
-// 64 moving-image bins of the 4x4x4 neighbourhood, packed 4 per word along z.  Fast path: two
-// aligned 32-bit loads per (x, y) row from the zero-padded bin volume and a funnel shift; the
-// padding is bin 0, which is the reference's value for nodes outside the moving grid
-// (MILikelihood.cpp:46-48).  Slow path (neighbourhood leaves the padded volume): per-node test.
+// Bins of the 4 x 4 x 4 (3D) or 4 x 4 (2D) neighbourhood, packed 4 per word along the last axis.
+// A 2D image is handled as an nx x 1 x ny volume: its y axis plays the packed (z) role and there
+// is a single node row per x, so DIM == 2 gathers 4 words (x rows) and DIM == 3 gathers 16
+// ((x, y) rows).  Fast path: two aligned 32-bit loads per row from the zero-padded bin volume and
+// a funnel shift; the padding is bin 0, which is the reference's value for nodes outside the
+// moving grid (MILikelihood.cpp:46-48).  Slow path (neighbourhood leaves the padded volume):
+// per-node test.
+template <int DIM>
 __device__ __forceinline__ void gather_bins(const EStepArgs &a, int ix, int iy, int iz,
-                                            uint32_t pk[16]) {
+                                            uint32_t (&pk)[DIM == 3 ? 16 : 4]) {
+    constexpr int Q = DIM == 3 ? 4 : 1;
     const int zz0 = iz - 1 + a.PZ;
+    const int Py = DIM == 3 ? a.P : 0;
+    const int y0 = DIM == 3 ? iy - 1 : 0;
     const bool fast = (ix - 1 + a.P >= 0) && (ix + 2 + a.P < a.nxn + 2 * a.P) &&
-                      (iy - 1 + a.P >= 0) && (iy + 2 + a.P < a.nyn + 2 * a.P) && (zz0 >= 0) &&
-                      ((zz0 >> 2) + 2 <= (a.zp >> 2));
+                      (DIM == 2 || ((iy - 1 + a.P >= 0) && (iy + 2 + a.P < a.nyn + 2 * a.P))) &&
+                      (zz0 >= 0) && ((zz0 >> 2) + 2 <= (a.zp >> 2));
     if (fast) {
         const int w = zz0 >> 2, sh = (zz0 & 3) * 8;
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 const uint32_t *row = reinterpret_cast<const uint32_t *>(
-                    a.vpad + ((long)(ix - 1 + p + a.P) * a.pyn + (iy - 1 + q + a.P)) * a.zp);
+                    a.vpad + ((long)(ix - 1 + p + a.P) * a.pyn + (y0 + q + Py)) * a.zp);
                 const uint32_t lo = __ldg(row + w), hi = __ldg(row + w + 1);
-                pk[p * 4 + q] = __funnelshift_r(lo, hi, sh);
+                pk[p * Q + q] = __funnelshift_r(lo, hi, sh);
             }
     } else {
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < Q; ++q) {
                 uint32_t word = 0;
-                const int X = ix - 1 + p, Y = iy - 1 + q;
+                const int X = ix - 1 + p, Y = y0 + q;
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const int Z = iz - 1 + c;
                     uint32_t b = 0;
                     if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn)
-                        b = a.vpad[((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp + (Z + a.PZ)];
+                        b = a.vpad[((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp + (Z + a.PZ)];
                     word |= b << (8 * c);
                 }
-                pk[p * 4 + q] = word;
+                pk[p * Q + q] = word;
             }
     }
 }
 
-// word (p, q) of gather_bins alone: bins of nodes (ix-1+p, iy-1+q, iz-1 .. iz+2)
+// word (p, q) of gather_bins alone: bins of nodes (ix-1+p, iy-1+q, iz-1 .. iz+2) (q = 0 in 2D)
+template <int DIM>
 __device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int iy, int iz, int p,
                                                 int q) {
     const int zz0 = iz - 1 + a.PZ;
-    const int X = ix - 1 + p, Y = iy - 1 + q;
-    const bool fast = (X + a.P >= 0) && (X + a.P < a.nxn + 2 * a.P) && (Y + a.P >= 0) &&
-                      (Y + a.P < a.nyn + 2 * a.P) && (zz0 >= 0) && ((zz0 >> 2) + 2 <= (a.zp >> 2));
+    const int Py = DIM == 3 ? a.P : 0;
+    const int X = ix - 1 + p, Y = DIM == 3 ? iy - 1 + q : 0;
+    const bool fast = (X + a.P >= 0) && (X + a.P < a.nxn + 2 * a.P) &&
+                      (DIM == 2 || ((Y + a.P >= 0) && (Y + a.P < a.nyn + 2 * a.P))) &&
+                      (zz0 >= 0) && ((zz0 >> 2) + 2 <= (a.zp >> 2));
     if (fast) {
         const uint32_t *rowp = reinterpret_cast<const uint32_t *>(
-            a.vpad + ((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp);
+            a.vpad + ((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp);
         const int w = zz0 >> 2, sh = (zz0 & 3) * 8;
         return __funnelshift_r(__ldg(rowp + w), __ldg(rowp + w + 1), sh);
     }
@@ -81,17 +91,45 @@ __device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int 
         const int Z = iz - 1 + c;
         uint32_t b = 0;
         if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn)
-            b = a.vpad[((long)(X + a.P) * a.pyn + (Y + a.P)) * a.zp + (Z + a.PZ)];
+            b = a.vpad[((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp + (Z + a.PZ)];
         word |= b << (8 * c);
     }
     return word;
 }
 
-__device__ __forceinline__ float voxel_coord(const EStepArgs &a, long i, int comp) {
-    if (a.x) return a.x[comp * a.V + i];
-    const long yz = (long)a.ny * a.nz;
-    return comp == 0 ? (float)(i / yz) : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
-}
+// One voxel's position and spline setup, shared by the E-step kernels.  Positions are SoA [N][V]
+// (N = DIM); in 2D the second component is the packed-axis position (z role) and y is absent.
+// Returns false for a degenerate position (outside any grid or not finite).
+template <int DIM>
+struct VoxelPos {
+    float px, py, pz;     // position (py = 0 in 2D)
+    float x0, x1, x2;     // voxel grid position
+    __device__ __forceinline__ bool load(const EStepArgs &a, unsigned i, unsigned V, unsigned ny,
+                                         unsigned nz) {
+        px = a.d[i];
+        py = DIM == 3 ? a.d[V + i] : 0.0f;
+        pz = a.d[(size_t)(DIM - 1) * V + i];
+        if (a.x) {
+            x0 = a.x[i];
+            x1 = DIM == 3 ? a.x[V + i] : 0.0f;
+            x2 = a.x[(size_t)(DIM - 1) * V + i];
+        } else {
+            const unsigned row = i / nz;
+            x2 = (float)(i - row * nz);
+            const unsigned xi = row / ny;
+            x1 = (float)(row - xi * ny);
+            x0 = (float)xi;
+        }
+        return fabsf(px) < 1.0e6f && (DIM == 2 || fabsf(py) < 1.0e6f) && fabsf(pz) < 1.0e6f;
+    }
+    // r = dream location - voxel position, components (x, [y,] z-role)
+    __device__ __forceinline__ void store_r(const EStepArgs &a, unsigned i, unsigned V, float vx,
+                                            float vy, float vz) const {
+        a.r[i] = vx - x0;
+        if (DIM == 3) a.r[V + i] = vy - x1;
+        a.r[(size_t)(DIM - 1) * V + i] = vz - x2;
+    }
+};
 
 // row pitch (floats) of the shared theta / histogram tables: >= n and 9 banks apart row to row
 __host__ __device__ constexpr int theta_pitch(int K) { return K + ((9 - K % 32) + 32) % 32; }
@@ -99,15 +137,15 @@ __host__ __device__ constexpr int theta_pitch(int K) { return K + ((9 - K % 32) 
 constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
 constexpr int kFastThreads = 256;
 
-// The 64-node pass of one EM voxel: weights w = bx[p] by[q] bz[c] theta[k] added to the
-// thread's private bin column col[k * TPB], their sum S, their first moments along each axis
-// (node offset -1 .. 2 times w) and the range of bins touched.  theta and the column are disjoint
-// regions of shared memory; the __restrict__ qualifiers let the compiler hoist the theta loads of
-// later nodes above earlier column updates.  Products and sums run on paired FP32 lanes (nodes
-// c = 0,1 and c = 2,3 of each packed word).
-template <int TPB>
+// The node pass of one EM voxel (4 x Q rows of 4 packed nodes; Q = 4 in 3D, 1 in 2D): weights
+// w = bx[p] by[q] bz[c] theta[k] added to the thread's private bin column col[k * TPB], their sum
+// S, their first moments along each axis (node offset -1 .. 2 times w) and the range of bins
+// touched.  theta and the column are disjoint regions of shared memory; the __restrict__
+// qualifiers let the compiler hoist the theta loads of later nodes above earlier column updates.
+// Products and sums run on paired FP32 lanes (nodes c = 0,1 and c = 2,3 of each packed word).
+template <int TPB, int Q>
 __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
-                                              float *__restrict__ col, const uint32_t (&pk)[16],
+                                              float *__restrict__ col, const uint32_t (&pk)[4 * Q],
                                               const float (&bx)[4], const float (&by)[4],
                                               const float (&bz)[4], float &S, float &Sx, float &Sy,
                                               float &Sz, int &kmin, int &kmax) {
@@ -120,11 +158,11 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float bxy = bx[p] * by[q];
+        for (int q = 0; q < Q; ++q) {
+            const float bxy = Q == 4 ? bx[p] * by[q] : bx[p];
             const float2 bb = make_float2(bxy, bxy);
             const float2 b01 = __fmul2_rn(bb, bz01), b23 = __fmul2_rn(bb, bz23);
-            const uint32_t word = pk[p * 4 + q];
+            const uint32_t word = pk[p * Q + q];
             const int k0 = word & 0xff, k1 = (word >> 8) & 0xff, k2 = (word >> 16) & 0xff,
                       k3 = word >> 24;
             const float2 w01 = __fmul2_rn(b01, make_float2(thu[k0], thu[k1]));
@@ -138,36 +176,38 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
             if (p == 0) { x01 = __ffma2_rn(m1, w01, x01); x23 = __ffma2_rn(m1, w23, x23); }
             if (p == 2) { x01 = __fadd2_rn(x01, w01); x23 = __fadd2_rn(x23, w23); }
             if (p == 3) { x01 = __ffma2_rn(p2, w01, x01); x23 = __ffma2_rn(p2, w23, x23); }
-            if (q == 0) { y01 = __ffma2_rn(m1, w01, y01); y23 = __ffma2_rn(m1, w23, y23); }
-            if (q == 2) { y01 = __fadd2_rn(y01, w01); y23 = __fadd2_rn(y23, w23); }
-            if (q == 3) { y01 = __ffma2_rn(p2, w01, y01); y23 = __ffma2_rn(p2, w23, y23); }
+            if (Q == 4) {
+                if (q == 0) { y01 = __ffma2_rn(m1, w01, y01); y23 = __ffma2_rn(m1, w23, y23); }
+                if (q == 2) { y01 = __fadd2_rn(y01, w01); y23 = __fadd2_rn(y23, w23); }
+                if (q == 3) { y01 = __ffma2_rn(p2, w01, y01); y23 = __ffma2_rn(p2, w23, y23); }
+            }
             lo = min(min(lo, min(k0, k1)), min(k2, k3));
             hi = max(max(hi, max(k0, k1)), max(k2, k3));
         }
     S = (a01.x + a01.y) + (a23.x + a23.y);
     Sx = (x01.x + x01.y) + (x23.x + x23.y);
     Sy = (y01.x + y01.y) + (y23.x + y23.y);
-    Sz = (a23.x - a01.x) + 2.0f * a23.y;  // offsets -1, 0, 1, 2 along z
+    Sz = (a23.x - a01.x) + 2.0f * a23.y;  // offsets -1, 0, 1, 2 along the packed axis
     kmin = lo;
     kmax = hi;
 }
 
 // EM E-step for K <= 64 (BINDER/src/cpu/Registration.cpp:219-330, sample == false), one pass over
-// the 64 neighbours.  The posterior mass of a voxel is collected per moving bin k in a private
-// shared-memory column hk[k][thread] (bank = thread % 32, so never a conflict and never an
-// atomic), while the smallest and largest bin touched are tracked; once the normaliser S is known
-// the columns in [kmin, kmax] that hold mass are flushed as hist[k][u] += hk[k] / S -- one shared
-// atomic per distinct bin instead of one per neighbour (the bin range of a 4x4x4 neighbourhood is
-// a handful of bins in smooth images).  The CTA histogram is 32-bit fixed point (scale a.hscale,
-// chosen by the host so that a cell cannot overflow: each voxel adds at most 1 to a cell), which
-// makes every flush a native integer shared atomic, and is converted to FP32 once per CTA.  Each
-// contribution is rounded to within 0.5 / hscale (4e-6 at 2^17); FP32 accumulation of the same
-// sums would round each addition relative to the running sum instead.  theta is staged
-// transposed (thT[u][k]); it and the histogram use a row pitch of 9 (mod 32) banks, so lanes
-// whose (u, k) pairs differ by small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the
-// host).
-template <int TPB>
+// the 64 (3D) or 16 (2D) neighbours.  The posterior mass of a voxel is collected per moving bin k
+// in a private shared-memory column hk[k][thread] (bank = thread % 32, so never a conflict and
+// never an atomic), while the smallest and largest bin touched are tracked; once the normaliser S
+// is known the columns in [kmin, kmax] that hold mass are flushed as hist[k][u] += hk[k] / S --
+// one shared atomic per distinct bin instead of one per neighbour (the bin range of a
+// neighbourhood is a handful of bins in smooth images).  The CTA histogram is 32-bit fixed point
+// (scale a.hscale, chosen by the host so that a cell cannot overflow), which makes every flush a
+// native integer shared atomic, and is converted to FP32 once per CTA.  Each contribution is
+// rounded to within 0.5 / hscale (4e-6 at 2^17); FP32 accumulation of the same sums would round
+// each addition relative to the running sum instead.  theta is staged transposed (thT[u][k]); it
+// and the histogram use a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ by
+// small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the host).
+template <int TPB, int DIM>
 __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
+    constexpr int Q = DIM == 3 ? 4 : 1;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
@@ -189,37 +229,25 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
     unsigned deg = 0;
     // unsigned: i + stride stays below 2^32 for any V < 2^31
     const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
-    const float *d0 = a.d, *d1 = a.d + V, *d2 = a.d + 2 * (size_t)V;
-    float *r0p = a.r, *r1p = a.r + V, *r2p = a.r + 2 * (size_t)V;
     for (unsigned i = blockIdx.x * TPB + threadIdx.x; i < V; i += gridDim.x * TPB) {
-        const float px = d0[i], py = d1[i], pz = d2[i];
-        float x0, x1, x2;
-        if (a.x) {
-            x0 = a.x[i]; x1 = a.x[V + i]; x2 = a.x[2 * (size_t)V + i];
-        } else {
-            const unsigned row = i / nz;
-            x2 = (float)(i - row * nz);
-            const unsigned xi = row / ny;
-            x1 = (float)(row - xi * ny);
-            x0 = (float)xi;
-        }
-        if (!(fabsf(px) < 1.0e6f && fabsf(py) < 1.0e6f && fabsf(pz) < 1.0e6f)) {
-            r0p[i] = px - x0; r1p[i] = py - x1; r2p[i] = pz - x2;
+        VoxelPos<DIM> vp;
+        if (!vp.load(a, i, V, ny, nz)) {
+            vp.store_r(a, i, V, vp.px, vp.py, vp.pz);
             ++deg;
             continue;
         }
-        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        const float fx = floorf(vp.px), fy = floorf(vp.py), fz = floorf(vp.pz);
         const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-        float bx[4], by[4], bz[4];
-        bspline3(px - fx, bx);
-        bspline3(py - fy, by);
-        bspline3(pz - fz, bz);
-        uint32_t pk[16];
-        gather_bins(a, ix, iy, iz, pk);
+        float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
+        bspline3(vp.px - fx, bx);
+        if (DIM == 3) bspline3(vp.py - fy, by);
+        bspline3(vp.pz - fz, bz);
+        uint32_t pk[4 * Q];
+        gather_bins<DIM>(a, ix, iy, iz, pk);
         const int ui = a.u[i];
         float S, Sx, Sy, Sz;
         int kmin, kmax;
-        em_accumulate<TPB>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin, kmax);
+        em_accumulate<TPB, Q>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin, kmax);
         const bool ok = S > 0.0f;
         const float inv = ok ? 1.0f / S : 0.0f;
         const float invs = inv * a.hscale;
@@ -232,14 +260,12 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
             }
         }
         if (!ok) {
-            r0p[i] = fx - x0; r1p[i] = fy - x1; r2p[i] = fz - x2;
+            vp.store_r(a, i, V, fx, fy, fz);
             ++deg;
             continue;
         }
         mll -= (double)logf(S);  // FP32 log, FP64 accumulation
-        r0p[i] = (fx + Sx * inv) - x0;
-        r1p[i] = (fy + Sy * inv) - x1;
-        r2p[i] = (fz + Sz * inv) - x2;
+        vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < KL; q += TPB) {
@@ -256,8 +282,10 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
 // for the Gibbs draw and for EM with K > 64.
-template <bool SAMPLE>
+template <bool SAMPLE, int DIM>
 __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) {
+    constexpr int Q = DIM == 3 ? 4 : 1;
+    constexpr int R = 4 * Q;  // node rows of 4 packed nodes
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int KL = a.K * a.L;
@@ -275,25 +303,23 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
     const uint32_t sweep = SAMPLE ? (uint32_t)a.st->sweep : 0u;
     double mll = 0.0;
     unsigned long long deg = 0;
-    const float *d0 = a.d, *d1 = a.d + a.V, *d2 = a.d + 2 * a.V;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.V;
-         i += (long)gridDim.x * blockDim.x) {
-        const float px = d0[i], py = d1[i], pz = d2[i];
-        const float x0 = voxel_coord(a, i, 0), x1 = voxel_coord(a, i, 1), x2 = voxel_coord(a, i, 2);
+    const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+        VoxelPos<DIM> vp;
         // positions far outside any grid (or non-finite) are degenerate: keep them as they are
-        if (!(fabsf(px) < 1.0e6f && fabsf(py) < 1.0e6f && fabsf(pz) < 1.0e6f)) {
-            a.r[i] = px - x0; a.r[a.V + i] = py - x1; a.r[2 * a.V + i] = pz - x2;
+        if (!vp.load(a, i, V, ny, nz)) {
+            vp.store_r(a, i, V, vp.px, vp.py, vp.pz);
             ++deg;
             continue;
         }
-        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        const float fx = floorf(vp.px), fy = floorf(vp.py), fz = floorf(vp.pz);
         const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-        float bx[4], by[4], bz[4];
-        bspline3(px - fx, bx);
-        bspline3(py - fy, by);
-        bspline3(pz - fz, bz);
-        uint32_t pk[16];
-        gather_bins(a, ix, iy, iz, pk);
+        float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
+        bspline3(vp.px - fx, bx);
+        if (DIM == 3) bspline3(vp.py - fy, by);
+        bspline3(vp.pz - fz, bz);
+        uint32_t pk[R];
+        gather_bins<DIM>(a, ix, iy, iz, pk);
         const float *thc = th + a.u[i];  // theta column of this voxel's bin: thc[k * L]
         const int L = a.L;
 
@@ -302,31 +328,29 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
 #pragma unroll
         for (int p = 0; p < 4; ++p)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float bxy = __fmul_rn(bx[p], by[q]);
-                const uint32_t word = pk[p * 4 + q];
+            for (int q = 0; q < Q; ++q) {
+                const float bxy = DIM == 3 ? __fmul_rn(bx[p], by[q]) : bx[p];
+                const uint32_t word = pk[p * Q + q];
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const int k = (word >> (8 * c)) & 0xff;
                     const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
                     S = __fadd_rn(S, w);
                     Sx = fmaf((float)(p - 1), w, Sx);
-                    Sy = fmaf((float)(q - 1), w, Sy);
+                    if (DIM == 3) Sy = fmaf((float)(q - 1), w, Sy);
                     Sz = fmaf((float)(c - 1), w, Sz);
                 }
-                if (SAMPLE) cps[(p * 4 + q) * kEThreads] = S;
+                if (SAMPLE) cps[(p * Q + q) * kEThreads] = S;
             }
         if (!(S > 0.0f)) {
-            a.r[i] = fx - x0; a.r[a.V + i] = fy - x1; a.r[2 * a.V + i] = fz - x2;
+            vp.store_r(a, i, V, fx, fy, fz);
             ++deg;
             continue;
         }
         if (!SAMPLE) {
             const float inv = 1.0f / S;
             mll -= log((double)S);
-            a.r[i] = (fx + Sx * inv) - x0;
-            a.r[a.V + i] = (fy + Sy * inv) - x1;
-            a.r[2 * a.V + i] = (fz + Sz * inv) - x2;
+            vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
             // pass 2: normalised posteriors into the histogram column u_i, runs of equal bins
             // combined in a register before each shared-memory atomic
             const int ui = a.u[i];
@@ -335,9 +359,9 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
 #pragma unroll
             for (int p = 0; p < 4; ++p)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float bxy = __fmul_rn(bx[p], by[q]);
-                    const uint32_t word = pk[p * 4 + q];
+                for (int q = 0; q < Q; ++q) {
+                    const float bxy = DIM == 3 ? __fmul_rn(bx[p], by[q]) : bx[p];
+                    const uint32_t word = pk[p * Q + q];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
                         const int k = (word >> (8 * c)) & 0xff;
@@ -357,11 +381,11 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
             // is the same sequence of FP32 additions as S above and never decreases (w >= 0), so
             // the first node row whose end value reaches the target holds the pick; only that
             // row's four nodes are summed again, from the previous row's end value.
-            const u32x4 rr = philox_draw(a.seed, (uint32_t)i, sweep, 1u, a.chain);
+            const u32x4 rr = philox_draw(a.seed, i, sweep, 1u, a.chain);
             const float t = u01_f24(rr.x) * S;
-            int row = 15;
+            int row = R - 1;
             float cdf = 0.0f;
-            for (int r = 0; r < 16; ++r) {
+            for (int r = 0; r < R; ++r) {
                 const float e = cps[r * kEThreads];
                 if (e >= t) {
                     row = r;
@@ -369,11 +393,11 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
                 }
                 cdf = e;
             }
-            const int p = row >> 2, q = row & 3;
+            const int p = row / Q, q = row % Q;
             const float bxp = p == 0 ? bx[0] : (p == 1 ? bx[1] : (p == 2 ? bx[2] : bx[3]));
             const float byq = q == 0 ? by[0] : (q == 1 ? by[1] : (q == 2 ? by[2] : by[3]));
-            const float bxy = __fmul_rn(bxp, byq);
-            const uint32_t word = gather_word(a, ix, iy, iz, p, q);
+            const float bxy = DIM == 3 ? __fmul_rn(bxp, byq) : bxp;
+            const uint32_t word = gather_word<DIM>(a, ix, iy, iz, p, q);
             int pick = -1, kp = 0;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -386,13 +410,12 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
                 }
             }
             if (pick < 0) {  // unreachable (cdf ends at S >= t); keep the last neighbour
-                pick = 63;
-                kp = (gather_word(a, ix, iy, iz, 3, 3) >> 24) & 0xff;
+                pick = 4 * R - 1;
+                kp = (gather_word<DIM>(a, ix, iy, iz, 3, Q - 1) >> 24) & 0xff;
             }
             atomicAdd(&hc[kp * L + a.u[i]], 1u);
-            a.r[i] = (fx + (float)(pick / 16 - 1)) - x0;
-            a.r[a.V + i] = (fy + (float)((pick / 4) % 4 - 1)) - x1;
-            a.r[2 * a.V + i] = (fz + (float)(pick % 4 - 1)) - x2;
+            const int ox = pick / (4 * Q) - 1, oy = (pick / 4) % Q - 1, oz = pick % 4 - 1;
+            vp.store_r(a, i, V, fx + (float)ox, fy + (float)oy, fz + (float)oz);
         }
     }
 
@@ -542,6 +565,9 @@ __global__ void em_finish_kernel(DevState *st, double *stats, int max_iter, doub
 }
 
 // Registration.cpp:593-623 in FP64 with the symmetric M2 (xx, xy, xz, yy, yz, zz)
+// N components: mean [N][V], M2 as its upper triangle [N (N + 1) / 2][V] (row-major: xx, xy, xz,
+// yy, yz, zz or xx, xy, yy)
+template <int N>
 __global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long V, int N_b,
                                  DevState *st) {
     if (st->done) return;
@@ -550,9 +576,9 @@ __global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long 
         const double inv_n = 1.0 / ((double)(sweep - N_b) + 1.0);
         for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
              i += (long)gridDim.x * blockDim.x) {
-            double d1[3], d2[3];
+            double d1[N], d2[N];
 #pragma unroll
-            for (int n = 0; n < 3; ++n) {
+            for (int n = 0; n < N; ++n) {
                 const double val = (double)d[n * V + i];
                 const double mo = mean[n * V + i];
                 d1[n] = val - mo;
@@ -560,12 +586,11 @@ __global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long 
                 mean[n * V + i] = mn;
                 d2[n] = val - mn;
             }
-            m2[0 * V + i] += d1[0] * d2[0];
-            m2[1 * V + i] += d1[0] * d2[1];
-            m2[2 * V + i] += d1[0] * d2[2];
-            m2[3 * V + i] += d1[1] * d2[1];
-            m2[4 * V + i] += d1[1] * d2[2];
-            m2[5 * V + i] += d1[2] * d2[2];
+            int e = 0;
+#pragma unroll
+            for (int r = 0; r < N; ++r)
+#pragma unroll
+                for (int c = r; c < N; ++c, ++e) m2[e * V + i] += d1[r] * d2[c];
         }
     }
 }
@@ -586,14 +611,32 @@ size_t estep_smem(bool sample, int K, int L) {
 }
 }  // namespace
 
-int estep_grid(bool sample, int K, int L, long V) {
+namespace {
+template <int DIM>
+const void *estep_fn(bool sample, int K) {
+    return sample ? (const void *)estep_kernel<true, DIM>
+                  : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads, DIM>
+                                  : (const void *)estep_kernel<false, DIM>);
+}
+
+template <int DIM>
+void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
+    if (sample)
+        count_launch(), estep_kernel<true, DIM><<<grid, kEThreads, smem, s>>>(a);
+    else if (a.K <= kSmallK)
+        count_launch(), estep_em_fast_kernel<kFastThreads, DIM><<<grid, kFastThreads, smem, s>>>(a);
+    else
+        count_launch(), estep_kernel<false, DIM><<<grid, kEThreads, smem, s>>>(a);
+}
+}  // namespace
+
+int estep_grid(bool sample, int K, int L, long V, int dim) {
+    BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t smem = estep_smem(sample, K, L);
-    const void *fn = sample ? (const void *)estep_kernel<true>
-                            : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads>
-                                            : (const void *)estep_kernel<false>);
+    const void *fn = dim == 3 ? estep_fn<3>(sample, K) : estep_fn<2>(sample, K);
     const int tpb = (!sample && K <= kSmallK) ? kFastThreads : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tpb, smem));
@@ -616,12 +659,9 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) 
     while (e > 0 && (double)per_cta * (std::ldexp(1.0, e) + 1.0) >= 4294967295.0) --e;
     a.hscale = (float)std::ldexp(1.0, e);
     a.hinv = (float)std::ldexp(1.0, -e);
-    if (sample)
-        count_launch(), estep_kernel<true><<<grid, kEThreads, smem, s>>>(a);
-    else if (a.K <= kSmallK)
-        count_launch(), estep_em_fast_kernel<kFastThreads><<<grid, kFastThreads, smem, s>>>(a);
-    else
-        count_launch(), estep_kernel<false><<<grid, kEThreads, smem, s>>>(a);
+    BINDER_CHECK(a.dim == 2 || a.dim == 3, "dimension must be 2 or 3");
+    if (a.dim == 3) launch_estep_dim<3>(a, sample, grid, smem, s);
+    else launch_estep_dim<2>(a, sample, grid, smem, s);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -651,14 +691,16 @@ void launch_em_finish(DevState *st, double *stats, int max_iter, double th, doub
     BINDER_CUDA(cudaGetLastError());
 }
 
-void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N_b, int total,
-                      DevState *st, cudaStream_t s) {
+void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N, int N_b,
+                      int total, DevState *st, cudaStream_t s) {
     int dev = 0, sms = 148;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     long need = (V + 255) / 256;
     const long g = need < (long)sms * 8 ? (need < 1 ? 1 : need) : (long)sms * 8;
-    count_launch(), sweep_end_kernel<<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    BINDER_CHECK(N == 2 || N == 3, "Welford moments need N = 2 or 3");
+    if (N == 3) count_launch(), sweep_end_kernel<3><<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    else count_launch(), sweep_end_kernel<2><<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
     BINDER_CUDA(cudaGetLastError());
     launch_sweep_advance(st, total, s);
 }

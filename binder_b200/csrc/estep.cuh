@@ -5,10 +5,12 @@
 
 namespace binder {
 
+// A 2D image nx x ny is passed as the volume nx x 1 x ny (ny, nyn = 1): its y axis is the packed
+// (z) axis of the bin volume and positions have N = dim = 2 components (x, y).
 struct EStepArgs {
-    const float *d;   // positions, SoA [3][V] (node-grid coordinates)
-    float *r;         // out: dream location minus voxel position, SoA [3][V]
-    const float *x;   // voxel positions SoA [3][V], or null for the identity grid
+    const float *d;   // positions, SoA [dim][V] (node-grid coordinates)
+    float *r;         // out: dream location minus voxel position, SoA [dim][V]
+    const float *x;   // voxel positions SoA [dim][V], or null for the identity grid
     const uint8_t *u;     // fixed-image bins [V]
     const uint8_t *vpad;  // moving-image bins, zero-padded [nxn+2P][nyn+2P][zp bytes]
     const float *theta;   // [K*L]
@@ -21,6 +23,7 @@ struct EStepArgs {
     int nxn, nyn, nzn;
     int P, PZ, pyn, zp;
     int K, L;
+    int dim;  // 2 or 3
     uint64_t seed;
     uint32_t chain;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
@@ -28,7 +31,7 @@ struct EStepArgs {
 };
 
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
-int estep_grid(bool sample, int K, int L, long V);
+int estep_grid(bool sample, int K, int L, long V, int dim);
 
 // theta <- (hist + alpha - 1)/rowsum (if update), Dirichlet prior cost into st->lp_lik,
 // hist zeroed for the next iteration.  One CTA.
@@ -44,10 +47,10 @@ void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, 
 // EM bookkeeping: min-log-posterior, per-iteration stats, convergence flag
 void launch_em_finish(DevState *st, double *stats, int max_iter, double th, double nzv,
                       cudaStream_t s);
-// Welford mean / symmetric M2 update in FP64 when sweep >= N_b, then sweep += 1 (done once
-// sweep reaches `total`)
-void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N_b, int total,
-                      DevState *st, cudaStream_t s);
+// Welford mean [N][V] / symmetric M2 [N (N + 1) / 2][V] update in FP64 when sweep >= N_b, then
+// sweep += 1 (done once sweep reaches `total`)
+void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N, int N_b,
+                      int total, DevState *st, cudaStream_t s);
 // sweep += 1 (done once sweep reaches `total`)
 void launch_sweep_advance(DevState *st, int total, cudaStream_t s);
 

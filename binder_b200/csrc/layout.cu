@@ -32,62 +32,52 @@ int blocks_for(long work) {
     return (int)(b < 1 ? 1 : (b > 148L * 16 ? 148L * 16 : b));
 }
 
-__device__ __forceinline__ float grid_coord(long i, int c, int ny, int nz) {
-    const long yz = (long)ny * nz;
-    return c == 0 ? (float)(i / yz) : (c == 1 ? (float)((i / nz) % ny) : (float)(i % nz));
+// index c of voxel i of the identity grid (a 2D image nx x ny x 1: c = 0 -> x, c = 1 -> y)
+__device__ __forceinline__ float grid_coord(long i, int c, const GridDims &g) {
+    const long yz = (long)g.ny * g.nz;
+    if (c == 0) return (float)(i / yz);
+    if (g.N == 2) return (float)(i % yz);
+    return c == 1 ? (float)((i / g.nz) % g.ny) : (float)(i % g.nz);
 }
 
-__global__ void aos_to_soa_kernel(const float *aos, float *soa, long V) {
+__global__ void aos_to_soa_kernel(const float *aos, float *soa, long V, int N) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
-         i += (long)gridDim.x * blockDim.x) {
-        const float a = aos[3 * i], b = aos[3 * i + 1], c = aos[3 * i + 2];
-        soa[i] = a;
-        soa[V + i] = b;
-        soa[2 * V + i] = c;
-    }
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < N; ++c) soa[c * V + i] = aos[N * i + c];
 }
 
-__global__ void soa_to_aos_kernel(const float *soa, float *aos, long V) {
+__global__ void soa_to_aos_kernel(const float *soa, float *aos, long V, int N) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
-         i += (long)gridDim.x * blockDim.x) {
-        aos[3 * i] = soa[i];
-        aos[3 * i + 1] = soa[V + i];
-        aos[3 * i + 2] = soa[2 * V + i];
-    }
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < N; ++c) aos[N * i + c] = soa[c * V + i];
 }
 
 __global__ void soa_to_aos_plus_kernel(const float *soa, const float *x, GridDims g, float *aos) {
     const long V = (long)g.nx * g.ny * g.nz;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
-         i += (long)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float b = x ? x[c * V + i] : grid_coord(i, c, g.ny, g.nz);
-            aos[3 * i + c] = soa[c * V + i] + b;
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < g.N; ++c) {
+            const float b = x ? x[c * V + i] : grid_coord(i, c, g);
+            aos[g.N * i + c] = soa[c * V + i] + b;
         }
-    }
 }
 
 __global__ void aos_minus_to_soa_kernel(const float *aos, const float *x, GridDims g, float *soa) {
     const long V = (long)g.nx * g.ny * g.nz;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
-         i += (long)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float b = x ? x[c * V + i] : grid_coord(i, c, g.ny, g.nz);
-            soa[c * V + i] = (aos ? aos[3 * i + c] : 0.0f) - b;
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < g.N; ++c) {
+            const float b = x ? x[c * V + i] : grid_coord(i, c, g);
+            soa[c * V + i] = (aos ? aos[g.N * i + c] : 0.0f) - b;
         }
-    }
 }
 
 __global__ void identity_check_kernel(const float *aos, GridDims g, unsigned *mismatch) {
     const long V = (long)g.nx * g.ny * g.nz;
     bool bad = false;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
-         i += (long)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) bad |= aos[3 * i + c] != grid_coord(i, c, g.ny, g.nz);
-    }
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < g.N; ++c) bad |= aos[g.N * i + c] != grid_coord(i, c, g);
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(mismatch, 1u);
 }
 
@@ -106,7 +96,7 @@ __global__ void bins_to_u8_kernel(const int *in, long n, int limit, uint8_t *out
 }
 
 __global__ void bins_to_padded_kernel(const int *in, int nx, int ny, int nz, int limit,
-                                      uint8_t *vpad, int P, int PZ, int pyn, int zp,
+                                      uint8_t *vpad, int P, int Py, int PZ, int pyn, int zp,
                                       unsigned long long *first_bad) {
     const long n = (long)nx * ny * nz;
     for (long j = (long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
@@ -117,22 +107,22 @@ __global__ void bins_to_padded_kernel(const int *in, int nx, int ny, int nz, int
             atomicMin(first_bad, (unsigned long long)j);
             b = 0;
         }
-        vpad[((long)(x + P) * pyn + (y + P)) * zp + (z + PZ)] = (uint8_t)b;
+        vpad[((long)(x + P) * pyn + (y + Py)) * zp + (z + PZ)] = (uint8_t)b;
     }
 }
 
-__global__ void moments_to_aos_kernel(const double *mean, const double *m2, long V, double scale,
-                                      double *mean_aos, double *cov_aos) {
-    // symmetric M2 stored as xx, xy, xz, yy, yz, zz
-    const int sym[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+__global__ void moments_to_aos_kernel(const double *mean, const double *m2, long V, int N,
+                                      double scale, double *mean_aos, double *cov_aos) {
+    // symmetric M2 stored as its upper triangle: xx, xy, xz, yy, yz, zz (N = 3) or xx, xy, yy
+    const int sym3[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    const int sym2[4] = {0, 1, 1, 2};
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
          i += (long)gridDim.x * blockDim.x) {
         if (mean_aos)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) mean_aos[3 * i + c] = mean[c * V + i];
+            for (int c = 0; c < N; ++c) mean_aos[N * i + c] = mean[c * V + i];
         if (cov_aos)
-#pragma unroll
-            for (int e = 0; e < 9; ++e) cov_aos[9 * i + e] = m2[sym[e] * V + i] * scale;
+            for (int e = 0; e < N * N; ++e)
+                cov_aos[N * N * i + e] = m2[(N == 3 ? sym3[e] : sym2[e]) * V + i] * scale;
     }
 }
 
@@ -150,13 +140,13 @@ void dev_free(void *p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
 }
 
-void launch_aos_to_soa(const float *aos, float *soa, long V, cudaStream_t s) {
-    count_launch(), aos_to_soa_kernel<<<blocks_for(V), 256, 0, s>>>(aos, soa, V);
+void launch_aos_to_soa(const float *aos, float *soa, long V, int N, cudaStream_t s) {
+    count_launch(), aos_to_soa_kernel<<<blocks_for(V), 256, 0, s>>>(aos, soa, V, N);
     BINDER_CUDA(cudaGetLastError());
 }
 
-void launch_soa_to_aos(const float *soa, float *aos, long V, cudaStream_t s) {
-    count_launch(), soa_to_aos_kernel<<<blocks_for(V), 256, 0, s>>>(soa, aos, V);
+void launch_soa_to_aos(const float *soa, float *aos, long V, int N, cudaStream_t s) {
+    count_launch(), soa_to_aos_kernel<<<blocks_for(V), 256, 0, s>>>(soa, aos, V, N);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -187,17 +177,17 @@ void launch_bins_to_u8(const int *in, long n, int limit, uint8_t *out,
 }
 
 void launch_bins_to_padded(const int *in, int nx, int ny, int nz, int limit, uint8_t *vpad, int P,
-                           int PZ, int pyn, int zp, unsigned long long *first_bad,
+                           int Py, int PZ, int pyn, int zp, unsigned long long *first_bad,
                            cudaStream_t s) {
     const long n = (long)nx * ny * nz;
     count_launch(), bins_to_padded_kernel<<<blocks_for(n), 256, 0, s>>>(
-        in, nx, ny, nz, limit, vpad, P, PZ, pyn, zp, first_bad);
+        in, nx, ny, nz, limit, vpad, P, Py, PZ, pyn, zp, first_bad);
     BINDER_CUDA(cudaGetLastError());
 }
 
-void launch_moments_to_aos(const double *mean, const double *m2, long V, double scale,
+void launch_moments_to_aos(const double *mean, const double *m2, long V, int N, double scale,
                            double *mean_aos, double *cov_aos, cudaStream_t s) {
-    count_launch(), moments_to_aos_kernel<<<blocks_for(V), 256, 0, s>>>(mean, m2, V, scale,
+    count_launch(), moments_to_aos_kernel<<<blocks_for(V), 256, 0, s>>>(mean, m2, V, N, scale,
                                                                          mean_aos, cov_aos);
     BINDER_CUDA(cudaGetLastError());
 }

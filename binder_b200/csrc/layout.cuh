@@ -30,15 +30,17 @@ void dev_free_p(T *&p, cudaStream_t s) {
     p = nullptr;
 }
 
-// identity voxel grid of an nx x ny x nz volume: component c of voxel i
+// identity voxel grid of an nx x ny x nz volume with N components per voxel (N = 3; a 2D image
+// nx x ny is described as nx x ny x 1 with N = 2): component c of voxel i is its c-th index
 struct GridDims {
     int nx, ny, nz;
+    int N;
 };
 
-// soa[c][i] = aos[i][c] (float, 3 components)
-void launch_aos_to_soa(const float *aos, float *soa, long V, cudaStream_t s);
+// soa[c][i] = aos[i][c] (float, N components)
+void launch_aos_to_soa(const float *aos, float *soa, long V, int N, cudaStream_t s);
 // aos[i][c] = soa[c][i]
-void launch_soa_to_aos(const float *soa, float *aos, long V, cudaStream_t s);
+void launch_soa_to_aos(const float *soa, float *aos, long V, int N, cudaStream_t s);
 // aos[i][c] = soa[c][i] + base[c][i], base = x (SoA) or, when x is null, the identity grid
 void launch_soa_to_aos_plus(const float *soa, const float *x, GridDims g, float *aos,
                             cudaStream_t s);
@@ -51,11 +53,13 @@ void launch_identity_check(const float *aos, GridDims g, unsigned *mismatch, cud
 void launch_bins_to_u8(const int *in, long n, int limit, uint8_t *out,
                        unsigned long long *first_bad, cudaStream_t s);
 // bins of an nx x ny x nz node grid into the interior of the zero-padded byte volume
-// vpad[(x + P) * pyn + (y + P)][z + PZ] (row length zp); range check as above
+// vpad[(x + P) * pyn + (y + Py)][z + PZ] (row length zp); range check as above
 void launch_bins_to_padded(const int *in, int nx, int ny, int nz, int limit, uint8_t *vpad, int P,
-                           int PZ, int pyn, int zp, unsigned long long *first_bad, cudaStream_t s);
-// Welford outputs: mean_aos[i][c] = mean[c][i]; cov_aos[i][r][c] = m2[sym(r, c)][i] * scale
-void launch_moments_to_aos(const double *mean, const double *m2, long V, double scale,
+                           int Py, int PZ, int pyn, int zp, unsigned long long *first_bad,
+                           cudaStream_t s);
+// Welford outputs: mean_aos[i][c] = mean[c][i]; cov_aos[i][r][c] = m2[sym(r, c)][i] * scale, M2
+// stored as its upper triangle (xx, xy, xz, yy, yz, zz for N = 3; xx, xy, yy for N = 2)
+void launch_moments_to_aos(const double *mean, const double *m2, long V, int N, double scale,
                            double *mean_aos, double *cov_aos, cudaStream_t s);
 
 }  // namespace binder

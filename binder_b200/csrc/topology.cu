@@ -108,6 +108,35 @@ __global__ void jacobian_kernel(const double *f, long ps, long cs, int nx, int n
     }
 }
 
+// BINDER/src/cpu/utils.cpp:10-98: the 2D Jacobian averaged over the 4 one-sided corners (orders
+// fxfy, bxfy, fxby, bxby), each the determinant of the forward / backward differences, with the
+// reference's expression grouping.  Field AoS [nx][ny][2].
+__global__ void jacobian2d_kernel(const double *f, int nx, int ny, double vol, double *J) {
+    const long V = (long)nx * ny;
+    const int dir[4][2] = {{1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / ny), y = (int)(p % ny);
+        const double w0 = f[p * 2], w1 = f[p * 2 + 1];
+        double tot = 0.0;
+        int valid = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int sx = dir[c][0], sy = dir[c][1];
+            if ((sx > 0 && x >= nx - 1) || (sx < 0 && x <= 0)) continue;
+            if ((sy > 0 && y >= ny - 1) || (sy < 0 && y <= 0)) continue;
+            const long qx = p + (long)sx * ny, qy = p + sy;
+            const double ax0 = sx > 0 ? f[qx * 2] - w0 : w0 - f[qx * 2];
+            const double ax1 = sx > 0 ? f[qx * 2 + 1] - w1 : w1 - f[qx * 2 + 1];
+            const double ay0 = sy > 0 ? f[qy * 2] - w0 : w0 - f[qy * 2];
+            const double ay1 = sy > 0 ? f[qy * 2 + 1] - w1 : w1 - f[qy * 2 + 1];
+            tot += (ax0 * ay1 - ay0 * ax1) * vol;
+            valid++;
+        }
+        J[p] = valid > 0 ? tot / valid : 1.0;
+    }
+}
+
 // topology_correction_3D.cpp:488-607: the 8 vertex Jacobians of every cell, in the vertex order
 // 000, 100, 010, 001, 011, 101, 110, 111, each from the three cell edges through its vertex.
 // Positions are SoA [3][V].
@@ -375,6 +404,34 @@ void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const do
     count_launch(), jacobian_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, 3, 1, nx, ny, nz,
                                                 1.0 / (vs[0] * vs[1] * vs[2]), J, 0.0, 0.0, nullptr);
     BINDER_CUDA(cudaGetLastError());
+}
+
+void jacobian2d_device(const double *field_aos, int nx, int ny, const double vs[2], double *J,
+                       cudaStream_t s) {
+    const long V = (long)nx * ny;
+    count_launch(), jacobian2d_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, nx, ny,
+                                                                  1.0 / (vs[0] * vs[1]), J);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void jacobian2d(const double *field_host, int nx, int ny, const double vs[2], double *J_host) {
+    BINDER_CHECK(nx > 0 && ny > 0, "dimensions must be positive");
+    const long V = (long)nx * ny;
+    cudaStream_t s = nullptr;
+    BINDER_CUDA(cudaStreamCreate(&s));
+    try {
+        DBuf<double> f(V * 2, s), J(V, s);
+        BINDER_CUDA(cudaMemcpyAsync(f.p, field_host, sizeof(double) * V * 2, cudaMemcpyHostToDevice, s));
+        jacobian2d_device(f.p, nx, ny, vs, J.p, s);
+        BINDER_CUDA(cudaMemcpyAsync(J_host, J.p, sizeof(double) * V, cudaMemcpyDeviceToHost, s));
+        BINDER_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    cudaStreamSynchronize(s);  // the buffers' stream-ordered frees
+    cudaStreamDestroy(s);
 }
 
 // ---- Jacobian through a fixed device scratch array ------------------------------------------

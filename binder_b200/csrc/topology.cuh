@@ -15,6 +15,12 @@ struct JacStats {
 void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const double vs[3],
                        double *J, cudaStream_t s);
 
+// 2D: the 4-corner Jacobian (BINDER/src/cpu/utils.cpp:10-98) of an AoS [nx][ny][2] field, FP64
+void jacobian2d_device(const double *field_aos, int nx, int ny, const double vs[2], double *J,
+                       cudaStream_t s);
+// the same from host memory into host memory (device buffers from the pool, own stream)
+void jacobian2d(const double *field_host, int nx, int ny, const double vs[2], double *J_host);
+
 // The same determinants from a host AoS field into host J, staged through a fixed array in the
 // library's device image instead of allocated buffers (grids up to kJacobianNoAllocMaxVoxels).
 // Runs on the legacy default stream of the current device and returns when J is on the host.

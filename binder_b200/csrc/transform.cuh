@@ -59,6 +59,7 @@ struct AxisArgs {
     // positions epilogue
     const float *xpos;  // SoA voxel positions or null for the identity grid
     int ny, nz;
+    int dims;           // 3, or 2 for an nx x ny image (nz = 1, components x, y)
     // Poisson epilogue: the periodic Laplacian symbol is 6 - 2cos_x - 2cos_y - 2cos_z
     const double *cos_x, *cos_y, *cos_z;  // cos(2 pi k / n) per axis
     double out_scale[3];   // kEpiTopoOut: per-component scale (voxel size / total)

@@ -47,6 +47,7 @@ struct UArgs {
     // positions epilogue
     const float *xpos;
     int ny, nz;
+    int dims;  // 3, or 2 for an image (the contiguous axis is then component 1)
     const int *skip;
 };
 
@@ -308,8 +309,9 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
             // `lane` of this warp and the row loop broadcasts it
             float rowc = 0.0f;
             if (MODE == kEpiPositions && !a.xpos) {
-                const int gi = (int)(l0 + warp * 32 + lane);
-                rowc = comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny);
+                const int gi = (int)(l0 + warp * 32 + lane);  // 3D: x * ny + y; 2D: x
+                rowc = a.dims == 2 ? (float)gi
+                                   : (comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
             }
             for (int cc = 0; cc < nchunks; ++cc) {
                 float v[32];
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                         float val = stg[r * 33 + lane];
                         if (MODE == kEpiPositions)
                             val += a.xpos ? __ldg(a.xpos + comp * a.V + g * n + k)
-                                          : (comp == 2 ? (float)k : rc);
+                                          : (comp == a.dims - 1 ? (float)k : rc);
                         out[g * n + k] = val;
                     }
                 }
@@ -483,7 +485,7 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     a.D = b.D; a.st = b.st; a.sigma2 = b.sigma2; a.sample = b.sample; a.want_raw = b.want_raw;
     a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
     for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
-    a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.skip = b.skip;
+    a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.skip = b.skip;
 #define BINDER_UMMA_CASE(MODE)                                                    \
     case MODE:                                                                    \
         if (planes == 2) launch_umma<MODE, 2>(a, ncomp, s);                       \

@@ -178,6 +178,11 @@ int binder_transform_get_shape(const binder_transform *h, int out[4]);
 int binder_jacobian_determinant_3d(const double *field, int Nx, int Ny, int Nz, double voxel_size_x,
                                    double voxel_size_y, double voxel_size_z, double *J_out);
 
+/* compute_jacobian_determinant_2D(field, Nx, Ny, vx, vy) -> [Nx,Ny]   cpu/bindings.cpp:535-560
+ * field AoS [Nx*Ny*2]; FP64, the reference's arithmetic (bit-identical). */
+int binder_jacobian_determinant_2d(const double *field, int Nx, int Ny, double voxel_size_x,
+                                   double voxel_size_y, double *J_out);
+
 /* No counterpart in the reference: binder_jacobian_determinant_3d without any device allocation.
  * The call above allocates device buffers for the field and the determinants (cudaMalloc) and
  * frees them (cudaFree) every time.  Some callers cannot do that: a framework whose caching
