@@ -20,7 +20,7 @@ backend = "b200"
 has_topology_correction = True
 
 __all__ = ["backend", "has_topology_correction", "Registration", "NonLinearTransformation",
-           "topology_correction_3D", "compute_jacobian_determinant_3D",
+           "topology_correction_3D", "topology_correction_2D", "compute_jacobian_determinant_3D",
            "compute_jacobian_determinant_2D", "BinderError"]
 
 
@@ -190,9 +190,14 @@ class Registration:
         """Topology correction of this object's positions on the device, in place (replaces the
         host round trip of FastRegistration.py:527-546).  Returns the iteration / count stats."""
         stats = np.zeros(6, np.int64)
+        vs = np.ones(3, np.float64)
+        v = np.asarray(voxel_sizes, np.float64).ravel()
+        if v.size not in (self._N, 3):
+            raise ValueError(f"voxel_sizes has {v.size} elements, expected {self._N}")
+        vs[:v.size] = v
         check(lib().binder_registration_correct_topology(
-            self._h, float(e1), float(e2), int(max_outer_it), int(max_it),
-            _f64(voxel_sizes, 3, "voxel_sizes"), stats.ctypes.data))
+            self._h, float(e1), float(e2), int(max_outer_it), int(max_it), vs,
+            stats.ctypes.data))
         return dict(zip(["outer_iterations", "inner_iterations", "below_e1_before",
                          "below_e1_after", "above_e2_before", "above_e2_after"], stats.tolist()))
 
@@ -265,6 +270,27 @@ class topology_correction_3D:
                                     "below_e1_after", "above_e2_before", "above_e2_after"],
                                    stats.tolist()))
         return out.reshape(int(Nx_v), int(Ny_v), int(Nz_v), 3)
+
+
+class topology_correction_2D:
+    """``_core.topology_correction_2D`` (cpu/bindings.cpp:447-480); FP64 throughout."""
+
+    def __init__(self):
+        self.last_stats = None
+
+    def correct_topology(self, h_init, e1, e2, max_outer_it, max_it, threads, voxel_sizes, Nx_v,
+                         Ny_v):
+        V = int(Nx_v) * int(Ny_v)
+        field = _f64(h_init, V * 2, "h_init")
+        out = np.zeros(V * 2, np.float64)
+        stats = np.zeros(6, np.int64)
+        check(lib().binder_topology_correct_2d(
+            field, float(e1), float(e2), int(max_outer_it), int(max_it), int(threads),
+            _f64(voxel_sizes, 2, "voxel_sizes"), int(Nx_v), int(Ny_v), out, stats.ctypes.data))
+        self.last_stats = dict(zip(["outer_iterations", "inner_iterations", "below_e1_before",
+                                    "below_e1_after", "above_e2_before", "above_e2_after"],
+                                   stats.tolist()))
+        return out.reshape(int(Nx_v), int(Ny_v), 2)
 
 
 def kernel_launch_count():

@@ -34,6 +34,7 @@ EXPORTS = [
     "binder_transform_create", "binder_transform_destroy",
     "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
     "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
+    "binder_topology_correct_2d",
     "binder_jacobian_determinant_3d_noalloc", "binder_jacobian_noalloc_max_voxels",
     "binder_jacobian_determinant_2d",
 ]
@@ -95,6 +96,7 @@ def _declare(lib):
         "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],
+        "binder_topology_correct_2d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _f64, _P],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

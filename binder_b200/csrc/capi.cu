@@ -376,6 +376,31 @@ int binder_jacobian_determinant_2d(const double *field, int Nx, int Ny, double v
     });
 }
 
+int binder_topology_correct_2d(const double *field, double e1, double e2, int max_outer_it,
+                               int max_it, int threads, const double voxel_sizes[2], int Nx,
+                               int Ny, double *out, long long *stats_out) {
+    (void)threads;
+    return guard([&] {
+        NEED(field);
+        NEED(voxel_sizes);
+        NEED(out);
+        BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
+                     "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
+        const long V = (long)Nx * Ny;
+        if (out != field) std::memcpy(out, field, sizeof(double) * V * 2);
+        const auto r = binder::topology_correct_2d(out, e1, e2, max_outer_it, max_it, voxel_sizes,
+                                                   Nx, Ny, 0);
+        if (stats_out) {
+            stats_out[0] = r.outer_iterations;
+            stats_out[1] = r.inner_iterations;
+            stats_out[2] = r.below_before;
+            stats_out[3] = r.below_after;
+            stats_out[4] = r.above_before;
+            stats_out[5] = r.above_after;
+        }
+    });
+}
+
 int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
                                int max_it, int threads, const double voxel_sizes[3], int Nx,
                                int Ny, int Nz, double *out, long long *stats_out) {

@@ -633,8 +633,6 @@ TopologyResult Registration::correct_topology(double e1, double e2, int max_oute
                                               const double vs[3]) {
     BINDER_CHECK(e1 <= 1.0 && e2 >= 1.0 && e1 < e2,
                  "topology correction needs e1 <= 1 <= e2 (the identity must be admissible)");
-    if (N_ == 2)
-        throw Error(kUnsupported, "topology correction of a 2D registration is not built");
     if (!topo_) topo_ = new TopologyWorkspace(nx_, ny_, nz_, own_stream_);
     topo_->load_float_grid(d_, vs, stream_);
     TopologyResult r = topo_->run(e1, e2, max_outer, max_inner, vs, stream_);

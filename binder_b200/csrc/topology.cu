@@ -110,14 +110,18 @@ __global__ void jacobian_kernel(const double *f, long ps, long cs, int nx, int n
 
 // BINDER/src/cpu/utils.cpp:10-98: the 2D Jacobian averaged over the 4 one-sided corners (orders
 // fxfy, bxfy, fxby, bxby), each the determinant of the forward / backward differences, with the
-// reference's expression grouping.  Field AoS [nx][ny][2].
-__global__ void jacobian2d_kernel(const double *f, int nx, int ny, double vol, double *J) {
+// reference's expression grouping.  Element (p, m) of the field is f[p*ps + m*cs]; J and red are
+// optional, as in jacobian_kernel.
+__global__ void jacobian2d_kernel(const double *f, long ps, long cs, int nx, int ny, double vol,
+                                  double *J, double e1, double e2, Red *red) {
     const long V = (long)nx * ny;
     const int dir[4][2] = {{1, 1}, {-1, 1}, {1, -1}, {-1, -1}};
+    double lmin = 1e300, lmax = -1e300;
+    unsigned long long lb = 0, la = 0, ln = 0;
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
          p += (long)gridDim.x * blockDim.x) {
         const int x = (int)(p / ny), y = (int)(p % ny);
-        const double w0 = f[p * 2], w1 = f[p * 2 + 1];
+        const double w0 = f[p * ps], w1 = f[p * ps + cs];
         double tot = 0.0;
         int valid = 0;
 #pragma unroll
@@ -126,14 +130,38 @@ __global__ void jacobian2d_kernel(const double *f, int nx, int ny, double vol, d
             if ((sx > 0 && x >= nx - 1) || (sx < 0 && x <= 0)) continue;
             if ((sy > 0 && y >= ny - 1) || (sy < 0 && y <= 0)) continue;
             const long qx = p + (long)sx * ny, qy = p + sy;
-            const double ax0 = sx > 0 ? f[qx * 2] - w0 : w0 - f[qx * 2];
-            const double ax1 = sx > 0 ? f[qx * 2 + 1] - w1 : w1 - f[qx * 2 + 1];
-            const double ay0 = sy > 0 ? f[qy * 2] - w0 : w0 - f[qy * 2];
-            const double ay1 = sy > 0 ? f[qy * 2 + 1] - w1 : w1 - f[qy * 2 + 1];
+            const double bx0 = f[qx * ps], bx1 = f[qx * ps + cs];
+            const double by0 = f[qy * ps], by1 = f[qy * ps + cs];
+            const double ax0 = sx > 0 ? bx0 - w0 : w0 - bx0;
+            const double ax1 = sx > 0 ? bx1 - w1 : w1 - bx1;
+            const double ay0 = sy > 0 ? by0 - w0 : w0 - by0;
+            const double ay1 = sy > 0 ? by1 - w1 : w1 - by1;
             tot += (ax0 * ay1 - ay0 * ax1) * vol;
             valid++;
         }
-        J[p] = valid > 0 ? tot / valid : 1.0;
+        const double jv = valid > 0 ? tot / valid : 1.0;
+        if (J) J[p] = jv;
+        lmin = fmin(lmin, jv);
+        lmax = fmax(lmax, jv);
+        lb += jv < e1;
+        la += jv > e2;
+        ln += jv < 0.0;
+    }
+    if (red) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+            lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+            lb += __shfl_xor_sync(0xffffffffu, lb, o);
+            la += __shfl_xor_sync(0xffffffffu, la, o);
+            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&red->mn, ordered(lmin));
+            atomicMax(&red->mx, ordered(lmax));
+            if (lb) atomicAdd(&red->below, lb);
+            if (la) atomicAdd(&red->above, la);
+            if (ln) atomicAdd(&red->negative, ln);
+        }
     }
 }
 
@@ -331,35 +359,198 @@ __global__ void divergence_kernel(const double *g, int nx, int ny, int nz, doubl
     }
 }
 
-__global__ void sum_kernel(const double *pos, long V, Red *red) {
+// topology_correction_2D.cpp:165-207: the 4 corner Jacobians of every cell in the vertex order
+// 00, 10, 01, 11 (the reference's Jff, Jbf, Jfb, Jbb).  Corner (vx, vy) pairs the x edge at
+// y + vy with the y edge at x + vx (hi - lo each).  `below` / `above` count cells with a corner
+// out of range, as the reference's counters do.  Positions are SoA [2][V].
+__global__ void corner2d_kernel(const double *pos, int nx, int ny, double vol, double e1,
+                                double e2, double *Jc, Red *red) {
+    const long V = (long)nx * ny;
+    const long cy = ny - 1;
+    const long cells = (long)(nx - 1) * cy;
+    unsigned long long lb = 0, la = 0;
+    for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < cells;
+         cell += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(cell / cy), y = (int)(cell % cy);
+        const long p00 = (long)x * ny + y, p10 = p00 + ny;
+        const double X00 = pos[p00], X01 = pos[p00 + 1], X10 = pos[p10], X11 = pos[p10 + 1];
+        const double Y00 = pos[V + p00], Y01 = pos[V + p00 + 1], Y10 = pos[V + p10],
+                     Y11 = pos[V + p10 + 1];
+        bool lo = false, hi = false;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int vx = c & 1, vy = c >> 1;
+            // x edge at y + vy, y edge at x + vx
+            const double ex0 = vy ? X11 - X01 : X10 - X00, ex1 = vy ? Y11 - Y01 : Y10 - Y00;
+            const double ey0 = vx ? X11 - X10 : X01 - X00, ey1 = vx ? Y11 - Y10 : Y01 - Y00;
+            const double j = (ex0 * ey1 - ey0 * ex1) * vol;
+            Jc[cell * 4 + c] = j;
+            lo |= j < e1;
+            hi |= j > e2;
+        }
+        lb += lo;
+        la += hi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lb += __shfl_xor_sync(0xffffffffu, lb, o);
+        la += __shfl_xor_sync(0xffffffffu, la, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (lb) atomicAdd(&red->below, lb);
+        if (la) atomicAdd(&red->above, la);
+    }
+}
+
+// topology_correction_2D.cpp:209-246: periodic forward differences, g[(n1*2+n2)][p] =
+// (pos_n1(p + e_n2) - pos_n1(p)) / vs[n1]
+__global__ void gradient2d_kernel(const double *pos, int nx, int ny, double v0, double v1,
+                                  double *g) {
+    const long V = (long)nx * ny;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / ny), y = (int)(p % ny);
+        const long px = (long)(x + 1 > nx - 1 ? x + 1 - nx : x + 1) * ny + y;
+        const long py = (long)x * ny + (y + 1 > ny - 1 ? y + 1 - ny : y + 1);
+        const double c0 = pos[p], c1 = pos[V + p];
+        g[0 * V + p] = (pos[px] - c0) / v0;
+        g[1 * V + p] = (pos[py] - c0) / v0;
+        g[2 * V + p] = (pos[V + px] - c1) / v1;
+        g[3 * V + p] = (pos[V + py] - c1) / v1;
+    }
+}
+
+__global__ void flag_cells2d_kernel(const double *Jc, int nx, int ny, double e1, double e2,
+                                    int *list, Red *red) {
+    const long cells = (long)(nx - 1) * (ny - 1);
+    for (long cell = (long)blockIdx.x * blockDim.x + threadIdx.x; cell < cells;
+         cell += (long)gridDim.x * blockDim.x) {
+        bool any = false;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double j = Jc[cell * 4 + c];
+            any |= (j < e1 || j > e2);
+        }
+        if (any) list[atomicAdd(&red->count, 1)] = (int)cell;
+    }
+}
+
+// topology_correction_2D.cpp:248-313.  Cells are visited in lexicographic order and a cell's 4
+// corners in order; a cell touches gradients only at its own 2x2 nodes, so two cells interact
+// only if they differ by at most 1 along both axes.  Level 2x + y orders every such pair as the
+// lexicographic walk does and never puts two of them on one level, so levels in increasing order
+// (cells of one level in parallel) reproduce the sequential result exactly.  Column n2 of a
+// corner's matrix is read at the corner's vertex with its n2 bit cleared.  One CTA.
+__global__ void __launch_bounds__(1024) limiter2d_kernel(const int *list, int *sorted,
+                                                         const double *Jc, double *g, int nx,
+                                                         int ny, double e1, double e2, int nlev,
+                                                         Red *red, unsigned *flags) {
+    extern __shared__ int sh[];
+    int *off = sh;             // nlev + 1
+    int *cur = sh + nlev + 1;  // nlev
+    const long V = (long)nx * ny;
+    const long cy = ny - 1;
+    const int n = red->count;
+    for (int l = threadIdx.x; l < nlev + 1; l += blockDim.x) off[l] = 0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const long cell = list[q];
+        atomicAdd(&off[2 * (int)(cell / cy) + (int)(cell % cy) + 1], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int l = 0; l < nlev; ++l) off[l + 1] += off[l];
+    __syncthreads();
+    for (int l = threadIdx.x; l < nlev; l += blockDim.x) cur[l] = off[l];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const long cell = list[q];
+        sorted[atomicAdd(&cur[2 * (int)(cell / cy) + (int)(cell % cy)], 1)] = (int)cell;
+    }
+    __syncthreads();
+    bool capped = false;
+    for (int l = 0; l < nlev; ++l) {
+        const int beg = off[l], end = off[l + 1];
+        if (beg == end) continue;  // uniform: every thread reads the same shared value
+        for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+            const long cell = sorted[q];
+            const int x = (int)(cell / cy), y = (int)(cell % cy);
+            for (int c = 0; c < 4; ++c) {
+                const double jv = Jc[cell * 4 + c];
+                if (!(jv < e1 || jv > e2)) continue;
+                const int vx = c & 1, vy = c >> 1;
+                const long gp[2] = {(long)x * ny + (y + vy), (long)(x + vx) * ny + y};
+                double J[2][2];
+                for (int n1 = 0; n1 < 2; ++n1)
+                    for (int n2 = 0; n2 < 2; ++n2) J[n1][n2] = g[(n1 * 2 + n2) * V + gp[n2]];
+                double alpha = 0.0;
+                double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                int steps = 0;
+                while (det > e2 || det < e1) {
+                    if (++steps > 11) {  // alpha == 1 (identity) already tried: [e1, e2] misses 1
+                        capped = true;
+                        break;
+                    }
+                    alpha += 0.1;
+                    if (alpha > 1.0) alpha = 1.0;
+                    double Jn[2][2];
+                    for (int n1 = 0; n1 < 2; ++n1)
+                        for (int n2 = 0; n2 < 2; ++n2)
+                            Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                    det = Jn[0][0] * Jn[1][1] - Jn[0][1] * Jn[1][0];
+                }
+                alpha += 0.1;
+                if (alpha > 1.0) alpha = 1.0;
+                for (int n1 = 0; n1 < 2; ++n1)
+                    for (int n2 = 0; n2 < 2; ++n2)
+                        g[(n1 * 2 + n2) * V + gp[n2]] =
+                            (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+            }
+        }
+        __syncthreads();
+    }
+    if (capped) atomicOr(flags, (unsigned)kFlagLimiterCapped);
+}
+
+// backward-difference divergence (periodic) of each component's 2D gradient row
+__global__ void divergence2d_kernel(const double *g, int nx, int ny, double *div) {
+    const long V = (long)nx * ny;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p / ny), y = (int)(p % ny);
+        const long px = (long)(x == 0 ? nx - 1 : x - 1) * ny + y;
+        const long py = (long)x * ny + (y == 0 ? ny - 1 : y - 1);
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+            const double *gx = g + (n * 2 + 0) * V, *gy = g + (n * 2 + 1) * V;
+            div[n * V + p] = (gx[p] - gx[px]) + (gy[p] - gy[py]);
+        }
+    }
+}
+
+__global__ void sum_kernel(const double *pos, long V, int N, Red *red) {
     double s[3] = {0.0, 0.0, 0.0};
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
          p += (long)gridDim.x * blockDim.x)
-        for (int n = 0; n < 3; ++n) s[n] += pos[n * V + p];
-    for (int n = 0; n < 3; ++n) {
+        for (int n = 0; n < N; ++n) s[n] += pos[n * V + p];
+    for (int n = 0; n < N; ++n) {
         double v = warp_sum(s[n]);
         if ((threadIdx.x & 31) == 0) atomicAdd(&red->sum[n], v);
     }
 }
 
-// AoS grid-unit field -> SoA physical (scale) and back
-__global__ void aos_to_soa_kernel(const double *aos, long V, double s0, double s1, double s2,
-                                  double *soa) {
+// AoS grid-unit field [V][N] -> SoA physical [N][V] (times the voxel size) and back
+struct Scale {
+    double v[3];
+};
+__global__ void aos_to_soa_kernel(const double *aos, long V, int N, Scale sc, double *soa) {
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
-         p += (long)gridDim.x * blockDim.x) {
-        soa[p] = aos[p * 3 + 0] * s0;
-        soa[V + p] = aos[p * 3 + 1] * s1;
-        soa[2 * V + p] = aos[p * 3 + 2] * s2;
-    }
+         p += (long)gridDim.x * blockDim.x)
+        for (int n = 0; n < N; ++n) soa[n * V + p] = aos[p * N + n] * sc.v[n];
 }
-__global__ void soa_to_aos_kernel(const double *soa, long V, double s0, double s1, double s2,
-                                  double *aos) {
+__global__ void soa_to_aos_kernel(const double *soa, long V, int N, Scale sc, double *aos) {
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
-         p += (long)gridDim.x * blockDim.x) {
-        aos[p * 3 + 0] = soa[p] / s0;
-        aos[p * 3 + 1] = soa[V + p] / s1;
-        aos[p * 3 + 2] = soa[2 * V + p] / s2;
-    }
+         p += (long)gridDim.x * blockDim.x)
+        for (int n = 0; n < N; ++n) aos[p * N + n] = soa[n * V + p] / sc.v[n];
 }
 
 int grid_for(long work) {
@@ -409,8 +600,8 @@ void jacobian3d_device(const double *field_aos, int nx, int ny, int nz, const do
 void jacobian2d_device(const double *field_aos, int nx, int ny, const double vs[2], double *J,
                        cudaStream_t s) {
     const long V = (long)nx * ny;
-    count_launch(), jacobian2d_kernel<<<grid_for(V), 256, 0, s>>>(field_aos, nx, ny,
-                                                                  1.0 / (vs[0] * vs[1]), J);
+    count_launch(), jacobian2d_kernel<<<grid_for(V), 256, 0, s>>>(
+                        field_aos, 2, 1, nx, ny, 1.0 / (vs[0] * vs[1]), J, 0.0, 0.0, nullptr);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -511,28 +702,21 @@ void jacobian3d_noalloc(const double *field_host, int nx, int ny, int nz, const 
 }
 
 namespace {
-__global__ void float_soa_to_physical_kernel(const float *d, long V, double s0, double s1, double s2,
-                                             double *pos) {
+__global__ void float_soa_to_physical_kernel(const float *d, long V, int N, Scale sc, double *pos) {
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
-         p += (long)gridDim.x * blockDim.x) {
-        pos[p] = (double)d[p] * s0;
-        pos[V + p] = (double)d[V + p] * s1;
-        pos[2 * V + p] = (double)d[2 * V + p] * s2;
-    }
+         p += (long)gridDim.x * blockDim.x)
+        for (int n = 0; n < N; ++n) pos[n * V + p] = (double)d[n * V + p] * sc.v[n];
 }
-__global__ void physical_to_float_soa_kernel(const double *pos, long V, double s0, double s1,
-                                             double s2, float *d) {
+__global__ void physical_to_float_soa_kernel(const double *pos, long V, int N, Scale sc, float *d) {
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < V;
-         p += (long)gridDim.x * blockDim.x) {
-        d[p] = (float)(pos[p] / s0);
-        d[V + p] = (float)(pos[V + p] / s1);
-        d[2 * V + p] = (float)(pos[2 * V + p] / s2);
-    }
+         p += (long)gridDim.x * blockDim.x)
+        for (int n = 0; n < N; ++n) d[n * V + p] = (float)(pos[n * V + p] / sc.v[n]);
 }
 }  // namespace
 
 struct TopologyWorkspace::Impl {
     int nx, ny, nz;
+    int N;  // 3, or 2 for an image (nz == 1)
     long V, cells;
     DBuf<double> pos, grad, jc, div, t1, t2;
     DBuf<int> list, sorted;
@@ -540,9 +724,11 @@ struct TopologyWorkspace::Impl {
     DBuf<unsigned> flags;
     DBuf<double> H[3], cs[3];
     Impl(int x, int y, int z, cudaStream_t st)
-        : nx(x), ny(y), nz(z), V((long)x * y * z), cells((long)(x - 1) * (y - 1) * (z - 1)),
-          pos(V * 3, st), grad(V * 9, st), jc(cells * 8, st), div(V * 3, st), t1(V * 3, st),
-          t2(V * 3, st), list(cells, st), sorted(cells, st), red(1, st), flags(1, st),
+        : nx(x), ny(y), nz(z), N(z == 1 ? 2 : 3), V((long)x * y * z),
+          cells(z == 1 ? (long)(x - 1) * (y - 1) : (long)(x - 1) * (y - 1) * (z - 1)),
+          pos(V * N, st), grad(V * N * N, st), jc(cells * (z == 1 ? 4 : 8), st), div(V * N, st),
+          t1(V * N, st), t2(V * N, st), list(cells, st), sorted(cells, st), red(1, st),
+          flags(1, st),
           H{DBuf<double>((size_t)x * x, st), DBuf<double>((size_t)y * y, st),
             DBuf<double>((size_t)z * z, st)},
           cs{DBuf<double>(x, st), DBuf<double>(y, st), DBuf<double>(z, st)} {
@@ -563,7 +749,8 @@ struct TopologyWorkspace::Impl {
 };
 
 TopologyWorkspace::TopologyWorkspace(int nx, int ny, int nz, cudaStream_t s) {
-    BINDER_CHECK(nx >= 2 && ny >= 2 && nz >= 2, "topology correction needs at least 2 voxels per axis");
+    BINDER_CHECK(nx >= 2 && ny >= 2 && (nz >= 2 || nz == 1),
+                 "topology correction needs at least 2 voxels per axis (nz == 1 for an image)");
     BINDER_CHECK(nx <= 256 && ny <= 256 && nz <= 256, "topology correction supports axes up to 256");
     impl_ = new Impl(nx, ny, nz, s);
 }
@@ -573,6 +760,7 @@ double *TopologyWorkspace::positions() { return impl_->pos.p; }
 // BINDER/src/cpu/topology_correction_3D.cpp:17-143 on the workspace's SoA physical positions
 TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int max_inner,
                                       const double vs[3], cudaStream_t s) {
+    if (impl_->N == 2) return run2d(e1, e2, max_outer, max_inner, vs, s);
     BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
     Impl &w = *impl_;
     const int nx = w.nx, ny = w.ny, nz = w.nz;
@@ -617,7 +805,7 @@ TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int m
             count_launch(), limiter_kernel<<<1, 1024, lim_smem, s>>>(w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny,
                                                      nz, e1, e2, nlev, w.red.p, w.flags.p);
             BINDER_CUDA(cudaGetLastError());
-            count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, w.red.p);
+            count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, 3, w.red.p);
             count_launch(), divergence_kernel<<<grid_for(V), 256, 0, s>>>(w.grad.p, nx, ny, nz, w.div.p);
             BINDER_CUDA(cudaGetLastError());
             Red sr = read_red(w.red.p, s);
@@ -667,15 +855,114 @@ TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int m
     return res;
 }
 
+// BINDER/src/cpu/topology_correction_2D.cpp:17-163: the 3D loop structure with 4 corners per
+// cell, 2x2 gradient matrices and a 2D Poisson solve (separable Hartley passes y, [x fused], y)
+TopologyResult TopologyWorkspace::run2d(double e1, double e2, int max_outer, int max_inner,
+                                        const double vs[3], cudaStream_t s) {
+    BINDER_CHECK(vs[0] > 0 && vs[1] > 0, "voxel sizes must be positive");
+    Impl &w = *impl_;
+    const int nx = w.nx, ny = w.ny;
+    const long V = w.V, cells = w.cells;
+    const double vol = 1.0 / (vs[0] * vs[1]);
+    TopologyResult res{};
+    BINDER_CUDA(cudaMemsetAsync(w.flags.p, 0, sizeof(unsigned), s));
+
+    auto jac_stats = [&]() {
+        reset_red(w.red.p, s);
+        count_launch(), jacobian2d_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, 1, V, nx, ny, vol,
+                                                                      nullptr, e1, e2, w.red.p);
+        BINDER_CUDA(cudaGetLastError());
+        return read_red(w.red.p, s);
+    };
+    auto corners = [&]() {
+        reset_red(w.red.p, s);
+        count_launch(), corner2d_kernel<<<grid_for(cells), 256, 0, s>>>(w.pos.p, nx, ny, vol, e1,
+                                                                        e2, w.jc.p, w.red.p);
+        BINDER_CUDA(cudaGetLastError());
+        return read_red(w.red.p, s);
+    };
+
+    Red r = jac_stats();
+    double jmin = unordered(r.mn), jmax = unordered(r.mx);
+    res.below_before = (long long)r.below;
+    res.above_before = (long long)r.above;
+    const int nlev = 2 * (nx - 2) + (ny - 2) + 1;
+    const size_t lim_smem = sizeof(int) * (2 * (size_t)nlev + 1);
+    BINDER_CUDA(cudaFuncSetAttribute(limiter2d_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim_smem));
+    int outer = 0;
+    while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+        Red c = corners();
+        int inner = 0;
+        while ((c.below > 0 || c.above > 0) && inner < max_inner) {
+            count_launch(), gradient2d_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, nx, ny, vs[0],
+                                                                          vs[1], w.grad.p);
+            reset_red(w.red.p, s);
+            count_launch(), flag_cells2d_kernel<<<grid_for(cells), 256, 0, s>>>(
+                                w.jc.p, nx, ny, e1, e2, w.list.p, w.red.p);
+            count_launch(), limiter2d_kernel<<<1, 1024, lim_smem, s>>>(
+                                w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny, e1, e2, nlev,
+                                w.red.p, w.flags.p);
+            BINDER_CUDA(cudaGetLastError());
+            count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, 2, w.red.p);
+            count_launch(), divergence2d_kernel<<<grid_for(V), 256, 0, s>>>(w.grad.p, nx, ny,
+                                                                            w.div.p);
+            BINDER_CUDA(cudaGetLastError());
+            Red sr = read_red(w.red.p, s);
+            double mean[2];
+            for (int n = 0; n < 2; ++n) mean[n] = sr.sum[n] / (nx * ny);
+
+            // u = -(1/V) H (H div / lambda) on the nx x ny grid (the volume nx x ny x 1, whose
+            // unit z axis contributes cos 0 = 1 to lambda = 6 - 2cos_x - 2cos_y - 2cos_z)
+            AxisArgs<double> a{};
+            a.comp_stride = V;
+            a.ny = ny;
+            a.nz = 1;
+            a.cos_x = w.cs[0].p;
+            a.cos_y = w.cs[1].p;
+            a.cos_z = w.cs[2].p;
+            a.in = w.div.p; a.out = w.t1.p; a.M = w.H[1].p; a.n = ny; a.outer = nx; a.s = 1;
+            launch_axis_pass(a, kEpiNone, 2, s);
+            a.in = w.t1.p; a.out = w.t2.p; a.M = w.H[0].p; a.M2 = w.H[0].p; a.n = nx; a.outer = 1;
+            a.s = ny;
+            launch_axis_pass(a, kEpiPoisson, 2, s);
+            // last pass: physical positions u * vs + mean
+            a.in = w.t2.p; a.out = w.pos.p; a.M = w.H[1].p; a.M2 = nullptr; a.n = ny; a.outer = nx;
+            a.s = 1;
+            for (int n = 0; n < 2; ++n) {
+                a.out_scale[n] = vs[n];
+                a.out_offset[n] = mean[n];
+            }
+            launch_axis_pass(a, kEpiTopoOut, 2, s);
+            c = corners();
+            inner++;
+            res.inner_iterations++;
+        }
+        r = jac_stats();
+        jmin = unordered(r.mn);
+        jmax = unordered(r.mx);
+        outer++;
+    }
+    res.outer_iterations = outer;
+    r = jac_stats();
+    res.below_after = (long long)r.below;
+    res.above_after = (long long)r.above;
+    BINDER_CUDA(cudaMemcpyAsync(&res.flags, w.flags.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));
+    return res;
+}
+
 void TopologyWorkspace::load_float_grid(const float *d_soa, const double vs[3], cudaStream_t s) {
-    count_launch(), float_soa_to_physical_kernel<<<grid_for(impl_->V), 256, 0, s>>>(d_soa, impl_->V, vs[0], vs[1],
-                                                                    vs[2], impl_->pos.p);
+    const Scale sc{{vs[0], vs[1], vs[2]}};
+    count_launch(), float_soa_to_physical_kernel<<<grid_for(impl_->V), 256, 0, s>>>(
+                        d_soa, impl_->V, impl_->N, sc, impl_->pos.p);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void TopologyWorkspace::store_float_grid(float *d_soa, const double vs[3], cudaStream_t s) {
-    count_launch(), physical_to_float_soa_kernel<<<grid_for(impl_->V), 256, 0, s>>>(impl_->pos.p, impl_->V, vs[0],
-                                                                    vs[1], vs[2], d_soa);
+    const Scale sc{{vs[0], vs[1], vs[2]}};
+    count_launch(), physical_to_float_soa_kernel<<<grid_for(impl_->V), 256, 0, s>>>(
+                        impl_->pos.p, impl_->V, impl_->N, sc, d_soa);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -683,16 +970,33 @@ TopologyResult topology_correct_3d(double *host, double e1, double e2, int max_o
                                    int max_inner, const double vs[3], int nx, int ny, int nz,
                                    cudaStream_t s) {
     BINDER_CHECK(vs[0] > 0 && vs[1] > 0 && vs[2] > 0, "voxel sizes must be positive");
+    BINDER_CHECK(nz >= 2, "a 3D field needs nz >= 2 (use the 2D entry point for images)");
+    return topology_correct(host, e1, e2, max_outer, max_inner, vs, nx, ny, nz, s);
+}
+
+TopologyResult topology_correct_2d(double *host, double e1, double e2, int max_outer,
+                                   int max_inner, const double vs[2], int nx, int ny,
+                                   cudaStream_t s) {
+    BINDER_CHECK(vs[0] > 0 && vs[1] > 0, "voxel sizes must be positive");
+    const double vs3[3] = {vs[0], vs[1], 1.0};
+    return topology_correct(host, e1, e2, max_outer, max_inner, vs3, nx, ny, 1, s);
+}
+
+// host AoS field (grid units) -> device SoA physical -> correction -> back, in place
+TopologyResult topology_correct(double *host, double e1, double e2, int max_outer, int max_inner,
+                                const double vs[3], int nx, int ny, int nz, cudaStream_t s) {
     TopologyWorkspace ws(nx, ny, nz, s);
     const long V = (long)nx * ny * nz;
-    DBuf<double> aos(V * 3, s);
-    BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));
-    count_launch(), aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, vs[0], vs[1], vs[2], ws.positions());
+    const int N = nz == 1 ? 2 : 3;
+    const Scale sc{{vs[0], vs[1], vs[2]}};
+    DBuf<double> aos(V * N, s);
+    BINDER_CUDA(cudaMemcpyAsync(aos.p, host, sizeof(double) * V * N, cudaMemcpyHostToDevice, s));
+    count_launch(), aos_to_soa_kernel<<<grid_for(V), 256, 0, s>>>(aos.p, V, N, sc, ws.positions());
     BINDER_CUDA(cudaGetLastError());
     TopologyResult res = ws.run(e1, e2, max_outer, max_inner, vs, s);
-    count_launch(), soa_to_aos_kernel<<<grid_for(V), 256, 0, s>>>(ws.positions(), V, vs[0], vs[1], vs[2], aos.p);
+    count_launch(), soa_to_aos_kernel<<<grid_for(V), 256, 0, s>>>(ws.positions(), V, N, sc, aos.p);
     BINDER_CUDA(cudaGetLastError());
-    BINDER_CUDA(cudaMemcpyAsync(host, aos.p, sizeof(double) * V * 3, cudaMemcpyDeviceToHost, s));
+    BINDER_CUDA(cudaMemcpyAsync(host, aos.p, sizeof(double) * V * N, cudaMemcpyDeviceToHost, s));
     BINDER_CUDA(cudaStreamSynchronize(s));
     return res;
 }

@@ -40,9 +40,18 @@ struct TopologyResult {
 TopologyResult topology_correct_3d(double *field_aos_host, double e1, double e2, int max_outer,
                                    int max_inner, const double vs[3], int nx, int ny, int nz,
                                    cudaStream_t s);
+// BINDER/src/cpu/topology_correction_2D.cpp:17-163 on a host AoS [nx][ny][2] field (in place)
+TopologyResult topology_correct_2d(double *field_aos_host, double e1, double e2, int max_outer,
+                                   int max_inner, const double vs[2], int nx, int ny,
+                                   cudaStream_t s);
+// either of the two (nz == 1: an image with two components)
+TopologyResult topology_correct(double *field_aos_host, double e1, double e2, int max_outer,
+                                int max_inner, const double vs[3], int nx, int ny, int nz,
+                                cudaStream_t s);
 
 // Device buffers of the correction for one grid (positions, gradients, corner Jacobians, Poisson
-// work space), reusable across calls.  Positions are SoA [3][V] in physical units.  The buffers
+// work space), reusable across calls.  Positions are SoA [N][V] in physical units, N = 3, or 2
+// for an image (nz == 1; vs[2] is then unused).  The buffers
 // come from the stream-ordered pool on stream `s`, which must outlive the workspace.
 class TopologyWorkspace {
   public:
@@ -58,6 +67,8 @@ class TopologyWorkspace {
                        cudaStream_t s);
 
   private:
+    TopologyResult run2d(double e1, double e2, int max_outer, int max_inner, const double vs[3],
+                         cudaStream_t s);
     struct Impl;
     Impl *impl_;
 };

@@ -120,8 +120,9 @@ int binder_registration_set_chain(binder_registration *h, uint32_t chain);
 int binder_registration_reset(binder_registration *h);
 
 /* Topology correction of the object's own current positions, on the device, in place.  Same
- * algorithm and arguments as binder_topology_correct_3d below; it replaces the round trip
- * get_final_locations -> topology_correction_3D().correct_topology -> next Registration that
+ * algorithm and arguments as binder_topology_correct_3d below (binder_topology_correct_2d for a
+ * 2D registration; voxel_sizes[2] is then unused); it replaces the round trip
+ * get_final_locations -> topology_correction_3D/2D().correct_topology -> next Registration that
  * BINDER/FastRegistration.py:515,527-546 performs.  stats_out as for binder_topology_correct_3d. */
 int binder_registration_correct_topology(binder_registration *h, double e1, double e2,
                                          int max_outer_it, int max_it,
@@ -214,6 +215,14 @@ long long binder_jacobian_noalloc_max_voxels(void);
 int binder_topology_correct_3d(const double *field, double e1, double e2, int max_outer_it,
                                int max_it, int threads, const double voxel_sizes[3], int Nx,
                                int Ny, int Nz, double *out, long long *stats_out);
+
+/* topology_correction_2D().correct_topology(h, e1, e2, max_outer_it, max_it, threads,
+ *                                           voxel_sizes, Nx, Ny) -> [Nx,Ny,2]
+ *                                                               cpu/bindings.cpp:447-480
+ * field / out AoS [Nx*Ny*2], voxel_sizes [2]; FP64; stats_out as for the 3D entry point. */
+int binder_topology_correct_2d(const double *field, double e1, double e2, int max_outer_it,
+                               int max_it, int threads, const double voxel_sizes[2], int Nx,
+                               int Ny, double *out, long long *stats_out);
 
 #ifdef __cplusplus
 }

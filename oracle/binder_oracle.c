@@ -843,6 +843,174 @@ int orc_topology3d(double *field, double e1, double e2, int max_outer, int max_i
     return outer;
 }
 
+/* ------------------------------------------------------------------------------------------ */
+/* 2D topology correction (BINDER/src/cpu/topology_correction_2D.cpp)                          */
+/* ------------------------------------------------------------------------------------------ */
+/* :165-207: 4 corner Jacobians per cell (x..x+1, y..y+1), in the vertex order 00, 10, 01, 11
+ * (the reference's Jff, Jbf, Jfb, Jbb).  Corner (vx, vy) uses the x edge at y + vy and the y edge
+ * at x + vx (hi - lo each): det = ex_x * ey_y - ey_x * ex_y, then times 1 / (vs0 vs1).  The
+ * counters count CELLS with a corner below e1 / above e2, as the reference's do. */
+void orc_corner_jacobians2d(const double *pos, int nx, int ny, const double vs[2], double e1,
+                            double e2, double *Jc, int *n_below, int *n_above) {
+    const double vol = 1.0 / (vs[0] * vs[1]);
+    long nb = 0, na = 0;
+    for (int x = 0; x < nx - 1; ++x)
+        for (int y = 0; y < ny - 1; ++y) {
+            const long cell = (long)x * (ny - 1) + y;
+            int lo = 0, hi = 0;
+            for (int c = 0; c < 4; ++c) {
+                const int vx = c & 1, vy = c >> 1;
+                const double *a0 = pos + ((long)x * ny + (y + vy)) * 2;        /* x edge, low  */
+                const double *a1 = pos + ((long)(x + 1) * ny + (y + vy)) * 2;  /* x edge, high */
+                const double *b0 = pos + ((long)(x + vx) * ny + y) * 2;        /* y edge, low  */
+                const double *b1 = pos + ((long)(x + vx) * ny + (y + 1)) * 2;  /* y edge, high */
+                const double j = ((a1[0] - a0[0]) * (b1[1] - b0[1]) -
+                                  (b1[0] - b0[0]) * (a1[1] - a0[1])) * vol;
+                Jc[cell * 4 + c] = j;
+                lo |= j < e1;
+                hi |= j > e2;
+            }
+            nb += lo;
+            na += hi;
+        }
+    if (n_below) *n_below = (int)nb;
+    if (n_above) *n_above = (int)na;
+}
+
+/* :209-246: periodic forward differences, g[p*4 + n1*2 + n2] = d pos_n1 / d axis_n2 / vs[n1] */
+void orc_gradients2d(const double *pos, int nx, int ny, const double vs[2], double *g) {
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y) {
+            const long p = (long)x * ny + y;
+            const long px = (long)((x + 1 > nx - 1) ? x + 1 - nx : x + 1) * ny + y;
+            const long py = (long)x * ny + ((y + 1 > ny - 1) ? y + 1 - ny : y + 1);
+            for (int n1 = 0; n1 < 2; ++n1) {
+                g[p * 4 + n1 * 2 + 0] = (pos[px * 2 + n1] - pos[p * 2 + n1]) / vs[n1];
+                g[p * 4 + n1 * 2 + 1] = (pos[py * 2 + n1] - pos[p * 2 + n1]) / vs[n1];
+            }
+        }
+}
+
+/* :248-313 and :390-406: the 3D limiter's rule on 2x2 gradient matrices -- lexicographic cell
+ * order, corners in order, column n2 read at the corner's vertex with its n2 bit cleared, blended
+ * toward the identity in 0.1 steps (capped at 11; returns the corners that hit the cap). */
+int orc_limit_gradients2d(double *g, const double *Jc, int nx, int ny, double e1, double e2) {
+    int capped = 0;
+    for (int x = 0; x < nx - 1; ++x)
+        for (int y = 0; y < ny - 1; ++y)
+            for (int c = 0; c < 4; ++c) {
+                const double jv = Jc[((long)x * (ny - 1) + y) * 4 + c];
+                if (!(jv < e1 || jv > e2)) continue;
+                const int vx = c & 1, vy = c >> 1;
+                const long gp[2] = {(long)x * ny + (y + vy), (long)(x + vx) * ny + y};
+                double J[2][2];
+                for (int n1 = 0; n1 < 2; ++n1)
+                    for (int n2 = 0; n2 < 2; ++n2) J[n1][n2] = g[gp[n2] * 4 + n1 * 2 + n2];
+                double alpha = 0.0;
+                double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                int steps = 0;
+                while (det > e2 || det < e1) {
+                    if (++steps > 11) { capped++; break; }
+                    alpha += 0.1;
+                    if (alpha > 1.0) alpha = 1.0;
+                    double Jn[2][2];
+                    for (int n1 = 0; n1 < 2; ++n1)
+                        for (int n2 = 0; n2 < 2; ++n2)
+                            Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                    det = Jn[0][0] * Jn[1][1] - Jn[0][1] * Jn[1][0];
+                }
+                alpha += 0.1;
+                if (alpha > 1.0) alpha = 1.0;
+                for (int n1 = 0; n1 < 2; ++n1)
+                    for (int n2 = 0; n2 < 2; ++n2)
+                        g[gp[n2] * 4 + n1 * 2 + n2] =
+                            (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+            }
+    return capped;
+}
+
+/* :315-388: per component, the gradient spectra X, Y combine to
+ * ((e^{-i tx} - 1) X + (e^{-i ty} - 1) Y) / (4 - 2 cos ty - 2 cos tx) (zero where that is
+ * <= 1e-10), inverse transformed, divided by nx ny, scaled by the voxel size, plus the mean */
+void orc_integrate2d(double *pos, const double *g, int nx, int ny, const double vs[2],
+                     const double mean[2]) {
+    const long V = (long)nx * ny;
+    double *xr = (double *)malloc(sizeof(double) * V), *xi = (double *)malloc(sizeof(double) * V);
+    double *yr = (double *)malloc(sizeof(double) * V), *yi = (double *)malloc(sizeof(double) * V);
+    for (int n = 0; n < 2; ++n) {
+        for (long p = 0; p < V; ++p) {
+            xr[p] = g[p * 4 + n * 2 + 0]; xi[p] = 0.0;
+            yr[p] = g[p * 4 + n * 2 + 1]; yi[p] = 0.0;
+        }
+        dft3(xr, xi, nx, ny, 1, -1);
+        dft3(yr, yi, nx, ny, 1, -1);
+        for (int x = 0; x < nx; ++x) {
+            const double cx = cos(2.0 * PI_D * x / nx), sx = sin(2.0 * PI_D * x / nx);
+            for (int y = 0; y < ny; ++y) {
+                const double cy = cos(2.0 * PI_D * y / ny), sy = sin(2.0 * PI_D * y / ny);
+                const long p = (long)x * ny + y;
+                const double nrm = 4.0 - 2.0 * cy - 2.0 * cx;
+                if (nrm > 1e-10) {
+                    const double r = (xr[p] * (cx - 1.0) + xi[p] * sx + yr[p] * (cy - 1.0) + yi[p] * sy) / nrm;
+                    const double i = (xi[p] * (cx - 1.0) - xr[p] * sx + yi[p] * (cy - 1.0) - yr[p] * sy) / nrm;
+                    xr[p] = r;
+                    xi[p] = i;
+                } else {
+                    xr[p] = 0.0;
+                    xi[p] = 0.0;
+                }
+            }
+        }
+        dft3(xr, xi, nx, ny, 1, +1);
+        for (long p = 0; p < V; ++p)
+            pos[p * 2 + n] = xr[p] * (1.0 / (nx * ny)) * vs[n] + mean[n];
+    }
+    free(xr); free(xi); free(yr); free(yi);
+}
+
+/* :17-163 on an AoS [nx][ny][2] field in grid units (in place); returns the outer iterations */
+int orc_topology2d(double *field, double e1, double e2, int max_outer, int max_inner,
+                   const double vs[2], int nx, int ny) {
+    const long V = (long)nx * ny;
+    for (long p = 0; p < V; ++p)
+        for (int n = 0; n < 2; ++n) field[p * 2 + n] *= vs[n];
+    double *J = (double *)malloc(sizeof(double) * V);
+    orc_jacobian2d(field, nx, ny, vs[0], vs[1], J);
+    double jmin, jmax;
+    minmax(J, V, &jmin, &jmax);
+    int outer = 0;
+    if (!(jmin >= e1 && jmax <= e2)) {
+        const long cells = (long)(nx - 1) * (ny - 1);
+        double *Jc = (double *)malloc(sizeof(double) * (cells > 0 ? cells : 1) * 4);
+        double *g = (double *)malloc(sizeof(double) * V * 4);
+        while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+            int nb = 0, na = 0;
+            orc_corner_jacobians2d(field, nx, ny, vs, e1, e2, Jc, &nb, &na);
+            int inner = 0;
+            while ((nb > 0 || na > 0) && inner < max_inner) {
+                orc_gradients2d(field, nx, ny, vs, g);
+                orc_limit_gradients2d(g, Jc, nx, ny, e1, e2);
+                double mean[2] = {0.0, 0.0};
+                for (long p = 0; p < V; ++p)
+                    for (int n = 0; n < 2; ++n) mean[n] += field[p * 2 + n];
+                for (int n = 0; n < 2; ++n) mean[n] = mean[n] / (nx * ny);
+                orc_integrate2d(field, g, nx, ny, vs, mean);
+                orc_corner_jacobians2d(field, nx, ny, vs, e1, e2, Jc, &nb, &na);
+                inner++;
+            }
+            orc_jacobian2d(field, nx, ny, vs[0], vs[1], J);
+            minmax(J, V, &jmin, &jmax);
+            outer++;
+        }
+        free(Jc);
+        free(g);
+    }
+    for (long p = 0; p < V; ++p)
+        for (int n = 0; n < 2; ++n) field[p * 2 + n] /= vs[n];
+    free(J);
+    return outer;
+}
+
 /* MI of the joint distribution given by a (soft) joint histogram */
 double orc_mutual_information(const double *h, int K, int L) {
     double tot = 0.0;

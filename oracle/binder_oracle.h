@@ -118,6 +118,15 @@ void orc_integrate3d(double *pos, const double *grad, int nx, int ny, int nz, co
 /* full driver; field in/out [V*3] grid units.  Returns the outer iterations run. */
 int  orc_topology3d(double *field, double e1, double e2, int max_outer, int max_inner,
                     const double vs[3], int nx, int ny, int nz);
+/* 2D topology correction (topology_correction_2D.cpp) on AoS [nx][ny][2] fields */
+void orc_corner_jacobians2d(const double *pos, int nx, int ny, const double vs[2], double e1,
+                            double e2, double *Jc, int *n_below, int *n_above);
+void orc_gradients2d(const double *pos, int nx, int ny, const double vs[2], double *g);
+int  orc_limit_gradients2d(double *g, const double *Jc, int nx, int ny, double e1, double e2);
+void orc_integrate2d(double *pos, const double *g, int nx, int ny, const double vs[2],
+                     const double mean[2]);
+int  orc_topology2d(double *field, double e1, double e2, int max_outer, int max_inner,
+                    const double vs[2], int nx, int ny);
 
 /* ---- mutual information of a joint histogram [K*L] (FP64) ----------------------------------- */
 double orc_mutual_information(const double *hist, int K, int L);

@@ -71,6 +71,9 @@ def _load_oracle():
     lib.orc_integrate3d.argtypes = [_dp, _dp, i, i, i, _dp, _dp]
     lib.orc_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i]
     lib.orc_topology3d.restype = i
+    lib.orc_corner_jacobians2d.argtypes = [_dp, i, i, _dp, d, d, _dp, C.POINTER(i), C.POINTER(i)]
+    lib.orc_topology2d.argtypes = [_dp, d, d, i, i, _dp, i, i]
+    lib.orc_topology2d.restype = i
     lib.orc_mutual_information.argtypes = [_dp, i, i]
     lib.orc_mutual_information.restype = d
     lib.orc_set_threads.argtypes = [i]
@@ -98,6 +101,7 @@ def ref_lib():
     r.ref_jacobian3d.argtypes = [_dp, i, i, i, d, d, d, _dp]
     r.ref_jacobian2d.argtypes = [_dp, i, i, d, d, _dp]
     r.ref_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i, _dp]
+    r.ref_topology2d.argtypes = [_dp, d, d, i, i, _dp, i, i, _dp]
     r.ref_smooth_deformation.argtypes = [_dp, _dp, _dp, _dp, i, i, i, d, d, _dp, _dp]
     r.ref_smooth_deformation.restype = d
     r.ref_mi_update.argtypes = [d, _dp, _dp, i, i, _dp]
@@ -284,6 +288,22 @@ def corner_jacobians3d(pos, shape, vs, e1, e2):
 def topology3d(field, e1, e2, max_outer, max_inner, vs, shape):
     f = _c64(field).ravel().copy()
     outer = lib().orc_topology3d(f, float(e1), float(e2), int(max_outer), int(max_inner),
+                                 _c64(vs), *shape)
+    return f, outer
+
+
+def corner_jacobians2d(pos, shape, vs, e1, e2):
+    nx, ny = shape
+    Jc = np.zeros(max(1, (nx - 1) * (ny - 1)) * 4)
+    nb, na = C.c_int(0), C.c_int(0)
+    lib().orc_corner_jacobians2d(_c64(pos).ravel(), nx, ny, _c64(vs), float(e1), float(e2), Jc,
+                                 C.byref(nb), C.byref(na))
+    return Jc, nb.value, na.value
+
+
+def topology2d(field, e1, e2, max_outer, max_inner, vs, shape):
+    f = _c64(field).ravel().copy()
+    outer = lib().orc_topology2d(f, float(e1), float(e2), int(max_outer), int(max_inner),
                                  _c64(vs), *shape)
     return f, outer
 

@@ -7,6 +7,7 @@
 #include "MILikelihood.h"
 #include "NonLinearTransformation.h"
 #include "Spline.h"
+#include "topology_correction_2D.h"
 #include "topology_correction_3D.h"
 #include "utils.h"
 
@@ -37,6 +38,14 @@ void ref_topology3d(const double *field, double e1, double e2, int max_outer, in
     topology_correction_3D tc;
     const double *r = tc.correct_topology(field, e1, e2, max_outer, max_inner, 1, vs, nx, ny, nz);
     std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * nz * 3);
+}
+
+// topology_correction_2D::correct_topology (BINDER/src/cpu/topology_correction_2D.cpp:17-163)
+void ref_topology2d(const double *field, double e1, double e2, int max_outer, int max_inner,
+                    const double *vs, int nx, int ny, double *out) {
+    topology_correction_2D tc;
+    const double *r = tc.correct_topology(field, e1, e2, max_outer, max_inner, 1, vs, nx, ny);
+    std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * 2);
 }
 
 // NonLinearTransformation::smooth_deformation (BINDER/src/cpu/NonLinearTransformation.cpp:226-278)

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference's own CPU sources.
 
 The reference's Spline.cpp, MILikelihood.cpp, utils.cpp, DCT.cpp, FFT.cpp,
-NonLinearTransformation.cpp and topology_correction_3D.cpp are compiled unmodified by
+NonLinearTransformation.cpp, topology_correction_3D.cpp and topology_correction_2D.cpp are compiled unmodified by
 oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in
 oracle/ref_shim).  This script feeds them seeded inputs and stores inputs and outputs as small
 .npz files, so the parity tests are pinned to the reference even where its sources are absent.
@@ -104,6 +104,23 @@ def main():
     cost = R.ref_smooth_deformation(gamma, one, one, D, *shape, 1.0, 0.0, field.ravel(), out)
     np.savez(os.path.join(HERE, "smoothing2d_ref.npz"), field=field, D=D, gamma=gamma, sigma=1.0,
              out=out.reshape(field.shape), cost=cost)
+    # 2D topology correction (topology_correction_2D.cpp:17-163)
+    cases = {}
+    # (shape, noise, voxel sizes, e1, e2): folds only; folds with anisotropic pixels; a tight band
+    # that also caps expansions
+    for k, (shape, sig, vs, e1, e2) in enumerate([((14, 12), 0.45, (1.0, 1.2), 0.01, 100.0),
+                                                 ((20, 17), 0.5, (1.0, 1.0), 0.01, 100.0),
+                                                 ((16, 15), 0.35, (0.9, 1.1), 0.5, 1.6)]):
+        f = np.stack(np.indices(shape), -1).astype(np.float64) + rng.normal(0, sig, shape + (2,))
+        out = np.zeros(f.size)
+        R.ref_topology2d(f.ravel(), e1, e2, 10, 10, np.asarray(vs, float), *shape, out)
+        cases[f"field{k}"] = f
+        cases[f"shape{k}"] = np.array(shape)
+        cases[f"vs{k}"] = np.array(vs, float)
+        cases[f"e{k}"] = np.array([e1, e2])
+        cases[f"out{k}"] = out.reshape(f.shape)
+    np.savez(os.path.join(HERE, "topology2d_ref.npz"), ncases=3, max_outer=10, max_inner=10,
+             **cases)
     print("golden fixtures written to", HERE)
 
 

@@ -45,8 +45,6 @@ def test_shapes_follow_the_reference(core):
     assert reg.get_shape() == [nx, ny, 1, 2]
     assert reg.get_final_locations_as_numpy_array().shape == (nx, ny, 1, 2)
     assert reg.get_dream_locations().size == nx * ny * 2
-    with pytest.raises(core.BinderError):
-        reg.correct_topology(0.01, 100.0, 2, 2, [1.0, 1.0, 1.0])
 
 
 def test_one_em_iteration_matches_oracle(core, oracle):
@@ -167,3 +165,49 @@ def test_jacobian2d_large_bit_exact_vs_oracle(core, oracle):
     J = core.compute_jacobian_determinant_2D(f, *shape, 0.8, 1.3).ravel()
     assert np.array_equal(J, oracle.jacobian2d(f, shape, (0.8, 1.3)))
     assert (J < 0).sum() > 0
+
+
+def test_topology2d_matches_reference_golden(core, oracle):
+    g = golden("topology2d_ref.npz")
+    tc = core.topology_correction_2D()
+    for k in range(int(g["ncases"])):
+        shape = tuple(int(s) for s in g[f"shape{k}"])
+        e1, e2 = (float(v) for v in g[f"e{k}"])
+        out = tc.correct_topology(g[f"field{k}"], e1, e2, 10, 10, 1, g[f"vs{k}"], *shape)
+        assert out.shape == shape + (2,)
+        ref = g[f"out{k}"]
+        np.testing.assert_allclose(out, ref, rtol=0, atol=1e-9)   # FP64 Hartley vs FFT Poisson
+        vs = tuple(g[f"vs{k}"])
+        Jg, Jr = oracle.jacobian2d(out, shape, vs), oracle.jacobian2d(ref, shape, vs)
+        assert np.array_equal((Jg < e1) | (Jg > e2), (Jr < e1) | (Jr > e2))
+        assert tc.last_stats["below_e1_before"] > 0
+        assert tc.last_stats["below_e1_after"] == 0 and tc.last_stats["above_e2_after"] == 0
+
+
+def test_topology2d_larger_field_matches_oracle(core, oracle):
+    from binder_b200 import phantoms
+    shape = (96, 80)
+    rng = np.random.default_rng(11)
+    f = phantoms.identity_positions(shape) + \
+        phantoms.smooth_random_field(shape, 2.5, 1.5, rng).astype(np.float64)
+    assert (oracle.jacobian2d(f, shape) < 0.01).sum() > 0
+    tc = core.topology_correction_2D()
+    out = tc.correct_topology(f, 0.01, 100.0, 10, 10, 1, [1.0, 1.0], *shape)
+    ref, _ = oracle.topology2d(f, 0.01, 100.0, 10, 10, [1.0, 1.0], shape)
+    np.testing.assert_allclose(out.ravel(), ref, rtol=0, atol=1e-8)
+    assert tc.last_stats["below_e1_after"] == 0
+
+
+def test_registration_topology2d_on_device(core):
+    """The device-side correction of a 2D registration's positions equals the host entry point
+    applied to the same (FP32) positions."""
+    c = make_case2d(seed=5, disp=2.0)
+    nx, ny = c["shape"]
+    reg = new_reg2d(core, c)
+    before = reg.get_final_locations_as_numpy_array().reshape(nx, ny, 2).astype(np.float64)
+    st = reg.correct_topology(0.01, 100.0, 10, 10, [1.0, 1.0])
+    after = reg.get_final_locations_as_numpy_array().reshape(nx, ny, 2)
+    host = core.topology_correction_2D().correct_topology(before, 0.01, 100.0, 10, 10, 1,
+                                                          [1.0, 1.0], nx, ny)
+    assert st["below_e1_before"] > 0 and st["below_e1_after"] == 0
+    np.testing.assert_allclose(after, host.astype(np.float32), rtol=0, atol=1e-5)

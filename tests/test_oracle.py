@@ -50,6 +50,18 @@ def test_topology_matches_reference(oracle):
         assert (oracle.jacobian3d(g[f"field{k}"], shape) < 0).sum() > 0
 
 
+def test_topology2d_matches_reference(oracle):
+    g = golden("topology2d_ref.npz")
+    for k in range(int(g["ncases"])):
+        shape = tuple(int(s) for s in g[f"shape{k}"])
+        e1, e2 = (float(v) for v in g[f"e{k}"])
+        out, outer = oracle.topology2d(g[f"field{k}"], e1, e2, 10, 10, g[f"vs{k}"], shape)
+        np.testing.assert_allclose(out, g[f"out{k}"].ravel(), rtol=0, atol=1e-12)
+        J0 = oracle.jacobian2d(g[f"field{k}"], shape, tuple(g[f"vs{k}"]))
+        J1 = oracle.jacobian2d(out, shape, tuple(g[f"vs{k}"]))
+        assert ((J0 < e1) | (J0 > e2)).sum() > 0 and not ((J1 < e1) | (J1 > e2)).any()
+
+
 def test_smoothing_matches_reference(oracle):
     g = golden("smoothing_ref.npz")
     shape = g["field"].shape[:3]
