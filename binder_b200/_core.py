@@ -249,6 +249,17 @@ class NonLinearTransformation:
             self._h, _f32(deformationField, self._V * N, "deformationField"), n, out))
         return out.reshape(n, *self._shape, N)
 
+    @staticmethod
+    def up_sample(deformation_field, N_x, N_y, N_z, N_x_o, N_y_o, N_z_o, threads):
+        """``NonLinearTransformation.up_sample`` (cpu/bindings.cpp:408-434), FP64 on the GPU."""
+        N = 2 if int(N_z_o) == 1 else 3
+        Vi = int(N_x) * int(N_y) * int(N_z)
+        out = np.zeros(int(N_x_o) * int(N_y_o) * int(N_z_o) * N, np.float64)
+        check(lib().binder_transform_up_sample(
+            _f64(deformation_field, Vi * N, "deformation_field"), int(N_x), int(N_y), int(N_z),
+            int(N_x_o), int(N_y_o), int(N_z_o), int(threads), out))
+        return out.reshape(int(N_x_o), int(N_y_o), int(N_z_o), N)
+
 
 class topology_correction_3D:
     """``_core.topology_correction_3D`` (gpu/bindings.cpp:259-287); FP64 throughout."""
@@ -306,6 +317,24 @@ def compute_jacobian_determinant_3D(field, Nx, Ny, Nz, voxel_size_x, voxel_size_
                                                int(Nz), float(voxel_size_x), float(voxel_size_y),
                                                float(voxel_size_z), J))
     return J.reshape(int(Nx), int(Ny), int(Nz))
+
+
+def resize_linear(field, output_shape, scale=1.0):
+    """skimage.transform.resize(field, output_shape, order=1) * scale on the GPU (FP64), for the
+    deformation fields FastRegistration.py:562-564 resamples between resolutions.  field is
+    [*shape, N] with a 2- or 3-D spatial shape; output_shape gives the new spatial shape."""
+    f = np.asarray(field, np.float64)
+    sp = tuple(int(s) for s in output_shape)
+    nd = len(sp)
+    if nd not in (2, 3) or f.ndim != nd + 1:
+        raise ValueError("field must be [*shape, N] with a 2-D or 3-D spatial shape")
+    ish = f.shape[:nd] + (1,) * (3 - nd)
+    osh = sp + (1,) * (3 - nd)
+    N = f.shape[-1]
+    out = np.zeros(int(np.prod(osh)) * N, np.float64)
+    check(lib().binder_resize_linear(_f64(f, f.size, "field"), *ish, int(N), *osh, float(scale),
+                                     out))
+    return out.reshape(*sp, N)
 
 
 def compute_jacobian_determinant_2D(field, Nx, Ny, voxel_size_x, voxel_size_y):

@@ -36,7 +36,8 @@ EXPORTS = [
     "binder_transform_get_shape", "binder_jacobian_determinant_3d", "binder_topology_correct_3d",
     "binder_topology_correct_2d",
     "binder_jacobian_determinant_3d_noalloc", "binder_jacobian_noalloc_max_voxels",
-    "binder_jacobian_determinant_2d",
+    "binder_jacobian_determinant_2d", "binder_transform_up_sample", "binder_resize_linear",
+    "binder_resample_matrix",
 ]
 
 
@@ -93,6 +94,9 @@ def _declare(lib):
         "binder_transform_get_shape": [_P, _i32],
         "binder_jacobian_determinant_3d": [_f64, _i, _i, _i, _d, _d, _d, _f64],
         "binder_jacobian_determinant_2d": [_f64, _i, _i, _d, _d, _f64],
+        "binder_transform_up_sample": [_f64, _i, _i, _i, _i, _i, _i, _i, _f64],
+        "binder_resize_linear": [_f64, _i, _i, _i, _i, _i, _i, _i, _d, _f64],
+        "binder_resample_matrix": [_i, _i, _i, _f64],
         "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],

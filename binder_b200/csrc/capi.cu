@@ -2,9 +2,11 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/binder_b200.h"
 #include "engine.cuh"
+#include "resample.cuh"
 
 struct binder_registration {
     binder::Registration *impl;
@@ -318,6 +320,39 @@ int binder_transform_get_shape(const binder_transform *h, int out[4]) {
         NEED(h);
         NEED(out);
         h->impl->get_shape(out);
+    });
+}
+
+int binder_transform_up_sample(const double *field, int Nx, int Ny, int Nz, int Nx_o, int Ny_o,
+                               int Nz_o, int threads, double *out) {
+    (void)threads;
+    return guard([&] {
+        NEED(field);
+        NEED(out);
+        binder::up_sample(field, Nx, Ny, Nz, Nx_o, Ny_o, Nz_o, out);
+    });
+}
+
+int binder_resample_matrix(int kind, int n, int m, double *out) {
+    return guard([&] {
+        NEED(out);
+        std::vector<double> M;
+        if (kind == 0)
+            binder::dct_upsample_matrix(n, m, M);
+        else if (kind == 1)
+            binder::linear_resize_matrix(n, m, M);
+        else
+            throw binder::Error(BINDER_STATUS_INVALID_ARGUMENT, "kind must be 0 or 1");
+        std::memcpy(out, M.data(), sizeof(double) * M.size());
+    });
+}
+
+int binder_resize_linear(const double *field, int Nx, int Ny, int Nz, int N, int Nx_o, int Ny_o,
+                         int Nz_o, double scale, double *out) {
+    return guard([&] {
+        NEED(field);
+        NEED(out);
+        binder::resize_linear(field, Nx, Ny, Nz, N, Nx_o, Ny_o, Nz_o, scale, out);
     });
 }
 

@@ -170,6 +170,22 @@ int binder_transform_smooth_deformation(binder_transform *h, const float *field,
 int binder_transform_sample_deformation_field(binder_transform *h, const float *field,
                                               int number_of_samples, float *out);
 int binder_transform_get_shape(const binder_transform *h, int out[4]);
+/* NonLinearTransformation.up_sample(field, N_x, N_y, N_z, N_x_o, N_y_o, N_z_o, threads)
+ *   -> [N_x_o, N_y_o, N_z_o, N]                                  cpu/bindings.cpp:408-434
+ * static: spectral zero-padding of an AoS field (N = 2 when N_z_o == 1), FP64; every output axis
+ * at least as long as its input axis.  `threads` is accepted for interface parity. */
+int binder_transform_up_sample(const double *field, int Nx, int Ny, int Nz, int Nx_o, int Ny_o,
+                               int Nz_o, int threads, double *out);
+
+/* No counterpart in the reference's module: skimage.transform.resize(field, (Nx_o, Ny_o, Nz_o),
+ * order=1) * scale on an AoS [Nx][Ny][Nz][N] FP64 field, as BINDER/FastRegistration.py:562-564
+ * resamples the deformation between resolutions (Gaussian anti-aliasing on shrinking axes, then
+ * pixel-centre-aligned linear interpolation, mirror boundaries). */
+int binder_resize_linear(const double *field, int Nx, int Ny, int Nz, int N, int Nx_o, int Ny_o,
+                         int Nz_o, double scale, double *out);
+/* The per-axis m x n matrix (row-major, host memory, no device work) that the two resamplers
+ * above apply along an axis of length n -> m: kind 0 spectral up-sampling, 1 linear resize. */
+int binder_resample_matrix(int kind, int n, int m, double *out);
 
 /* ---- Jacobian determinant and topology correction ----------------------------------------- */
 

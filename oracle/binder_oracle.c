@@ -408,6 +408,31 @@ void orc_sample_field(const double *field, const double *D, const double gamma[3
     free(zeros);
 }
 
+/* NonLinearTransformation.cpp:366-430 (static up_sample): per component, the orthonormal DCT-II on
+ * the input grid, its coefficients written into the low-index corner of a zero output spectrum,
+ * and the orthonormal DCT-III on the output grid.  AoS [nx][ny][nz][N] -> [nxo][nyo][nzo][N],
+ * N = 2 when nzo == 1; every output axis at least as long as the input one. */
+void orc_up_sample(const double *in, int nx, int ny, int nz, int nxo, int nyo, int nzo,
+                   double *out) {
+    const int N = (nzo == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz, Vo = (long)nxo * nyo * nzo;
+    double *c = (double *)malloc(sizeof(double) * V);
+    double *co = (double *)malloc(sizeof(double) * Vo);
+    for (int n = 0; n < N; ++n) {
+        for (long p = 0; p < V; ++p) c[p] = in[p * N + n];
+        orc_dct3(c, c, nx, ny, nz, 0);
+        for (long q = 0; q < Vo; ++q) co[q] = 0.0;
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y)
+                for (int z = 0; z < nz; ++z)
+                    co[((long)x * nyo + y) * nzo + z] = c[((long)x * ny + y) * nz + z];
+        orc_dct3(co, co, nxo, nyo, nzo, 1);
+        for (long q = 0; q < Vo; ++q) out[q * N + n] = co[q];
+    }
+    free(c);
+    free(co);
+}
+
 /* Registration.cpp:122-217 */
 int orc_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
            double *theta, double alpha, const double *D, const double gamma[3], double sigma,

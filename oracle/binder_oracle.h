@@ -61,6 +61,9 @@ double orc_gamma_sample(double shape, uint64_t seed, uint32_t index, uint32_t sw
 
 /* ---- orthonormal 3D DCT-II / DCT-III: BINDER/src/cpu/DCT.cpp:83-175 --------------------------- */
 void orc_dct3(const double *in, double *out, int nx, int ny, int nz, int inverse);
+/* NonLinearTransformation::up_sample: spectral zero-padding of an AoS field */
+void orc_up_sample(const double *in, int nx, int ny, int nz, int nxo, int nyo, int nzo,
+                   double *out);
 
 /* ---- DCT-prior M-step: BINDER/src/cpu/NonLinearTransformation.cpp:58-76,128-137,173-223 -------
  * dream, voxel_pos: [V*N];  D: [V];  gamma[N];  out final [V*N].  Returns the prior cost.

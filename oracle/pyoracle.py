@@ -51,6 +51,7 @@ def _load_oracle():
     lib.orc_gamma_sample.argtypes = [d, u64, u32, u32, u32, u32, C.POINTER(i)]
     lib.orc_gamma_sample.restype = d
     lib.orc_dct3.argtypes = [_dp, _dp, i, i, i, i]
+    lib.orc_up_sample.argtypes = [_dp, i, i, i, i, i, i, _dp]
     lib.orc_smooth.argtypes = [_dp, _dp, _dp, _dp, d, i, i, i, _dp, i, u64, u32, u32,
                                C.c_void_p, C.c_void_p, C.c_void_p]
     lib.orc_smooth.restype = d
@@ -102,6 +103,7 @@ def ref_lib():
     r.ref_jacobian2d.argtypes = [_dp, i, i, d, d, _dp]
     r.ref_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i, _dp]
     r.ref_topology2d.argtypes = [_dp, d, d, i, i, _dp, i, i, _dp]
+    r.ref_up_sample.argtypes = [_dp, i, i, i, i, i, i, _dp]
     r.ref_smooth_deformation.argtypes = [_dp, _dp, _dp, _dp, i, i, i, d, d, _dp, _dp]
     r.ref_smooth_deformation.restype = d
     r.ref_mi_update.argtypes = [d, _dp, _dp, i, i, _dp]
@@ -209,6 +211,36 @@ def smooth(dream, voxel_pos, D, gamma, sigma, shape, noise=None, rho=None, eta=N
     if want_raw:
         return cost, out, raw.value
     return cost, out
+
+
+def up_sample(field, shape, oshape):
+    """NonLinearTransformation.up_sample on an AoS field: shape -> oshape (nz == 1: 2D)."""
+    N = 2 if oshape[2] == 1 else 3
+    out = np.zeros(int(np.prod(oshape)) * N)
+    lib().orc_up_sample(_c64(field).ravel(), *shape, *oshape, out)
+    return out.reshape(*oshape, N)
+
+
+def resize_linear(field, oshape, scale=1.0):
+    """skimage.transform.resize(field, oshape, order=1) * scale, the call at
+    BINDER/FastRegistration.py:562-564, restated from scikit-image's published resize (0.19 and
+    later; the package is not installed here): with the default mode 'reflect' and anti-aliasing
+    on when any axis shrinks, it Gaussian-filters with sigma = max(0, (n/m - 1)/2) per axis
+    (scipy.ndimage 'mirror' boundary), zooms with scipy.ndimage.zoom(order=1, grid_mode=True,
+    mode='mirror') and clips to the input's value range.  field is [*shape, N]; oshape the new
+    spatial shape (the component axis keeps its length)."""
+    from scipy import ndimage as ndi
+    f = np.asarray(field, np.float64)
+    ishape = f.shape
+    out_shape = tuple(int(s) for s in oshape) + ishape[len(oshape):]
+    factors = np.divide(ishape, out_shape)
+    g = f
+    if any(o < i for o, i in zip(out_shape, ishape)):
+        sig = np.maximum(0, (factors - 1) / 2)
+        g = ndi.gaussian_filter(f, sig, mode="mirror")
+    z = ndi.zoom(g, [1 / x for x in factors], order=1, mode="mirror", grid_mode=True)
+    z = np.clip(z, f.min(), f.max())
+    return z * scale
 
 
 def sample_field(field, D, gamma, sigma, shape, n, seed=1234, sweep0=0):

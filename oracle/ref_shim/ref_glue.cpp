@@ -48,6 +48,13 @@ void ref_topology2d(const double *field, double e1, double e2, int max_outer, in
     std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * 2);
 }
 
+// NonLinearTransformation::up_sample (BINDER/src/cpu/NonLinearTransformation.cpp:366-430)
+void ref_up_sample(const double *field, int nx, int ny, int nz, int nxo, int nyo, int nzo,
+                   double *out) {
+    const auto r = NonLinearTransformation::up_sample(field, nx, ny, nz, nxo, nyo, nzo, 1);
+    std::memcpy(out, r.data(), sizeof(double) * r.size());
+}
+
 // NonLinearTransformation::smooth_deformation (BINDER/src/cpu/NonLinearTransformation.cpp:226-278)
 double ref_smooth_deformation(const double gamma[3], const double rho[3], const double eta[3],
                               const double *D, int nx, int ny, int nz, double sigma, double offset,

@@ -121,6 +121,18 @@ def main():
         cases[f"out{k}"] = out.reshape(f.shape)
     np.savez(os.path.join(HERE, "topology2d_ref.npz"), ncases=3, max_outer=10, max_inner=10,
              **cases)
+    # spectral up-sampling of a displacement field (NonLinearTransformation.cpp:366-430): a
+    # resolution-2 -> 1 step in 3D and 2D, odd and even sizes
+    ups = {}
+    for k, (shape, oshape) in enumerate([((6, 7, 5), (12, 13, 10)), ((9, 8, 1), (17, 16, 1))]):
+        N = 2 if oshape[2] == 1 else 3
+        f = rng.standard_normal(shape + (N,))
+        out = np.zeros(int(np.prod(oshape)) * N)
+        R.ref_up_sample(f.ravel(), *shape, *oshape, out)
+        ups[f"field{k}"] = f
+        ups[f"oshape{k}"] = np.array(oshape)
+        ups[f"out{k}"] = out.reshape(oshape + (N,))
+    np.savez(os.path.join(HERE, "upsample_ref.npz"), ncases=2, **ups)
     print("golden fixtures written to", HERE)
 
 
