@@ -68,6 +68,18 @@ class Registration:
         self._N = N
         self._K = self._L = None
 
+    @classmethod
+    def _adopt(cls, handle, shape, nshape, K, L):
+        """Wrap a registration the library created (binder_pyramid_level); takes ownership."""
+        self = cls.__new__(cls)
+        self._h = handle
+        self._shape = tuple(int(s) for s in shape)
+        self._nshape = tuple(int(s) for s in nshape)
+        self._V = int(np.prod(self._shape))
+        self._N = 2 if self._shape[2] == 1 else 3
+        self._K, self._L = int(K), int(L)
+        return self
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

@@ -6,6 +6,7 @@
 
 #include "../../include/binder_b200.h"
 #include "engine.cuh"
+#include "multires.cuh"
 #include "resample.cuh"
 
 struct binder_registration {
@@ -13,6 +14,9 @@ struct binder_registration {
 };
 struct binder_transform {
     binder::PriorTransform *impl;
+};
+struct binder_pyramid {
+    binder::Pyramid *impl;
 };
 
 namespace {
@@ -320,6 +324,69 @@ int binder_transform_get_shape(const binder_transform *h, int out[4]) {
         NEED(h);
         NEED(out);
         h->impl->get_shape(out);
+    });
+}
+
+int binder_pyramid_create(binder_pyramid **out, const int32_t *binned_voxels,
+                          const int32_t *binned_nodes, const double *voxel_pos, int Nx_v, int Ny_v,
+                          int Nz_v, int Nx_n, int Ny_n, int Nz_n,
+                          const double voxels_voxel_size[3], const double nodes_voxel_size[3],
+                          double gamma, int finite_difference_order,
+                          int increase_gamma_at_DS_resolution, int upsample_in_frequency_domain,
+                          int spline_order) {
+    return guard([&] {
+        NEED(out);
+        NEED(binned_voxels);
+        NEED(binned_nodes);
+        NEED(voxels_voxel_size);
+        NEED(nodes_voxel_size);
+        *out = nullptr;
+        binder::PyramidConfig c{};
+        c.nx = Nx_v; c.ny = Ny_v; c.nz = Nz_v;
+        c.nxn = Nx_n; c.nyn = Ny_n; c.nzn = Nz_n;
+        for (int a = 0; a < 3; ++a) {
+            c.voxel_size[a] = voxels_voxel_size[a];
+            c.node_size[a] = nodes_voxel_size[a];
+        }
+        c.gamma_init = gamma;
+        c.finite_difference_order = finite_difference_order;
+        c.increase_gamma_at_ds = increase_gamma_at_DS_resolution;
+        c.upsample_in_frequency_domain = upsample_in_frequency_domain;
+        c.spline_order = spline_order;
+        auto *impl = new binder::Pyramid(c, binned_voxels, binned_nodes, voxel_pos);
+        *out = new binder_pyramid{impl};
+    });
+}
+
+int binder_pyramid_destroy(binder_pyramid *p) {
+    return guard([&] {
+        if (!p) return;
+        delete p->impl;
+        delete p;
+    });
+}
+
+int binder_pyramid_level(binder_pyramid *p, int resolution, const binder_registration *prev,
+                         int prev_resolution, double alpha, const float *theta, int K, int L,
+                         binder_registration **out, double info_out[16]) {
+    return guard([&] {
+        NEED(p);
+        NEED(out);
+        *out = nullptr;
+        binder::LevelInfo li{};
+        binder::Registration *r = p->impl->level(resolution, prev ? prev->impl : nullptr,
+                                                 prev_resolution, alpha, theta, K, L, &li);
+        *out = new binder_registration{r};
+        if (info_out) {
+            for (int a = 0; a < 3; ++a) {
+                info_out[a] = li.voxels_shape[a];
+                info_out[3 + a] = li.nodes_shape[a];
+                info_out[6 + a] = li.gamma[a];
+                info_out[9 + a] = li.voxel_size[a];
+                info_out[12 + a] = li.node_size[a];
+            }
+            info_out[15] = li.non_zero_voxels;
+        }
     });
 }
 

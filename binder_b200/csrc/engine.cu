@@ -245,12 +245,13 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
     BINDER_CUDA(cudaMemsetAsync(st_, 0, sizeof(DevState), s));
     // the caller's AoS arrays go to the device as they are (r_ is the staging buffer) and are
     // rearranged there
-    BINDER_CUDA(cudaMemcpyAsync(r_, final_locations, sizeof(float) * VN, cudaMemcpyHostToDevice, s));
+    // inputs may be host or device memory (the multi-resolution step passes device arrays)
+    BINDER_CUDA(cudaMemcpyAsync(r_, final_locations, sizeof(float) * VN, cudaMemcpyDefault, s));
     launch_aos_to_soa(r_, d_, V_, N_, s);
     BINDER_CUDA(cudaMemcpyAsync(d0_, d_, sizeof(float) * VN, cudaMemcpyDeviceToDevice, s));
     // the identity voxel grid (the common case) is recomputed in the kernels instead of read
     if (voxel_pos != final_locations)
-        BINDER_CUDA(cudaMemcpyAsync(r_, voxel_pos, sizeof(float) * VN, cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemcpyAsync(r_, voxel_pos, sizeof(float) * VN, cudaMemcpyDefault, s));
     launch_identity_check(r_, g, &st_->flags, s);
     unsigned mismatch = 0;
     BINDER_CUDA(cudaMemcpyAsync(&mismatch, &st_->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -310,14 +311,13 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     int *bins = dalloc<int>((size_t)(V_ + Vn_), s);
     unsigned long long *bad = dalloc<unsigned long long>(2, s);
     BINDER_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(unsigned long long), s));
-    BINDER_CUDA(cudaMemcpyAsync(bins, binned_voxels, sizeof(int) * V_, cudaMemcpyHostToDevice, s));
-    BINDER_CUDA(cudaMemcpyAsync(bins + V_, binned_nodes, sizeof(int) * Vn_,
-                                cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(bins, binned_voxels, sizeof(int) * V_, cudaMemcpyDefault, s));
+    BINDER_CUDA(cudaMemcpyAsync(bins + V_, binned_nodes, sizeof(int) * Vn_, cudaMemcpyDefault, s));
     launch_bins_to_u8(bins, V_, L, u_, bad, s);
     BINDER_CUDA(cudaMemsetAsync(vpad_, 0, padded, s));
     launch_bins_to_padded(bins + V_, w.nxn, w.nyn, w.nzn, K, vpad_, P_, Py, PZ_, pyn_, zp_, bad + 1,
                           s);
-    BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * K * L, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * K * L, cudaMemcpyDefault, s));
     BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * K * L, cudaMemcpyDeviceToDevice, s));
     BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K * L, s));
     BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K * L, s));
@@ -328,11 +328,18 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     dfree(bins, s);
     if (hbad[0] != ~0ull || hbad[1] != ~0ull) {
         have_mi_ = false;
+        // the offending value, read through a copy (the arrays may be device memory)
+        auto value_at = [](const int *a, unsigned long long i) {
+            int v = 0;
+            BINDER_CUDA(cudaMemcpy(&v, a + i, sizeof(int), cudaMemcpyDefault));
+            return v;
+        };
         if (hbad[0] != ~0ull)
             throw Error(kInvalidArgument, "binned_voxels value " +
-                                              std::to_string(binned_voxels[hbad[0]]) +
+                                              std::to_string(value_at(binned_voxels, hbad[0])) +
                                               " outside [0, L) at voxel " + std::to_string(hbad[0]));
-        throw Error(kInvalidArgument, "binned_nodes value " + std::to_string(binned_nodes[hbad[1]]) +
+        throw Error(kInvalidArgument, "binned_nodes value " +
+                                          std::to_string(value_at(binned_nodes, hbad[1])) +
                                           " outside [0, K) at node " + std::to_string(hbad[1]));
     }
     K_ = K;
@@ -354,7 +361,7 @@ void Registration::set_nonlinear_transformation(const double gamma[3], const dou
     em_graph_.clear();
     dfree(D_, own_stream_);
     D_ = dalloc<float>((size_t)V_, own_stream_);
-    BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyHostToDevice, own_stream_));
+    BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyDefault, own_stream_));
     BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     sigma2_ = kSigmaCubic2;
     have_tr_ = true;

@@ -90,6 +90,11 @@ class Registration {
 
     int K() const { return K_; }
     int L() const { return L_; }
+    // device views for the multi-resolution step; valid while no call on this object runs
+    const float *positions_device() const { return d_; }  // SoA [N][V], grid units
+    const float *theta_device() const { return theta_; }  // [K][L] or null before set-up
+    int components() const { return N_; }
+    void dims(int out[3]) const { out[0] = nx_; out[1] = ny_; out[2] = nz_; }
 
   private:
     // grid dimensions as the E-step sees them (a 2D image nx x ny is the volume nx x 1 x ny)

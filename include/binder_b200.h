@@ -37,6 +37,7 @@ extern "C" {
 
 typedef struct binder_registration binder_registration;
 typedef struct binder_transform binder_transform;
+typedef struct binder_pyramid binder_pyramid;
 
 /* last error message of this thread ("" when none) */
 const char *binder_last_error(void);
@@ -183,6 +184,34 @@ int binder_transform_up_sample(const double *field, int Nx, int Ny, int Nz, int 
  * pixel-centre-aligned linear interpolation, mirror boundaries). */
 int binder_resize_linear(const double *field, int Nx, int Ny, int Nz, int N, int Nx_o, int Ny_o,
                          int Nz_o, double scale, double *out);
+/* ---- the multi-resolution step on the device ------------------------------------------------
+ * No counterpart in the reference's module: FastRegistration.move_resolution
+ * (BINDER/FastRegistration.py:550-650) plus the Registration set-up of run() (:443-486) for the
+ * MI metric, done on the device from full-resolution data the pyramid keeps.
+ *
+ * binder_pyramid_create: full-resolution bins (int32, fixed image [V], moving image [Vn]) and the
+ * voxel positions in node space (AoS [V*N] FP64, N = 2 when Nz_v == 1; NULL for the identity
+ * grid), the two images' voxel sizes, and the options of FastRegistration of the same names
+ * (`gamma` is its gamma_init).  The `smooth` option (Smoothing_Spline) is not built. */
+int binder_pyramid_create(binder_pyramid **out, const int32_t *binned_voxels,
+                          const int32_t *binned_nodes, const double *voxel_pos, int Nx_v, int Ny_v,
+                          int Nz_v, int Nx_n, int Ny_n, int Nz_n,
+                          const double voxels_voxel_size[3], const double nodes_voxel_size[3],
+                          double gamma, int finite_difference_order,
+                          int increase_gamma_at_DS_resolution, int upsample_in_frequency_domain,
+                          int spline_order);
+int binder_pyramid_destroy(binder_pyramid *p);
+/* move_resolution(resolution) and a new registration for that level (*out; destroy it with
+ * binder_registration_destroy), with setNonLinearTransformation and setMILikelihood applied.
+ * The deformation comes from `prev`, a registration of this pyramid at prev_resolution, or from
+ * the full-resolution voxel positions when prev is NULL (FastRegistration starts at resolution
+ * 1).  theta [K*L] (host or device memory) or NULL to carry prev's over.  info_out (optional):
+ * voxels_shape[3], nodes_shape[3], gamma_x/y/z, current voxel sizes[3], current node sizes[3],
+ * non_zero_voxels. */
+int binder_pyramid_level(binder_pyramid *p, int resolution, const binder_registration *prev,
+                         int prev_resolution, double alpha, const float *theta, int K, int L,
+                         binder_registration **out, double info_out[16]);
+
 /* The per-axis m x n matrix (row-major, host memory, no device work) that the two resamplers
  * above apply along an axis of length n -> m: kind 0 spectral up-sampling, 1 linear resize. */
 int binder_resample_matrix(int kind, int n, int m, double *out);
