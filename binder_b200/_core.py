@@ -11,6 +11,7 @@ FP64.  Errors raise ``BinderError`` (a RuntimeError), as the reference's std::ru
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -36,6 +37,24 @@ def _f64(a, n=None, name="array"):
     if n is not None and a.size != n:
         raise ValueError(f"{name} has {a.size} elements, expected {n}")
     return a
+
+
+_PINNED_MIN_BYTES = 1 << 20
+
+
+def _out(n, dtype):
+    """A fresh 1-D output array of n elements.  From 1 MiB up it lives in page-locked memory from
+    the library's cache, so the device-to-host copy into it runs at link speed; the buffer goes
+    back to the cache when the array (and every view of it) is gone."""
+    dt = np.dtype(dtype)
+    nbytes = int(n) * dt.itemsize
+    if nbytes < _PINNED_MIN_BYTES:
+        return np.empty(int(n), dt)
+    p = C.c_void_p()
+    check(lib().binder_pinned_alloc(nbytes, C.byref(p)))
+    buf = (C.c_char * nbytes).from_address(p.value)
+    weakref.finalize(buf, lib().binder_pinned_free, p.value, nbytes)
+    return np.frombuffer(buf, dtype=dt, count=int(n))
 
 
 def _i32(a, n=None, name="array"):
@@ -113,8 +132,8 @@ class Registration:
     def sampler(self, seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
                 sample_likelihood_parameters, sample_transformation_parameters):
         N = self._N
-        mean = np.zeros(self._V * N, np.float64)
-        cov = np.zeros(self._V * N * N, np.float64)
+        mean = _out(self._V * N, np.float64)
+        cov = _out(self._V * N * N, np.float64)
         check(lib().binder_registration_sampler(
             self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, int(N_b), int(N_s), int(sample_gamma),
             int(sample_gamma_every), int(sample_posteriors), int(sample_likelihood_parameters),
@@ -123,7 +142,7 @@ class Registration:
 
     # -- getters / setters -------------------------------------------------------------------
     def get_final_locations_as_numpy_array(self):
-        out = np.zeros(self._V * self._N, np.float32)
+        out = _out(self._V * self._N, np.float32)
         check(lib().binder_registration_get_final_locations(self._h, out))
         return out.reshape(*self._shape, self._N)
 
@@ -131,7 +150,7 @@ class Registration:
         return self.get_final_locations_as_numpy_array().reshape(-1)
 
     def get_dream_locations(self):
-        out = np.zeros(self._V * self._N, np.float32)
+        out = _out(self._V * self._N, np.float32)
         check(lib().binder_registration_get_dream_locations(self._h, out))
         return out
 
@@ -247,7 +266,7 @@ class NonLinearTransformation:
 
     def smooth_deformation(self, deformation):
         N = self._N
-        out = np.zeros(self._V * N, np.float32)
+        out = _out(self._V * N, np.float32)
         cost = C.c_double(0)
         check(lib().binder_transform_smooth_deformation(
             self._h, _f32(deformation, self._V * N, "deformation"), out, C.byref(cost)))
@@ -256,7 +275,7 @@ class NonLinearTransformation:
     def sampleDeformationField(self, deformationField, number_of_samples):
         n = int(number_of_samples)
         N = self._N
-        out = np.zeros(max(n, 0) * self._V * N, np.float32)
+        out = _out(max(n, 0) * self._V * N, np.float32)
         check(lib().binder_transform_sample_deformation_field(
             self._h, _f32(deformationField, self._V * N, "deformationField"), n, out))
         return out.reshape(n, *self._shape, N)
@@ -266,7 +285,7 @@ class NonLinearTransformation:
         """``NonLinearTransformation.up_sample`` (cpu/bindings.cpp:408-434), FP64 on the GPU."""
         N = 2 if int(N_z_o) == 1 else 3
         Vi = int(N_x) * int(N_y) * int(N_z)
-        out = np.zeros(int(N_x_o) * int(N_y_o) * int(N_z_o) * N, np.float64)
+        out = _out(int(N_x_o) * int(N_y_o) * int(N_z_o) * N, np.float64)
         check(lib().binder_transform_up_sample(
             _f64(deformation_field, Vi * N, "deformation_field"), int(N_x), int(N_y), int(N_z),
             int(N_x_o), int(N_y_o), int(N_z_o), int(threads), out))
@@ -283,7 +302,7 @@ class topology_correction_3D:
                          Ny_v, Nz_v):
         V = int(Nx_v) * int(Ny_v) * int(Nz_v)
         field = _f64(h_init, V * 3, "h_init")
-        out = np.zeros(V * 3, np.float64)
+        out = _out(V * 3, np.float64)
         stats = np.zeros(6, np.int64)
         check(lib().binder_topology_correct_3d(
             field, float(e1), float(e2), int(max_outer_it), int(max_it), int(threads),
@@ -305,7 +324,7 @@ class topology_correction_2D:
                          Ny_v):
         V = int(Nx_v) * int(Ny_v)
         field = _f64(h_init, V * 2, "h_init")
-        out = np.zeros(V * 2, np.float64)
+        out = _out(V * 2, np.float64)
         stats = np.zeros(6, np.int64)
         check(lib().binder_topology_correct_2d(
             field, float(e1), float(e2), int(max_outer_it), int(max_it), int(threads),
@@ -324,7 +343,7 @@ def kernel_launch_count():
 def compute_jacobian_determinant_3D(field, Nx, Ny, Nz, voxel_size_x, voxel_size_y, voxel_size_z):
     """``_core.compute_jacobian_determinant_3D`` (cpu/bindings.cpp:564-593), FP64 on the GPU."""
     V = int(Nx) * int(Ny) * int(Nz)
-    J = np.zeros(V, np.float64)
+    J = _out(V, np.float64)
     check(lib().binder_jacobian_determinant_3d(_f64(field, V * 3, "field"), int(Nx), int(Ny),
                                                int(Nz), float(voxel_size_x), float(voxel_size_y),
                                                float(voxel_size_z), J))
@@ -343,7 +362,7 @@ def resize_linear(field, output_shape, scale=1.0):
     ish = f.shape[:nd] + (1,) * (3 - nd)
     osh = sp + (1,) * (3 - nd)
     N = f.shape[-1]
-    out = np.zeros(int(np.prod(osh)) * N, np.float64)
+    out = _out(int(np.prod(osh)) * N, np.float64)
     check(lib().binder_resize_linear(_f64(f, f.size, "field"), *ish, int(N), *osh, float(scale),
                                      out))
     return out.reshape(*sp, N)
@@ -352,7 +371,7 @@ def resize_linear(field, output_shape, scale=1.0):
 def compute_jacobian_determinant_2D(field, Nx, Ny, voxel_size_x, voxel_size_y):
     """``_core.compute_jacobian_determinant_2D`` (cpu/bindings.cpp:535-560), FP64 on the GPU."""
     V = int(Nx) * int(Ny)
-    J = np.zeros(V, np.float64)
+    J = _out(V, np.float64)
     check(lib().binder_jacobian_determinant_2d(_f64(field, V * 2, "field"), int(Nx), int(Ny),
                                                float(voxel_size_x), float(voxel_size_y), J))
     return J.reshape(int(Nx), int(Ny))

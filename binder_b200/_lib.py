@@ -38,7 +38,7 @@ EXPORTS = [
     "binder_jacobian_determinant_3d_noalloc", "binder_jacobian_noalloc_max_voxels",
     "binder_jacobian_determinant_2d", "binder_transform_up_sample", "binder_resize_linear",
     "binder_resample_matrix", "binder_pyramid_create", "binder_pyramid_destroy",
-    "binder_pyramid_level",
+    "binder_pyramid_level", "binder_pinned_alloc", "binder_pinned_free",
 ]
 
 
@@ -101,6 +101,8 @@ def _declare(lib):
         "binder_pyramid_create": [C.POINTER(_P), _i32, _i32, _P, _i, _i, _i, _i, _i, _i, _f64,
                                   _f64, _d, _i, _i, _i, _i],
         "binder_pyramid_destroy": [_P],
+        "binder_pinned_alloc": [C.c_size_t, C.POINTER(_P)],
+        "binder_pinned_free": [_P, C.c_size_t],
         "binder_pyramid_level": [_P, _i, _P, _i, _d, _P, _i, _i, _P, _P],
         "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],

@@ -1,5 +1,7 @@
 // extern "C" boundary: status codes instead of exceptions, thread-local error text.
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -270,6 +272,50 @@ int binder_registration_profile_stage(binder_registration *h, int stage, int n, 
 }
 
 long long binder_kernel_launch_count(void) { return binder::launch_counter(); }
+
+// Page-locked host buffers for outputs, cached by size: a device-to-host copy into pinned memory
+// runs at PCIe/C2C speed, one into fresh pageable memory pays the driver's staging and the first
+// touch of every page.  Freed buffers are kept for reuse up to kPinnedCacheBytes in total.
+namespace {
+constexpr size_t kPinnedCacheBytes = size_t(8) << 30;
+std::mutex g_pinned_mu;
+std::multimap<size_t, void *> g_pinned_free;
+size_t g_pinned_cached = 0;
+}  // namespace
+
+int binder_pinned_alloc(size_t bytes, void **out) {
+    return guard([&] {
+        NEED(out);
+        *out = nullptr;
+        BINDER_CHECK(bytes > 0, "size must be positive");
+        {
+            std::lock_guard<std::mutex> lock(g_pinned_mu);
+            auto it = g_pinned_free.find(bytes);
+            if (it != g_pinned_free.end()) {
+                *out = it->second;
+                g_pinned_cached -= bytes;
+                g_pinned_free.erase(it);
+                return;
+            }
+        }
+        BINDER_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocDefault));
+    });
+}
+
+int binder_pinned_free(void *p, size_t bytes) {
+    return guard([&] {
+        if (!p) return;
+        {
+            std::lock_guard<std::mutex> lock(g_pinned_mu);
+            if (g_pinned_cached + bytes <= kPinnedCacheBytes) {
+                g_pinned_free.emplace(bytes, p);
+                g_pinned_cached += bytes;
+                return;
+            }
+        }
+        BINDER_CUDA(cudaFreeHost(p));
+    });
+}
 
 int binder_transform_create(binder_transform **out, double gamma_x, double gamma_y,
                             double gamma_z, double voxels_size_x, double voxels_size_y,

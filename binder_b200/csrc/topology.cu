@@ -567,7 +567,13 @@ template <typename T>
 struct DBuf {
     T *p = nullptr;
     cudaStream_t s = 0;
+    DBuf() = default;
     DBuf(size_t n, cudaStream_t stream) : s(stream) { p = dev_alloc_n<T>(n, s); }
+    void alloc(size_t n, cudaStream_t stream) {
+        dev_free(p, s);
+        s = stream;
+        p = dev_alloc_n<T>(n, s);
+    }
     ~DBuf() { dev_free(p, s); }
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
@@ -718,24 +724,35 @@ struct TopologyWorkspace::Impl {
     int nx, ny, nz;
     int N;  // 3, or 2 for an image (nz == 1)
     long V, cells;
-    DBuf<double> pos, grad, jc, div, t1, t2;
-    DBuf<int> list, sorted;
+    cudaStream_t st;  // pool stream of every buffer
+    // always present: what the Jacobian statistics need
+    DBuf<double> pos;
     DBuf<Red> red;
     DBuf<unsigned> flags;
+    // allocated when a correction first iterates (most calls find every Jacobian in range)
+    bool ready = false;
+    DBuf<double> grad, jc, div, t1, t2;
+    DBuf<int> list, sorted;
     DBuf<double> H[3], cs[3];
-    Impl(int x, int y, int z, cudaStream_t st)
+    Impl(int x, int y, int z, cudaStream_t s)
         : nx(x), ny(y), nz(z), N(z == 1 ? 2 : 3), V((long)x * y * z),
-          cells(z == 1 ? (long)(x - 1) * (y - 1) : (long)(x - 1) * (y - 1) * (z - 1)),
-          pos(V * N, st), grad(V * N * N, st), jc(cells * (z == 1 ? 4 : 8), st), div(V * N, st),
-          t1(V * N, st), t2(V * N, st), list(cells, st), sorted(cells, st), red(1, st),
-          flags(1, st),
-          H{DBuf<double>((size_t)x * x, st), DBuf<double>((size_t)y * y, st),
-            DBuf<double>((size_t)z * z, st)},
-          cs{DBuf<double>(x, st), DBuf<double>(y, st), DBuf<double>(z, st)} {
-        const int dims[3] = {x, y, z};
+          cells(z == 1 ? (long)(x - 1) * (y - 1) : (long)(x - 1) * (y - 1) * (z - 1)), st(s),
+          pos(V * N, s), red(1, s), flags(1, s) {}
+    void ensure() {
+        if (ready) return;
+        grad.alloc(V * N * N, st);
+        jc.alloc(cells * (nz == 1 ? 4 : 8), st);
+        div.alloc(V * N, st);
+        t1.alloc(V * N, st);
+        t2.alloc(V * N, st);
+        list.alloc(cells, st);
+        sorted.alloc(cells, st);
+        const int dims[3] = {nx, ny, nz};
         const double pi = 3.14159265358979323846;
         for (int a = 0; a < 3; ++a) {
             const int n = dims[a];
+            H[a].alloc((size_t)n * n, st);
+            cs[a].alloc(n, st);
             std::vector<double> M((size_t)n * n), c(n);
             hartley_matrix(n, M.data());
             for (int k = 0; k < n; ++k) c[k] = std::cos(2.0 * pi * k / (n * 1.0));
@@ -745,6 +762,7 @@ struct TopologyWorkspace::Impl {
                                         cudaMemcpyHostToDevice, st));
             BINDER_CUDA(cudaStreamSynchronize(st));  // the host tables go out of scope
         }
+        ready = true;
     }
 };
 
@@ -794,6 +812,7 @@ TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int m
                                      (int)lim_smem));
     int outer = 0;
     while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+        w.ensure();
         Red c = corners();
         int inner = 0;
         while ((c.below > 0 || c.above > 0) && inner < max_inner) {
@@ -892,6 +911,7 @@ TopologyResult TopologyWorkspace::run2d(double e1, double e2, int max_outer, int
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim_smem));
     int outer = 0;
     while ((jmin < e1 || jmax > e2) && outer < max_outer) {
+        w.ensure();
         Red c = corners();
         int inner = 0;
         while ((c.below > 0 || c.above > 0) && inner < max_inner) {

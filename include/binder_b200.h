@@ -17,6 +17,7 @@
 #ifndef BINDER_B200_H
 #define BINDER_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -153,6 +154,11 @@ int binder_registration_profile_stage(binder_registration *h, int stage, int n, 
 /* No counterpart in the reference: number of kernels this library has launched in this process
  * (each replay of a captured CUDA graph counts all of its kernels). */
 long long binder_kernel_launch_count(void);
+/* No counterpart in the reference: page-locked host memory for output arrays, cached by size
+ * (a later alloc of the same size reuses a freed buffer).  binder_pinned_free takes the size
+ * given to binder_pinned_alloc. */
+int binder_pinned_alloc(size_t bytes, void **out);
+int binder_pinned_free(void *p, size_t bytes);
 
 /* ---- _core.NonLinearTransformation --------------------------------------------------------- */
 
