@@ -129,6 +129,11 @@ void MStep::init(int x, int y, int z, cudaStream_t s) {
     t1 = dalloc<float>((size_t)V * 3, s);
     t2 = dalloc<float>((size_t)V * 3, s);
     precision = default_precision();
+    for (int i = 0; i < 2; ++i) {
+        BINDER_CUDA(cudaStreamCreate(&side[i]));
+        BINDER_CUDA(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
+    }
+    BINDER_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
 }
 
 int default_precision() {
@@ -141,6 +146,14 @@ void MStep::release(cudaStream_t s) {
     dct.release(s);
     dfree(t1, s);
     dfree(t2, s);
+    for (int i = 0; i < 2; ++i) {
+        if (side[i]) cudaStreamSynchronize(side[i]), cudaStreamDestroy(side[i]);
+        if (join[i]) cudaEventDestroy(join[i]);
+        side[i] = nullptr;
+        join[i] = nullptr;
+    }
+    if (fork) cudaEventDestroy(fork);
+    fork = nullptr;
 }
 
 void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
@@ -153,21 +166,41 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     a.skip = skip;
     a.ny = ny;
     a.nz = nz;
-    const bool two_d = nz == 1;
-    const int ncomp = two_d ? 2 : 3;
+    const int ncomp = nz == 1 ? 2 : 3;
     a.dims = ncomp;
     a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
     a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
     const bool tc = precision != kPrecFP32Simt;
     const int planes = precision == kPrecTF32 ? 1 : 2;
+    // the tensor-core path runs one chain of passes per component, each on its own stream
+    const bool branches = tc && side[0] && side[1];
+    if (branches) {
+        BINDER_CUDA(cudaEventRecord(fork, s));
+        for (int c = 1; c < ncomp; ++c) BINDER_CUDA(cudaStreamWaitEvent(side[c - 1], fork, 0));
+        for (int c = 0; c < ncomp; ++c)
+            run_chain(a, c, 1, c == 0 ? s : side[c - 1], r, d, xpos, tc, planes);
+        for (int c = 1; c < ncomp; ++c) {
+            BINDER_CUDA(cudaEventRecord(join[c - 1], side[c - 1]));
+            BINDER_CUDA(cudaStreamWaitEvent(s, join[c - 1], 0));
+        }
+    } else {
+        run_chain(a, 0, ncomp, s, r, d, xpos, tc, planes);
+    }
+}
+
+// the pass sequence of one M-step for components [c0, c0 + nc) on stream s
+void MStep::run_chain(AxisArgs<float> a, int c0, int nc, cudaStream_t s, const float *r, float *d,
+                  const float *xpos, bool tc, int planes) {
+    a.comp0 = c0;
+    const bool two_d = nz == 1;
     auto pass = [&](int axis, bool inverse, int mode) {
         if (tc)
             launch_axis_pass_tc(a, inverse ? dct.uinv[axis] : dct.ufwd[axis],
-                                mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, ncomp,
+                                mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, nc,
                                 planes, s);
         else
-            launch_axis_pass(a, mode, ncomp, s);
+            launch_axis_pass(a, mode, nc, s);
     };
     if (two_d) {
         // an nx x ny image, components (x, y): forward along y, then x with the prior scaling,

@@ -28,12 +28,18 @@ struct MStep {
     DctSet dct;
     float *t1 = nullptr, *t2 = nullptr;
     int precision = kPrecFP32Simt;  // TransformPrecision
+    // the tensor-core passes of components 1 and 2 run on their own streams (graph branches), so
+    // one component's last partial wave of tiles overlaps the other components' passes
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
     // buffers from the stream-ordered pool on stream s
     void init(int nx, int ny, int nz, cudaStream_t s);
     void release(cudaStream_t s);
     void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
                  double sigma2, int sample, int want_raw, int every, uint64_t seed, uint32_t chain,
                  double rho_p, const double eta2[3], const int *skip, cudaStream_t s);
+    void run_chain(AxisArgs<float> a, int c0, int nc, cudaStream_t s, const float *r, float *d,
+                   const float *xpos, bool tc, int planes);
 };
 
 // A captured chunk of EM iterations, replayed by later EM calls while the parameters it was

@@ -639,6 +639,10 @@ int estep_grid(bool sample, int K, int L, long V, int dim) {
     const void *fn = dim == 3 ? estep_fn<3>(sample, K) : estep_fn<2>(sample, K);
     const int tpb = (!sample && K <= kSmallK) ? kFastThreads : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // all of the unified L1 / shared array as shared memory, so the CTAs the occupancy query
+    // counts are the CTAs that become resident (the default carveout may be smaller)
+    BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
     BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tpb, smem));
     per_sm = per_sm < 1 ? 1 : per_sm;
     const long need = (V + tpb - 1) / tpb;

@@ -41,6 +41,7 @@ struct AxisArgs {
     const T *in;
     T *out;
     long comp_stride;  // elements between components (V)
+    int comp0;         // component of blockIdx.z == 0 (the tensor-core passes run one per launch)
     const T *M;        // n x n, row-major
     const T *M2;       // second matrix of a fused pass (inverse), n x n
     int n;

@@ -48,6 +48,7 @@ struct UArgs {
     const float *xpos;
     int ny, nz;
     int dims;  // 3, or 2 for an image (the contiguous axis is then component 1)
+    int comp0;  // component of blockIdx.z == 0
     const int *skip;
 };
 
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     const uint32_t tmem = *holder;
     const uint32_t tlane = (uint32_t)(warp * 32) << 16;
 
-    const int comp = blockIdx.z;
+    const int comp = a.comp0 + (int)blockIdx.z;
     const float *in = a.in + comp * a.V;
     float *out = a.out + comp * a.V;
     const long nlines = a.outer * a.s;
@@ -439,6 +440,11 @@ void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
     BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
     BINDER_CUDA(cudaFuncSetAttribute(umma_axis_kernel<MODE, PLANES>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the whole unified L1 / shared array as shared memory: with the default carveout the
+    // driver may configure too little for two of these CTAs, halving the SM's occupancy
+    BINDER_CUDA(cudaFuncSetAttribute(umma_axis_kernel<MODE, PLANES>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
     const long tiles = (a.outer * a.s + kLines - 1) / kLines;
     BINDER_CHECK(tiles < (1L << 31), "transform grid too large");
     dim3 grid((unsigned)tiles, 1, (unsigned)ncomp);
@@ -485,7 +491,7 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     a.D = b.D; a.st = b.st; a.sigma2 = b.sigma2; a.sample = b.sample; a.want_raw = b.want_raw;
     a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
     for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
-    a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.skip = b.skip;
+    a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.comp0 = b.comp0; a.skip = b.skip;
 #define BINDER_UMMA_CASE(MODE)                                                    \
     case MODE:                                                                    \
         if (planes == 2) launch_umma<MODE, 2>(a, ncomp, s);                       \
