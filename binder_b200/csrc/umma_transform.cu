@@ -411,6 +411,318 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     if (warp == 0) umma::tmem_dealloc(tmem, ncols);
 }
 
+
+// ---- warp-specialised pass: 4 producer / epilogue warps + 1 MMA warp -------------------------
+// Warps 0-3 own the tile's 128 lines (thread tid <-> line tid <-> TMEM lane tid): they load the
+// data chunks from global memory (prefetched kPre chunks ahead in registers), split them into
+// TF32 planes in an A stage, copy their part of the matrix chunk into a B slot (cp.async), and
+// arrive on full[stage].  Warp 4 (one lane) waits on full[], issues the chunk's MMAs and commits
+// them to done[]; the producers only wait on done[] before reusing a stage, two chunks later, so
+// the MMA issue -- which blocks while the tensor core's queue is full -- never stalls them.
+constexpr int kWsThreads = 160;
+constexpr int kPre = 2;  // A chunks in flight per producer thread
+
+template <int MODE, int PLANES>
+__global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp < 4;
+    const int Npad = a.Npad, n = a.n, nkc = a.nkc;
+    const uint32_t bplane = (uint32_t)Npad * kKC;
+    float *As = reinterpret_cast<float *>(smem_raw);  // [2 stages][PLANES][kAPlane]
+    float *Bs = As + 2 * PLANES * kAPlane;            // [3 slots][PLANES][bplane]
+    uint64_t *full = reinterpret_cast<uint64_t *>(Bs + 3 * PLANES * bplane);  // [2]
+    uint64_t *done = full + 2;                                               // [3]
+    uint64_t *drain = done + 3;                                              // [1]
+    uint32_t *holder = reinterpret_cast<uint32_t *>(drain + 1);
+    int *s_err = reinterpret_cast<int *>(holder + 1);
+    __shared__ double red[32];
+
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)Npad) ncols <<= 1;
+    if (warp == 0) umma::tmem_alloc(holder, ncols);
+    if (tid == 32) {
+        umma::mbar_init(&full[0], 128);
+        umma::mbar_init(&full[1], 128);
+        for (int i = 0; i < 3; ++i) umma::mbar_init(&done[i], 1);
+        umma::mbar_init(drain, 1);
+        *s_err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *holder;
+    const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
+
+    const int comp = a.comp0 + (int)blockIdx.z;
+    const float *in = a.in + comp * a.V;
+    float *out = a.out + comp * a.V;
+    const long nlines = a.outer * a.s;
+    const long l0 = (long)blockIdx.x * kLines;
+    const bool contig = (a.s == 1);
+    const long lg = l0 + (producer ? tid : 0);
+    const bool valid = producer && lg < nlines;
+    const long o = valid ? lg / a.s : 0, t = valid ? lg - o * a.s : 0;
+    const long lbase = o * (long)n * a.s + t;  // element (line, j) at lbase + j * s
+    const int cr = lane & 7, cq = lane >> 3;   // contiguous-axis load mapping
+
+    if (!producer) {
+        // ---- MMA warp ------------------------------------------------------------------------
+        if (lane == 0) {
+            const uint32_t idesc = umma::instr_desc(kLines, Npad, umma::kFmtTF32);
+            for (int kc = 0; kc < nkc; ++kc) {
+                if (!umma::mbar_wait(&full[kc & 1], (uint32_t)(kc >> 1) & 1u, kWaitLimit) ||
+                    *(volatile int *)s_err) {
+                    *(volatile int *)s_err = 1;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t abase = umma::smem_u32(As + (kc & 1) * PLANES * kAPlane);
+                const uint32_t bbase = umma::smem_u32(Bs + (kc % 3) * PLANES * bplane);
+#pragma unroll
+                for (int ks = 0; ks < kKC / 8; ++ks) {
+                    const uint32_t ao = (uint32_t)ks * 2u * 2048u;
+                    const uint32_t bo = (uint32_t)ks * 2u * (uint32_t)Npad * 16u;
+                    const uint64_t ahi = umma::smem_desc(abase + ao, 2048u, 128u);
+                    const uint64_t bhi = umma::smem_desc(bbase + bo, (uint32_t)Npad * 16u, 128u);
+                    umma::mma_tf32(tmem, ahi, bhi, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+                    if (PLANES == 2) {
+                        const uint64_t alo = umma::smem_desc(abase + kAPlane * 4u + ao, 2048u, 128u);
+                        const uint64_t blo =
+                            umma::smem_desc(bbase + bplane * 4u + bo, (uint32_t)Npad * 16u, 128u);
+                        umma::mma_tf32(tmem, ahi, blo, idesc, 1u);
+                        umma::mma_tf32(tmem, alo, bhi, idesc, 1u);
+                    }
+                }
+                umma::commit(&done[kc % 3]);
+            }
+        }
+    } else {
+        // ---- producers -----------------------------------------------------------------------
+        auto load_global = [&](int kc, AChunk &r) {
+            if (kc >= nkc) return;
+            if (contig) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int line = (warp + 4 * i) * 8 + cr;
+                    const long g = l0 + line;
+                    const int j0 = kc * kKC + cq * 4;
+                    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (g < nlines) {
+                        const float *p = in + g * n + j0;
+                        if ((n & 3) == 0 && j0 + 3 < n) {
+                            v = __ldg(reinterpret_cast<const float4 *>(p));
+                        } else {
+                            v.x = j0 < n ? __ldg(p) : 0.f;
+                            v.y = j0 + 1 < n ? __ldg(p + 1) : 0.f;
+                            v.z = j0 + 2 < n ? __ldg(p + 2) : 0.f;
+                            v.w = j0 + 3 < n ? __ldg(p + 3) : 0.f;
+                        }
+                    }
+                    r.v[i] = v;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j0 = kc * kKC + q * 4;
+                    float4 v;
+                    v.x = (valid && j0 < n) ? __ldg(in + lbase + (long)j0 * a.s) : 0.f;
+                    v.y = (valid && j0 + 1 < n) ? __ldg(in + lbase + (long)(j0 + 1) * a.s) : 0.f;
+                    v.z = (valid && j0 + 2 < n) ? __ldg(in + lbase + (long)(j0 + 2) * a.s) : 0.f;
+                    v.w = (valid && j0 + 3 < n) ? __ldg(in + lbase + (long)(j0 + 3) * a.s) : 0.f;
+                    r.v[q] = v;
+                }
+            }
+        };
+        auto issue_b = [&](int kc) {
+            if (kc < nkc) {
+                const float *srcb = a.B1 + (size_t)kc * 2 * bplane;
+                float *Bp = Bs + (kc % 3) * PLANES * bplane;
+                const int nv = PLANES * (int)bplane / 4;
+                for (int qv = tid; qv < nv; qv += 128) umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
+            }
+            umma::cp_async_commit();  // possibly empty: one group per chunk
+        };
+        // one chunk: false once this warp has to stop (a wait gave up, or another warp did)
+        auto step = [&](int kc, AChunk &cur) -> bool {
+            // stage kc & 1 and slot (kc + 1) % 3 were last read by the MMAs of chunk kc - 2
+            if (kc >= 2) {
+                const bool ok = umma::mbar_wait(&done[(kc - 2) % 3],
+                                                (uint32_t)((kc - 2) / 3) & 1u, kWaitLimit);
+                if (__any_sync(0xffffffffu, !ok) || *(volatile int *)s_err) {
+                    *(volatile int *)s_err = 1;
+                    return false;
+                }
+            }
+            issue_b(kc + 1);
+            float *Ap = As + (kc & 1) * PLANES * kAPlane;
+            if (contig) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    store_split<PLANES>(Ap, a_slot((warp + 4 * i) * 8 + cr, cq), cur.v[i]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) store_split<PLANES>(Ap, a_slot(tid, q), cur.v[q]);
+            }
+            load_global(kc + kPre, cur);                          // in flight for kPre chunks
+            asm volatile("cp.async.wait_group 1;" ::: "memory");  // my part of B chunk kc landed
+            umma::fence_proxy_async_smem();
+            umma::mbar_arrive(&full[kc & 1]);
+            return true;
+        };
+        AChunk pre[kPre];  // chunks kc .. kc + kPre - 1 in flight; static indices after unrolling
+#pragma unroll
+        for (int q = 0; q < kPre; ++q) load_global(q, pre[q]);
+        issue_b(0);
+        bool go = true;
+        for (int kc = 0; kc < nkc && go; kc += kPre) {
+#pragma unroll
+            for (int q = 0; q < kPre; ++q)
+                if (go && kc + q < nkc) go = step(kc + q, pre[q]);
+        }
+        umma::cp_async_wait_all();
+        // the whole accumulation
+        if (!*(volatile int *)s_err) {
+            const bool ok = umma::mbar_wait(&done[(nkc - 1) % 3],
+                                            (uint32_t)((nkc - 1) / 3) & 1u, kWaitLimit);
+            if (__any_sync(0xffffffffu, !ok)) *(volatile int *)s_err = 1;
+        }
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+
+    double part_cost = 0.0, part_raw = 0.0;
+    const uint32_t sweep = (MODE == kEpiSpectralOut && a.sample) ? (uint32_t)a.st->sweep : 0u;
+    const bool want_raw = MODE == kEpiSpectralOut && a.want_raw && (a.st->sweep % a.every == 0);
+    const double gamma = MODE == kEpiSpectralOut ? a.st->gamma[comp] : 0.0;
+    const float gs2 = (float)(gamma * a.sigma2);
+    if (producer && !*s_err) {
+        // ---- epilogue: 32 TMEM columns at a time -------------------------------------------
+        const int nchunks = (n + 31) / 32;
+        if (contig) {
+            float *stg = reinterpret_cast<float *>(smem_raw) + warp * 32 * 33;
+            float rowc = 0.0f;
+            if (MODE == kEpiPositions && !a.xpos) {
+                const int gi = (int)(l0 + warp * 32 + lane);  // 3D: x * ny + y; 2D: x
+                rowc = a.dims == 2 ? (float)gi
+                                   : (comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
+            }
+            for (int cc = 0; cc < nchunks; ++cc) {
+                float v[32];
+                umma::tmem_ld32(tmem + tlane + (uint32_t)(cc * 32), v);
+#pragma unroll
+                for (int m = 0; m < 32; ++m) stg[lane * 33 + m] = v[m];
+                __syncwarp();
+                const int k = cc * 32 + lane;
+#pragma unroll 4
+                for (int r = 0; r < 32; ++r) {
+                    const long g = l0 + warp * 32 + r;
+                    const float rc = __shfl_sync(0xffffffffu, rowc, r);
+                    if (g < nlines && k < n) {
+                        float val = stg[r * 33 + lane];
+                        if (MODE == kEpiPositions)
+                            val += a.xpos ? __ldg(a.xpos + comp * a.V + g * n + k)
+                                          : (comp == a.dims - 1 ? (float)k : rc);
+                        out[g * n + k] = val;
+                    }
+                }
+                __syncwarp();
+            }
+        } else {
+            float dnext[32];
+            auto load_dchunk = [&](int cc) {
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = cc * 32 + m;
+                    dnext[m] = (valid && k < n) ? __ldg(a.D + (long)k * a.s + t) : 0.0f;
+                }
+            };
+            if (MODE == kEpiSpectralOut) load_dchunk(0);
+            for (int cc = 0; cc < nchunks; ++cc) {
+                float v[32], dcur[32];
+                umma::tmem_ld32(tmem + tlane + (uint32_t)(cc * 32), v);
+                if (MODE == kEpiSpectralOut) {
+#pragma unroll
+                    for (int m = 0; m < 32; ++m) dcur[m] = dnext[m];
+                    if (cc + 1 < nchunks) load_dchunk(cc + 1);
+                }
+                if (!valid) continue;
+                float ccost = 0.0f;
+                float *op = out + lbase;
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = cc * 32 + m;
+                    if (k < n) {
+                        float val = v[m];
+                        if (MODE == kEpiSpectralOut) {
+                            const float Dv = dcur[m];
+                            const float f = __frcp_rn(fmaf(gs2, Dv, 1.0f));
+                            val *= f;
+                            if (a.sample)
+                                val += sqrtf((float)a.sigma2 * f) *
+                                       prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
+                                                       a.chain, comp);
+                            ccost += Dv * val * val;
+                        }
+                        op[(long)k * a.s] = val;
+                    }
+                }
+                if (MODE == kEpiSpectralOut) {
+                    part_cost += 0.5 * gamma * (double)ccost;
+                    if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)ccost;
+                }
+            }
+        }
+    }
+    if (MODE == kEpiSpectralOut) {
+        const double sc = block_sum(part_cost, red);
+        if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
+        if (a.want_raw) {
+            const double sr = block_sum(part_raw, red);
+            if (tid == 0) atomicAdd(&a.st->raw_reg, sr);
+        }
+    }
+
+    // ---- teardown: after an error, let every tcgen05 op still in flight finish (bounded) ----
+    if (*s_err && tid == 128) {
+        umma::commit(drain);  // arrives once all MMAs this thread issued have completed
+        umma::mbar_wait(drain, 0, kWaitLimit);
+        if (a.st) atomicOr(&a.st->flags, (unsigned)kFlagTensorTimeout);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
+template <int MODE, int PLANES>
+void launch_ws(const UArgs &a, int ncomp, cudaStream_t s) {
+    // A stages, B slots, then 6 mbarriers, the TMEM address and the error word
+    size_t need = (size_t)(2 * PLANES * kAPlane + 3 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
+    const size_t staging = (size_t)4 * 32 * 33 * sizeof(float) + 64;  // contiguous-axis epilogue
+    if (need < staging) need = staging;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)a.Npad) ncols <<= 1;
+    // never more CTAs per SM than its 512 TMEM columns hold at once (a surplus CTA would only
+    // wait inside tcgen05.alloc): pad the shared-memory request accordingly
+    const size_t per_sm = 228 * 1024;
+    const size_t max_ctas = 512 / ncols;
+    const size_t floor_smem = per_sm / (max_ctas + 1) + 1024;
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
+    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+    const long tiles = (a.outer * a.s + kLines - 1) / kLines;
+    BINDER_CHECK(tiles < (1L << 31), "transform grid too large");
+    dim3 grid((unsigned)tiles, 1, (unsigned)ncomp);
+    count_launch(), umma_ws_kernel<MODE, PLANES><<<grid, kWsThreads, smem, s>>>(a);
+    BINDER_CUDA(cudaGetLastError());
+}
+
 float tf32_rna_host(float x) {
     uint32_t u;
     std::memcpy(&u, &x, 4);
@@ -494,16 +806,16 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.comp0 = b.comp0; a.skip = b.skip;
 #define BINDER_UMMA_CASE(MODE)                                                    \
     case MODE:                                                                    \
-        if (planes == 2) launch_umma<MODE, 2>(a, ncomp, s);                       \
-        else launch_umma<MODE, 1>(a, ncomp, s);                                   \
+        if (planes == 2) launch_ws<MODE, 2>(a, ncomp, s);                         \
+        else launch_ws<MODE, 1>(a, ncomp, s);                                     \
         break;
     switch (mode) {
         BINDER_UMMA_CASE(kEpiNone)
         BINDER_UMMA_CASE(kEpiPositions)
         case kEpiSpectralOut:
             BINDER_CHECK(b.outer == 1, "prior scaling runs on the outermost axis");
-            if (planes == 2) launch_umma<kEpiSpectralOut, 2>(a, ncomp, s);
-            else launch_umma<kEpiSpectralOut, 1>(a, ncomp, s);
+            if (planes == 2) launch_ws<kEpiSpectralOut, 2>(a, ncomp, s);
+            else launch_ws<kEpiSpectralOut, 1>(a, ncomp, s);
             break;
         case kEpiSpectral:
             BINDER_CHECK(M2 && M2->n == b.n, "fused pass needs the inverse matrix");
