@@ -39,6 +39,7 @@ EXPORTS = [
     "binder_jacobian_determinant_2d", "binder_transform_up_sample", "binder_resize_linear",
     "binder_resample_matrix", "binder_pyramid_create", "binder_pyramid_destroy",
     "binder_pyramid_level", "binder_pinned_alloc", "binder_pinned_free",
+    "binder_bin_signal_robust", "binder_bin_signal", "binder_center_of_mass", "binder_warp_image",
 ]
 
 
@@ -103,6 +104,10 @@ def _declare(lib):
         "binder_pyramid_destroy": [_P],
         "binder_pinned_alloc": [C.c_size_t, C.POINTER(_P)],
         "binder_pinned_free": [_P, C.c_size_t],
+        "binder_bin_signal_robust": [_P, _i, C.c_longlong, _i, _d, _d, _P, _P],
+        "binder_bin_signal": [_P, _i, C.c_longlong, _i, _P],
+        "binder_center_of_mass": [_i32, _i, _i, _i, _f64],
+        "binder_warp_image": [_f64, _i, _i, _i, _f64, C.c_longlong, _i, _f64],
         "binder_pyramid_level": [_P, _i, _P, _i, _d, _P, _i, _i, _P, _P],
         "binder_jacobian_determinant_3d_noalloc": [_f64, _i, _i, _i, _d, _d, _d, _f64,
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],

@@ -9,6 +9,7 @@
 #include "../../include/binder_b200.h"
 #include "engine.cuh"
 #include "multires.cuh"
+#include "preprocess.cuh"
 #include "resample.cuh"
 
 struct binder_registration {
@@ -433,6 +434,56 @@ int binder_pyramid_level(binder_pyramid *p, int resolution, const binder_registr
             }
             info_out[15] = li.non_zero_voxels;
         }
+    });
+}
+
+int binder_bin_signal_robust(const void *signal, int is_double, long long n, int number_of_bins,
+                             double lower_percentile, double higher_percentile,
+                             int32_t *binned_out, double *bin_edges_out) {
+    return guard([&] {
+        NEED(signal);
+        NEED(binned_out);
+        if (is_double)
+            binder::bin_signal_robust(static_cast<const double *>(signal), (long)n,
+                                      number_of_bins, lower_percentile, higher_percentile,
+                                      binned_out, bin_edges_out);
+        else
+            binder::bin_signal_robust(static_cast<const float *>(signal), (long)n,
+                                      number_of_bins, lower_percentile, higher_percentile,
+                                      binned_out, bin_edges_out);
+    });
+}
+
+int binder_bin_signal(const void *signal, int is_double, long long n, int number_of_bins,
+                      int32_t *binned_out) {
+    return guard([&] {
+        NEED(signal);
+        NEED(binned_out);
+        if (is_double)
+            binder::bin_signal(static_cast<const double *>(signal), (long)n, number_of_bins,
+                               binned_out);
+        else
+            binder::bin_signal(static_cast<const float *>(signal), (long)n, number_of_bins,
+                               binned_out);
+    });
+}
+
+int binder_center_of_mass(const int32_t *bins, int Nx, int Ny, int Nz, double out[3]) {
+    return guard([&] {
+        NEED(bins);
+        NEED(out);
+        if (!binder::center_of_mass_nonzero(bins, Nx, Ny, Nz, out))
+            throw binder::Error(BINDER_STATUS_INVALID_ARGUMENT, "no voxel has a non-zero bin");
+    });
+}
+
+int binder_warp_image(const double *image, int Nx, int Ny, int Nz, const double *positions,
+                      long long M, int order, double *out) {
+    return guard([&] {
+        NEED(image);
+        NEED(positions);
+        NEED(out);
+        binder::warp_image(image, Nx, Ny, Nz, positions, (long)M, order, out);
     });
 }
 

@@ -190,6 +190,29 @@ int binder_transform_up_sample(const double *field, int Nx, int Ny, int Nz, int 
  * pixel-centre-aligned linear interpolation, mirror boundaries). */
 int binder_resize_linear(const double *field, int Nx, int Ny, int Nz, int N, int Nx_o, int Ny_o,
                          int Nz_o, double scale, double *out);
+/* ---- preprocessing and output of the registration driver ----------------------------------
+ * No counterparts in the reference's module: the numpy / scipy / skimage steps that
+ * BINDER/FastRegistration.py runs around it, on the GPU.  Pointers may be host or device memory.
+ *
+ * utils.bin_signal_robust(signal, number_of_bins, lower, higher)   BINDER/utils.py:20-82
+ * signal: n values, float32 (is_double 0) or float64 (1), computed in that type with numpy's
+ * operation order (bit-identical bins); binned_out int32[n]; bin_edges_out (optional) the
+ * number_of_bins + 1 returned edges.  A constant signal is rejected. */
+int binder_bin_signal_robust(const void *signal, int is_double, long long n, int number_of_bins,
+                             double lower_percentile, double higher_percentile,
+                             int32_t *binned_out, double *bin_edges_out);
+/* utils.bin_signal(signal, number_of_bins)                          BINDER/utils.py:12-17 */
+int binder_bin_signal(const void *signal, int is_double, long long n, int number_of_bins,
+                      int32_t *binned_out);
+/* scipy.ndimage.center_of_mass(bins > 0) as FastRegistration.py:387-395 computes it; index
+ * space, exact (integer sums, one division).  No non-zero voxel: INVALID_ARGUMENT. */
+int binder_center_of_mass(const int32_t *bins, int Nx, int Ny, int Nz, double out[3]);
+/* the resampling of utils.save_warped_image (BINDER/utils.py:222-227): skimage.transform.warp of
+ * the moving image [Nx][Ny][Nz] (FP64) at positions [M][3] (index space) with order 0 or 1,
+ * zero outside, clipped to the input range as skimage clips; out [M] FP64. */
+int binder_warp_image(const double *image, int Nx, int Ny, int Nz, const double *positions,
+                      long long M, int order, double *out);
+
 /* ---- the multi-resolution step on the device ------------------------------------------------
  * No counterpart in the reference's module: FastRegistration.move_resolution
  * (BINDER/FastRegistration.py:550-650) plus the Registration set-up of run() (:443-486) for the

@@ -243,6 +243,24 @@ def resize_linear(field, oshape, scale=1.0):
     return z * scale
 
 
+def warp_image(image, positions, order=1):
+    """The resampling of BINDER/utils.py:222-227 (skimage.transform.warp with mode 'constant',
+    cval 0, clip, preserve_range), restated from scikit-image's published warp (not installed
+    here): scipy.ndimage.map_coordinates(order, mode='grid-constant', prefilter only above order
+    1), then the output clipped to the input's range, widened to 0 when 0 lies outside the input's
+    range but inside the output's."""
+    from scipy import ndimage as ndi
+    im = np.asarray(image, np.float64)
+    pos = np.asarray(positions, np.float64)
+    coords = np.moveaxis(pos, -1, 0)
+    out = ndi.map_coordinates(im, coords, order=order, mode="grid-constant", cval=0.0,
+                              prefilter=order > 1)
+    lo, hi = im.min(), im.max()
+    if not (lo <= 0.0 <= hi) and out.min() <= 0.0 <= out.max():
+        lo, hi = min(lo, 0.0), max(hi, 0.0)
+    return np.clip(out, lo, hi)
+
+
 def sample_field(field, D, gamma, sigma, shape, n, seed=1234, sweep0=0):
     nx, ny, nz = shape
     N = 2 if nz == 1 else 3

@@ -21,9 +21,24 @@ sys.path.insert(0, ROOT)
 
 from oracle import pyoracle  # noqa: E402
 
+REF_ROOT = "/root/reference"
+
 
 def grid(shape):
     return np.stack(np.indices(shape), -1).astype(np.float64)
+
+
+def reference_functions(names):
+    """Module-level functions of the reference's BINDER/utils.py, compiled from its source with
+    numpy as their only global (their other imports are not needed by these functions)."""
+    import ast
+    src = open(os.path.join(REF_ROOT, "BINDER", "utils.py")).read()
+    tree = ast.parse(src)
+    ns = {"np": np}
+    for node in tree.body:
+        if isinstance(node, ast.FunctionDef) and node.name in names:
+            exec(compile(ast.Module(body=[node], type_ignores=[]), "BINDER/utils.py", "exec"), ns)
+    return {n: ns[n] for n in names}
 
 
 def main():
@@ -133,6 +148,26 @@ def main():
         ups[f"oshape{k}"] = np.array(oshape)
         ups[f"out{k}"] = out.reshape(oshape + (N,))
     np.savez(os.path.join(HERE, "upsample_ref.npz"), ncases=2, **ups)
+    # intensity binning (BINDER/utils.py:12-82): the reference's own functions, taken from its
+    # source (the module itself imports packages absent here) and run under numpy
+    fns = reference_functions(["bin_signal", "bin_signal_robust"])
+    from binder_b200 import phantoms
+    prep = {}
+    img = phantoms.ellipsoid_phantom((40, 36, 30), 12, (3.0, 15.0), 1.0, 0.02, rng).astype(np.float64)
+    mask = (rng.random(img.shape) > 0.1).astype(np.float64)
+    img32 = (img * 3.7 + 0.2).astype(np.float32)
+    # 62 % of the mass at the minimum: the lower percentile needs the reference's raising loop
+    spiky = np.concatenate([np.zeros(5000), np.abs(rng.normal(0, 1, 3000)), [40.0]])
+    cases = [("f64", img * mask, 64), ("f32", img32, 32), ("spiky", spiky, 16)]
+    for name, sig, nb in cases:
+        b, e = fns["bin_signal_robust"](sig, nb)
+        prep[f"{name}_signal"] = sig
+        prep[f"{name}_bins"] = np.int32(nb)
+        prep[f"{name}_robust"] = b
+        prep[f"{name}_edges"] = e
+        prep[f"{name}_plain"] = fns["bin_signal"](sig, nb)
+    np.savez(os.path.join(HERE, "preprocess_ref.npz"), names=np.array([c[0] for c in cases]),
+             **prep)
     print("golden fixtures written to", HERE)
 
 
