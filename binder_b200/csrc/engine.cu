@@ -30,7 +30,14 @@ bool verbose() {
 
 // the B-spline prior's standard deviation for cubic splines, sqrt(9 / (8 pi))
 // (BINDER/src/cpu/Spline.cpp:22)
-constexpr double kSigmaCubic2 = 9.0 / (8.0 * 3.14159265358979323846);
+// sigma_spline^2 of the Gaussian approximating the B-spline of each order
+// (BINDER/src/cpu/Spline.cpp:19-41): sqrt(9 / (8 pi)), sqrt(8 / (9 pi)), 0.4
+double spline_sigma2(int order) {
+    const double pi = 3.14159265358979323846;
+    if (order == 2) return 8.0 / (9.0 * pi);
+    if (order == 1) return 0.4 * 0.4;
+    return 9.0 / (8.0 * pi);
+}
 
 struct Graph {
     cudaGraph_t g = nullptr;
@@ -258,8 +265,9 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
     : nx_(nx), ny_(ny), nz_(nz), nxn_(nxn), nyn_(nyn), nzn_(nzn) {
     BINDER_CHECK(nx > 0 && ny > 0 && nz > 0 && nxn > 0 && nyn > 0 && nzn > 0,
                  "grid dimensions must be positive");
-    if (spline_order != 3)
-        throw Error(kUnsupported, "only cubic B-splines (spline_order = 3) are built");
+    if (spline_order < 1 || spline_order > 3)
+        throw Error(kUnsupported, "spline_order must be 1, 2 or 3");
+    order_ = spline_order;
     BINDER_CHECK((long)nx * ny * nz < (1L << 31), "volume too large");
     BINDER_CHECK(nz > 1 || nzn == 1, "a 2D image (Nz_v == 1) needs a 2D node grid (Nz_n == 1)");
     N_ = nz == 1 ? 2 : 3;  // a 2D image has two displacement components
@@ -396,7 +404,7 @@ void Registration::set_nonlinear_transformation(const double gamma[3], const dou
     D_ = dalloc<float>((size_t)V_, own_stream_);
     BINDER_CUDA(cudaMemcpyAsync(D_, D, sizeof(float) * V_, cudaMemcpyDefault, own_stream_));
     BINDER_CUDA(cudaStreamSynchronize(own_stream_));
-    sigma2_ = kSigmaCubic2;
+    sigma2_ = spline_sigma2(order_);
     have_tr_ = true;
 }
 
@@ -439,7 +447,7 @@ EStepArgs Registration::estep_args(const int *skip) const {
     e.hcnt = hcnt_; e.st = st_; e.skip = skip; e.V = V_;
     e.nx = w.nx; e.ny = w.ny; e.nz = w.nz; e.nxn = w.nxn; e.nyn = w.nyn; e.nzn = w.nzn;
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
-    e.seed = seed_; e.chain = chain_;
+    e.seed = seed_; e.chain = chain_; e.order = order_;
     return e;
 }
 

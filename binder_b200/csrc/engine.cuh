@@ -142,6 +142,7 @@ class Registration {
     int egrid_e_ = 0, egrid_s_ = 0;
     uint64_t seed_ = 12345;
     int iters_done_ = 0;
+    int order_ = 3;  // B-spline order of the E-step
     double last_ms_ = 0.0;
 };
 

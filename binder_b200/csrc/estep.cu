@@ -21,6 +21,33 @@ __device__ __forceinline__ void bspline3(float t, float w[4]) {
     w[3] = t3 * (1.0f / 6.0f);
 }
 
+// base node index of position p and its four weights on the node offsets -1, 0, 1, 2 for spline
+// order 1, 2 or 3 (BINDER/src/cpu/Spline.cpp:9-41 and :44-123): order 3 around floor(p); order
+// 2 around floor(p + 0.5) on the offsets -1, 0, 1; order 1 around floor(p) on the offsets 0, 1.
+// The unused taps carry weight 0, so they add nothing to the posterior, the histogram or the
+// dream location.
+__device__ __forceinline__ int spline_setup(float p, int order, float w[4]) {
+    if (order == 2) {
+        const float f = floorf(p + 0.5f), d = p - f;
+        const float a = -2.0f * d + 1.0f, b = -2.0f * d - 1.0f;
+        w[0] = 0.125f * (a * a);
+        w[1] = 0.75f - d * d;
+        w[2] = 0.125f * (b * b);
+        w[3] = 0.0f;
+        return (int)f;
+    }
+    const float f = floorf(p), d = p - f;
+    if (order == 1) {
+        w[0] = 0.0f;
+        w[1] = 1.0f - d;
+        w[2] = d;
+        w[3] = 0.0f;
+    } else {
+        bspline3(d, w);
+    }
+    return (int)f;
+}
+
 // Bins of the 4 x 4 x 4 (3D) or 4 x 4 (2D) neighbourhood, packed 4 per word along the last axis.
 // A 2D image is handled as an nx x 1 x ny volume: its y axis plays the packed (z) role and there
 // is a single node row per x, so DIM == 2 gathers 4 words (x rows) and DIM == 3 gathers 16
@@ -236,12 +263,11 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
             ++deg;
             continue;
         }
-        const float fx = floorf(vp.px), fy = floorf(vp.py), fz = floorf(vp.pz);
-        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
         float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
-        bspline3(vp.px - fx, bx);
-        if (DIM == 3) bspline3(vp.py - fy, by);
-        bspline3(vp.pz - fz, bz);
+        const int ix = spline_setup(vp.px, a.order, bx);
+        const int iy = DIM == 3 ? spline_setup(vp.py, a.order, by) : 0;
+        const int iz = spline_setup(vp.pz, a.order, bz);
+        const float fx = (float)ix, fy = (float)iy, fz = (float)iz;
         uint32_t pk[4 * Q];
         gather_bins<DIM>(a, ix, iy, iz, pk);
         const int ui = a.u[i];
@@ -312,12 +338,11 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
             ++deg;
             continue;
         }
-        const float fx = floorf(vp.px), fy = floorf(vp.py), fz = floorf(vp.pz);
-        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
         float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
-        bspline3(vp.px - fx, bx);
-        if (DIM == 3) bspline3(vp.py - fy, by);
-        bspline3(vp.pz - fz, bz);
+        const int ix = spline_setup(vp.px, a.order, bx);
+        const int iy = DIM == 3 ? spline_setup(vp.py, a.order, by) : 0;
+        const int iz = spline_setup(vp.pz, a.order, bz);
+        const float fx = (float)ix, fy = (float)iy, fz = (float)iz;
         uint32_t pk[R];
         gather_bins<DIM>(a, ix, iy, iz, pk);
         const float *thc = th + a.u[i];  // theta column of this voxel's bin: thc[k * L]

@@ -23,7 +23,8 @@ struct EStepArgs {
     int nxn, nyn, nzn;
     int P, PZ, pyn, zp;
     int K, L;
-    int dim;  // 2 or 3
+    int dim;    // 2 or 3
+    int order;  // spline order 1, 2 or 3 (Spline.cpp:9-41), on the stencil of offsets -1 .. 2
     uint64_t seed;
     uint32_t chain;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)

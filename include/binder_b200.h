@@ -53,7 +53,9 @@ int binder_has_topology_correction(void);
 /* Registration(final_locations, threads, voxel_pos, node_pos, Nx_v, Ny_v, Nz_v, Nx_n, Ny_n, Nz_n,
  *              spline_order, non_zero_voxels)                    gpu/bindings.cpp:18-47
  * final_locations, voxel_pos, node_pos: [Nx_v*Ny_v*Nz_v*3] floats.  `threads` is accepted for
- * interface parity and unused.  node_pos may be NULL (the reference never reads it). */
+ * interface parity and unused.  node_pos may be NULL (the reference never reads it).
+ * spline_order 1, 2 or 3 with the CPU backend's offsets and sigma_spline (Spline.cpp:9-41; the
+ * reference GPU backend builds only 3). */
 int binder_registration_create(binder_registration **out, const float *final_locations,
                                int threads, const float *voxel_pos, const float *node_pos,
                                int Nx_v, int Ny_v, int Nz_v, int Nx_n, int Ny_n, int Nz_n,

@@ -72,6 +72,45 @@ void orc_spline3(double d, double w[4]) {
     w[3] = d3 / 6.0;
 }
 
+/* Spline.cpp:9-41 (offsets, index offset) and :93-123 (orders 2 and 1), placed on the cubic
+ * stencil of node offsets -1, 0, 1, 2: order 2 uses -1, 0, 1 around floor(p + 0.5), order 1 uses
+ * 0, 1 around floor(p); the unused taps carry weight 0. */
+static int g_spline_order = 3;
+void orc_set_spline_order(int order) { g_spline_order = (order == 1 || order == 2) ? order : 3; }
+int orc_get_spline_order(void) { return g_spline_order; }
+
+/* Spline::spline(d) as the reference returns it: the weights of its own offsets (order 3:
+ * -1..2, order 2: -1..1, order 1: 0..1), zero-filled to four */
+void orc_spline(int order, double d, double w[4]) {
+    if (order == 2) {
+        const double a = -2.0 * d + 1.0, b = -2.0 * d - 1.0;
+        w[0] = 0.125 * (a * a);
+        w[1] = 0.75 - d * d;
+        w[2] = 0.125 * (b * b);
+        w[3] = 0.0;
+    } else if (order == 1) {
+        w[0] = 1.0 - d;
+        w[1] = d;
+        w[2] = 0.0;
+        w[3] = 0.0;
+    } else {
+        orc_spline3(d, w);
+    }
+}
+
+/* base node index of position p, and its four weights on the offsets -1 .. 2 */
+static int spline_setup(double p, double w[4]) {
+    const double f = floor(p + (g_spline_order == 2 ? 0.5 : 0.0)), d = p - f;
+    double r[4];
+    orc_spline(g_spline_order, d, r);
+    if (g_spline_order == 1) {  /* offsets 0, 1 sit at stencil taps 1, 2 */
+        w[0] = 0.0; w[1] = r[0]; w[2] = r[1]; w[3] = 0.0;
+    } else {
+        for (int t = 0; t < 4; ++t) w[t] = r[t];
+    }
+    return (int)f;
+}
+
 /* moving-image bin at a node; outside the moving grid the likelihood uses row 0
  * (BINDER/src/cpu/MILikelihood.cpp:46-48, :92-93) */
 static inline int node_bin(const int *v, int x, int y, int z, int nxn, int nyn, int nzn) {
@@ -85,6 +124,7 @@ typedef struct {
     int node[64][3];
     int n;
     double S;
+    int base[3];  /* the spline's base node index per axis */
 } neigh_t;
 
 /* weights B(y_j - d_i) * theta[v_j, u_i] for the 4x4x4 (3D) or 4x4 (2D) neighbourhood,
@@ -92,11 +132,9 @@ typedef struct {
 static void neighbourhood(const double *di, int ui, const int *v, const double *theta, int is2D,
                           int nxn, int nyn, int nzn, int L, neigh_t *nb) {
     double bx[4], by[4], bz[4] = {1.0, 1.0, 1.0, 1.0};
-    const int ix = (int)floor(di[0]), iy = (int)floor(di[1]);
-    const int iz = is2D ? 0 : (int)floor(di[2]);
-    orc_spline3(di[0] - floor(di[0]), bx);
-    orc_spline3(di[1] - floor(di[1]), by);
-    if (!is2D) orc_spline3(di[2] - floor(di[2]), bz);
+    const int ix = spline_setup(di[0], bx), iy = spline_setup(di[1], by);
+    const int iz = is2D ? 0 : spline_setup(di[2], bz);
+    nb->base[0] = ix; nb->base[1] = iy; nb->base[2] = iz;
     const int ZZ = is2D ? 1 : 4;
     int j = 0;
     double S = 0.0;
@@ -147,7 +185,7 @@ double orc_estep(const double *d, const int *u, const int *v, const double *thet
             neighbourhood(di, u[i], v, theta, is2D, nxn, nyn, nzn, L, &nb);
             double *dr = dream + i * N;
             if (!(nb.S > 0.0)) {
-                for (int n = 0; n < N; ++n) dr[n] = floor(di[n]);
+                for (int n = 0; n < N; ++n) dr[n] = (double)nb.base[n];
                 deg += 1;
                 continue;
             }
@@ -197,7 +235,7 @@ double orc_estep_sample(const double *d, const int *u, const int *v, const doubl
             neighbourhood(di, u[i], v, theta, is2D, nxn, nyn, nzn, L, &nb);
             double *dr = dream + i * N;
             if (!(nb.S > 0.0)) {
-                for (int n = 0; n < N; ++n) dr[n] = floor(di[n]);
+                for (int n = 0; n < N; ++n) dr[n] = (double)nb.base[n];
                 continue;
             }
             mll += -log(nb.S);

@@ -30,6 +30,11 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 
 /* ---- cubic B-spline weights: BINDER/src/cpu/Spline.cpp:44-73 ---------------------------------- */
 void orc_spline3(double d, double w[4]);
+/* Spline::spline(d) of order 1, 2 or 3 (the reference's own four-weight layout) */
+void orc_spline(int order, double d, double w[4]);
+/* spline order (1, 2 or 3) of every E-step, EM and sampler call that follows */
+void orc_set_spline_order(int order);
+int  orc_get_spline_order(void);
 
 /* ---- E-step (EM): BINDER/src/cpu/Registration.cpp:219-330 (sample == false branch) -------------
  * d      : positions [V*N] (node-grid coordinates)

@@ -39,6 +39,9 @@ def _load_oracle():
     i, d, ll, u64, u32 = C.c_int, C.c_double, C.c_longlong, C.c_uint64, C.c_uint32
     lib.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
     lib.orc_spline3.argtypes = [d, _dp]
+    lib.orc_set_spline_order.argtypes = [i]
+    lib.orc_spline.argtypes = [i, d, _dp]
+    lib.orc_get_spline_order.restype = i
     lib.orc_estep.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [_dp, _dp, C.POINTER(ll)]
     lib.orc_estep.restype = d
     lib.orc_estep_sample.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [u64, u32, u32, _dp, _dp]
@@ -129,6 +132,17 @@ def philox(ctr, key):
     out = np.zeros(4, np.uint32)
     lib().orc_philox4x32_10(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
     return out
+
+
+def spline(order: int, d: float):
+    w = np.zeros(4)
+    lib().orc_spline(int(order), float(d), w)
+    return w
+
+
+def set_spline_order(order: int) -> None:
+    """Spline order (1, 2 or 3) of the E-step, EM and sampler calls that follow."""
+    lib().orc_set_spline_order(int(order))
 
 
 def spline3(d: float):

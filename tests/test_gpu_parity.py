@@ -224,7 +224,7 @@ def test_errors_are_reported(core):
         reg.setMILikelihood(2.0, c["theta"], c["K"], c["L"], 1, bad, c["u"])
     assert e.value.status == 1
     with pytest.raises(core.BinderError) as e:
-        core.Registration(c["d0"], 1, c["grid"], c["grid"], *shape, *shape, 2, 10.0)
+        core.Registration(c["d0"], 1, c["grid"], c["grid"], *shape, *shape, 4, 10.0)
     assert e.value.status == 3
 
 

@@ -25,6 +25,9 @@ def test_spline_matches_reference(oracle):
     g = golden("spline_ref.npz")
     for d, w in zip(g["d"], g["weights"][2]):
         np.testing.assert_allclose(oracle.spline3(d), w, rtol=0, atol=1e-15)
+    for order in (1, 2, 3):   # Spline.cpp:44-123, every order
+        for d, w in zip(g["d"], g["weights"][order - 1]):
+            np.testing.assert_allclose(oracle.spline(order, d), w, rtol=0, atol=1e-15)
     # partition of unity (tests/cpu/test_check_spline.py)
     for d in np.linspace(0, 1, 17, endpoint=False):
         assert abs(oracle.spline3(d).sum() - 1.0) < 1e-14
