@@ -113,6 +113,25 @@ class Registration:
             self._h, float(alpha), _f32(theta, K * L, "theta"), K, L, int(threads),
             _i32(binned_nodes, Vn, "binned_nodes"), _i32(binned_voxels, self._V, "binned_voxels")))
         self._K, self._L = K, L
+        self._ssd = False
+
+    def setSSDLikelihood(self, bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
+                         binned_voxels, alpha_0, beta_0):
+        """``setSSDLikelihood`` of the CPU module (cpu/bindings.cpp:120-152); EM only."""
+        bins = int(bins)
+        Vn = int(np.prod(self._nshape))
+        check(lib().binder_registration_set_ssd_likelihood(
+            self._h, bins, int(threads), float(sigma_sq), int(scale_shift), float(scale),
+            float(shift), _i32(binned_nodes, Vn, "binned_nodes"),
+            _i32(binned_voxels, self._V, "binned_voxels"), float(alpha_0), float(beta_0)))
+        self._K = self._L = bins
+        self._ssd = True
+
+    def ssd_parameters(self):
+        """(sigma^2, shift, scale) of the SSD likelihood (no reference counterpart)."""
+        out = np.zeros(3, np.float64)
+        check(lib().binder_registration_get_ssd_parameters(self._h, out))
+        return {"sigma_sq": float(out[0]), "shift": float(out[1]), "scale": float(out[2])}
 
     def setNonLinearTransformation(self, gamma_x, gamma_y, gamma_z, voxels_size_x, voxels_size_y,
                                    voxels_size_z, nodes_size_x, nodes_size_y, nodes_size_z, D):
@@ -161,9 +180,10 @@ class Registration:
     def get_likelihood_parameters(self):
         if self._K is None:
             raise BinderError(4, "setMILikelihood has not been called")
+        n = 2 if getattr(self, "_ssd", False) else self._K * self._L  # SSD: (scale, shift)
         out = np.zeros(self._K * self._L, np.float32)
         check(lib().binder_registration_get_likelihood_parameters(self._h, out))
-        return out
+        return out[:n]
 
     def get_shape(self):
         out = np.zeros(4, np.int32)

@@ -40,6 +40,7 @@ EXPORTS = [
     "binder_resample_matrix", "binder_pyramid_create", "binder_pyramid_destroy",
     "binder_pyramid_level", "binder_pinned_alloc", "binder_pinned_free",
     "binder_bin_signal_robust", "binder_bin_signal", "binder_center_of_mass", "binder_warp_image",
+    "binder_registration_set_ssd_likelihood", "binder_registration_get_ssd_parameters",
 ]
 
 
@@ -106,6 +107,9 @@ def _declare(lib):
         "binder_pinned_free": [_P, C.c_size_t],
         "binder_bin_signal_robust": [_P, _i, C.c_longlong, _i, _d, _d, _P, _P],
         "binder_bin_signal": [_P, _i, C.c_longlong, _i, _P],
+        "binder_registration_set_ssd_likelihood": [_P, _i, _i, _d, _i, _d, _d, _i32, _i32, _d,
+                                                   _d],
+        "binder_registration_get_ssd_parameters": [_P, _f64],
         "binder_center_of_mass": [_i32, _i, _i, _i, _f64],
         "binder_warp_image": [_f64, _i, _i, _i, _f64, C.c_longlong, _i, _f64],
         "binder_pyramid_level": [_P, _i, _P, _i, _d, _P, _i, _i, _P, _P],

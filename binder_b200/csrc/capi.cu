@@ -96,6 +96,29 @@ int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, 
     });
 }
 
+int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int threads,
+                                           double sigma_sq, int scale_shift, double scale,
+                                           double shift, const int32_t *binned_nodes,
+                                           const int32_t *binned_voxels, double alpha_0,
+                                           double beta_0) {
+    (void)threads;
+    return guard([&] {
+        NEED(h);
+        NEED(binned_nodes);
+        NEED(binned_voxels);
+        h->impl->set_ssd_likelihood(bins, sigma_sq, scale_shift, scale, shift, binned_nodes,
+                                    binned_voxels, alpha_0, beta_0);
+    });
+}
+
+int binder_registration_get_ssd_parameters(const binder_registration *h, double out[3]) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_ssd_parameters(out);
+    });
+}
+
 int binder_registration_set_nonlinear_transformation(binder_registration *h, double gamma_x,
                                                      double gamma_y, double gamma_z,
                                                      double voxels_size_x, double voxels_size_y,

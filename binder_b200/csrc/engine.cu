@@ -317,6 +317,7 @@ Registration::~Registration() {
     dfree(d_, s); dfree(x_, s); dfree(r_, s); dfree(D_, s); dfree(theta_, s); dfree(hist_, s);
     dfree(hcnt_, s); dfree(u_, s); dfree(vpad_, s); dfree(mean_, s); dfree(m2_, s);
     dfree(stats_, s); dfree(st_, s); dfree(d0_, s); dfree(theta0_, s);
+    dfree(ssd_, s); dfree(ssd0_, s); dfree(colmax_, s); dfree(colmax0_, s);
     delete topo_;
     mstep_.release(s);
     cudaStreamSynchronize(s);  // the frees complete, so the next object can reuse the memory
@@ -325,6 +326,7 @@ Registration::~Registration() {
 
 void Registration::set_mi_likelihood(double alpha, const float *theta, int K, int L,
                                      const int *binned_nodes, const int *binned_voxels) {
+    lk_ = 0;
     BINDER_CHECK(K >= 1 && K <= 256 && L >= 1 && L <= 256,
                  "numbers of bins K and L must be in [1, 256]");
     BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
@@ -391,6 +393,53 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     have_mi_ = true;
 }
 
+// The SSD likelihood is a K x L table over (node bin, voxel bin) -- outside nodes count as bin
+// 0, whose value is 0 -- so the bins, histogram and E-step of the MI path carry it; the table
+// lives in log2 (per voxel bin relative to its best node bin) and the E-step runs in log space,
+// and its parameters follow from moments of the joint histogram.
+void Registration::set_ssd_likelihood(int bins, double sigma2, int shift_scale, double scale,
+                                      double shift, const int *binned_nodes,
+                                      const int *binned_voxels, double alpha0, double beta0) {
+    BINDER_CHECK(bins >= 1 && bins <= kLogMaxBins, "SSD bins must be in [1, 64]");
+    BINDER_CHECK(sigma2 > 0.0, "sigma_sq must be positive");
+    BINDER_CHECK(alpha0 > 0.0 && beta0 > 0.0, "alpha_0 and beta_0 must be positive");
+    const std::vector<float> flat((size_t)bins * bins, 1.0f / bins);
+    set_mi_likelihood(2.0, flat.data(), bins, bins, binned_nodes, binned_voxels);
+    const cudaStream_t s = own_stream_;
+    dfree(ssd_, s); dfree(ssd0_, s); dfree(colmax_, s); dfree(colmax0_, s);
+    ssd_ = dalloc<SsdState>(1, s);
+    ssd0_ = dalloc<SsdState>(1, s);
+    colmax_ = dalloc<float>((size_t)bins, s);
+    colmax0_ = dalloc<float>((size_t)bins, s);
+    SsdState h{};
+    h.sigma2 = sigma2;
+    h.shift = shift_scale ? shift : 0.0;
+    h.scale = shift_scale ? scale : 1.0;
+    h.alpha0 = alpha0;
+    h.beta0 = beta0;
+    h.shift_scale = shift_scale ? 1 : 0;
+    BINDER_CUDA(cudaMemcpyAsync(ssd_, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(ssd0_, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    launch_ssd_update(theta_, colmax_, nullptr, bins, bins, 0, ssd_, nullptr, s);
+    BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * bins * bins,
+                                cudaMemcpyDeviceToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(colmax0_, colmax_, sizeof(float) * bins, cudaMemcpyDeviceToDevice,
+                                s));
+    BINDER_CUDA(cudaStreamSynchronize(s));  // `h` goes out of scope
+    lk_ = 1;
+    egrid_e_ = estep_grid(false, bins, bins, V_, N_, true);
+}
+
+void Registration::get_ssd_parameters(double out[3]) const {
+    if (lk_ != 1) throw Error(kNotReady, "setSSDLikelihood has not been called");
+    SsdState h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, ssd_, sizeof h, cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    out[0] = h.sigma2;
+    out[1] = h.shift;
+    out[2] = h.scale;
+}
+
 void Registration::set_nonlinear_transformation(const double gamma[3], const double rho[3],
                                                 const double eta[3], const float *D) {
     for (int n = 0; n < 3; ++n) {
@@ -448,12 +497,16 @@ EStepArgs Registration::estep_args(const int *skip) const {
     e.nx = w.nx; e.ny = w.ny; e.nz = w.nz; e.nxn = w.nxn; e.nyn = w.nyn; e.nzn = w.nzn;
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
     e.seed = seed_; e.chain = chain_; e.order = order_;
+    e.logt = lk_ == 1; e.colmax = colmax_;
     return e;
 }
 
 void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
     launch_estep(estep_args(&st_->done), false, egrid_e_, stream_);
-    launch_theta_update(theta_, hist_, K_, L_, alpha_, update, st_, stream_);
+    if (lk_ == 1)
+        launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, stream_);
+    else
+        launch_theta_update(theta_, hist_, K_, L_, alpha_, update, st_, stream_);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
                    rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, stream_);
@@ -543,6 +596,8 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     if (sample_posteriors || sample_likelihood_parameters) {
         if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
     }
+    if (lk_ == 1)
+        throw Error(kUnsupported, "the sampler with the SSD likelihood is not built (EM only)");
     if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
     BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
     BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
@@ -625,6 +680,8 @@ double Registration::profile_stage(int stage, int n) {
         else if (stage == 1)
             mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
                            rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
+        else if (lk_ == 1)
+            launch_ssd_update(theta_, colmax_, hist_, K_, L_, 0, ssd_, st_, stream_);
         else launch_theta_update(theta_, hist_, K_, L_, alpha_, 1, st_, stream_);
     };
     one();  // warm-up
@@ -672,6 +729,12 @@ void Registration::reset() {
                                     cudaMemcpyDeviceToDevice, stream_));
         BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
         BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K_ * L_, stream_));
+    }
+    if (lk_ == 1) {
+        BINDER_CUDA(cudaMemcpyAsync(ssd_, ssd0_, sizeof(SsdState), cudaMemcpyDeviceToDevice,
+                                    stream_));
+        BINDER_CUDA(cudaMemcpyAsync(colmax_, colmax0_, sizeof(float) * L_,
+                                    cudaMemcpyDeviceToDevice, stream_));
     }
     BINDER_CUDA(cudaStreamSynchronize(stream_));
     reset_state(false);
@@ -721,6 +784,13 @@ void Registration::set_dream_locations(const float *in) {
 
 void Registration::get_likelihood_parameters(float *out) const {
     if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    if (lk_ == 1) {  // SSDLikelihood::get_parameters (SSDLikelihood.cpp:328-334): scale, shift
+        double p[3];
+        get_ssd_parameters(p);
+        out[0] = (float)p[2];
+        out[1] = (float)p[1];
+        return;
+    }
     BINDER_CUDA(cudaMemcpyAsync(out, theta_, sizeof(float) * K_ * L_, cudaMemcpyDeviceToHost,
                                 stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));

@@ -65,6 +65,11 @@ class Registration {
                            const int *binned_voxels);
     void set_nonlinear_transformation(const double gamma[3], const double rho[3],
                                       const double eta[3], const float *D);
+    // the SSD likelihood instead of MI (BINDER/src/cpu/Registration.cpp:472-479), EM only
+    void set_ssd_likelihood(int bins, double sigma2, int shift_scale, double scale, double shift,
+                            const int *binned_nodes, const int *binned_voxels, double alpha0,
+                            double beta0);
+    void get_ssd_parameters(double out[3]) const;  // sigma^2, shift, scale
     int em(int max_iterations, double convergence_th, int update_likelihood_parameters, int debug);
     void sampler(uint64_t seed, int N_b, int N_s, int sample_gamma, int sample_gamma_every,
                  int sample_posteriors, int sample_likelihood_parameters,
@@ -143,6 +148,9 @@ class Registration {
     uint64_t seed_ = 12345;
     int iters_done_ = 0;
     int order_ = 3;  // B-spline order of the E-step
+    int lk_ = 0;     // likelihood: 0 MI (theta_ is theta), 1 SSD (theta_ is its log2 table)
+    SsdState *ssd_ = nullptr, *ssd0_ = nullptr;  // SSD parameters, and as set
+    float *colmax_ = nullptr, *colmax0_ = nullptr;  // SSD table column maxima, and as set
     double last_ms_ = 0.0;
 };
 

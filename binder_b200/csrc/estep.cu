@@ -219,6 +219,65 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
     kmax = hi;
 }
 
+// em_accumulate in log space (Registration.cpp:331-470): the table entries are log2 likelihoods,
+// the spline weights enter as log2 too, and every term is exponentiated relative to the voxel's
+// largest term, so no neighbourhood underflows.  mlog returns that largest term (log2).
+template <int TPB, int Q>
+__device__ __forceinline__ void em_accumulate_log(const float *__restrict__ thu,
+                                                  float *__restrict__ col,
+                                                  const uint32_t (&pk)[4 * Q],
+                                                  const float (&bx)[4], const float (&by)[4],
+                                                  const float (&bz)[4], float &S, float &Sx,
+                                                  float &Sy, float &Sz, int &kmin, int &kmax,
+                                                  float &mlog) {
+    float lx[4], ly[4], lz[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        lx[t] = log2f(bx[t]);  // -inf for a zero tap, whose term then vanishes
+        ly[t] = Q == 4 ? log2f(by[t]) : 0.0f;
+        lz[t] = log2f(bz[t]);
+    }
+    float m = -INFINITY;
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float lxy = lx[p] + ly[q];
+            const uint32_t word = pk[p * Q + q];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                m = fmaxf(m, lxy + lz[c] + thu[(word >> (8 * c)) & 0xff]);
+        }
+    float a = 0.f, x = 0.f, y = 0.f, z = 0.f;
+    int lo = 255, hi = 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float lxy = lx[p] + ly[q] - m;
+            const uint32_t word = pk[p * Q + q];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int k = (word >> (8 * c)) & 0xff;
+                const float w = exp2f(lxy + lz[c] + thu[k]);
+                col[k * TPB] += w;
+                a += w;
+                x = fmaf((float)(p - 1), w, x);
+                if (Q == 4) y = fmaf((float)(q - 1), w, y);
+                z = fmaf((float)(c - 1), w, z);
+                lo = min(lo, k);
+                hi = max(hi, k);
+            }
+        }
+    S = a;
+    Sx = x;
+    Sy = y;
+    Sz = z;
+    kmin = lo;
+    kmax = hi;
+    mlog = m;
+}
+
 // EM E-step for K <= 64 (BINDER/src/cpu/Registration.cpp:219-330, sample == false), one pass over
 // the 64 (3D) or 16 (2D) neighbours.  The posterior mass of a voxel is collected per moving bin k
 // in a private shared-memory column hk[k][thread] (bank = thread % 32, so never a conflict and
@@ -232,7 +291,7 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
 // each addition relative to the running sum instead.  theta is staged transposed (thT[u][k]); it
 // and the histogram use a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ by
 // small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the host).
-template <int TPB, int DIM>
+template <int TPB, int DIM, bool LOGT>
 __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     if (a.skip && *a.skip) return;
@@ -242,7 +301,10 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
     float *thT = sm;                                             // [L][KP]
     unsigned *hs = reinterpret_cast<unsigned *>(sm + L * KP);    // [K][LP] CTA histogram (fixed)
     float *hk = sm + L * KP + K * LP;                            // [K][TPB] per-thread bin masses
+    float *cmx = hk + K * TPB;                                   // [L] log-space column maxima
     __shared__ double red[32];
+    if (LOGT)
+        for (int l = threadIdx.x; l < L; l += TPB) cmx[l] = a.colmax[l];
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L, l = q - k * L;
         thT[l * KP + k] = a.theta[q];
@@ -273,7 +335,12 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
         const int ui = a.u[i];
         float S, Sx, Sy, Sz;
         int kmin, kmax;
-        em_accumulate<TPB, Q>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin, kmax);
+        float mlog = 0.0f;
+        if (LOGT)
+            em_accumulate_log<TPB, Q>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin,
+                                      kmax, mlog);
+        else
+            em_accumulate<TPB, Q>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin, kmax);
         const bool ok = S > 0.0f;
         const float inv = ok ? 1.0f / S : 0.0f;
         const float invs = inv * a.hscale;
@@ -291,6 +358,7 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
             continue;
         }
         mll -= (double)logf(S);  // FP32 log, FP64 accumulation
+        if (LOGT) mll -= (double)mlog * 0.6931471805599453 + (double)cmx[ui];
         vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
     }
     __syncthreads();
@@ -629,40 +697,48 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 }  // namespace
 
 namespace {
-size_t estep_smem(bool sample, int K, int L) {
+size_t estep_smem(bool sample, int K, int L, bool logt = false) {
     if (!sample && K <= kSmallK)
-        return (size_t)(L * theta_pitch(K) + K * theta_pitch(L) + K * kFastThreads) * sizeof(float);
+        return (size_t)(L * theta_pitch(K) + K * theta_pitch(L) + K * kFastThreads +
+                        (logt ? L : 0)) * sizeof(float);
     return (size_t)(2 * K * L + (sample ? 16 * kEThreads : 0)) * sizeof(float);
 }
 }  // namespace
 
 namespace {
 template <int DIM>
-const void *estep_fn(bool sample, int K) {
+const void *estep_fn(bool sample, int K, bool logt) {
+    if (logt) return (const void *)estep_em_fast_kernel<kFastThreads, DIM, true>;
     return sample ? (const void *)estep_kernel<true, DIM>
-                  : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads, DIM>
+                  : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads, DIM, false>
                                   : (const void *)estep_kernel<false, DIM>);
 }
 
 template <int DIM>
 void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
-    if (sample)
+    if (a.logt)
+        count_launch(), estep_em_fast_kernel<kFastThreads, DIM, true>
+                            <<<grid, kFastThreads, smem, s>>>(a);
+    else if (sample)
         count_launch(), estep_kernel<true, DIM><<<grid, kEThreads, smem, s>>>(a);
     else if (a.K <= kSmallK)
-        count_launch(), estep_em_fast_kernel<kFastThreads, DIM><<<grid, kFastThreads, smem, s>>>(a);
+        count_launch(), estep_em_fast_kernel<kFastThreads, DIM, false>
+                            <<<grid, kFastThreads, smem, s>>>(a);
     else
         count_launch(), estep_kernel<false, DIM><<<grid, kEThreads, smem, s>>>(a);
 }
 }  // namespace
 
-int estep_grid(bool sample, int K, int L, long V, int dim) {
+int estep_grid(bool sample, int K, int L, long V, int dim, bool logt) {
     BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
+    BINDER_CHECK(!logt || (!sample && K <= kSmallK && K <= kLogMaxBins),
+                 "the log-space E-step supports EM with at most 64 bins");
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = estep_smem(sample, K, L);
-    const void *fn = dim == 3 ? estep_fn<3>(sample, K) : estep_fn<2>(sample, K);
-    const int tpb = (!sample && K <= kSmallK) ? kFastThreads : kEThreads;
+    const size_t smem = estep_smem(sample, K, L, logt);
+    const void *fn = dim == 3 ? estep_fn<3>(sample, K, logt) : estep_fn<2>(sample, K, logt);
+    const int tpb = (logt || (!sample && K <= kSmallK)) ? kFastThreads : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // all of the unified L1 / shared array as shared memory, so the CTAs the occupancy query
     // counts are the CTAs that become resident (the default carveout may be smaller)
@@ -677,7 +753,9 @@ int estep_grid(bool sample, int K, int L, long V, int dim) {
 }
 
 void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) {
-    const size_t smem = estep_smem(sample, args.K, args.L);
+    BINDER_CHECK(!args.logt || (!sample && args.K <= kSmallK && args.colmax),
+                 "the log-space E-step runs EM only, with at most 64 bins");
+    const size_t smem = estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
     // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
     // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a
@@ -697,6 +775,108 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) 
 void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, int update,
                          DevState *st, cudaStream_t s) {
     count_launch(), theta_update_kernel<<<1, 1024, 0, s>>>(theta, hist, K, L, alpha, update, st);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+namespace {
+// SSDLikelihood.cpp:58-82 in natural log: log N(l; shift + scale k, sigma^2) (shift_scale 0:
+// shift 0, scale 1); bin 0 also stands for the nodes outside the grid, whose value is 0
+__device__ __forceinline__ double ssd_loglik(int k, int l, const SsdState &p) {
+    const double adj = p.shift_scale ? (double)l - p.shift - p.scale * (double)k
+                                     : (double)l - (double)k;
+    return (adj * adj) / (-2.0 * p.sigma2) - log(sqrt(2.0 * 3.14159265358979323846 * p.sigma2));
+}
+
+__global__ void ssd_update_kernel(float *table, float *colmax, float *hist, int K, int L,
+                                  int update, SsdState *ps, DevState *st) {
+    if (st && st->done) return;
+    __shared__ double G[kLogMaxBins], S1[kLogMaxBins], S2[kLogMaxBins], D2[kLogMaxBins];
+    __shared__ SsdState p;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) p = *ps;
+    __syncthreads();
+    if (update && hist) {
+        // per node bin k: posterior mass, its first and second moments in the voxel bin, and
+        // the squared differences for the shiftScale-0 update (SSDLikelihood.cpp:111-141)
+        for (int k = wid; k < K; k += nw) {
+            double g = 0.0, s1 = 0.0, s2 = 0.0, d2 = 0.0;
+            for (int l = lane; l < L; l += 32) {
+                const double h = (double)hist[k * L + l], df = (double)l - (double)k;
+                g += h;
+                s1 += h * (double)l;
+                s2 += h * (double)l * (double)l;
+                d2 += h * df * df;
+            }
+            g = warp_sum(g);
+            s1 = warp_sum(s1);
+            s2 = warp_sum(s2);
+            d2 = warp_sum(d2);
+            if (lane == 0) {
+                G[k] = g;
+                S1[k] = s1;
+                S2[k] = s2;
+                D2[k] = d2;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double den = 0.0, num = 0.0;
+            if (!p.shift_scale) {  // :147-163
+                for (int k = 0; k < K; ++k) {
+                    num += D2[k];
+                    den += G[k];
+                }
+            } else {  // :167-285, the 2x2 normal equations in closed form
+                double A00 = 0.0, A01 = 0.0, A11 = 0.0, b0 = 0.0, b1 = 0.0;
+                for (int k = 0; k < K; ++k) {
+                    A00 += G[k];
+                    A01 += G[k] * (double)k;
+                    A11 += G[k] * (double)k * (double)k;
+                    b0 += S1[k];
+                    b1 += S1[k] * (double)k;
+                }
+                const double det = A00 * A11 - A01 * A01;
+                if (det != 0.0 && isfinite(det)) {
+                    p.shift = (b0 * A11 - A01 * b1) / det;
+                    p.scale = (A00 * b1 - A01 * b0) / det;
+                }
+                for (int k = 0; k < K; ++k) {
+                    const double t1 = p.shift + p.scale * (double)k;
+                    num += S2[k] + -2.0 * S1[k] * t1 + G[k] * (t1 * t1);
+                    den += G[k];
+                }
+            }
+            num += p.alpha0 * p.beta0;
+            den += p.alpha0;
+            p.sigma2 = num / den;
+            *ps = p;
+        }
+        __syncthreads();
+    }
+    if (st && threadIdx.x == 0) {  // compute_cost (:314-326): -log InvGamma(sigma^2; a, a beta0)
+        const double a = p.alpha0, b = p.alpha0 * p.beta0, x = p.sigma2;
+        st->lp_lik = -(a * log(b) - lgamma(a) + (-a - 1.0) * log(x) - b / x);
+        if (!isfinite(p.sigma2) || !(p.sigma2 > 0.0)) atomicOr(&st->flags, (unsigned)kFlagNonFinite);
+    }
+    // the next E-step's table: log2 likelihoods minus their maximum over k per voxel bin l
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        double m = -INFINITY;
+        for (int k = 0; k < K; ++k) m = fmax(m, ssd_loglik(k, l, p));
+        colmax[l] = (float)m;
+        for (int k = 0; k < K; ++k)
+            table[k * L + l] = (float)((ssd_loglik(k, l, p) - m) * 1.4426950408889634);
+    }
+    if (st && hist) {
+        __syncthreads();  // every row was read before the histogram is cleared
+        for (int q = threadIdx.x; q < K * L; q += blockDim.x) hist[q] = 0.0f;
+    }
+}
+}  // namespace
+
+void launch_ssd_update(float *table, float *colmax, float *hist, int K, int L, int update,
+                       SsdState *p, DevState *st, cudaStream_t s) {
+    BINDER_CHECK(K >= 1 && K <= kLogMaxBins && L >= 1, "SSD bins must be in [1, 64]");
+    count_launch(), ssd_update_kernel<<<1, 256, 0, s>>>(table, colmax, hist, K, L, update, p, st);
     BINDER_CUDA(cudaGetLastError());
 }
 

@@ -25,6 +25,10 @@ struct EStepArgs {
     int K, L;
     int dim;    // 2 or 3
     int order;  // spline order 1, 2 or 3 (Spline.cpp:9-41), on the stencil of offsets -1 .. 2
+    // log-space likelihood (the SSD likelihood): `theta` holds log2 likelihoods normalised per
+    // voxel bin l by their maximum over k, whose natural log is colmax[l]
+    int logt;
+    const float *colmax;
     uint64_t seed;
     uint32_t chain;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
@@ -32,7 +36,23 @@ struct EStepArgs {
 };
 
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
-int estep_grid(bool sample, int K, int L, long V, int dim);
+int estep_grid(bool sample, int K, int L, long V, int dim, bool logt = false);
+// largest number of bins of the log-space (SSD) E-step
+constexpr int kLogMaxBins = 64;
+
+// State of the SSD likelihood (BINDER/src/cpu/SSDLikelihood.cpp): sigma^2, shift, scale and the
+// inverse-gamma prior (alpha0, beta0) of sigma^2
+struct SsdState {
+    double sigma2, shift, scale, alpha0, beta0;
+    int shift_scale;
+    int pad;
+};
+// SSDLikelihood::update_parameters from the joint histogram when `update` (:143-285), the cost
+// of sigma^2 into st->lp_lik (:314-326), the log2 likelihood table [K][L] (normalised per column)
+// and its column maxima rebuilt from the parameters, and the histogram cleared.  st may be null
+// (table only, no histogram).  One CTA.
+void launch_ssd_update(float *table, float *colmax, float *hist, int K, int L, int update,
+                       SsdState *p, DevState *st, cudaStream_t s);
 
 // theta <- (hist + alpha - 1)/rowsum (if update), Dirichlet prior cost into st->lp_lik,
 // hist zeroed for the next iteration.  One CTA.

@@ -68,6 +68,19 @@ int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, 
                                           int K, int L, int threads, const int32_t *binned_nodes,
                                           const int32_t *binned_voxels);
 
+/* setSSDLikelihood(bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
+ *                  binned_voxels, alpha_0, beta_0)                  cpu/bindings.cpp:120-152
+ * The CPU backend's SSD likelihood (SSDLikelihood.cpp): the bins are the intensities, bins <= 64;
+ * scale_shift 0 fits sigma^2 only, 1 also shift and scale.  EM only (the sampler rejects it).
+ * get_likelihood_parameters then returns (scale, shift). */
+int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int threads,
+                                           double sigma_sq, int scale_shift, double scale,
+                                           double shift, const int32_t *binned_nodes,
+                                           const int32_t *binned_voxels, double alpha_0,
+                                           double beta_0);
+/* No counterpart in the reference (it prints sigmaSq): the SSD parameters sigma^2, shift, scale */
+int binder_registration_get_ssd_parameters(const binder_registration *h, double out[3]);
+
 /* setNonLinearTransformation(gamma_x..z, voxels_size_x..z, nodes_size_x..z, D)
  *                                                               gpu/bindings.cpp:72-95; D [V] */
 int binder_registration_set_nonlinear_transformation(binder_registration *h, double gamma_x,

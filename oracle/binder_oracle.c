@@ -509,6 +509,162 @@ int orc_em(double *final_locations, const double *voxel_pos, const int *u, const
     return it;
 }
 
+/* SSDLikelihood.cpp:58-82: log N(u; shift + scale * k, sigmaSq), k = 0 outside the node grid
+ * (shiftScale 0: shift 0, scale 1) */
+static double ssd_loglik(double uval, int k, const orc_ssd *p) {
+    const double adj = p->shift_scale ? uval - p->shift - p->scale * (double)k : uval - (double)k;
+    return (adj * adj) / (-2.0 * p->sigma2) - log(sqrt(2.0 * PI_D * p->sigma2));
+}
+
+double orc_ssd_estep(const double *d, const int *u, const int *v, const orc_ssd *p, int nx,
+                     int ny, int nz, int nxn, int nyn, int nzn, int K, int L, double *dream,
+                     double *hist) {
+    const int is2D = (nz == 1);
+    const int N = is2D ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    const int T = orc_get_threads();
+    double *hist_t = (double *)calloc((size_t)T * K * L, sizeof(double));
+    double mll = 0.0;
+#pragma omp parallel num_threads(T) reduction(+ : mll)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        double *h = hist_t + (size_t)tid * K * L;
+#pragma omp for schedule(static)
+        for (long i = 0; i < V; ++i) {
+            const double *di = d + i * N;
+            double bx[4], by[4], bz[4] = {1.0, 1.0, 1.0, 1.0};
+            const int ix = spline_setup(di[0], bx), iy = spline_setup(di[1], by);
+            const int iz = is2D ? 0 : spline_setup(di[2], bz);
+            const int ZZ = is2D ? 1 : 4;
+            double lp[64];
+            int kb[64], node[64][3];
+            int n = 0;
+            double mx = -INFINITY;
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b)
+                    for (int c = 0; c < ZZ; ++c) {
+                        const double w = bx[a] * by[b] * bz[c];
+                        if (!(w > 0.0)) continue;  /* the reference's log weight is -1e100 */
+                        const int X = ix + a - 1, Y = iy + b - 1, Z = is2D ? 0 : iz + c - 1;
+                        const int k = node_bin(v, X, Y, Z, nxn, nyn, nzn);
+                        lp[n] = log(bx[a]) + log(by[b]) + (is2D ? 0.0 : log(bz[c])) +
+                                ssd_loglik((double)u[i], k, p);
+                        kb[n] = k;
+                        node[n][0] = X; node[n][1] = Y; node[n][2] = Z;
+                        if (lp[n] > mx) mx = lp[n];
+                        ++n;
+                    }
+            double norm = 0.0;
+            for (int j = 0; j < n; ++j) norm += exp(lp[j] - mx);
+            const double lnorm = log(norm) + mx;
+            mll += -lnorm;
+            double acc[3] = {0.0, 0.0, 0.0};
+            for (int j = 0; j < n; ++j) {
+                const double pj = exp(lp[j] - lnorm);
+                h[(long)kb[j] * L + u[i]] += pj;
+                for (int m = 0; m < N; ++m) acc[m] += pj * (double)node[j][m];
+            }
+            for (int m = 0; m < N; ++m) dream[i * N + m] = acc[m];
+        }
+    }
+    for (long q = 0; q < (long)K * L; ++q) {
+        double s = 0.0;
+        for (int t = 0; t < T; ++t) s += hist_t[(size_t)t * K * L + q];
+        hist[q] = s;
+    }
+    free(hist_t);
+    return mll;
+}
+
+/* update_parameters / update_shift_and_scale / update_sigma (:143-285) from the histogram: the
+ * per-node sums of accumulate_info (:111-141) grouped by node bin k (bin 0 also holds the nodes
+ * outside the grid, whose contribution is that of a node of value 0); the 2x2 normal equations
+ * solved in closed form.  Returns compute_cost (:314-326), the inverse-gamma prior of sigmaSq. */
+double orc_ssd_update(const double *hist, int K, int L, orc_ssd *p, int update) {
+    if (update) {
+        if (!p->shift_scale) {
+            double num = 0.0, den = 0.0;
+            for (int k = 0; k < K; ++k)
+                for (int l = 0; l < L; ++l) {
+                    const double h = hist[(long)k * L + l], df = (double)l - (double)k;
+                    num += h * df * df;
+                    den += h;
+                }
+            num += p->alpha0 * p->beta0;
+            den += p->alpha0;
+            p->sigma2 = num / den;
+        } else {
+            double G[256], S1[256], S2[256];
+            double A00 = 0, A01 = 0, A11 = 0, b0 = 0, b1 = 0;
+            for (int k = 0; k < K; ++k) {
+                G[k] = S1[k] = S2[k] = 0.0;
+                for (int l = 0; l < L; ++l) {
+                    const double h = hist[(long)k * L + l];
+                    G[k] += h;
+                    S1[k] += h * (double)l;
+                    S2[k] += h * (double)l * (double)l;
+                }
+                A00 += G[k];
+                A01 += G[k] * (double)k;
+                A11 += G[k] * (double)k * (double)k;
+                b0 += S1[k];
+                b1 += S1[k] * (double)k;
+            }
+            const double det = A00 * A11 - A01 * A01;
+            p->shift = (b0 * A11 - A01 * b1) / det;
+            p->scale = (A00 * b1 - A01 * b0) / det;
+            double num = 0.0, den = 0.0;
+            for (int k = 0; k < K; ++k) {
+                const double t1 = p->shift + p->scale * (double)k;
+                num += S2[k] + -2.0 * S1[k] * t1 + G[k] * (t1 * t1);
+                den += G[k];
+            }
+            num += p->alpha0 * p->beta0;
+            den += p->alpha0;
+            p->sigma2 = num / den;
+        }
+    }
+    const double a = p->alpha0, b = p->alpha0 * p->beta0, x = p->sigma2;
+    return -(a * log(b) - lgamma(a) + (-a - 1.0) * log(x) - b / x);
+}
+
+/* Registration.cpp:122-217 with the SSD likelihood */
+int orc_ssd_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
+               orc_ssd *p, const double *D, const double gamma[3], double sigma, int nx, int ny,
+               int nz, int nxn, int nyn, int nzn, int K, int L, double non_zero_voxels,
+               int max_iter, double convergence_th, int update, orc_iter_stats *stats) {
+    const int N = (nz == 1) ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    double *dream = (double *)malloc(sizeof(double) * V * N);
+    double *hist = (double *)malloc(sizeof(double) * K * L);
+    double mlp_old = 1e100;
+    int it = 0;
+    while (it < max_iter) {
+        const double mll = orc_ssd_estep(final_locations, u, v, p, nx, ny, nz, nxn, nyn, nzn, K,
+                                         L, dream, hist);
+        const double lpl = orc_ssd_update(hist, K, L, p, update);
+        const double lpt = orc_smooth(dream, voxel_pos, D, gamma, sigma, nx, ny, nz,
+                                      final_locations, 0, 0, 0, 0, NULL, NULL, NULL);
+        const double mlp = mll + lpt + lpl;
+        if (stats) {
+            stats[it].mll = mll;
+            stats[it].log_prior_likelihood = lpl;
+            stats[it].log_prior_transformation = lpt;
+            stats[it].mlp = mlp;
+        }
+        ++it;
+        if ((mlp_old - mlp) / non_zero_voxels < convergence_th) break;
+        mlp_old = mlp;
+    }
+    free(dream);
+    free(hist);
+    return it;
+}
+
 /* Registration.cpp:515-642 with NonLinearTransformation.cpp:79-126 for block 3 */
 int orc_sampler(double *final_locations, double *dream, const double *voxel_pos, const int *u,
                 const int *v, double *theta, double alpha, const double *D, double gamma[3],

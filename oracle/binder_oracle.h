@@ -99,6 +99,23 @@ int orc_em(double *final_locations, const double *voxel_pos, const int *u, const
            double non_zero_voxels, int max_iter, double convergence_th, int update_theta,
            orc_iter_stats *stats /* [max_iter] or NULL */);
 
+/* ---- SSD likelihood: BINDER/src/cpu/SSDLikelihood.cpp ------------------------------------------ */
+typedef struct {
+    int shift_scale;
+    double sigma2, shift, scale, alpha0, beta0;
+} orc_ssd;
+/* log-space E-step (Registration.cpp:331-470) with the SSD log-likelihood; hist[k][l] is the
+ * posterior mass of node bin k at voxel bin l (bins >= 0; outside nodes count as bin 0) */
+double orc_ssd_estep(const double *d, const int *u, const int *v, const orc_ssd *p, int nx,
+                     int ny, int nz, int nxn, int nyn, int nzn, int K, int L, double *dream,
+                     double *hist);
+/* update_parameters (:143-285) from the joint histogram, then compute_cost (:314-326) */
+double orc_ssd_update(const double *hist, int K, int L, orc_ssd *p, int update);
+int orc_ssd_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
+               orc_ssd *p, const double *D, const double gamma[3], double sigma, int nx, int ny,
+               int nz, int nxn, int nyn, int nzn, int K, int L, double non_zero_voxels,
+               int max_iter, double convergence_th, int update, orc_iter_stats *stats);
+
 /* ---- Gibbs sampler driver: BINDER/src/cpu/Registration.cpp:515-642 ----------------------------
  * mean_out [V*N], cov_out [V*N*N] (M2 / (N_s - 1)).  dream is the working dream-location buffer
  * (set by the caller when sample_posteriors == 0). */

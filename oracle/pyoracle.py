@@ -40,6 +40,13 @@ def _load_oracle():
     lib.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
     lib.orc_spline3.argtypes = [d, _dp]
     lib.orc_set_spline_order.argtypes = [i]
+    lib.orc_ssd_estep.argtypes = [_dp, _ip, _ip, C.c_void_p] + [i] * 8 + [_dp, _dp]
+    lib.orc_ssd_estep.restype = d
+    lib.orc_ssd_update.argtypes = [_dp, i, i, C.c_void_p, i]
+    lib.orc_ssd_update.restype = d
+    lib.orc_ssd_em.argtypes = [_dp, _dp, _ip, _ip, C.c_void_p, _dp, _dp, d] + [i] * 8 + \
+        [d, i, d, i, C.c_void_p]
+    lib.orc_ssd_em.restype = i
     lib.orc_spline.argtypes = [i, d, _dp]
     lib.orc_get_spline_order.restype = i
     lib.orc_estep.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [_dp, _dp, C.POINTER(ll)]
@@ -324,6 +331,44 @@ def sampler(final_locations, dream, voxel_pos, u, v, theta, alpha, D, gamma, sig
                                sample_posteriors, sample_likelihood_parameters,
                                sample_transformation_parameters, mean, cov)
     return mean, cov, fl, th, g, capped
+
+
+class SSDParams(C.Structure):
+    """orc_ssd: the SSD likelihood's state (BINDER/src/cpu/SSDLikelihood.cpp)."""
+    _fields_ = [("shift_scale", C.c_int), ("sigma2", C.c_double), ("shift", C.c_double),
+                ("scale", C.c_double), ("alpha0", C.c_double), ("beta0", C.c_double)]
+
+
+def ssd_estep(d, u, v, params, vshape, nshape, K, L):
+    """Log-space E-step with the SSD likelihood. Returns (mll, dream[V*N], hist[K*L])."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    dream = np.zeros(nx * ny * nz * N)
+    hist = np.zeros(K * L)
+    mll = lib().orc_ssd_estep(_c64(d).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                              C.addressof(params), nx, ny, nz, *nshape, K, L, dream, hist)
+    return mll, dream, hist
+
+
+def ssd_update(hist, K, L, params, update=True):
+    return lib().orc_ssd_update(_c64(hist).ravel(), K, L, C.addressof(params), int(update))
+
+
+def ssd_em(final_locations, voxel_pos, u, v, params, D, gamma, sigma, vshape, nshape, K, L,
+           non_zero_voxels, max_iter, convergence_th, update=True):
+    """Full EM with the SSD likelihood. Returns (iterations, final[V*N], stats[iters, 4]);
+    params is updated in place."""
+    fl = _c64(final_locations).ravel().copy()
+    stats = (_IterStats * max(1, max_iter))()
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    it = lib().orc_ssd_em(fl, _c64(voxel_pos).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                          C.addressof(params), _c64(D).ravel(), g, float(sigma), *vshape,
+                          *nshape, K, L, float(non_zero_voxels), int(max_iter),
+                          float(convergence_th), int(update), C.addressof(stats))
+    st = np.array([[s.mll, s.log_prior_likelihood, s.log_prior_transformation, s.mlp]
+                   for s in stats[:it]])
+    return it, fl, st
 
 
 def jacobian3d(field, shape, vs=(1.0, 1.0, 1.0)):
