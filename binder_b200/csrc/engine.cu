@@ -96,7 +96,9 @@ void DctSet::init(int nx, int ny, int nz, cudaStream_t s) {
     for (int a = 0; a < 3; ++a) {
         const int m = dims[a];
         n[a] = m;
-        if (m < 2) continue;  // the unit z axis of a 2D image has no transform
+        // the unit z axis of a 2D image has no transform; a unit axis of the image itself has
+        // the 1 x 1 identity
+        if (a == 2 && nz == 1) continue;
         std::vector<double> C((size_t)m * m);
         dct2_matrix(m, C.data());
         std::vector<float> F((size_t)m * m), I((size_t)m * m);

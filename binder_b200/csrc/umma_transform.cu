@@ -467,6 +467,7 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     const long o = valid ? lg / a.s : 0, t = valid ? lg - o * a.s : 0;
     const long lbase = o * (long)n * a.s + t;  // element (line, j) at lbase + j * s
     const int cr = lane & 7, cq = lane >> 3;   // contiguous-axis load mapping
+    float dfirst[32];  // prior eigenvalues of the epilogue's first 32 coefficients
 
     if (!producer) {
         // ---- MMA warp ------------------------------------------------------------------------
@@ -583,6 +584,11 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                 if (go && kc + q < nkc) go = step(kc + q, pre[q]);
         }
         umma::cp_async_wait_all();
+        if (MODE == kEpiSpectralOut) {  // in flight while the last MMAs finish
+#pragma unroll
+            for (int m = 0; m < 32; ++m)
+                dfirst[m] = (valid && m < n) ? __ldg(a.D + (long)m * a.s + t) : 0.0f;
+        }
         // the whole accumulation
         if (!*(volatile int *)s_err) {
             const bool ok = umma::mbar_wait(&done[(nkc - 1) % 3],
@@ -601,7 +607,8 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     if (producer && !*s_err) {
         // ---- epilogue: 32 TMEM columns at a time -------------------------------------------
         const int nchunks = (n + 31) / 32;
-        if (contig) {
+        // the prior scaling runs per line (its unit-stride case, a one-row image, included)
+        if (contig && MODE != kEpiSpectralOut) {
             float *stg = reinterpret_cast<float *>(smem_raw) + warp * 32 * 33;
             float rowc = 0.0f;
             if (MODE == kEpiPositions && !a.xpos) {
@@ -639,7 +646,9 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                     dnext[m] = (valid && k < n) ? __ldg(a.D + (long)k * a.s + t) : 0.0f;
                 }
             };
-            if (MODE == kEpiSpectralOut) load_dchunk(0);
+            if (MODE == kEpiSpectralOut)
+#pragma unroll
+                for (int m = 0; m < 32; ++m) dnext[m] = dfirst[m];
             for (int cc = 0; cc < nchunks; ++cc) {
                 float v[32], dcur[32];
                 umma::tmem_ld32(tmem + tlane + (uint32_t)(cc * 32), v);
@@ -658,7 +667,7 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                         float val = v[m];
                         if (MODE == kEpiSpectralOut) {
                             const float Dv = dcur[m];
-                            const float f = __frcp_rn(fmaf(gs2, Dv, 1.0f));
+                            const float f = __fdividef(1.0f, fmaf(gs2, Dv, 1.0f));
                             val *= f;
                             if (a.sample)
                                 val += sqrtf((float)a.sigma2 * f) *
