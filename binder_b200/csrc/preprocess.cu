@@ -362,6 +362,110 @@ __global__ void warp_kernel(const double *im, int nx, int ny, int nz, const doub
     }
 }
 
+// ---- order 3: cubic B-spline interpolation (scipy.ndimage.map_coordinates, order 3, mode
+// 'grid-constant', prefilter on).  The image is padded by kSplinePad zero samples on every side,
+// the padded array is converted to cubic B-spline coefficients by the recursive filter of Unser,
+// Aldroubi and Eden ("B-spline signal processing", IEEE Trans. Signal Process. 41, 1993): per
+// line, gain 6, a causal pass from a truncated mirror-symmetric start, an anti-causal pass from
+// the mirror-symmetric end condition, pole z = sqrt(3) - 2.  An output sample is the 64-tap
+// cubic B-spline sum of the coefficients around its position; taps outside the padded array
+// read 0.  Zero padding makes the boundary condition of the filter immaterial to FP64 precision
+// (its influence decays as |z|^12 before reaching the image and again before returning).
+constexpr int kSplinePad = 12;
+constexpr double kPole3 = -0.267949192431122706472553658494127633;  // sqrt(3) - 2
+
+__global__ void pad_kernel(const double *im, int nx, int ny, int nz, double *c, int qx, int qy,
+                           int qz) {
+    const long n = (long)qx * qy * qz;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        const long Z = i % qz, r = i / qz, Y = r % qy, X = r / qy;
+        const long x = X - kSplinePad, y = Y - kSplinePad, z = Z - kSplinePad;
+        c[i] = (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz)
+                   ? im[(x * ny + y) * nz + z]
+                   : 0.0;
+    }
+}
+
+// one thread per line of length n (n >= 3) and element stride s: lines (o, t), o < outer, t < s,
+// element k at o * n * s + t + k * s; in place
+__global__ void spline_line_kernel(double *c, long outer, int n, long s) {
+    const long nlines = outer * s;
+    for (long l = (long)blockIdx.x * blockDim.x + threadIdx.x; l < nlines;
+         l += (long)gridDim.x * blockDim.x) {
+        const long o = l / s, t = l - o * s;
+        double *p = c + o * (long)n * s + t;
+        const double z = kPole3;
+        // causal start: sum_k z^k c[k] over the terms above double precision
+        const int h = n < 40 ? n : 40;
+        double acc = 0.0, zk = 1.0;
+        for (int k = 0; k < h; ++k) {
+            acc = fma(zk, 6.0 * p[(long)k * s], acc);
+            zk *= z;
+        }
+        double prev = acc;
+        p[0] = prev;
+        for (int k = 1; k < n; ++k) {
+            prev = fma(z, prev, 6.0 * p[(long)k * s]);
+            p[(long)k * s] = prev;
+        }
+        // anti-causal start from the last two causal values, then backwards in place
+        double next = (z / (z * z - 1.0)) * (prev + z * p[(long)(n - 2) * s]);
+        p[(long)(n - 1) * s] = next;
+        for (int k = n - 2; k >= 0; --k) {
+            next = z * (next - p[(long)k * s]);
+            p[(long)k * s] = next;
+        }
+    }
+}
+
+__device__ __forceinline__ void bspline3_d(double t, double w[4]) {
+    const double e = 1.0 - t;
+    w[0] = e * e * e * (1.0 / 6.0);
+    w[1] = (2.0 / 3.0) - t * t + 0.5 * t * t * t;
+    w[2] = (2.0 / 3.0) - e * e + 0.5 * e * e * e;
+    w[3] = t * t * t * (1.0 / 6.0);
+}
+
+__global__ void warp3_kernel(const double *c, int qx, int qy, int qz, const double *pos, long M,
+                             double *out) {
+    for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < M;
+         m += (long)gridDim.x * blockDim.x) {
+        const double cx = pos[m * 3] + kSplinePad, cy = pos[m * 3 + 1] + kSplinePad,
+                     cz = pos[m * 3 + 2] + kSplinePad;
+        double v = 0.0;
+        // non-finite, or every tap outside the padded array: the fill value
+        const bool near = cx > -3.0 && cy > -3.0 && cz > -3.0 && cx < qx + 2.0 &&
+                          cy < qy + 2.0 && cz < qz + 2.0;
+        if (near) {
+            const double fx = floor(cx), fy = floor(cy), fz = floor(cz);
+            double wx[4], wy[4], wz[4];
+            bspline3_d(cx - fx, wx);
+            bspline3_d(cy - fy, wy);
+            bspline3_d(cz - fz, wz);
+            const int bx = (int)fx - 1, by = (int)fy - 1, bz = (int)fz - 1;
+            for (int i = 0; i < 4; ++i) {
+                const int X = bx + i;
+                if (X < 0 || X >= qx) continue;
+                double ay = 0.0;
+                for (int j = 0; j < 4; ++j) {
+                    const int Y = by + j;
+                    if (Y < 0 || Y >= qy) continue;
+                    const double *row = c + ((long)X * qy + Y) * qz;
+                    double az = 0.0;
+                    for (int k = 0; k < 4; ++k) {
+                        const int Zi = bz + k;
+                        if (Zi >= 0 && Zi < qz) az = fma(wz[k], row[Zi], az);
+                    }
+                    ay = fma(wy[j], az, ay);
+                }
+                v = fma(wx[i], ay, v);
+            }
+        }
+        out[m] = v;
+    }
+}
+
 __global__ void clip_kernel(double *out, long M, double lo, double hi) {
     for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < M;
          m += (long)gridDim.x * blockDim.x)
@@ -372,16 +476,36 @@ __global__ void clip_kernel(double *out, long M, double lo, double hi) {
 void warp_image(const double *image, int nx, int ny, int nz, const double *positions, long M,
                 int order, double *out) {
     BINDER_CHECK(nx > 0 && ny > 0 && nz > 0 && M > 0, "sizes must be positive");
-    BINDER_CHECK(order == 0 || order == 1, "interpolation order must be 0 or 1");
+    BINDER_CHECK(order == 0 || order == 1 || order == 3, "interpolation order must be 0, 1 or 3");
     const long V = (long)nx * ny * nz;
     Stream st;
     const cudaStream_t s = st.s;
     DBuf<double> di(V, s), dp(M * 3, s), dout(M, s);
     BINDER_CUDA(cudaMemcpyAsync(di.p, image, sizeof(double) * V, cudaMemcpyDefault, s));
     BINDER_CUDA(cudaMemcpyAsync(dp.p, positions, sizeof(double) * M * 3, cudaMemcpyDefault, s));
-    count_launch(), warp_kernel<<<blocks(M), 256, 0, s>>>(di.p, nx, ny, nz, dp.p, M, order,
-                                                          dout.p);
-    BINDER_CUDA(cudaGetLastError());
+    if (order == 3) {
+        const int qx = nx + 2 * kSplinePad, qy = ny + 2 * kSplinePad, qz = nz + 2 * kSplinePad;
+        const long Q = (long)qx * qy * qz;
+        DBuf<double> dc(Q, s);
+        count_launch(), pad_kernel<<<blocks(Q), 256, 0, s>>>(di.p, nx, ny, nz, dc.p, qx, qy, qz);
+        BINDER_CUDA(cudaGetLastError());
+        // x and y lines: neighbouring threads take neighbouring z, so every access is coalesced;
+        // z lines are contiguous per thread
+        count_launch(), spline_line_kernel<<<blocks((long)qy * qz), 256, 0, s>>>(
+            dc.p, 1, qx, (long)qy * qz);
+        count_launch(), spline_line_kernel<<<blocks((long)qx * qz), 256, 0, s>>>(dc.p, qx, qy,
+                                                                                   qz);
+        count_launch(), spline_line_kernel<<<blocks((long)qx * qy), 256, 0, s>>>(
+            dc.p, (long)qx * qy, qz, 1);
+        count_launch(), warp3_kernel<<<blocks(M), 256, 0, s>>>(dc.p, qx, qy, qz, dp.p, M,
+                                                               dout.p);
+        BINDER_CUDA(cudaGetLastError());
+        // dc is released on s after the interpolation
+    } else {
+        count_launch(), warp_kernel<<<blocks(M), 256, 0, s>>>(di.p, nx, ny, nz, dp.p, M, order,
+                                                              dout.p);
+        BINDER_CUDA(cudaGetLastError());
+    }
     // skimage clips the output to the input's range, widened to the fill value 0 when 0 lies
     // outside that range but inside the output's
     double imn, imx, omn, omx;

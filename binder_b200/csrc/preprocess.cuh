@@ -3,7 +3,7 @@
 //   - the centre of mass of the non-zero bins (BINDER/FastRegistration.py:387-395, scipy's
 //     center_of_mass of a boolean mask);
 //   - utils.save_warped_image's resampling of the moving image through the final positions
-//     (BINDER/utils.py:222-227: skimage.transform.warp, order 0 or 1, constant zero outside).
+//     (BINDER/utils.py:222-227: skimage.transform.warp, order 0, 1 or 3, constant zero outside).
 #pragma once
 
 #include <stdint.h>
@@ -26,8 +26,9 @@ void bin_signal(const T *signal, long n, int number_of_bins, int32_t *binned);
 // centre of mass (index space) of the voxels with bins > 0; false when there is none
 bool center_of_mass_nonzero(const int32_t *bins, int nx, int ny, int nz, double out[3]);
 
-// out[m] = image sampled at positions[m] (AoS [M][3], index space) with order 0 (nearest) or 1
-// (trilinear) interpolation, zero outside the image, clipped as skimage clips warp output.
+// out[m] = image sampled at positions[m] (AoS [M][3], index space) with order 0 (nearest), 1
+// (trilinear) or 3 (cubic B-spline, spline-prefiltered) interpolation, zero outside the image,
+// clipped as skimage clips warp output.
 // image [nx][ny][nz], out [M]; host or device memory.
 void warp_image(const double *image, int nx, int ny, int nz, const double *positions, long M,
                 int order, double *out);

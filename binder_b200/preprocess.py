@@ -56,7 +56,7 @@ def center_of_mass_nonzero(bins):
 
 def warp_image(moving_image, deformed_position, order=1):
     """The resampling of ``utils.save_warped_image`` (BINDER/utils.py:222-227): the moving image
-    sampled at the deformed positions [..., 3] (index space), order 0 or 1, zero outside,
+    sampled at the deformed positions [..., 3] (index space), order 0, 1 or 3, zero outside,
     clipped as skimage clips.  Returns an array of the positions' spatial shape."""
     im = np.ascontiguousarray(moving_image, dtype=np.float64)
     pos = np.ascontiguousarray(deformed_position, dtype=np.float64)

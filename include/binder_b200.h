@@ -223,7 +223,8 @@ int binder_bin_signal(const void *signal, int is_double, long long n, int number
  * space, exact (integer sums, one division).  No non-zero voxel: INVALID_ARGUMENT. */
 int binder_center_of_mass(const int32_t *bins, int Nx, int Ny, int Nz, double out[3]);
 /* the resampling of utils.save_warped_image (BINDER/utils.py:222-227): skimage.transform.warp of
- * the moving image [Nx][Ny][Nz] (FP64) at positions [M][3] (index space) with order 0 or 1,
+ * the moving image [Nx][Ny][Nz] (FP64) at positions [M][3] (index space) with order 0, 1 or 3
+ * (cubic B-spline with the spline prefilter, as run_BINDER.py's default --output-interpolation),
  * zero outside, clipped to the input range as skimage clips; out [M] FP64. */
 int binder_warp_image(const double *image, int Nx, int Ny, int Nz, const double *positions,
                       long long M, int order, double *out);

@@ -13,6 +13,8 @@ def test_warp_restatement_identity(oracle):
     pos = np.stack(np.indices(im.shape), -1).astype(np.float64)
     for order in (0, 1):
         np.testing.assert_array_equal(oracle.warp_image(im, pos, order), im)
+    # the cubic spline interpolates its samples
+    np.testing.assert_allclose(oracle.warp_image(im, pos, 3), im, rtol=0, atol=1e-12)
 
 
 @pytest.mark.gpu
@@ -66,7 +68,7 @@ def test_center_of_mass_matches_scipy(core, shape):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("order", [0, 1])
+@pytest.mark.parametrize("order", [0, 1, 3])
 def test_warp_image_matches_restatement(core, oracle, order):
     from binder_b200 import phantoms, preprocess as pp
     rng = np.random.default_rng(7 + order)
@@ -84,3 +86,22 @@ def test_warp_image_matches_restatement(core, oracle, order):
         np.testing.assert_array_equal(got[ok], want[ok])
     else:
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_warp_cubic_far_outside_and_small(core, oracle):
+    """Order 3 on a small image at points inside, at the edge, beyond the 12-sample padding the
+    spline prefilter uses, and non-finite ones; the input range excludes 0 (clip widening)."""
+    from binder_b200 import preprocess as pp
+    rng = np.random.default_rng(3)
+    im = rng.random((9, 7, 11)) * 5.0 + 1.0
+    pos = np.concatenate([
+        rng.uniform(-3.0, np.array(im.shape) + 2.0, (400, 3)),
+        np.array([[-11.5, 3.0, 3.0], [-12.7, 2.2, 4.1], [3.0, 20.3, 5.0], [-30.0, 1.0, 1.0],
+                  [8.9, 6.9, 10.9], [0.0, 0.0, 0.0], [4.0, 3.0, 33.9]])])
+    got = pp.warp_image(im, pos, 3)
+    want = oracle.warp_image(im, pos, 3)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+    # non-finite and huge coordinates give the fill value (scipy gives NaN, or overflows)
+    bad = np.array([[np.nan, 1.0, 1.0], [2.0, np.inf, 2.0], [1e300, 0.0, 0.0]])
+    assert np.all(pp.warp_image(im, bad, 3) == 0.0)
