@@ -112,7 +112,25 @@ class Registration:
         check(lib().binder_registration_set_mi_likelihood(
             self._h, float(alpha), _f32(theta, K * L, "theta"), K, L, int(threads),
             _i32(binned_nodes, Vn, "binned_nodes"), _i32(binned_voxels, self._V, "binned_voxels")))
-        self._K, self._L = K, L
+        self._K, self._L, self._M = K, L, 1
+        self._ssd = False
+
+    def setMILikelihoodFilter(self, alpha, theta, threads, binned_nodes, binned_voxels, K, L, M):
+        """``setMILikelihoodFilter`` of the CPU module (cpu/bindings.cpp:90-115): M channels,
+        theta [M][K][L]; channel m of voxel (node) i is read at [i + m] as MILikelihoodFilter.cpp
+        reads it, so the bin arrays need at least V + M - 1 (Vn + M - 1) entries (the usual
+        [..., M] arrays have more).  EM only."""
+        K, L, M = int(K), int(L), int(M)
+        Vn = int(np.prod(self._nshape))
+        nodes = _i32(binned_nodes)
+        voxels = _i32(binned_voxels)
+        if nodes.size < Vn + M - 1 or voxels.size < self._V + M - 1:
+            raise ValueError(f"binned_nodes / binned_voxels need at least {Vn + M - 1} / "
+                             f"{self._V + M - 1} bins for M = {M}")
+        check(lib().binder_registration_set_mi_likelihood_filter(
+            self._h, float(alpha), _f32(theta, M * K * L, "theta"), int(threads), nodes, voxels,
+            K, L, M))
+        self._K, self._L, self._M = K, L, M
         self._ssd = False
 
     def setSSDLikelihood(self, bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
@@ -125,6 +143,7 @@ class Registration:
             float(shift), _i32(binned_nodes, Vn, "binned_nodes"),
             _i32(binned_voxels, self._V, "binned_voxels"), float(alpha_0), float(beta_0)))
         self._K = self._L = bins
+        self._M = 1
         self._ssd = True
 
     def ssd_parameters(self):
@@ -180,8 +199,9 @@ class Registration:
     def get_likelihood_parameters(self):
         if self._K is None:
             raise BinderError(4, "setMILikelihood has not been called")
-        n = 2 if getattr(self, "_ssd", False) else self._K * self._L  # SSD: (scale, shift)
-        out = np.zeros(self._K * self._L, np.float32)
+        M = getattr(self, "_M", 1)
+        n = 2 if getattr(self, "_ssd", False) else M * self._K * self._L  # SSD: (scale, shift)
+        out = np.zeros(max(n, self._K * self._L), np.float32)
         check(lib().binder_registration_get_likelihood_parameters(self._h, out))
         return out[:n]
 

@@ -21,6 +21,7 @@ EXPORTS = [
     "binder_last_error", "binder_backend", "binder_has_topology_correction",
     "binder_registration_create", "binder_registration_destroy",
     "binder_registration_set_mi_likelihood", "binder_registration_set_nonlinear_transformation",
+    "binder_registration_set_mi_likelihood_filter",
     "binder_registration_em", "binder_registration_sampler",
     "binder_registration_get_final_locations", "binder_registration_get_dream_locations",
     "binder_registration_set_dream_locations", "binder_registration_get_likelihood_parameters",
@@ -70,6 +71,7 @@ def _declare(lib):
         "binder_registration_create": [C.POINTER(_P), _f32, _i, _f32, _P] + [_i] * 7 + [_d],
         "binder_registration_destroy": [_P],
         "binder_registration_set_mi_likelihood": [_P, _d, _f32, _i, _i, _i, _i32, _i32],
+        "binder_registration_set_mi_likelihood_filter": [_P, _d, _f32, _i, _i32, _i32, _i, _i, _i],
         "binder_registration_set_nonlinear_transformation": [_P] + [_d] * 9 + [_f32],
         "binder_registration_em": [_P, _i, _d, _i, _i, C.POINTER(_i)],
         "binder_registration_sampler": [_P, _u64, _i, _i, _i, _i, _i, _i, _i, _f64, _f64],

@@ -96,6 +96,21 @@ int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, 
     });
 }
 
+int binder_registration_set_mi_likelihood_filter(binder_registration *h, double alpha,
+                                                 const float *theta, int threads,
+                                                 const int32_t *binned_nodes,
+                                                 const int32_t *binned_voxels, int K, int L,
+                                                 int M) {
+    (void)threads;
+    return guard([&] {
+        NEED(h);
+        NEED(theta);
+        NEED(binned_nodes);
+        NEED(binned_voxels);
+        h->impl->set_mi_filter_likelihood(alpha, theta, K, L, M, binned_nodes, binned_voxels);
+    });
+}
+
 int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int threads,
                                            double sigma_sq, int scale_shift, double scale,
                                            double shift, const int32_t *binned_nodes,

@@ -328,15 +328,42 @@ Registration::~Registration() {
 
 void Registration::set_mi_likelihood(double alpha, const float *theta, int K, int L,
                                      const int *binned_nodes, const int *binned_voxels) {
+    BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
+    load_bins(alpha, theta, K, L, 1, binned_nodes, binned_voxels);
     lk_ = 0;
+    egrid_e_ = estep_grid(false, K, L, V_, N_);
+    egrid_s_ = estep_grid(true, K, L, V_, N_);
+    have_mi_ = true;
+}
+
+// The MI filter likelihood (BINDER/src/cpu/Registration.cpp:466-470, MILikelihoodFilter.cpp):
+// M channels of bins, channel m of voxel i at binned_voxels[i + m] and of node j at
+// binned_nodes[j + m] (so the arrays hold at least V + M - 1 and Vn + M - 1 bins); theta
+// [M][K][L].  Its theta update and cost are the MI ones over M * K rows.
+void Registration::set_mi_filter_likelihood(double alpha, const float *theta, int K, int L,
+                                            int M, const int *binned_nodes,
+                                            const int *binned_voxels) {
+    BINDER_CHECK(M >= 1 && M <= kMaxChannels, "the number of channels M must be in [1, 8]");
+    BINDER_CHECK((long)M * K * L <= kFilterMaxCells,
+                 "M * K * L must be at most 24576 (shared-memory theta and histograms)");
+    load_bins(alpha, theta, K, L, M, binned_nodes, binned_voxels);
+    lk_ = 2;
+    egrid_e_ = estep_filter_grid(K, L, M, V_, N_);
+    egrid_s_ = 0;
+    have_mi_ = true;
+}
+
+void Registration::load_bins(double alpha, const float *theta, int K, int L, int M,
+                             const int *binned_nodes, const int *binned_voxels) {
+    have_mi_ = false;
     BINDER_CHECK(K >= 1 && K <= 256 && L >= 1 && L <= 256,
                  "numbers of bins K and L must be in [1, 256]");
-    BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
     BINDER_CUDA(cudaStreamSynchronize(stream_));  // buffers below may be in use
     em_graph_.clear();
     const cudaStream_t s = own_stream_;
     // zero-padded byte volume of the node bins, in the E-step's view (a 2D node grid nxn x nyn
-    // is the volume nxn x 1 x nyn: its y axis is the packed axis and has no padded y rows)
+    // is the volume nxn x 1 x nyn: its y axis is the packed axis and has no padded y rows); one
+    // per channel.  The voxel bins of channel m are the byte array shifted by m.
     const View w = estep_view();
     P_ = 8;
     PZ_ = 8;
@@ -344,35 +371,41 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     pyn_ = w.nyn + 2 * Py;
     zp_ = ((w.nzn + 2 * PZ_ + 3) / 4) * 4 + 4;
     const size_t padded = (size_t)(w.nxn + 2 * P_) * pyn_ * zp_;
+    const long nv = V_ + M - 1, nn = Vn_ + M - 1;  // bins read: [index + m], m < M
+    const long cells = (long)M * K * L;
     dfree(u_, s); dfree(vpad_, s); dfree(theta_, s); dfree(hist_, s); dfree(hcnt_, s);
     dfree(theta0_, s);
-    u_ = dalloc<uint8_t>((size_t)V_, s);
-    theta0_ = dalloc<float>((size_t)K * L, s);
-    vpad_ = dalloc<uint8_t>(padded, s);
-    theta_ = dalloc<float>((size_t)K * L, s);
-    hist_ = dalloc<float>((size_t)K * L, s);
-    hcnt_ = dalloc<unsigned>((size_t)K * L, s);
+    u_ = dalloc<uint8_t>((size_t)nv, s);
+    theta0_ = dalloc<float>((size_t)cells, s);
+    vpad_ = dalloc<uint8_t>(padded * M, s);
+    theta_ = dalloc<float>((size_t)cells, s);
+    hist_ = dalloc<float>((size_t)cells, s);
+    hcnt_ = dalloc<unsigned>((size_t)cells, s);
     // int32 bins to the device as they are, narrowed to bytes (and range-checked) there
-    int *bins = dalloc<int>((size_t)(V_ + Vn_), s);
-    unsigned long long *bad = dalloc<unsigned long long>(2, s);
-    BINDER_CUDA(cudaMemsetAsync(bad, 0xff, 2 * sizeof(unsigned long long), s));
-    BINDER_CUDA(cudaMemcpyAsync(bins, binned_voxels, sizeof(int) * V_, cudaMemcpyDefault, s));
-    BINDER_CUDA(cudaMemcpyAsync(bins + V_, binned_nodes, sizeof(int) * Vn_, cudaMemcpyDefault, s));
-    launch_bins_to_u8(bins, V_, L, u_, bad, s);
-    BINDER_CUDA(cudaMemsetAsync(vpad_, 0, padded, s));
-    launch_bins_to_padded(bins + V_, w.nxn, w.nyn, w.nzn, K, vpad_, P_, Py, PZ_, pyn_, zp_, bad + 1,
-                          s);
-    BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * K * L, cudaMemcpyDefault, s));
-    BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * K * L, cudaMemcpyDeviceToDevice, s));
-    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K * L, s));
-    BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K * L, s));
+    int *bins = dalloc<int>((size_t)(nv + nn), s);
+    uint8_t *nodes8 = M > 1 ? dalloc<uint8_t>((size_t)nn, s) : nullptr;
+    unsigned long long *bad = dalloc<unsigned long long>(3, s);
+    BINDER_CUDA(cudaMemsetAsync(bad, 0xff, 3 * sizeof(unsigned long long), s));
+    BINDER_CUDA(cudaMemcpyAsync(bins, binned_voxels, sizeof(int) * nv, cudaMemcpyDefault, s));
+    BINDER_CUDA(cudaMemcpyAsync(bins + nv, binned_nodes, sizeof(int) * nn, cudaMemcpyDefault, s));
+    launch_bins_to_u8(bins, nv, L, u_, bad, s);
+    // every node bin is checked once here; the padded volumes below check their windows again
+    if (nodes8) launch_bins_to_u8(bins + nv, nn, K, nodes8, bad + 1, s);
+    BINDER_CUDA(cudaMemsetAsync(vpad_, 0, padded * M, s));
+    for (int m = 0; m < M; ++m)
+        launch_bins_to_padded(bins + nv + m, w.nxn, w.nyn, w.nzn, K, vpad_ + padded * m, P_, Py,
+                              PZ_, pyn_, zp_, M > 1 ? bad + 2 : bad + 1, s);
+    BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * cells, cudaMemcpyDefault, s));
+    BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * cells, cudaMemcpyDeviceToDevice, s));
+    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * cells, s));
+    BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * cells, s));
     unsigned long long hbad[2];
     BINDER_CUDA(cudaMemcpyAsync(hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, s));
     BINDER_CUDA(cudaStreamSynchronize(s));
     dfree(bad, s);
     dfree(bins, s);
+    if (nodes8) dfree(nodes8, s);
     if (hbad[0] != ~0ull || hbad[1] != ~0ull) {
-        have_mi_ = false;
         // the offending value, read through a copy (the arrays may be device memory)
         auto value_at = [](const int *a, unsigned long long i) {
             int v = 0;
@@ -389,10 +422,9 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     }
     K_ = K;
     L_ = L;
+    M_ = M;
+    vch_ = (long)padded;
     alpha_ = alpha;
-    egrid_e_ = estep_grid(false, K, L, V_, N_);
-    egrid_s_ = estep_grid(true, K, L, V_, N_);
-    have_mi_ = true;
 }
 
 // The SSD likelihood is a K x L table over (node bin, voxel bin) -- outside nodes count as bin
@@ -500,6 +532,7 @@ EStepArgs Registration::estep_args(const int *skip) const {
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
     e.seed = seed_; e.chain = chain_; e.order = order_;
     e.logt = lk_ == 1; e.colmax = colmax_;
+    e.M = M_; e.filter = lk_ == 2; e.uch = 1; e.vch = vch_;
     return e;
 }
 
@@ -508,7 +541,7 @@ void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
     if (lk_ == 1)
         launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, stream_);
     else
-        launch_theta_update(theta_, hist_, K_, L_, alpha_, update, st_, stream_);
+        launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, stream_);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
                    rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, stream_);
@@ -600,6 +633,9 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     }
     if (lk_ == 1)
         throw Error(kUnsupported, "the sampler with the SSD likelihood is not built (EM only)");
+    if (lk_ == 2)
+        throw Error(kUnsupported,
+                    "the sampler with the MI filter likelihood is not built (EM only)");
     if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
     BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
     BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
@@ -684,7 +720,7 @@ double Registration::profile_stage(int stage, int n) {
                            rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
         else if (lk_ == 1)
             launch_ssd_update(theta_, colmax_, hist_, K_, L_, 0, ssd_, st_, stream_);
-        else launch_theta_update(theta_, hist_, K_, L_, alpha_, 1, st_, stream_);
+        else launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, 1, st_, stream_);
     };
     one();  // warm-up
     cudaEvent_t t0, t1;
@@ -698,7 +734,7 @@ double Registration::profile_stage(int stage, int n) {
     BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
+    BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * M_ * K_ * L_, stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
     return ms / n;
 }
@@ -727,10 +763,10 @@ void PriorTransform::set_precision(int p) {
 void Registration::reset() {
     BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * N_, cudaMemcpyDeviceToDevice, stream_));
     if (have_mi_) {
-        BINDER_CUDA(cudaMemcpyAsync(theta_, theta0_, sizeof(float) * K_ * L_,
+        BINDER_CUDA(cudaMemcpyAsync(theta_, theta0_, sizeof(float) * M_ * K_ * L_,
                                     cudaMemcpyDeviceToDevice, stream_));
-        BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * K_ * L_, stream_));
-        BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * K_ * L_, stream_));
+        BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * M_ * K_ * L_, stream_));
+        BINDER_CUDA(cudaMemsetAsync(hcnt_, 0, sizeof(unsigned) * M_ * K_ * L_, stream_));
     }
     if (lk_ == 1) {
         BINDER_CUDA(cudaMemcpyAsync(ssd_, ssd0_, sizeof(SsdState), cudaMemcpyDeviceToDevice,
@@ -793,7 +829,7 @@ void Registration::get_likelihood_parameters(float *out) const {
         out[1] = (float)p[1];
         return;
     }
-    BINDER_CUDA(cudaMemcpyAsync(out, theta_, sizeof(float) * K_ * L_, cudaMemcpyDeviceToHost,
+    BINDER_CUDA(cudaMemcpyAsync(out, theta_, sizeof(float) * M_ * K_ * L_, cudaMemcpyDeviceToHost,
                                 stream_));
     BINDER_CUDA(cudaStreamSynchronize(stream_));
 }

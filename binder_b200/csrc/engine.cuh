@@ -63,6 +63,10 @@ class Registration {
 
     void set_mi_likelihood(double alpha, const float *theta, int K, int L, const int *binned_nodes,
                            const int *binned_voxels);
+    // the MI filter likelihood (BINDER/src/cpu/Registration.cpp:466-470): M channels, theta
+    // [M][K][L], bins of channel m read at [index + m]; EM only
+    void set_mi_filter_likelihood(double alpha, const float *theta, int K, int L, int M,
+                                  const int *binned_nodes, const int *binned_voxels);
     void set_nonlinear_transformation(const double gamma[3], const double rho[3],
                                       const double eta[3], const float *D);
     // the SSD likelihood instead of MI (BINDER/src/cpu/Registration.cpp:472-479), EM only
@@ -118,6 +122,9 @@ class Registration {
     void enqueue_em_iteration(int max_iter, double th, int update);
     void reset_state(bool for_sampler);
     void require_ready() const;
+    // bins, theta and histogram buffers of an M-channel MI-type likelihood
+    void load_bins(double alpha, const float *theta, int K, int L, int M, const int *binned_nodes,
+                   const int *binned_voxels);
 
     int nx_, ny_, nz_, nxn_, nyn_, nzn_, N_;
     long V_, Vn_;
@@ -140,6 +147,8 @@ class Registration {
     // likelihood / prior parameters
     bool have_mi_ = false, have_tr_ = false;
     int K_ = 0, L_ = 0;
+    int M_ = 1;      // channels of the MI filter likelihood (1 otherwise)
+    long vch_ = 0;   // bytes between the channels' padded bin volumes
     double alpha_ = 2.0;
     double gamma0_[3] = {0, 0, 0}, rho_[3] = {1, 1, 1}, eta_[3] = {1, 1, 1};
     double sigma2_ = 0.0;
@@ -148,7 +157,8 @@ class Registration {
     uint64_t seed_ = 12345;
     int iters_done_ = 0;
     int order_ = 3;  // B-spline order of the E-step
-    int lk_ = 0;     // likelihood: 0 MI (theta_ is theta), 1 SSD (theta_ is its log2 table)
+    int lk_ = 0;     // likelihood: 0 MI (theta_ is theta), 1 SSD (theta_ is its log2 table),
+                     // 2 MI filter (theta_ is [M][K][L])
     SsdState *ssd_ = nullptr, *ssd0_ = nullptr;  // SSD parameters, and as set
     float *colmax_ = nullptr, *colmax0_ = nullptr;  // SSD table column maxima, and as set
     double last_ms_ = 0.0;

@@ -96,10 +96,11 @@ __device__ __forceinline__ void gather_bins(const EStepArgs &a, int ix, int iy, 
     }
 }
 
-// word (p, q) of gather_bins alone: bins of nodes (ix-1+p, iy-1+q, iz-1 .. iz+2) (q = 0 in 2D)
+// word (p, q) of gather_bins alone: bins of nodes (ix-1+p, iy-1+q, iz-1 .. iz+2) (q = 0 in 2D),
+// from the padded bin volume vpad (a.vpad, or one channel's volume of the filter likelihood)
 template <int DIM>
-__device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int iy, int iz, int p,
-                                                int q) {
+__device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, const uint8_t *vpad, int ix,
+                                                int iy, int iz, int p, int q) {
     const int zz0 = iz - 1 + a.PZ;
     const int Py = DIM == 3 ? a.P : 0;
     const int X = ix - 1 + p, Y = DIM == 3 ? iy - 1 + q : 0;
@@ -108,7 +109,7 @@ __device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int 
                       (zz0 >= 0) && ((zz0 >> 2) + 2 <= (a.zp >> 2));
     if (fast) {
         const uint32_t *rowp = reinterpret_cast<const uint32_t *>(
-            a.vpad + ((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp);
+            vpad + ((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp);
         const int w = zz0 >> 2, sh = (zz0 & 3) * 8;
         return __funnelshift_r(__ldg(rowp + w), __ldg(rowp + w + 1), sh);
     }
@@ -118,7 +119,7 @@ __device__ __forceinline__ uint32_t gather_word(const EStepArgs &a, int ix, int 
         const int Z = iz - 1 + c;
         uint32_t b = 0;
         if (X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn)
-            b = a.vpad[((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp + (Z + a.PZ)];
+            b = vpad[((long)(X + a.P) * a.pyn + (Y + Py)) * a.zp + (Z + a.PZ)];
         word |= b << (8 * c);
     }
     return word;
@@ -373,6 +374,120 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
     if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
 }
 
+// EM E-step with the MI filter likelihood (BINDER/src/cpu/MILikelihoodFilter.cpp:53-68 and
+// :110-124 inside Registration.cpp:219-330): the weight of a neighbour is its spline weight times
+// prod_m theta[m][k_m][u_m], the bins of channel m being read at [index + m] -- which the host has
+// resolved into one shifted bin volume per channel -- and the posterior mass goes to every
+// channel's histogram.  theta [M][L][KP] (transposed per channel) and the histograms [M][K][LP]
+// live in shared memory; the second pass recomputes the weights and adds p = w / S with one
+// shared atomic per channel and neighbour.
+template <int DIM>
+__global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepArgs a) {
+    constexpr int Q = DIM == 3 ? 4 : 1;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) float sm[];
+    const int K = a.K, L = a.L, M = a.M;
+    const int KP = theta_pitch(K), LP = theta_pitch(L);
+    const int KL = K * L;
+    float *thT = sm;                        // [M][L][KP]
+    float *hs = sm + (size_t)M * L * KP;    // [M][K][LP]
+    for (int q = threadIdx.x; q < M * KL; q += blockDim.x) {
+        const int m = q / KL, r = q - m * KL, k = r / L, l = r - k * L;
+        thT[(m * L + l) * KP + k] = a.theta[q];
+        hs[(m * K + k) * LP + l] = 0.0f;
+    }
+    __syncthreads();
+
+    double mll = 0.0;
+    unsigned deg = 0;
+    const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+        VoxelPos<DIM> vp;
+        if (!vp.load(a, i, V, ny, nz)) {
+            vp.store_r(a, i, V, vp.px, vp.py, vp.pz);
+            ++deg;
+            continue;
+        }
+        float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
+        const int ix = spline_setup(vp.px, a.order, bx);
+        const int iy = DIM == 3 ? spline_setup(vp.py, a.order, by) : 0;
+        const int iz = spline_setup(vp.pz, a.order, bz);
+        const float fx = (float)ix, fy = (float)iy, fz = (float)iz;
+        int um[kMaxChannels];
+#pragma unroll
+        for (int m = 0; m < kMaxChannels; ++m) um[m] = m < M ? a.u[m * a.uch + i] : 0;
+        // pass 1: normaliser and first moments
+        float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p)
+#pragma unroll 1
+            for (int q = 0; q < Q; ++q) {
+                const float bxy = Q == 4 ? bx[p] * by[q] : bx[p];
+                float t[4] = {bxy * bz[0], bxy * bz[1], bxy * bz[2], bxy * bz[3]};
+#pragma unroll
+                for (int m = 0; m < kMaxChannels; ++m) {
+                    if (m >= M) break;
+                    const uint32_t w = gather_word<DIM>(a, a.vpad + m * a.vch, ix, iy, iz, p, q);
+                    const float *th = thT + (m * L + um[m]) * KP;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) t[c] *= th[(w >> (8 * c)) & 0xff];
+                }
+                const float s4 = (t[0] + t[1]) + (t[2] + t[3]);
+                S += s4;
+                Sx += (float)(p - 1) * s4;
+                if (Q == 4) Sy += (float)(q - 1) * s4;
+                Sz += (t[2] - t[0]) + 2.0f * t[3];
+            }
+        if (!(S > 0.0f)) {
+            vp.store_r(a, i, V, fx, fy, fz);
+            ++deg;
+            continue;
+        }
+        const float inv = 1.0f / S;
+        // pass 2: the posterior of every neighbour into every channel's histogram
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p)
+#pragma unroll 1
+            for (int q = 0; q < Q; ++q) {
+                const float bxy = Q == 4 ? bx[p] * by[q] : bx[p];
+                float t[4] = {bxy * bz[0], bxy * bz[1], bxy * bz[2], bxy * bz[3]};
+                uint32_t wd[kMaxChannels];
+#pragma unroll
+                for (int m = 0; m < kMaxChannels; ++m) {
+                    if (m >= M) break;
+                    wd[m] = gather_word<DIM>(a, a.vpad + m * a.vch, ix, iy, iz, p, q);
+                    const float *th = thT + (m * L + um[m]) * KP;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) t[c] *= th[(wd[m] >> (8 * c)) & 0xff];
+                }
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float pc = t[c] * inv;
+                    if (pc == 0.0f) continue;
+#pragma unroll
+                    for (int m = 0; m < kMaxChannels; ++m) {
+                        if (m >= M) break;
+                        const int k = (wd[m] >> (8 * c)) & 0xff;
+                        atomicAdd(&hs[(m * K + k) * LP + um[m]], pc);
+                    }
+                }
+            }
+        mll -= (double)logf(S);
+        vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < M * KL; q += blockDim.x) {
+        const int m = q / KL, r = q - m * KL, k = r / L, l = r - k * L;
+        const float v = hs[(m * K + k) * LP + l];
+        if (v != 0.0f) atomicAdd(&a.hist[q], v);
+    }
+    __shared__ double red[32];
+    const double ms = block_sum(mll, red);
+    if (threadIdx.x == 0) atomicAdd(&a.st->mll, ms);
+    const double dg = block_sum((double)deg, red);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+}
+
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
 // for the Gibbs draw and for EM with K > 64.
@@ -490,7 +605,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
             const float bxp = p == 0 ? bx[0] : (p == 1 ? bx[1] : (p == 2 ? bx[2] : bx[3]));
             const float byq = q == 0 ? by[0] : (q == 1 ? by[1] : (q == 2 ? by[2] : by[3]));
             const float bxy = DIM == 3 ? __fmul_rn(bxp, byq) : bxp;
-            const uint32_t word = gather_word<DIM>(a, ix, iy, iz, p, q);
+            const uint32_t word = gather_word<DIM>(a, a.vpad, ix, iy, iz, p, q);
             int pick = -1, kp = 0;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -504,7 +619,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) 
             }
             if (pick < 0) {  // unreachable (cdf ends at S >= t); keep the last neighbour
                 pick = 4 * R - 1;
-                kp = (gather_word<DIM>(a, ix, iy, iz, 3, Q - 1) >> 24) & 0xff;
+                kp = (gather_word<DIM>(a, a.vpad, ix, iy, iz, 3, Q - 1) >> 24) & 0xff;
             }
             atomicAdd(&hc[kp * L + a.u[i]], 1u);
             const int ox = pick / (4 * Q) - 1, oy = (pick / 4) % Q - 1, oz = pick % 4 - 1;
@@ -714,9 +829,15 @@ const void *estep_fn(bool sample, int K, bool logt) {
                                   : (const void *)estep_kernel<false, DIM>);
 }
 
+size_t filter_smem(int K, int L, int M) {
+    return (size_t)M * (L * theta_pitch(K) + K * theta_pitch(L)) * sizeof(float);
+}
+
 template <int DIM>
 void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
-    if (a.logt)
+    if (a.filter)
+        count_launch(), estep_filter_kernel<DIM><<<grid, kEThreads, smem, s>>>(a);
+    else if (a.logt)
         count_launch(), estep_em_fast_kernel<kFastThreads, DIM, true>
                             <<<grid, kFastThreads, smem, s>>>(a);
     else if (sample)
@@ -752,10 +873,38 @@ int estep_grid(bool sample, int K, int L, long V, int dim, bool logt) {
     return (int)g;
 }
 
+int estep_filter_grid(int K, int L, int M, long V, int dim) {
+    BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
+    BINDER_CHECK(M >= 1 && M <= kMaxChannels && (long)M * K * L <= kFilterMaxCells,
+                 "the MI filter likelihood needs 1 <= M <= 8 and M * K * L <= 24576");
+    int dev = 0, sms = 148, per_sm = 1;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem = filter_smem(K, L, M);
+    BINDER_CHECK(smem <= 227 * 1024,
+                 "the MI filter likelihood's theta and histograms do not fit in shared memory");
+    const void *fn = dim == 3 ? (const void *)estep_filter_kernel<3>
+                              : (const void *)estep_filter_kernel<2>;
+    BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+    BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kEThreads, smem));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const long need = (V + kEThreads - 1) / kEThreads;
+    long g = (long)sms * per_sm;
+    if (need < g) g = need < 1 ? 1 : need;
+    return (int)g;
+}
+
 void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) {
     BINDER_CHECK(!args.logt || (!sample && args.K <= kSmallK && args.colmax),
                  "the log-space E-step runs EM only, with at most 64 bins");
-    const size_t smem = estep_smem(sample, args.K, args.L, args.logt != 0);
+    BINDER_CHECK(!args.filter || (!sample && !args.logt && args.M >= 1 &&
+                                  args.M <= kMaxChannels &&
+                                  (long)args.M * args.K * args.L <= kFilterMaxCells),
+                 "the MI filter E-step runs EM only, with 1 <= M <= 8 and M * K * L <= 24576");
+    const size_t smem = args.filter ? filter_smem(args.K, args.L, args.M)
+                                    : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
     // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
     // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a

@@ -29,6 +29,11 @@ struct EStepArgs {
     // voxel bin l by their maximum over k, whose natural log is colmax[l]
     int logt;
     const float *colmax;
+    // the MI filter likelihood (M > 1 channels, or M == 1 with filter set): `u` and `vpad` hold
+    // one volume per channel, uch / vch bytes apart; theta and hist are [M][K][L]
+    int M;
+    int filter;
+    long uch, vch;
     uint64_t seed;
     uint32_t chain;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
@@ -39,6 +44,11 @@ void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
 int estep_grid(bool sample, int K, int L, long V, int dim, bool logt = false);
 // largest number of bins of the log-space (SSD) E-step
 constexpr int kLogMaxBins = 64;
+// largest number of channels of the MI filter likelihood, and of M * K * L (its shared-memory
+// theta and histograms)
+constexpr int kMaxChannels = 8;
+constexpr long kFilterMaxCells = 24576;
+int estep_filter_grid(int K, int L, int M, long V, int dim);
 
 // State of the SSD likelihood (BINDER/src/cpu/SSDLikelihood.cpp): sigma^2, shift, scale and the
 // inverse-gamma prior (alpha0, beta0) of sigma^2

@@ -68,6 +68,19 @@ int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, 
                                           int K, int L, int threads, const int32_t *binned_nodes,
                                           const int32_t *binned_voxels);
 
+/* setMILikelihoodFilter(alpha, theta, threads, binned_nodes, binned_voxels, K, L, M)
+ *                                                                  cpu/bindings.cpp:90-115
+ * The CPU backend's multi-channel MI likelihood (MILikelihoodFilter.cpp): theta [M][K][L]; the
+ * bins of channel m are read at [index + m] as the reference reads them, so binned_nodes holds
+ * at least Nx_n*Ny_n*Nz_n + M - 1 bins in [0, K) and binned_voxels Nx_v*Ny_v*Nz_v + M - 1 in
+ * [0, L).  1 <= M <= 8, M*K*L <= 24576.  EM only (the sampler rejects it);
+ * get_likelihood_parameters then returns M*K*L values. */
+int binder_registration_set_mi_likelihood_filter(binder_registration *h, double alpha,
+                                                 const float *theta, int threads,
+                                                 const int32_t *binned_nodes,
+                                                 const int32_t *binned_voxels, int K, int L,
+                                                 int M);
+
 /* setSSDLikelihood(bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
  *                  binned_voxels, alpha_0, beta_0)                  cpu/bindings.cpp:120-152
  * The CPU backend's SSD likelihood (SSDLikelihood.cpp): the bins are the intensities, bins <= 64;
@@ -111,7 +124,8 @@ int binder_registration_get_final_locations(const binder_registration *h, float 
 /* get_dream_locations() / set_dream_locations(arr)              gpu/bindings.cpp:133-140 */
 int binder_registration_get_dream_locations(const binder_registration *h, float *out);
 int binder_registration_set_dream_locations(binder_registration *h, const float *in);
-/* get_likelihood_parameters() -> K*L                            gpu/bindings.cpp:97 */
+/* get_likelihood_parameters() -> K*L (M*K*L with the filter likelihood, (scale, shift) with
+ * SSD)                                                                 gpu/bindings.cpp:97 */
 int binder_registration_get_likelihood_parameters(const binder_registration *h, float *out);
 /* get_shape() -> (Nx, Ny, Nz, N)                                cpu/bindings.cpp:294 */
 int binder_registration_get_shape(const binder_registration *h, int out[4]);

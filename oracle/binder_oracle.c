@@ -207,6 +207,98 @@ double orc_estep(const double *d, const int *u, const int *v, const double *thet
     return mll;
 }
 
+/* MILikelihoodFilter::compute_likelihood (BINDER/src/cpu/MILikelihoodFilter.cpp:53-68): the
+ * product over the M channels of theta[m][k_m][l_m], channel m of voxel i being u[i + m] and of
+ * node j v[j + m] (the reference's indexing: the channel windows overlap), a node outside the
+ * grid having bin 0 in every channel. */
+double orc_mi_filter_likelihood(const double *theta, const int *u, const int *v, int K, int L,
+                                int M, int nxn, int nyn, int nzn, long voxel, int x, int y, int z) {
+    const long KL = (long)K * L;
+    const int outside = x < 0 || y < 0 || z < 0 || x >= nxn || y >= nyn || z >= nzn;
+    const long node = outside ? 0 : ((long)x * nyn + y) * nzn + z;
+    double t = 1.0;
+    for (int m = 0; m < M; ++m) {
+        const int k = outside ? 0 : v[node + m];
+        t *= theta[m * KL + (long)k * L + u[voxel + m]];
+    }
+    return t;
+}
+
+/* The EM E-step (Registration.cpp:219-330, sample == false) with the MI filter likelihood:
+ * weights B(y_j - d_i) * prod_m theta[m][k_m(j)][u_m(i)], posterior mass added to every
+ * channel's histogram (MILikelihoodFilter.cpp:110-124).  hist [M][K][L]. */
+double orc_estep_filter(const double *d, const int *u, const int *v, const double *theta,
+                        int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L, int M,
+                        double *dream, double *hist, long long *degenerate) {
+    const int is2D = (nz == 1);
+    const int N = is2D ? 2 : 3;
+    const long V = (long)nx * ny * nz;
+    const long KL = (long)K * L;
+    const int T = orc_get_threads();
+    double *hist_t = (double *)calloc((size_t)T * M * KL, sizeof(double));
+    double mll = 0.0;
+    long long deg = 0;
+#pragma omp parallel num_threads(T) reduction(+ : mll, deg)
+    {
+#ifdef _OPENMP
+        const int tid = omp_get_thread_num();
+#else
+        const int tid = 0;
+#endif
+        double *h = hist_t + (size_t)tid * M * KL;
+#pragma omp for schedule(static)
+        for (long i = 0; i < V; ++i) {
+            const double *di = d + i * N;
+            double bx[4], by[4], bz[4] = {1.0, 1.0, 1.0, 1.0};
+            const int ix = spline_setup(di[0], bx), iy = spline_setup(di[1], by);
+            const int iz = is2D ? 0 : spline_setup(di[2], bz);
+            const int ZZ = is2D ? 1 : 4;
+            double w[64];
+            int nodes[64][3];
+            int n = 0;
+            double S = 0.0;
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b)
+                    for (int c = 0; c < ZZ; ++c) {
+                        const int X = ix + a - 1, Y = iy + b - 1, Z = is2D ? 0 : iz + c - 1;
+                        w[n] = bx[a] * by[b] * bz[c] *
+                               orc_mi_filter_likelihood(theta, u, v, K, L, M, nxn, nyn, nzn, i,
+                                                        X, Y, Z);
+                        nodes[n][0] = X; nodes[n][1] = Y; nodes[n][2] = Z;
+                        S += w[n];
+                        ++n;
+                    }
+            double *dr = dream + i * N;
+            if (!(S > 0.0)) {
+                dr[0] = ix; dr[1] = iy;
+                if (!is2D) dr[2] = iz;
+                deg += 1;
+                continue;
+            }
+            mll += -log(S);
+            double acc[3] = {0.0, 0.0, 0.0};
+            for (int j = 0; j < n; ++j) {
+                const double p = w[j] / S;
+                const int X = nodes[j][0], Y = nodes[j][1], Z = nodes[j][2];
+                const int outside = X < 0 || Y < 0 || Z < 0 || X >= nxn || Y >= nyn || Z >= nzn;
+                const long node = outside ? 0 : ((long)X * nyn + Y) * nzn + Z;
+                for (int m = 0; m < M; ++m) {
+                    const int k = outside ? 0 : v[node + m];
+                    h[m * KL + (long)k * L + u[i + m]] += p;
+                }
+                for (int q = 0; q < N; ++q) acc[q] += p * (double)nodes[j][q];
+            }
+            for (int q = 0; q < N; ++q) dr[q] = acc[q];
+        }
+    }
+    memset(hist, 0, sizeof(double) * M * KL);
+    for (int t = 0; t < T; ++t)
+        for (long q = 0; q < M * KL; ++q) hist[q] += hist_t[(size_t)t * M * KL + q];
+    free(hist_t);
+    if (degenerate) *degenerate = deg;
+    return mll;
+}
+
 /* Registration.cpp:278-307 (sample == true): categorical draw over the neighbourhood.
  * The draw is t = u * S and the first neighbour whose running sum reaches t is taken, which is
  * the reference's normalised-CDF test (random_number <= cumulative_probability). */

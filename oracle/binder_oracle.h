@@ -46,6 +46,11 @@ int  orc_get_spline_order(void);
 double orc_estep(const double *d, const int *u, const int *v, const double *theta,
                  int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L,
                  double *dream, double *hist, long long *degenerate);
+double orc_mi_filter_likelihood(const double *theta, const int *u, const int *v, int K, int L,
+                                int M, int nxn, int nyn, int nzn, long voxel, int x, int y, int z);
+double orc_estep_filter(const double *d, const int *u, const int *v, const double *theta,
+                        int nx, int ny, int nz, int nxn, int nyn, int nzn, int K, int L, int M,
+                        double *dream, double *hist, long long *degenerate);
 
 /* ---- sampled E-step (Gibbs block 1): Registration.cpp:278-307 (sample == true branch) ---------
  * Categorical draw over the 4x4x4 (4x4 in 2D) neighbours with the Philox stream

@@ -51,6 +51,10 @@ def _load_oracle():
     lib.orc_get_spline_order.restype = i
     lib.orc_estep.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [_dp, _dp, C.POINTER(ll)]
     lib.orc_estep.restype = d
+    lib.orc_mi_filter_likelihood.argtypes = [_dp, _ip, _ip] + [i] * 6 + [C.c_long, i, i, i]
+    lib.orc_mi_filter_likelihood.restype = d
+    lib.orc_estep_filter.argtypes = [_dp, _ip, _ip, _dp] + [i] * 9 + [_dp, _dp, C.POINTER(ll)]
+    lib.orc_estep_filter.restype = d
     lib.orc_estep_sample.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [u64, u32, u32, _dp, _dp]
     lib.orc_estep_sample.restype = d
     lib.orc_theta_map.argtypes = [_dp, i, i, d]
@@ -120,6 +124,10 @@ def ref_lib():
     r.ref_mi_update.restype = d
     r.ref_dirichlet_cost.argtypes = [d, _dp, i, i]
     r.ref_dirichlet_cost.restype = d
+    r.ref_mi_filter_likelihood.argtypes = [_dp, _ip, _ip] + [i] * 9 + [i, i, i, i]
+    r.ref_mi_filter_likelihood.restype = d
+    r.ref_mi_filter_update.argtypes = [d, _dp, _ip, _ip] + [i] * 9 + [i, _ip, _dp, _dp]
+    r.ref_mi_filter_update.restype = d
     return r
 
 
@@ -169,6 +177,25 @@ def estep(d, u, v, theta, vshape, nshape, K, L):
                           _c64(theta).ravel(), nx, ny, nz, *nshape, K, L, dream, hist,
                           C.byref(deg))
     return mll, dream, hist, deg.value
+
+
+def estep_filter(d, u, v, theta, vshape, nshape, K, L, M):
+    """EM E-step with the MI filter likelihood (M channels; u and v hold at least V + M - 1 and
+    Vn + M - 1 bins, read at [index + m]).  Returns (mll, dream[V*N], hist[M*K*L], degenerate)."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    dream = np.zeros(nx * ny * nz * N)
+    hist = np.zeros(M * K * L)
+    deg = C.c_longlong(0)
+    mll = lib().orc_estep_filter(_c64(d).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                                 _c64(theta).ravel(), nx, ny, nz, *nshape, K, L, M, dream, hist,
+                                 C.byref(deg))
+    return mll, dream, hist, deg.value
+
+
+def mi_filter_likelihood(theta, u, v, K, L, M, nshape, voxel, node):
+    return lib().orc_mi_filter_likelihood(_c64(theta).ravel(), _c32i(u).ravel(), _c32i(v).ravel(),
+                                          K, L, M, *nshape, int(voxel), *[int(t) for t in node])
 
 
 def estep_sample(d, u, v, theta, vshape, nshape, K, L, seed, sweep, chain=0):

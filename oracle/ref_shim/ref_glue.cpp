@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "MILikelihood.h"
+#include "MILikelihoodFilter.h"
 #include "NonLinearTransformation.h"
 #include "Spline.h"
 #include "topology_correction_2D.h"
@@ -90,6 +91,31 @@ double ref_dirichlet_cost(double alpha, const double *theta, int K, int L) {
     std::vector<int> nodes(K, 0), voxels(L, 0);
     MILikelihood mi(alpha, theta, 1, nodes.data(), voxels.data(), K, L, K, 1, 1, L, 1, 1);
     return mi.compute_cost();
+}
+
+// MILikelihoodFilter::compute_likelihood (BINDER/src/cpu/MILikelihoodFilter.cpp:53-68) for one
+// (voxel, node) pair; theta [M][K][L], bins read by the class at [index + m]
+double ref_mi_filter_likelihood(const double *theta, const int *voxels, const int *nodes, int K,
+                                int L, int M, int nxn, int nyn, int nzn, int nxv, int nyv, int nzv,
+                                int voxel, int x, int y, int z) {
+    MILikelihoodFilter f(2.0, theta, 1, nodes, voxels, K, L, M, nxn, nyn, nzn, nxv, nyv, nzv);
+    return f.compute_likelihood(voxel, x, y, z);
+}
+
+// accumulate_info over n (voxel, node, posterior) triples, then update_parameters and
+// compute_cost (MILikelihoodFilter.cpp:87-124 and :38-51); theta_out [M][K][L]
+double ref_mi_filter_update(double alpha, const double *theta, const int *voxels, const int *nodes,
+                            int K, int L, int M, int nxn, int nyn, int nzn, int nxv, int nyv,
+                            int nzv, int n, const int *vxyz, const double *post,
+                            double *theta_out) {
+    MILikelihoodFilter f(alpha, theta, 1, nodes, voxels, K, L, M, nxn, nyn, nzn, nxv, nyv, nzv);
+    for (int t = 0; t < n; ++t)
+        f.accumulate_info(0, vxyz[4 * t], vxyz[4 * t + 1], vxyz[4 * t + 2], vxyz[4 * t + 3],
+                          post[t]);
+    f.update_parameters();
+    const auto th = f.get_parameters();
+    std::memcpy(theta_out, th.data(), sizeof(double) * th.size());
+    return f.compute_cost();
 }
 
 }  // extern "C"

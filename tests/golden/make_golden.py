@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this directory from the reference's own CPU sources.
 
-The reference's Spline.cpp, MILikelihood.cpp, utils.cpp, DCT.cpp, FFT.cpp,
+The reference's Spline.cpp, MILikelihood.cpp, MILikelihoodFilter.cpp, utils.cpp, DCT.cpp, FFT.cpp,
 NonLinearTransformation.cpp, topology_correction_3D.cpp and topology_correction_2D.cpp are compiled unmodified by
 oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in
 oracle/ref_shim).  This script feeds them seeded inputs and stores inputs and outputs as small
@@ -168,6 +168,30 @@ def main():
         prep[f"{name}_plain"] = fns["bin_signal"](sig, nb)
     np.savez(os.path.join(HERE, "preprocess_ref.npz"), names=np.array([c[0] for c in cases]),
              **prep)
+
+    # MI filter likelihood (MILikelihoodFilter.cpp:38-124): M channels, bins read at [index + m],
+    # nodes outside the grid included; then accumulate_info / update_parameters / compute_cost
+    M, K, L = 3, 5, 4
+    nshape, vshape = (4, 3, 5), (6, 5, 4)
+    Vn, V = int(np.prod(nshape)), int(np.prod(vshape))
+    theta = rng.random((M, K, L)) + 0.05
+    theta /= theta.sum(-1, keepdims=True)
+    nodes = rng.integers(0, K, Vn + M - 1).astype(np.int32)
+    voxels = rng.integers(0, L, V + M - 1).astype(np.int32)
+    npairs = 200
+    pv = rng.integers(0, V, npairs)
+    pn = np.stack([rng.integers(-2, n + 2, npairs) for n in nshape], -1)
+    like = np.array([R.ref_mi_filter_likelihood(theta.ravel(), voxels, nodes, K, L, M, *nshape,
+                                                *vshape, int(v), *[int(t) for t in xyz])
+                     for v, xyz in zip(pv, pn)])
+    vxyz = np.ascontiguousarray(np.concatenate([pv[:, None], pn], 1).astype(np.int32))
+    post = rng.random(npairs) * 3.0
+    th_out = np.zeros(M * K * L)
+    fcost = R.ref_mi_filter_update(2.0, theta.ravel(), voxels, nodes, K, L, M, *nshape, *vshape,
+                                   npairs, vxyz.ravel(), post, th_out)
+    np.savez(os.path.join(HERE, "mi_filter_ref.npz"), M=M, K=K, L=L, nshape=nshape,
+             vshape=vshape, theta=theta, nodes=nodes, voxels=voxels, pairs=vxyz, likelihood=like,
+             posterior=post, alpha=2.0, theta_out=th_out.reshape(M, K, L), cost=fcost)
     print("golden fixtures written to", HERE)
 
 

@@ -129,6 +129,53 @@ def test_mi_update_matches_reference(oracle):
                                                                                rel=1e-13)
 
 
+def test_mi_filter_matches_reference(oracle):
+    """MILikelihoodFilter (compute_likelihood, accumulate_info, update_parameters, compute_cost)
+    against the reference's compiled class: bins of channel m read at [index + m]."""
+    g = golden("mi_filter_ref.npz")
+    M, K, L = int(g["M"]), int(g["K"]), int(g["L"])
+    nshape = tuple(int(t) for t in g["nshape"])
+    theta, nodes, voxels = g["theta"], g["nodes"], g["voxels"]
+    for (v, x, y, z), want in zip(g["pairs"], g["likelihood"]):
+        got = oracle.mi_filter_likelihood(theta, voxels, nodes, K, L, M, nshape, v, (x, y, z))
+        assert got == want                                                  # bit-exact
+    # the histogram of the same (voxel, node, posterior) triples, indexed as the likelihood reads
+    hist = np.zeros((M, K, L))
+    for (v, x, y, z), p in zip(g["pairs"], g["posterior"]):
+        inside = 0 <= x < nshape[0] and 0 <= y < nshape[1] and 0 <= z < nshape[2]
+        node = (x * nshape[1] + y) * nshape[2] + z
+        for m in range(M):
+            hist[m, nodes[node + m] if inside else 0, voxels[v + m]] += p
+    th = oracle.theta_map(hist, M * K, L, float(g["alpha"]))
+    np.testing.assert_allclose(th.reshape(M, K, L), g["theta_out"], rtol=1e-15, atol=0)
+    assert oracle.dirichlet_cost(th, M * K, L, float(g["alpha"])) == \
+        pytest.approx(float(g["cost"]), rel=1e-13)
+
+
+def test_mi_filter_estep_reduces_to_mi(oracle):
+    """One channel is the MI likelihood exactly; a second channel with a flat theta scales every
+    weight by 1/L, so posteriors and channel 0's histogram are unchanged and mll grows by V log L."""
+    rng = np.random.default_rng(11)
+    vshape, nshape, K, L = (7, 6, 5), (7, 6, 5), 6, 5
+    V = int(np.prod(vshape))
+    d = np.stack(np.indices(vshape), -1).reshape(-1, 3) + rng.normal(0, 0.7, (V, 3))
+    u = rng.integers(0, L, V + 1).astype(np.int32)
+    v = rng.integers(0, K, V + 1).astype(np.int32)
+    th = rng.random((K, L)) + 0.05
+    th /= th.sum(1, keepdims=True)
+    mll, dream, hist, deg = oracle.estep(d, u[:V], v[:V], th, vshape, nshape, K, L)
+    mll1, dream1, hist1, deg1 = oracle.estep_filter(d, u[:V], v[:V], th, vshape, nshape, K, L, 1)
+    assert mll1 == mll and deg1 == deg
+    np.testing.assert_array_equal(dream1, dream)
+    np.testing.assert_array_equal(hist1, hist)
+    th2 = np.stack([th, np.full((K, L), 1.0 / L)])
+    mll2, dream2, hist2, _ = oracle.estep_filter(d, u, v, th2, vshape, nshape, K, L, 2)
+    assert mll2 == pytest.approx(mll + V * np.log(L), rel=1e-12)
+    np.testing.assert_allclose(dream2, dream, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(hist2[:K * L], hist, rtol=1e-12, atol=1e-12)
+    assert hist2[K * L:].sum() == pytest.approx(hist.sum(), rel=1e-12)
+
+
 def _prior_covariance(shape, gamma, sigma, order):
     """sigma^2 (I + gamma sigma^2 Gamma)^-1 with Neumann finite differences
     (tests/gpu/test_sampling_DCT_3D.py), in Fortran voxel order."""
