@@ -114,6 +114,7 @@ class Registration:
             _i32(binned_nodes, Vn, "binned_nodes"), _i32(binned_voxels, self._V, "binned_voxels")))
         self._K, self._L, self._M = K, L, 1
         self._ssd = False
+        self._ssdf = (0, 0)
 
     def setMILikelihoodFilter(self, alpha, theta, threads, binned_nodes, binned_voxels, K, L, M):
         """``setMILikelihoodFilter`` of the CPU module (cpu/bindings.cpp:90-115): M channels,
@@ -132,6 +133,32 @@ class Registration:
             K, L, M))
         self._K, self._L, self._M = K, L, M
         self._ssd = False
+        self._ssdf = (0, 0)
+
+    def setSSDLikelihoodFilter(self, coeff, threads, sigma, features_nodes, features_voxels,
+                               reg_across_features, alpha_0, beta_0, M, F):
+        """``setSSDLikelihoodFilter`` of the CPU module (cpu/bindings.cpp:154-189): M fixed-image
+        channels ([V][M] features), F moving-image features ([Vn][F], or [Vn][M] with
+        reg_across_features), coeff [M][F], sigma [M].  EM only."""
+        M, F = int(M), int(F)
+        Fn = M if reg_across_features else F
+        Vn = int(np.prod(self._nshape))
+        check(lib().binder_registration_set_ssd_likelihood_filter(
+            self._h, _f64(coeff, M * F, "coeff"), int(threads), _f64(sigma, M, "sigma"),
+            _f64(features_nodes, Vn * Fn, "features_nodes"),
+            _f64(features_voxels, self._V * M, "features_voxels"), int(reg_across_features),
+            float(alpha_0), float(beta_0), M, F))
+        self._K, self._L, self._M = F, M, 1
+        self._ssd, self._ssdf = False, (M, F)
+
+    def ssd_filter_parameters(self):
+        """(coeff [M][F], sigma [M]) of the SSD filter likelihood."""
+        M, F = getattr(self, "_ssdf", (0, 0))
+        if not M:
+            raise BinderError(4, "setSSDLikelihoodFilter has not been called")
+        c, s = np.zeros(M * F), np.zeros(M)
+        check(lib().binder_registration_get_ssd_filter_parameters(self._h, c, s))
+        return c.reshape(M, F), s
 
     def setSSDLikelihood(self, bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
                          binned_voxels, alpha_0, beta_0):
@@ -145,6 +172,7 @@ class Registration:
         self._K = self._L = bins
         self._M = 1
         self._ssd = True
+        self._ssdf = (0, 0)
 
     def ssd_parameters(self):
         """(sigma^2, shift, scale) of the SSD likelihood (no reference counterpart)."""

@@ -22,6 +22,7 @@ EXPORTS = [
     "binder_registration_create", "binder_registration_destroy",
     "binder_registration_set_mi_likelihood", "binder_registration_set_nonlinear_transformation",
     "binder_registration_set_mi_likelihood_filter",
+    "binder_registration_set_ssd_likelihood_filter", "binder_registration_get_ssd_filter_parameters",
     "binder_registration_em", "binder_registration_sampler",
     "binder_registration_get_final_locations", "binder_registration_get_dream_locations",
     "binder_registration_set_dream_locations", "binder_registration_get_likelihood_parameters",
@@ -72,6 +73,9 @@ def _declare(lib):
         "binder_registration_destroy": [_P],
         "binder_registration_set_mi_likelihood": [_P, _d, _f32, _i, _i, _i, _i32, _i32],
         "binder_registration_set_mi_likelihood_filter": [_P, _d, _f32, _i, _i32, _i32, _i, _i, _i],
+        "binder_registration_set_ssd_likelihood_filter": [_P, _f64, _i, _f64, _f64, _f64, _i, _d,
+                                                          _d, _i, _i],
+        "binder_registration_get_ssd_filter_parameters": [_P, _f64, _f64],
         "binder_registration_set_nonlinear_transformation": [_P] + [_d] * 9 + [_f32],
         "binder_registration_em": [_P, _i, _d, _i, _i, C.POINTER(_i)],
         "binder_registration_sampler": [_P, _u64, _i, _i, _i, _i, _i, _i, _i, _f64, _f64],

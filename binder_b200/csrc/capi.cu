@@ -126,6 +126,32 @@ int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int
     });
 }
 
+int binder_registration_set_ssd_likelihood_filter(binder_registration *h, const double *coeff,
+                                                  int threads, const double *sigma,
+                                                  const double *features_nodes,
+                                                  const double *features_voxels,
+                                                  int reg_across_features, double alpha_0,
+                                                  double beta_0, int M, int F) {
+    (void)threads;
+    return guard([&] {
+        NEED(h);
+        NEED(coeff);
+        NEED(sigma);
+        NEED(features_nodes);
+        NEED(features_voxels);
+        h->impl->set_ssd_filter_likelihood(coeff, sigma, features_nodes, features_voxels,
+                                           reg_across_features, alpha_0, beta_0, M, F);
+    });
+}
+
+int binder_registration_get_ssd_filter_parameters(const binder_registration *h, double *coeff,
+                                                  double *sigma) {
+    return guard([&] {
+        NEED(h);
+        h->impl->get_ssd_filter_parameters(coeff, sigma);
+    });
+}
+
 int binder_registration_get_ssd_parameters(const binder_registration *h, double out[3]) {
     return guard([&] {
         NEED(h);

@@ -320,6 +320,7 @@ Registration::~Registration() {
     dfree(hcnt_, s); dfree(u_, s); dfree(vpad_, s); dfree(mean_, s); dfree(m2_, s);
     dfree(stats_, s); dfree(st_, s); dfree(d0_, s); dfree(theta0_, s);
     dfree(ssd_, s); dfree(ssd0_, s); dfree(colmax_, s); dfree(colmax0_, s);
+    dfree(fx_, s); dfree(fn_, s); dfree(fst_, s); dfree(fst0_, s); dfree(fstats_, s);
     delete topo_;
     mstep_.release(s);
     cudaStreamSynchronize(s);  // the frees complete, so the next object can reuse the memory
@@ -464,6 +465,72 @@ void Registration::set_ssd_likelihood(int bins, double sigma2, int shift_scale, 
     egrid_e_ = estep_grid(false, bins, bins, V_, N_, true);
 }
 
+// The SSD filter likelihood (SSDLikelihoodFilter.cpp): continuous features, EM in log space.
+// The features go to the device as FP64 SoA; the parameters stay FP64 in an SsdfState.
+void Registration::set_ssd_filter_likelihood(const double *coeff, const double *sigma,
+                                             const double *features_nodes,
+                                             const double *features_voxels,
+                                             int reg_across_features, double alpha0,
+                                             double beta0, int M, int F) {
+    BINDER_CHECK(M >= 1 && M <= kSsdfMax && F >= 1 && F <= kSsdfMax,
+                 "the SSD filter likelihood needs 1 <= M, F <= 8");
+    BINDER_CHECK(alpha0 > 0.0 && beta0 > 0.0, "alpha_0 and beta_0 must be positive");
+    for (int m = 0; m < M; ++m)
+        BINDER_CHECK(sigma[m] > 0.0 && std::isfinite(sigma[m]), "sigma must be positive");
+    const int Fn = reg_across_features ? M : F;
+    have_mi_ = false;
+    BINDER_CUDA(cudaStreamSynchronize(stream_));  // buffers below may be in use
+    em_graph_.clear();
+    const cudaStream_t s = own_stream_;
+    dfree(fx_, s); dfree(fn_, s); dfree(fst_, s); dfree(fst0_, s); dfree(fstats_, s);
+    fx_ = dalloc<double>((size_t)V_ * M, s);
+    fn_ = dalloc<double>((size_t)Vn_ * Fn, s);
+    fst_ = dalloc<SsdfState>(1, s);
+    fst0_ = dalloc<SsdfState>(1, s);
+    fstats_ = dalloc<double>(kSsdfStats, s);
+    const long nmax = (long)V_ * M > (long)Vn_ * Fn ? (long)V_ * M : (long)Vn_ * Fn;
+    double *stage = dalloc<double>((size_t)nmax, s);
+    BINDER_CUDA(cudaMemcpyAsync(stage, features_voxels, sizeof(double) * V_ * M,
+                                cudaMemcpyDefault, s));
+    launch_features_to_soa(stage, V_, M, fx_, s);
+    BINDER_CUDA(cudaMemcpyAsync(stage, features_nodes, sizeof(double) * Vn_ * Fn,
+                                cudaMemcpyDefault, s));
+    launch_features_to_soa(stage, Vn_, Fn, fn_, s);
+    dfree(stage, s);
+    SsdfState h{};
+    h.M = M;
+    h.F = F;
+    h.Fn = Fn;
+    h.rfa = reg_across_features ? 1 : 0;
+    h.alpha0 = alpha0;
+    h.beta0 = beta0;
+    for (int q = 0; q < M * F; ++q) h.coeff[q] = coeff[q];
+    for (int m = 0; m < M; ++m) h.sigma[m] = sigma[m];
+    ssdf_refresh_host(h);
+    BINDER_CUDA(cudaMemcpyAsync(fst_, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(fst0_, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemsetAsync(fstats_, 0, sizeof(double) * kSsdfStats, s));
+    BINDER_CUDA(cudaStreamSynchronize(s));  // `h` goes out of scope
+    fM_ = M;
+    fF_ = F;
+    fFn_ = Fn;
+    lk_ = 3;
+    egrid_e_ = estep_ssdf_grid(M, Fn, V_, N_);
+    egrid_s_ = 0;
+    have_mi_ = true;
+}
+
+void Registration::get_ssd_filter_parameters(double *coeff, double *sigma) const {
+    if (lk_ != 3) throw Error(kNotReady, "setSSDLikelihoodFilter has not been called");
+    SsdfState h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, fst_, sizeof h, cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    if (coeff)
+        for (int q = 0; q < h.M * h.F; ++q) coeff[q] = h.coeff[q];
+    if (sigma)
+        for (int m = 0; m < h.M; ++m) sigma[m] = h.sigma[m];
+}
+
 void Registration::get_ssd_parameters(double out[3]) const {
     if (lk_ != 1) throw Error(kNotReady, "setSSDLikelihood has not been called");
     SsdState h{};
@@ -532,7 +599,8 @@ EStepArgs Registration::estep_args(const int *skip) const {
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
     e.seed = seed_; e.chain = chain_; e.order = order_;
     e.logt = lk_ == 1; e.colmax = colmax_;
-    e.M = M_; e.filter = lk_ == 2; e.uch = 1; e.vch = vch_;
+    e.M = lk_ == 3 ? fM_ : M_; e.filter = lk_ == 2; e.uch = 1; e.vch = vch_;
+    e.ssdf = lk_ == 3; e.Fn = fFn_; e.fx = fx_; e.fn = fn_; e.fstate = fst_; e.fstats = fstats_;
     return e;
 }
 
@@ -540,6 +608,8 @@ void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
     launch_estep(estep_args(&st_->done), false, egrid_e_, stream_);
     if (lk_ == 1)
         launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, stream_);
+    else if (lk_ == 3)
+        launch_ssdf_update(fst_, fstats_, update, st_, stream_);
     else
         launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, stream_);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
@@ -633,9 +703,9 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     }
     if (lk_ == 1)
         throw Error(kUnsupported, "the sampler with the SSD likelihood is not built (EM only)");
-    if (lk_ == 2)
+    if (lk_ == 2 || lk_ == 3)
         throw Error(kUnsupported,
-                    "the sampler with the MI filter likelihood is not built (EM only)");
+                    "the sampler with a filter (feature) likelihood is not built (EM only)");
     if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
     BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
     BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
@@ -720,6 +790,8 @@ double Registration::profile_stage(int stage, int n) {
                            rho_[0] * rho_[1] * rho_[2], eta2, nullptr, stream_);
         else if (lk_ == 1)
             launch_ssd_update(theta_, colmax_, hist_, K_, L_, 0, ssd_, st_, stream_);
+        else if (lk_ == 3)
+            launch_ssdf_update(fst_, fstats_, 0, st_, stream_);
         else launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, 1, st_, stream_);
     };
     one();  // warm-up
@@ -762,7 +834,11 @@ void PriorTransform::set_precision(int p) {
 
 void Registration::reset() {
     BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * N_, cudaMemcpyDeviceToDevice, stream_));
-    if (have_mi_) {
+    if (lk_ == 3) {
+        BINDER_CUDA(cudaMemcpyAsync(fst_, fst0_, sizeof(SsdfState), cudaMemcpyDeviceToDevice,
+                                    stream_));
+        BINDER_CUDA(cudaMemsetAsync(fstats_, 0, sizeof(double) * kSsdfStats, stream_));
+    } else if (have_mi_) {
         BINDER_CUDA(cudaMemcpyAsync(theta_, theta0_, sizeof(float) * M_ * K_ * L_,
                                     cudaMemcpyDeviceToDevice, stream_));
         BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * M_ * K_ * L_, stream_));
@@ -822,6 +898,12 @@ void Registration::set_dream_locations(const float *in) {
 
 void Registration::get_likelihood_parameters(float *out) const {
     if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    if (lk_ == 3) {  // SSDLikelihoodFilter::get_parameters (:457-466): the coefficients
+        std::vector<double> c((size_t)fM_ * fF_);
+        get_ssd_filter_parameters(c.data(), nullptr);
+        for (size_t q = 0; q < c.size(); ++q) out[q] = (float)c[q];
+        return;
+    }
     if (lk_ == 1) {  // SSDLikelihood::get_parameters (SSDLikelihood.cpp:328-334): scale, shift
         double p[3];
         get_ssd_parameters(p);

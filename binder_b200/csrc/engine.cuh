@@ -63,6 +63,19 @@ class Registration {
 
     void set_mi_likelihood(double alpha, const float *theta, int K, int L, const int *binned_nodes,
                            const int *binned_voxels);
+    // the SSD filter likelihood (BINDER/src/cpu/Registration.cpp:481-487): coeff [M][F] and sigma
+    // [M] host memory, features_nodes [Vn][F] ([Vn][M] with reg_across_features) and
+    // features_voxels [V][M] host or device memory; EM only
+    void set_ssd_filter_likelihood(const double *coeff, const double *sigma,
+                                   const double *features_nodes, const double *features_voxels,
+                                   int reg_across_features, double alpha0, double beta0, int M,
+                                   int F);
+    // coeff [M][F], sigma [M]
+    void get_ssd_filter_parameters(double *coeff, double *sigma) const;
+    int ssd_filter_channels(int *F) const {
+        if (F) *F = fF_;
+        return fM_;
+    }
     // the MI filter likelihood (BINDER/src/cpu/Registration.cpp:466-470): M channels, theta
     // [M][K][L], bins of channel m read at [index + m]; EM only
     void set_mi_filter_likelihood(double alpha, const float *theta, int K, int L, int M,
@@ -158,7 +171,11 @@ class Registration {
     int iters_done_ = 0;
     int order_ = 3;  // B-spline order of the E-step
     int lk_ = 0;     // likelihood: 0 MI (theta_ is theta), 1 SSD (theta_ is its log2 table),
-                     // 2 MI filter (theta_ is [M][K][L])
+                     // 2 MI filter (theta_ is [M][K][L]), 3 SSD filter (the f* buffers)
+    double *fx_ = nullptr, *fn_ = nullptr;          // SSD filter: voxel / node features (SoA)
+    SsdfState *fst_ = nullptr, *fst0_ = nullptr;    // SSD filter parameters, and as set
+    double *fstats_ = nullptr;                      // SSD filter E-step statistics
+    int fM_ = 0, fF_ = 0, fFn_ = 0;
     SsdState *ssd_ = nullptr, *ssd0_ = nullptr;  // SSD parameters, and as set
     float *colmax_ = nullptr, *colmax0_ = nullptr;  // SSD table column maxima, and as set
     double last_ms_ = 0.0;

@@ -488,6 +488,273 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepA
     if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
 }
 
+// ---- the SSD filter likelihood (BINDER/src/cpu/SSDLikelihoodFilter.cpp) -------------------
+constexpr int kSsdfThreads = 128;
+
+// number of per-thread statistics: packed A (Fn (Fn + 1) / 2), b (M Fn), S2 (M), eff
+__host__ __device__ constexpr int ssdf_nstats(int M, int Fn) {
+    return Fn * (Fn + 1) / 2 + M * Fn + M + 1;
+}
+
+// Log-space EM E-step (Registration.cpp:331-470) with compute_log_likelihood (:123-158) written
+// as sum_m -(x_m - t_m(j))^2 / (2 sigma_m) + log_constant_m, where t_m(j) = sum_f cf[m][f] n_f(j)
+// is channel m's prediction from the node's features (0 outside the grid).  accumulate_info's
+// per-node sums (:160-198) are only ever used through A = sum p n n^T, b_m = sum p x_m n,
+// S2_m = sum p x_m^2 and eff = sum p (update_coefficients :205-290 and update_sigma :292-346,
+// whose sigma numerator is S2_m - 2 c_m . b_m + c_m^T A c_m for the new coefficients c_m), so
+// each voxel adds its posterior moments of n to per-thread FP64 columns in shared memory, reduced
+// once per CTA.  Two passes over the neighbours: the largest term, then exp(term - max).
+template <int DIM, int FM>
+__global__ void __launch_bounds__(kSsdfThreads) estep_ssdf_kernel(const EStepArgs a) {
+    constexpr int Q = DIM == 3 ? 4 : 1;
+    constexpr int NA = FM * (FM + 1) / 2;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) double cols[];  // [nstats][kSsdfThreads]
+    __shared__ double cf[kSsdfMax * kSsdfMax], hh[kSsdfMax];
+    __shared__ double red[32];
+    const SsdfState *ps = a.fstate;
+    const int M = ps->M, Fn = ps->Fn;
+    const int nst = ssdf_nstats(M, Fn);
+    for (int q = threadIdx.x; q < kSsdfMax * kSsdfMax; q += blockDim.x) cf[q] = ps->cf[q];
+    if (threadIdx.x < kSsdfMax) hh[threadIdx.x] = ps->h[threadIdx.x];
+    const double lc = ps->lc;
+    double *my = cols + threadIdx.x;  // my[s * kSsdfThreads]
+    for (int s = 0; s < nst; ++s) my[s * kSsdfThreads] = 0.0;
+    __syncthreads();
+
+    const long Vn = (long)a.nxn * a.nyn * a.nzn;
+    double mll = 0.0;
+    unsigned deg = 0;
+    const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+        VoxelPos<DIM> vp;
+        if (!vp.load(a, i, V, ny, nz)) {
+            vp.store_r(a, i, V, vp.px, vp.py, vp.pz);
+            ++deg;
+            continue;
+        }
+        float bx[4], by[4] = {1.f, 1.f, 1.f, 1.f}, bz[4];
+        const int ix = spline_setup(vp.px, a.order, bx);
+        const int iy = DIM == 3 ? spline_setup(vp.py, a.order, by) : 0;
+        const int iz = spline_setup(vp.pz, a.order, bz);
+        float lx[4], ly[4], lz[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            lx[t] = logf(bx[t]);  // -inf for a zero tap, whose term then vanishes
+            ly[t] = DIM == 3 ? logf(by[t]) : 0.0f;
+            lz[t] = logf(bz[t]);
+        }
+        double xv[kSsdfMax];
+#pragma unroll
+        for (int m = 0; m < kSsdfMax; ++m) xv[m] = m < M ? a.fx[(long)m * V + i] : 0.0;
+        // the log term of neighbour (p, q, c) and the node's features, in FP64: with poor
+        // coefficients the residual sums reach the hundreds, where FP32 would shift posteriors
+        auto term_of = [&](int p, int q, int c, double (&n)[FM]) -> double {
+            const int X = ix - 1 + p, Y = DIM == 3 ? iy - 1 + q : 0, Z = iz - 1 + c;
+            const bool in = X >= 0 && Y >= 0 && Z >= 0 && X < a.nxn && Y < a.nyn && Z < a.nzn;
+            const long j = in ? ((long)X * a.nyn + Y) * a.nzn + Z : 0;
+#pragma unroll
+            for (int f = 0; f < FM; ++f) n[f] = (in && f < Fn) ? __ldg(a.fn + f * Vn + j) : 0.0;
+            double qs = 0.0;
+#pragma unroll
+            for (int m = 0; m < kSsdfMax; ++m) {
+                if (m >= M) break;
+                double t = 0.0;
+#pragma unroll
+                for (int f = 0; f < FM; ++f)
+                    if (f < Fn) t = fma(cf[m * Fn + f], n[f], t);
+                const double r = xv[m] - t;
+                qs = fma(r * r, hh[m], qs);
+            }
+            return (double)((lx[p] + ly[q]) + lz[c]) - qs;
+        };
+        double mx = -INFINITY;
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p)
+#pragma unroll 1
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double n[FM];
+                    mx = fmax(mx, term_of(p, q, c, n));
+                }
+        float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f, Bn[FM], A[NA];
+#pragma unroll
+        for (int f = 0; f < FM; ++f) Bn[f] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NA; ++k) A[k] = 0.0f;
+#pragma unroll 1
+        for (int p = 0; p < 4; ++p)
+#pragma unroll 1
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    double nd[FM];
+                    const float e = expf((float)(term_of(p, q, c, nd) - mx));
+                    float n[FM];
+#pragma unroll
+                    for (int f = 0; f < FM; ++f) n[f] = (float)nd[f];
+                    S += e;
+                    Sx = fmaf((float)(p - 1), e, Sx);
+                    if (Q == 4) Sy = fmaf((float)(q - 1), e, Sy);
+                    Sz = fmaf((float)(c - 1), e, Sz);
+                    int k = 0;
+#pragma unroll
+                    for (int f = 0; f < FM; ++f) {
+                        Bn[f] = fmaf(e, n[f], Bn[f]);
+                        const float en = e * n[f];
+#pragma unroll
+                        for (int g = f; g < FM; ++g, ++k) A[k] = fmaf(en, n[g], A[k]);
+                    }
+                }
+        const float inv = 1.0f / S;
+        mll -= mx + log((double)S) + lc;
+        vp.store_r(a, i, V, (float)ix + Sx * inv, (float)iy + Sy * inv, (float)iz + Sz * inv);
+        // this voxel's statistics: A (packed f <= g), b [m][f], S2 [m], eff
+        int s = 0;
+#pragma unroll
+        for (int f = 0; f < FM; ++f)
+#pragma unroll
+            for (int g = f; g < FM; ++g)
+                if (g < Fn) my[(s++) * kSsdfThreads] += (double)A[f * FM - f * (f - 1) / 2 + (g - f)] * inv;
+#pragma unroll
+        for (int m = 0; m < kSsdfMax; ++m) {
+            if (m >= M) break;
+#pragma unroll
+            for (int f = 0; f < FM; ++f)
+                if (f < Fn) my[(s++) * kSsdfThreads] += xv[m] * ((double)Bn[f] * inv);
+        }
+#pragma unroll
+        for (int m = 0; m < kSsdfMax; ++m) {
+            if (m >= M) break;
+            my[(s++) * kSsdfThreads] += xv[m] * xv[m];
+        }
+        my[s * kSsdfThreads] += 1.0;
+    }
+    __syncthreads();
+    // column s: thread s sums it and adds it at its place in the full layout of fstats
+    if ((int)threadIdx.x < nst) {
+        const int s = threadIdx.x;
+        double v = 0.0;
+        for (int t = 0; t < kSsdfThreads; ++t) v += cols[s * kSsdfThreads + t];
+        const int na = Fn * (Fn + 1) / 2;
+        if (s < na) {
+            int f = 0, r = s;
+            while (r >= Fn - f) r -= Fn - f++;
+            const int g = f + r;
+            atomicAdd(&a.fstats[kSsdfA + f * Fn + g], v);
+            if (g != f) atomicAdd(&a.fstats[kSsdfA + g * Fn + f], v);
+        } else if (s < na + M * Fn) {
+            atomicAdd(&a.fstats[kSsdfB + (s - na)], v);
+        } else if (s < na + M * Fn + M) {
+            atomicAdd(&a.fstats[kSsdfS2 + (s - na - M * Fn)], v);
+        } else {
+            atomicAdd(&a.fstats[kSsdfEff], v);
+        }
+    }
+    const double ms = block_sum(mll, red);
+    if (threadIdx.x == 0) atomicAdd(&a.st->mll, ms);
+    const double dg = block_sum((double)deg, red);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+}
+
+__host__ __device__ void ssdf_refresh(SsdfState &p) {
+    const double pi = 3.14159265358979323846;
+    double lc = 0.0;
+    for (int m = 0; m < p.M; ++m) {
+        for (int f = 0; f < p.Fn; ++f)
+            p.cf[m * p.Fn + f] = p.rfa ? (m == f ? 1.0 : 0.0) : p.coeff[m * p.F + f];
+        p.h[m] = 0.5 / p.sigma[m];
+        lc += -0.5 * log(2.0 * pi * p.sigma[m]);
+    }
+    p.lc = lc;
+}
+
+// SSDLikelihoodFilter::solve_linear_system (:348-389): Gaussian elimination with partial pivoting
+__device__ void ssdf_solve(int n, const double *A, const double *b, double *x) {
+    double aug[kSsdfMax][kSsdfMax + 1];
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) aug[i][j] = A[i * n + j];
+        aug[i][n] = b[i];
+    }
+    for (int i = 0; i < n; ++i) {
+        int piv = i;
+        for (int j = i + 1; j < n; ++j)
+            if (fabs(aug[j][i]) > fabs(aug[piv][i])) piv = j;
+        if (piv != i)
+            for (int k = 0; k <= n; ++k) {
+                const double t = aug[i][k];
+                aug[i][k] = aug[piv][k];
+                aug[piv][k] = t;
+            }
+        for (int j = i + 1; j < n; ++j) {
+            const double f = aug[j][i] / aug[i][i];
+            for (int k = i; k <= n; ++k) aug[j][k] -= f * aug[i][k];
+        }
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int j = i + 1; j < n; ++j) s += aug[i][j] * x[j];
+        x[i] = (aug[i][n] - s) / aug[i][i];
+    }
+}
+
+// update_parameters (:200-346) from the statistics, compute_cost (:72-89); one thread
+__global__ void ssdf_update_kernel(SsdfState *ps, double *stats, int update, DevState *st) {
+    if (st && st->done) return;
+    if (threadIdx.x == 0) {
+        SsdfState &p = *ps;
+        const int M = p.M, Fn = p.Fn;
+        if (update) {
+            const double *A = stats + kSsdfA, *b = stats + kSsdfB;
+            double c[kSsdfMax * kSsdfMax];
+            for (int m = 0; m < M; ++m) {
+                if (p.rfa) {
+                    for (int f = 0; f < Fn; ++f) c[m * Fn + f] = m == f ? 1.0 : 0.0;
+                } else {
+                    ssdf_solve(Fn, A, b + m * Fn, c + m * Fn);
+                    for (int f = 0; f < Fn; ++f) p.coeff[m * p.F + f] = c[m * Fn + f];
+                }
+            }
+            const double den = stats[kSsdfEff] + 2.0 * p.alpha0;
+            for (int m = 0; m < M; ++m) {
+                const double *cm = c + m * Fn;
+                double cb = 0.0, cac = 0.0;
+                for (int f = 0; f < Fn; ++f) {
+                    cb += cm[f] * b[m * Fn + f];
+                    double af = 0.0;
+                    for (int g = 0; g < Fn; ++g) af += A[f * Fn + g] * cm[g];
+                    cac += cm[f] * af;
+                }
+                const double num =
+                    stats[kSsdfS2 + m] - 2.0 * cb + cac + 2.0 * p.alpha0 * p.beta0;
+                p.sigma[m] = num / den;
+                if (!isfinite(p.sigma[m]) || !(p.sigma[m] > 0.0) || !isfinite(p.coeff[0]))
+                    atomicOr(&st->flags, (unsigned)kFlagNonFinite);
+            }
+            ssdf_refresh(p);
+        }
+        const double a = p.alpha0, bb = p.alpha0 * p.beta0;
+        double cost = 0.0;
+        for (int m = 0; m < M; ++m) {
+            const double x = p.sigma[m];
+            cost += -(a * log(bb) - lgamma(a) + (-a - 1.0) * log(x) - bb / x);
+        }
+        if (st) st->lp_lik = cost;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kSsdfStats; q += blockDim.x) stats[q] = 0.0;
+}
+
+__global__ void features_to_soa_kernel(const double *in, long n, int C, double *out) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n * C;
+         q += (long)gridDim.x * blockDim.x) {
+        const long i = q / C;
+        const int c = (int)(q - i * C);
+        out[(long)c * n + i] = in[q];
+    }
+}
+
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
 // for the Gibbs draw and for EM with K > 64.
@@ -833,9 +1100,30 @@ size_t filter_smem(int K, int L, int M) {
     return (size_t)M * (L * theta_pitch(K) + K * theta_pitch(L)) * sizeof(float);
 }
 
+size_t ssdf_smem(int M, int Fn) { return (size_t)ssdf_nstats(M, Fn) * kSsdfThreads * 8; }
+
+template <int DIM>
+const void *ssdf_fn(int Fn) {
+    if (Fn <= 2) return (const void *)estep_ssdf_kernel<DIM, 2>;
+    if (Fn <= 4) return (const void *)estep_ssdf_kernel<DIM, 4>;
+    return (const void *)estep_ssdf_kernel<DIM, 8>;
+}
+
+template <int DIM>
+void launch_ssdf_dim(const EStepArgs &a, int grid, size_t smem, cudaStream_t s) {
+    if (a.Fn <= 2)
+        count_launch(), estep_ssdf_kernel<DIM, 2><<<grid, kSsdfThreads, smem, s>>>(a);
+    else if (a.Fn <= 4)
+        count_launch(), estep_ssdf_kernel<DIM, 4><<<grid, kSsdfThreads, smem, s>>>(a);
+    else
+        count_launch(), estep_ssdf_kernel<DIM, 8><<<grid, kSsdfThreads, smem, s>>>(a);
+}
+
 template <int DIM>
 void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
-    if (a.filter)
+    if (a.ssdf)
+        launch_ssdf_dim<DIM>(a, grid, smem, s);
+    else if (a.filter)
         count_launch(), estep_filter_kernel<DIM><<<grid, kEThreads, smem, s>>>(a);
     else if (a.logt)
         count_launch(), estep_em_fast_kernel<kFastThreads, DIM, true>
@@ -896,6 +1184,45 @@ int estep_filter_grid(int K, int L, int M, long V, int dim) {
     return (int)g;
 }
 
+int estep_ssdf_grid(int M, int Fn, long V, int dim) {
+    BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
+    BINDER_CHECK(M >= 1 && M <= kSsdfMax && Fn >= 1 && Fn <= kSsdfMax,
+                 "the SSD filter likelihood needs 1 <= M, F <= 8");
+    int dev = 0, sms = 148, per_sm = 1;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem = ssdf_smem(M, Fn);
+    // both dimensions' kernels for this feature count
+    const void *fns[2] = {ssdf_fn<2>(Fn), ssdf_fn<3>(Fn)};
+    for (const void *f : fns) {
+        BINDER_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+        BINDER_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
+    }
+    BINDER_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[dim - 2], kSsdfThreads,
+                                                              smem));
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const long need = (V + kSsdfThreads - 1) / kSsdfThreads;
+    long g = (long)sms * per_sm;
+    if (need < g) g = need < 1 ? 1 : need;
+    return (int)g;
+}
+
+void ssdf_refresh_host(SsdfState &p) { ssdf_refresh(p); }
+
+void launch_ssdf_update(SsdfState *p, double *stats, int update, DevState *st, cudaStream_t s) {
+    count_launch(), ssdf_update_kernel<<<1, 160, 0, s>>>(p, stats, update, st);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_features_to_soa(const double *in, long n, int C, double *out, cudaStream_t s) {
+    long b = (n * C + 255) / 256;
+    b = b < 1 ? 1 : (b > 148L * 16 ? 148L * 16 : b);
+    count_launch(), features_to_soa_kernel<<<(int)b, 256, 0, s>>>(in, n, C, out);
+    BINDER_CUDA(cudaGetLastError());
+}
+
 void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) {
     BINDER_CHECK(!args.logt || (!sample && args.K <= kSmallK && args.colmax),
                  "the log-space E-step runs EM only, with at most 64 bins");
@@ -903,8 +1230,12 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) 
                                   args.M <= kMaxChannels &&
                                   (long)args.M * args.K * args.L <= kFilterMaxCells),
                  "the MI filter E-step runs EM only, with 1 <= M <= 8 and M * K * L <= 24576");
-    const size_t smem = args.filter ? filter_smem(args.K, args.L, args.M)
-                                    : estep_smem(sample, args.K, args.L, args.logt != 0);
+    BINDER_CHECK(!args.ssdf || (!sample && args.fstate && args.fstats && args.M >= 1 &&
+                                args.M <= kSsdfMax && args.Fn >= 1 && args.Fn <= kSsdfMax),
+                 "the SSD filter E-step runs EM only, with 1 <= M, F <= 8");
+    const size_t smem = args.ssdf     ? ssdf_smem(args.M, args.Fn)
+                        : args.filter ? filter_smem(args.K, args.L, args.M)
+                                      : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
     // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
     // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a

@@ -7,6 +7,8 @@ namespace binder {
 
 // A 2D image nx x ny is passed as the volume nx x 1 x ny (ny, nyn = 1): its y axis is the packed
 // (z) axis of the bin volume and positions have N = dim = 2 components (x, y).
+struct SsdfState;
+
 struct EStepArgs {
     const float *d;   // positions, SoA [dim][V] (node-grid coordinates)
     float *r;         // out: dream location minus voxel position, SoA [dim][V]
@@ -34,6 +36,14 @@ struct EStepArgs {
     int M;
     int filter;
     long uch, vch;
+    // the SSD filter likelihood: voxel features [M][V] and node features [Fn][Vn] (FP64 SoA,
+    // node index in the E-step's view), its state and the E-step's statistics
+    int ssdf;
+    int Fn;
+    const double *fx;
+    const double *fn;
+    SsdfState *fstate;
+    double *fstats;
     uint64_t seed;
     uint32_t chain;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
@@ -49,6 +59,31 @@ constexpr int kLogMaxBins = 64;
 constexpr int kMaxChannels = 8;
 constexpr long kFilterMaxCells = 24576;
 int estep_filter_grid(int K, int L, int M, long V, int dim);
+
+// State of the SSD filter likelihood (BINDER/src/cpu/SSDLikelihoodFilter.cpp): M fixed-image
+// channels, F moving-image features (Fn = F, or M with reg_across_features, whose prediction of
+// channel m at a node is its feature m: coefficients = identity), coeff [M][F], sigma [M], the
+// inverse-gamma prior, and what the E-step reads.
+constexpr int kSsdfMax = 8;
+struct SsdfState {
+    double coeff[kSsdfMax * kSsdfMax];
+    double sigma[kSsdfMax];
+    double alpha0, beta0;
+    double lc;                        // sum_m -log(2 pi sigma_m) / 2
+    double cf[kSsdfMax * kSsdfMax];   // prediction coefficients [M][Fn]
+    double h[kSsdfMax];               // 1 / (2 sigma_m)
+    int M, F, Fn, rfa;
+};
+// E-step statistics: A [Fn][Fn] = sum p n n^T, b [M][Fn] = sum p x_m n, S2 [M] = sum p x_m^2,
+// eff = sum p (n the node's features, 0 outside the grid)
+constexpr int kSsdfA = 0, kSsdfB = 64, kSsdfS2 = 128, kSsdfEff = 136, kSsdfStats = 137;
+void ssdf_refresh_host(SsdfState &p);  // cf, h, lc from coeff, sigma
+int estep_ssdf_grid(int M, int Fn, long V, int dim);
+// update_parameters (when update) and compute_cost of the SSD filter likelihood from stats,
+// which it clears; the cost goes to st->lp_lik
+void launch_ssdf_update(SsdfState *p, double *stats, int update, DevState *st, cudaStream_t s);
+// [n][C] features (device memory) to SoA [C][n]
+void launch_features_to_soa(const double *in, long n, int C, double *out, cudaStream_t s);
 
 // State of the SSD likelihood (BINDER/src/cpu/SSDLikelihood.cpp): sigma^2, shift, scale and the
 // inverse-gamma prior (alpha0, beta0) of sigma^2

@@ -94,6 +94,24 @@ int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int
 /* No counterpart in the reference (it prints sigmaSq): the SSD parameters sigma^2, shift, scale */
 int binder_registration_get_ssd_parameters(const binder_registration *h, double out[3]);
 
+/* setSSDLikelihoodFilter(coeff, threads, sigma, features_nodes, features_voxels,
+ *                        reg_across_features, alpha_0, beta_0, M, F)   cpu/bindings.cpp:154-189
+ * The CPU backend's feature SSD likelihood (SSDLikelihoodFilter.cpp): M fixed-image channels
+ * (features_voxels [Nx_v*Ny_v*Nz_v][M]), F moving-image features (features_nodes
+ * [Nx_n*Ny_n*Nz_n][F], or [..][M] with reg_across_features, which then predicts channel m by
+ * feature m and fits no coefficients), coeff [M][F] and sigma [M] in host memory; 1 <= M, F <= 8.
+ * EM in log space only (the sampler rejects it); get_likelihood_parameters then returns the M*F
+ * coefficients. */
+int binder_registration_set_ssd_likelihood_filter(binder_registration *h, const double *coeff,
+                                                  int threads, const double *sigma,
+                                                  const double *features_nodes,
+                                                  const double *features_voxels,
+                                                  int reg_across_features, double alpha_0,
+                                                  double beta_0, int M, int F);
+/* coeff [M][F] and sigma [M] of the SSD filter likelihood (either may be null) */
+int binder_registration_get_ssd_filter_parameters(const binder_registration *h, double *coeff,
+                                                  double *sigma);
+
 /* setNonLinearTransformation(gamma_x..z, voxels_size_x..z, nodes_size_x..z, D)
  *                                                               gpu/bindings.cpp:72-95; D [V] */
 int binder_registration_set_nonlinear_transformation(binder_registration *h, double gamma_x,

@@ -1343,3 +1343,173 @@ double orc_mutual_information(const double *h, int K, int L) {
     free(pl);
     return mi;
 }
+
+/* ---- SSD filter likelihood: BINDER/src/cpu/SSDLikelihoodFilter.cpp ------------------------- */
+
+/* the predicted value of channel m at node j: sum_f coeff[m][f] nodes[j][f] (reg_across_features
+ * 0, nodes [Vn][F]) or nodes[j][m] (1, nodes [Vn][M]); 0 outside the grid */
+static double ssdf_pred(const orc_ssdf *p, const double *nodes, long node, int m) {
+    if (node < 0) return 0.0;
+    if (p->rfa) return nodes[node * p->M + m];
+    double t = 0.0;
+    for (int f = 0; f < p->F; ++f) t += p->coeff[m * p->F + f] * nodes[node * p->F + f];
+    return t;
+}
+
+/* compute_log_likelihood (:123-158) */
+double orc_ssdf_loglik(const orc_ssdf *p, const double *nodes, const double *voxels, int nxn,
+                       int nyn, int nzn, long voxel, int x, int y, int z) {
+    const int outside = x < 0 || y < 0 || z < 0 || x >= nxn || y >= nyn || z >= nzn;
+    const long node = outside ? -1 : ((long)x * nyn + y) * nzn + z;
+    double ll = 0.0;
+    for (int m = 0; m < p->M; ++m) {
+        double t = voxels[voxel * p->M + m];
+        if (!outside) t -= ssdf_pred(p, nodes, node, m);
+        ll += (t * t) / (-2.0 * p->sigma[m]) - 0.5 * log(2.0 * PI_D * p->sigma[m]);
+    }
+    return ll;
+}
+
+/* The log-space E-step (Registration.cpp:331-470) with the filter likelihood and the
+ * accumulators of accumulate_info (:160-198): gamma [Vn], s1 [M][Vn], s2 [M][Vn] per node;
+ * outside [1 + 2M] = (gamma, s1[M], s2[M]) of the nodes outside the grid.  Serial. */
+double orc_ssdf_estep(const double *d, const double *nodes, const double *voxels,
+                      const orc_ssdf *p, int nx, int ny, int nz, int nxn, int nyn, int nzn,
+                      double *dream, double *gamma, double *s1, double *s2, double *outside) {
+    const int is2D = (nz == 1);
+    const int N = is2D ? 2 : 3;
+    const long V = (long)nx * ny * nz, Vn = (long)nxn * nyn * nzn;
+    const int M = p->M;
+    memset(gamma, 0, sizeof(double) * Vn);
+    memset(s1, 0, sizeof(double) * M * Vn);
+    memset(s2, 0, sizeof(double) * M * Vn);
+    memset(outside, 0, sizeof(double) * (1 + 2 * M));
+    double mll = 0.0;
+    for (long i = 0; i < V; ++i) {
+        const double *di = d + i * N;
+        double bx[4], by[4], bz[4] = {1.0, 1.0, 1.0, 1.0};
+        const int ix = spline_setup(di[0], bx), iy = spline_setup(di[1], by);
+        const int iz = is2D ? 0 : spline_setup(di[2], bz);
+        const int ZZ = is2D ? 1 : 4;
+        double lp[64];
+        int node[64][3];
+        int n = 0;
+        double mx = -INFINITY;
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b)
+                for (int c = 0; c < ZZ; ++c) {
+                    const double w = bx[a] * by[b] * bz[c];
+                    if (!(w > 0.0)) continue;  /* a zero tap has no posterior mass */
+                    const int X = ix + a - 1, Y = iy + b - 1, Z = is2D ? 0 : iz + c - 1;
+                    lp[n] = log(bx[a]) + log(by[b]) + (is2D ? 0.0 : log(bz[c])) +
+                            orc_ssdf_loglik(p, nodes, voxels, nxn, nyn, nzn, i, X, Y, Z);
+                    node[n][0] = X; node[n][1] = Y; node[n][2] = Z;
+                    if (lp[n] > mx) mx = lp[n];
+                    ++n;
+                }
+        double norm = 0.0;
+        for (int j = 0; j < n; ++j) norm += exp(lp[j] - mx);
+        const double lnorm = log(norm) + mx;
+        mll += -lnorm;
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < n; ++j) {
+            const double pj = exp(lp[j] - lnorm);
+            const int X = node[j][0], Y = node[j][1], Z = node[j][2];
+            const int out = X < 0 || Y < 0 || Z < 0 || X >= nxn || Y >= nyn || Z >= nzn;
+            if (!out) {
+                const long nj = ((long)X * nyn + Y) * nzn + Z;
+                gamma[nj] += pj;
+                for (int m = 0; m < M; ++m) {
+                    const double xv = voxels[i * M + m];
+                    s1[m * Vn + nj] += pj * xv;
+                    s2[m * Vn + nj] += pj * xv * xv;
+                }
+            } else {
+                outside[0] += pj;
+                for (int m = 0; m < M; ++m) {
+                    const double xv = voxels[i * M + m];
+                    outside[1 + m] += pj * xv;
+                    outside[1 + M + m] += pj * xv * xv;
+                }
+            }
+            for (int q = 0; q < N; ++q) acc[q] += pj * (double)node[j][q];
+        }
+        for (int q = 0; q < N; ++q) dream[i * N + q] = acc[q];
+    }
+    return mll;
+}
+
+/* solve_linear_system (:348-389): Gaussian elimination with partial pivoting on [A | b] */
+static void ssdf_solve(int n, const double *A, const double *b, double *x) {
+    double aug[8][9];
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) aug[i][j] = A[i * n + j];
+        aug[i][n] = b[i];
+    }
+    for (int i = 0; i < n; ++i) {
+        int piv = i;
+        for (int j = i + 1; j < n; ++j)
+            if (fabs(aug[j][i]) > fabs(aug[piv][i])) piv = j;
+        if (piv != i)
+            for (int k = 0; k <= n; ++k) {
+                const double t = aug[i][k];
+                aug[i][k] = aug[piv][k];
+                aug[piv][k] = t;
+            }
+        for (int j = i + 1; j < n; ++j) {
+            const double f = aug[j][i] / aug[i][i];
+            for (int k = i; k <= n; ++k) aug[j][k] -= f * aug[i][k];
+        }
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = 0.0;
+        for (int j = i + 1; j < n; ++j) s += aug[i][j] * x[j];
+        x[i] = (aug[i][n] - s) / aug[i][i];
+    }
+}
+
+/* update_parameters (:200-203): update_coefficients (:205-290, EM branch) then update_sigma
+ * (:292-346), from the accumulators of orc_ssdf_estep; then compute_cost (:72-89).  With
+ * update == 0 only the cost. */
+double orc_ssdf_update(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
+                       const double *gamma, const double *s1, const double *s2,
+                       const double *outside, int update) {
+    const int M = p->M, F = p->F;
+    const long Vn = (long)nxn * nyn * nzn;
+    if (update) {
+        double eff = outside[0];
+        for (long j = 0; j < Vn; ++j) eff += gamma[j];
+        if (!p->rfa) {
+            double A[64] = {0}, b[64] = {0}, x[8];
+            for (long j = 0; j < Vn; ++j)
+                for (int f1 = 0; f1 < F; ++f1)
+                    for (int f2 = 0; f2 < F; ++f2)
+                        A[f1 * F + f2] += nodes[j * F + f1] * nodes[j * F + f2] * gamma[j];
+            for (int m = 0; m < M; ++m)
+                for (long j = 0; j < Vn; ++j)
+                    for (int f = 0; f < F; ++f) b[m * F + f] += s1[m * Vn + j] * nodes[j * F + f];
+            for (int m = 0; m < M; ++m) {
+                ssdf_solve(F, A, b + m * F, x);
+                for (int f = 0; f < F; ++f) p->coeff[m * F + f] = x[f];
+            }
+        }
+        for (int m = 0; m < M; ++m) {
+            double num = 0.0;
+            for (long j = 0; j < Vn; ++j) {
+                const double t = ssdf_pred(p, nodes, j, m);
+                num += s2[m * Vn + j] + (-2.0 * s1[m * Vn + j] * t) + gamma[j] * t * t;
+            }
+            num += outside[1 + M + m];
+            num += 2.0 * p->alpha0 * p->beta0;
+            p->sigma[m] = num / (eff + 2.0 * p->alpha0);
+        }
+    }
+    const double a = p->alpha0, bb = p->alpha0 * p->beta0;
+    double cost = 0.0;
+    for (int m = 0; m < M; ++m) {
+        const double x = p->sigma[m];
+        cost += -(a * log(bb) - lgamma(a) + (-a - 1.0) * log(x) - bb / x);
+    }
+    return cost;
+}
+

@@ -121,6 +121,24 @@ int orc_ssd_em(double *final_locations, const double *voxel_pos, const int *u, c
                int nz, int nxn, int nyn, int nzn, int K, int L, double non_zero_voxels,
                int max_iter, double convergence_th, int update, orc_iter_stats *stats);
 
+/* ---- SSD filter likelihood: BINDER/src/cpu/SSDLikelihoodFilter.cpp ----------------------------
+ * M fixed-image channels (voxels [V][M]), F moving-image features (nodes [Vn][F], or [Vn][M] with
+ * reg_across_features), coeff [M][F], sigma [M]; M, F <= 8 */
+typedef struct {
+    int M, F, rfa;
+    double alpha0, beta0;
+    double coeff[64];
+    double sigma[8];
+} orc_ssdf;
+double orc_ssdf_loglik(const orc_ssdf *p, const double *nodes, const double *voxels, int nxn,
+                       int nyn, int nzn, long voxel, int x, int y, int z);
+double orc_ssdf_estep(const double *d, const double *nodes, const double *voxels,
+                      const orc_ssdf *p, int nx, int ny, int nz, int nxn, int nyn, int nzn,
+                      double *dream, double *gamma, double *s1, double *s2, double *outside);
+double orc_ssdf_update(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
+                       const double *gamma, const double *s1, const double *s2,
+                       const double *outside, int update);
+
 /* ---- Gibbs sampler driver: BINDER/src/cpu/Registration.cpp:515-642 ----------------------------
  * mean_out [V*N], cov_out [V*N*N] (M2 / (N_s - 1)).  dream is the working dream-location buffer
  * (set by the caller when sample_posteriors == 0). */

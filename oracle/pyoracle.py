@@ -55,6 +55,12 @@ def _load_oracle():
     lib.orc_mi_filter_likelihood.restype = d
     lib.orc_estep_filter.argtypes = [_dp, _ip, _ip, _dp] + [i] * 9 + [_dp, _dp, C.POINTER(ll)]
     lib.orc_estep_filter.restype = d
+    lib.orc_ssdf_loglik.argtypes = [C.c_void_p, _dp, _dp, i, i, i, C.c_long, i, i, i]
+    lib.orc_ssdf_loglik.restype = d
+    lib.orc_ssdf_estep.argtypes = [_dp, _dp, _dp, C.c_void_p] + [i] * 6 + [_dp] * 5
+    lib.orc_ssdf_estep.restype = d
+    lib.orc_ssdf_update.argtypes = [C.c_void_p, _dp, i, i, i, _dp, _dp, _dp, _dp, i]
+    lib.orc_ssdf_update.restype = d
     lib.orc_estep_sample.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [u64, u32, u32, _dp, _dp]
     lib.orc_estep_sample.restype = d
     lib.orc_theta_map.argtypes = [_dp, i, i, d]
@@ -128,6 +134,11 @@ def ref_lib():
     r.ref_mi_filter_likelihood.restype = d
     r.ref_mi_filter_update.argtypes = [d, _dp, _ip, _ip] + [i] * 9 + [i, _ip, _dp, _dp]
     r.ref_mi_filter_update.restype = d
+    r.ref_ssdf_loglik.argtypes = [_dp, _dp, _dp, _dp, i, d, d, i, i] + [i] * 6 + [i, i, i, i]
+    r.ref_ssdf_loglik.restype = d
+    r.ref_ssdf_update.argtypes = [_dp, _dp, _dp, _dp, i, d, d, i, i] + [i] * 6 + \
+        [i, _ip, _dp, _dp, _dp]
+    r.ref_ssdf_update.restype = d
     return r
 
 
@@ -446,3 +457,45 @@ def topology2d(field, e1, e2, max_outer, max_inner, vs, shape):
 
 def mutual_information(hist, K, L):
     return lib().orc_mutual_information(_c64(hist).ravel(), K, L)
+
+
+class SSDFParams(C.Structure):
+    """orc_ssdf: the SSD filter likelihood's state (BINDER/src/cpu/SSDLikelihoodFilter.cpp)."""
+    _fields_ = [("M", C.c_int), ("F", C.c_int), ("rfa", C.c_int), ("alpha0", C.c_double),
+                ("beta0", C.c_double), ("coeff", C.c_double * 64), ("sigma", C.c_double * 8)]
+
+
+def ssdf_params(coeff, sigma, rfa, alpha0, beta0):
+    coeff = np.asarray(coeff, np.float64)
+    M, F = coeff.shape
+    p = SSDFParams(M=M, F=F, rfa=int(rfa), alpha0=float(alpha0), beta0=float(beta0))
+    for q, v in enumerate(coeff.ravel()):
+        p.coeff[q] = v
+    for m, v in enumerate(np.asarray(sigma, np.float64).ravel()):
+        p.sigma[m] = v
+    return p
+
+
+def ssdf_loglik(params, nodes, voxels, nshape, voxel, node):
+    return lib().orc_ssdf_loglik(C.addressof(params), _c64(nodes).ravel(), _c64(voxels).ravel(),
+                                 *nshape, int(voxel), *[int(t) for t in node])
+
+
+def ssdf_estep(d, nodes, voxels, params, vshape, nshape):
+    """Log-space E-step with the SSD filter likelihood.  Returns (mll, dream[V*N], acc) with acc
+    the accumulate_info sums (gamma [Vn], s1 [M*Vn], s2 [M*Vn], outside [1 + 2M])."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    Vn, M = int(np.prod(nshape)), params.M
+    dream = np.zeros(nx * ny * nz * N)
+    acc = (np.zeros(Vn), np.zeros(M * Vn), np.zeros(M * Vn), np.zeros(1 + 2 * M))
+    mll = lib().orc_ssdf_estep(_c64(d).ravel(), _c64(nodes).ravel(), _c64(voxels).ravel(),
+                               C.addressof(params), nx, ny, nz, *nshape, dream, *acc)
+    return mll, dream, acc
+
+
+def ssdf_update(params, nodes, nshape, acc, update=True):
+    """update_parameters (when update) and compute_cost; params is updated in place."""
+    return lib().orc_ssdf_update(C.addressof(params), _c64(nodes).ravel(), *nshape, *acc,
+                                 int(update))
+

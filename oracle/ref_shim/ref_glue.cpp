@@ -6,6 +6,7 @@
 
 #include "MILikelihood.h"
 #include "MILikelihoodFilter.h"
+#include "SSDLikelihoodFilter.h"
 #include "NonLinearTransformation.h"
 #include "Spline.h"
 #include "topology_correction_2D.h"
@@ -116,6 +117,49 @@ double ref_mi_filter_update(double alpha, const double *theta, const int *voxels
     const auto th = f.get_parameters();
     std::memcpy(theta_out, th.data(), sizeof(double) * th.size());
     return f.compute_cost();
+}
+
+// SSDLikelihoodFilter::compute_log_likelihood (BINDER/src/cpu/SSDLikelihoodFilter.cpp:123-158)
+double ref_ssdf_loglik(const double *coeff, const double *sigma, const double *nodes,
+                       const double *voxels, int rfa, double alpha0, double beta0, int M, int F,
+                       int nxn, int nyn, int nzn, int nxv, int nyv, int nzv, int voxel, int x,
+                       int y, int z) {
+    SSDLikelihoodFilter f(coeff, 1, sigma, nodes, voxels, rfa, alpha0, beta0, M, F, nxn, nyn, nzn,
+                          nxv, nyv, nzv);
+    return f.compute_log_likelihood(voxel, x, y, z);
+}
+
+// accumulate_info over n (voxel, node, posterior) triples, update_parameters, compute_cost
+// (:160-346, :72-89); coeff_out [M][F], sigma_out [M]
+double ref_ssdf_update(const double *coeff, const double *sigma, const double *nodes,
+                       const double *voxels, int rfa, double alpha0, double beta0, int M, int F,
+                       int nxn, int nyn, int nzn, int nxv, int nyv, int nzv, int n,
+                       const int *vxyz, const double *post, double *coeff_out,
+                       double *sigma_out) {
+    // the class keeps a pointer to the voxel features: give it a copy that can be probed below
+    std::vector<double> vox(voxels, voxels + (size_t)nxv * nyv * nzv * M);
+    SSDLikelihoodFilter f(coeff, 1, sigma, nodes, vox.data(), rfa, alpha0, beta0, M, F, nxn, nyn,
+                          nzn, nxv, nyv, nzv);
+    for (int t = 0; t < n; ++t)
+        f.accumulate_info(0, vxyz[4 * t], vxyz[4 * t + 1], vxyz[4 * t + 2], vxyz[4 * t + 3],
+                          post[t]);
+    f.update_parameters();
+    const auto c = f.get_parameters();
+    std::memcpy(coeff_out, c.data(), sizeof(double) * c.size());
+    const double cost = f.compute_cost();
+    // sigma is private: read it back through compute_log_likelihood at a node outside the grid,
+    // where the log-likelihood of voxel 0 is sum_m (x_m^2 / (-2 sigma_m) + c_m).  With x = 0 that
+    // is sum_m c_m; with x = X in channel m alone it adds -X^2 / (2 sigma_m).
+    const double X = 1.0e4;
+    for (int m = 0; m < M; ++m) vox[m] = 0.0;
+    const double base = f.compute_log_likelihood(0, -1, -1, -1);
+    for (int m = 0; m < M; ++m) {
+        vox[m] = X;
+        const double lm = f.compute_log_likelihood(0, -1, -1, -1);
+        vox[m] = 0.0;
+        sigma_out[m] = -(X * X) / (2.0 * (lm - base));
+    }
+    return cost;
 }
 
 }  // extern "C"

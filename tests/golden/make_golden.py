@@ -1,9 +1,10 @@
 """Generate the golden fixtures in this directory from the reference's own CPU sources.
 
-The reference's Spline.cpp, MILikelihood.cpp, MILikelihoodFilter.cpp, utils.cpp, DCT.cpp, FFT.cpp,
-NonLinearTransformation.cpp, topology_correction_3D.cpp and topology_correction_2D.cpp are compiled unmodified by
-oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in
-oracle/ref_shim).  This script feeds them seeded inputs and stores inputs and outputs as small
+The reference's Spline.cpp, MILikelihood.cpp, MILikelihoodFilter.cpp, SSDLikelihoodFilter.cpp,
+utils.cpp, DCT.cpp, FFT.cpp, NonLinearTransformation.cpp, topology_correction_3D.cpp and
+topology_correction_2D.cpp are compiled unmodified by oracle/Makefile into
+oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in oracle/ref_shim, and
+Eigen's Dense header, included but unused, by an empty file there).  This script feeds them seeded inputs and stores inputs and outputs as small
 .npz files, so the parity tests are pinned to the reference even where its sources are absent.
 
 Run from the repository root:  python tests/golden/make_golden.py
@@ -192,6 +193,32 @@ def main():
     np.savez(os.path.join(HERE, "mi_filter_ref.npz"), M=M, K=K, L=L, nshape=nshape,
              vshape=vshape, theta=theta, nodes=nodes, voxels=voxels, pairs=vxyz, likelihood=like,
              posterior=post, alpha=2.0, theta_out=th_out.reshape(M, K, L), cost=fcost)
+
+    # SSD filter likelihood (SSDLikelihoodFilter.cpp:72-389): compute_log_likelihood at (voxel,
+    # node) pairs, then accumulate_info / update_parameters / compute_cost, for both layouts
+    # (reg_across_features 0: nodes [Vn][F] and a coefficient fit; 1: nodes [Vn][M])
+    ssdf = {}
+    for rfa, M, F in ((0, 2, 3), (1, 3, 3)):
+        Fn = M if rfa else F
+        nodes_f = rng.normal(0.0, 2.0, (Vn, Fn)) + 1.0
+        voxels_f = rng.normal(0.0, 2.0, (V, M))
+        coeff = rng.normal(0.0, 1.0, (M, F))
+        sig = rng.random(M) * 2.0 + 0.5
+        like = np.array([R.ref_ssdf_loglik(coeff.ravel(), sig, nodes_f.ravel(), voxels_f.ravel(),
+                                           rfa, 3.0, 0.7, M, F, *nshape, *vshape, int(v),
+                                           *[int(t) for t in xyz])
+                         for v, xyz in zip(pv, pn)])
+        c_out, s_out = np.zeros(M * F), np.zeros(M)
+        scost = R.ref_ssdf_update(coeff.ravel(), sig, nodes_f.ravel(), voxels_f.ravel(), rfa, 3.0,
+                                  0.7, M, F, *nshape, *vshape, npairs, vxyz.ravel(), post,
+                                  c_out, s_out)
+        key = f"rfa{rfa}_"
+        ssdf.update({key + "M": M, key + "F": F, key + "nodes": nodes_f, key + "voxels": voxels_f,
+                     key + "coeff": coeff, key + "sigma": sig, key + "loglik": like,
+                     key + "coeff_out": c_out.reshape(M, F), key + "sigma_out": s_out,
+                     key + "cost": scost})
+    np.savez(os.path.join(HERE, "ssd_filter_ref.npz"), nshape=nshape, vshape=vshape, pairs=vxyz,
+             posterior=post, alpha0=3.0, beta0=0.7, **ssdf)
     print("golden fixtures written to", HERE)
 
 

@@ -165,7 +165,7 @@ def test_mi_filter_estep_reduces_to_mi(oracle):
     th /= th.sum(1, keepdims=True)
     mll, dream, hist, deg = oracle.estep(d, u[:V], v[:V], th, vshape, nshape, K, L)
     mll1, dream1, hist1, deg1 = oracle.estep_filter(d, u[:V], v[:V], th, vshape, nshape, K, L, 1)
-    assert mll1 == mll and deg1 == deg
+    assert mll1 == pytest.approx(mll, rel=1e-13) and deg1 == deg  # OpenMP reduction order
     np.testing.assert_array_equal(dream1, dream)
     np.testing.assert_array_equal(hist1, hist)
     th2 = np.stack([th, np.full((K, L), 1.0 / L)])
@@ -212,3 +212,38 @@ def test_prior_sampling_covariance(oracle, order):
     x = s[..., 0].reshape(-1, np.prod(shape), order="F")
     emp = x.T @ x / x.shape[0]
     np.testing.assert_allclose(emp, cov, rtol=1e-3, atol=1e-3)
+
+
+@pytest.mark.parametrize("rfa", [0, 1])
+def test_ssd_filter_matches_reference(oracle, rfa):
+    """SSDLikelihoodFilter (compute_log_likelihood, accumulate_info, update_parameters with the
+    coefficient solve and the sigma update, compute_cost) against the reference's compiled class."""
+    g = golden("ssd_filter_ref.npz")
+    k = f"rfa{rfa}_"
+    M, F = int(g[k + "M"]), int(g[k + "F"])
+    nshape = tuple(int(t) for t in g["nshape"])
+    nodes, voxels = g[k + "nodes"], g[k + "voxels"]
+    p = oracle.ssdf_params(g[k + "coeff"], g[k + "sigma"], rfa, float(g["alpha0"]),
+                           float(g["beta0"]))
+    got = [oracle.ssdf_loglik(p, nodes, voxels, nshape, v, (x, y, z))
+           for v, x, y, z in g["pairs"]]
+    np.testing.assert_allclose(got, g[k + "loglik"], rtol=1e-14, atol=0)
+    # the accumulators of the same (voxel, node, posterior) triples, as accumulate_info sums them
+    Vn = int(np.prod(nshape))
+    gam, s1, s2, out = np.zeros(Vn), np.zeros(M * Vn), np.zeros(M * Vn), np.zeros(1 + 2 * M)
+    for (v, x, y, z), w in zip(g["pairs"], g["posterior"]):
+        xv = voxels[v]
+        if 0 <= x < nshape[0] and 0 <= y < nshape[1] and 0 <= z < nshape[2]:
+            j = (x * nshape[1] + y) * nshape[2] + z
+            gam[j] += w
+            s1[np.arange(M) * Vn + j] += w * xv
+            s2[np.arange(M) * Vn + j] += w * xv * xv
+        else:
+            out[0] += w
+            out[1:1 + M] += w * xv
+            out[1 + M:] += w * xv * xv
+    cost = oracle.ssdf_update(p, nodes, nshape, (gam, s1, s2, out))
+    np.testing.assert_allclose(np.array(p.coeff[:M * F]).reshape(M, F), g[k + "coeff_out"],
+                               rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(np.array(p.sigma[:M]), g[k + "sigma_out"], rtol=1e-10)
+    assert cost == pytest.approx(float(g[k + "cost"]), rel=1e-10)
