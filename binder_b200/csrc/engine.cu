@@ -138,11 +138,17 @@ void MStep::init(int x, int y, int z, cudaStream_t s) {
     t1 = dalloc<float>((size_t)V * 3, s);
     t2 = dalloc<float>((size_t)V * 3, s);
     precision = default_precision();
+    persistent = default_persistent();
     for (int i = 0; i < 2; ++i) {
         BINDER_CUDA(cudaStreamCreate(&side[i]));
         BINDER_CUDA(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
     }
     BINDER_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+}
+
+bool default_persistent() {
+    const char *e = std::getenv("BINDER_B200_PERSISTENT");
+    return e && e[0] == '1' && e[1] == 0;
 }
 
 int default_precision() {
@@ -183,7 +189,7 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     const bool tc = precision != kPrecFP32Simt;
     const int planes = precision == kPrecTF32 ? 1 : 2;
     // the tensor-core path runs one chain of passes per component, each on its own stream
-    const bool branches = tc && side[0] && side[1];
+    const bool branches = tc && !persistent && side[0] && side[1];
     if (branches) {
         BINDER_CUDA(cudaEventRecord(fork, s));
         for (int c = 1; c < ncomp; ++c) BINDER_CUDA(cudaStreamWaitEvent(side[c - 1], fork, 0));
@@ -207,7 +213,7 @@ void MStep::run_chain(AxisArgs<float> a, int c0, int nc, cudaStream_t s, const f
         if (tc)
             launch_axis_pass_tc(a, inverse ? dct.uinv[axis] : dct.ufwd[axis],
                                 mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, nc,
-                                planes, s);
+                                planes, s, persistent);
         else
             launch_axis_pass(a, mode, nc, s);
     };

@@ -28,6 +28,9 @@ struct MStep {
     DctSet dct;
     float *t1 = nullptr, *t2 = nullptr;
     int precision = kPrecFP32Simt;  // TransformPrecision
+    // tensor-core passes: one CTA per 128-line tile with the components on their own streams, or
+    // persistent (all components per launch, one CTA per SM; measured slower on B200)
+    bool persistent = false;
     // the tensor-core passes of components 1 and 2 run on their own streams (graph branches), so
     // one component's last partial wave of tiles overlaps the other components' passes
     cudaStream_t side[2] = {nullptr, nullptr};
@@ -208,6 +211,8 @@ class PriorTransform {
 
 // default transform precision: BINDER_B200_PRECISION (0 FP32 SIMT, 1 3xTF32, 2 TF32) or 3xTF32
 int default_precision();
+// default tensor-core pass kind: BINDER_B200_PERSISTENT (0 per-tile CTAs, 1 persistent) or 0
+bool default_persistent();
 
 
 }  // namespace binder

@@ -49,6 +49,7 @@ struct UArgs {
     int ny, nz;
     int dims;  // 3, or 2 for an image (the contiguous axis is then component 1)
     int comp0;  // component of blockIdx.z == 0
+    int ncomp;  // components of one persistent launch
     const int *skip;
 };
 
@@ -732,6 +733,469 @@ void launch_ws(const UArgs &a, int ncomp, cudaStream_t s) {
     BINDER_CUDA(cudaGetLastError());
 }
 
+// ---- persistent pass: 4 producer warps, 1 MMA warp, 4 epilogue warps -------------------------
+// One CTA per SM walks tiles blockIdx.x, blockIdx.x + gridDim.x, ... of every component of the
+// pass, as one flat sequence of K chunks (chunk g = tile g / nkc, K chunk g % nkc), so the A
+// stages and B slots of the warp-specialised pipeline above run on across tile boundaries.  The
+// accumulator is double-buffered in TMEM (buffer it & 1 for the CTA's it-th tile): the MMA warp
+// commits a finished tile to accf[b]; warps 5-8 drain it (TMEM -> registers -> global, the
+// epilogues of umma_ws_kernel) and release it on acce[b] while the next tile accumulates in the
+// other buffer.  Every wait is bounded; on expiry the CTA sets an error flag and winds down.
+constexpr int kPtProd = 256;                  // producer threads (warps 0-7)
+constexpr int kPtMma = kPtProd;               // the MMA thread (warp 8, lane 0)
+constexpr int kPtThreads = kPtProd + 32 + 128;  // + MMA warp + 4 epilogue warps
+// A stages (kPtStages, a template parameter: 3 where shared memory allows, else 2) bound how far
+// the producers run ahead of the MMAs' completion; B is copied kPtDist chunks ahead into
+// kPtStages + kPtDist slots
+constexpr int kPtDist = 2;
+constexpr int kPtRaw = 4;                 // raw FP32 A slots (A copied kPtRaw - 1 chunks ahead)
+constexpr int kRawContig = 20;            // floats per line of a contiguous-axis raw slot (padded)
+constexpr int kRawSlot = kLines * kRawContig;  // floats per raw slot (either layout fits)
+
+// cp.async of `bytes` (4 or 16) with zero fill: src_bytes of them read from global memory
+__device__ __forceinline__ void cp_async_zfill(float *dst, const float *src, int bytes,
+                                               int src_bytes) {
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_u32(dst)),
+                     "l"(src), "r"(src_bytes)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(umma::smem_u32(dst)),
+                     "l"(src), "r"(src_bytes)
+                     : "memory");
+}
+
+// barrier 1 over the kPtProd producer threads, OR of `pred` returned to all of them
+__device__ __forceinline__ bool producers_sync_or(bool pred) {
+    uint32_t r;
+    __syncwarp();
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, 256, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void producers_sync() {
+    __syncwarp();
+    asm volatile("bar.sync 1, 256;" ::: "memory");
+}
+
+template <int MODE, int PLANES, int kPtStages>
+__global__ void __launch_bounds__(kPtThreads, 1) umma_pt_kernel(const UArgs a) {
+    constexpr int kPtSlots = kPtStages + kPtDist;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Npad = a.Npad, n = a.n, nkc = a.nkc;
+    const uint32_t bplane = (uint32_t)Npad * kKC;
+    float *As = reinterpret_cast<float *>(smem_raw);  // [kPtStages][PLANES][kAPlane]
+    float *Bs = As + kPtStages * PLANES * kAPlane;    // [kPtSlots][PLANES][bplane]
+    float *raw = Bs + kPtSlots * PLANES * bplane;     // [kPtRaw][kRawSlot] raw A chunks
+    float *stg0 = raw + kPtRaw * kRawSlot;            // [4 warps][32][33] epilogue staging
+    uint64_t *full = reinterpret_cast<uint64_t *>(stg0 + 4 * 32 * 33);  // [kPtStages]
+    uint64_t *done = full + kPtStages;                                  // [kPtSlots]
+    uint64_t *accf = done + kPtSlots;                                   // [2]
+    uint64_t *acce = accf + 2;                                          // [2]
+    uint64_t *drain = acce + 2;                                         // [1]
+    uint32_t *holder = reinterpret_cast<uint32_t *>(drain + 1);
+    int *s_err = reinterpret_cast<int *>(holder + 1);
+    __shared__ double red[32];
+
+    uint32_t acols = 32;  // columns of one accumulator
+    while (acols < (uint32_t)Npad) acols <<= 1;
+    const uint32_t ncols = 2 * acols;
+    if (warp == 0) umma::tmem_alloc(holder, ncols);
+    if (tid == 32) {
+        for (int i = 0; i < kPtStages; ++i) umma::mbar_init(&full[i], kPtProd);
+        for (int i = 0; i < kPtSlots; ++i) umma::mbar_init(&done[i], 1);
+        umma::mbar_init(&accf[0], 1);
+        umma::mbar_init(&accf[1], 1);
+        umma::mbar_init(&acce[0], 128);
+        umma::mbar_init(&acce[1], 128);
+        umma::mbar_init(drain, 1);
+        *s_err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *holder;
+
+    const long nlines = a.outer * a.s;
+    const long tiles = (nlines + kLines - 1) / kLines;  // per component
+    const long total = tiles * a.ncomp;
+    const long G = gridDim.x;
+    const int my_tiles = blockIdx.x < total ? (int)((total - 1 - blockIdx.x) / G + 1) : 0;
+    const long nchunk = (long)my_tiles * nkc;
+    const bool contig = (a.s == 1);
+    const int cr = lane & 7, cq = lane >> 3;  // contiguous-axis load mapping
+
+    double part_cost = 0.0, part_raw = 0.0;
+
+    if (warp == kPtProd / 32) {
+        // ---- MMA warp ------------------------------------------------------------------------
+        if (lane == 0) {
+            const uint32_t idesc = umma::instr_desc(kLines, Npad, umma::kFmtTF32);
+            long g = 0;
+            for (int it = 0; it < my_tiles; ++it) {
+                const int b = it & 1;
+                if (it >= 2 && (!umma::mbar_wait(&acce[b], (uint32_t)((it - 2) >> 1) & 1u,
+                                                 kWaitLimit) ||
+                                *(volatile int *)s_err)) {
+                    *(volatile int *)s_err = 1;
+                    break;
+                }
+                umma::fence_after_sync();
+                const uint32_t tacc = tmem + (uint32_t)b * acols;
+                bool ok = true;
+                for (int kc = 0; kc < nkc; ++kc, ++g) {
+                    if (!umma::mbar_wait_spin(&full[g % kPtStages],
+                                              (uint32_t)(g / kPtStages) & 1u, kWaitLimit) ||
+                        *(volatile int *)s_err) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after_sync();
+                    const uint32_t abase =
+                        umma::smem_u32(As + (g % kPtStages) * PLANES * kAPlane);
+                    const uint32_t bbase = umma::smem_u32(Bs + (g % kPtSlots) * PLANES * bplane);
+#pragma unroll
+                    for (int ks = 0; ks < kKC / 8; ++ks) {
+                        const uint32_t ao = (uint32_t)ks * 2u * 2048u;
+                        const uint32_t bo = (uint32_t)ks * 2u * (uint32_t)Npad * 16u;
+                        const uint64_t ahi = umma::smem_desc(abase + ao, 2048u, 128u);
+                        const uint64_t bhi =
+                            umma::smem_desc(bbase + bo, (uint32_t)Npad * 16u, 128u);
+                        umma::mma_tf32(tacc, ahi, bhi, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+                        if (PLANES == 2) {
+                            const uint64_t alo =
+                                umma::smem_desc(abase + kAPlane * 4u + ao, 2048u, 128u);
+                            const uint64_t blo = umma::smem_desc(bbase + bplane * 4u + bo,
+                                                                 (uint32_t)Npad * 16u, 128u);
+                            umma::mma_tf32(tacc, ahi, blo, idesc, 1u);
+                            umma::mma_tf32(tacc, alo, bhi, idesc, 1u);
+                        }
+                    }
+                    umma::commit(&done[g % kPtSlots]);
+                }
+                if (!ok) {
+                    *(volatile int *)s_err = 1;
+                    break;
+                }
+                umma::commit(&accf[b]);  // arrives when this tile's MMAs have completed
+            }
+        }
+    } else if (warp < kPtProd / 32) {
+        // ---- producers -----------------------------------------------------------------------
+        // A chunks are copied raw (FP32) into a kPtRaw-slot ring by cp.async, kPtRaw - 1 chunks
+        // ahead, then split into TF32 planes from shared memory (thread tid <-> row tid & 127,
+        // K slots 2 (tid >> 7) and 2 (tid >> 7) + 1).  Layouts:
+        //   strided axis:    raw[j][line] (16 x 128); 16-byte copies of 4 neighbouring lines when
+        //                    s % 4 == 0 (the 4 lines then share o and start 16-byte aligned),
+        //                    4-byte copies of the thread's row and K half otherwise;
+        //   contiguous axis: raw[line][kRawContig]; 16-byte copies of 4 elements of a line when
+        //                    n % 4 == 0 (every line then starts 16-byte aligned), else 4-byte.
+        // Out-of-range lines and elements are zero-filled (source bytes 0).
+        const bool wide = contig ? (n & 3) == 0 : (a.s & 3) == 0;
+        const int row = tid & (kLines - 1), half = tid >> 7;
+        // the A chunks are copied in order: a cursor over (tile, K chunk) instead of divisions
+        long cg = 0;        // next chunk to copy
+        int ckc = 0;        // its K chunk
+        long ctau = blockIdx.x;
+        const float *cin = nullptr;
+        long cl0 = 0;
+        const float *lbase[2];  // this thread's line (group) bases, per tile
+        bool lval[2];
+        auto set_tile = [&]() {
+            const long cm = ctau / tiles;
+            cin = a.in + (a.comp0 + cm) * a.V;
+            cl0 = (ctau - cm * tiles) * kLines;
+            if (contig) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const long gl = cl0 + (wide ? (tid >> 2) + 64 * i : row);
+                    lval[i] = gl < nlines;
+                    lbase[i] = lval[i] ? cin + gl * n : cin;
+                }
+            } else {
+                const long lg = cl0 + (wide ? 4 * lane : row);
+                const bool v = lg < nlines;
+                const long o = v ? lg / a.s : 0, t = v ? lg - o * a.s : 0;
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    lval[i] = v;
+                    lbase[i] = cin + o * (long)n * a.s + t;
+                }
+            }
+        };
+        set_tile();
+        // raw copy of chunk cg into its slot, cursor advanced (no copy past the last chunk)
+        auto copy_next = [&]() {
+            if (cg >= nchunk) return;
+            float *rs = raw + (cg % kPtRaw) * kRawSlot;
+            const int jb = ckc * kKC;
+            if (contig) {
+                if (wide) {
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const int line = (tid >> 2) + 64 * i, qd = tid & 3;
+                        const int j0 = jb + 4 * qd;
+                        const bool ok = lval[i] && j0 < n;
+                        cp_async_zfill(rs + line * kRawContig + 4 * qd,
+                                       ok ? lbase[i] + j0 : cin, 16, ok ? 16 : 0);
+                    }
+                } else {
+#pragma unroll
+                    for (int jh = 0; jh < kKC / 2; ++jh) {
+                        const int jj = 8 * half + jh;
+                        const bool ok = lval[0] && jb + jj < n;
+                        cp_async_zfill(rs + row * kRawContig + jj, ok ? lbase[0] + jb + jj : cin,
+                                       4, ok ? 4 : 0);
+                    }
+                }
+            } else {
+                if (wide) {
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        const int jj = warp + 8 * i;
+                        const bool ok = lval[0] && jb + jj < n;
+                        cp_async_zfill(rs + jj * kLines + 4 * lane,
+                                       ok ? lbase[0] + (long)(jb + jj) * a.s : cin, 16,
+                                       ok ? 16 : 0);
+                    }
+                } else {
+#pragma unroll
+                    for (int jh = 0; jh < kKC / 2; ++jh) {
+                        const int jj = 8 * half + jh;
+                        const bool ok = lval[0] && jb + jj < n;
+                        cp_async_zfill(rs + jj * kLines + row,
+                                       ok ? lbase[0] + (long)(jb + jj) * a.s : cin, 4,
+                                       ok ? 4 : 0);
+                    }
+                }
+            }
+            ++cg;
+            if (++ckc == nkc) {
+                ckc = 0;
+                ctau += G;
+                if (cg < nchunk) set_tile();
+            }
+        };
+        int kb = 0;   // matrix chunk of the next B copy
+        long gb = 0;  // chunk of the next B copy
+        auto issue_b = [&]() {
+            if (gb < nchunk) {
+                const float *srcb = a.B1 + (size_t)kb * 2 * bplane;
+                float *Bp = Bs + (gb % kPtSlots) * PLANES * bplane;
+                const int nv = PLANES * (int)bplane / 4;
+                for (int qv = tid; qv < nv; qv += kPtProd)
+                    umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
+            }
+            ++gb;
+            if (++kb == nkc) kb = 0;
+        };
+        // prologue: groups 0 .. kPtRaw - 2 hold raw chunks 0 .. kPtRaw - 2 and B chunks
+        // 0 .. kPtDist - 1; step g adds one group with raw chunk g + kPtRaw - 1 and B chunk
+        // g + kPtDist, so raw(g) and B(g) are complete once at most 2 groups are pending
+        static_assert(kPtRaw - 1 >= kPtDist && kPtRaw >= 3, "group accounting");
+        for (int q = 0; q < kPtRaw - 1; ++q) {
+            copy_next();
+            if (q < kPtDist) issue_b();
+            umma::cp_async_commit();
+        }
+        for (long g = 0; g < nchunk; ++g) {
+            // A stage g % kPtStages and B slot (g + kPtDist) % kPtSlots were last read by the
+            // MMAs of chunk g - kPtStages; the raw slot of chunk g + kPtRaw - 1 by the split of
+            // chunk g - 1.  One stop decision for all producers.
+            bool stop = *(volatile int *)s_err != 0;
+            if (g >= kPtStages) {
+                const long gp = g - kPtStages;
+                stop |= !umma::mbar_wait_spin(&done[gp % kPtSlots],
+                                              (uint32_t)(gp / kPtSlots) & 1u, kWaitLimit);
+            }
+            if (producers_sync_or(stop)) {
+                *(volatile int *)s_err = 1;
+                break;
+            }
+            copy_next();
+            issue_b();
+            umma::cp_async_commit();
+            asm volatile("cp.async.wait_group 2;" ::: "memory");
+            producers_sync();  // every producer's copies of raw chunk g have landed
+            const float *rs = raw + (g % kPtRaw) * kRawSlot;
+            float *Ap = As + (g % kPtStages) * PLANES * kAPlane;
+#pragma unroll
+            for (int qh = 0; qh < 2; ++qh) {
+                const int q = 2 * half + qh;
+                float4 v;
+                if (contig) {
+                    v = *reinterpret_cast<const float4 *>(rs + row * kRawContig + 4 * q);
+                } else {
+                    v.x = rs[(4 * q + 0) * kLines + row];
+                    v.y = rs[(4 * q + 1) * kLines + row];
+                    v.z = rs[(4 * q + 2) * kLines + row];
+                    v.w = rs[(4 * q + 3) * kLines + row];
+                }
+                store_split<PLANES>(Ap, a_slot(row, q), v);
+            }
+            umma::fence_proxy_async_smem();  // this thread's part of B chunk g and A stage
+            umma::mbar_arrive(&full[g % kPtStages]);
+        }
+        umma::cp_async_wait_all();
+    } else {
+        // ---- epilogue warps 5-8: TMEM lane quarter ew = warp % 4 -----------------------------
+        const int ew = warp & 3;
+        const uint32_t tlane = (uint32_t)(ew * 32) << 16;
+        const int row = ew * 32 + lane;  // this thread's row of the tile
+        float *stg = stg0 + ew * 32 * 33;
+        const uint32_t sweep = (MODE == kEpiSpectralOut && a.sample) ? (uint32_t)a.st->sweep : 0u;
+        const bool want_raw =
+            MODE == kEpiSpectralOut && a.want_raw && (a.st->sweep % a.every == 0);
+        const int nchunks = (n + 31) / 32;
+        for (int it = 0; it < my_tiles; ++it) {
+            const int b = it & 1;
+            const bool ok = umma::mbar_wait(&accf[b], (uint32_t)(it >> 1) & 1u, kWaitLimit);
+            if (__any_sync(0xffffffffu, !ok || *(volatile int *)s_err)) {
+                *(volatile int *)s_err = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            const uint32_t tacc = tmem + tlane + (uint32_t)b * acols;
+            const long tau = blockIdx.x + (long)it * G;
+            const long cm = tau / tiles;
+            const int comp = a.comp0 + (int)cm;
+            float *out = a.out + comp * a.V;
+            const long l0 = (tau - cm * tiles) * kLines;
+            if (contig && MODE != kEpiSpectralOut) {
+                float rowc = 0.0f;
+                if (MODE == kEpiPositions && !a.xpos) {
+                    const int gi = (int)(l0 + ew * 32 + lane);  // 3D: x * ny + y; 2D: x
+                    rowc = a.dims == 2 ? (float)gi
+                                       : (comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
+                }
+                for (int cc = 0; cc < nchunks; ++cc) {
+                    float v[32];
+                    umma::tmem_ld32(tacc + (uint32_t)(cc * 32), v);
+#pragma unroll
+                    for (int m = 0; m < 32; ++m) stg[lane * 33 + m] = v[m];
+                    __syncwarp();
+                    const int k = cc * 32 + lane;
+#pragma unroll 4
+                    for (int r = 0; r < 32; ++r) {
+                        const long gl = l0 + ew * 32 + r;
+                        const float rc = __shfl_sync(0xffffffffu, rowc, r);
+                        if (gl < nlines && k < n) {
+                            float val = stg[r * 33 + lane];
+                            if (MODE == kEpiPositions)
+                                val += a.xpos ? __ldg(a.xpos + comp * a.V + gl * n + k)
+                                              : (comp == a.dims - 1 ? (float)k : rc);
+                            out[gl * n + k] = val;
+                        }
+                    }
+                    __syncwarp();
+                }
+            } else {
+                const long lg = l0 + row;
+                const bool valid = lg < nlines;
+                const long o = valid ? lg / a.s : 0, t = valid ? lg - o * a.s : 0;
+                float *op = out + o * (long)n * a.s + t;
+                const double gamma = MODE == kEpiSpectralOut ? a.st->gamma[comp] : 0.0;
+                const float gs2 = (float)(gamma * a.sigma2);
+                float ccost = 0.0f;
+                for (int cc = 0; cc < nchunks; ++cc) {
+                    float v[32];
+                    umma::tmem_ld32(tacc + (uint32_t)(cc * 32), v);
+                    if (!valid) continue;
+#pragma unroll
+                    for (int m = 0; m < 32; ++m) {
+                        const int k = cc * 32 + m;
+                        if (k < n) {
+                            float val = v[m];
+                            if (MODE == kEpiSpectralOut) {
+                                const float Dv = __ldg(a.D + (long)k * a.s + t);
+                                const float f = __fdividef(1.0f, fmaf(gs2, Dv, 1.0f));
+                                val *= f;
+                                if (a.sample)
+                                    val += sqrtf((float)a.sigma2 * f) *
+                                           prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t),
+                                                           sweep, a.chain, comp);
+                                ccost += Dv * val * val;
+                            }
+                            op[(long)k * a.s] = val;
+                        }
+                    }
+                }
+                if (MODE == kEpiSpectralOut) {
+                    part_cost += 0.5 * gamma * (double)ccost;
+                    if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)ccost;
+                }
+            }
+            // this tile's TMEM reads are complete (tcgen05.wait::ld): release the buffer
+            umma::fence_before_sync();
+            umma::mbar_arrive(&acce[b]);
+        }
+    }
+
+    if (MODE == kEpiSpectralOut) {
+        const double sc = block_sum(part_cost, red);
+        if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
+        if (a.want_raw) {
+            const double sr = block_sum(part_raw, red);
+            if (tid == 0) atomicAdd(&a.st->raw_reg, sr);
+        }
+    }
+    // ---- teardown: after an error, let every tcgen05 op still in flight finish (bounded) ----
+    __syncthreads();
+    if (*s_err && tid == kPtMma) {
+        umma::commit(drain);
+        umma::mbar_wait(drain, 0, kWaitLimit);
+        if (a.st) atomicOr(&a.st->flags, (unsigned)kFlagTensorTimeout);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, ncols);
+}
+
+template <int MODE, int PLANES, int S>
+size_t pt_smem(int Npad) {
+    return (size_t)(S * PLANES * kAPlane + (S + kPtDist) * PLANES * Npad * kKC +
+                    kPtRaw * kRawSlot + 4 * 32 * 33) * sizeof(float) + 256;
+}
+
+template <int MODE, int PLANES, int S>
+void launch_pt_s(const UArgs &a, size_t need, cudaStream_t s) {
+    uint32_t acols = 32;
+    while (acols < (uint32_t)a.Npad) acols <<= 1;
+    // never more CTAs per SM than its 512 TMEM columns hold at once (a surplus CTA would only
+    // wait inside tcgen05.alloc): pad the shared-memory request accordingly
+    const size_t per_sm = 228 * 1024;
+    const size_t max_ctas = 512 / (2 * acols);
+    const size_t floor_smem = per_sm / (max_ctas + 1) + 1024;
+    const size_t smem = need > floor_smem ? need : floor_smem;
+    BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
+    BINDER_CUDA(cudaFuncSetAttribute(umma_pt_kernel<MODE, PLANES, S>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BINDER_CUDA(cudaFuncSetAttribute(umma_pt_kernel<MODE, PLANES, S>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+    int dev = 0, sms = 148;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long tiles = (a.outer * a.s + kLines - 1) / kLines * a.ncomp;
+    const long grid = tiles < (long)sms * (long)max_ctas ? tiles : (long)sms * (long)max_ctas;
+    count_launch(), umma_pt_kernel<MODE, PLANES, S><<<(unsigned)grid, kPtThreads, smem, s>>>(a);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+template <int MODE, int PLANES>
+void launch_pt(const UArgs &a, cudaStream_t s) {
+    const size_t n3 = pt_smem<MODE, PLANES, 3>(a.Npad);
+    if (n3 <= 227 * 1024) launch_pt_s<MODE, PLANES, 3>(a, n3, s);
+    else launch_pt_s<MODE, PLANES, 2>(a, pt_smem<MODE, PLANES, 2>(a.Npad), s);
+}
+
 float tf32_rna_host(float x) {
     uint32_t u;
     std::memcpy(&u, &x, 4);
@@ -803,7 +1267,7 @@ void UmmaMatrix::init(const double *M, int n_, cudaStream_t s) {
 void UmmaMatrix::release(cudaStream_t s) { dev_free_p(dev, s); }
 
 void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const UmmaMatrix *M2,
-                         int mode, int ncomp, int planes, cudaStream_t s) {
+                         int mode, int ncomp, int planes, cudaStream_t s, bool persistent) {
     BINDER_CHECK(b.n == M1.n, "matrix / axis length mismatch");
     BINDER_CHECK(planes == 1 || planes == 2, "planes must be 1 (TF32) or 2 (3xTF32)");
     UArgs a{};
@@ -813,6 +1277,27 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
     for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
     a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.comp0 = b.comp0; a.skip = b.skip;
+    a.ncomp = ncomp;
+    if (persistent && mode != kEpiSpectral) {
+        BINDER_CHECK(mode != kEpiSpectralOut || b.outer == 1,
+                     "prior scaling runs on the outermost axis");
+        switch (mode) {
+            case kEpiNone:
+                if (planes == 2) launch_pt<kEpiNone, 2>(a, s);
+                else launch_pt<kEpiNone, 1>(a, s);
+                break;
+            case kEpiPositions:
+                if (planes == 2) launch_pt<kEpiPositions, 2>(a, s);
+                else launch_pt<kEpiPositions, 1>(a, s);
+                break;
+            case kEpiSpectralOut:
+                if (planes == 2) launch_pt<kEpiSpectralOut, 2>(a, s);
+                else launch_pt<kEpiSpectralOut, 1>(a, s);
+                break;
+            default: BINDER_CHECK(false, "unsupported epilogue on the tensor-core path");
+        }
+        return;
+    }
 #define BINDER_UMMA_CASE(MODE)                                                    \
     case MODE:                                                                    \
         if (planes == 2) launch_ws<MODE, 2>(a, ncomp, s);                         \

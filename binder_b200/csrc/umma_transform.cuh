@@ -23,7 +23,9 @@ enum TransformPrecision : int {
 };
 
 // One pass on the tensor cores: modes kEpiNone, kEpiPositions, kEpiSpectral (M2 = inverse).
+// persistent: one launch for all ncomp components, one CTA per SM walking the tiles with a
+// double-buffered TMEM accumulator (modes kEpiNone, kEpiPositions, kEpiSpectralOut)
 void launch_axis_pass_tc(const AxisArgs<float> &a, const UmmaMatrix &M1, const UmmaMatrix *M2,
-                         int mode, int ncomp, int planes, cudaStream_t s);
+                         int mode, int ncomp, int planes, cudaStream_t s, bool persistent = false);
 
 }  // namespace binder

@@ -104,3 +104,13 @@ def test_thin_images_match_oracle(core, oracle, shape):
     assert st[2] == pytest.approx(lpt, rel=2e-4)
     np.testing.assert_allclose(reg.get_final_locations_as_numpy_array().ravel(), final, rtol=0,
                                atol=2e-4)
+
+
+@pytest.mark.parametrize("shape", [(12, 14, 10), (17, 3, 33), (7, 5, 9)])
+def test_persistent_passes_match_oracle(core, oracle, shape, monkeypatch):
+    """The persistent tensor-core pass kernel (BINDER_B200_PERSISTENT=1: all components in one
+    launch, one CTA per SM, double-buffered TMEM accumulator, cp.async-staged A chunks) gives the
+    oracle's M-step like the default per-tile kernel."""
+    monkeypatch.setenv("BINDER_B200_PERSISTENT", "1")
+    c = make_case(shape=shape, K=8, L=6, seed=sum(shape) + 1)
+    one_iteration(core, oracle, c)
