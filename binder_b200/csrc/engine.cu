@@ -454,8 +454,10 @@ void Registration::set_ssd_likelihood(int bins, double sigma2, int shift_scale, 
     colmax0_ = dalloc<float>((size_t)bins, s);
     SsdState h{};
     h.sigma2 = sigma2;
-    h.shift = shift_scale ? shift : 0.0;
-    h.scale = shift_scale ? scale : 1.0;
+    // kept as given with shiftScale 0 too: the likelihood then ignores them, and
+    // get_likelihood_parameters reports them (SSDLikelihood.cpp:328-334)
+    h.shift = shift;
+    h.scale = scale;
     h.alpha0 = alpha0;
     h.beta0 = beta0;
     h.shift_scale = shift_scale ? 1 : 0;

@@ -139,6 +139,8 @@ def ref_lib():
     r.ref_ssdf_update.argtypes = [_dp, _dp, _dp, _dp, i, d, d, i, i] + [i] * 6 + \
         [i, _ip, _dp, _dp, _dp]
     r.ref_ssdf_update.restype = d
+    r.ref_em.argtypes = [_dp, _dp, _dp] + [i] * 7 + [d, _dp, _dp, _dp, _dp, i, d, _dp, i, i, _dp,
+                                                      _ip, _ip, i, d, i, _dp, _dp]
     return r
 
 
@@ -498,4 +500,32 @@ def ssdf_update(params, nodes, nshape, acc, update=True):
     """update_parameters (when update) and compute_cost; params is updated in place."""
     return lib().orc_ssdf_update(C.addressof(params), _c64(nodes).ravel(), *nshape, *acc,
                                  int(update))
+
+
+def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxels, max_iter,
+           mi=None, ssd=None, spline_order=3, non_zero_voxels=None, th=-1e30, update=True):
+    """The reference's own Registration::EM (compiled in oracle/_ref; R = ref_lib()).  mi =
+    (alpha, theta[K][L]) or ssd = (bins, sigmaSq, shiftScale, scale, shift, alpha_0, beta_0).
+    Returns (final [V*N], likelihood parameters)."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    V = nx * ny * nz
+    fl = _c64(final_locations).ravel()
+    vp = _c64(voxel_pos).ravel()
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    out = np.zeros(V * N)
+    if mi is not None:
+        alpha, theta = mi
+        K, L = np.asarray(theta).shape
+        lk, th_arr, ssd_arr, npar = 0, _c64(theta).ravel(), np.zeros(6), K * L
+    else:
+        K = L = int(ssd[0])
+        lk, alpha, th_arr, ssd_arr, npar = 1, 0.0, np.zeros(1), _c64(ssd[1:]), 2
+    params = np.zeros(max(npar, 2))
+    nzv = float(V if non_zero_voxels is None else non_zero_voxels)
+    R.ref_em(fl, vp, vp, nx, ny, nz, *nshape, int(spline_order), nzv, g, np.ones(3), np.ones(3),
+             _c64(D).ravel(), lk, float(alpha), th_arr, K, L, ssd_arr, _c32i(nodes).ravel(),
+             _c32i(voxels).ravel(), int(max_iter), float(th), int(update), out, params)
+    return out, params[:npar]
 

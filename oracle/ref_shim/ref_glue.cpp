@@ -8,6 +8,7 @@
 #include "MILikelihoodFilter.h"
 #include "SSDLikelihoodFilter.h"
 #include "NonLinearTransformation.h"
+#include "Registration.h"
 #include "Spline.h"
 #include "topology_correction_2D.h"
 #include "topology_correction_3D.h"
@@ -160,6 +161,32 @@ double ref_ssdf_update(const double *coeff, const double *sigma, const double *n
         sigma_out[m] = -(X * X) / (2.0 * (lm - base));
     }
     return cost;
+}
+
+// The reference's own EM driver (Registration.cpp:122-217) on one thread: construction,
+// setNonLinearTransformation, the MI likelihood (lk 0: theta [K][L]) or the SSD likelihood (lk 1:
+// ssd = {sigmaSq, shiftScale, scale, shift, alpha_0, beta_0}), EM(max_iter, th, update); returns
+// the final locations [V*N] and get_likelihood_parameters (theta [K*L], or {scale, shift}).
+void ref_em(const double *final_locations, const double *voxel_pos, const double *node_pos,
+            int nx, int ny, int nz, int nxn, int nyn, int nzn, int spline_order,
+            double non_zero_voxels, const double gamma[3], const double rho[3],
+            const double eta[3], const double *D, int lk, double alpha, const double *theta,
+            int K, int L, const double *ssd, const int *nodes, const int *voxels, int max_iter,
+            double th, int update, double *final_out, double *params_out) {
+    Registration r(final_locations, 1, voxel_pos, node_pos, nx, ny, nz, nxn, nyn, nzn,
+                   spline_order, non_zero_voxels);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], rho[0], rho[1], rho[2], eta[0],
+                                 eta[1], eta[2], D);
+    if (lk == 0)
+        r.setMILikelihood(alpha, theta, K, L, 1, nodes, voxels);
+    else
+        r.setSSDLikelihood(K, 1, ssd[0], (int)ssd[1], ssd[2], ssd[3], nodes, voxels, ssd[4],
+                           ssd[5]);
+    r.EM(max_iter, th, update != 0, false);
+    const auto f = r.get_final_locations();
+    std::memcpy(final_out, f.data(), sizeof(double) * f.size());
+    const auto p = r.get_likelihood_parameters();
+    std::memcpy(params_out, p.data(), sizeof(double) * p.size());
 }
 
 }  // extern "C"

@@ -1,10 +1,10 @@
 """Generate the golden fixtures in this directory from the reference's own CPU sources.
 
-The reference's Spline.cpp, MILikelihood.cpp, MILikelihoodFilter.cpp, SSDLikelihoodFilter.cpp,
-utils.cpp, DCT.cpp, FFT.cpp, NonLinearTransformation.cpp, topology_correction_3D.cpp and
-topology_correction_2D.cpp are compiled unmodified by oracle/Makefile into
-oracle/_ref/libbinder_ref.so (FFTW replaced by the project-written subset in oracle/ref_shim, and
-Eigen's Dense header, included but unused, by an empty file there).  This script feeds them seeded inputs and stores inputs and outputs as small
+The reference's Spline.cpp, MILikelihood.cpp, MILikelihoodFilter.cpp, SSDLikelihood.cpp,
+SSDLikelihoodFilter.cpp, Registration.cpp, utils.cpp, DCT.cpp, FFT.cpp,
+NonLinearTransformation.cpp, topology_correction_3D.cpp and topology_correction_2D.cpp are compiled
+unmodified by oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW and Eigen replaced by the
+project-written subsets in oracle/ref_shim, the affine / rigid transformations by stand-ins).  This script feeds them seeded inputs and stores inputs and outputs as small
 .npz files, so the parity tests are pinned to the reference even where its sources are absent.
 
 Run from the repository root:  python tests/golden/make_golden.py
@@ -219,6 +219,42 @@ def main():
                      key + "cost": scost})
     np.savez(os.path.join(HERE, "ssd_filter_ref.npz"), nshape=nshape, vshape=vshape, pairs=vxyz,
              posterior=post, alpha0=3.0, beta0=0.7, **ssdf)
+
+    # whole EM runs through the reference's own driver (Registration.cpp:122-217, one thread):
+    # MI in 3D and 2D, spline orders 1 and 2, SSD with both fits
+    from binder_b200.utils import bin_signal_robust, initialize_fourier_domain_smoothing
+    em = {}
+
+    def em_case(name, shape, K, L, seed, iters, ssd=None, order=3):
+        rs = np.random.default_rng(seed)
+        pair = phantoms.make_pair(shape, seed, bins=L, n_objects=10, axes=(2.0, 6.0), rms=1.0,
+                                  spacing=3.0)
+        v, _ = bin_signal_robust(pair.moving, K)
+        g = phantoms.identity_positions(shape).astype(np.float64)
+        d0 = g + phantoms.smooth_random_field(shape, 0.6, 3.0, rs)
+        th = rs.random((K, L)) + 0.05
+        th /= th.sum(1, keepdims=True)
+        D = initialize_fourier_domain_smoothing(shape, True, 2, len(shape))
+        gamma = (0.8, 0.6, 1.1)
+        vs = shape if len(shape) == 3 else shape + (1,)
+        out, par = pyoracle.ref_em(R, d0, g, D, gamma, vs, vs, v.astype(np.int32),
+                                   pair.u.astype(np.int32), iters,
+                                   mi=None if ssd else (2.0, th), ssd=ssd, spline_order=order)
+        em.update({f"{name}_shape": np.array(vs), f"{name}_K": K, f"{name}_L": L,
+                   f"{name}_iters": iters, f"{name}_order": order, f"{name}_d0": d0,
+                   f"{name}_grid": g, f"{name}_D": D, f"{name}_gamma": np.array(gamma),
+                   f"{name}_v": v.astype(np.int32), f"{name}_u": pair.u.astype(np.int32),
+                   f"{name}_theta": th, f"{name}_final": out, f"{name}_params": par,
+                   f"{name}_ssd": np.array(ssd if ssd else [0.0] * 7)})
+
+    em_case("mi3d", (12, 10, 9), 8, 6, 101, 6)
+    em_case("mi2d", (24, 20), 8, 6, 102, 6)
+    em_case("order1", (10, 9, 8), 8, 6, 103, 4, order=1)
+    em_case("order2", (10, 9, 8), 8, 6, 104, 4, order=2)
+    em_case("ssd0", (10, 9, 8), 16, 16, 105, 4, ssd=(16, 4.0, 0, 0.9, 0.5, 1.0, 1.0))
+    em_case("ssd1", (10, 9, 8), 16, 16, 106, 4, ssd=(16, 4.0, 1, 0.9, 0.5, 1.0, 1.0))
+    np.savez(os.path.join(HERE, "em_ref.npz"),
+             names=np.array(["mi3d", "mi2d", "order1", "order2", "ssd0", "ssd1"]), **em)
     print("golden fixtures written to", HERE)
 
 

@@ -247,3 +247,37 @@ def test_ssd_filter_matches_reference(oracle, rfa):
                                rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(np.array(p.sigma[:M]), g[k + "sigma_out"], rtol=1e-10)
     assert cost == pytest.approx(float(g[k + "cost"]), rel=1e-10)
+
+
+def test_em_runs_match_reference_driver(oracle):
+    """Whole EM runs (MI 3D and 2D, spline orders 1 and 2, SSD with both fits) of the oracle against
+    the reference's own EM driver (Registration.cpp:122-217, compiled in oracle/_ref)."""
+    import math
+    g = golden("em_ref.npz")
+    sig = {3: math.sqrt(9.0 / (8.0 * math.pi)), 2: math.sqrt(8.0 / (9.0 * math.pi)), 1: 0.4}
+    for name in g["names"]:
+        vs = tuple(int(t) for t in g[f"{name}_shape"])
+        K, L, it = int(g[f"{name}_K"]), int(g[f"{name}_L"]), int(g[f"{name}_iters"])
+        order = int(g[f"{name}_order"])
+        oracle.set_spline_order(order)
+        try:
+            if name.startswith("ssd"):
+                s = g[f"{name}_ssd"]
+                p = oracle.SSDParams(int(s[2]), s[1], s[4], s[3], s[5], s[6])
+                n, final, _ = oracle.ssd_em(g[f"{name}_d0"], g[f"{name}_grid"], g[f"{name}_u"],
+                                            g[f"{name}_v"], p, g[f"{name}_D"],
+                                            g[f"{name}_gamma"], sig[order], vs, vs, K, L,
+                                            float(np.prod(vs)), it, -1e30)
+                np.testing.assert_allclose([p.scale, p.shift], g[f"{name}_params"], rtol=1e-12,
+                                           err_msg=name)
+            else:
+                n, final, theta, _ = oracle.em(g[f"{name}_d0"], g[f"{name}_grid"], g[f"{name}_u"],
+                                               g[f"{name}_v"], g[f"{name}_theta"], 2.0,
+                                               g[f"{name}_D"], g[f"{name}_gamma"], sig[order], vs,
+                                               vs, K, L, float(np.prod(vs)), it, -1e30)
+                np.testing.assert_allclose(theta, g[f"{name}_params"], rtol=0, atol=1e-13,
+                                           err_msg=name)
+        finally:
+            oracle.set_spline_order(3)
+        assert n == it
+        np.testing.assert_allclose(final, g[f"{name}_final"], rtol=0, atol=1e-11, err_msg=name)
