@@ -141,6 +141,9 @@ def ref_lib():
     r.ref_ssdf_update.restype = d
     r.ref_em.argtypes = [_dp, _dp, _dp] + [i] * 7 + [d, _dp, _dp, _dp, _dp, i, d, _dp, i, i, _dp,
                                                       _ip, _ip, i, d, i, _dp, _dp]
+    r.ref_em_filter.argtypes = [_dp, _dp] + [i] * 7 + [d, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
+                                                       _dp, _dp, _dp, _dp, i, d, d, i, i, d, i,
+                                                       _dp, _dp]
     return r
 
 
@@ -528,4 +531,36 @@ def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxel
              _c64(D).ravel(), lk, float(alpha), th_arr, K, L, ssd_arr, _c32i(nodes).ravel(),
              _c32i(voxels).ravel(), int(max_iter), float(th), int(update), out, params)
     return out, params[:npar]
+
+
+def ref_em_filter(R, final_locations, voxel_pos, D, gamma, vshape, max_iter, mi=None, ssd=None,
+                  th=-1e30, update=True):
+    """The reference's Registration::EM with setMILikelihoodFilter (mi = (alpha, theta[M][K][L],
+    nodes, voxels)) or setSSDLikelihoodFilter (ssd = (coeff[M][F], sigma[M], fnodes, fvoxels, rfa,
+    alpha_0, beta_0)).  Returns (final [V*N], theta or coeff)."""
+    nx, ny, nz = vshape
+    N = 2 if nz == 1 else 3
+    out = np.zeros(nx * ny * nz * N)
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    z, zi = np.zeros(1), np.zeros(1, np.int32)
+    if mi is not None:
+        alpha, theta, nodes, voxels = mi
+        M, K, L = np.asarray(theta).shape
+        params = np.zeros(M * K * L)
+        R.ref_em_filter(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz, nx,
+                        ny, nz, 3, float(nx * ny * nz), g, _c64(D).ravel(), 2, float(alpha),
+                        _c64(theta).ravel(), K, L, M, _c32i(nodes).ravel(), _c32i(voxels).ravel(),
+                        z, z, z, z, 0, 1.0, 1.0, 1, int(max_iter), float(th), int(update), out,
+                        params)
+    else:
+        coeff, sigma, fnodes, fvoxels, rfa, a0, b0 = ssd
+        M, F = np.asarray(coeff).shape
+        params = np.zeros(M * F)
+        R.ref_em_filter(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz, nx,
+                        ny, nz, 3, float(nx * ny * nz), g, _c64(D).ravel(), 3, 2.0, z, 1, 1, M, zi,
+                        zi, _c64(coeff).ravel(), _c64(sigma).ravel(), _c64(fnodes).ravel(),
+                        _c64(fvoxels).ravel(), int(rfa), float(a0), float(b0), F, int(max_iter),
+                        float(th), int(update), out, params)
+    return out, params
 

@@ -189,4 +189,28 @@ void ref_em(const double *final_locations, const double *voxel_pos, const double
     std::memcpy(params_out, p.data(), sizeof(double) * p.size());
 }
 
+// Registration::EM with a filter likelihood: lk 2 = setMILikelihoodFilter(alpha, theta [M][K][L],
+// nodes, voxels (int bins), K, L, M); lk 3 = setSSDLikelihoodFilter(coeff [M][F], sigma [M],
+// fnodes, fvoxels (features), rfa, alpha_0, beta_0, M, F).  params_out: theta or coeff.
+void ref_em_filter(const double *final_locations, const double *voxel_pos, int nx, int ny, int nz,
+                   int nxn, int nyn, int nzn, int spline_order, double non_zero_voxels,
+                   const double gamma[3], const double *D, int lk, double alpha,
+                   const double *theta, int K, int L, int M, const int *nodes, const int *voxels,
+                   const double *coeff, const double *sigma, const double *fnodes,
+                   const double *fvoxels, int rfa, double alpha0, double beta0, int F,
+                   int max_iter, double th, int update, double *final_out, double *params_out) {
+    Registration r(final_locations, 1, voxel_pos, voxel_pos, nx, ny, nz, nxn, nyn, nzn,
+                   spline_order, non_zero_voxels);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], 1, 1, 1, 1, 1, 1, D);
+    if (lk == 2)
+        r.setMILikelihoodFilter(alpha, theta, 1, nodes, voxels, K, L, M);
+    else
+        r.setSSDLikelihoodFilter(coeff, 1, sigma, fnodes, fvoxels, rfa, alpha0, beta0, M, F);
+    r.EM(max_iter, th, update != 0, false);
+    const auto f = r.get_final_locations();
+    std::memcpy(final_out, f.data(), sizeof(double) * f.size());
+    const auto p = r.get_likelihood_parameters();
+    std::memcpy(params_out, p.data(), sizeof(double) * p.size());
+}
+
 }  // extern "C"

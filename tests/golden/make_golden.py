@@ -255,6 +255,38 @@ def main():
     em_case("ssd1", (10, 9, 8), 16, 16, 106, 4, ssd=(16, 4.0, 1, 0.9, 0.5, 1.0, 1.0))
     np.savez(os.path.join(HERE, "em_ref.npz"),
              names=np.array(["mi3d", "mi2d", "order1", "order2", "ssd0", "ssd1"]), **em)
+
+    # EM runs with the filter likelihoods through the reference's driver (3 iterations each)
+    from scipy import ndimage as ndi
+    rs = np.random.default_rng(107)
+    shape = (10, 9, 8)
+    V = int(np.prod(shape))
+    g = phantoms.identity_positions(shape).astype(np.float64)
+    d0 = g + phantoms.smooth_random_field(shape, 0.6, 3.0, rs)
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3)
+    gamma = np.array([0.8, 0.6, 1.1])
+    M, K, L = 2, 6, 5
+    smooth = np.stack([ndi.gaussian_filter(rs.normal(0, 1, shape), 1.5) for _ in range(2)], -1)
+    bins_n = np.clip(((smooth - smooth.min()) / np.ptp(smooth) * K).astype(np.int32), 0, K - 1)
+    bins_v = np.clip((np.roll(smooth, 1, 0) - smooth.min()) / np.ptp(smooth) * L, 0,
+                     L - 1).astype(np.int32)
+    th = rs.random((M, K, L)) + 0.05
+    th /= th.sum(-1, keepdims=True)
+    mif_out, mif_par = pyoracle.ref_em_filter(R, d0, g, D, gamma, shape, 3,
+                                              mi=(2.0, th, bins_n.ravel(), bins_v.ravel()))
+    Mf, F = 2, 3
+    fn = np.stack([ndi.gaussian_filter(rs.normal(0, 1, shape), 1.5) * 6.0 + f for f in range(F)], -1)
+    fv = fn[..., :Mf] @ rs.normal(0, 1, (Mf, Mf)).T + rs.normal(0, 0.3, shape + (Mf,))
+    coeff = rs.normal(0.0, 1.0, (Mf, F))
+    sig = rs.random(Mf) * 1.5 + 0.5
+    ssdf_out, ssdf_par = pyoracle.ref_em_filter(R, d0, g, D, gamma, shape, 3,
+                                                ssd=(coeff, sig, fn.reshape(-1, F),
+                                                     fv.reshape(-1, Mf), 0, 2.0, 0.5))
+    np.savez(os.path.join(HERE, "em_filter_ref.npz"), shape=np.array(shape), d0=d0, grid=g, D=D,
+             gamma=gamma, iters=3, mif_theta=th, mif_nodes=bins_n.ravel(),
+             mif_voxels=bins_v.ravel(), mif_final=mif_out, mif_params=mif_par, ssdf_coeff=coeff,
+             ssdf_sigma=sig, ssdf_nodes=fn.reshape(-1, F), ssdf_voxels=fv.reshape(-1, Mf),
+             ssdf_alpha0=2.0, ssdf_beta0=0.5, ssdf_final=ssdf_out, ssdf_params=ssdf_par)
     print("golden fixtures written to", HERE)
 
 

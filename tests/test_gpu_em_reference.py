@@ -37,3 +37,29 @@ def test_em_matches_reference_driver(core, name):
         np.testing.assert_allclose(params, g[f"{name}_params"], rtol=1e-3, atol=1e-4)
     else:
         np.testing.assert_allclose(params, g[f"{name}_params"], rtol=2e-3, atol=1e-5)
+
+
+@pytest.mark.parametrize("lk", ["mif", "ssdf"])
+def test_filter_em_matches_reference_driver(core, lk):
+    g = golden("em_filter_ref.npz")
+    shape = tuple(int(t) for t in g["shape"])
+    it = int(g["iters"])
+    reg = core.Registration(g["d0"].astype(np.float32).reshape(-1, 3), 1,
+                            g["grid"].astype(np.float32).reshape(-1, 3),
+                            g["grid"].astype(np.float32).reshape(-1, 3), *shape, *shape, 3,
+                            float(np.prod(shape)))
+    reg.setNonLinearTransformation(*g["gamma"], 1, 1, 1, 1, 1, 1, g["D"].astype(np.float32))
+    if lk == "mif":
+        M, K, L = g["mif_theta"].shape
+        reg.setMILikelihoodFilter(2.0, g["mif_theta"].astype(np.float32), 1, g["mif_nodes"],
+                                  g["mif_voxels"], K, L, M)
+    else:
+        M, F = g["ssdf_coeff"].shape
+        reg.setSSDLikelihoodFilter(g["ssdf_coeff"], 1, g["ssdf_sigma"], g["ssdf_nodes"],
+                                   g["ssdf_voxels"], 0, float(g["ssdf_alpha0"]),
+                                   float(g["ssdf_beta0"]), M, F)
+    assert reg.EM(it, -1e30, 1, 0) == it
+    np.testing.assert_allclose(reg.get_final_locations_as_numpy_array().ravel(), g[f"{lk}_final"],
+                               rtol=0, atol=1e-3)
+    np.testing.assert_allclose(reg.get_likelihood_parameters(), g[f"{lk}_params"], rtol=1e-3,
+                               atol=1e-5)

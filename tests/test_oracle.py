@@ -281,3 +281,31 @@ def test_em_runs_match_reference_driver(oracle):
             oracle.set_spline_order(3)
         assert n == it
         np.testing.assert_allclose(final, g[f"{name}_final"], rtol=0, atol=1e-11, err_msg=name)
+
+
+def test_filter_em_runs_match_reference_driver(oracle):
+    """EM runs with the MI filter and SSD filter likelihoods: the oracle's E-steps and updates,
+    iterated with its smoothing, against the reference's own EM driver."""
+    import math
+    g = golden("em_filter_ref.npz")
+    shape = tuple(int(t) for t in g["shape"])
+    sig = math.sqrt(9.0 / (8.0 * math.pi))
+    M, K, L = g["mif_theta"].shape
+    d, th = g["d0"], g["mif_theta"]
+    for _ in range(int(g["iters"])):
+        _, dream, hist, _ = oracle.estep_filter(d, g["mif_voxels"], g["mif_nodes"], th, shape,
+                                                shape, K, L, M)
+        th = oracle.theta_map(hist, M * K, L, 2.0)
+        _, d = oracle.smooth(dream, g["grid"], g["D"], g["gamma"], sig, shape)
+    np.testing.assert_allclose(d, g["mif_final"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(th, g["mif_params"], rtol=0, atol=1e-13)
+    p = oracle.ssdf_params(g["ssdf_coeff"], g["ssdf_sigma"], 0, float(g["ssdf_alpha0"]),
+                           float(g["ssdf_beta0"]))
+    d = g["d0"]
+    for _ in range(int(g["iters"])):
+        _, dream, acc = oracle.ssdf_estep(d, g["ssdf_nodes"], g["ssdf_voxels"], p, shape, shape)
+        oracle.ssdf_update(p, g["ssdf_nodes"], shape, acc, True)
+        _, d = oracle.smooth(dream, g["grid"], g["D"], g["gamma"], sig, shape)
+    np.testing.assert_allclose(d, g["ssdf_final"], rtol=0, atol=1e-11)
+    Mf, F = g["ssdf_coeff"].shape
+    np.testing.assert_allclose(np.array(p.coeff[:Mf * F]), g["ssdf_params"], rtol=1e-10, atol=1e-12)
