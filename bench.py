@@ -13,8 +13,9 @@ Inputs are seeded synthetic volumes standing in for the reference's unpublished 
   e2e   : the same through the public API with host buffers: create the Registration from host
           arrays, set likelihood/prior, EM, topology correction, read the final field back.
 
-`--impl reference` times the reference algorithm's CPU implementation (the FP64 oracle port,
-OpenMP over all host cores) on a bounded sample of the same workload.  Under torchrun every rank
+`--impl reference` times the reference's own CPU implementation (BINDER/src/cpu's EM driver and
+classes, compiled in oracle/_ref with FFT-based DCTs in place of FFTW; OpenMP over all host cores)
+on a bounded sample of the same workload, or the FP64 oracle port where that library is absent.  Under torchrun every rank
 registers its own pair (replicas; no data-path collective) and rank 0 reports the max over ranks.
 """
 from __future__ import annotations
@@ -95,13 +96,56 @@ def run_gibbs(core, rank, chains, dist):
             "cpu_baseline": cpu}
 
 
+REF_NOTE = ("the reference's own CPU sources (BINDER/src/cpu: Registration.cpp and the classes it "
+            "drives) compiled in oracle/_ref, with FFT-based DCTs in place of FFTW")
+
+
+def ref_lib():
+    """The reference's CPU sources compiled in oracle/_ref, or None where that library is absent
+    (the CPU legs then time the FP64 oracle port instead)."""
+    from oracle import pyoracle
+    try:
+        return pyoracle.ref_lib()
+    except OSError:
+        return None
+
+
+class stdout_to_stderr:
+    """The reference prints progress on stdout; this script's stdout carries one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def cpu_gibbs(pair, grid, D, g, sweeps=2):
-    """Sweeps/s of the FP64 oracle sampler (OpenMP, all host cores) on the same 96^3 pair."""
+    """Sweeps/s of the reference's own sampler (Registration::sampler, all host cores) on the same
+    96^3 pair, or of the FP64 oracle sampler where the reference library is absent."""
     from oracle import pyoracle
     threads = os.cpu_count() or 1
-    pyoracle.set_threads(threads)
     shape = GIBBS_SHAPE
     x = grid.astype(np.float64)
+    R = ref_lib()
+    if R is not None:
+        theta = np.full(BINS * BINS, 1.0 / BINS)
+        with stdout_to_stderr():
+            t = R.ref_sampler_seconds(np.ascontiguousarray(x).ravel(),
+                                      np.ascontiguousarray(x).ravel(), *shape,
+                                      np.array([g, g, g], np.float64),
+                                      np.ascontiguousarray(D, np.float64).ravel(), ALPHA, theta,
+                                      BINS, BINS, np.ascontiguousarray(pair.v, np.int32).ravel(),
+                                      np.ascontiguousarray(pair.u, np.int32).ravel(), GIBBS_SEED,
+                                      0, sweeps, 1, 1, 1, 1, 1, threads)
+        return {"value": sweeps / t, "unit": "sweeps/s", "cores": threads, "kind": "reference",
+                "sample": f"{sweeps} sweeps of the 96^3 pair from the identity grid ({t:.2f} s) "
+                          f"by {REF_NOTE}"}
+    pyoracle.set_threads(threads)
     t0 = time.perf_counter()
     pyoracle.sampler(x, x, x, pair.u, pair.v, np.full(BINS * BINS, 1.0 / BINS), ALPHA,
                      D.astype(np.float64), (g, g, g), math.sqrt(9.0 / (8.0 * math.pi)),
@@ -184,17 +228,26 @@ def run_2d(core, rank, em_iters, dist):
     if rank == 0:
         from oracle import pyoracle
         threads = os.cpu_count() or 1
-        pyoracle.set_threads(threads)
         vshape = shape + (1,)
         it = em_iters
-        t0 = time.perf_counter()
-        pyoracle.em(grid, grid, pair.u, pair.v, theta, ALPHA, D, (g, g, g),
-                    math.sqrt(9.0 / (8.0 * math.pi)), vshape, vshape, C1_BINS, C1_BINS, nzv, it,
-                    -1e300)
-        t = time.perf_counter() - t0
+        R = ref_lib()
+        if R is not None:
+            tm = []
+            with stdout_to_stderr():
+                pyoracle.ref_em(R, grid, grid, D, (g, g, g), vshape, vshape, pair.v, pair.u, it,
+                                mi=(ALPHA, theta.reshape(C1_BINS, C1_BINS)), non_zero_voxels=nzv,
+                                threads=threads, timing=tm)
+            t, kind, who = tm[0], "reference", f" by {REF_NOTE}"
+        else:
+            pyoracle.set_threads(threads)
+            t0 = time.perf_counter()
+            pyoracle.em(grid, grid, pair.u, pair.v, theta, ALPHA, D, (g, g, g),
+                        math.sqrt(9.0 / (8.0 * math.pi)), vshape, vshape, C1_BINS, C1_BINS, nzv,
+                        it, -1e300)
+            t, kind, who = time.perf_counter() - t0, "port", ""
         cpu = {"value": 1.0 / t, "unit": "registrations/s", "cores": threads,
-               "kind": "port", "sample": f"{it} EM iterations of the 128x128 pair ({t:.2f} s), "
-                                         "topology excluded"}
+               "kind": kind, "sample": f"{it} EM iterations of the 128x128 pair ({t:.2f} s)"
+                                       f"{who}, topology excluded"}
     h2d = grid.nbytes + D.nbytes + theta.nbytes + pair.u.nbytes + pair.v.nbytes
     return {"metric": f"2D registrations/s (128x128 MI pair, 32 bins, {em_iters} EM iterations + "
                       "topology correction)",
@@ -454,26 +507,40 @@ def read_profile_traffic():
 
 
 def cpu_time_em_iteration(inp, threads):
-    """Seconds of one EM iteration (E-step + theta update + DCT M-step) of the FP64 oracle."""
+    """(seconds, kind) of one EM iteration (E-step + theta update + DCT M-step) by the
+    reference's own EM driver (the EM call alone), or by the FP64 oracle port where the reference
+    library is absent."""
     from oracle import pyoracle
-    pyoracle.set_threads(threads)
     pair = inp["pair"]
     grid = inp["grid"].astype(np.float64)
+    R = ref_lib()
+    if R is not None:
+        tm = []
+        with stdout_to_stderr():
+            pyoracle.ref_em(R, grid, grid, inp["D"], inp["gamma"], SHAPE, SHAPE, pair.v, pair.u,
+                            1, mi=(ALPHA, inp["theta"].astype(np.float64).reshape(BINS, BINS)),
+                            non_zero_voxels=inp["nzv"], threads=threads, timing=tm)
+        return tm[0], "reference"
+    pyoracle.set_threads(threads)
     t0 = time.perf_counter()
     pyoracle.em(grid, grid, pair.u, pair.v, inp["theta"].astype(np.float64), ALPHA, inp["D"],
                 inp["gamma"], math.sqrt(9.0 / (8.0 * math.pi)), SHAPE, SHAPE, BINS, BINS,
                 inp["nzv"], 1, -1e300)
-    return time.perf_counter() - t0
+    return time.perf_counter() - t0, "port"
+
+
+def cpu_sample_text(kind, threads, t, em_iters, tail=""):
+    who = f" by {REF_NOTE}" if kind == "reference" else " by the FP64 oracle port"
+    return (f"1 EM iteration of the 160x192x160 pair{who} on {threads} threads ({t:.2f} s{tail}), "
+            f"extrapolated to {em_iters} iterations; topology correction excluded (it would only "
+            "lower the CPU figure)")
 
 
 def cpu_baseline(inp, em_iters):
     threads = os.cpu_count() or 1
-    t = cpu_time_em_iteration(inp, threads)
+    t, kind = cpu_time_em_iteration(inp, threads)
     return {"value": 1.0 / (em_iters * t), "unit": "registrations/s", "cores": threads,
-            "kind": "port",
-            "sample": f"1 EM iteration of the 160x192x160 pair on {threads} threads "
-                      f"({t:.2f} s), extrapolated to {em_iters} iterations; topology "
-                      "correction excluded (it would only lower the CPU figure)"}
+            "kind": kind, "sample": cpu_sample_text(kind, threads, t, em_iters)}
 
 
 def run_reference(args, rank, world):
@@ -483,12 +550,11 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     for _ in range(max(0, min(args.warmup, 1))):
         pass  # the oracle has no warm-up state; a warm-up would only repeat the bounded sample
-    times = [cpu_time_em_iteration(inp, threads) for _ in range(max(1, min(args.steps, 2)))]
+    runs = [cpu_time_em_iteration(inp, threads) for _ in range(max(1, min(args.steps, 2)))]
+    times, kind = [r[0] for r in runs], runs[0][1]
     t = statistics.median(times)
     value = 1.0 / (args.em_iters * t)
-    sample = (f"1 EM iteration of the 160x192x160 pair per step on {threads} threads "
-              f"({t:.2f} s median of {len(times)}), extrapolated to {args.em_iters} iterations; "
-              "topology correction excluded")
+    sample = cpu_sample_text(kind, threads, t, args.em_iters, f" median of {len(times)} steps")
     return {"metric": metric(args.em_iters), "value": value, "unit": "registrations/s", "n_gpus": world,
             "steps": len(times), "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -496,7 +562,7 @@ def run_reference(args, rank, world):
             "config": {"workload": "C2 3D MI registration 160x192x160, 64 bins",
                        "em_iterations": args.em_iters, "parallelism": "host cores"},
             "cpu_baseline": {"value": value, "unit": "registrations/s", "cores": threads,
-                             "kind": "port", "sample": sample},
+                             "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "registrations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "gibbs": reference_gibbs()}

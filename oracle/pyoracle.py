@@ -140,7 +140,11 @@ def ref_lib():
         [i, _ip, _dp, _dp, _dp]
     r.ref_ssdf_update.restype = d
     r.ref_em.argtypes = [_dp, _dp, _dp] + [i] * 7 + [d, _dp, _dp, _dp, _dp, i, d, _dp, i, i, _dp,
-                                                      _ip, _ip, i, d, i, _dp, _dp]
+                                                      _ip, _ip, i, d, i, _dp, _dp, i,
+                                                      C.POINTER(d)]
+    r.ref_sampler_seconds.argtypes = [_dp, _dp, i, i, i, _dp, _dp, d, _dp, i, i, _ip, _ip] + \
+        [i] * 9
+    r.ref_sampler_seconds.restype = d
     r.ref_em_filter.argtypes = [_dp, _dp] + [i] * 7 + [d, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
                                                        _dp, _dp, _dp, _dp, i, d, d, i, i, d, i,
                                                        _dp, _dp]
@@ -506,10 +510,11 @@ def ssdf_update(params, nodes, nshape, acc, update=True):
 
 
 def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxels, max_iter,
-           mi=None, ssd=None, spline_order=3, non_zero_voxels=None, th=-1e30, update=True):
+           mi=None, ssd=None, spline_order=3, non_zero_voxels=None, th=-1e30, update=True,
+           threads=1, timing=None):
     """The reference's own Registration::EM (compiled in oracle/_ref; R = ref_lib()).  mi =
     (alpha, theta[K][L]) or ssd = (bins, sigmaSq, shiftScale, scale, shift, alpha_0, beta_0).
-    Returns (final [V*N], likelihood parameters)."""
+    Returns (final [V*N], likelihood parameters); timing (a list) receives the EM call's seconds."""
     nx, ny, nz = vshape
     N = 2 if nz == 1 else 3
     V = nx * ny * nz
@@ -527,9 +532,13 @@ def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxel
         lk, alpha, th_arr, ssd_arr, npar = 1, 0.0, np.zeros(1), _c64(ssd[1:]), 2
     params = np.zeros(max(npar, 2))
     nzv = float(V if non_zero_voxels is None else non_zero_voxels)
+    sec = C.c_double(0.0)
     R.ref_em(fl, vp, vp, nx, ny, nz, *nshape, int(spline_order), nzv, g, np.ones(3), np.ones(3),
              _c64(D).ravel(), lk, float(alpha), th_arr, K, L, ssd_arr, _c32i(nodes).ravel(),
-             _c32i(voxels).ravel(), int(max_iter), float(th), int(update), out, params)
+             _c32i(voxels).ravel(), int(max_iter), float(th), int(update), out, params,
+             int(threads), C.byref(sec))
+    if timing is not None:
+        timing.append(sec.value)
     return out, params[:npar]
 
 

@@ -7,8 +7,9 @@
  * (Y_k = 2 sum_j X_j cos(pi (2j+1) k / 2n)), REDFT01 the unnormalised DCT-III
  * (Y_k = X_0 + 2 sum_{j>0} X_j cos(pi j (2k+1) / 2n)), and the complex DFT is
  * Y_k = sum_j X_j exp(sign * 2 pi i jk / n), all applied separably over the dimensions of a
- * row-major array.  Transforms are evaluated directly (O(n) per output), in double precision;
- * planning flags, threads and wisdom are accepted and ignored (wisdom is never written to disk).
+ * row-major array, in double precision.  The DCTs run in O(n log n) on the plan's thread count
+ * (fftw_plan_with_nthreads); the complex DFTs are evaluated directly.  Planning flags and wisdom
+ * are accepted and ignored (wisdom is never written to disk).
  */
 #ifndef BINDER_ORACLE_FFTW_SHIM_H
 #define BINDER_ORACLE_FFTW_SHIM_H

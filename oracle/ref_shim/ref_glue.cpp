@@ -1,5 +1,6 @@
 // extern "C" entry points over the reference's own CPU classes, compiled from the unmodified
 // reference sources into oracle/_ref/libbinder_ref.so (test infrastructure: a checker only).
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -163,26 +164,31 @@ double ref_ssdf_update(const double *coeff, const double *sigma, const double *n
     return cost;
 }
 
-// The reference's own EM driver (Registration.cpp:122-217) on one thread: construction,
+// The reference's own EM driver (Registration.cpp:122-217) on `threads` threads: construction,
 // setNonLinearTransformation, the MI likelihood (lk 0: theta [K][L]) or the SSD likelihood (lk 1:
 // ssd = {sigmaSq, shiftScale, scale, shift, alpha_0, beta_0}), EM(max_iter, th, update); returns
-// the final locations [V*N] and get_likelihood_parameters (theta [K*L], or {scale, shift}).
+// the final locations [V*N], get_likelihood_parameters (theta [K*L], or {scale, shift}) and the
+// wall seconds of the EM call alone.
 void ref_em(const double *final_locations, const double *voxel_pos, const double *node_pos,
             int nx, int ny, int nz, int nxn, int nyn, int nzn, int spline_order,
             double non_zero_voxels, const double gamma[3], const double rho[3],
             const double eta[3], const double *D, int lk, double alpha, const double *theta,
             int K, int L, const double *ssd, const int *nodes, const int *voxels, int max_iter,
-            double th, int update, double *final_out, double *params_out) {
-    Registration r(final_locations, 1, voxel_pos, node_pos, nx, ny, nz, nxn, nyn, nzn,
+            double th, int update, double *final_out, double *params_out, int threads,
+            double *seconds) {
+    Registration r(final_locations, threads, voxel_pos, node_pos, nx, ny, nz, nxn, nyn, nzn,
                    spline_order, non_zero_voxels);
     r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], rho[0], rho[1], rho[2], eta[0],
                                  eta[1], eta[2], D);
     if (lk == 0)
-        r.setMILikelihood(alpha, theta, K, L, 1, nodes, voxels);
+        r.setMILikelihood(alpha, theta, K, L, threads, nodes, voxels);
     else
-        r.setSSDLikelihood(K, 1, ssd[0], (int)ssd[1], ssd[2], ssd[3], nodes, voxels, ssd[4],
+        r.setSSDLikelihood(K, threads, ssd[0], (int)ssd[1], ssd[2], ssd[3], nodes, voxels, ssd[4],
                            ssd[5]);
+    const auto t0 = std::chrono::steady_clock::now();
     r.EM(max_iter, th, update != 0, false);
+    if (seconds)
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     const auto f = r.get_final_locations();
     std::memcpy(final_out, f.data(), sizeof(double) * f.size());
     const auto p = r.get_likelihood_parameters();
@@ -211,6 +217,24 @@ void ref_em_filter(const double *final_locations, const double *voxel_pos, int n
     std::memcpy(final_out, f.data(), sizeof(double) * f.size());
     const auto p = r.get_likelihood_parameters();
     std::memcpy(params_out, p.data(), sizeof(double) * p.size());
+}
+
+// Registration::sampler (Registration.cpp:515-642) with the MI likelihood on `threads` threads:
+// N_b + N_s sweeps with the given switches; returns the wall seconds of the sampler call
+double ref_sampler_seconds(const double *final_locations, const double *voxel_pos, int nx, int ny,
+                           int nz, const double gamma[3], const double *D, double alpha,
+                           const double *theta, int K, int L, const int *nodes, const int *voxels,
+                           int seed, int N_b, int N_s, int sample_gamma, int every,
+                           int posteriors, int lik_params, int transf_params, int threads) {
+    Registration r(final_locations, threads, voxel_pos, voxel_pos, nx, ny, nz, nx, ny, nz, 3,
+                   (double)nx * ny * nz);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], 1, 1, 1, 1, 1, 1, D);
+    r.setMILikelihood(alpha, theta, K, L, threads, nodes, voxels);
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = r.sampler(seed, N_b, N_s, sample_gamma, every, posteriors, lik_params,
+                               transf_params);
+    (void)res;
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 }  // extern "C"
