@@ -23,8 +23,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 # per-file extra flags: the FP64 Jacobian/topology kernels must not contract a*b+c into FMA so
 # the determinants match the reference's CPU evaluation bit for bit
 EXTRA = {"topology.cu": ["-fmad=false"]}
-SOURCES = ["layout.cu", "transform.cu", "umma_transform.cu", "estep.cu", "topology.cu",
-           "resample.cu", "engine.cu", "multires.cu", "preprocess.cu", "capi.cu"]
+SOURCES = ["layout.cu", "transform.cu", "umma_transform.cu", "mstep2d.cu", "estep.cu",
+           "topology.cu", "resample.cu", "engine.cu", "multires.cu", "preprocess.cu", "capi.cu"]
 
 
 def _newest(paths):

@@ -92,6 +92,18 @@ __host__ __device__ __forceinline__ u32x4 philox_draw(uint64_t seed, uint32_t in
 __host__ __device__ __forceinline__ float u01_f24(uint32_t x) {
     return ((float)(x >> 9) + 0.5f) * (1.0f / 8388608.0f);
 }
+// prior-sampling normal for DCT coefficient i of component comp (Box-Muller on Philox tag 2 for
+// the x / y components, tag 3 for z; the oracle draws the same stream)
+__device__ __forceinline__ float dct_prior_normal(uint64_t seed, uint32_t i, uint32_t sweep,
+                                                  uint32_t chain, int comp) {
+    const u32x4 r = philox_draw(seed, i, sweep, comp < 2 ? 2u : 3u, chain);
+    const float u1 = u01_f24(r.x), u2 = u01_f24(r.y);
+    const float rad = sqrtf(-2.0f * logf(u1));
+    float sn, cs;
+    sincospif(2.0f * u2, &sn, &cs);
+    return comp == 1 ? rad * sn : rad * cs;
+}
+
 // uniform in (0,1) with 32 random bits in double
 __host__ __device__ __forceinline__ double u01_d32(uint32_t x) {
     return ((double)x + 0.5) * (1.0 / 4294967296.0);

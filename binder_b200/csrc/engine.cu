@@ -8,6 +8,7 @@
 
 #include "engine.cuh"
 #include "layout.cuh"
+#include "mstep2d.cuh"
 
 namespace binder {
 
@@ -139,6 +140,11 @@ void MStep::init(int x, int y, int z, cudaStream_t s) {
     t2 = dalloc<float>((size_t)V * 3, s);
     precision = default_precision();
     persistent = default_persistent();
+    {
+        const char *e = std::getenv("BINDER_B200_FUSED2D");
+        const bool off = e && e[0] == '0' && e[1] == 0;
+        fused2d = !off && z == 1 && x <= kM2dMaxN && y <= kM2dMaxN;
+    }
     for (int i = 0; i < 2; ++i) {
         BINDER_CUDA(cudaStreamCreate(&side[i]));
         BINDER_CUDA(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
@@ -183,6 +189,15 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     a.nz = nz;
     const int ncomp = nz == 1 ? 2 : 3;
     a.dims = ncomp;
+    if (fused2d) {
+        a.comp0 = 0;
+        a.xpos = xpos;
+        a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
+        a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
+        for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
+        launch_mstep2d(a, r, d, nx, ny, dct.fwd[0], dct.inv[0], dct.fwd[1], dct.inv[1], s);
+        return;
+    }
     a.D = D; a.sigma2 = sigma2; a.sample = sample; a.want_raw = want_raw;
     a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];

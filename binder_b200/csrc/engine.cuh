@@ -31,6 +31,8 @@ struct MStep {
     // tensor-core passes: one CTA per 128-line tile with the components on their own streams, or
     // persistent (all components per launch, one CTA per SM; measured slower on B200)
     bool persistent = false;
+    // 2D images up to 128 x 128: the whole M-step in one launch (mstep2d.cu)
+    bool fused2d = false;
     // the tensor-core passes of components 1 and 2 run on their own streams (graph branches), so
     // one component's last partial wave of tiles overlaps the other components' passes
     cudaStream_t side[2] = {nullptr, nullptr};

@@ -65,12 +65,7 @@ __device__ __forceinline__ void gemm_tile(const T *__restrict__ M, int n, const 
 // prior-sampling normal for DCT coefficient i of component comp (matches the oracle's stream)
 __device__ __forceinline__ float prior_normal(uint64_t seed, uint32_t i, uint32_t sweep,
                                               uint32_t chain, int comp) {
-    const u32x4 r = philox_draw(seed, i, sweep, comp < 2 ? 2u : 3u, chain);
-    const float u1 = u01_f24(r.x), u2 = u01_f24(r.y);
-    const float rad = sqrtf(-2.0f * logf(u1));
-    float sn, cs;
-    sincospif(2.0f * u2, &sn, &cs);
-    return comp == 1 ? rad * sn : rad * cs;
+    return dct_prior_normal(seed, i, sweep, chain, comp);
 }
 
 template <typename T, int R, int MODE>

@@ -211,3 +211,22 @@ def test_registration_topology2d_on_device(core):
                                                           [1.0, 1.0], nx, ny)
     assert st["below_e1_before"] > 0 and st["below_e1_after"] == 0
     np.testing.assert_allclose(after, host.astype(np.float32), rtol=0, atol=1e-5)
+
+
+@pytest.mark.parametrize("fused", ["1", "0"])
+def test_small_image_m_step_kinds_match_oracle(core, oracle, fused, monkeypatch):
+    """Images up to 128 x 128 run the whole M-step as one cluster launch (mstep2d.cu);
+    BINDER_B200_FUSED2D=0 keeps the separate tensor-core passes.  Both give the oracle's
+    iteration, on a ragged shape whose rows and columns do not split evenly over the cluster."""
+    monkeypatch.setenv("BINDER_B200_FUSED2D", fused)
+    c = make_case2d(shape=(45, 38), seed=8)
+    vshape, K, L = c["vshape"], c["K"], c["L"]
+    reg = new_reg2d(core, c)
+    assert reg.EM(1, -1e30, 1, 0) == 1
+    mll, dream, hist, _ = oracle.estep(c["d0"].astype(np.float64), c["u"], c["v"],
+                                       c["theta"].astype(np.float64), vshape, vshape, K, L)
+    lpt, final = oracle.smooth(dream, c["grid"], c["D"], c["gamma"], SIGMA_CUBIC, vshape)
+    st = reg.iteration_stats()[0]
+    assert st[2] == pytest.approx(lpt, rel=2e-4)
+    np.testing.assert_allclose(reg.get_final_locations_as_numpy_array().ravel(), final, rtol=0,
+                               atol=2e-4)
