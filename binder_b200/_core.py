@@ -101,7 +101,9 @@ class Registration:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        # at interpreter shutdown the module's globals may already be gone; the process exit then
+        # releases the device memory
+        if h and callable(lib):
             lib().binder_registration_destroy(h)
             self._h = C.c_void_p()
 
@@ -319,7 +321,7 @@ class NonLinearTransformation:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and callable(lib):  # see Registration.__del__
             lib().binder_transform_destroy(h)
             self._h = C.c_void_p()
 
