@@ -55,7 +55,7 @@ class Pyramid:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and callable(lib):  # module globals may be gone at interpreter shutdown
             lib().binder_pyramid_destroy(h)
             self._h = C.c_void_p()
 
