@@ -252,13 +252,66 @@ __global__ void flag_cells_kernel(const double *Jc, int nx, int ny, int nz, doub
     }
 }
 
+// the limiter step of one flagged corner (topology_correction_3D.cpp:279-345,
+// topology_correction_2D.cpp:257-309): J the corner's N x N gradient matrix (column n2 read at
+// vertex n2), replaced by (1 - a) J + a I.  The reference steps
+// alpha by 0.1 (capped at 1) until det((1 - alpha) J + alpha I) lies in [e1, e2], at most 11
+// steps, then takes one step more.  The alphas are constants, so the 11 trial determinants are
+// evaluated independently (the same expressions the loop evaluates) and the first one in range
+// picks the step: a walk whose time is the latency of one corner after another gains the ILP.
+template <int N>
+__device__ __forceinline__ double detn(const double (&J)[N][N]) {
+    if constexpr (N == 2)
+        return J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    else
+        return det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0], J[2][1], J[2][2]);
+}
+
+template <int N>
+__device__ __forceinline__ void limit_corner(double (&J)[N][N], double e1, double e2,
+                                             bool &capped) {
+    constexpr int kSteps = 11;
+    double al[kSteps + 2];  // al[k]: alpha after k steps (constant-folded)
+    al[0] = 0.0;
+#pragma unroll
+    for (int k = 1; k < kSteps + 2; ++k) {
+        al[k] = al[k - 1] + 0.1;
+        if (al[k] > 1.0) al[k] = 1.0;
+    }
+    const double det0 = detn<N>(J);
+    // k steps taken (the first k whose determinant lies in [e1, e2]): the final alpha is al[k + 1]
+    double alpha = al[1];
+    if (det0 > e2 || det0 < e1) {
+        bool none = true;  // alpha == 1 (identity) tried as well: [e1, e2] misses 1
+        alpha = al[kSteps + 1];
+#pragma unroll
+        for (int t = kSteps; t >= 1; --t) {
+            const double a = al[t];
+            double Jn[N][N];
+            for (int n1 = 0; n1 < N; ++n1)
+                for (int n2 = 0; n2 < N; ++n2)
+                    Jn[n1][n2] = (1 - a) * J[n1][n2] + a * (n1 == n2 ? 1.0 : 0.0);
+            const double det = detn<N>(Jn);
+            if (!(det > e2 || det < e1)) {
+                alpha = al[t + 1];
+                none = false;
+            }
+        }
+        if (none) capped = true;
+    }
+    for (int n1 = 0; n1 < N; ++n1)
+        for (int n2 = 0; n2 < N; ++n2)
+            J[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+}
+
 // topology_correction_3D.cpp:247-332.  The reference visits cells in lexicographic order and a
 // cell's 8 corners in order; a cell reads and writes gradients only inside its 2x2x2 footprint,
 // so two cells interact only if they differ by at most 1 along every axis.  Level 4x + 2y + z
 // orders every such pair exactly as the lexicographic walk does and never puts two of them on
 // the same level, so processing levels in increasing order (cells of one level in parallel)
-// reproduces the sequential result exactly.  One CTA; levels are separated by __syncthreads.
-__global__ void __launch_bounds__(1024) limiter_kernel(const int *list, int *sorted, const double *Jc,
+// reproduces the sequential result exactly.  One CTA of 256 threads; levels are separated by
+// __syncthreads.
+__global__ void __launch_bounds__(256) limiter_kernel(const int *list, int *sorted, const double *Jc,
                                                        double *g, int nx, int ny, int nz,
                                                        double e1, double e2, int nlev, Red *red,
                                                        unsigned *flags) {
@@ -308,30 +361,9 @@ __global__ void __launch_bounds__(1024) limiter_kernel(const int *list, int *sor
                 double J[3][3];
                 for (int n1 = 0; n1 < 3; ++n1)
                     for (int n2 = 0; n2 < 3; ++n2) J[n1][n2] = g[(n1 * 3 + n2) * V + gp[n2]];
-                double alpha = 0.0;
-                double det = det3(J[0][0], J[0][1], J[0][2], J[1][0], J[1][1], J[1][2], J[2][0],
-                                  J[2][1], J[2][2]);
-                int steps = 0;
-                while (det > e2 || det < e1) {
-                    if (++steps > 11) {  // alpha == 1 (identity) already tried: [e1, e2] misses 1
-                        capped = true;
-                        break;
-                    }
-                    alpha += 0.1;
-                    if (alpha > 1.0) alpha = 1.0;
-                    double Jn[3][3];
-                    for (int n1 = 0; n1 < 3; ++n1)
-                        for (int n2 = 0; n2 < 3; ++n2)
-                            Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
-                    det = det3(Jn[0][0], Jn[0][1], Jn[0][2], Jn[1][0], Jn[1][1], Jn[1][2], Jn[2][0],
-                               Jn[2][1], Jn[2][2]);
-                }
-                alpha += 0.1;
-                if (alpha > 1.0) alpha = 1.0;
+                limit_corner<3>(J, e1, e2, capped);
                 for (int n1 = 0; n1 < 3; ++n1)
-                    for (int n2 = 0; n2 < 3; ++n2)
-                        g[(n1 * 3 + n2) * V + gp[n2]] =
-                            (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+                    for (int n2 = 0; n2 < 3; ++n2) g[(n1 * 3 + n2) * V + gp[n2]] = J[n1][n2];
             }
         }
         __syncthreads();
@@ -439,74 +471,163 @@ __global__ void flag_cells2d_kernel(const double *Jc, int nx, int ny, double e1,
 // only if they differ by at most 1 along both axes.  Level 2x + y orders every such pair as the
 // lexicographic walk does and never puts two of them on one level, so levels in increasing order
 // (cells of one level in parallel) reproduce the sequential result exactly.  Column n2 of a
-// corner's matrix is read at the corner's vertex with its n2 bit cleared.  One CTA.
-__global__ void __launch_bounds__(1024) limiter2d_kernel(const int *list, int *sorted,
-                                                         const double *Jc, double *g, int nx,
-                                                         int ny, double e1, double e2, int nlev,
-                                                         Red *red, unsigned *flags) {
-    extern __shared__ int sh[];
-    int *off = sh;             // nlev + 1
-    int *cur = sh + nlev + 1;  // nlev
+// corner's matrix is read at the corner's vertex with its n2 bit cleared, so a corner reads
+// nodes (0, vy) and (vx, 0) of its cell and node (1, 1) is never read.
+//
+// The walk is a chain of some 3 max(nx, ny) short levels, so its time is the chain's length times
+// the latency of one level.  One warp walks (a warp barrier per level), on shared-memory copies:
+// the block first gives every node a flagged corner reads a slot (a V-sized map, -1 between
+// calls), gathers those nodes' gradients and the cells' flagged-corner masks, and afterwards
+// scatters the gradients back.  More than kStageCells cells or kStageNodes nodes: the warp walks
+// global memory.  Either way the arithmetic and its order are those of the sequential walk.
+constexpr int kLimiterThreads = 1024;
+constexpr int kStageCells = 4096;
+constexpr int kStageNodes = 4096;
+// shared bytes of the staged walk: per node 4 gradients and its index, per cell 4 slots and a mask
+constexpr size_t kStageBytes = kStageNodes * (4 * sizeof(double) + sizeof(int)) +
+                               kStageCells * (4 * sizeof(int) + 1);
+
+__global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *list, int *sorted,
+                                                                    const double *Jc, double *g,
+                                                                    int nx, int ny, double e1,
+                                                                    double e2, int nlev, Red *red,
+                                                                    unsigned *flags, int *slot) {
+    extern __shared__ __align__(16) unsigned char lsm[];
+    int *off = reinterpret_cast<int *>(lsm);  // nlev + 1
+    int *cur = off + nlev + 1;                // nlev
+    const size_t o = ((size_t)(2 * nlev + 1) * sizeof(int) + 15) & ~(size_t)15;
+    double *gs = reinterpret_cast<double *>(lsm + o);                   // [kStageNodes][4]
+    int *snode = reinterpret_cast<int *>(gs + (size_t)kStageNodes * 4);  // [kStageNodes]
+    int *cs = snode + kStageNodes;                                       // [kStageCells][4]
+    unsigned char *cmask = reinterpret_cast<unsigned char *>(cs + (size_t)kStageCells * 4);
+    __shared__ int nslot;
     const long V = (long)nx * ny;
     const long cy = ny - 1;
     const int n = red->count;
-    for (int l = threadIdx.x; l < nlev + 1; l += blockDim.x) off[l] = 0;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int l = tid; l < nlev + 1; l += blockDim.x) off[l] = 0;
+    if (tid == 0) nslot = 0;
     __syncthreads();
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    for (int q = tid; q < n; q += blockDim.x) {
         const long cell = list[q];
         atomicAdd(&off[2 * (int)(cell / cy) + (int)(cell % cy) + 1], 1);
     }
     __syncthreads();
-    if (threadIdx.x == 0)
+    if (tid == 0)
         for (int l = 0; l < nlev; ++l) off[l + 1] += off[l];
     __syncthreads();
-    for (int l = threadIdx.x; l < nlev; l += blockDim.x) cur[l] = off[l];
+    for (int l = tid; l < nlev; l += blockDim.x) cur[l] = off[l];
     __syncthreads();
-    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    for (int q = tid; q < n; q += blockDim.x) {
         const long cell = list[q];
         sorted[atomicAdd(&cur[2 * (int)(cell / cy) + (int)(cell % cy)], 1)] = (int)cell;
     }
     __syncthreads();
-    bool capped = false;
-    for (int l = 0; l < nlev; ++l) {
-        const int beg = off[l], end = off[l + 1];
-        if (beg == end) continue;  // uniform: every thread reads the same shared value
-        for (int q = beg + threadIdx.x; q < end; q += blockDim.x) {
+    bool staged = false;
+    if (n <= kStageCells) {
+        // claim a slot for every node (0, 0), (1, 0), (0, 1) a flagged corner reads
+        for (int q = tid; q < n; q += blockDim.x) {
             const long cell = sorted[q];
             const int x = (int)(cell / cy), y = (int)(cell % cy);
+            unsigned m = 0;
             for (int c = 0; c < 4; ++c) {
                 const double jv = Jc[cell * 4 + c];
-                if (!(jv < e1 || jv > e2)) continue;
-                const int vx = c & 1, vy = c >> 1;
-                const long gp[2] = {(long)x * ny + (y + vy), (long)(x + vx) * ny + y};
-                double J[2][2];
-                for (int n1 = 0; n1 < 2; ++n1)
-                    for (int n2 = 0; n2 < 2; ++n2) J[n1][n2] = g[(n1 * 2 + n2) * V + gp[n2]];
-                double alpha = 0.0;
-                double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
-                int steps = 0;
-                while (det > e2 || det < e1) {
-                    if (++steps > 11) {  // alpha == 1 (identity) already tried: [e1, e2] misses 1
-                        capped = true;
-                        break;
-                    }
-                    alpha += 0.1;
-                    if (alpha > 1.0) alpha = 1.0;
-                    double Jn[2][2];
-                    for (int n1 = 0; n1 < 2; ++n1)
-                        for (int n2 = 0; n2 < 2; ++n2)
-                            Jn[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
-                    det = Jn[0][0] * Jn[1][1] - Jn[0][1] * Jn[1][0];
+                m |= (jv < e1 || jv > e2) ? 1u << c : 0u;
+            }
+            cmask[q] = (unsigned char)m;
+            const unsigned need = ((m & 1u) ? 1u : 0u) | ((m & 2u) ? 3u : 0u) |
+                                  ((m & 4u) ? 5u : 0u) | ((m & 8u) ? 6u : 0u);  // bit d: node d
+            int old[3];
+            long p[3];
+            for (int d = 0; d < 3; ++d) {
+                p[d] = (long)(x + (d & 1)) * ny + (y + (d >> 1));
+                old[d] = (need >> d & 1u) ? atomicCAS(&slot[p[d]], -1, -2) : 0;
+            }
+            for (int d = 0; d < 3; ++d)
+                if ((need >> d & 1u) && old[d] == -1) {
+                    const int sl = atomicAdd(&nslot, 1);
+                    if (sl < kStageNodes) snode[sl] = (int)p[d];
+                    slot[p[d]] = sl;
                 }
-                alpha += 0.1;
-                if (alpha > 1.0) alpha = 1.0;
-                for (int n1 = 0; n1 < 2; ++n1)
-                    for (int n2 = 0; n2 < 2; ++n2)
-                        g[(n1 * 2 + n2) * V + gp[n2]] =
-                            (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+        }
+        __syncthreads();  // every claimed node holds its slot number
+        const int ns = nslot;
+        if (ns <= kStageNodes) {
+            staged = true;
+            for (int q = tid; q < n; q += blockDim.x) {
+                const long cell = sorted[q];
+                const int x = (int)(cell / cy), y = (int)(cell % cy);
+                const unsigned m = cmask[q];
+                const unsigned need = ((m & 1u) ? 1u : 0u) | ((m & 2u) ? 3u : 0u) |
+                                      ((m & 4u) ? 5u : 0u) | ((m & 8u) ? 6u : 0u);
+                for (int d = 0; d < 3; ++d)
+                    cs[q * 4 + d] = (need >> d & 1u)
+                                        ? slot[(long)(x + (d & 1)) * ny + (y + (d >> 1))]
+                                        : -1;
+            }
+            for (int sl = tid; sl < ns; sl += blockDim.x)
+                for (int k = 0; k < 4; ++k) gs[sl * 4 + k] = g[k * V + snode[sl]];
+        } else {
+            // too many nodes: release the map and walk global memory
+            for (int q = tid; q < n; q += blockDim.x) {
+                const long cell = sorted[q];
+                const int x = (int)(cell / cy), y = (int)(cell % cy);
+                for (int d = 0; d < 3; ++d) slot[(long)(x + (d & 1)) * ny + (y + (d >> 1))] = -1;
             }
         }
         __syncthreads();
+    }
+    bool capped = false;
+    if (tid < 32) {
+        for (int l = 0; l < nlev; ++l) {
+            const int beg = off[l], end = off[l + 1];
+            if (beg == end) continue;  // uniform: every lane reads the same shared value
+            for (int q = beg + lane; q < end; q += 32) {
+                if (staged) {
+                    const unsigned m = cmask[q];
+                    for (int c = 0; c < 4; ++c) {
+                        if (!(m >> c & 1u)) continue;
+                        const int vx = c & 1, vy = c >> 1;
+                        const int sv[2] = {cs[q * 4 + 2 * vy], cs[q * 4 + vx]};
+                        double J[2][2];
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                J[n1][n2] = gs[sv[n2] * 4 + n1 * 2 + n2];
+                        limit_corner<2>(J, e1, e2, capped);
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                gs[sv[n2] * 4 + n1 * 2 + n2] = J[n1][n2];
+                    }
+                } else {
+                    const long cell = sorted[q];
+                    const int x = (int)(cell / cy), y = (int)(cell % cy);
+                    for (int c = 0; c < 4; ++c) {
+                        const double jv = Jc[cell * 4 + c];
+                        if (!(jv < e1 || jv > e2)) continue;
+                        const int vx = c & 1, vy = c >> 1;
+                        const long gp[2] = {(long)x * ny + (y + vy), (long)(x + vx) * ny + y};
+                        double J[2][2];
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                J[n1][n2] = g[(n1 * 2 + n2) * V + gp[n2]];
+                        limit_corner<2>(J, e1, e2, capped);
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                g[(n1 * 2 + n2) * V + gp[n2]] = J[n1][n2];
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (staged) {
+        __syncthreads();
+        const int ns = nslot;
+        for (int sl = tid; sl < ns; sl += blockDim.x) {
+            const long p = snode[sl];
+            for (int k = 0; k < 4; ++k) g[k * V + p] = gs[sl * 4 + k];
+            slot[p] = -1;
+        }
     }
     if (capped) atomicOr(flags, (unsigned)kFlagLimiterCapped);
 }
@@ -733,6 +854,7 @@ struct TopologyWorkspace::Impl {
     bool ready = false;
     DBuf<double> grad, jc, div, t1, t2;
     DBuf<int> list, sorted;
+    DBuf<int> slot;  // image node -> shared-memory slot of the 2D limiter, -1 between calls
     DBuf<double> H[3], cs[3];
     Impl(int x, int y, int z, cudaStream_t s)
         : nx(x), ny(y), nz(z), N(z == 1 ? 2 : 3), V((long)x * y * z),
@@ -747,6 +869,10 @@ struct TopologyWorkspace::Impl {
         t2.alloc(V * N, st);
         list.alloc(cells, st);
         sorted.alloc(cells, st);
+        if (nz == 1) {
+            slot.alloc(V, st);
+            BINDER_CUDA(cudaMemsetAsync(slot.p, 0xff, sizeof(int) * V, st));
+        }
         const int dims[3] = {nx, ny, nz};
         const double pi = 3.14159265358979323846;
         for (int a = 0; a < 3; ++a) {
@@ -821,7 +947,7 @@ TopologyResult TopologyWorkspace::run(double e1, double e2, int max_outer, int m
             reset_red(w.red.p, s);
             count_launch(), flag_cells_kernel<<<grid_for(cells), 256, 0, s>>>(w.jc.p, nx, ny, nz, e1, e2, w.list.p,
                                                               w.red.p);
-            count_launch(), limiter_kernel<<<1, 1024, lim_smem, s>>>(w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny,
+            count_launch(), limiter_kernel<<<1, 256, lim_smem, s>>>(w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny,
                                                      nz, e1, e2, nlev, w.red.p, w.flags.p);
             BINDER_CUDA(cudaGetLastError());
             count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, 3, w.red.p);
@@ -906,7 +1032,8 @@ TopologyResult TopologyWorkspace::run2d(double e1, double e2, int max_outer, int
     res.below_before = (long long)r.below;
     res.above_before = (long long)r.above;
     const int nlev = 2 * (nx - 2) + (ny - 2) + 1;
-    const size_t lim_smem = sizeof(int) * (2 * (size_t)nlev + 1);
+    const size_t lim_smem =
+        ((sizeof(int) * (2 * (size_t)nlev + 1) + 15) & ~(size_t)15) + kStageBytes;
     BINDER_CUDA(cudaFuncSetAttribute(limiter2d_kernel,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim_smem));
     int outer = 0;
@@ -920,9 +1047,9 @@ TopologyResult TopologyWorkspace::run2d(double e1, double e2, int max_outer, int
             reset_red(w.red.p, s);
             count_launch(), flag_cells2d_kernel<<<grid_for(cells), 256, 0, s>>>(
                                 w.jc.p, nx, ny, e1, e2, w.list.p, w.red.p);
-            count_launch(), limiter2d_kernel<<<1, 1024, lim_smem, s>>>(
+            count_launch(), limiter2d_kernel<<<1, kLimiterThreads, lim_smem, s>>>(
                                 w.list.p, w.sorted.p, w.jc.p, w.grad.p, nx, ny, e1, e2, nlev,
-                                w.red.p, w.flags.p);
+                                w.red.p, w.flags.p, w.slot.p);
             BINDER_CUDA(cudaGetLastError());
             count_launch(), sum_kernel<<<grid_for(V), 256, 0, s>>>(w.pos.p, V, 2, w.red.p);
             count_launch(), divergence2d_kernel<<<grid_for(V), 256, 0, s>>>(w.grad.p, nx, ny,
