@@ -256,9 +256,9 @@ __global__ void flag_cells_kernel(const double *Jc, int nx, int ny, int nz, doub
 // topology_correction_2D.cpp:257-309): J the corner's N x N gradient matrix (column n2 read at
 // vertex n2), replaced by (1 - a) J + a I.  The reference steps
 // alpha by 0.1 (capped at 1) until det((1 - alpha) J + alpha I) lies in [e1, e2], at most 11
-// steps, then takes one step more.  The alphas are constants, so the 11 trial determinants are
-// evaluated independently (the same expressions the loop evaluates) and the first one in range
-// picks the step: a walk whose time is the latency of one corner after another gains the ILP.
+// steps, then takes one step more.  The alphas are constants, so the trial determinants are
+// evaluated independently, a group at a time (the same expressions the loop evaluates), and the
+// first one in range picks the step: the walk, one corner after another, gains the ILP.
 template <int N>
 __device__ __forceinline__ double detn(const double (&J)[N][N]) {
     if constexpr (N == 2)
@@ -284,23 +284,60 @@ __device__ __forceinline__ void limit_corner(double (&J)[N][N], double e1, doubl
     if (det0 > e2 || det0 < e1) {
         bool none = true;  // alpha == 1 (identity) tried as well: [e1, e2] misses 1
         alpha = al[kSteps + 1];
+        // trials in groups of kGroup (independent within a group), stopping at the first group
+        // with a determinant in range
+        constexpr int kGroup = 4;
 #pragma unroll
-        for (int t = kSteps; t >= 1; --t) {
-            const double a = al[t];
-            double Jn[N][N];
-            for (int n1 = 0; n1 < N; ++n1)
-                for (int n2 = 0; n2 < N; ++n2)
-                    Jn[n1][n2] = (1 - a) * J[n1][n2] + a * (n1 == n2 ? 1.0 : 0.0);
-            const double det = detn<N>(Jn);
-            if (!(det > e2 || det < e1)) {
-                alpha = al[t + 1];
-                none = false;
+        for (int t0 = 1; t0 <= kSteps; t0 += kGroup) {
+            const int t1 = t0 + kGroup - 1 < kSteps ? t0 + kGroup - 1 : kSteps;
+#pragma unroll
+            for (int t = t1; t >= t0; --t) {
+                const double a = al[t];
+                double Jn[N][N];
+                for (int n1 = 0; n1 < N; ++n1)
+                    for (int n2 = 0; n2 < N; ++n2)
+                        Jn[n1][n2] = (1 - a) * J[n1][n2] + a * (n1 == n2 ? 1.0 : 0.0);
+                const double det = detn<N>(Jn);
+                if (!(det > e2 || det < e1)) {
+                    alpha = al[t + 1];
+                    none = false;
+                }
             }
+            if (!none) break;
         }
         if (none) capped = true;
     }
     for (int n1 = 0; n1 < N; ++n1)
         for (int n2 = 0; n2 < N; ++n2)
+            J[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
+}
+
+// limit_corner by a group of 16 lanes holding the same J: lane t (1 <= t <= 11) evaluates trial
+// t, and the lowest lane whose determinant lies in [e1, e2] picks the step.  The same expressions
+// and the same choice as limit_corner; every lane of the group ends with the new J.  gmask names
+// the group's lanes, which all take this call together.
+__device__ __forceinline__ void limit_corner_lanes(double (&J)[2][2], double e1, double e2,
+                                                   bool &capped, int gl, unsigned gmask,
+                                                   double at, double an) {
+    const double det0 = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    double alpha = 0.1;  // one step from 0
+    if (det0 > e2 || det0 < e1) {  // uniform across the group
+        bool in = false;
+        if (gl >= 1 && gl <= 11) {
+            double Jn[2][2];
+            for (int n1 = 0; n1 < 2; ++n1)
+                for (int n2 = 0; n2 < 2; ++n2)
+                    Jn[n1][n2] = (1 - at) * J[n1][n2] + at * (n1 == n2 ? 1.0 : 0.0);
+            const double det = Jn[0][0] * Jn[1][1] - Jn[0][1] * Jn[1][0];
+            in = !(det > e2 || det < e1);
+        }
+        const unsigned b = __ballot_sync(gmask, in) & gmask;
+        const int k = b ? __ffs((int)b) - 1 : -1;  // lane of the warp
+        alpha = __shfl_sync(gmask, an, k < 0 ? 11 : (k & 15), 16);  // al[k + 1], or al[12] = 1
+        if (k < 0) capped = true;
+    }
+    for (int n1 = 0; n1 < 2; ++n1)
+        for (int n2 = 0; n2 < 2; ++n2)
             J[n1][n2] = (1 - alpha) * J[n1][n2] + alpha * (n1 == n2 ? 1.0 : 0.0);
 }
 
@@ -482,10 +519,13 @@ __global__ void flag_cells2d_kernel(const double *Jc, int nx, int ny, double e1,
 // global memory.  Either way the arithmetic and its order are those of the sequential walk.
 constexpr int kLimiterThreads = 1024;
 constexpr int kStageCells = 4096;
-constexpr int kStageNodes = 4096;
-// shared bytes of the staged walk: per node 4 gradients and its index, per cell 4 slots and a mask
-constexpr size_t kStageBytes = kStageNodes * (4 * sizeof(double) + sizeof(int)) +
-                               kStageCells * (4 * sizeof(int) + 1);
+constexpr int kStageNodes = 6016;
+// shared bytes of the staged walk: per node 4 gradients, per cell 3 slots and the corner mask
+// (16 bits each)
+constexpr size_t kStageBytes =
+    kStageNodes * 4 * sizeof(double) + kStageCells * 4 * sizeof(unsigned short);
+constexpr unsigned short kNoSlot = 0xffff;
+static_assert(kStageNodes < kNoSlot, "slots are 16-bit");
 
 __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *list, int *sorted,
                                                                     const double *Jc, double *g,
@@ -496,10 +536,9 @@ __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *l
     int *off = reinterpret_cast<int *>(lsm);  // nlev + 1
     int *cur = off + nlev + 1;                // nlev
     const size_t o = ((size_t)(2 * nlev + 1) * sizeof(int) + 15) & ~(size_t)15;
-    double *gs = reinterpret_cast<double *>(lsm + o);                   // [kStageNodes][4]
-    int *snode = reinterpret_cast<int *>(gs + (size_t)kStageNodes * 4);  // [kStageNodes]
-    int *cs = snode + kStageNodes;                                       // [kStageCells][4]
-    unsigned char *cmask = reinterpret_cast<unsigned char *>(cs + (size_t)kStageCells * 4);
+    double *gs = reinterpret_cast<double *>(lsm + o);  // [kStageNodes][4]
+    // [kStageCells][4]: slots of nodes (0, 0), (1, 0), (0, 1), then the flagged-corner mask
+    unsigned short *cs = reinterpret_cast<unsigned short *>(gs + (size_t)kStageNodes * 4);
     __shared__ int nslot;
     const long V = (long)nx * ny;
     const long cy = ny - 1;
@@ -534,7 +573,7 @@ __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *l
                 const double jv = Jc[cell * 4 + c];
                 m |= (jv < e1 || jv > e2) ? 1u << c : 0u;
             }
-            cmask[q] = (unsigned char)m;
+            cs[q * 4 + 3] = (unsigned short)m;
             const unsigned need = ((m & 1u) ? 1u : 0u) | ((m & 2u) ? 3u : 0u) |
                                   ((m & 4u) ? 5u : 0u) | ((m & 8u) ? 6u : 0u);  // bit d: node d
             int old[3];
@@ -545,28 +584,31 @@ __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *l
             }
             for (int d = 0; d < 3; ++d)
                 if ((need >> d & 1u) && old[d] == -1) {
-                    const int sl = atomicAdd(&nslot, 1);
-                    if (sl < kStageNodes) snode[sl] = (int)p[d];
-                    slot[p[d]] = sl;
+                    slot[p[d]] = atomicAdd(&nslot, 1);
                 }
         }
         __syncthreads();  // every claimed node holds its slot number
         const int ns = nslot;
         if (ns <= kStageNodes) {
             staged = true;
+            // slots of the cells and the nodes' gradients (a node shared by cells is gathered
+            // once per cell, the same values into the same slot)
             for (int q = tid; q < n; q += blockDim.x) {
                 const long cell = sorted[q];
                 const int x = (int)(cell / cy), y = (int)(cell % cy);
-                const unsigned m = cmask[q];
+                const unsigned m = cs[q * 4 + 3];
                 const unsigned need = ((m & 1u) ? 1u : 0u) | ((m & 2u) ? 3u : 0u) |
                                       ((m & 4u) ? 5u : 0u) | ((m & 8u) ? 6u : 0u);
-                for (int d = 0; d < 3; ++d)
-                    cs[q * 4 + d] = (need >> d & 1u)
-                                        ? slot[(long)(x + (d & 1)) * ny + (y + (d >> 1))]
-                                        : -1;
+                for (int d = 0; d < 3; ++d) {
+                    unsigned short sl = kNoSlot;
+                    if (need >> d & 1u) {
+                        const long p = (long)(x + (d & 1)) * ny + (y + (d >> 1));
+                        sl = (unsigned short)slot[p];
+                        for (int k = 0; k < 4; ++k) gs[sl * 4 + k] = g[k * V + p];
+                    }
+                    cs[q * 4 + d] = sl;
+                }
             }
-            for (int sl = tid; sl < ns; sl += blockDim.x)
-                for (int k = 0; k < 4; ++k) gs[sl * 4 + k] = g[k * V + snode[sl]];
         } else {
             // too many nodes: release the map and walk global memory
             for (int q = tid; q < n; q += blockDim.x) {
@@ -579,12 +621,47 @@ __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *l
     }
     bool capped = false;
     if (tid < 32) {
+        // lane gl of a 16-lane group: alpha of trial gl and of the step after it
+        const int grp = lane >> 4, gl = lane & 15;
+        const unsigned gmask = grp ? 0xffff0000u : 0x0000ffffu;
+        double at = 0.0, an = 0.0, a = 0.0;
+        for (int t = 0; t <= 11; ++t) {
+            const double a1 = fmin(a + 0.1, 1.0);  // alpha += 0.1, capped at 1
+            if (t == gl) {
+                at = a;
+                an = a1;
+            }
+            a = a1;
+        }
         for (int l = 0; l < nlev; ++l) {
             const int beg = off[l], end = off[l + 1];
             if (beg == end) continue;  // uniform: every lane reads the same shared value
+            if (staged && end - beg <= 2) {
+                // one or two cells: a group of 16 lanes per cell, the trials across the lanes
+                const int q = beg + grp;
+                if (q < end) {  // uniform across the group
+                    const unsigned m = cs[q * 4 + 3];
+                    for (int c = 0; c < 4; ++c) {
+                        if (!(m >> c & 1u)) continue;
+                        const int vx = c & 1, vy = c >> 1;
+                        const int sv[2] = {cs[q * 4 + 2 * vy], cs[q * 4 + vx]};
+                        double J[2][2];
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                J[n1][n2] = gs[sv[n2] * 4 + n1 * 2 + n2];
+                        limit_corner_lanes(J, e1, e2, capped, gl, gmask, at, an);
+                        // every lane stores the same values; each reads its own store back
+                        for (int n1 = 0; n1 < 2; ++n1)
+                            for (int n2 = 0; n2 < 2; ++n2)
+                                gs[sv[n2] * 4 + n1 * 2 + n2] = J[n1][n2];
+                    }
+                }
+                __syncwarp();
+                continue;
+            }
             for (int q = beg + lane; q < end; q += 32) {
                 if (staged) {
-                    const unsigned m = cmask[q];
+                    const unsigned m = cs[q * 4 + 3];
                     for (int c = 0; c < 4; ++c) {
                         if (!(m >> c & 1u)) continue;
                         const int vx = c & 1, vy = c >> 1;
@@ -622,11 +699,17 @@ __global__ void __launch_bounds__(kLimiterThreads) limiter2d_kernel(const int *l
     }
     if (staged) {
         __syncthreads();
-        const int ns = nslot;
-        for (int sl = tid; sl < ns; sl += blockDim.x) {
-            const long p = snode[sl];
-            for (int k = 0; k < 4; ++k) g[k * V + p] = gs[sl * 4 + k];
-            slot[p] = -1;
+        // scatter back (a shared node once per cell, the same values) and release the map
+        for (int q = tid; q < n; q += blockDim.x) {
+            const long cell = sorted[q];
+            const int x = (int)(cell / cy), y = (int)(cell % cy);
+            for (int d = 0; d < 3; ++d) {
+                const unsigned short sl = cs[q * 4 + d];
+                if (sl == kNoSlot) continue;
+                const long p = (long)(x + (d & 1)) * ny + (y + (d >> 1));
+                for (int k = 0; k < 4; ++k) g[k * V + p] = gs[sl * 4 + k];
+                slot[p] = -1;
+            }
         }
     }
     if (capped) atomicOr(flags, (unsigned)kFlagLimiterCapped);

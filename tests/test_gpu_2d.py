@@ -198,6 +198,47 @@ def test_topology2d_larger_field_matches_oracle(core, oracle):
     assert tc.last_stats["below_e1_after"] == 0
 
 
+def first_walk_size(f, shape, e1, e2):
+    """Flagged cells of the limiter's first walk and the nodes their flagged corners read (corner
+    (vx, vy) of cell (x, y): the cell's x edge on row y + vy and y edge on column x + vx)."""
+    P = f.reshape(shape + (2,))
+    nx, ny = shape
+    flag = np.zeros((nx - 1, ny - 1), bool)
+    nodes = set()
+    for vx in (0, 1):
+        for vy in (0, 1):
+            ex = P[1:, vy:ny - 1 + vy] - P[:-1, vy:ny - 1 + vy]
+            ey = P[vx:nx - 1 + vx, 1:] - P[vx:nx - 1 + vx, :-1]
+            det = ex[..., 0] * ey[..., 1] - ey[..., 0] * ex[..., 1]
+            out = (det < e1) | (det > e2)
+            flag |= out
+            for x, y in zip(*np.nonzero(out)):
+                nodes.update({(x, y + vy), (x + vx, y)})
+    return int(flag.sum()), len(nodes)
+
+
+# the limiter walks shared-memory copies of up to 4096 cells and 6016 nodes, else global memory
+@pytest.mark.parametrize("shape,amp,sigma,seed,regime", [
+    ((200, 200), 0.35, 0.5, 4, "staged"),
+    ((200, 200), 0.404, 0.5, 4, "too many nodes"),
+    ((200, 180), 3.0, 1.0, 1, "too many cells"),
+])
+def test_topology2d_limiter_walks_match_oracle(core, oracle, shape, amp, sigma, seed, regime):
+    from binder_b200 import phantoms
+    rng = np.random.default_rng(seed)
+    f = phantoms.identity_positions(shape) + \
+        phantoms.smooth_random_field(shape, amp, sigma, rng).astype(np.float64)
+    cells, nodes = first_walk_size(f, shape, 0.01, 100.0)
+    assert {"staged": cells <= 4096 and nodes <= 6016,
+            "too many nodes": cells <= 4096 and nodes > 6016,
+            "too many cells": cells > 4096}[regime], (cells, nodes)
+    tc = core.topology_correction_2D()
+    out = tc.correct_topology(f, 0.01, 100.0, 10, 10, 1, [1.0, 1.0], *shape)
+    ref, _ = oracle.topology2d(f, 0.01, 100.0, 10, 10, [1.0, 1.0], shape)
+    np.testing.assert_allclose(out.ravel(), ref, rtol=0, atol=1e-8)
+    assert tc.last_stats["below_e1_after"] == (oracle.jacobian2d(ref, shape) < 0.01).sum()
+
+
 def test_registration_topology2d_on_device(core):
     """The device-side correction of a 2D registration's positions equals the host entry point
     applied to the same (FP32) positions."""
