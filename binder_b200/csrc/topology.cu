@@ -1153,11 +1153,14 @@ TopologyResult TopologyWorkspace::run2d(double e1, double e2, int max_outer, int
             a.cos_z = w.cs[2].p;
             a.in = w.div.p; a.out = w.t1.p; a.M = w.H[1].p; a.n = ny; a.outer = nx; a.s = 1;
             launch_axis_pass(a, kEpiNone, 2, s);
-            a.in = w.t1.p; a.out = w.t2.p; a.M = w.H[0].p; a.M2 = w.H[0].p; a.n = nx; a.outer = 1;
-            a.s = ny;
-            launch_axis_pass(a, kEpiPoisson, 2, s);
+            // the x passes as two launches (forward with -1/lambda, inverse), each split into row
+            // blocks: fused into one, a 2D image's x pass fills only a few CTAs
+            a.in = w.t1.p; a.out = w.t2.p; a.M = w.H[0].p; a.n = nx; a.outer = 1; a.s = ny;
+            launch_axis_pass(a, kEpiPoissonFwd, 2, s);
+            a.in = w.t2.p; a.out = w.t1.p;
+            launch_axis_pass(a, kEpiNone, 2, s);
             // last pass: physical positions u * vs + mean
-            a.in = w.t2.p; a.out = w.pos.p; a.M = w.H[1].p; a.M2 = nullptr; a.n = ny; a.outer = nx;
+            a.in = w.t1.p; a.out = w.pos.p; a.M = w.H[1].p; a.M2 = nullptr; a.n = ny; a.outer = nx;
             a.s = 1;
             for (int n = 0; n < 2; ++n) {
                 a.out_scale[n] = vs[n];

@@ -32,10 +32,10 @@ __device__ __forceinline__ void load4(const double *p, double v[4]) {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-// acc[r][q] = sum_j M[k][j] * Xs[j][c] for rows k = ty + 16 r and columns c = 4 tx + q
+// acc[r][q] = sum_j M[k][j] * Xs[j][c] for rows k = k0 + ty + 16 r and columns c = 4 tx + q
 template <typename T, int R>
 __device__ __forceinline__ void gemm_tile(const T *__restrict__ M, int n, const T *Xs, T *Ms,
-                                          T (&acc)[R][4], int tx, int ty) {
+                                          T (&acc)[R][4], int tx, int ty, int k0) {
     constexpr int P = Pitch<T>::v;
 #pragma unroll
     for (int r = 0; r < R; ++r)
@@ -45,7 +45,7 @@ __device__ __forceinline__ void gemm_tile(const T *__restrict__ M, int n, const 
         __syncthreads();
         for (int f = threadIdx.x; f < 16 * R * JC; f += kThreads) {
             const int k = f / JC, jj = f - k * JC, j = j0 + jj;
-            Ms[k * (JC + 1) + jj] = (k < n && j < n) ? M[(long)k * n + j] : T(0);
+            Ms[k * (JC + 1) + jj] = (k0 + k < n && j < n) ? M[(long)(k0 + k) * n + j] : T(0);
         }
         __syncthreads();
         const int jn = min(JC, n - j0);
@@ -68,13 +68,37 @@ __device__ __forceinline__ float prior_normal(uint64_t seed, uint32_t i, uint32_
     return dct_prior_normal(seed, i, sweep, chain, comp);
 }
 
+// Hartley Poisson step of an x-axis pass (outer == 1, s == ny*nz) on rows k = k0 + ty + 16 r:
+// c <- -c / (lambda * V), lambda = 6 - 2cos z - 2cos x - 2cos y
+template <typename T, int R>
+__device__ __forceinline__ void poisson_scale(const AxisArgs<T> &a, T (&acc)[R][4], int k0,
+                                              long t0, int ncol, int tx, int ty) {
+    const int n = a.n, nz = a.nz;
+    const double inv_total = 1.0 / ((double)n * (double)a.s);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = k0 + ty + 16 * r;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = tx * 4 + q;
+            if (k < n && c < ncol) {
+                const long t = t0 + c;
+                const int ky = (int)(t / nz), kz = (int)(t - (long)ky * nz);
+                const double lam =
+                    6.0 - 2.0 * a.cos_z[kz] - 2.0 * a.cos_x[k] - 2.0 * a.cos_y[ky];
+                acc[r][q] = fabs(lam) > 1e-10 ? (T)(-(double)acc[r][q] / lam * inv_total) : T(0);
+            }
+        }
+    }
+}
+
 template <typename T, int R, int MODE>
 __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
     if (a.skip && *a.skip) return;
     constexpr int P = Pitch<T>::v;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *Xs = reinterpret_cast<T *>(smem_raw);
-    T *Ms = Xs + 16 * R * P;
+    T *Ms = Xs + (size_t)a.n * P;  // the slab holds all n rows
     __shared__ double red[32];
 
     const int comp = blockIdx.z;
@@ -83,6 +107,9 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
     const int n = a.n;
     const bool contig = (a.s == 1);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // output rows of this CTA: k0 .. k0 + 16R - 1 (one row block, k0 = 0, unless the launch splits
+    // the rows of a plain or position-storing pass over blockIdx.y)
+    const int k0 = blockIdx.y * 16 * R;
 
     long o, t0 = 0;
     int ncol;
@@ -117,7 +144,8 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
     }
 
     T acc[R][4];
-    gemm_tile<T, R>(a.M, n, Xs, Ms, acc, tx, ty);
+    gemm_tile<T, R>(a.M, n, Xs, Ms, acc, tx, ty, k0);
+    if constexpr (MODE == kEpiPoissonFwd) poisson_scale<T, R>(a, acc, k0, t0, ncol, tx, ty);
 
     if constexpr (MODE == kEpiSpectral || MODE == kEpiPoisson) {
         // x-axis pass (outer == 1, s == ny*nz): coefficient (k, t) has flat index k*s + t
@@ -148,25 +176,8 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
                     }
                 }
             }
-        } else {  // Poisson: c <- -c / (lambda * V), lambda = 6 - 2cos z - 2cos x - 2cos y
-            const int nz = a.nz;
-            const double inv_total = 1.0 / ((double)n * (double)a.s);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int k = ty + 16 * r;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int c = tx * 4 + q;
-                    if (k < n && c < ncol) {
-                        const long t = t0 + c;
-                        const int ky = (int)(t / nz), kz = (int)(t - (long)ky * nz);
-                        const double lam = 6.0 - 2.0 * a.cos_z[kz] - 2.0 * a.cos_x[k] -
-                                           2.0 * a.cos_y[ky];
-                        acc[r][q] = fabs(lam) > 1e-10 ? (T)(-(double)acc[r][q] / lam * inv_total)
-                                                      : T(0);
-                    }
-                }
-            }
+        } else {
+            poisson_scale<T, R>(a, acc, 0, t0, ncol, tx, ty);
         }
         if constexpr (MODE == kEpiSpectral) {
             const double sc = block_sum(part_cost, red);
@@ -184,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) Xs[k * P + tx * 4 + q] = acc[r][q];
         }
-        gemm_tile<T, R>(a.M2, n, Xs, Ms, acc, tx, ty);
+        gemm_tile<T, R>(a.M2, n, Xs, Ms, acc, tx, ty, 0);
     }
 
     // ---- store ----
@@ -192,7 +203,7 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int k = ty + 16 * r;
+            const int k = k0 + ty + 16 * r;
             if (k < n)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) Xs[k * P + tx * 4 + q] = acc[r][q];
@@ -200,11 +211,13 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
         __syncthreads();
         T *dst = out + o * n;
         const long base = o * n;
-        for (int f = threadIdx.x; f < ncol * n; f += kThreads) {
-            const int c = f / n, j = f - c * n;
+        const int nr = min(16 * R, n - k0);  // rows of this CTA
+        for (int f = threadIdx.x; f < ncol * nr; f += kThreads) {
+            const int c = f / nr, j = k0 + (f - c * nr);
+            const int e = c * n + j;  // element of the tile's lines
             T val = Xs[j * P + c];
             if constexpr (MODE == kEpiPositions) {
-                const long i = base + f;
+                const long i = base + e;
                 float xv;
                 if (a.xpos) {
                     xv = a.xpos[comp * a.comp_stride + i];
@@ -217,13 +230,13 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
             } else if constexpr (MODE == kEpiTopoOut) {
                 val = (T)((double)val * a.out_scale[comp] + a.out_offset[comp]);
             }
-            dst[f] = val;
+            dst[e] = val;
         }
     } else {
         T *dst = out + o * n * a.s + t0;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int k = ty + 16 * r;
+            const int k = k0 + ty + 16 * r;
             if (k < n)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -237,17 +250,18 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
 template <typename T, int R, int MODE>
 void launch_r(const AxisArgs<T> &a, int ncomp, cudaStream_t stream) {
     constexpr int P = Pitch<T>::v;
-    const size_t smem = (size_t)16 * R * (P + JC + 1) * sizeof(T);
+    const size_t smem = ((size_t)a.n * P + (size_t)16 * R * (JC + 1)) * sizeof(T);
     static bool configured = false;  // per instantiation; attribute is per-function
-    if (!configured) {
+    if (!configured) {  // room for the longest axis, 256
+        const size_t most = ((size_t)256 * P + (size_t)16 * R * (JC + 1)) * sizeof(T);
         BINDER_CUDA(cudaFuncSetAttribute(axis_kernel<T, R, MODE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
         configured = true;
     }
     const bool contig = (a.s == 1);
     const long gx = contig ? (a.outer + TC - 1) / TC : a.outer * ((a.s + TC - 1) / TC);
     BINDER_CHECK(gx < (1L << 31), "transform grid too large");
-    dim3 grid((unsigned)gx, 1, (unsigned)ncomp);
+    dim3 grid((unsigned)gx, (unsigned)((a.n + 16 * R - 1) / (16 * R)), (unsigned)ncomp);
     count_launch(), axis_kernel<T, R, MODE><<<grid, kThreads, smem, stream>>>(a);
     BINDER_CUDA(cudaGetLastError());
 }
@@ -255,6 +269,12 @@ void launch_r(const AxisArgs<T> &a, int ncomp, cudaStream_t stream) {
 template <typename T, int MODE>
 void launch_mode(const AxisArgs<T> &a, int ncomp, cudaStream_t stream) {
     const int n = a.n;
+    if constexpr (std::is_same<T, double>::value &&
+                  (MODE == kEpiNone || MODE == kEpiTopoOut || MODE == kEpiPoissonFwd)) {
+        // FP64 passes of a small image fill a few CTAs: split the rows into 16-row blocks
+        const long gx = a.s == 1 ? (a.outer + TC - 1) / TC : a.outer * ((a.s + TC - 1) / TC);
+        if (n > 16 && gx * ncomp < 148) return launch_r<T, 1, MODE>(a, ncomp, stream);
+    }
     if (n <= 32)
         launch_r<T, 2, MODE>(a, ncomp, stream);
     else if (n <= 64)
@@ -285,6 +305,10 @@ void launch_axis_pass(const AxisArgs<T> &a, int mode, int ncomp, cudaStream_t st
             break;
         case kEpiTopoOut:
             if constexpr (std::is_same<T, double>::value) launch_mode<T, kEpiTopoOut>(a, ncomp, stream);
+            break;
+        case kEpiPoissonFwd:
+            if constexpr (std::is_same<T, double>::value)
+                launch_mode<T, kEpiPoissonFwd>(a, ncomp, stream);
             break;
         default: BINDER_CHECK(false, "unknown transform epilogue");
     }

@@ -34,6 +34,7 @@ enum EpilogueMode : int {
     kEpiPoisson = 3,    // fused fwd -> -1/lambda (Hartley Poisson) -> inverse (x axis)
     kEpiTopoOut = 4,    // store u * scale + mean into a physical-position field (FP64)
     kEpiSpectralOut = 5,  // forward pass whose epilogue applies the prior scaling and stores it
+    kEpiPoissonFwd = 6,   // forward pass whose epilogue applies -1/lambda and stores it (FP64)
 };
 
 template <typename T>

@@ -830,7 +830,6 @@ __global__ void __launch_bounds__(kPtThreads, 1) umma_pt_kernel(const UArgs a) {
     const int my_tiles = blockIdx.x < total ? (int)((total - 1 - blockIdx.x) / G + 1) : 0;
     const long nchunk = (long)my_tiles * nkc;
     const bool contig = (a.s == 1);
-    const int cr = lane & 7, cq = lane >> 3;  // contiguous-axis load mapping
 
     double part_cost = 0.0, part_raw = 0.0;
 
