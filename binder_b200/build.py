@@ -40,16 +40,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     src_time = max(hdr_time, _newest([os.path.join(CSRC, s) for s in SOURCES]))
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= src_time:
         return LIB  # up to date (objects may be absent where only the library was shipped)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_time):
-            cmd = [NVCC, *ARCH, *COMMON, *EXTRA.get(src, []), "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append([NVCC, *ARCH, *COMMON, *EXTRA.get(src, []), "-c", s, "-o", o])
+    # the translation units compile independently: one nvcc per host core at most
+    from concurrent.futures import ThreadPoolExecutor
+
+    def compile_one(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(compile_one, c) for c in cmds]:
+            f.result()
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
         cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         if verbose:

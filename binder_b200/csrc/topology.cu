@@ -851,7 +851,9 @@ static __device__ __align__(256) unsigned char
 constexpr int kNoAllocMaxDevices = 64;
 
 // address of the scratch array on the current device, looked up once per device (with that
-// device current) and kept; the lock guards only this table, not the scratch itself
+// device current) and kept for the life of the process; the lock guards only this table, not the
+// scratch itself.  A cudaDeviceReset after the first call may place the module elsewhere in the
+// next context, so the entry point does not support a device reset after its first call.
 unsigned char *jacobian_scratch_address() {
     static std::mutex mu;
     static unsigned char *addr[kNoAllocMaxDevices] = {};
@@ -890,7 +892,9 @@ void jacobian3d_noalloc(const double *field_host, int nx, int ny, int nz, const 
     Red *red = reinterpret_cast<Red *>(base);
     double *df = reinterpret_cast<double *>(base + kNoAllocHeader);
     double *dj = df + 3 * kJacobianNoAllocMaxVoxels;
-    const cudaStream_t s = 0;
+    // the calling thread's per-thread default stream: unlike the legacy stream 0 it does not
+    // wait for (or hold up) work on the caller's other blocking streams
+    const cudaStream_t s = cudaStreamPerThread;
     count_launch(), clear_red_kernel<<<1, 1, 0, s>>>(red);
     BINDER_CUDA(cudaGetLastError());
     BINDER_CUDA(cudaMemcpyAsync(df, field_host, sizeof(double) * V * 3, cudaMemcpyHostToDevice, s));

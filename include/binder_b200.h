@@ -316,8 +316,10 @@ int binder_jacobian_determinant_2d(const double *field, int Nx, int Ny, double v
  * grids of at most binder_jacobian_noalloc_max_voxels() voxels (524288; e.g. 80x80x80) and
  * rejects larger ones with BINDER_STATUS_INVALID_ARGUMENT.  The summary is reset on every call.
  *   - The first call on each device looks up the array's device address (with that device
- *     current) and keeps it; make that first call before any stream capture begins.
- *   - Work runs on the legacy default stream of the calling thread's current device; the call
+ *     current) and keeps it; make that first call before any stream capture begins.  A
+ *     cudaDeviceReset after that first call is not supported (the address kept may be stale).
+ *   - Work runs on the per-thread default stream (cudaStreamPerThread) of the calling thread's
+ *     current device, which does not synchronise with the caller's other streams; the call
  *     returns when J_out is filled.
  *   - Calls that overlap in time on the same device share the array and race: serialise them.
  * J_out as for binder_jacobian_determinant_3d (bit-identical values).  minmax_out (optional, 2

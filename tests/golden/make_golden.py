@@ -7,7 +7,8 @@ unmodified by oracle/Makefile into oracle/_ref/libbinder_ref.so (FFTW and Eigen 
 project-written subsets in oracle/ref_shim, the affine / rigid transformations by stand-ins).  This script feeds them seeded inputs and stores inputs and outputs as small
 .npz files, so the parity tests are pinned to the reference even where its sources are absent.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [--reference <checkout>]
+(default: $BINDER_REFERENCE_ROOT).
 """
 from __future__ import annotations
 
@@ -22,7 +23,10 @@ sys.path.insert(0, ROOT)
 
 from oracle import pyoracle  # noqa: E402
 
-REF_ROOT = "/root/reference"
+# the reference checkout: BINDER_REFERENCE_ROOT, or --reference <dir> on the command line
+REF_ROOT = os.environ.get("BINDER_REFERENCE_ROOT", "/root/reference")
+if "--reference" in sys.argv:
+    REF_ROOT = sys.argv[sys.argv.index("--reference") + 1]
 
 
 def grid(shape):

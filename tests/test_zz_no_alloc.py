@@ -64,12 +64,13 @@ def test_noalloc_largest_grid_then_rejection_then_small(core):
     Jr = _allocating(L, check, f, shape, (1.0, 1.0, 1.0))
     assert np.array_equal(J, Jr)
     assert (jmin, jmax, neg) == (Jr.min(), Jr.max(), int((Jr < 0).sum()))
-    # one voxel plane too many: rejected before any device work
-    big = (80, 80, 82)
-    fb = np.zeros(int(np.prod(big)) * 3)
-    with pytest.raises(BinderError, match="no-allocation limit"):
-        check(L.binder_jacobian_determinant_3d_noalloc(fb, *big, 1.0, 1.0, 1.0,
-                                                         np.zeros(int(np.prod(big))), None, None))
+    # one voxel past the limit, and a grid well past it: rejected before any device work
+    for big in ((1, 1, MAX_VOXELS + 1), (80, 80, 82)):
+        fb = np.zeros(int(np.prod(big)) * 3)
+        with pytest.raises(BinderError, match="no-allocation limit"):
+            check(L.binder_jacobian_determinant_3d_noalloc(fb, *big, 1.0, 1.0, 1.0,
+                                                             np.zeros(int(np.prod(big))), None,
+                                                             None))
     # and the entry point still works afterwards
     small = (9, 10, 11)
     fs = _field(small, 0.7, 14)
@@ -81,10 +82,11 @@ def test_noalloc_rejects_oversized_grid(core):
     """The size check comes before any CUDA call, so it holds without a device too."""
     from binder_b200._lib import lib
     L = lib()
-    big = (80, 80, 82)
-    assert int(np.prod(big)) > MAX_VOXELS
-    st = L.binder_jacobian_determinant_3d_noalloc(np.zeros(int(np.prod(big)) * 3), *big,
-                                                  1.0, 1.0, 1.0, np.zeros(int(np.prod(big))),
-                                                  None, None)
-    assert st == 1
-    assert b"no-allocation limit of 524288 voxels" in L.binder_last_error()
+    # exactly one voxel past the limit (64 x 64 x 128 + 1), and 80 x 80 x 82 (524,800 voxels)
+    for big in ((1, 1, MAX_VOXELS + 1), (80, 80, 82)):
+        assert int(np.prod(big)) > MAX_VOXELS
+        st = L.binder_jacobian_determinant_3d_noalloc(np.zeros(int(np.prod(big)) * 3), *big,
+                                                      1.0, 1.0, 1.0, np.zeros(int(np.prod(big))),
+                                                      None, None)
+        assert st == 1
+        assert b"no-allocation limit of 524288 voxels" in L.binder_last_error()
