@@ -567,7 +567,7 @@ void Registration::get_ssd_parameters(double out[3]) const {
 void Registration::set_nonlinear_transformation(const double gamma[3], const double rho[3],
                                                 const double eta[3], const float *D) {
     for (int n = 0; n < 3; ++n) {
-        gamma0_[n] = gamma[n];
+        gamma0_[n] = gamma_set_[n] = gamma[n];
         rho_[n] = rho[n];
         eta_[n] = eta[n];
     }
@@ -856,6 +856,7 @@ void PriorTransform::set_precision(int p) {
 }
 
 void Registration::reset() {
+    for (int n = 0; n < 3; ++n) gamma0_[n] = gamma_set_[n];  // the sampler keeps sampled gammas
     BINDER_CUDA(cudaMemcpyAsync(d_, d0_, sizeof(float) * V_ * N_, cudaMemcpyDeviceToDevice, stream_));
     if (lk_ == 3) {
         BINDER_CUDA(cudaMemcpyAsync(fst_, fst0_, sizeof(SsdfState), cudaMemcpyDeviceToDevice,

@@ -97,8 +97,9 @@ class Registration {
                  int sample_posteriors, int sample_likelihood_parameters,
                  int sample_transformation_parameters, double *mean_out, double *cov_out);
 
-    // restore the positions given at construction, the theta given to set_mi_likelihood and a
-    // fresh device state (device-to-device, no host transfer)
+    // restore the positions given at construction, the theta given to set_mi_likelihood, the
+    // gammas given to set_nonlinear_transformation and a fresh device state (device-to-device,
+    // no host transfer)
     void reset();
     // topology correction of the object's own positions on the device (FP64), in place
     TopologyResult correct_topology(double e1, double e2, int max_outer, int max_inner,
@@ -169,6 +170,7 @@ class Registration {
     long vch_ = 0;   // bytes between the channels' padded bin volumes
     double alpha_ = 2.0;
     double gamma0_[3] = {0, 0, 0}, rho_[3] = {1, 1, 1}, eta_[3] = {1, 1, 1};
+    double gamma_set_[3] = {0, 0, 0};  // as given to set_nonlinear_transformation (reset restores)
     double sigma2_ = 0.0;
     int P_ = 8, PZ_ = 8, pyn_ = 0, zp_ = 0;
     int egrid_e_ = 0, egrid_s_ = 0;

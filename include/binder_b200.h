@@ -165,7 +165,8 @@ int binder_registration_set_stream(binder_registration *h, void *cuda_stream);
 int binder_registration_set_chain(binder_registration *h, uint32_t chain);
 
 /* No counterpart in the reference: restore the positions given at creation, the theta given to
- * set_mi_likelihood and a fresh iteration state, device to device (re-runs without host I/O). */
+ * set_mi_likelihood, the gammas given to set_nonlinear_transformation (the sampler keeps the
+ * gammas it draws) and a fresh iteration state, device to device (re-runs without host I/O). */
 int binder_registration_reset(binder_registration *h);
 
 /* Topology correction of the object's own current positions, on the device, in place.  Same

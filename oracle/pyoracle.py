@@ -123,6 +123,7 @@ def ref_lib():
     r.ref_jacobian2d.argtypes = [_dp, i, i, d, d, _dp]
     r.ref_topology3d.argtypes = [_dp, d, d, i, i, _dp, i, i, i, _dp]
     r.ref_topology2d.argtypes = [_dp, d, d, i, i, _dp, i, i, _dp]
+    r.ref_topology3d_mt.argtypes = [_dp, d, d, i, i, _dp, i, i, i, _dp, i, C.POINTER(d)]
     r.ref_up_sample.argtypes = [_dp, i, i, i, i, i, i, _dp]
     r.ref_smooth_deformation.argtypes = [_dp, _dp, _dp, _dp, i, i, i, d, d, _dp, _dp]
     r.ref_smooth_deformation.restype = d
@@ -145,6 +146,9 @@ def ref_lib():
     r.ref_sampler_seconds.argtypes = [_dp, _dp, i, i, i, _dp, _dp, d, _dp, i, i, _ip, _ip] + \
         [i] * 9
     r.ref_sampler_seconds.restype = d
+    r.ref_sampler.argtypes = [_dp, _dp, i, i, i, _dp, _dp, d, _dp, i, i, _ip, _ip] + \
+        [i] * 9 + [_dp, _dp]
+    r.ref_sampler.restype = d
     r.ref_em_filter.argtypes = [_dp, _dp] + [i] * 7 + [d, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
                                                        _dp, _dp, _dp, _dp, i, d, d, i, i, d, i,
                                                        _dp, _dp]
@@ -540,6 +544,24 @@ def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxel
     if timing is not None:
         timing.append(sec.value)
     return out, params[:npar]
+
+
+def ref_sampler(R, final_locations, voxel_pos, D, gamma, shape, nodes, voxels, alpha, theta,
+                seed, N_b, N_s, sample_gamma=1, every=1, posteriors=1, lik=1, transf=1,
+                threads=1):
+    """The reference's own Registration::sampler (compiled in oracle/_ref; R = ref_lib()) with the
+    MI likelihood from the given positions and theta [K][L].  Returns (mean [V*3], cov [V*9],
+    seconds of the sampler call)."""
+    nx, ny, nz = shape
+    V = nx * ny * nz
+    K, L = np.asarray(theta).shape
+    mean, cov = np.zeros(V * 3), np.zeros(V * 9)
+    sec = R.ref_sampler(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz,
+                        _c64(np.asarray(gamma, np.float64)), _c64(D).ravel(), float(alpha),
+                        _c64(theta).ravel(), K, L, _c32i(nodes).ravel(), _c32i(voxels).ravel(),
+                        int(seed), int(N_b), int(N_s), int(sample_gamma), int(every),
+                        int(posteriors), int(lik), int(transf), int(threads), mean, cov)
+    return mean, cov, sec
 
 
 def ref_em_filter(R, final_locations, voxel_pos, D, gamma, vshape, max_iter, mi=None, ssd=None,

@@ -44,6 +44,19 @@ void ref_topology3d(const double *field, double e1, double e2, int max_outer, in
     std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * nz * 3);
 }
 
+// the same on `threads` threads (the FFT plans' thread count), with the wall seconds of the call
+void ref_topology3d_mt(const double *field, double e1, double e2, int max_outer, int max_inner,
+                       const double *vs, int nx, int ny, int nz, double *out, int threads,
+                       double *seconds) {
+    topology_correction_3D tc;
+    const auto t0 = std::chrono::steady_clock::now();
+    const double *r =
+        tc.correct_topology(field, e1, e2, max_outer, max_inner, threads, vs, nx, ny, nz);
+    if (seconds)
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::memcpy(out, r, sizeof(double) * (size_t)nx * ny * nz * 3);
+}
+
 // topology_correction_2D::correct_topology (BINDER/src/cpu/topology_correction_2D.cpp:17-163)
 void ref_topology2d(const double *field, double e1, double e2, int max_outer, int max_inner,
                     const double *vs, int nx, int ny, double *out) {
@@ -220,7 +233,29 @@ void ref_em_filter(const double *final_locations, const double *voxel_pos, int n
 }
 
 // Registration::sampler (Registration.cpp:515-642) with the MI likelihood on `threads` threads:
-// N_b + N_s sweeps with the given switches; returns the wall seconds of the sampler call
+// N_b + N_s sweeps with the given switches from the given positions and theta; mean_out [V*N]
+// and cov_out [V*N*N] receive the sampler's moments (mean, M2 / (N_s - 1)); returns the wall
+// seconds of the sampler call
+double ref_sampler(const double *final_locations, const double *voxel_pos, int nx, int ny, int nz,
+                   const double gamma[3], const double *D, double alpha, const double *theta,
+                   int K, int L, const int *nodes, const int *voxels, int seed, int N_b, int N_s,
+                   int sample_gamma, int every, int posteriors, int lik_params,
+                   int transf_params, int threads, double *mean_out, double *cov_out) {
+    Registration r(final_locations, threads, voxel_pos, voxel_pos, nx, ny, nz, nx, ny, nz, 3,
+                   (double)nx * ny * nz);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], 1, 1, 1, 1, 1, 1, D);
+    r.setMILikelihood(alpha, theta, K, L, threads, nodes, voxels);
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = r.sampler(seed, N_b, N_s, sample_gamma, every, posteriors, lik_params,
+                               transf_params);
+    const double sec =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (mean_out) std::memcpy(mean_out, res.first.data(), sizeof(double) * res.first.size());
+    if (cov_out) std::memcpy(cov_out, res.second.data(), sizeof(double) * res.second.size());
+    return sec;
+}
+
+// the same, the wall seconds alone
 double ref_sampler_seconds(const double *final_locations, const double *voxel_pos, int nx, int ny,
                            int nz, const double gamma[3], const double *D, double alpha,
                            const double *theta, int K, int L, const int *nodes, const int *voxels,

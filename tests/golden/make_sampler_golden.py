@@ -1,0 +1,83 @@
+"""Fixture for the sampler's parity in distribution: the reference's own Registration::sampler
+(BINDER/src/cpu/Registration.cpp:515-642, compiled unmodified in oracle/_ref) run as 32 independent
+chains from the same positions and theta, every sampling switch on.
+
+Draws cannot match draw for draw (the reference uses std::mt19937 streams, this project Philox), so
+the fixture holds per-voxel chain statistics: the mean over chains of each chain's sampler mean
+and covariance, and their variance over chains.  A sampler whose chains follow the same Markov
+kernel from the same start has the same expected chain mean and covariance whatever its random
+numbers, so the difference of the two across-chain means divided by its standard error is a
+z-score per voxel (tests/test_oracle.py and tests/test_gpu_sampler_reference.py).
+
+Run from the repository root:  python tests/golden/make_sampler_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from binder_b200 import phantoms  # noqa: E402
+from binder_b200.utils import bin_signal_robust, initialize_fourier_domain_smoothing  # noqa: E402
+from oracle import pyoracle  # noqa: E402
+
+SHAPE, K, L = (12, 14, 10), 16, 12
+CHAINS, N_B, N_S = 32, 20, 200
+SEED0 = 1000
+UPPER = [0, 1, 2, 4, 5, 8]  # xx, xy, xz, yy, yz, zz of a row-major 3x3
+
+
+def case():
+    rng = np.random.default_rng(20261204)
+    pair = phantoms.make_pair(SHAPE, 7, bins=L, n_objects=10, axes=(2.0, 6.0), rms=1.0,
+                              spacing=3.0)
+    v, _ = bin_signal_robust(pair.moving, K)
+    grid = phantoms.identity_positions(SHAPE)
+    d0 = grid + phantoms.smooth_random_field(SHAPE, 0.6, 3.0, rng)
+    theta = rng.random((K, L)) + 0.05
+    theta /= theta.sum(1, keepdims=True)
+    D = initialize_fourier_domain_smoothing(SHAPE, True, 2, 3)
+    return dict(d0=d0, grid=grid, u=pair.u.astype(np.int32), v=v.astype(np.int32), theta=theta,
+                D=D, gamma=np.array([0.8, 0.6, 1.1]))
+
+
+def chain_stats(means, covs):
+    """per-voxel mean over chains and variance over chains (ddof 1) of the chain means [C, V, 3]
+    and of the upper-triangle covariances [C, V, 6]"""
+    m, c = np.asarray(means), np.asarray(covs)
+    return m.mean(0), m.var(0, ddof=1), c.mean(0), c.var(0, ddof=1)
+
+
+def main():
+    R = pyoracle.ref_lib()
+    assert R is not None, "oracle/_ref/libbinder_ref.so is needed (make -C oracle)"
+    c = case()
+    V = int(np.prod(SHAPE))
+    means, covs = [], []
+    # the reference prints every sweep on stdout
+    saved = os.dup(1)
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    try:
+        for ch in range(CHAINS):
+            m, cv, _ = pyoracle.ref_sampler(R, c["d0"], c["grid"], c["D"], c["gamma"], SHAPE,
+                                            c["v"], c["u"], 2.0, c["theta"], SEED0 + ch, N_B, N_S)
+            means.append(m.reshape(V, 3))
+            covs.append(cv.reshape(V, 9)[:, UPPER])
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    mm, mv, cm, cvv = chain_stats(means, covs)
+    np.savez_compressed(os.path.join(HERE, "sampler_ref.npz"), shape=np.array(SHAPE), K=K, L=L,
+                        chains=CHAINS, N_b=N_B, N_s=N_S, alpha=2.0, d0=c["d0"], u=c["u"],
+                        v=c["v"], theta=c["theta"], D=c["D"], gamma=c["gamma"], mean_mean=mm,
+                        mean_var=mv, cov_mean=cm, cov_var=cvv)
+    print("sampler_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
+
+
+if __name__ == "__main__":
+    main()

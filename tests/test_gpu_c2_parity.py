@@ -1,0 +1,93 @@
+"""Parity at the full 160x192x160 size against the reference's own CPU code
+(tests/golden/c2_ref.npz, from tests/golden/make_c2_golden.py).
+
+EM: the benchmark's MI pair (64 bins, seed 20260001) from the identity grid, 5 EM iterations,
+against the reference's Registration::EM.  Tolerances: positions 2e-3 voxels (FP32 positions and
+FP32 histogram over 4.9 M voxels against FP64), theta 1e-3 relative where theta > 1e-3, the
+min-log-posterior per voxel 1e-5 relative per iteration, and the FP64 mutual information of the
+final field within 1e-3 relative (the bar for "equal final MI").  The Jacobian statistics of the
+final field (negative count, counts outside [0.01, 100]) are identical.
+
+Topology: a 160x192x160 field violating [0.01, 100] in 3,549 voxels, corrected by the GPU
+(FP64) and by the reference's topology_correction_3D: the same outer / inner iteration counts,
+the same Jacobian counts before and after, and the corrected positions within 1e-8 at 20,000
+random voxels and at every initially violating voxel."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixture_module():
+    spec = importlib.util.spec_from_file_location(
+        "make_c2_golden", os.path.join(GOLDEN, "make_c2_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+@pytest.fixture(scope="module")
+def c2():
+    return _fixture_module(), golden("c2_ref.npz")
+
+
+def test_c2_em_matches_reference(core, oracle, c2):
+    mk, g = c2
+    import bench
+    inp = bench.make_inputs(0)
+    pair, V = inp["pair"], inp["V"]
+    np.testing.assert_array_equal(mk.checksum(pair.u), g["u_sum"])  # the same phantom pair
+    np.testing.assert_array_equal(mk.checksum(pair.v), g["v_sum"])
+    its = int(g["em_iters"])
+    reg = bench.setup_registration(core, inp)
+    assert reg.EM(its, -1e300, 1, 0) == its
+    final = reg.get_final_locations_as_numpy_array().reshape(V, 3).astype(np.float64)
+    theta = reg.get_likelihood_parameters()[: bench.BINS ** 2].reshape(bench.BINS, bench.BINS)
+    mlp = reg.iteration_stats()[:, 3] / inp["nzv"]
+    idx = g["idx"]
+    dpos = np.abs(final[idx] - g["em_final"])
+    th_ref = g["em_theta"]
+    big = th_ref > 1e-3
+    th_rel = np.abs(theta.astype(np.float64)[big] - th_ref[big]) / th_ref[big]
+    oracle.set_threads(os.cpu_count() or 1)
+    _, _, hist, _ = oracle.estep(final, pair.u, pair.v, theta.astype(np.float64), bench.SHAPE,
+                                 bench.SHAPE, bench.BINS, bench.BINS)
+    mi = oracle.mutual_information(hist, bench.BINS, bench.BINS)
+    mi_rel = abs(mi - float(g["em_mi"])) / float(g["em_mi"])
+    print(f"C2 EM: max |dpos| {dpos.max():.2e} (99.9% {np.quantile(dpos, 0.999):.2e}), theta max "
+          f"rel {th_rel.max():.2e}, mlp/voxel rel {np.max(np.abs(mlp / g['em_mlp_per_voxel'] - 1)):.2e}"
+          f", MI {mi:.8f} vs {float(g['em_mi']):.8f} (rel {mi_rel:.2e})")
+    assert dpos.max() < 2e-3
+    assert th_rel.max() < 1e-3
+    np.testing.assert_allclose(mlp, g["em_mlp_per_voxel"], rtol=1e-5)
+    assert mi_rel < 1e-3
+    J = core.compute_jacobian_determinant_3D(final, *bench.SHAPE, 1.0, 1.0, 1.0).ravel()
+    jr = g["em_jac"]
+    assert (int((J < 0).sum()), int((J < 0.01).sum()), int((J > 100).sum())) == \
+        (int(jr[2]), int(jr[3]), int(jr[4]))
+    np.testing.assert_allclose([J.min(), J.max()], jr[:2], rtol=1e-3)
+
+
+def test_c2_topology_matches_reference(core, c2):
+    mk, g = c2
+    import bench
+    f0 = mk.topology_field()
+    np.testing.assert_array_equal(mk.checksum(f0), g["topo_field_sum"])
+    e1, e2, outer, inner = g["topo_e"]
+    tc = core.topology_correction_3D()
+    out = tc.correct_topology(f0, e1, e2, int(outer), int(inner), 1, [1.0, 1.0, 1.0],
+                              *bench.SHAPE).reshape(-1, 3)
+    st = tc.last_stats
+    assert (st["outer_iterations"], st["inner_iterations"]) == tuple(int(x) for x in g["topo_iters"])
+    tb, ta = g["topo_before"], g["topo_after"]
+    assert (st["below_e1_before"], st["above_e2_before"]) == (int(tb[3]), int(tb[4]))
+    assert (st["below_e1_after"], st["above_e2_after"]) == (int(ta[3]), int(ta[4]))
+    err_idx = np.abs(out[g["idx"]] - g["topo_out_at_idx"]).max()
+    err_viol = np.abs(out[g["topo_viol_idx"]] - g["topo_out_at_viol"]).max()
+    print(f"C2 topology: max |d| {err_idx:.2e} (random voxels), {err_viol:.2e} (violating voxels)")
+    assert err_idx < 1e-8 and err_viol < 1e-8

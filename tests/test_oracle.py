@@ -1,5 +1,7 @@
 """The FP64 oracle against the reference's own outputs (golden fixtures from its compiled CPU
 sources), published known-answer vectors, and the analytic checks of the reference's tests."""
+import os
+
 import numpy as np
 import pytest
 from scipy import fft as sfft
@@ -309,3 +311,43 @@ def test_filter_em_runs_match_reference_driver(oracle):
     np.testing.assert_allclose(d, g["ssdf_final"], rtol=0, atol=1e-11)
     Mf, F = g["ssdf_coeff"].shape
     np.testing.assert_allclose(np.array(p.coeff[:Mf * F]), g["ssdf_params"], rtol=1e-10, atol=1e-12)
+
+
+def _oracle_chains(oracle, g, gamma, chains=32, seed0=5000):
+    import math
+    from sampler_stats import UPPER
+    shape = tuple(int(s) for s in g["shape"])
+    V = int(np.prod(shape))
+    K, L = int(g["K"]), int(g["L"])
+    grid = np.stack(np.indices(shape), -1).astype(np.float64)
+    oracle.set_threads(os.cpu_count() or 1)
+    means, covs = [], []
+    for ch in range(chains):
+        m, cv, *_ = oracle.sampler(g["d0"], np.zeros_like(g["d0"]), grid, g["u"], g["v"],
+                                   g["theta"], float(g["alpha"]), g["D"], gamma,
+                                   math.sqrt(9.0 / (8.0 * math.pi)), [1, 1, 1], [1, 1, 1], shape,
+                                   shape, K, L, seed0 + ch, int(g["N_b"]), int(g["N_s"]),
+                                   sample_gamma=1, sample_gamma_every=1, chain=ch)
+        means.append(m.reshape(V, 3))
+        covs.append(cv.reshape(V, 9)[:, UPPER])
+    return means, covs
+
+
+def test_oracle_sampler_matches_reference_in_distribution(oracle):
+    """32 oracle chains against 32 chains of the reference's own Registration::sampler from the
+    same start, every switch on (categorical draws, Dirichlet theta, DCT-domain noise, nu):
+    chain means and covariances agree within Monte Carlo error."""
+    from sampler_stats import agrees, fixture, summary, zscores
+    g = fixture()
+    zm, zc = zscores(g, *_oracle_chains(oracle, g, g["gamma"]))
+    assert agrees(zm), summary(zm)
+    assert agrees(zc), summary(zc)
+
+
+def test_sampler_parity_check_has_power(oracle):
+    """The same check rejects a sampler with a planted mistake: the oracle run with the prior's
+    precisions gamma tripled (a wrong model) leaves Monte Carlo error far behind."""
+    from sampler_stats import agrees, fixture, summary, zscores
+    g = fixture()
+    zm, zc = zscores(g, *_oracle_chains(oracle, g, 3.0 * g["gamma"], chains=8))
+    assert not agrees(zm) or not agrees(zc), (summary(zm), summary(zc))
