@@ -51,13 +51,18 @@ GIBBS_SHAPE = (96, 96, 96)
 GIBBS_CHAINS = 32
 GIBBS_BURN, GIBBS_SAMPLES = 20, 80  # sweeps per chain in the timed window
 GIBBS_SEED = 1000
+# compulsory HBM bytes per voxel of one post-burn-in sweep: E-step (positions 12, bins ~2, dream
+# 12), M-step (dream 12, positions 12), FP64 Welford (positions 12, mean 24 x 2, M2 48 x 2) ~ 210
+GIBBS_BYTES_PER_VOXEL = 210.0
 
 
 def run_gibbs(core, rank, chains, dist):
-    """Gibbs sweeps/s: `chains` chains of GIBBS_BURN + GIBBS_SAMPLES sweeps on a 96^3 MI pair
-    (64 bins) after 10 EM iterations, one Registration, Philox chain index = chain number.  The
-    device time of each sampler call (CUDA events on the engine stream) is summed; e2e adds the
-    FP64 mean / covariance read-back of every call."""
+    """Gibbs sweeps/s: `chains` chains of GIBBS_BURN + GIBBS_SAMPLES sweeps on a 96^3 MI pair (64
+    bins) after 10 EM iterations, all chains in one batch (sampler_chains: every kernel of a sweep
+    launched once for all chains; Philox chain index = chain number).  value: device time of the
+    batch call (CUDA events on the engine stream); e2e: the call through the public API with the
+    chains' pooled FP64 mean / covariance read back.  For comparison the same chains run one
+    sampler call after another (the reference's one-chain-per-object shape)."""
     from binder_b200 import phantoms
     from binder_b200.replicas import unit_seed
     from binder_b200.utils import initialize_fourier_domain_smoothing
@@ -72,27 +77,43 @@ def run_gibbs(core, rank, chains, dist):
     reg.setMILikelihood(ALPHA, np.full((BINS, BINS), 1.0 / BINS, np.float32), BINS, BINS, 1,
                         pair.v, pair.u)
     reg.EM(10, -1e300, 1, 0)
-    reg.sampler(GIBBS_SEED, 2, 3, 1, 1, 1, 1, 1)  # warm-up
+    start = reg.get_final_locations_as_numpy_array().astype(np.float64)
+    theta = reg.get_likelihood_parameters()[: BINS * BINS].astype(np.float64)
+    sweeps_per_chain = GIBBS_BURN + GIBBS_SAMPLES
+    seed = unit_seed(GIBBS_SEED, rank)
+    reg.sampler_chains(seed, chains, 2, 3, 1, 1, 1, 1, 1, per_chain=False)  # warm-up
     barrier(dist)
-    dev_ms = 0.0
+    reg.sampler_chains(seed, chains, GIBBS_BURN, GIBBS_SAMPLES, 1, 1, 1, 1, 1, per_chain=False,
+                       pooled=False)
+    dev_ms = max_over_ranks(reg.last_elapsed_ms(), dist)
     t0 = time.perf_counter()
-    for c in range(chains):
+    reg.sampler_chains(seed, chains, GIBBS_BURN, GIBBS_SAMPLES, 1, 1, 1, 1, 1, per_chain=False)
+    wall = max_over_ranks(time.perf_counter() - t0, dist)
+    # the same chains one call after another
+    seq_ms = 0.0
+    n_seq = min(chains, 4)
+    for c in range(n_seq):
         reg.set_chain(c)
-        reg.sampler(unit_seed(GIBBS_SEED, c), GIBBS_BURN, GIBBS_SAMPLES, 1, 1, 1, 1, 1)
-        dev_ms += reg.last_elapsed_ms()
-    wall = time.perf_counter() - t0
-    dev_ms = max_over_ranks(dev_ms, dist)
-    wall = max_over_ranks(wall, dist)
+        reg.sampler(seed, GIBBS_BURN, GIBBS_SAMPLES, 1, 1, 1, 1, 1)
+        seq_ms += reg.last_elapsed_ms()
+        reg.reset()
     world = dist.get_world_size() if dist is not None else 1
-    sweeps = world * chains * (GIBBS_BURN + GIBBS_SAMPLES)
-    cpu = cpu_gibbs(pair, grid, D, g) if rank == 0 else None
+    sweeps = world * chains * sweeps_per_chain
+    hbm = hbm_peak()[0]
+    achieved = GIBBS_BYTES_PER_VOXEL * V * chains * sweeps_per_chain / (dev_ms * 1e-3) / 1e9
+    cpu = cpu_gibbs(pair, start, theta, D, g) if rank == 0 else None
     return {"metric": f"Gibbs sweeps/s (96x96x96 MI pair, 64 bins, {chains} chains x "
-                      f"{GIBBS_BURN + GIBBS_SAMPLES} sweeps, all sampling switches on)",
+                      f"{sweeps_per_chain} sweeps in one batch, all sampling switches on)",
             "value": sweeps / (dev_ms / 1e3), "unit": "sweeps/s", "higher_is_better": True,
-            "ms_per_sweep": dev_ms / (chains * (GIBBS_BURN + GIBBS_SAMPLES)),
+            "ms_per_sweep": dev_ms / (chains * sweeps_per_chain),
+            "ms_per_batch_sweep": dev_ms / sweeps_per_chain,
+            "sequential_chains_sweeps_per_s": n_seq * sweeps_per_chain / (seq_ms / 1e3),
             "e2e": {"value": sweeps / wall, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": int(chains * V * 12 * 8)},
-            "sample_moments": "FP64 Welford, mean [V,3] + covariance [V,3,3] per chain",
+                    "d2h_bytes_per_step": int(V * 12 * 8)},
+            "roofline": {"bound": "hbm", "bytes_per_voxel_sweep": GIBBS_BYTES_PER_VOXEL,
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm},
+            "sample_moments": "FP64 Welford per chain, pooled mean [V,3] + covariance [V,3,3]",
             "cpu_baseline": cpu}
 
 
@@ -124,36 +145,38 @@ class stdout_to_stderr:
         os.close(self.saved)
 
 
-def cpu_gibbs(pair, grid, D, g, sweeps=2):
+def cpu_gibbs(pair, start, theta, D, g, sweeps=3):
     """Sweeps/s of the reference's own sampler (Registration::sampler, all host cores) on the same
-    96^3 pair, or of the FP64 oracle sampler where the reference library is absent."""
+    96^3 pair from the same state as the GPU chains (the positions and theta after the 10 EM
+    iterations), or of the FP64 oracle sampler where the reference library is absent."""
     from oracle import pyoracle
     threads = os.cpu_count() or 1
     shape = GIBBS_SHAPE
-    x = grid.astype(np.float64)
+    x = phantoms_grid(shape)
     R = ref_lib()
     if R is not None:
-        theta = np.full(BINS * BINS, 1.0 / BINS)
         with stdout_to_stderr():
-            t = R.ref_sampler_seconds(np.ascontiguousarray(x).ravel(),
-                                      np.ascontiguousarray(x).ravel(), *shape,
-                                      np.array([g, g, g], np.float64),
-                                      np.ascontiguousarray(D, np.float64).ravel(), ALPHA, theta,
-                                      BINS, BINS, np.ascontiguousarray(pair.v, np.int32).ravel(),
-                                      np.ascontiguousarray(pair.u, np.int32).ravel(), GIBBS_SEED,
-                                      0, sweeps, 1, 1, 1, 1, 1, threads)
+            _, _, t = pyoracle.ref_sampler(R, start, x, D.astype(np.float64), (g, g, g), shape,
+                                           pair.v, pair.u, ALPHA, theta.reshape(BINS, BINS),
+                                           GIBBS_SEED, 0, sweeps, threads=threads)
         return {"value": sweeps / t, "unit": "sweeps/s", "cores": threads, "kind": "reference",
-                "sample": f"{sweeps} sweeps of the 96^3 pair from the identity grid ({t:.2f} s) "
-                          f"by {REF_NOTE}"}
+                "sample": f"{sweeps} sweeps (every switch on) of the 96^3 pair from the GPU chains' "
+                          f"start state ({t:.2f} s) by {REF_NOTE}"}
     pyoracle.set_threads(threads)
     t0 = time.perf_counter()
-    pyoracle.sampler(x, x, x, pair.u, pair.v, np.full(BINS * BINS, 1.0 / BINS), ALPHA,
-                     D.astype(np.float64), (g, g, g), math.sqrt(9.0 / (8.0 * math.pi)),
-                     (1.0, 1.0, 1.0), (1.0, 1.0, 1.0), shape, shape, BINS, BINS, GIBBS_SEED, 0,
-                     sweeps, 1, 1, 1, 1, 1)
+    pyoracle.sampler(start, start, x, pair.u, pair.v, theta, ALPHA, D.astype(np.float64),
+                     (g, g, g), math.sqrt(9.0 / (8.0 * math.pi)), (1.0, 1.0, 1.0),
+                     (1.0, 1.0, 1.0), shape, shape, BINS, BINS, GIBBS_SEED, 0, sweeps, 1, 1, 1,
+                     1, 1)
     t = time.perf_counter() - t0
     return {"value": sweeps / t, "unit": "sweeps/s", "cores": threads, "kind": "port",
-            "sample": f"{sweeps} sweeps of the 96^3 pair from the identity grid ({t:.2f} s)"}
+            "sample": f"{sweeps} sweeps of the 96^3 pair from the GPU chains' start state "
+                      f"({t:.2f} s)"}
+
+
+def phantoms_grid(shape):
+    from binder_b200 import phantoms
+    return phantoms.identity_positions(shape).astype(np.float64)
 
 
 C1_SHAPE = (128, 128)
@@ -368,6 +391,105 @@ def setup_registration(core, inp):
     return reg
 
 
+def hbm_peak():
+    """(GB/s, source) of the roofline denominator: the measured copy bandwidth in
+    MEASURED_PEAKS.json, else the pool's earlier measurement."""
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        hbm = None
+    return (float(hbm), "measured") if hbm else (6650.0, "fallback")
+
+
+# the violating 160x192x160 field of the timed topology correction: identity plus a smooth random
+# displacement (seed 777, 0.8-voxel RMS, 3-voxel correlation) with 3,549 voxels below e1 = 0.01
+TOPO_FIELD = dict(seed=777, rms=0.8, spacing=3.0)
+
+
+def topology_field():
+    from binder_b200 import phantoms
+    rng = np.random.default_rng(TOPO_FIELD["seed"])
+    return (phantoms.identity_positions(SHAPE).astype(np.float64) +
+            phantoms.smooth_random_field(SHAPE, TOPO_FIELD["rms"], TOPO_FIELD["spacing"], rng)
+            .astype(np.float64))
+
+
+def time_registration(core, inp, args, precision, steps, warmup):
+    """(ms per registration, final min-log-posterior per non-zero voxel, topology stats) of the
+    C2 step -- reset, EM, topology correction -- at a DCT precision, device-timed on the engine
+    stream"""
+    import torch
+    reg = setup_registration(core, inp)
+    reg.set_precision(precision)
+    stream = torch.cuda.ExternalStream(reg.stream())
+    topo = {}
+
+    def step():
+        reg.reset()
+        reg.EM(args.em_iters, -1e300, 1, 0)
+        topo.update(reg.correct_topology(TOPO["e1"], TOPO["e2"], TOPO["max_outer"],
+                                         TOPO["max_inner"], [1.0, 1.0, 1.0]))
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    mlp = float(reg.iteration_stats()[-1, 3] / inp["nzv"])
+    del reg
+    return e0.elapsed_time(e1) / steps, mlp, dict(topo)
+
+
+def run_topology(core, rank, dist):
+    """Topology correction of the violating 160x192x160 field (3,549 voxels with J < 0.01):
+    device-timed on the engine stream (positions restored device-to-device each repeat), and
+    through the public C-ABI entry point with the FP64 field from host memory and back."""
+    import torch
+    f0 = topology_field()
+    grid = f0.astype(np.float32)
+    reg = core.Registration(grid, 1, grid, grid, *SHAPE, *SHAPE, 3, float(np.prod(SHAPE)))
+    stream = torch.cuda.ExternalStream(reg.stream())
+    stats = {}
+    for _ in range(2):
+        reg.reset()
+        stats = reg.correct_topology(TOPO["e1"], TOPO["e2"], TOPO["max_outer"],
+                                     TOPO["max_inner"], [1.0, 1.0, 1.0])
+    reps = 3
+    torch.cuda.synchronize()
+    ms = 0.0
+    for _ in range(reps):
+        reg.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reg.correct_topology(TOPO["e1"], TOPO["e2"], TOPO["max_outer"], TOPO["max_inner"],
+                             [1.0, 1.0, 1.0])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms = max_over_ranks(ms / reps, dist)
+    del reg
+    tc = core.topology_correction_3D()
+    tc.correct_topology(f0, TOPO["e1"], TOPO["e2"], TOPO["max_outer"], TOPO["max_inner"], 1,
+                        [1.0, 1.0, 1.0], *SHAPE)
+    t0 = time.perf_counter()
+    tc.correct_topology(f0, TOPO["e1"], TOPO["e2"], TOPO["max_outer"], TOPO["max_inner"], 1,
+                        [1.0, 1.0, 1.0], *SHAPE)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    out = {"metric": "topology corrections/s (160x192x160 field violating [0.01, 100] in 3,549 "
+                     "voxels, 10/10 iterations)",
+           "value": 1e3 / ms, "unit": "corrections/s", "ms_per_correction": ms,
+           "iterations": [stats.get("outer_iterations"), stats.get("inner_iterations")],
+           "e2e": {"value": 1.0 / e2e_s, "unit": "corrections/s",
+                   "h2d_bytes_per_step": int(f0.nbytes), "d2h_bytes_per_step": int(f0.nbytes)}}
+    if rank == 0:
+        out["cpu_baseline"] = cpu_topology(f0)
+    return out
+
+
 def run_b200(args, rank, world, local, dist):
     import torch
     from binder_b200 import build
@@ -406,13 +528,13 @@ def run_b200(args, rank, world, local, dist):
     barrier(dist)
     ms = max_over_ranks(ms_local, dist)
     value = world * args.steps / (ms / 1e3)
+    mlp_fast = float(reg.iteration_stats()[-1, 3] / inp["nzv"])
 
     # per-stage device times (CUDA events, eager launches) and the E-step roofline
     est_ms = reg.profile_stage(0, 10)
     mstep_ms = reg.profile_stage(1, 5)
     theta_ms = reg.profile_stage(2, 10)
     reg.reset()
-    em_ms = None
     reg.EM(args.em_iters, -1e300, 1, 0)
     em_ms = reg.last_elapsed_ms()
     reg.reset()
@@ -447,23 +569,31 @@ def run_b200(args, rank, world, local, dist):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     e2e_value = world * args.steps / e2e_s
-
-    # Gibbs sampling throughput on the 96^3 pair (every rank runs its own chains)
     del reg
+
+    # the metric's comparison: the same registration with the plain FP32 DCT (CUDA cores) against
+    # the tensor-core path timed above
+    plain_ms, mlp_plain, topo_plain = time_registration(core, inp, args, 0, max(2, args.steps // 4),
+                                                        2)
+    plain_ms = max_over_ranks(plain_ms, dist)
+    arms = {"plain_fp32": {"ms_per_registration": plain_ms, "registrations_per_s": 1e3 / plain_ms,
+                           "final_mlp_per_voxel": mlp_plain,
+                           "J_below_e1": topo_plain.get("below_e1_before")},
+            "tensor_3xtf32": {"ms_per_registration": ms / args.steps,
+                              "registrations_per_s": 1e3 * args.steps / ms,
+                              "final_mlp_per_voxel": mlp_fast,
+                              "J_below_e1": topo_stats.get("below_e1_before")},
+            "speedup_vs_plain_fp32": plain_ms / (ms / args.steps)}
+
+    topology = run_topology(core, rank, dist)
+    # Gibbs sampling throughput on the 96^3 pair (every rank runs its own chains)
     gibbs = run_gibbs(core, rank, args.gibbs_chains, dist)
     # 2D registrations on the 128x128 pair
     reg2d = run_2d(core, rank, args.em_iters, dist)
 
     if rank != 0:
         return None
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except (OSError, ValueError):
-        pass
-    hbm = peaks.get("hbm_gbs")
-    peak_src = "measured" if hbm else "fallback"
-    hbm = hbm or 6650.0
+    hbm, peak_src = hbm_peak()
     achieved = ESTEP_BYTES_PER_VOXEL * V / (est_ms * 1e-3) / 1e9
     traffic = read_profile_traffic()
     line = {
@@ -471,27 +601,34 @@ def run_b200(args, rank, world, local, dist):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded phantom pair per rank)",
-        "config": {"workload": "C2 3D MI registration 160x192x160, 64 bins", "em_iterations":
-                   args.em_iters, "topology": TOPO, "gamma": GAMMA_INIT, "alpha": ALPHA,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "working set ~330 MB > 126 MB L2 (no flush needed)"},
+        "config": config_dict(args, world),
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": "registrations/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "estep_kernel<EM>", "bound": "hbm", "achieved": achieved,
-                     "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
+        "roofline": {"kernel": "estep_em_fast_kernel (E-step)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": ESTEP_BYTES_PER_VOXEL * V},
         "stage_ms": {"estep": est_ms, "mstep_dct": mstep_ms, "theta": theta_ms,
                      "em_iteration": (em_ms / args.em_iters) if em_ms else None,
                      "topology_stats": topo_stats},
         "em_iterations_per_s": world * args.em_iters / ((em_ms or 1) / 1e3),
+        "precision_arms": arms,
+        "topology_c2": topology,
         "gibbs": gibbs,
         "registration_2d": reg2d,
         "cpu_baseline": cpu_baseline(inp, args.em_iters),
     }
     return line
+
+
+def config_dict(args, world):
+    """the workload, shared by both arms' lines"""
+    return {"workload": "C2 3D MI registration 160x192x160, 64 bins", "em_iterations":
+            args.em_iters, "topology": TOPO, "gamma": GAMMA_INIT, "alpha": ALPHA,
+            "parallelism": f"replicas x{world}",
+            "l2": "working set ~330 MB > 126 MB L2 (no flush needed)"}
 
 
 def read_profile_traffic():
@@ -506,77 +643,156 @@ def read_profile_traffic():
     return None
 
 
-def cpu_time_em_iteration(inp, threads):
-    """(seconds, kind) of one EM iteration (E-step + theta update + DCT M-step) by the
-    reference's own EM driver (the EM call alone), or by the FP64 oracle port where the reference
-    library is absent."""
+class captured_stdout:
+    """The reference prints its per-phase times on stdout: collect them in a file (this
+    script's stdout carries one JSON line)."""
+
+    def __enter__(self):
+        import tempfile
+        sys.stdout.flush()
+        self.f = tempfile.TemporaryFile(mode="w+")
+        self.saved = os.dup(1)
+        os.dup2(self.f.fileno(), 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        self.f.seek(0)
+        self.text = self.f.read()
+        self.f.close()
+        sys.stderr.write(self.text[-4000:])
+
+
+def cpu_em_phases(inp, threads, iters):
+    """The reference's own EM driver on the C2 pair for `iters` iterations (all host cores): the
+    EM call's wall seconds and the per-iteration E-step ("Time updating theta and dream
+    locations") and M-step ("Time constraining transformation") seconds it prints
+    (BINDER/src/cpu/Registration.cpp:150-193); (None, ...) where the reference library is
+    absent, with the FP64 oracle port timed instead."""
+    import re
     from oracle import pyoracle
     pair = inp["pair"]
     grid = inp["grid"].astype(np.float64)
     R = ref_lib()
     if R is not None:
         tm = []
-        with stdout_to_stderr():
-            pyoracle.ref_em(R, grid, grid, inp["D"], inp["gamma"], SHAPE, SHAPE, pair.v, pair.u,
-                            1, mi=(ALPHA, inp["theta"].astype(np.float64).reshape(BINS, BINS)),
-                            non_zero_voxels=inp["nzv"], threads=threads, timing=tm)
-        return tm[0], "reference"
+        with captured_stdout() as log:
+            final, _ = pyoracle.ref_em(R, grid, grid, inp["D"], inp["gamma"], SHAPE, SHAPE,
+                                       pair.v, pair.u, iters,
+                                       mi=(ALPHA, inp["theta"].astype(np.float64).reshape(BINS,
+                                                                                          BINS)),
+                                       non_zero_voxels=inp["nzv"], threads=threads, timing=tm)
+        num = r"([-0-9.eE+]+)"
+        est = [float(x) for x in re.findall("Time updating theta and dream locations: " + num,
+                                            log.text)]
+        mst = [float(x) for x in re.findall("Time constraining transformation: " + num,
+                                            log.text)]
+        return "reference", tm[0], est, mst, final
     pyoracle.set_threads(threads)
     t0 = time.perf_counter()
-    pyoracle.em(grid, grid, pair.u, pair.v, inp["theta"].astype(np.float64), ALPHA, inp["D"],
-                inp["gamma"], math.sqrt(9.0 / (8.0 * math.pi)), SHAPE, SHAPE, BINS, BINS,
-                inp["nzv"], 1, -1e300)
-    return time.perf_counter() - t0, "port"
+    _, final, _, _ = pyoracle.em(grid, grid, pair.u, pair.v, inp["theta"].astype(np.float64),
+                                 ALPHA, inp["D"], inp["gamma"], math.sqrt(9.0 / (8.0 * math.pi)),
+                                 SHAPE, SHAPE, BINS, BINS, inp["nzv"], iters, -1e300)
+    t = time.perf_counter() - t0
+    return "port", t, [], [], final
 
 
-def cpu_sample_text(kind, threads, t, em_iters, tail=""):
-    who = f" by {REF_NOTE}" if kind == "reference" else " by the FP64 oracle port"
-    return (f"1 EM iteration of the 160x192x160 pair{who} on {threads} threads ({t:.2f} s{tail}), "
-            f"extrapolated to {em_iters} iterations; topology correction excluded (it would only "
-            "lower the CPU figure)")
+def cpu_topology_seconds(field, threads):
+    """wall seconds of the reference's topology_correction_3D::correct_topology (all host cores
+    for its FFTs) on `field` with the benchmark's e1, e2 and iteration limits, or None"""
+    from oracle import pyoracle
+    R = ref_lib()
+    if R is None:
+        return None
+    out = np.zeros(field.size)
+    sec = pyoracle.C.c_double(0.0)
+    with captured_stdout():
+        R.ref_topology3d_mt(np.ascontiguousarray(field, np.float64).ravel(), TOPO["e1"],
+                            TOPO["e2"], TOPO["max_outer"], TOPO["max_inner"], np.ones(3), *SHAPE,
+                            out, threads, pyoracle.C.byref(sec))
+    return sec.value
+
+
+def cpu_topology(field):
+    threads = os.cpu_count() or 1
+    t = cpu_topology_seconds(field, threads)
+    if t is None:
+        return None
+    return {"value": 1.0 / t, "unit": "corrections/s", "cores": threads, "kind": "reference",
+            "sample": f"one correction of the violating 160x192x160 field ({t:.2f} s) by "
+                      "BINDER/src/cpu/topology_correction_3D.cpp compiled in oracle/_ref "
+                      "(FFTW replaced by an FFT-based stand-in; its FFTs threaded over lines)"}
+
+
+CPU_EM_ITERS = 4  # the first iteration is dropped from the per-iteration means
+
+
+def cpu_registration(inp, em_iters, iters=CPU_EM_ITERS):
+    """The reference's CPU registration time of the C2 step, assembled from a bounded sample: the
+    mean E-step and M-step seconds of EM iterations 2..iters, times em_iters, plus its topology
+    correction of the sample's final field (which, like the GPU's, finds no violation)."""
+    threads = os.cpu_count() or 1
+    kind, wall, est, mst, final = cpu_em_phases(inp, threads, iters)
+    if est and mst and len(est) >= 2:
+        e, m = float(np.mean(est[1:])), float(np.mean(mst[1:]))
+        rest = max(0.0, wall - sum(est) - sum(mst)) / iters
+        t_iter = e + m + rest
+    else:
+        e = m = rest = None
+        t_iter = wall / iters
+    t_topo = cpu_topology_seconds(final, threads) or 0.0
+    t = em_iters * t_iter + t_topo
+    who = f"by {REF_NOTE}" if kind == "reference" else "by the FP64 oracle port"
+    return {"value": 1.0 / t, "unit": "registrations/s", "cores": threads, "kind": kind,
+            "seconds_per_registration": t,
+            "estep_s": e, "mstep_s": m, "other_s_per_iteration": rest, "topology_s": t_topo,
+            "sample": f"{iters} EM iterations of the 160x192x160 pair {who} on {threads} threads "
+                      f"(EM call {wall:.2f} s); per-iteration E-step {e} s and M-step {m} s "
+                      f"(means of iterations 2..{iters}; the M-step's DCTs run on the FFT-based "
+                      f"FFTW stand-in), x {em_iters} iterations, + topology correction of the "
+                      f"final field {t_topo:.2f} s"}
 
 
 def cpu_baseline(inp, em_iters):
-    threads = os.cpu_count() or 1
-    t, kind = cpu_time_em_iteration(inp, threads)
-    return {"value": 1.0 / (em_iters * t), "unit": "registrations/s", "cores": threads,
-            "kind": kind, "sample": cpu_sample_text(kind, threads, t, em_iters)}
+    return cpu_registration(inp, em_iters)
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation on the host cores (rank 0 only): `steps` EM
+    iterations of the C2 pair in one EM call (the per-iteration E-step and M-step times the
+    reference prints), extrapolated to a registration of em_iters iterations plus its topology
+    correction; the Gibbs and full-size topology figures alongside."""
     if rank != 0:
         return None
     inp = make_inputs(0)
-    threads = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        pass  # the oracle has no warm-up state; a warm-up would only repeat the bounded sample
-    runs = [cpu_time_em_iteration(inp, threads) for _ in range(max(1, min(args.steps, 2)))]
-    times, kind = [r[0] for r in runs], runs[0][1]
-    t = statistics.median(times)
-    value = 1.0 / (args.em_iters * t)
-    sample = cpu_sample_text(kind, threads, t, args.em_iters, f" median of {len(times)} steps")
-    return {"metric": metric(args.em_iters), "value": value, "unit": "registrations/s", "n_gpus": world,
-            "steps": len(times), "warmup": args.warmup, "ms_per_step": t * 1e3,
+    iters = max(CPU_EM_ITERS, args.steps)
+    cpu = cpu_registration(inp, args.em_iters, iters)
+    value = cpu["value"]
+    return {"metric": metric(args.em_iters), "value": value, "unit": "registrations/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cpu["seconds_per_registration"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded phantom pair)", "impl": "reference",
-            "config": {"workload": "C2 3D MI registration 160x192x160, 64 bins",
-                       "em_iterations": args.em_iters, "parallelism": "host cores"},
-            "cpu_baseline": {"value": value, "unit": "registrations/s", "cores": threads,
-                             "kind": kind, "sample": sample},
+            "data": "synthetic (seeded phantom pair per rank)", "impl": "reference",
+            "config": config_dict(args, world),
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": "registrations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
+            "topology_c2": cpu_topology(topology_field()),
             "gibbs": reference_gibbs()}
 
 
 def reference_gibbs():
-    """Gibbs sweeps/s of the oracle sampler on the 96^3 pair (the --impl reference line)."""
+    """Gibbs sweeps/s of the reference's sampler on the 96^3 pair from the identity grid (the
+    --impl reference line has no GPU EM to start from)."""
     from binder_b200 import phantoms
     from binder_b200.utils import initialize_fourier_domain_smoothing
     shape = GIBBS_SHAPE
     pair = phantoms.make_pair(shape, GIBBS_SEED, bins=BINS)
-    grid = phantoms.identity_positions(shape).astype(np.float32)
     D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
-    cpu = cpu_gibbs(pair, grid, D, GAMMA_INIT * float(np.prod(shape)))
+    cpu = cpu_gibbs(pair, phantoms_grid(shape), np.full(BINS * BINS, 1.0 / BINS), D,
+                    GAMMA_INIT * float(np.prod(shape)))
     return {"metric": "Gibbs sweeps/s (96x96x96 MI pair, 64 bins)", "value": cpu["value"],
             "unit": "sweeps/s", "cpu_baseline": cpu}
 

@@ -208,6 +208,33 @@ class Registration:
             int(sample_transformation_parameters), mean, cov))
         return mean.reshape(*self._shape, N), cov.reshape(*self._shape, N, N)
 
+    def sampler_chains(self, seed, chains, N_b, N_s, sample_gamma, sample_gamma_every,
+                       sample_posteriors, sample_likelihood_parameters,
+                       sample_transformation_parameters, per_chain=True, pooled=True):
+        """`chains` independent chains in one batch (no counterpart in the reference, which runs
+        one chain per object).  Returns (means [chains, *shape, N], covs [chains, *shape, N, N])
+        when per_chain, and (pooled mean [*shape, N], pooled cov [*shape, N, N]) when pooled, in
+        that order; chain c equals sampler() after set_chain(chain index + c), draw for draw."""
+        N, V, C = self._N, self._V, int(chains)
+        mean = _out(C * V * N, np.float64) if per_chain else None
+        cov = _out(C * V * N * N, np.float64) if per_chain else None
+        pm = _out(V * N, np.float64) if pooled else None
+        pc = _out(V * N * N, np.float64) if pooled else None
+
+        def ptr(a):
+            return None if a is None else a.ctypes.data
+
+        check(lib().binder_registration_sampler_chains(
+            self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, C, int(N_b), int(N_s), int(sample_gamma),
+            int(sample_gamma_every), int(sample_posteriors), int(sample_likelihood_parameters),
+            int(sample_transformation_parameters), ptr(mean), ptr(cov), ptr(pm), ptr(pc)))
+        out = []
+        if per_chain:
+            out += [mean.reshape(C, *self._shape, N), cov.reshape(C, *self._shape, N, N)]
+        if pooled:
+            out += [pm.reshape(*self._shape, N), pc.reshape(*self._shape, N, N)]
+        return tuple(out)
+
     # -- getters / setters -------------------------------------------------------------------
     def get_final_locations_as_numpy_array(self):
         out = _out(self._V * self._N, np.float32)
@@ -267,7 +294,8 @@ class Registration:
         check(lib().binder_registration_set_chain(self._h, int(chain)))
 
     def set_precision(self, precision):
-        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32."""
+        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32,
+        3 tensor-core BF16 split (three products), 4 tensor-core BF16."""
         check(lib().binder_registration_set_precision(self._h, int(precision)))
 
     def stream(self):
@@ -331,7 +359,8 @@ class NonLinearTransformation:
         return [int(v) for v in out]
 
     def set_precision(self, precision):
-        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32."""
+        """DCT pass arithmetic: 0 FP32 CUDA cores, 1 tensor-core 3xTF32, 2 tensor-core TF32,
+        3 tensor-core BF16 split (three products), 4 tensor-core BF16."""
         check(lib().binder_transform_set_precision(self._h, int(precision)))
 
     def smooth_deformation(self, deformation):

@@ -23,7 +23,7 @@ EXPORTS = [
     "binder_registration_set_mi_likelihood", "binder_registration_set_nonlinear_transformation",
     "binder_registration_set_mi_likelihood_filter",
     "binder_registration_set_ssd_likelihood_filter", "binder_registration_get_ssd_filter_parameters",
-    "binder_registration_em", "binder_registration_sampler",
+    "binder_registration_em", "binder_registration_sampler", "binder_registration_sampler_chains",
     "binder_registration_get_final_locations", "binder_registration_get_dream_locations",
     "binder_registration_set_dream_locations", "binder_registration_get_likelihood_parameters",
     "binder_registration_get_shape", "binder_registration_get_iteration_stats",
@@ -79,6 +79,7 @@ def _declare(lib):
         "binder_registration_set_nonlinear_transformation": [_P] + [_d] * 9 + [_f32],
         "binder_registration_em": [_P, _i, _d, _i, _i, C.POINTER(_i)],
         "binder_registration_sampler": [_P, _u64, _i, _i, _i, _i, _i, _i, _i, _f64, _f64],
+        "binder_registration_sampler_chains": [_P, _u64] + [_i] * 8 + [_P] * 4,
         "binder_registration_get_final_locations": [_P, _f32],
         "binder_registration_get_dream_locations": [_P, _f32],
         "binder_registration_set_dream_locations": [_P, _f32],

@@ -200,6 +200,22 @@ int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, 
     });
 }
 
+int binder_registration_sampler_chains(binder_registration *h, uint64_t seed, int chains,
+                                       int N_b, int N_s, int sample_gamma,
+                                       int sample_gamma_every, int sample_posteriors,
+                                       int sample_likelihood_parameters,
+                                       int sample_transformation_parameters, double *mean_out,
+                                       double *cov_out, double *pooled_mean_out,
+                                       double *pooled_cov_out) {
+    return guard([&] {
+        NEED(h);
+        h->impl->sampler_chains(seed, chains, N_b, N_s, sample_gamma, sample_gamma_every,
+                                sample_posteriors, sample_likelihood_parameters,
+                                sample_transformation_parameters, mean_out, cov_out,
+                                pooled_mean_out, pooled_cov_out);
+    });
+}
+
 int binder_registration_get_final_locations(const binder_registration *h, float *out) {
     return guard([&] {
         NEED(h);

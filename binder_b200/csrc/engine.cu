@@ -132,18 +132,21 @@ void DctSet::release(cudaStream_t s) {
     }
 }
 
-void MStep::init(int x, int y, int z, cudaStream_t s) {
+void MStep::init(int x, int y, int z, cudaStream_t s, int nchains) {
     nx = x; ny = y; nz = z;
     V = (long)x * y * z;
+    chains = nchains < 1 ? 1 : nchains;
     dct.init(x, y, z, s);
-    t1 = dalloc<float>((size_t)V * 3, s);
-    t2 = dalloc<float>((size_t)V * 3, s);
+    t1 = dalloc<float>((size_t)V * 3 * chains, s);
+    t2 = dalloc<float>((size_t)V * 3 * chains, s);
     precision = default_precision();
-    persistent = default_persistent();
+    // a persistent CTA's tiles span components (its cost sums could mix chains), and the fused 2D
+    // M-step runs one chain
+    persistent = chains == 1 && default_persistent();
     {
         const char *e = std::getenv("BINDER_B200_FUSED2D");
         const bool off = e && e[0] == '0' && e[1] == 0;
-        fused2d = !off && z == 1 && x <= kM2dMaxN && y <= kM2dMaxN;
+        fused2d = chains == 1 && !off && z == 1 && x <= kM2dMaxN && y <= kM2dMaxN;
     }
     for (int i = 0; i < 2; ++i) {
         BINDER_CUDA(cudaStreamCreate(&side[i]));
@@ -159,7 +162,7 @@ bool default_persistent() {
 
 int default_precision() {
     const char *e = std::getenv("BINDER_B200_PRECISION");
-    if (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == 0) return e[0] - '0';
+    if (e && e[0] >= '0' && e[0] <= '4' && e[1] == 0) return e[0] - '0';
     return kPrecTF32x3;
 }
 
@@ -202,7 +205,13 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     a.every = every < 1 ? 1 : every; a.seed = seed; a.chain = chain; a.rho_p = rho_p;
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
     const bool tc = precision != kPrecFP32Simt;
-    const int planes = precision == kPrecTF32 ? 1 : 2;
+    const int planes = (precision == kPrecTF32 || precision == kPrecBF16) ? 1 : 2;
+    if (chains > 1) {
+        // chains x components per launch: enough tiles to fill the GPU without stream branches
+        a.chain_comps = ncomp;
+        run_chain(a, 0, ncomp * chains, s, r, d, xpos, tc, planes);
+        return;
+    }
     // the tensor-core path runs one chain of passes per component, each on its own stream
     const bool branches = tc && !persistent && side[0] && side[1];
     if (branches) {
@@ -224,11 +233,12 @@ void MStep::run_chain(AxisArgs<float> a, int c0, int nc, cudaStream_t s, const f
                   const float *xpos, bool tc, int planes) {
     a.comp0 = c0;
     const bool two_d = nz == 1;
+    const bool bf16 = precision == kPrecBF16x3 || precision == kPrecBF16;
     auto pass = [&](int axis, bool inverse, int mode) {
         if (tc)
             launch_axis_pass_tc(a, inverse ? dct.uinv[axis] : dct.ufwd[axis],
                                 mode == kEpiSpectral ? &dct.uinv[axis] : nullptr, mode, nc,
-                                planes, s, persistent);
+                                planes, s, persistent && !bf16, bf16);
         else
             launch_axis_pass(a, mode, nc, s);
     };
@@ -342,6 +352,7 @@ Registration::~Registration() {
     dfree(stats_, s); dfree(st_, s); dfree(d0_, s); dfree(theta0_, s);
     dfree(ssd_, s); dfree(ssd0_, s); dfree(colmax_, s); dfree(colmax0_, s);
     dfree(fx_, s); dfree(fn_, s); dfree(fst_, s); dfree(fst0_, s); dfree(fstats_, s);
+    release_chains();
     delete topo_;
     mstep_.release(s);
     cudaStreamSynchronize(s);  // the frees complete, so the next object can reuse the memory
@@ -382,6 +393,7 @@ void Registration::load_bins(double alpha, const float *theta, int K, int L, int
                  "numbers of bins K and L must be in [1, 256]");
     BINDER_CUDA(cudaStreamSynchronize(stream_));  // buffers below may be in use
     em_graph_.clear();
+    release_chains();  // their theta and count buffers have the old K x L
     const cudaStream_t s = own_stream_;
     // zero-padded byte volume of the node bins, in the E-step's view (a 2D node grid nxn x nyn
     // is the volume nxn x 1 x nyn: its y axis is the packed axis and has no padded y rows); one
@@ -799,6 +811,156 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     for (int n = 0; n < 3; ++n) gamma0_[n] = h.gamma[n];  // the prior keeps sampled gammas
 }
 
+void Registration::release_chains() {
+    if (!cb_) return;
+    const cudaStream_t s = own_stream_;
+    dfree(cb_->d, s); dfree(cb_->r, s); dfree(cb_->theta, s); dfree(cb_->hcnt, s);
+    dfree(cb_->st, s); dfree(cb_->mean, s); dfree(cb_->m2, s);
+    cb_->mstep.release(s);
+    delete cb_;
+    cb_ = nullptr;
+}
+
+// The sweep of sampler() (BINDER/src/cpu/Registration.cpp:545-625) for a batch of independent
+// chains: each kernel of a sweep runs once for all chains (chain = blockIdx.y of the E-step,
+// Dirichlet and Welford kernels; chains x components of every DCT pass), so a sweep of C chains is
+// one graph of the same length as a sweep of one chain.
+void Registration::sampler_chains(uint64_t seed, int chains, int N_b, int N_s, int sample_gamma,
+                                  int sample_gamma_every, int sample_posteriors,
+                                  int sample_likelihood_parameters,
+                                  int sample_transformation_parameters, double *mean_out,
+                                  double *cov_out, double *pooled_mean, double *pooled_cov) {
+    if (lk_ != 0 && (sample_posteriors || sample_likelihood_parameters))
+        throw Error(kUnsupported, "a batch of chains samples with the MI likelihood only");
+    if (sample_posteriors || sample_likelihood_parameters) {
+        if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
+    }
+    if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
+    BINDER_CHECK(chains >= 1 && chains <= 1024, "chains must be in [1, 1024]");
+    BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
+    BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
+    BINDER_CHECK(!(pooled_mean || pooled_cov) || N_s >= 1,
+                 "pooled moments need at least one sample per chain");
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    const cudaStream_t so = own_stream_;
+    const int C = chains, N = N_, NM2 = N_ * (N_ + 1) / 2;
+    const size_t VN = (size_t)V_ * N, KL = (size_t)(K_ > 0 ? K_ : 1) * (L_ > 0 ? L_ : 1);
+    if (!cb_ || cb_->chains != C) {
+        release_chains();
+        cb_ = new ChainBatch();
+        cb_->chains = C;
+        cb_->d = dalloc<float>(VN * C, so);
+        cb_->r = dalloc<float>(VN * C, so);
+        cb_->theta = dalloc<float>(KL * C, so);
+        cb_->hcnt = dalloc<unsigned>(KL * C, so);
+        cb_->st = dalloc<DevState>((size_t)C, so);
+        cb_->mean = dalloc<double>(VN * C, so);
+        cb_->m2 = dalloc<double>((size_t)V_ * NM2 * C, so);
+        cb_->mstep.init(nx_, ny_, nz_, so, C);
+        BINDER_CUDA(cudaStreamSynchronize(so));
+    }
+    cb_->mstep.precision = mstep_.precision;
+    ChainBatch &b = *cb_;
+    // every chain starts from the object's positions, dream locations, theta and gammas
+    for (int c = 0; c < C; ++c) {
+        BINDER_CUDA(cudaMemcpyAsync(b.d + VN * c, d_, sizeof(float) * VN,
+                                    cudaMemcpyDeviceToDevice, stream_));
+        BINDER_CUDA(cudaMemcpyAsync(b.r + VN * c, r_, sizeof(float) * VN,
+                                    cudaMemcpyDeviceToDevice, stream_));
+        if (have_mi_)
+            BINDER_CUDA(cudaMemcpyAsync(b.theta + KL * c, theta_, sizeof(float) * KL,
+                                        cudaMemcpyDeviceToDevice, stream_));
+    }
+    BINDER_CUDA(cudaMemsetAsync(b.hcnt, 0, sizeof(unsigned) * KL * C, stream_));
+    BINDER_CUDA(cudaMemsetAsync(b.mean, 0, sizeof(double) * VN * C, stream_));
+    BINDER_CUDA(cudaMemsetAsync(b.m2, 0, sizeof(double) * V_ * NM2 * C, stream_));
+    {
+        DevState h{};
+        for (int n = 0; n < 3; ++n) h.gamma[n] = gamma0_[n];
+        h.mlp_old = 1e100;
+        const double rp = rho_[0] * rho_[1] * rho_[2];
+        h.nu = gamma0_[0] / (rp * eta_[0] * eta_[0] * (double)V_);  // NonLinearTransformation.cpp:43
+        std::vector<DevState> hs((size_t)C, h);
+        BINDER_CUDA(cudaMemcpyAsync(b.st, hs.data(), sizeof(DevState) * C,
+                                    cudaMemcpyHostToDevice, stream_));
+        BINDER_CUDA(cudaStreamSynchronize(stream_));  // `hs` goes out of scope
+    }
+    const int total = N_b + N_s;
+    if (total > 0) {
+        const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
+        const double rho_p = rho_[0] * rho_[1] * rho_[2];
+        const int every = sample_gamma_every < 1 ? 1 : sample_gamma_every;
+        const int chunk = total < 16 ? total : 16;
+        EStepArgs e = estep_args(&b.st->done);
+        e.d = b.d; e.r = b.r; e.theta = b.theta; e.hcnt = b.hcnt; e.st = b.st; e.seed = seed;
+        Graph graph;
+        const long long kernels = capture_graph(stream_, graph, [&] {
+            for (int c = 0; c < chunk; ++c) {
+                if (sample_posteriors) launch_estep(e, true, egrid_s_, stream_, C);
+                if (sample_likelihood_parameters)
+                    launch_dirichlet_sample(b.theta, b.hcnt, K_, L_, alpha_, seed, chain_, b.st,
+                                            stream_, C);
+                if (sample_transformation_parameters) {
+                    b.mstep.enqueue(b.r, b.d, x_, D_, b.st, sigma2_, 1, sample_gamma, every, seed,
+                                    chain_, rho_p, eta2, &b.st->done, stream_);
+                    if (sample_gamma)
+                        launch_nu_sample(b.st, sample_gamma, every, N_, V_, rho_p, eta2, seed,
+                                         chain_, stream_, C);
+                }
+                launch_sweep_end(b.d, b.mean, b.m2, V_, N_, N_b, total, b.st, stream_, C);
+            }
+        });
+        cudaEvent_t t0, t1;
+        BINDER_CUDA(cudaEventCreate(&t0));
+        BINDER_CUDA(cudaEventCreate(&t1));
+        BINDER_CUDA(cudaEventRecord(t0, stream_));
+        for (int done = 0; done < total; done += chunk) replay(graph, kernels, stream_);
+        BINDER_CUDA(cudaEventRecord(t1, stream_));
+        BINDER_CUDA(cudaEventSynchronize(t1));
+        float ms = 0.0f;
+        BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+        last_ms_ = ms;
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (verbose())
+            std::printf("sampler: %d chains x %d sweeps in %.3f ms\n", C, total, ms);
+    }
+    // moments: per chain rearranged to AoS on the device and read back in one copy each, and / or
+    // pooled over the chains
+    const double scale = 1.0 / (double)(N_s - 1);
+    double *mstage = (mean_out || pooled_mean) ? dalloc<double>(VN * (mean_out ? C : 1), stream_)
+                                               : nullptr;
+    double *cstage = (cov_out || pooled_cov)
+                         ? dalloc<double>(VN * N * (cov_out ? C : 1), stream_)
+                         : nullptr;
+    if (mean_out || cov_out) {
+        for (int c = 0; c < C; ++c)
+            launch_moments_to_aos(b.mean + VN * c, b.m2 + (size_t)V_ * NM2 * c, V_, N, scale,
+                                  mean_out ? mstage + VN * c : nullptr,
+                                  cov_out ? cstage + VN * N * c : nullptr, stream_);
+        if (mean_out)
+            BINDER_CUDA(cudaMemcpyAsync(mean_out, mstage, sizeof(double) * VN * C,
+                                        cudaMemcpyDeviceToHost, stream_));
+        if (cov_out)
+            BINDER_CUDA(cudaMemcpyAsync(cov_out, cstage, sizeof(double) * VN * N * C,
+                                        cudaMemcpyDeviceToHost, stream_));
+    }
+    if (pooled_mean || pooled_cov) {
+        // after the per-chain copies above (same stream), the staging buffers are reused
+        launch_pool_moments(b.mean, b.m2, V_, N, C, (double)N_s, pooled_mean ? mstage : nullptr,
+                            pooled_cov ? cstage : nullptr, stream_);
+        if (pooled_mean)
+            BINDER_CUDA(cudaMemcpyAsync(pooled_mean, mstage, sizeof(double) * VN,
+                                        cudaMemcpyDeviceToHost, stream_));
+        if (pooled_cov)
+            BINDER_CUDA(cudaMemcpyAsync(pooled_cov, cstage, sizeof(double) * VN * N,
+                                        cudaMemcpyDeviceToHost, stream_));
+    }
+    dfree(mstage, stream_);
+    dfree(cstage, stream_);
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+}
+
 double Registration::profile_stage(int stage, int n) {
     require_ready();
     BINDER_CHECK(stage >= 0 && stage <= 2, "stage must be 0 (E-step), 1 (M-step) or 2 (theta)");
@@ -835,7 +997,8 @@ double Registration::profile_stage(int stage, int n) {
 }
 
 void Registration::set_precision(int p) {
-    BINDER_CHECK(p >= 0 && p <= 2, "precision must be 0 (FP32), 1 (3xTF32) or 2 (TF32)");
+    BINDER_CHECK(p >= 0 && p <= 4,
+                 "precision must be 0 (FP32), 1 (3xTF32), 2 (TF32), 3 (BF16x3) or 4 (BF16)");
     mstep_.precision = p;
     em_graph_.clear();
 }
@@ -851,7 +1014,8 @@ void Registration::set_chain(uint32_t c) {
 }
 
 void PriorTransform::set_precision(int p) {
-    BINDER_CHECK(p >= 0 && p <= 2, "precision must be 0 (FP32), 1 (3xTF32) or 2 (TF32)");
+    BINDER_CHECK(p >= 0 && p <= 4,
+                 "precision must be 0 (FP32), 1 (3xTF32), 2 (TF32), 3 (BF16x3) or 4 (BF16)");
     mstep_.precision = p;
 }
 

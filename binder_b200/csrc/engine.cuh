@@ -37,8 +37,11 @@ struct MStep {
     // one component's last partial wave of tiles overlaps the other components' passes
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    // a batch of chains: every pass runs over chains x components in one launch (per-tile
+    // tensor-core passes or the SIMT passes), the scratch holds [chains][3][V]
+    int chains = 1;
     // buffers from the stream-ordered pool on stream s
-    void init(int nx, int ny, int nz, cudaStream_t s);
+    void init(int nx, int ny, int nz, cudaStream_t s, int chains = 1);
     void release(cudaStream_t s);
     void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
                  double sigma2, int sample, int want_raw, int every, uint64_t seed, uint32_t chain,
@@ -96,6 +99,16 @@ class Registration {
     void sampler(uint64_t seed, int N_b, int N_s, int sample_gamma, int sample_gamma_every,
                  int sample_posteriors, int sample_likelihood_parameters,
                  int sample_transformation_parameters, double *mean_out, double *cov_out);
+    // `chains` independent chains of the sampler in one pass per step: chain c draws Philox chain
+    // index chain_ + c (what sampler() draws after set_chain(chain_ + c)) and starts from the
+    // object's current positions, theta and gammas, which stay as they are.  Per-chain moments
+    // mean_out [chains][V][N] / cov_out [chains][V][N][N], and / or the chains' pooled moments
+    // pooled_mean [V][N] / pooled_cov [V][N][N]; any output may be null.
+    void sampler_chains(uint64_t seed, int chains, int N_b, int N_s, int sample_gamma,
+                        int sample_gamma_every, int sample_posteriors,
+                        int sample_likelihood_parameters, int sample_transformation_parameters,
+                        double *mean_out, double *cov_out, double *pooled_mean,
+                        double *pooled_cov);
 
     // restore the positions given at construction, the theta given to set_mi_likelihood, the
     // gammas given to set_nonlinear_transformation and a fresh device state (device-to-device,
@@ -163,6 +176,17 @@ class Registration {
     DevState *st_ = nullptr;
     MStep mstep_;
     EmGraphCache em_graph_;
+    // buffers of the last batch of chains (kept for the next call with the same count)
+    struct ChainBatch {
+        int chains = 0;
+        float *d = nullptr, *r = nullptr, *theta = nullptr;
+        unsigned *hcnt = nullptr;
+        DevState *st = nullptr;
+        double *mean = nullptr, *m2 = nullptr;
+        MStep mstep;
+    };
+    ChainBatch *cb_ = nullptr;
+    void release_chains();
     // likelihood / prior parameters
     bool have_mi_ = false, have_tr_ = false;
     int K_ = 0, L_ = 0;

@@ -759,10 +759,24 @@ __global__ void features_to_soa_kernel(const double *in, long n, int C, double *
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
 // for the Gibbs draw and for EM with K > 64.
 template <bool SAMPLE, int DIM>
-__global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs a) {
+__global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs args) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     constexpr int R = 4 * Q;  // node rows of 4 packed nodes
-    if (a.skip && *a.skip) return;
+    if (args.skip && *args.skip) return;
+    // a batch of chains (gridDim.y > 1, sampling only): chain blockIdx.y has its own positions
+    // and dream locations [dim][V], theta and counts [K][L] and state, one chain after another,
+    // and Philox chain index chain + blockIdx.y; the bins are shared
+    EStepArgs a = args;
+    if (SAMPLE && blockIdx.y) {
+        const long cs = (long)blockIdx.y * a.dim * a.V;
+        const long ks = (long)blockIdx.y * a.K * a.L;
+        a.d += cs;
+        a.r += cs;
+        a.theta += ks;
+        a.hcnt += ks;
+        a.st += blockIdx.y;
+        a.chain += blockIdx.y;
+    }
     extern __shared__ __align__(16) float sm[];
     const int KL = a.K * a.L;
     float *th = sm;
@@ -979,6 +993,11 @@ __device__ double gamma_mt(double shape, uint64_t seed, uint32_t index, uint32_t
 // MILikelihood.cpp:132-169 (Registration.cu:426-442 on the GPU): one CTA per row k
 __global__ void dirichlet_sample_kernel(float *theta, unsigned *hcnt, int K, int L, double alpha,
                                         uint64_t seed, uint32_t chain, DevState *st) {
+    // chain blockIdx.y of a batch: its own theta, counts and state
+    theta += (long)blockIdx.y * K * L;
+    hcnt += (long)blockIdx.y * K * L;
+    st += blockIdx.y;
+    chain += blockIdx.y;
     if (st->done) return;
     __shared__ double red[32];
     const int k = blockIdx.x;
@@ -1003,6 +1022,8 @@ __global__ void dirichlet_sample_kernel(float *theta, unsigned *hcnt, int K, int
 __global__ void nu_sample_kernel(DevState *st, int sample_gamma, int every, int N, long V,
                                  double rho_p, double e0, double e1, double e2, uint64_t seed,
                                  uint32_t chain) {
+    st += blockIdx.x;  // chain blockIdx.x of a batch
+    chain += blockIdx.x;
     if (st->done) return;
     const int sweep = st->sweep;
     if (sample_gamma && (sweep % every == 0)) {
@@ -1045,6 +1066,11 @@ __global__ void em_finish_kernel(DevState *st, double *stats, int max_iter, doub
 template <int N>
 __global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long V, int N_b,
                                  DevState *st) {
+    // chain blockIdx.y of a batch: positions [N][V], mean [N][V], M2 [N (N + 1) / 2][V] per chain
+    d += (long)blockIdx.y * N * V;
+    mean += (long)blockIdx.y * N * V;
+    m2 += (long)blockIdx.y * (N * (N + 1) / 2) * V;
+    st += blockIdx.y;
     if (st->done) return;
     const int sweep = st->sweep;
     if (sweep >= N_b) {
@@ -1071,6 +1097,7 @@ __global__ void sweep_end_kernel(const float *d, double *mean, double *m2, long 
 }
 
 __global__ void sweep_advance_kernel(DevState *st, int total) {
+    st += blockIdx.x;  // chain blockIdx.x of a batch
     if (st->done) return;
     st->sweep += 1;
     if (st->sweep >= total) st->done = 1;
@@ -1223,7 +1250,7 @@ void launch_features_to_soa(const double *in, long n, int C, double *out, cudaSt
     BINDER_CUDA(cudaGetLastError());
 }
 
-void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) {
+void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, int chains) {
     BINDER_CHECK(!args.logt || (!sample && args.K <= kSmallK && args.colmax),
                  "the log-space E-step runs EM only, with at most 64 bins");
     BINDER_CHECK(!args.filter || (!sample && !args.logt && args.M >= 1 &&
@@ -1247,8 +1274,21 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s) 
     a.hscale = (float)std::ldexp(1.0, e);
     a.hinv = (float)std::ldexp(1.0, -e);
     BINDER_CHECK(a.dim == 2 || a.dim == 3, "dimension must be 2 or 3");
-    if (a.dim == 3) launch_estep_dim<3>(a, sample, grid, smem, s);
-    else launch_estep_dim<2>(a, sample, grid, smem, s);
+    BINDER_CHECK(chains >= 1 && chains <= 65535 && (chains == 1 || sample),
+                 "a batch of chains runs the sampling E-step only");
+    if (chains > 1) {
+        // the single-chain grid shared out over the chains (every CTA still loops over voxels)
+        const int gx = (grid + chains - 1) / chains;
+        const dim3 g2((unsigned)gx, (unsigned)chains, 1);
+        if (a.dim == 3)
+            count_launch(), estep_kernel<true, 3><<<g2, kEThreads, smem, s>>>(a);
+        else
+            count_launch(), estep_kernel<true, 2><<<g2, kEThreads, smem, s>>>(a);
+    } else if (a.dim == 3) {
+        launch_estep_dim<3>(a, sample, grid, smem, s);
+    } else {
+        launch_estep_dim<2>(a, sample, grid, smem, s);
+    }
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -1361,15 +1401,18 @@ void launch_ssd_update(float *table, float *colmax, float *hist, int K, int L, i
 }
 
 void launch_dirichlet_sample(float *theta, unsigned *hcnt, int K, int L, double alpha,
-                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s) {
+                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s,
+                             int chains) {
     const int threads = ((L + 31) / 32) * 32;
-    count_launch(), dirichlet_sample_kernel<<<K, threads, 0, s>>>(theta, hcnt, K, L, alpha, seed, chain, st);
+    count_launch(), dirichlet_sample_kernel<<<dim3((unsigned)K, (unsigned)chains), threads, 0, s>>>(
+                        theta, hcnt, K, L, alpha, seed, chain, st);
     BINDER_CUDA(cudaGetLastError());
 }
 
 void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, double rho_p,
-                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s) {
-    count_launch(), nu_sample_kernel<<<1, 1, 0, s>>>(st, sample_gamma, every, N, V, rho_p, eta2[0], eta2[1],
+                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s,
+                      int chains) {
+    count_launch(), nu_sample_kernel<<<chains, 1, 0, s>>>(st, sample_gamma, every, N, V, rho_p, eta2[0], eta2[1],
                                      eta2[2], seed, chain);
     BINDER_CUDA(cudaGetLastError());
 }
@@ -1381,21 +1424,23 @@ void launch_em_finish(DevState *st, double *stats, int max_iter, double th, doub
 }
 
 void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N, int N_b,
-                      int total, DevState *st, cudaStream_t s) {
+                      int total, DevState *st, cudaStream_t s, int chains) {
     int dev = 0, sms = 148;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     long need = (V + 255) / 256;
-    const long g = need < (long)sms * 8 ? (need < 1 ? 1 : need) : (long)sms * 8;
+    long g = need < (long)sms * 8 ? (need < 1 ? 1 : need) : (long)sms * 8;
+    if (chains > 1) g = (g + chains - 1) / chains;  // the same total CTAs over the chains
+    const dim3 grid((unsigned)g, (unsigned)chains);
     BINDER_CHECK(N == 2 || N == 3, "Welford moments need N = 2 or 3");
-    if (N == 3) count_launch(), sweep_end_kernel<3><<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
-    else count_launch(), sweep_end_kernel<2><<<(int)g, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    if (N == 3) count_launch(), sweep_end_kernel<3><<<grid, 256, 0, s>>>(d, mean, m2, V, N_b, st);
+    else count_launch(), sweep_end_kernel<2><<<grid, 256, 0, s>>>(d, mean, m2, V, N_b, st);
     BINDER_CUDA(cudaGetLastError());
-    launch_sweep_advance(st, total, s);
+    launch_sweep_advance(st, total, s, chains);
 }
 
-void launch_sweep_advance(DevState *st, int total, cudaStream_t s) {
-    count_launch(), sweep_advance_kernel<<<1, 1, 0, s>>>(st, total);
+void launch_sweep_advance(DevState *st, int total, cudaStream_t s, int chains) {
+    count_launch(), sweep_advance_kernel<<<chains, 1, 0, s>>>(st, total);
     BINDER_CUDA(cudaGetLastError());
 }
 

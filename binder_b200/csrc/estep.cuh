@@ -50,7 +50,9 @@ struct EStepArgs {
     float hscale, hinv;
 };
 
-void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s);
+// chains > 1: a batch of chains, the sampling E-step only (chain = blockIdx.y; buffers
+// [chains][dim][V] positions / dream locations, [chains][K][L] theta / counts, [chains] states)
+void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s, int chains = 1);
 int estep_grid(bool sample, int K, int L, long V, int dim, bool logt = false);
 // largest number of bins of the log-space (SSD) E-step
 constexpr int kLogMaxBins = 64;
@@ -105,19 +107,21 @@ void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, 
                          DevState *st, cudaStream_t s);
 // theta_k ~ Dirichlet(counts_k + alpha) with Philox gammas (tag 4, sweep = st->sweep); counts zeroed
 void launch_dirichlet_sample(float *theta, unsigned *hcnt, int K, int L, double alpha,
-                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s);
+                             uint64_t seed, uint32_t chain, DevState *st, cudaStream_t s,
+                             int chains = 1);
 // nu ~ Gamma(alpha0 + N V/2, beta0 + V/2 raw) when sample_gamma and sweep % every == 0;
 // gammas refreshed from nu.  Also resets raw_reg.
 void launch_nu_sample(DevState *st, int sample_gamma, int every, int N, long V, double rho_p,
-                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s);
+                      const double eta2[3], uint64_t seed, uint32_t chain, cudaStream_t s,
+                      int chains = 1);
 // EM bookkeeping: min-log-posterior, per-iteration stats, convergence flag
 void launch_em_finish(DevState *st, double *stats, int max_iter, double th, double nzv,
                       cudaStream_t s);
 // Welford mean [N][V] / symmetric M2 [N (N + 1) / 2][V] update in FP64 when sweep >= N_b, then
 // sweep += 1 (done once sweep reaches `total`)
 void launch_sweep_end(const float *d, double *mean, double *m2, long V, int N, int N_b,
-                      int total, DevState *st, cudaStream_t s);
+                      int total, DevState *st, cudaStream_t s, int chains = 1);
 // sweep += 1 (done once sweep reaches `total`)
-void launch_sweep_advance(DevState *st, int total, cudaStream_t s);
+void launch_sweep_advance(DevState *st, int total, cudaStream_t s, int chains = 1);
 
 }  // namespace binder

@@ -126,7 +126,46 @@ __global__ void moments_to_aos_kernel(const double *mean, const double *m2, long
     }
 }
 
+// moments of C chains of n samples each pooled (Chan et al.'s pairwise combination with equal
+// counts): mean = the average of the chain means, M2 = sum_c M2_c + n sum_c (m_c - m)(m_c - m)^T,
+// cov = M2 / (C n - 1); AoS outputs
+__global__ void pool_moments_kernel(const double *mean, const double *m2, long V, int N, int C,
+                                    double n, double *mean_aos, double *cov_aos) {
+    const int sym3[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    const int sym2[4] = {0, 1, 1, 2};
+    const int NM2 = N * (N + 1) / 2;
+    const double scale = 1.0 / ((double)C * n - 1.0);
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
+         i += (long)gridDim.x * blockDim.x) {
+        double m[3] = {0.0, 0.0, 0.0};
+        for (int c = 0; c < C; ++c)
+            for (int a = 0; a < N; ++a) m[a] += mean[((long)c * N + a) * V + i];
+        for (int a = 0; a < N; ++a) m[a] /= (double)C;
+        double q[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = 0; c < C; ++c) {
+            double dm[3];
+            for (int a = 0; a < N; ++a) dm[a] = mean[((long)c * N + a) * V + i] - m[a];
+            int e = 0;
+            for (int r = 0; r < N; ++r)
+                for (int t = r; t < N; ++t, ++e)
+                    q[e] += m2[((long)c * NM2 + e) * V + i] + n * dm[r] * dm[t];
+        }
+        if (mean_aos)
+            for (int a = 0; a < N; ++a) mean_aos[N * i + a] = m[a];
+        if (cov_aos)
+            for (int e = 0; e < N * N; ++e)
+                cov_aos[N * N * i + e] = q[N == 3 ? sym3[e] : sym2[e]] * scale;
+    }
+}
+
 }  // namespace
+
+void launch_pool_moments(const double *mean, const double *m2, long V, int N, int C, double n,
+                         double *mean_aos, double *cov_aos, cudaStream_t s) {
+    count_launch(), pool_moments_kernel<<<blocks_for(V), 256, 0, s>>>(mean, m2, V, N, C, n,
+                                                                       mean_aos, cov_aos);
+    BINDER_CUDA(cudaGetLastError());
+}
 
 void *dev_alloc(size_t bytes, cudaStream_t s) {
     if (!bytes) return nullptr;

@@ -61,5 +61,9 @@ void launch_bins_to_padded(const int *in, int nx, int ny, int nz, int limit, uin
 // stored as its upper triangle (xx, xy, xz, yy, yz, zz for N = 3; xx, xy, yy for N = 2)
 void launch_moments_to_aos(const double *mean, const double *m2, long V, int N, double scale,
                            double *mean_aos, double *cov_aos, cudaStream_t s);
+// C chains' FP64 moments (mean [C][N][V], upper-triangle M2 [C][N (N + 1) / 2][V], n samples per
+// chain) pooled into one mean [V][N] and covariance [V][N][N] (M2 / (C n - 1))
+void launch_pool_moments(const double *mean, const double *m2, long V, int N, int C, double n,
+                         double *mean_aos, double *cov_aos, cudaStream_t s);
 
 }  // namespace binder

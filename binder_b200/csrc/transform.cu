@@ -102,6 +102,12 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
     __shared__ double red[32];
 
     const int comp = blockIdx.z;
+    // components of a batch of chains are numbered chain * chain_comps + component: the chain
+    // picks the state and the Philox chain index, the component within it everything else
+    const int bch = a.chain_comps ? comp / a.chain_comps : 0;
+    const int cn = comp - bch * a.chain_comps;
+    DevState *const st = a.st ? a.st + bch : nullptr;
+    const uint32_t chain = a.chain + (uint32_t)bch;
     const T *in = a.in + comp * a.comp_stride;
     T *out = a.out + comp * a.comp_stride;
     const int n = a.n;
@@ -151,10 +157,10 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
         // x-axis pass (outer == 1, s == ny*nz): coefficient (k, t) has flat index k*s + t
         double part_cost = 0.0, part_raw = 0.0;
         if constexpr (MODE == kEpiSpectral) {
-            const double g = a.st->gamma[comp];
+            const double g = st->gamma[cn];
             const float gs2 = (float)(g * a.sigma2);
-            const uint32_t sweep = (uint32_t)a.st->sweep;
-            const bool want_raw = a.want_raw && (a.st->sweep % a.every == 0);
+            const uint32_t sweep = (uint32_t)st->sweep;
+            const bool want_raw = a.want_raw && (st->sweep % a.every == 0);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int k = ty + 16 * r;
@@ -168,10 +174,10 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
                         float v = (float)acc[r][q] * f;
                         if (a.sample)
                             v += sqrtf((float)a.sigma2 * f) *
-                                 prior_normal(a.seed, (uint32_t)i, sweep, a.chain, comp);
+                                 prior_normal(a.seed, (uint32_t)i, sweep, chain, cn);
                         const double v2 = (double)v * (double)v;
                         part_cost += 0.5 * g * (double)Dv * v2;
-                        if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)Dv * v2;
+                        if (want_raw) part_raw += a.eta2[cn] * a.rho_p * (double)Dv * v2;
                         acc[r][q] = (T)v;
                     }
                 }
@@ -181,10 +187,10 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
         }
         if constexpr (MODE == kEpiSpectral) {
             const double sc = block_sum(part_cost, red);
-            if (threadIdx.x == 0) atomicAdd(&a.st->lp_tr, sc);
+            if (threadIdx.x == 0) atomicAdd(&st->lp_tr, sc);
             if (a.want_raw) {  // uniform across the block: every thread takes the same branch
                 const double sr = block_sum(part_raw, red);
-                if (threadIdx.x == 0) atomicAdd(&a.st->raw_reg, sr);
+                if (threadIdx.x == 0) atomicAdd(&st->raw_reg, sr);
             }
         }
         __syncthreads();  // everyone is done reading Xs
@@ -220,15 +226,15 @@ __global__ void __launch_bounds__(kThreads) axis_kernel(const AxisArgs<T> a) {
                 const long i = base + e;
                 float xv;
                 if (a.xpos) {
-                    xv = a.xpos[comp * a.comp_stride + i];
+                    xv = a.xpos[cn * a.comp_stride + i];
                 } else {
                     const long yz = (long)a.ny * a.nz;
-                    xv = comp == 0 ? (float)(i / yz)
-                                   : (comp == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
+                    xv = cn == 0 ? (float)(i / yz)
+                                   : (cn == 1 ? (float)((i / a.nz) % a.ny) : (float)(i % a.nz));
                 }
                 val = (T)((float)val + xv);
             } else if constexpr (MODE == kEpiTopoOut) {
-                val = (T)((double)val * a.out_scale[comp] + a.out_offset[comp]);
+                val = (T)((double)val * a.out_scale[cn] + a.out_offset[cn]);
             }
             dst[e] = val;
         }

@@ -67,6 +67,9 @@ struct AxisArgs {
     double out_scale[3];   // kEpiTopoOut: per-component scale (voxel size / total)
     double out_offset[3];  // kEpiTopoOut: per-component offset (mean)
     const int *skip;       // when non-null and *skip != 0 the pass is a no-op
+    // a batch of chains: components chain * chain_comps + n (n < chain_comps) with states
+    // st[chain] and Philox chain indices chain + chain; 0 for one chain
+    int chain_comps;
 };
 
 // Launch one pass over `ncomp` components (blockIdx.z = component).

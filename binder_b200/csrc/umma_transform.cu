@@ -18,6 +18,8 @@
 #include "layout.cuh"
 #include "transform.cuh"
 #include "umma.cuh"
+#include <cuda_bf16.h>
+
 #include "umma_transform.cuh"
 
 namespace binder {
@@ -50,6 +52,7 @@ struct UArgs {
     int dims;  // 3, or 2 for an image (the contiguous axis is then component 1)
     int comp0;  // component of blockIdx.z == 0
     int ncomp;  // components of one persistent launch
+    int chain_comps;  // components per chain of a batch of chains (0: one chain)
     const int *skip;
 };
 
@@ -80,6 +83,36 @@ __device__ __forceinline__ void store_split(float *plane0, int off, float4 v) {
         const float4 lo = make_float4(umma::to_tf32(v.x - hi.x), umma::to_tf32(v.y - hi.y),
                                       umma::to_tf32(v.z - hi.z), umma::to_tf32(v.w - hi.w));
         *reinterpret_cast<float4 *>(plane0 + kAPlane + off) = lo;
+    }
+}
+
+// byte offset in a BF16 A plane of row `line`, K elements 4q .. 4q+3 of the chunk: two 16-byte K
+// columns of 8 elements 2 KB apart (LBO), 8-row groups 128 B apart (SBO), rows 16 B apart; four
+// elements fill half of a 16-byte slot
+__device__ __forceinline__ int a_slot_b16(int line, int q) {
+    return (q >> 1) * 2048 + (line >> 3) * 128 + (line & 7) * 16 + (q & 1) * 8;
+}
+
+// FP32 -> BF16 hi (round to nearest even) and, with PLANES == 2, lo = BF16(x - hi): the split of
+// the 3-product BF16 pass (hi.hi + hi.lo + lo.hi keeps ~16 mantissa bits of every product)
+template <int PLANES>
+__device__ __forceinline__ void store_split_b16(unsigned char *plane0, int off, float4 v) {
+    const __nv_bfloat162 h01 = __floats2bfloat162_rn(v.x, v.y);
+    const __nv_bfloat162 h23 = __floats2bfloat162_rn(v.z, v.w);
+    uint2 hw;
+    hw.x = *reinterpret_cast<const uint32_t *>(&h01);
+    hw.y = *reinterpret_cast<const uint32_t *>(&h23);
+    *reinterpret_cast<uint2 *>(plane0 + off) = hw;
+    if (PLANES == 2) {
+        // hi as FP32: the BF16 bits in the upper half of the word (exact)
+        const float hx = __uint_as_float(hw.x << 16), hy = __uint_as_float(hw.x & 0xffff0000u);
+        const float hz = __uint_as_float(hw.y << 16), hq = __uint_as_float(hw.y & 0xffff0000u);
+        const __nv_bfloat162 l01 = __floats2bfloat162_rn(v.x - hx, v.y - hy);
+        const __nv_bfloat162 l23 = __floats2bfloat162_rn(v.z - hz, v.w - hq);
+        uint2 lw;
+        lw.x = *reinterpret_cast<const uint32_t *>(&l01);
+        lw.y = *reinterpret_cast<const uint32_t *>(&l23);
+        *reinterpret_cast<uint2 *>(plane0 + kAPlane * 2 + off) = lw;
     }
 }
 
@@ -122,6 +155,12 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
     const uint32_t tlane = (uint32_t)(warp * 32) << 16;
 
     const int comp = a.comp0 + (int)blockIdx.z;
+    // components of a batch of chains are numbered chain * chain_comps + component: the chain
+    // picks the state and the Philox chain index, the component within it everything else
+    const int bch = a.chain_comps ? comp / a.chain_comps : 0;
+    const int cn = comp - bch * a.chain_comps;
+    DevState *const st = a.st ? a.st + bch : nullptr;
+    const uint32_t chain = a.chain + (uint32_t)bch;
     const float *in = a.in + comp * a.V;
     float *out = a.out + comp * a.V;
     const long nlines = a.outer * a.s;
@@ -138,9 +177,9 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
 
     uint32_t chunk = 0;  // running chunk counter over both GEMMs: stage = chunk & 1
     double part_cost = 0.0, part_raw = 0.0;
-    const uint32_t sweep = ((MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.sample) ? (uint32_t)a.st->sweep : 0u;
-    const bool want_raw = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.want_raw && (a.st->sweep % a.every == 0);
-    const double gamma = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) ? a.st->gamma[comp] : 0.0;
+    const uint32_t sweep = ((MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.sample) ? (uint32_t)st->sweep : 0u;
+    const bool want_raw = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) && a.want_raw && (st->sweep % a.every == 0);
+    const double gamma = (MODE == kEpiSpectral || MODE == kEpiSpectralOut) ? st->gamma[cn] : 0.0;
     const float gs2 = (float)(gamma * a.sigma2);
 
     auto load_global = [&](int kc, AChunk &r) {
@@ -247,13 +286,13 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                         if (a.sample)
                             cval += sqrtf((float)a.sigma2 * f) *
                                     prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
-                                                    a.chain, comp);
+                                                    chain, cn);
                         ccost += Dv * cval * cval;
                     }
                     v[m] = cval;
                 }
                 part_cost += 0.5 * gamma * (double)ccost;
-                if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)ccost;
+                if (want_raw) part_raw += a.eta2[cn] * a.rho_p * (double)ccost;
                 if (kc + 1 < a.nkc) load_d(kc + 1);
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
@@ -313,7 +352,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
             if (MODE == kEpiPositions && !a.xpos) {
                 const int gi = (int)(l0 + warp * 32 + lane);  // 3D: x * ny + y; 2D: x
                 rowc = a.dims == 2 ? (float)gi
-                                   : (comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
+                                   : (cn == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
             }
             for (int cc = 0; cc < nchunks; ++cc) {
                 float v[32];
@@ -329,8 +368,8 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                     if (g < nlines && k < n) {
                         float val = stg[r * 33 + lane];
                         if (MODE == kEpiPositions)
-                            val += a.xpos ? __ldg(a.xpos + comp * a.V + g * n + k)
-                                          : (comp == a.dims - 1 ? (float)k : rc);
+                            val += a.xpos ? __ldg(a.xpos + cn * a.V + g * n + k)
+                                          : (cn == a.dims - 1 ? (float)k : rc);
                         out[g * n + k] = val;
                     }
                 }
@@ -373,7 +412,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                             if (a.sample)
                                 val += sqrtf((float)a.sigma2 * f) *
                                        prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
-                                                       a.chain, comp);
+                                                       chain, cn);
                             const float dv2 = Dv * val * val;
                             ccost += dv2;
                             craw += dv2;
@@ -383,7 +422,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
                 }
                 if (MODE == kEpiSpectralOut) {
                     part_cost += 0.5 * gamma * (double)ccost;
-                    if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)craw;
+                    if (want_raw) part_raw += a.eta2[cn] * a.rho_p * (double)craw;
                 }
             }
         }
@@ -391,10 +430,10 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
 
     if (MODE == kEpiSpectral || MODE == kEpiSpectralOut) {
         const double sc = block_sum(part_cost, red);
-        if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
+        if (tid == 0) atomicAdd(&st->lp_tr, sc);
         if (a.want_raw) {
             const double sr = block_sum(part_raw, red);
-            if (tid == 0) atomicAdd(&a.st->raw_reg, sr);
+            if (tid == 0) atomicAdd(&st->raw_reg, sr);
         }
     }
 
@@ -404,7 +443,7 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
         if (tid == 0) {
             umma::commit(&mbar[2]);
             umma::mbar_wait(&mbar[2], 0, kWaitLimit);
-            if (a.st) atomicOr(&a.st->flags, (unsigned)kFlagTensorTimeout);
+            if (st) atomicOr(&st->flags, (unsigned)kFlagTensorTimeout);
         }
     }
     umma::fence_before_sync();
@@ -423,17 +462,21 @@ __global__ void __launch_bounds__(128, 2) umma_axis_kernel(const UArgs a) {
 constexpr int kWsThreads = 160;
 constexpr int kPre = 2;  // A chunks in flight per producer thread
 
-template <int MODE, int PLANES>
+template <int MODE, int PLANES, bool BF>
 __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool producer = warp < 4;
     const int Npad = a.Npad, n = a.n, nkc = a.nkc;
-    const uint32_t bplane = (uint32_t)Npad * kKC;
-    float *As = reinterpret_cast<float *>(smem_raw);  // [2 stages][PLANES][kAPlane]
-    float *Bs = As + 2 * PLANES * kAPlane;            // [3 slots][PLANES][bplane]
-    uint64_t *full = reinterpret_cast<uint64_t *>(Bs + 3 * PLANES * bplane);  // [2]
+    // operands are TF32 in 4-byte elements, or BF16 (BF) in 2-byte elements with the same
+    // canonical layout of 16-byte K columns
+    constexpr uint32_t EB = BF ? 2u : 4u;
+    constexpr uint32_t kAPlaneB = kAPlane * EB;            // bytes per A plane
+    const uint32_t bplaneB = (uint32_t)Npad * kKC * EB;    // bytes per B plane
+    unsigned char *As = smem_raw;                          // [2 stages][PLANES][kAPlaneB]
+    unsigned char *Bs = As + 2 * PLANES * kAPlaneB;        // [3 slots][PLANES][bplaneB]
+    uint64_t *full = reinterpret_cast<uint64_t *>(Bs + 3 * PLANES * bplaneB);  // [2]
     uint64_t *done = full + 2;                                               // [3]
     uint64_t *drain = done + 3;                                              // [1]
     uint32_t *holder = reinterpret_cast<uint32_t *>(drain + 1);
@@ -458,6 +501,12 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
 
     const int comp = a.comp0 + (int)blockIdx.z;
+    // components of a batch of chains are numbered chain * chain_comps + component: the chain
+    // picks the state and the Philox chain index, the component within it everything else
+    const int bch = a.chain_comps ? comp / a.chain_comps : 0;
+    const int cn = comp - bch * a.chain_comps;
+    DevState *const st = a.st ? a.st + bch : nullptr;
+    const uint32_t chain = a.chain + (uint32_t)bch;
     const float *in = a.in + comp * a.V;
     float *out = a.out + comp * a.V;
     const long nlines = a.outer * a.s;
@@ -473,7 +522,8 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     if (!producer) {
         // ---- MMA warp ------------------------------------------------------------------------
         if (lane == 0) {
-            const uint32_t idesc = umma::instr_desc(kLines, Npad, umma::kFmtTF32);
+            const uint32_t idesc =
+                umma::instr_desc(kLines, Npad, BF ? umma::kFmtBF16 : umma::kFmtTF32);
             for (int kc = 0; kc < nkc; ++kc) {
                 if (!umma::mbar_wait(&full[kc & 1], (uint32_t)(kc >> 1) & 1u, kWaitLimit) ||
                     *(volatile int *)s_err) {
@@ -481,21 +531,37 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                     break;
                 }
                 umma::fence_after_sync();
-                const uint32_t abase = umma::smem_u32(As + (kc & 1) * PLANES * kAPlane);
-                const uint32_t bbase = umma::smem_u32(Bs + (kc % 3) * PLANES * bplane);
-#pragma unroll
-                for (int ks = 0; ks < kKC / 8; ++ks) {
-                    const uint32_t ao = (uint32_t)ks * 2u * 2048u;
-                    const uint32_t bo = (uint32_t)ks * 2u * (uint32_t)Npad * 16u;
-                    const uint64_t ahi = umma::smem_desc(abase + ao, 2048u, 128u);
-                    const uint64_t bhi = umma::smem_desc(bbase + bo, (uint32_t)Npad * 16u, 128u);
-                    umma::mma_tf32(tmem, ahi, bhi, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+                const uint32_t abase = umma::smem_u32(As + (kc & 1) * PLANES * kAPlaneB);
+                const uint32_t bbase = umma::smem_u32(Bs + (kc % 3) * PLANES * bplaneB);
+                if (BF) {
+                    // one kind::f16 MMA (K = 16) covers the chunk: its two 16-byte K columns
+                    const uint64_t ahi = umma::smem_desc(abase, 2048u, 128u);
+                    const uint64_t bhi = umma::smem_desc(bbase, (uint32_t)Npad * 16u, 128u);
+                    umma::mma_bf16(tmem, ahi, bhi, idesc, kc > 0 ? 1u : 0u);
                     if (PLANES == 2) {
-                        const uint64_t alo = umma::smem_desc(abase + kAPlane * 4u + ao, 2048u, 128u);
+                        const uint64_t alo = umma::smem_desc(abase + kAPlaneB, 2048u, 128u);
                         const uint64_t blo =
-                            umma::smem_desc(bbase + bplane * 4u + bo, (uint32_t)Npad * 16u, 128u);
-                        umma::mma_tf32(tmem, ahi, blo, idesc, 1u);
-                        umma::mma_tf32(tmem, alo, bhi, idesc, 1u);
+                            umma::smem_desc(bbase + bplaneB, (uint32_t)Npad * 16u, 128u);
+                        umma::mma_bf16(tmem, ahi, blo, idesc, 1u);
+                        umma::mma_bf16(tmem, alo, bhi, idesc, 1u);
+                    }
+                } else {
+#pragma unroll
+                    for (int ks = 0; ks < kKC / 8; ++ks) {
+                        const uint32_t ao = (uint32_t)ks * 2u * 2048u;
+                        const uint32_t bo = (uint32_t)ks * 2u * (uint32_t)Npad * 16u;
+                        const uint64_t ahi = umma::smem_desc(abase + ao, 2048u, 128u);
+                        const uint64_t bhi =
+                            umma::smem_desc(bbase + bo, (uint32_t)Npad * 16u, 128u);
+                        umma::mma_tf32(tmem, ahi, bhi, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+                        if (PLANES == 2) {
+                            const uint64_t alo =
+                                umma::smem_desc(abase + kAPlaneB + ao, 2048u, 128u);
+                            const uint64_t blo = umma::smem_desc(bbase + bplaneB + bo,
+                                                                 (uint32_t)Npad * 16u, 128u);
+                            umma::mma_tf32(tmem, ahi, blo, idesc, 1u);
+                            umma::mma_tf32(tmem, alo, bhi, idesc, 1u);
+                        }
                     }
                 }
                 umma::commit(&done[kc % 3]);
@@ -540,10 +606,12 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
         };
         auto issue_b = [&](int kc) {
             if (kc < nkc) {
-                const float *srcb = a.B1 + (size_t)kc * 2 * bplane;
-                float *Bp = Bs + (kc % 3) * PLANES * bplane;
-                const int nv = PLANES * (int)bplane / 4;
-                for (int qv = tid; qv < nv; qv += 128) umma::cp_async16(Bp + 4 * qv, srcb + 4 * qv);
+                const unsigned char *srcb =
+                    reinterpret_cast<const unsigned char *>(a.B1) + (size_t)kc * 2 * bplaneB;
+                unsigned char *Bp = Bs + (kc % 3) * PLANES * bplaneB;
+                const int nv = PLANES * (int)bplaneB / 16;
+                for (int qv = tid; qv < nv; qv += 128)
+                    umma::cp_async16(Bp + 16 * qv, srcb + 16 * qv);
             }
             umma::cp_async_commit();  // possibly empty: one group per chunk
         };
@@ -559,14 +627,22 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                 }
             }
             issue_b(kc + 1);
-            float *Ap = As + (kc & 1) * PLANES * kAPlane;
+            unsigned char *Ap = As + (kc & 1) * PLANES * kAPlaneB;
             if (contig) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    store_split<PLANES>(Ap, a_slot((warp + 4 * i) * 8 + cr, cq), cur.v[i]);
+                for (int i = 0; i < 4; ++i) {
+                    const int line = (warp + 4 * i) * 8 + cr;
+                    if (BF) store_split_b16<PLANES>(Ap, a_slot_b16(line, cq), cur.v[i]);
+                    else store_split<PLANES>(reinterpret_cast<float *>(Ap), a_slot(line, cq),
+                                             cur.v[i]);
+                }
             } else {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) store_split<PLANES>(Ap, a_slot(tid, q), cur.v[q]);
+                for (int q = 0; q < 4; ++q) {
+                    if (BF) store_split_b16<PLANES>(Ap, a_slot_b16(tid, q), cur.v[q]);
+                    else store_split<PLANES>(reinterpret_cast<float *>(Ap), a_slot(tid, q),
+                                             cur.v[q]);
+                }
             }
             load_global(kc + kPre, cur);                          // in flight for kPre chunks
             asm volatile("cp.async.wait_group 1;" ::: "memory");  // my part of B chunk kc landed
@@ -601,9 +677,9 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     umma::fence_after_sync();
 
     double part_cost = 0.0, part_raw = 0.0;
-    const uint32_t sweep = (MODE == kEpiSpectralOut && a.sample) ? (uint32_t)a.st->sweep : 0u;
-    const bool want_raw = MODE == kEpiSpectralOut && a.want_raw && (a.st->sweep % a.every == 0);
-    const double gamma = MODE == kEpiSpectralOut ? a.st->gamma[comp] : 0.0;
+    const uint32_t sweep = (MODE == kEpiSpectralOut && a.sample) ? (uint32_t)st->sweep : 0u;
+    const bool want_raw = MODE == kEpiSpectralOut && a.want_raw && (st->sweep % a.every == 0);
+    const double gamma = MODE == kEpiSpectralOut ? st->gamma[cn] : 0.0;
     const float gs2 = (float)(gamma * a.sigma2);
     if (producer && !*s_err) {
         // ---- epilogue: 32 TMEM columns at a time -------------------------------------------
@@ -615,7 +691,7 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
             if (MODE == kEpiPositions && !a.xpos) {
                 const int gi = (int)(l0 + warp * 32 + lane);  // 3D: x * ny + y; 2D: x
                 rowc = a.dims == 2 ? (float)gi
-                                   : (comp == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
+                                   : (cn == 0 ? (float)(gi / a.ny) : (float)(gi % a.ny));
             }
             for (int cc = 0; cc < nchunks; ++cc) {
                 float v[32];
@@ -631,8 +707,8 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                     if (g < nlines && k < n) {
                         float val = stg[r * 33 + lane];
                         if (MODE == kEpiPositions)
-                            val += a.xpos ? __ldg(a.xpos + comp * a.V + g * n + k)
-                                          : (comp == a.dims - 1 ? (float)k : rc);
+                            val += a.xpos ? __ldg(a.xpos + cn * a.V + g * n + k)
+                                          : (cn == a.dims - 1 ? (float)k : rc);
                         out[g * n + k] = val;
                     }
                 }
@@ -673,7 +749,7 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                             if (a.sample)
                                 val += sqrtf((float)a.sigma2 * f) *
                                        prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
-                                                       a.chain, comp);
+                                                       chain, cn);
                             ccost += Dv * val * val;
                         }
                         op[(long)k * a.s] = val;
@@ -681,17 +757,17 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                 }
                 if (MODE == kEpiSpectralOut) {
                     part_cost += 0.5 * gamma * (double)ccost;
-                    if (want_raw) part_raw += a.eta2[comp] * a.rho_p * (double)ccost;
+                    if (want_raw) part_raw += a.eta2[cn] * a.rho_p * (double)ccost;
                 }
             }
         }
     }
     if (MODE == kEpiSpectralOut) {
         const double sc = block_sum(part_cost, red);
-        if (tid == 0) atomicAdd(&a.st->lp_tr, sc);
+        if (tid == 0) atomicAdd(&st->lp_tr, sc);
         if (a.want_raw) {
             const double sr = block_sum(part_raw, red);
-            if (tid == 0) atomicAdd(&a.st->raw_reg, sr);
+            if (tid == 0) atomicAdd(&st->raw_reg, sr);
         }
     }
 
@@ -699,17 +775,17 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     if (*s_err && tid == 128) {
         umma::commit(drain);  // arrives once all MMAs this thread issued have completed
         umma::mbar_wait(drain, 0, kWaitLimit);
-        if (a.st) atomicOr(&a.st->flags, (unsigned)kFlagTensorTimeout);
+        if (st) atomicOr(&st->flags, (unsigned)kFlagTensorTimeout);
     }
     umma::fence_before_sync();
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(tmem, ncols);
 }
 
-template <int MODE, int PLANES>
+template <int MODE, int PLANES, bool BF>
 void launch_ws(const UArgs &a, int ncomp, cudaStream_t s) {
     // A stages, B slots, then 6 mbarriers, the TMEM address and the error word
-    size_t need = (size_t)(2 * PLANES * kAPlane + 3 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
+    size_t need = (size_t)(2 * PLANES * kAPlane + 3 * PLANES * a.Npad * kKC) * (BF ? 2 : 4) + 64;
     const size_t staging = (size_t)4 * 32 * 33 * sizeof(float) + 64;  // contiguous-axis epilogue
     if (need < staging) need = staging;
     uint32_t ncols = 32;
@@ -721,15 +797,15 @@ void launch_ws(const UArgs &a, int ncomp, cudaStream_t s) {
     const size_t floor_smem = per_sm / (max_ctas + 1) + 1024;
     const size_t smem = need > floor_smem ? need : floor_smem;
     BINDER_CHECK(smem <= 227 * 1024, "tensor-core transform tile does not fit in shared memory");
-    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES>,
+    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES, BF>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES>,
+    BINDER_CUDA(cudaFuncSetAttribute(umma_ws_kernel<MODE, PLANES, BF>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared));
     const long tiles = (a.outer * a.s + kLines - 1) / kLines;
     BINDER_CHECK(tiles < (1L << 31), "transform grid too large");
     dim3 grid((unsigned)tiles, 1, (unsigned)ncomp);
-    count_launch(), umma_ws_kernel<MODE, PLANES><<<grid, kWsThreads, smem, s>>>(a);
+    count_launch(), umma_ws_kernel<MODE, PLANES, BF><<<grid, kWsThreads, smem, s>>>(a);
     BINDER_CUDA(cudaGetLastError());
 }
 
@@ -1207,6 +1283,22 @@ float tf32_rna_host(float x) {
     return r;
 }
 
+// FP32 -> BF16 bits, round to nearest even (NaN kept a quiet NaN); host side of the B planes
+uint16_t bf16_rne_host(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)((u >> 16) | ((u & 0xffffu) ? 0x40u : 0u));
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+float bf16_to_float_host(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
 template <int MODE, int PLANES>
 void launch_umma(const UArgs &a, int ncomp, cudaStream_t s) {
     size_t need = (size_t)(2 * PLANES * kAPlane + 3 * PLANES * a.Npad * kKC) * sizeof(float) + 64;
@@ -1257,26 +1349,55 @@ void UmmaMatrix::init(const double *M, int n_, cudaStream_t s) {
                 host[(size_t)kc * 2 * plane + off] = hi;
                 host[(size_t)kc * 2 * plane + plane + off] = lo;
             }
+    // the same chunks as BF16 hi / lo planes (2-byte elements, the same canonical layout: 16-byte
+    // K columns of 8 elements Npad * 16 bytes apart, 8-row groups 128 bytes apart)
+    std::vector<uint16_t> host16((size_t)nkc * 2 * plane, 0);
+    for (int kc = 0; kc < nkc; ++kc)
+        for (int k = 0; k < n; ++k)
+            for (int jj = 0; jj < kKC; ++jj) {
+                const int j = kc * kKC + jj;
+                if (j >= n) continue;
+                const float v = (float)M[(size_t)k * n + j];
+                const uint16_t hi = bf16_rne_host(v);
+                const uint16_t lo = bf16_rne_host(v - bf16_to_float_host(hi));
+                const size_t off = (size_t)(jj / 8) * (Npad * 8) + (k / 8) * 64 + (k % 8) * 8 + (jj % 8);
+                host16[(size_t)kc * 2 * plane + off] = hi;
+                host16[(size_t)kc * 2 * plane + plane + off] = lo;
+            }
     dev = dev_alloc_n<float>(host.size(), s);
+    dev16 = dev_alloc_n<uint16_t>(host16.size(), s);
     BINDER_CUDA(cudaMemcpyAsync(dev, host.data(), host.size() * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    BINDER_CUDA(cudaMemcpyAsync(dev16, host16.data(), host16.size() * sizeof(uint16_t),
                                 cudaMemcpyHostToDevice, s));
     BINDER_CUDA(cudaStreamSynchronize(s));  // `host` goes out of scope
 }
 
-void UmmaMatrix::release(cudaStream_t s) { dev_free_p(dev, s); }
+void UmmaMatrix::release(cudaStream_t s) {
+    dev_free_p(dev, s);
+    dev_free_p(dev16, s);
+}
 
 void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const UmmaMatrix *M2,
-                         int mode, int ncomp, int planes, cudaStream_t s, bool persistent) {
+                         int mode, int ncomp, int planes, cudaStream_t s, bool persistent,
+                         bool bf16) {
     BINDER_CHECK(b.n == M1.n, "matrix / axis length mismatch");
-    BINDER_CHECK(planes == 1 || planes == 2, "planes must be 1 (TF32) or 2 (3xTF32)");
+    BINDER_CHECK(planes == 1 || planes == 2, "planes must be 1 (one product) or 2 (split)");
+    BINDER_CHECK(!bf16 || !persistent, "BF16 operands run on the per-tile passes");
     UArgs a{};
     a.in = b.in; a.out = b.out; a.V = b.comp_stride; a.n = b.n; a.Npad = M1.Npad; a.nkc = M1.nkc;
-    a.outer = b.outer; a.s = b.s; a.B1 = M1.dev; a.B2 = M2 ? M2->dev : nullptr;
+    a.outer = b.outer; a.s = b.s;
+    a.B1 = bf16 ? reinterpret_cast<const float *>(M1.dev16) : M1.dev;
+    a.B2 = M2 ? M2->dev : nullptr;
     a.D = b.D; a.st = b.st; a.sigma2 = b.sigma2; a.sample = b.sample; a.want_raw = b.want_raw;
     a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
     for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
     a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.comp0 = b.comp0; a.skip = b.skip;
     a.ncomp = ncomp;
+    a.chain_comps = b.chain_comps;
+    // a persistent CTA's tiles span components, so its per-CTA cost sums could mix chains
+    BINDER_CHECK(!persistent || b.chain_comps == 0,
+                 "a batch of chains runs on the per-tile tensor-core passes");
     if (persistent && mode != kEpiSpectral) {
         BINDER_CHECK(mode != kEpiSpectralOut || b.outer == 1,
                      "prior scaling runs on the outermost axis");
@@ -1299,18 +1420,29 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     }
 #define BINDER_UMMA_CASE(MODE)                                                    \
     case MODE:                                                                    \
-        if (planes == 2) launch_ws<MODE, 2>(a, ncomp, s);                         \
-        else launch_ws<MODE, 1>(a, ncomp, s);                                     \
+        if (bf16) {                                                               \
+            if (planes == 2) launch_ws<MODE, 2, true>(a, ncomp, s);               \
+            else launch_ws<MODE, 1, true>(a, ncomp, s);                           \
+        } else {                                                                  \
+            if (planes == 2) launch_ws<MODE, 2, false>(a, ncomp, s);              \
+            else launch_ws<MODE, 1, false>(a, ncomp, s);                          \
+        }                                                                         \
         break;
     switch (mode) {
         BINDER_UMMA_CASE(kEpiNone)
         BINDER_UMMA_CASE(kEpiPositions)
         case kEpiSpectralOut:
             BINDER_CHECK(b.outer == 1, "prior scaling runs on the outermost axis");
-            if (planes == 2) launch_ws<kEpiSpectralOut, 2>(a, ncomp, s);
-            else launch_ws<kEpiSpectralOut, 1>(a, ncomp, s);
+            if (bf16) {
+                if (planes == 2) launch_ws<kEpiSpectralOut, 2, true>(a, ncomp, s);
+                else launch_ws<kEpiSpectralOut, 1, true>(a, ncomp, s);
+            } else {
+                if (planes == 2) launch_ws<kEpiSpectralOut, 2, false>(a, ncomp, s);
+                else launch_ws<kEpiSpectralOut, 1, false>(a, ncomp, s);
+            }
             break;
         case kEpiSpectral:
+            BINDER_CHECK(!bf16, "the fused prior pass runs with TF32 operands");
             BINDER_CHECK(M2 && M2->n == b.n, "fused pass needs the inverse matrix");
             BINDER_CHECK(b.outer == 1, "fused prior pass runs on the outermost axis");
             if (planes == 2) launch_umma<kEpiSpectral, 2>(a, ncomp, s);

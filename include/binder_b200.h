@@ -137,6 +137,23 @@ int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, 
                                 int sample_transformation_parameters, double *mean_out,
                                 double *cov_out);
 
+/* No counterpart in the reference (it runs one chain per Registration object,
+ * gpu/Registration.cu:917-1026, cpu/Registration.cpp:515-642): `chains` independent chains of
+ * the sampler above, every kernel of a sweep launched once for all of them.  Chain c draws with
+ * Philox chain index (the object's chain index + c), so it equals, draw for draw, sampler() after
+ * binder_registration_set_chain(chain index + c) from the same state.  Every chain starts from the
+ * object's current positions, dream locations, theta and gammas, which the call leaves as they
+ * are.  MI likelihood only.  Outputs (FP64, each optional / NULL): mean_out [chains*V*N] and
+ * cov_out [chains*V*N*N] per chain (M2 / (N_s - 1)); pooled_mean_out [V*N] and pooled_cov_out
+ * [V*N*N], the chains' samples pooled (M2 / (chains * N_s - 1)). */
+int binder_registration_sampler_chains(binder_registration *h, uint64_t seed, int chains,
+                                       int N_b, int N_s, int sample_gamma,
+                                       int sample_gamma_every, int sample_posteriors,
+                                       int sample_likelihood_parameters,
+                                       int sample_transformation_parameters, double *mean_out,
+                                       double *cov_out, double *pooled_mean_out,
+                                       double *pooled_cov_out);
+
 /* get_final_locations_as_numpy_array() -> [Nx,Ny,Nz,3]          gpu/bindings.cpp:142-157 */
 int binder_registration_get_final_locations(const binder_registration *h, float *out);
 /* get_dream_locations() / set_dream_locations(arr)              gpu/bindings.cpp:133-140 */
@@ -180,12 +197,15 @@ int binder_registration_correct_topology(binder_registration *h, double e1, doub
 
 /* No counterpart in the reference (its GPU backend is FP32 cuFFT only): arithmetic of the DCT
  * passes.  BINDER_PRECISION_FP32 = FP32 FMA on the CUDA cores; _TF32X3 = tensor cores (tcgen05)
- * with hi/lo TF32 operand splitting, FP32-level accuracy; _TF32 = one TF32 tensor-core product
- * (about 1e-3 relative error per pass).  All accumulate in FP32.  The default comes from the
- * BINDER_B200_PRECISION environment variable (0, 1 or 2), else TF32X3. */
+ * with hi/lo TF32 operand splitting, FP32-level accuracy; _TF32 = one TF32 tensor-core product;
+ * _BF16X3 = BF16 hi/lo operand splitting, three kind::f16 products (about 16 mantissa bits);
+ * _BF16 = one BF16 product.  All accumulate in FP32.  The default comes from the
+ * BINDER_B200_PRECISION environment variable (0 to 4), else TF32X3. */
 #define BINDER_PRECISION_FP32 0
 #define BINDER_PRECISION_TF32X3 1
 #define BINDER_PRECISION_TF32 2
+#define BINDER_PRECISION_BF16X3 3
+#define BINDER_PRECISION_BF16 4
 int binder_registration_set_precision(binder_registration *h, int precision);
 int binder_transform_set_precision(binder_transform *h, int precision);
 

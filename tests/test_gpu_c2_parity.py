@@ -91,3 +91,49 @@ def test_c2_topology_matches_reference(core, c2):
     err_viol = np.abs(out[g["topo_viol_idx"]] - g["topo_out_at_viol"]).max()
     print(f"C2 topology: max |d| {err_idx:.2e} (random voxels), {err_viol:.2e} (violating voxels)")
     assert err_idx < 1e-8 and err_viol < 1e-8
+
+
+# FP64 error table of the DCT precision modes at the full size: every mode runs the same 5 EM
+# iterations from the identity grid and is compared with the reference's FP64 run.  Bounds:
+# FP32, 3xTF32 and the BF16 split meet the bar of the FP32 path (MI within 1e-3 relative,
+# positions within 2e-3 voxels); one TF32 or one BF16 product per pass is reported with looser
+# bounds (MI within 1e-2 relative).
+MODES = {0: ("FP32", 1e-3, 2e-3), 1: ("3xTF32", 1e-3, 2e-3), 2: ("TF32", 1e-2, 5e-2),
+         3: ("BF16x3", 1e-3, 2e-3), 4: ("BF16", 1e-2, 5e-2)}
+
+
+def test_c2_precision_error_table(core, oracle, c2):
+    mk, g = c2
+    import bench
+    inp = bench.make_inputs(0)
+    pair, V = inp["pair"], inp["V"]
+    its = int(g["em_iters"])
+    idx = g["idx"]
+    ref_mi = float(g["em_mi"])
+    th_ref = g["em_theta"]
+    big = th_ref > 1e-3
+    oracle.set_threads(os.cpu_count() or 1)
+    reg = bench.setup_registration(core, inp)
+    rows = []
+    for prec, (name, mi_bound, pos_bound) in MODES.items():
+        reg.reset()
+        reg.set_precision(prec)
+        assert reg.EM(its, -1e300, 1, 0) == its
+        final = reg.get_final_locations_as_numpy_array().reshape(V, 3).astype(np.float64)
+        theta = reg.get_likelihood_parameters()[: bench.BINS ** 2].reshape(bench.BINS,
+                                                                           bench.BINS)
+        dpos = np.abs(final[idx] - g["em_final"])
+        th_rel = np.abs(theta.astype(np.float64)[big] - th_ref[big]) / th_ref[big]
+        _, _, hist, _ = oracle.estep(final, pair.u, pair.v, theta.astype(np.float64),
+                                     bench.SHAPE, bench.SHAPE, bench.BINS, bench.BINS)
+        mi = oracle.mutual_information(hist, bench.BINS, bench.BINS)
+        mlp = reg.iteration_stats()[-1, 3] / inp["nzv"]
+        row = dict(mode=name, pos_max=float(dpos.max()), pos_rms=float(np.sqrt((dpos ** 2).mean())),
+                   theta_rel=float(th_rel.max()), mi_rel=abs(mi - ref_mi) / ref_mi,
+                   mlp_rel=abs(mlp / g["em_mlp_per_voxel"][-1] - 1))
+        rows.append(row)
+        print("C2 error vs FP64: " + ", ".join(f"{k} {v:.2e}" if isinstance(v, float) else
+                                                 f"{k} {v}" for k, v in row.items()))
+        assert row["mi_rel"] < mi_bound, row
+        assert row["pos_max"] < pos_bound, row
+    reg.set_precision(1)

@@ -34,3 +34,21 @@ def test_gpu_sampler_matches_reference_in_distribution(core):
     zm, zc = zscores(g, *gpu_chains(core, g))
     assert agrees(zm), summary(zm)
     assert agrees(zc), summary(zc)
+
+
+def test_gpu_chain_batch_matches_reference_in_distribution(core):
+    """The same check with the 32 chains run as one batch (sampler_chains)."""
+    g = fixture()
+    shape = tuple(int(s) for s in g["shape"])
+    V = int(np.prod(shape))
+    K, L = int(g["K"]), int(g["L"])
+    grid = np.stack(np.indices(shape), -1).astype(np.float32)
+    reg = core.Registration(g["d0"].astype(np.float32), 1, grid, grid, *shape, *shape, 3, float(V))
+    reg.setNonLinearTransformation(*[float(x) for x in g["gamma"]], 1, 1, 1, 1, 1, 1,
+                                   g["D"].astype(np.float32))
+    reg.setMILikelihood(float(g["alpha"]), g["theta"].astype(np.float32), K, L, 1, g["v"], g["u"])
+    means, covs = reg.sampler_chains(4242, 32, int(g["N_b"]), int(g["N_s"]), 1, 1, 1, 1, 1,
+                                     pooled=False)
+    zm, zc = zscores(g, means.reshape(32, V, 3), covs.reshape(32, V, 9)[:, :, UPPER])
+    assert agrees(zm), summary(zm)
+    assert agrees(zc), summary(zc)
