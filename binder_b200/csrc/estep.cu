@@ -195,10 +195,13 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
                       k3 = word >> 24;
             const float2 w01 = __fmul2_rn(b01, make_float2(thu[k0], thu[k1]));
             const float2 w23 = __fmul2_rn(b23, make_float2(thu[k2], thu[k3]));
-            col[k0 * TPB] += w01.x;
-            col[k1 * TPB] += w01.y;
-            col[k2 * TPB] += w23.x;
-            col[k3 * TPB] += w23.y;
+            // fire-and-forget shared-memory reductions: nodes of one neighbourhood may share a
+            // bin, so load-add-store updates would form one dependent chain per voxel; the
+            // reductions need no result and the bank (thread % 32) never conflicts
+            atomicAdd(&col[k0 * TPB], w01.x);
+            atomicAdd(&col[k1 * TPB], w01.y);
+            atomicAdd(&col[k2 * TPB], w23.x);
+            atomicAdd(&col[k3 * TPB], w23.y);
             a01 = __fadd2_rn(a01, w01);
             a23 = __fadd2_rn(a23, w23);
             if (p == 0) { x01 = __ffma2_rn(m1, w01, x01); x23 = __ffma2_rn(m1, w23, x23); }
