@@ -132,11 +132,13 @@ template <int DIM>
 struct VoxelPos {
     float px, py, pz;     // position (py = 0 in 2D)
     float x0, x1, x2;     // voxel grid position
+    // pos_off: elements from a.d to this chain's positions (a batch of chains; 0 otherwise)
     __device__ __forceinline__ bool load(const EStepArgs &a, unsigned i, unsigned V, unsigned ny,
-                                         unsigned nz) {
-        px = a.d[i];
-        py = DIM == 3 ? a.d[V + i] : 0.0f;
-        pz = a.d[(size_t)(DIM - 1) * V + i];
+                                         unsigned nz, long pos_off = 0) {
+        const float *d = a.d + pos_off;
+        px = d[i];
+        py = DIM == 3 ? d[V + i] : 0.0f;
+        pz = d[(size_t)(DIM - 1) * V + i];
         if (a.x) {
             x0 = a.x[i];
             x1 = DIM == 3 ? a.x[V + i] : 0.0f;
@@ -152,10 +154,11 @@ struct VoxelPos {
     }
     // r = dream location - voxel position, components (x, [y,] z-role)
     __device__ __forceinline__ void store_r(const EStepArgs &a, unsigned i, unsigned V, float vx,
-                                            float vy, float vz) const {
-        a.r[i] = vx - x0;
-        if (DIM == 3) a.r[V + i] = vy - x1;
-        a.r[(size_t)(DIM - 1) * V + i] = vz - x2;
+                                            float vy, float vz, long pos_off = 0) const {
+        float *r = a.r + pos_off;
+        r[i] = vx - x0;
+        if (DIM == 3) r[V + i] = vy - x1;
+        r[(size_t)(DIM - 1) * V + i] = vz - x2;
     }
 };
 
@@ -195,13 +198,10 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
                       k3 = word >> 24;
             const float2 w01 = __fmul2_rn(b01, make_float2(thu[k0], thu[k1]));
             const float2 w23 = __fmul2_rn(b23, make_float2(thu[k2], thu[k3]));
-            // fire-and-forget shared-memory reductions: nodes of one neighbourhood may share a
-            // bin, so load-add-store updates would form one dependent chain per voxel; the
-            // reductions need no result and the bank (thread % 32) never conflicts
-            atomicAdd(&col[k0 * TPB], w01.x);
-            atomicAdd(&col[k1 * TPB], w01.y);
-            atomicAdd(&col[k2 * TPB], w23.x);
-            atomicAdd(&col[k3 * TPB], w23.y);
+            col[k0 * TPB] += w01.x;
+            col[k1 * TPB] += w01.y;
+            col[k2 * TPB] += w23.x;
+            col[k3 * TPB] += w23.y;
             a01 = __fadd2_rn(a01, w01);
             a23 = __fadd2_rn(a23, w23);
             if (p == 0) { x01 = __ffma2_rn(m1, w01, x01); x23 = __ffma2_rn(m1, w23, x23); }
@@ -769,17 +769,11 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
     // a batch of chains (gridDim.y > 1, sampling only): chain blockIdx.y has its own positions
     // and dream locations [dim][V], theta and counts [K][L] and state, one chain after another,
     // and Philox chain index chain + blockIdx.y; the bins are shared
-    EStepArgs a = args;
-    if (SAMPLE && blockIdx.y) {
-        const long cs = (long)blockIdx.y * a.dim * a.V;
-        const long ks = (long)blockIdx.y * a.K * a.L;
-        a.d += cs;
-        a.r += cs;
-        a.theta += ks;
-        a.hcnt += ks;
-        a.st += blockIdx.y;
-        a.chain += blockIdx.y;
-    }
+    const EStepArgs &a = args;
+    const long cs = SAMPLE ? (long)blockIdx.y * a.dim * a.V : 0;  // positions / dream offset
+    const long ks = SAMPLE ? (long)blockIdx.y * a.K * a.L : 0;    // theta / counts offset
+    DevState *const st = SAMPLE ? a.st + blockIdx.y : a.st;
+    const uint32_t chain = SAMPLE ? a.chain + blockIdx.y : a.chain;
     extern __shared__ __align__(16) float sm[];
     const int KL = a.K * a.L;
     float *th = sm;
@@ -788,20 +782,20 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
     float *cps = sm + 2 * KL + threadIdx.x;  // Gibbs: cdf at the end of node row r, cps[r * kEThreads]
     __shared__ double red[32];
     for (int q = threadIdx.x; q < KL; q += blockDim.x) {
-        th[q] = a.theta[q];
+        th[q] = a.theta[ks + q];
         if (SAMPLE) hc[q] = 0u; else hs[q] = 0.0f;
     }
     __syncthreads();
 
-    const uint32_t sweep = SAMPLE ? (uint32_t)a.st->sweep : 0u;
+    const uint32_t sweep = SAMPLE ? (uint32_t)st->sweep : 0u;
     double mll = 0.0;
     unsigned long long deg = 0;
     const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
         VoxelPos<DIM> vp;
         // positions far outside any grid (or non-finite) are degenerate: keep them as they are
-        if (!vp.load(a, i, V, ny, nz)) {
-            vp.store_r(a, i, V, vp.px, vp.py, vp.pz);
+        if (!vp.load(a, i, V, ny, nz, cs)) {
+            vp.store_r(a, i, V, vp.px, vp.py, vp.pz, cs);
             ++deg;
             continue;
         }
@@ -835,14 +829,14 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
                 if (SAMPLE) cps[(p * Q + q) * kEThreads] = S;
             }
         if (!(S > 0.0f)) {
-            vp.store_r(a, i, V, fx, fy, fz);
+            vp.store_r(a, i, V, fx, fy, fz, cs);
             ++deg;
             continue;
         }
         if (!SAMPLE) {
             const float inv = 1.0f / S;
             mll -= log((double)S);
-            vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
+            vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv, cs);
             // pass 2: normalised posteriors into the histogram column u_i, runs of equal bins
             // combined in a register before each shared-memory atomic
             const int ui = a.u[i];
@@ -873,7 +867,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
             // is the same sequence of FP32 additions as S above and never decreases (w >= 0), so
             // the first node row whose end value reaches the target holds the pick; only that
             // row's four nodes are summed again, from the previous row's end value.
-            const u32x4 rr = philox_draw(a.seed, i, sweep, 1u, a.chain);
+            const u32x4 rr = philox_draw(a.seed, i, sweep, 1u, chain);
             const float t = u01_f24(rr.x) * S;
             int row = R - 1;
             float cdf = 0.0f;
@@ -907,7 +901,7 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
             }
             atomicAdd(&hc[kp * L + a.u[i]], 1u);
             const int ox = pick / (4 * Q) - 1, oy = (pick / 4) % Q - 1, oz = pick % 4 - 1;
-            vp.store_r(a, i, V, fx + (float)ox, fy + (float)oy, fz + (float)oz);
+            vp.store_r(a, i, V, fx + (float)ox, fy + (float)oy, fz + (float)oz, cs);
         }
     }
 
@@ -916,16 +910,16 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
     for (int q = threadIdx.x; q < KL; q += blockDim.x) {
         if (SAMPLE) {
             const unsigned v = hc[q];
-            if (v) atomicAdd(&a.hcnt[q], v);
+            if (v) atomicAdd(&a.hcnt[ks + q], v);
         } else {
             const float v = hs[q];
             if (v != 0.0f) atomicAdd(&a.hist[q], v);
         }
     }
     const double m = block_sum(mll, red);
-    if (threadIdx.x == 0 && !SAMPLE) atomicAdd(&a.st->mll, m);
+    if (threadIdx.x == 0 && !SAMPLE) atomicAdd(&st->mll, m);
     const double dg = block_sum((double)deg, red);
-    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&st->degenerate, (unsigned long long)dg);
 }
 
 // MILikelihood.cpp:71-86 (update) and :33-39, :183-206 (cost), one CTA
