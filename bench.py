@@ -579,7 +579,7 @@ def run_b200(args, rank, world, local, dist):
     arms = {"plain_fp32": {"ms_per_registration": plain_ms, "registrations_per_s": 1e3 / plain_ms,
                            "final_mlp_per_voxel": mlp_plain,
                            "J_below_e1": topo_plain.get("below_e1_before")},
-            "tensor_3xtf32": {"ms_per_registration": ms / args.steps,
+            "tensor_bf16x3": {"ms_per_registration": ms / args.steps,
                               "registrations_per_s": 1e3 * args.steps / ms,
                               "final_mlp_per_voxel": mlp_fast,
                               "J_below_e1": topo_stats.get("below_e1_before")},

@@ -43,6 +43,9 @@ EXPORTS = [
     "binder_pyramid_level", "binder_pinned_alloc", "binder_pinned_free",
     "binder_bin_signal_robust", "binder_bin_signal", "binder_center_of_mass", "binder_warp_image",
     "binder_registration_set_ssd_likelihood", "binder_registration_get_ssd_parameters",
+    "binder_initnet_create", "binder_initnet_destroy", "binder_initnet_parameter_count",
+    "binder_initnet_get_parameters", "binder_initnet_set_parameters", "binder_initnet_predict",
+    "binder_initnet_train_step", "binder_initnet_gradients",
 ]
 
 
@@ -124,6 +127,14 @@ def _declare(lib):
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],
         "binder_topology_correct_2d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _f64, _P],
+        "binder_initnet_create": [C.POINTER(_P), _i, _i, _u64],
+        "binder_initnet_destroy": [_P],
+        "binder_initnet_parameter_count": [_P, C.POINTER(C.c_longlong)],
+        "binder_initnet_get_parameters": [_P, _P],
+        "binder_initnet_set_parameters": [_P, _P],
+        "binder_initnet_predict": [_P, _P, _P],
+        "binder_initnet_train_step": [_P, _P, _P, _d, C.POINTER(_d), _P],
+        "binder_initnet_gradients": [_P, _P, _P, C.POINTER(_d), _P],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

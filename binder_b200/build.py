@@ -24,7 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 # the determinants match the reference's CPU evaluation bit for bit
 EXTRA = {"topology.cu": ["-fmad=false"]}
 SOURCES = ["layout.cu", "transform.cu", "umma_transform.cu", "mstep2d.cu", "estep.cu",
-           "topology.cu", "resample.cu", "engine.cu", "multires.cu", "preprocess.cu", "capi.cu"]
+           "topology.cu", "resample.cu", "engine.cu", "multires.cu", "preprocess.cu", "initnet.cu", "capi.cu"]
 
 
 def _newest(paths):

@@ -8,6 +8,7 @@
 
 #include "../../include/binder_b200.h"
 #include "engine.cuh"
+#include "initnet.cuh"
 #include "multires.cuh"
 #include "preprocess.cuh"
 #include "resample.cuh"
@@ -20,6 +21,9 @@ struct binder_transform {
 };
 struct binder_pyramid {
     binder::Pyramid *impl;
+};
+struct binder_initnet {
+    binder::InitNet *impl;
 };
 
 namespace {
@@ -702,6 +706,85 @@ int binder_topology_correct_3d(const double *field, double e1, double e2, int ma
             stats_out[4] = r.above_before;
             stats_out[5] = r.above_after;
         }
+    });
+}
+
+// ---- learned initialiser ----------------------------------------------------------------------
+int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed) {
+    return guard([&] {
+        NEED(out);
+        *out = nullptr;
+        auto *h = new binder_initnet{nullptr};
+        try {
+            h->impl = new binder::InitNet(batch, size, seed);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int binder_initnet_destroy(binder_initnet *h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->impl;
+        delete h;
+    });
+}
+
+int binder_initnet_parameter_count(const binder_initnet *h, long long *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        *out = h->impl->parameter_count();
+    });
+}
+
+int binder_initnet_get_parameters(const binder_initnet *h, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(out);
+        h->impl->get_parameters(out);
+    });
+}
+
+int binder_initnet_set_parameters(binder_initnet *h, const float *in) {
+    return guard([&] {
+        NEED(h);
+        NEED(in);
+        h->impl->set_parameters(in);
+    });
+}
+
+int binder_initnet_predict(binder_initnet *h, const float *in, float *out) {
+    return guard([&] {
+        NEED(h);
+        NEED(in);
+        NEED(out);
+        h->impl->predict(in, out);
+    });
+}
+
+int binder_initnet_train_step(binder_initnet *h, const float *in, const float *target, double lr,
+                              double *loss_out, float *grads_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(in);
+        NEED(target);
+        const double l = h->impl->train_step(in, target, lr, grads_out);
+        if (loss_out) *loss_out = l;
+    });
+}
+
+int binder_initnet_gradients(binder_initnet *h, const float *in, const float *target,
+                             double *loss_out, float *grads_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(in);
+        NEED(target);
+        const double l = h->impl->gradients(in, target, grads_out);
+        if (loss_out) *loss_out = l;
     });
 }
 

@@ -1,0 +1,238 @@
+"""Learned initialiser of the registration (no counterpart in the reference).
+
+A 3D convolutional encoder-decoder (channels 16-32-64-128) predicts, from a moving / fixed image
+pair, the displacement on the grid of every 4th voxel; up-sampled to the full grid it seeds the
+positions the EM starts from -- the reference's own hook for an initial deformation is the
+final_locations argument of Registration (BINDER/FastRegistration.py:443-450).  The registration
+stays the judge: it runs to convergence from the seeded positions exactly as from the identity.
+
+The network trains and runs on the library's hand-written kernels (binder_initnet_* in
+include/binder_b200.h).  Training pairs are generated by this package itself, the way the
+benchmark's phantoms are: random-ellipsoid phantoms warped by prior-sampled deformations, then
+registered by the plain method (FP32 DCT passes, from the identity, to convergence) -- the
+network learns the field the method itself converges to.
+
+Recipe (a checkpoint is an .npz of the FP32 parameters):
+    python -m binder_b200.initnet --out initnet.npz --pairs 512 --steps 1500
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import time
+
+import numpy as np
+
+from ._lib import check, lib
+
+SIZE = 64             # training / inference grid (voxels per side)
+COARSE = 4            # output spacing (voxels)
+BINS = 64
+GAMMA_INIT = 1e-6     # run_BINDER's default gamma, scaled as FastRegistration.py:412-417
+ALPHA = 2.0
+CONVERGENCE = 2.5e-5  # run_BINDER's default EM convergence threshold
+MAX_EM = 400
+
+
+class InitNet:
+    """ctypes front of binder_initnet_*: batch x size^3 x 2 FP32 input (moving, fixed), batch x
+    (size/4)^3 x 3 FP32 output (displacement in voxels)."""
+
+    def __init__(self, batch=4, size=SIZE, seed=0):
+        self.batch, self.size = int(batch), int(size)
+        self._h = C.c_void_p()
+        check(lib().binder_initnet_create(C.byref(self._h), self.batch, self.size, int(seed)))
+        n = C.c_longlong(0)
+        check(lib().binder_initnet_parameter_count(self._h, C.byref(n)))
+        self.nparam = int(n.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binder_initnet_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self._h = C.c_void_p()
+
+    def _in(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        if x.size != self.batch * self.size ** 3 * 2:
+            raise ValueError(f"input must hold {self.batch} x {self.size}^3 x 2 values")
+        return x
+
+    def _tgt(self, t):
+        c = self.size // COARSE
+        t = np.ascontiguousarray(t, np.float32)
+        if t.size != self.batch * c ** 3 * 3:
+            raise ValueError(f"target must hold {self.batch} x {c}^3 x 3 values")
+        return t
+
+    def get_parameters(self):
+        out = np.empty(self.nparam, np.float32)
+        check(lib().binder_initnet_get_parameters(self._h, out.ctypes.data))
+        return out
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, np.float32).ravel()
+        if p.size != self.nparam:
+            raise ValueError(f"expected {self.nparam} parameters")
+        check(lib().binder_initnet_set_parameters(self._h, p.ctypes.data))
+
+    def predict(self, x):
+        x = self._in(x)
+        c = self.size // COARSE
+        out = np.empty((self.batch, c, c, c, 3), np.float32)
+        check(lib().binder_initnet_predict(self._h, x.ctypes.data, out.ctypes.data))
+        return out
+
+    def train_step(self, x, target, lr):
+        x, t = self._in(x), self._tgt(target)
+        loss = C.c_double(0)
+        check(lib().binder_initnet_train_step(self._h, x.ctypes.data, t.ctypes.data, float(lr),
+                                              C.byref(loss), None))
+        return loss.value
+
+    def gradients(self, x, target):
+        x, t = self._in(x), self._tgt(target)
+        g = np.empty(self.nparam, np.float32)
+        loss = C.c_double(0)
+        check(lib().binder_initnet_gradients(self._h, x.ctypes.data, t.ctypes.data,
+                                             C.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def save(self, path):
+        np.savez_compressed(path, params=self.get_parameters(), size=self.size)
+
+    def load(self, path):
+        z = np.load(path)
+        if int(z["size"]) != self.size:
+            raise ValueError("checkpoint was trained for another grid size")
+        self.set_parameters(z["params"])
+
+
+# ---- data ---------------------------------------------------------------------------------------
+def network_input(pair):
+    """[S, S, S, 2] FP32: moving and fixed intensities, each scaled to [0, 1] by its maximum"""
+    mv = pair.moving.astype(np.float32)
+    fx = pair.fixed.astype(np.float32)
+    mv = mv / max(float(mv.max()), 1e-6)
+    fx = np.clip(fx, 0.0, None) / max(float(fx.max()), 1e-6)
+    return np.stack([mv, fx], -1)
+
+
+def coarse_target(displacement, f=COARSE):
+    """block means of a [S, S, S, 3] displacement over f^3 blocks: the [S/f]^3 x 3 target"""
+    S = displacement.shape[0]
+    c = S // f
+    return displacement.reshape(c, f, c, f, c, f, 3).mean(axis=(1, 3, 5)).astype(np.float32)
+
+
+def upsample_displacement(coarse, shape):
+    """the coarse displacement on the full grid (order-1 resize on the GPU, the resampling
+    FastRegistration.py:562-564 applies between resolutions)"""
+    from . import _core
+    return _core.resize_linear(np.asarray(coarse, np.float64), shape)
+
+
+def make_pair(seed, size=SIZE):
+    from . import phantoms
+    return phantoms.make_pair((size,) * 3, seed, bins=BINS)
+
+
+def registration(core, pair, init_displacement=None, precision=None):
+    """a Registration of the pair from the identity grid, or from identity + init_displacement"""
+    from . import phantoms
+    from .utils import initialize_fourier_domain_smoothing
+    shape = pair.u.shape
+    V = int(np.prod(shape))
+    grid = phantoms.identity_positions(shape).astype(np.float32)
+    start = grid if init_displacement is None else \
+        (grid + np.asarray(init_displacement, np.float32)).astype(np.float32)
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
+    g = GAMMA_INIT * V
+    reg = core.Registration(start, 1, grid, grid, *shape, *shape, 3,
+                            float(np.count_nonzero(pair.u)))
+    reg.setNonLinearTransformation(g, g, g, 1, 1, 1, 1, 1, 1, D)
+    reg.setMILikelihood(ALPHA, np.full((BINS, BINS), 1.0 / BINS, np.float32), BINS, BINS, 1,
+                        pair.v, pair.u)
+    if precision is not None:
+        reg.set_precision(precision)
+    return reg
+
+
+def refine(core, pair, init_displacement=None, precision=0, max_iter=MAX_EM, th=CONVERGENCE):
+    """the plain method to convergence: (iterations, final displacement [S,S,S,3], final
+    min-log-posterior per non-zero voxel, the Registration)"""
+    from . import phantoms
+    reg = registration(core, pair, init_displacement, precision)
+    it = reg.EM(max_iter, th, 1, 0)
+    fin = reg.get_final_locations_as_numpy_array().astype(np.float64)
+    disp = fin - phantoms.identity_positions(pair.u.shape)
+    mlp = float(reg.iteration_stats()[-1, 3] / np.count_nonzero(pair.u))
+    return it, disp, mlp, reg
+
+
+def training_set(core, seeds, size=SIZE):
+    """inputs [n, S, S, S, 2] and targets [n, S/4, S/4, S/4, 3]: phantom pairs of this package's
+    generator, targets the plain method's converged displacements"""
+    xs, ts = [], []
+    for sd in seeds:
+        pair = make_pair(int(sd), size)
+        _, disp, _, _ = refine(core, pair)
+        xs.append(network_input(pair))
+        ts.append(coarse_target(disp))
+    return np.stack(xs), np.stack(ts)
+
+
+def train(net, xs, ts, steps, lr=1e-3, seed=0, log=None):
+    """Adam on random mini-batches of the training set; returns the loss history"""
+    rng = np.random.default_rng(seed)
+    n = len(xs)
+    hist = []
+    for step in range(steps):
+        idx = rng.choice(n, net.batch, replace=n < net.batch)
+        # random flips of the three axes (the displacement component flips with its axis)
+        x, t = xs[idx].copy(), ts[idx].copy()
+        for a in range(3):
+            if rng.random() < 0.5:
+                x = np.flip(x, axis=1 + a)
+                t = np.flip(t, axis=1 + a)
+                t[..., a] = -t[..., a]
+        cur = lr * (0.5 * (1 + np.cos(np.pi * step / max(1, steps))))  # cosine decay
+        hist.append(net.train_step(np.ascontiguousarray(x), np.ascontiguousarray(t), cur))
+        if log and (step % 100 == 0 or step == steps - 1):
+            log(f"step {step}: loss {hist[-1]:.5f}")
+    return hist
+
+
+def predict_displacement(net, pair):
+    """the network's displacement for one pair, up-sampled to the full grid"""
+    x = np.zeros((net.batch,) + network_input(pair).shape, np.float32)
+    x[0] = network_input(pair)
+    coarse = net.predict(x)[0]
+    return upsample_displacement(coarse, pair.u.shape)
+
+
+def main():
+    from . import _core as core
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--pairs", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    t0 = time.time()
+    xs, ts = training_set(core, range(a.seed, a.seed + a.pairs))
+    print(f"{a.pairs} training pairs in {time.time() - t0:.1f} s", flush=True)
+    net = InitNet(a.batch, SIZE, a.seed)
+    t0 = time.time()
+    train(net, xs, ts, a.steps, a.lr, a.seed, log=lambda s: print(s, flush=True))
+    print(f"{a.steps} steps in {time.time() - t0:.1f} s", flush=True)
+    net.save(a.out)
+
+
+if __name__ == "__main__":
+    main()

@@ -39,6 +39,7 @@ extern "C" {
 typedef struct binder_registration binder_registration;
 typedef struct binder_transform binder_transform;
 typedef struct binder_pyramid binder_pyramid;
+typedef struct binder_initnet binder_initnet;
 
 /* last error message of this thread ("" when none) */
 const char *binder_last_error(void);
@@ -200,7 +201,7 @@ int binder_registration_correct_topology(binder_registration *h, double e1, doub
  * with hi/lo TF32 operand splitting, FP32-level accuracy; _TF32 = one TF32 tensor-core product;
  * _BF16X3 = BF16 hi/lo operand splitting, three kind::f16 products (about 16 mantissa bits);
  * _BF16 = one BF16 product.  All accumulate in FP32.  The default comes from the
- * BINDER_B200_PRECISION environment variable (0 to 4), else TF32X3. */
+ * BINDER_B200_PRECISION environment variable (0 to 4), else BF16X3. */
 #define BINDER_PRECISION_FP32 0
 #define BINDER_PRECISION_TF32X3 1
 #define BINDER_PRECISION_TF32 2
@@ -368,6 +369,31 @@ int binder_topology_correct_3d(const double *field, double e1, double e2, int ma
 int binder_topology_correct_2d(const double *field, double e1, double e2, int max_outer_it,
                                int max_it, int threads, const double voxel_sizes[2], int Nx,
                                int Ny, double *out, long long *stats_out);
+
+/* ---- learned initialiser: no counterpart in the reference -----------------------------------
+ * A 3D convolutional encoder-decoder (channels 16-32-64-128, 3x3x3 convolutions with leaky ReLU,
+ * 2x2x2 average pooling, a skip connection at the 4-voxel level) whose prediction seeds the
+ * positions a registration starts from (the reference's hook is the final_locations argument of
+ * Registration, FastRegistration.py:443-450).  Input: batch x S^3 voxels x 2 channels (moving and
+ * fixed intensities in [0, 1]), FP32, channels last; S a multiple of 8.  Output: the displacement
+ * on the grid of every 4th voxel, batch x (S/4)^3 x 3, FP32, in voxels.  Every layer runs on
+ * hand-written sm_100a kernels: im2col gathers into BF16 operands, a tcgen05 BF16 GEMM with FP32
+ * accumulation in TMEM, FP32 master weights and Adam.  Pointers may be host or device memory. */
+int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed);
+int binder_initnet_destroy(binder_initnet *h);
+int binder_initnet_parameter_count(const binder_initnet *h, long long *out);
+/* FP32 parameters layer by layer: W [Cout][27 Cin] (tap-major: tap = (dx*3+dy)*3+dz, then Cin),
+ * then b [Cout]; layers in forward order */
+int binder_initnet_get_parameters(const binder_initnet *h, float *out);
+int binder_initnet_set_parameters(binder_initnet *h, const float *in);
+int binder_initnet_predict(binder_initnet *h, const float *in, float *out);
+/* one Adam step (beta 0.9 / 0.999) on the mean squared error against target; loss_out (optional)
+ * receives the loss before the step, grads_out (optional) its gradient */
+int binder_initnet_train_step(binder_initnet *h, const float *in, const float *target, double lr,
+                              double *loss_out, float *grads_out);
+/* the loss and its gradient without a step */
+int binder_initnet_gradients(binder_initnet *h, const float *in, const float *target,
+                             double *loss_out, float *grads_out);
 
 #ifdef __cplusplus
 }
