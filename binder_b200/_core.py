@@ -298,6 +298,10 @@ class Registration:
         3 tensor-core BF16 split (three products), 4 tensor-core BF16."""
         check(lib().binder_registration_set_precision(self._h, int(precision)))
 
+    def set_estep_grid(self, ctas):
+        """CTAs of the EM E-step launch (0: the default, every SM times its occupancy)."""
+        check(lib().binder_registration_set_estep_grid(self._h, int(ctas)))
+
     def stream(self):
         """The object's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
         p = C.c_void_p()
@@ -329,6 +333,36 @@ class Registration:
             stats.ctypes.data))
         return dict(zip(["outer_iterations", "inner_iterations", "below_e1_before",
                          "below_e1_after", "above_e2_before", "above_e2_after"], stats.tolist()))
+
+
+class RegistrationBatch:
+    """Many Registration objects (pairs of any sizes) run as one: each chunk of EM iterations is
+    one CUDA graph with every pair's kernels on a branch of its own (no counterpart in the
+    reference, which runs one pair per object).  Keeps references to its registrations."""
+
+    def __init__(self, registrations):
+        self._regs = list(registrations)
+        arr = (C.c_void_p * len(self._regs))(*[r._h.value for r in self._regs])
+        self._h = C.c_void_p()
+        check(lib().binder_batch_create(arr, len(self._regs), C.byref(self._h)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().binder_batch_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self._h = C.c_void_p()
+
+    def EM(self, max_EM_iterations, convergence_th, update_likelihood_parameters):
+        """EM of every pair; returns the iteration counts and sets last_ms (device time)"""
+        its = np.zeros(len(self._regs), np.int32)
+        ms = C.c_double(0)
+        check(lib().binder_batch_em(self._h, int(max_EM_iterations), float(convergence_th),
+                                    int(update_likelihood_parameters), its, C.byref(ms)))
+        self.last_ms = ms.value
+        return its
 
 
 class NonLinearTransformation:

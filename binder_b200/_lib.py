@@ -46,6 +46,8 @@ EXPORTS = [
     "binder_initnet_create", "binder_initnet_destroy", "binder_initnet_parameter_count",
     "binder_initnet_get_parameters", "binder_initnet_set_parameters", "binder_initnet_predict",
     "binder_initnet_train_step", "binder_initnet_gradients",
+    "binder_batch_create", "binder_batch_destroy", "binder_batch_em", "binder_gemm_bf16",
+    "binder_registration_set_estep_grid",
 ]
 
 
@@ -135,6 +137,11 @@ def _declare(lib):
         "binder_initnet_predict": [_P, _P, _P],
         "binder_initnet_train_step": [_P, _P, _P, _d, C.POINTER(_d), _P],
         "binder_initnet_gradients": [_P, _P, _P, C.POINTER(_d), _P],
+        "binder_batch_create": [_P, _i, C.POINTER(_P)],
+        "binder_gemm_bf16": [_P, _P, _P, _i, _i, _i],
+        "binder_batch_destroy": [_P],
+        "binder_batch_em": [_P, _i, _d, _i, _i32, C.POINTER(_d)],
+        "binder_registration_set_estep_grid": [_P, _i],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

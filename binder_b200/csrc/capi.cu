@@ -25,6 +25,9 @@ struct binder_pyramid {
 struct binder_initnet {
     binder::InitNet *impl;
 };
+struct binder_batch {
+    binder::RegistrationBatch *impl;
+};
 
 namespace {
 thread_local std::string g_err;
@@ -709,7 +712,65 @@ int binder_topology_correct_3d(const double *field, double e1, double e2, int ma
     });
 }
 
+// ---- batches of registrations ----------------------------------------------------------------
+int binder_batch_create(binder_registration *const *regs, int n, binder_batch **out) {
+    return guard([&] {
+        NEED(regs);
+        NEED(out);
+        *out = nullptr;
+        BINDER_CHECK(n >= 1, "a batch needs at least one registration");
+        std::vector<binder::Registration *> v;
+        for (int i = 0; i < n; ++i) {
+            NEED(regs[i]);
+            v.push_back(regs[i]->impl);
+        }
+        auto *h = new binder_batch{nullptr};
+        try {
+            h->impl = new binder::RegistrationBatch(v);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int binder_batch_destroy(binder_batch *h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->impl;
+        delete h;
+    });
+}
+
+int binder_batch_em(binder_batch *h, int max_iterations, double convergence_th,
+                    int update_likelihood_parameters, int *iterations_out, double *ms_out) {
+    return guard([&] {
+        NEED(h);
+        NEED(iterations_out);
+        h->impl->em(max_iterations, convergence_th, update_likelihood_parameters,
+                    iterations_out);
+        if (ms_out) *ms_out = h->impl->last_elapsed_ms();
+    });
+}
+
+int binder_registration_set_estep_grid(binder_registration *h, int ctas) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_estep_grid(ctas);
+    });
+}
+
 // ---- learned initialiser ----------------------------------------------------------------------
+int binder_gemm_bf16(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K) {
+    return guard([&] {
+        NEED(A);
+        NEED(B);
+        NEED(C);
+        binder::gemm_bf16_host(A, B, C, M, N, K);
+    });
+}
+
 int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed) {
     return guard([&] {
         NEED(out);

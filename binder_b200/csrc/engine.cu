@@ -641,18 +641,60 @@ EStepArgs Registration::estep_args(const int *skip) const {
     return e;
 }
 
-void Registration::enqueue_em_iteration(int max_iter, double th, int update) {
-    launch_estep(estep_args(&st_->done), false, egrid_e_, stream_);
+void Registration::enqueue_em_iteration(int max_iter, double th, int update, cudaStream_t s) {
+    const int grid = estep_grid_override_ > 0 ? estep_grid_override_ : egrid_e_;
+    launch_estep(estep_args(&st_->done), false, grid, s);
     if (lk_ == 1)
-        launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, stream_);
+        launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, s);
     else if (lk_ == 3)
-        launch_ssdf_update(fst_, fstats_, update, st_, stream_);
+        launch_ssdf_update(fst_, fstats_, update, st_, s);
     else
-        launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, stream_);
+        launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, s);
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
-                   rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, stream_);
-    launch_em_finish(st_, stats_, max_iter, th, nzv_, stream_);
+                   rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, s);
+    launch_em_finish(st_, stats_, max_iter, th, nzv_, s);
+}
+
+void Registration::em_prepare(int max_iterations) {
+    require_ready();
+    BINDER_CHECK(max_iterations >= 1, "max_iterations must be >= 1");
+    if (stats_cap_ < max_iterations) {
+        BINDER_CUDA(cudaStreamSynchronize(stream_));
+        dfree(stats_, own_stream_);
+        stats_ = dalloc<double>((size_t)max_iterations * 4, own_stream_);
+        stats_cap_ = max_iterations;
+        BINDER_CUDA(cudaStreamSynchronize(own_stream_));
+    }
+    BINDER_CUDA(cudaMemsetAsync(stats_, 0, sizeof(double) * 4 * max_iterations, stream_));
+    reset_state(false);
+    em_graph_.clear();
+}
+
+void Registration::enqueue_em(int n, int max_iterations, double th, int update, cudaStream_t s) {
+    for (int i = 0; i < n; ++i) enqueue_em_iteration(max_iterations, th, update, s);
+}
+
+int Registration::em_finish(double ms) {
+    DevState h{};
+    BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    iters_done_ = h.iter;
+    last_ms_ = ms;
+    return h.iter;
+}
+
+bool Registration::em_done() const {
+    int done = 0;
+    BINDER_CUDA(cudaMemcpyAsync(&done, &st_->done, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    BINDER_CUDA(cudaStreamSynchronize(stream_));
+    return done != 0;
+}
+
+void Registration::set_estep_grid(int g) {
+    BINDER_CHECK(g >= 0, "the E-step grid must be >= 0 (0: the default)");
+    estep_grid_override_ = g;
+    em_graph_.clear();
 }
 
 int Registration::em(int max_iterations, double convergence_th, int update, int debug) {
@@ -680,7 +722,7 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
         Graph graph;
         gc.kernels = capture_graph(stream_, graph, [&] {
             for (int c = 0; c < chunk; ++c)
-                enqueue_em_iteration(max_iterations, convergence_th, update);
+                enqueue_em_iteration(max_iterations, convergence_th, update, stream_);
         });
         gc.g = graph.g;
         gc.e = graph.e;
@@ -1130,6 +1172,75 @@ void Registration::get_state(double *gamma_out, double *nu_out, unsigned long lo
     if (nu_out) *nu_out = h.nu;
     if (degenerate) *degenerate = h.degenerate;
     if (flags) *flags = h.flags;
+}
+
+// ------------------------------------------------------------------------------------------
+RegistrationBatch::RegistrationBatch(const std::vector<Registration *> &regs) : regs_(regs) {
+    BINDER_CHECK(!regs.empty(), "a batch needs at least one registration");
+    for (auto *r : regs) BINDER_CHECK(r != nullptr, "a batch member is null");
+    BINDER_CUDA(cudaStreamCreateWithFlags(&master_, cudaStreamNonBlocking));
+    BINDER_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    branch_.resize(regs.size(), nullptr);
+    join_.resize(regs.size(), nullptr);
+    for (size_t i = 0; i < regs.size(); ++i) {
+        BINDER_CUDA(cudaStreamCreateWithFlags(&branch_[i], cudaStreamNonBlocking));
+        BINDER_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
+    }
+}
+
+RegistrationBatch::~RegistrationBatch() {
+    if (master_) cudaStreamSynchronize(master_);
+    for (size_t i = 0; i < branch_.size(); ++i) {
+        if (branch_[i]) cudaStreamSynchronize(branch_[i]), cudaStreamDestroy(branch_[i]);
+        if (join_[i]) cudaEventDestroy(join_[i]);
+    }
+    if (fork_) cudaEventDestroy(fork_);
+    if (master_) cudaStreamDestroy(master_);
+}
+
+void RegistrationBatch::em(int max_iterations, double th, int update, int *its_out) {
+    if (max_iterations <= 0) {
+        for (size_t i = 0; i < regs_.size(); ++i) its_out[i] = 0;
+        return;
+    }
+    for (auto *r : regs_) r->em_prepare(max_iterations);
+    const int chunk = max_iterations < 8 ? max_iterations : 8;
+    Graph graph;
+    const long long kernels = capture_graph(master_, graph, [&] {
+        BINDER_CUDA(cudaEventRecord(fork_, master_));
+        for (size_t i = 0; i < regs_.size(); ++i) {
+            BINDER_CUDA(cudaStreamWaitEvent(branch_[i], fork_, 0));
+            regs_[i]->enqueue_em(chunk, max_iterations, th, update, branch_[i]);
+            BINDER_CUDA(cudaEventRecord(join_[i], branch_[i]));
+            BINDER_CUDA(cudaStreamWaitEvent(master_, join_[i], 0));
+        }
+    });
+    cudaEvent_t t0, t1;
+    BINDER_CUDA(cudaEventCreate(&t0));
+    BINDER_CUDA(cudaEventCreate(&t1));
+    BINDER_CUDA(cudaEventRecord(t0, master_));
+    int launched = 0;
+    while (true) {
+        replay(graph, kernels, master_);
+        launched += chunk;
+        BINDER_CUDA(cudaStreamSynchronize(master_));
+        if (launched >= max_iterations) break;
+        bool all = true;
+        for (auto *r : regs_)
+            if (!r->em_done()) {
+                all = false;
+                break;
+            }
+        if (all) break;
+    }
+    BINDER_CUDA(cudaEventRecord(t1, master_));
+    BINDER_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    BINDER_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    last_ms_ = ms;
+    for (size_t i = 0; i < regs_.size(); ++i) its_out[i] = regs_[i]->em_finish(ms);
 }
 
 // ------------------------------------------------------------------------------------------

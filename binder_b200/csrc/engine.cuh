@@ -110,6 +110,17 @@ class Registration {
                         double *mean_out, double *cov_out, double *pooled_mean,
                         double *pooled_cov);
 
+    // em() in pieces, for running many registrations in one graph (RegistrationBatch): a fresh
+    // state and statistics buffer (host-synchronising), n iterations enqueued on stream s (each
+    // a no-op once the convergence rule has fired), and the iteration count afterwards
+    void em_prepare(int max_iterations);
+    void enqueue_em(int n, int max_iterations, double th, int update, cudaStream_t s);
+    int em_finish(double ms);
+    bool em_done() const;
+    // CTAs of the EM E-step launch (0: every SM times its occupancy, the default)
+    void set_estep_grid(int g);
+    long voxels() const { return V_; }
+
     // restore the positions given at construction, the theta given to set_mi_likelihood, the
     // gammas given to set_nonlinear_transformation and a fresh device state (device-to-device,
     // no host transfer)
@@ -151,7 +162,7 @@ class Registration {
     View estep_view() const;
     GridDims grid_dims() const;
     EStepArgs estep_args(const int *skip) const;
-    void enqueue_em_iteration(int max_iter, double th, int update);
+    void enqueue_em_iteration(int max_iter, double th, int update, cudaStream_t s);
     void reset_state(bool for_sampler);
     void require_ready() const;
     // bins, theta and histogram buffers of an M-channel MI-type likelihood
@@ -187,6 +198,7 @@ class Registration {
     };
     ChainBatch *cb_ = nullptr;
     void release_chains();
+    int estep_grid_override_ = 0;
     // likelihood / prior parameters
     bool have_mi_ = false, have_tr_ = false;
     int K_ = 0, L_ = 0;
@@ -209,6 +221,28 @@ class Registration {
     int fM_ = 0, fF_ = 0, fFn_ = 0;
     SsdState *ssd_ = nullptr, *ssd0_ = nullptr;  // SSD parameters, and as set
     float *colmax_ = nullptr, *colmax0_ = nullptr;  // SSD table column maxima, and as set
+    double last_ms_ = 0.0;
+};
+
+// Many registrations -- image pairs of any sizes, each its own Registration -- run as one: every
+// chunk of EM iterations is one CUDA graph holding each pair's kernels on a branch of its own, so
+// the pairs' kernels overlap on the GPU and the whole batch advances with one graph launch per
+// chunk.  Each pair keeps its own convergence test (its kernels become no-ops once it fires).
+class RegistrationBatch {
+  public:
+    explicit RegistrationBatch(const std::vector<Registration *> &regs);
+    ~RegistrationBatch();
+    // Registration::em for every pair; its_out[i] receives pair i's iteration count
+    void em(int max_iterations, double convergence_th, int update, int *its_out);
+    double last_elapsed_ms() const { return last_ms_; }
+    int size() const { return (int)regs_.size(); }
+
+  private:
+    std::vector<Registration *> regs_;
+    cudaStream_t master_ = nullptr;
+    std::vector<cudaStream_t> branch_;
+    cudaEvent_t fork_ = nullptr;
+    std::vector<cudaEvent_t> join_;
     double last_ms_ = 0.0;
 };
 

@@ -530,7 +530,7 @@ InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(bat
                              {64, 128, S3, 1}, {128, 128, S3, 1}, {128, 64, S2, 1},
                              {64, 64, S2, 1},  {64, 3, S2, 0}};
     long off = 0;
-    size_t col_max = 0;
+    size_t col_max = 0, dzt_max = 0;
     for (const auto &q : spec) {
         Layer l;
         l.cin = q[0]; l.cout = q[1]; l.S = q[2]; l.act = q[3] != 0;
@@ -541,7 +541,9 @@ InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(bat
         l.boff = off;
         off += l.cout;
         const long M = (long)batch * l.S * l.S * l.S;
-        col_max = std::max(col_max, (size_t)M * std::max(l.Kp, l.Kq));
+        const long Mp = round64((int)M);  // the weight-gradient GEMM's K, padded with zeros
+        col_max = std::max(col_max, (size_t)Mp * std::max(l.Kp, l.Kq));
+        dzt_max = std::max(dzt_max, (size_t)Mp * l.cout);
         m.L.push_back(l);
     }
     nparam_ = off;
@@ -579,7 +581,7 @@ InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(bat
     m.colT = m.alloc<uint16_t>(col_max);
     m.dz = m.alloc<float>(vox(S0) * 16);
     m.dzb = m.alloc<uint16_t>(vox(S0) * 16);
-    m.dzT = m.alloc<uint16_t>(vox(S0) * 16);
+    m.dzT = m.alloc<uint16_t>(dzt_max);
     // He-normal weights (the head 100 times smaller, so an untrained net predicts ~ 0), zero bias
     std::vector<float> h((size_t)nparam_, 0.0f);
     HostRng rng{seed * 0x2545F4914F6CDD1Dull + 1};
@@ -650,14 +652,21 @@ double InitNet::forward_backward(const float *in, const float *target, bool back
         const int cb = (int)std::min<long>((M + 255) / 256, 64);
         count_launch(), column_sum_kernel<<<dim3((unsigned)cb, (unsigned)l.cout), 256, 0, s>>>(
                             m.dz, M, l.cout, m.G + l.boff);
-        // weight gradient: dW [cout][27 cin] = dz^T . im2col(x), K = the voxels, split over CTAs
-        transpose(m.dzb, M, l.cout, l.cout, m.dzT, M);
+        // weight gradient: dW [cout][27 cin] = dz^T . im2col(x), K = the voxels (zero-padded to a
+        // multiple of 64), split over CTAs
+        const long Mp = round64((int)M);
+        if (Mp != M) {
+            BINDER_CUDA(cudaMemsetAsync(m.dzT, 0, sizeof(uint16_t) * Mp * l.cout, s));
+            BINDER_CUDA(cudaMemsetAsync(m.colT, 0, sizeof(uint16_t) * Mp * l.Kp, s));
+        }
+        transpose(m.dzb, M, l.cout, l.cout, m.dzT, Mp);
         im2col(x, l.S, l.cin, l.Kp);
-        transpose(m.col, M, l.Kp, l.Kp, m.colT, M);
-        long splits = M / 4096;
+        transpose(m.col, M, l.Kp, l.Kp, m.colT, Mp);
+        long splits = Mp / 4096;
         splits = splits < 1 ? 1 : (splits > 256 ? 256 : splits);
-        const int ks = round64((int)((M + splits - 1) / splits));
-        gemm_run(m.dzT, M, m.colT, M, l.cout, 27 * l.cin, (int)M, m.G + l.woff, 27L * l.cin, ks, 1);
+        const int ks = round64((int)((Mp + splits - 1) / splits));
+        gemm_run(m.dzT, Mp, m.colT, Mp, l.cout, 27 * l.cin, (int)Mp, m.G + l.woff, 27L * l.cin, ks,
+                 1);
         // data gradient: dx [M][cin] += im2col(dz) . flipped W, accumulated onto what dx holds
         if (dx) {
             im2col(m.dzb, l.S, l.cout, l.Kq);
@@ -775,6 +784,42 @@ double InitNet::train_step(const float *in, const float *target, double lr, floa
     }
     BINDER_CUDA(cudaGetLastError());
     return loss;
+}
+
+void gemm_bf16_host(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K) {
+    BINDER_CHECK(M > 0 && N > 0 && K > 0 && K % 64 == 0, "M, N > 0 and K a positive multiple of 64");
+    cudaStream_t s = nullptr;
+    BINDER_CUDA(cudaStreamCreate(&s));
+    uint16_t *a = nullptr, *b = nullptr;
+    float *c = nullptr;
+    int *err = nullptr;
+    try {
+        a = dev_alloc_n<uint16_t>((size_t)M * K, s);
+        b = dev_alloc_n<uint16_t>((size_t)N * K, s);
+        c = dev_alloc_n<float>((size_t)M * N, s);
+        err = dev_alloc_n<int>(1, s);
+        BINDER_CUDA(cudaMemcpyAsync(a, A, sizeof(uint16_t) * M * K, cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemcpyAsync(b, B, sizeof(uint16_t) * N * K, cudaMemcpyHostToDevice, s));
+        BINDER_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        // K split over CTAs when K is long (atomic accumulation), as the weight gradients run
+        const int ks = K > 4096 ? 1024 : K;
+        if (ks < K) BINDER_CUDA(cudaMemsetAsync(c, 0, sizeof(float) * M * N, s));
+        GemmArgs g{a, b, c, M, N, K, K, K, N, ks, ks < K ? 1 : 0, err};
+        launch_gemm_bf16(g, s);
+        int h = 0;
+        BINDER_CUDA(cudaMemcpyAsync(C, c, sizeof(float) * M * N, cudaMemcpyDeviceToHost, s));
+        BINDER_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        BINDER_CUDA(cudaStreamSynchronize(s));
+        if (h) throw Error(kDeviceFault, "a tensor-core GEMM wait timed out");
+    } catch (...) {
+        dev_free_p(a, s); dev_free_p(b, s); dev_free_p(c, s); dev_free_p(err, s);
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        throw;
+    }
+    dev_free_p(a, s); dev_free_p(b, s); dev_free_p(c, s); dev_free_p(err, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
 }
 
 }  // namespace binder

@@ -26,6 +26,8 @@ struct GemmArgs {
     int *err;        // set to 1 when a bounded wait gives up
 };
 void launch_gemm_bf16(const GemmArgs &g, cudaStream_t s);
+// the same on host arrays (row-major, leading dimensions K, K, N), through device copies
+void gemm_bf16_host(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K);
 
 // the network's shape: input [B][S][S][S][2] (moving, fixed intensities), output the coarse
 // displacement [B][S/4][S/4][S/4][3] in voxels of the input grid; S a multiple of 8

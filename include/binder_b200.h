@@ -40,6 +40,7 @@ typedef struct binder_registration binder_registration;
 typedef struct binder_transform binder_transform;
 typedef struct binder_pyramid binder_pyramid;
 typedef struct binder_initnet binder_initnet;
+typedef struct binder_batch binder_batch;
 
 /* last error message of this thread ("" when none) */
 const char *binder_last_error(void);
@@ -370,6 +371,23 @@ int binder_topology_correct_2d(const double *field, double e1, double e2, int ma
                                int max_it, int threads, const double voxel_sizes[2], int Nx,
                                int Ny, double *out, long long *stats_out);
 
+/* ---- batches of registrations: no counterpart in the reference, which runs one pair per
+ * Registration object (FastRegistration.py:443-486) ---------------------------------------------
+ * Many registrations, image pairs of any sizes each set up as usual, run as one: every chunk of
+ * EM iterations is one CUDA graph holding each pair's kernels on a branch of its own, so the
+ * pairs' kernels overlap on the GPU and the whole batch advances with one graph launch per chunk.
+ * Each pair keeps its own convergence test.  The registrations must outlive the batch; a
+ * registration's own calls must not run while the batch runs. */
+int binder_batch_create(binder_registration *const *regs, int n, binder_batch **out);
+int binder_batch_destroy(binder_batch *h);
+/* EM(max_iterations, convergence_th, update_likelihood_parameters) of every pair;
+ * iterations_out [n] receives each pair's iteration count, ms_out (optional) the device time */
+int binder_batch_em(binder_batch *h, int max_iterations, double convergence_th,
+                    int update_likelihood_parameters, int *iterations_out, double *ms_out);
+/* No counterpart in the reference: CTAs of the EM E-step launch (0 restores the default, every SM
+ * times its occupancy); smaller grids let the pairs of a batch share the GPU */
+int binder_registration_set_estep_grid(binder_registration *h, int ctas);
+
 /* ---- learned initialiser: no counterpart in the reference -----------------------------------
  * A 3D convolutional encoder-decoder (channels 16-32-64-128, 3x3x3 convolutions with leaky ReLU,
  * 2x2x2 average pooling, a skip connection at the 4-voxel level) whose prediction seeds the
@@ -379,6 +397,10 @@ int binder_topology_correct_2d(const double *field, double e1, double e2, int ma
  * on the grid of every 4th voxel, batch x (S/4)^3 x 3, FP32, in voxels.  Every layer runs on
  * hand-written sm_100a kernels: im2col gathers into BF16 operands, a tcgen05 BF16 GEMM with FP32
  * accumulation in TMEM, FP32 master weights and Adam.  Pointers may be host or device memory. */
+/* The network's matrix product on host arrays: C [M][N] (FP32) = A [M][K] . B [N][K]^T with
+ * BF16 operands (raw bits, row-major, K contiguous), K a multiple of 64, on the tcgen05 kernel
+ * every convolution runs on (FP32 accumulation in TMEM; K split over CTAs above 4096). */
+int binder_gemm_bf16(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K);
 int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed);
 int binder_initnet_destroy(binder_initnet *h);
 int binder_initnet_parameter_count(const binder_initnet *h, long long *out);
