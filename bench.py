@@ -179,6 +179,67 @@ def phantoms_grid(shape):
     return phantoms.identity_positions(shape).astype(np.float64)
 
 
+C4_PAIRS = 64
+C4_SIDES = (48, 160)
+C4_SEED = 4242
+
+
+def _c4_pair(args):
+    """one pair of the batch (a module-level function, so a spawn pool can run it)"""
+    shape, seed = args
+    from binder_b200 import phantoms
+    return phantoms.make_pair(tuple(int(x) for x in shape), int(seed), bins=BINS)
+
+
+def c4_shapes():
+    rng = np.random.default_rng(C4_SEED)
+    return [tuple(int(v) for v in rng.integers(C4_SIDES[0], C4_SIDES[1] + 1, 3))
+            for _ in range(C4_PAIRS)]
+
+
+def run_batch(core, rank, em_iters, dist):
+    """Batched serving-style workload: 64 phantom pairs of uneven sizes (sides uniform in
+    48..160, seed 4242), each registered by em_iters EM iterations, all pairs in one batch
+    (RegistrationBatch: one graph per EM chunk, every pair on a branch of its own; launch shapes
+    per size class from the autotuner).  value: pairs/s by device time; compared with the same
+    registrations one after another (each pair's own EM calls)."""
+    import multiprocessing as mp
+    import tempfile
+
+    from binder_b200 import autotune
+    from binder_b200.initnet import registration
+    shapes = c4_shapes()
+    work = [(s, C4_SEED + i + 1000 * rank) for i, s in enumerate(shapes)]
+    with mp.get_context("spawn").Pool(min(len(work), os.cpu_count() or 1)) as pool:
+        pairs = pool.map(_c4_pair, work)
+    regs = [registration(core, p) for p in pairs]
+    # one by one
+    seq_ms = 0.0
+    for r in regs:
+        r.EM(em_iters, -1e300, 1, 0)
+        r.reset()
+        r.EM(em_iters, -1e300, 1, 0)
+        seq_ms += r.last_elapsed_ms()
+        r.reset()
+    cache = os.path.join(tempfile.gettempdir(), "binder_b200_autotune.json")
+    table = autotune.tune(core, regs, shapes, cache=cache, retune=True)
+    batch = core.RegistrationBatch(regs)
+    batch.EM(em_iters, -1e300, 1)  # warm-up
+    for r in regs:
+        r.reset()
+    barrier(dist)
+    its = batch.EM(em_iters, -1e300, 1)
+    ms = max_over_ranks(batch.last_ms, dist)
+    world = dist.get_world_size() if dist is not None else 1
+    voxels = int(sum(np.prod(s) for s in shapes))
+    return {"metric": f"batched registrations/s ({C4_PAIRS} MI pairs, sides 48..160, 64 bins, "
+                      f"{em_iters} EM iterations each, one batch)",
+            "value": world * C4_PAIRS / (ms / 1e3), "unit": "pairs/s", "higher_is_better": True,
+            "ms_per_batch": ms, "one_by_one_pairs_per_s": C4_PAIRS / (seq_ms / 1e3),
+            "speedup_vs_one_by_one": seq_ms / ms, "total_voxels": voxels,
+            "iterations": sorted(set(int(i) for i in its)), "autotune": table}
+
+
 C1_SHAPE = (128, 128)
 C1_BINS = 32
 C1_SEED = 12345
@@ -588,6 +649,8 @@ def run_b200(args, rank, world, local, dist):
     topology = run_topology(core, rank, dist)
     # Gibbs sampling throughput on the 96^3 pair (every rank runs its own chains)
     gibbs = run_gibbs(core, rank, args.gibbs_chains, dist)
+    # 64 pairs of uneven sizes in one batch
+    batched = run_batch(core, rank, args.em_iters, dist)
     # 2D registrations on the 128x128 pair
     reg2d = run_2d(core, rank, args.em_iters, dist)
 
@@ -617,6 +680,7 @@ def run_b200(args, rank, world, local, dist):
         "precision_arms": arms,
         "topology_c2": topology,
         "gibbs": gibbs,
+        "batch_c4": batched,
         "registration_2d": reg2d,
         "cpu_baseline": cpu_baseline(inp, args.em_iters),
     }

@@ -1,0 +1,75 @@
+"""Launch-shape autotuner for batches of registrations (no counterpart in the reference).
+
+When many pairs of uneven sizes run as one batch (RegistrationBatch), each pair's kernels share
+the GPU with the others', and the best launch shape per pair depends on its size: a small pair's
+E-step wants few CTAs (its voxels fill few SMs and leave the rest to other pairs), a large pair's
+wants the whole GPU.  This module groups pairs into size classes by voxel count, times a few EM
+iterations of each class's sub-batch under every candidate -- the E-step's CTA count and the DCT
+passes' operand format -- and keeps the fastest per class.  Results are cached in a JSON file
+keyed by class, so later batches reuse them without timing.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+# E-step CTAs (0: every SM times its occupancy) x DCT operand format (3 BF16 split, 1 TF32 split)
+CANDIDATES = [dict(estep_ctas=c, precision=p) for c in (0, 148, 74, 37) for p in (3, 1)]
+CLASS_EDGES = (64 ** 3, 112 ** 3)  # voxel counts separating the small / medium / large classes
+
+
+def size_class(shape):
+    V = int(np.prod(shape))
+    if V <= CLASS_EDGES[0]:
+        return "small"
+    return "medium" if V <= CLASS_EDGES[1] else "large"
+
+
+def apply(reg, config):
+    reg.set_estep_grid(int(config["estep_ctas"]))
+    reg.set_precision(int(config["precision"]))
+
+
+def load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def tune(core, regs, shapes, cache=None, iterations=6, retune=False):
+    """the fastest candidate per size class of the given registrations (timed on sub-batches of
+    at most 8 pairs per class), applied to every registration; returns {class: config}"""
+    table = {} if (retune or not cache) else load(cache)
+    by_class = {}
+    for r, s in zip(regs, shapes):
+        by_class.setdefault(size_class(s), []).append(r)
+    for cls, members in by_class.items():
+        if cls in table:
+            continue
+        sub = members[:8]
+        best = None
+        for cand in CANDIDATES:
+            for r in sub:
+                apply(r, cand)
+                r.reset()
+            b = core.RegistrationBatch(sub)
+            b.EM(iterations, -1e300, 1)  # warm-up (graph capture, first launches)
+            for r in sub:
+                r.reset()
+            b.EM(iterations, -1e300, 1)
+            ms = b.last_ms
+            if best is None or ms < best[0]:
+                best = (ms, cand)
+        table[cls] = dict(best[1], ms_per_iteration=best[0] / iterations, pairs=len(sub))
+    for r, s in zip(regs, shapes):
+        apply(r, table[size_class(s)])
+        r.reset()
+    if cache:
+        os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+        with open(cache, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+    return table

@@ -173,12 +173,28 @@ def refine(core, pair, init_displacement=None, precision=0, max_iter=MAX_EM, th=
     return it, disp, mlp, reg
 
 
+def _pair_job(args):
+    """one phantom pair (module level, so a spawn pool can run it)"""
+    return make_pair(*args)
+
+
+def make_pairs(seeds, size=SIZE, workers=None):
+    """phantom pairs for the seeds, generated on the host cores by a spawn pool"""
+    import multiprocessing as mp
+    import os
+    jobs = [(int(sd), size) for sd in seeds]
+    n = min(len(jobs), workers or os.cpu_count() or 1)
+    if n <= 1:
+        return [_pair_job(j) for j in jobs]
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(_pair_job, jobs, chunksize=max(1, len(jobs) // (4 * n)))
+
+
 def training_set(core, seeds, size=SIZE):
     """inputs [n, S, S, S, 2] and targets [n, S/4, S/4, S/4, 3]: phantom pairs of this package's
     generator, targets the plain method's converged displacements"""
     xs, ts = [], []
-    for sd in seeds:
-        pair = make_pair(int(sd), size)
+    for pair in make_pairs(seeds, size):
         _, disp, _, _ = refine(core, pair)
         xs.append(network_input(pair))
         ts.append(coarse_target(disp))
