@@ -350,7 +350,8 @@ Registration::~Registration() {
     em_graph_.clear();
     const cudaStream_t s = own_stream_;
     dfree(d_, s); dfree(x_, s); dfree(r_, s); dfree(D_, s); dfree(theta_, s); dfree(hist_, s);
-    dfree(hcnt_, s); dfree(u_, s); dfree(vpad_, s); dfree(mean_, s); dfree(m2_, s);
+    dfree(hcnt_, s); dfree(u_, s); dfree(vpad_, s); dfree(mean_, s);
+    dfree(m2_, s); dfree(hfix_, s); dfree(mpart_, s); dfree(hdone_, s);
     dfree(stats_, s); dfree(st_, s); dfree(d0_, s); dfree(theta0_, s);
     dfree(ssd_, s); dfree(ssd0_, s); dfree(colmax_, s); dfree(colmax0_, s);
     dfree(fx_, s); dfree(fn_, s); dfree(fst_, s); dfree(fst0_, s); dfree(fstats_, s);
@@ -409,7 +410,8 @@ void Registration::load_bins(double alpha, const float *theta, int K, int L, int
     const size_t padded = (size_t)(w.nxn + 2 * P_) * pyn_ * zp_;
     const long nv = V_ + M - 1, nn = Vn_ + M - 1;  // bins read: [index + m], m < M
     const long cells = (long)M * K * L;
-    dfree(u_, s); dfree(vpad_, s); dfree(theta_, s); dfree(hist_, s); dfree(hcnt_, s);
+    dfree(u_, s); dfree(vpad_, s); dfree(theta_, s); dfree(hist_, s);
+    dfree(hcnt_, s); dfree(hfix_, s); dfree(mpart_, s); dfree(hdone_, s);
     dfree(theta0_, s);
     u_ = dalloc<uint8_t>((size_t)nv, s);
     theta0_ = dalloc<float>((size_t)cells, s);
@@ -431,6 +433,15 @@ void Registration::load_bins(double alpha, const float *theta, int K, int L, int
     for (int m = 0; m < M; ++m)
         launch_bins_to_padded(bins + nv + m, w.nxn, w.nyn, w.nzn, K, vpad_ + padded * m, P_, Py,
                               PZ_, pyn_, zp_, M > 1 ? bad + 2 : bad + 1, s);
+    // the buffers of the order-independent histogram merge of the single-pass EM kernel (one
+    // channel, K <= 64)
+    if (M == 1 && K <= 64) {
+        hfix_ = dalloc<unsigned long long>((size_t)K * L, s);
+        mpart_ = dalloc<double>(kMaxEmCtas, s);
+        hdone_ = dalloc<unsigned>(1, s);
+        BINDER_CUDA(cudaMemsetAsync(hfix_, 0, sizeof(unsigned long long) * K * L, s));
+        BINDER_CUDA(cudaMemsetAsync(hdone_, 0, sizeof(unsigned), s));
+    }
     BINDER_CUDA(cudaMemcpyAsync(theta_, theta, sizeof(float) * cells, cudaMemcpyDefault, s));
     BINDER_CUDA(cudaMemcpyAsync(theta0_, theta_, sizeof(float) * cells, cudaMemcpyDeviceToDevice, s));
     BINDER_CUDA(cudaMemsetAsync(hist_, 0, sizeof(float) * cells, s));
@@ -631,6 +642,7 @@ EStepArgs Registration::estep_args(const int *skip) const {
     const View w = estep_view();
     EStepArgs e{};
     e.d = d_; e.r = r_; e.x = x_; e.u = u_; e.vpad = vpad_; e.theta = theta_; e.hist = hist_;
+    e.hfix = hfix_; e.mpart = mpart_; e.hdone = hdone_;
     e.hcnt = hcnt_; e.st = st_; e.skip = skip; e.V = V_;
     e.nx = w.nx; e.ny = w.ny; e.nz = w.nz; e.nxn = w.nxn; e.nyn = w.nyn; e.nzn = w.nzn;
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;

@@ -182,6 +182,9 @@ class Registration {
     TopologyWorkspace *topo_ = nullptr;
     unsigned *hcnt_ = nullptr;
     uint8_t *u_ = nullptr, *vpad_ = nullptr;
+    unsigned long long *hfix_ = nullptr;  // order-independent EM histogram merge (EStepArgs)
+    double *mpart_ = nullptr;
+    unsigned *hdone_ = nullptr;
     double *mean_ = nullptr, *m2_ = nullptr, *stats_ = nullptr;
     int stats_cap_ = 0;
     DevState *st_ = nullptr;

@@ -366,15 +366,50 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
         vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
     }
     __syncthreads();
+    const double m = block_sum(mll, red);
+    const double dg = block_sum((double)deg, red);
+    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+    if (!a.hfix) {
+        for (int q = threadIdx.x; q < KL; q += TPB) {
+            const int k = q / L;
+            const unsigned v = hs[k * LP + (q - k * L)];
+            if (v) atomicAdd(&a.hist[q], (float)v * a.hinv);
+        }
+        if (threadIdx.x == 0) atomicAdd(&a.st->mll, m);
+        return;
+    }
+    // Order-independent merge, so that EM is bitwise repeatable: the CTA histograms are integers
+    // and their 64-bit global sums are exact whatever order the CTAs arrive in; the last CTA to
+    // finish converts the sums to the FP32 histogram (one rounding per cell) and adds the CTAs'
+    // log-likelihood partials in CTA order.
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L;
         const unsigned v = hs[k * LP + (q - k * L)];
-        if (v) atomicAdd(&a.hist[q], (float)v * a.hinv);
+        if (v) atomicAdd(&a.hfix[q], (unsigned long long)v);
     }
-    const double m = block_sum(mll, red);
-    if (threadIdx.x == 0) atomicAdd(&a.st->mll, m);
-    const double dg = block_sum((double)deg, red);
-    if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
+    if (threadIdx.x == 0) a.mpart[blockIdx.x] = m;
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned last;
+    if (threadIdx.x == 0) last = atomicAdd(a.hdone, 1u) == gridDim.x - 1 ? 1u : 0u;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const double hinv = (double)a.hinv;
+    for (int q = threadIdx.x; q < KL; q += TPB) {
+        const unsigned long long v = __ldcg(a.hfix + q);
+        if (v) {
+            a.hist[q] += (float)((double)v * hinv);
+            a.hfix[q] = 0ull;
+        }
+    }
+    double part = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += TPB) part += __ldcg(a.mpart + b);
+    const double tot = block_sum(part, red);
+    if (threadIdx.x == 0) {
+        a.st->mll += tot;
+        *a.hdone = 0u;
+    }
 }
 
 // EM E-step with the MI filter likelihood (BINDER/src/cpu/MILikelihoodFilter.cpp:53-68 and
@@ -1261,6 +1296,8 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
                         : args.filter ? filter_smem(args.K, args.L, args.M)
                                       : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
+    // the order-independent merge of the single-pass EM kernel keeps one partial per CTA
+    if (a.hfix && grid > kMaxEmCtas) grid = kMaxEmCtas;
     // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
     // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a
     // cell, fit in 32 bits

@@ -17,6 +17,12 @@ struct EStepArgs {
     const uint8_t *vpad;  // moving-image bins, zero-padded [nxn+2P][nyn+2P][zp bytes]
     const float *theta;   // [K*L]
     float *hist;          // EM: soft joint histogram [K*L] (accumulated)
+    // the single-pass EM kernel's order-independent merge (all three null: FP32 atomics instead):
+    // 64-bit fixed-point sums [K*L] (zero between launches), one log-likelihood partial per CTA
+    // [kMaxEmCtas], and the count of CTAs done (zero between launches)
+    unsigned long long *hfix;
+    double *mpart;
+    unsigned *hdone;
     unsigned *hcnt;       // Gibbs: joint counts [K*L] (accumulated)
     DevState *st;
     const int *skip;
@@ -50,6 +56,8 @@ struct EStepArgs {
     float hscale, hinv;
 };
 
+// CTAs of the single-pass EM kernel at most when it merges in fixed order (EStepArgs::mpart)
+constexpr int kMaxEmCtas = 2048;
 // chains > 1: a batch of chains, the sampling E-step only (chain = blockIdx.y; buffers
 // [chains][dim][V] positions / dream locations, [chains][K][L] theta / counts, [chains] states)
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s, int chains = 1);

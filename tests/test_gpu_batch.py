@@ -1,7 +1,7 @@
 """A batch of registrations of uneven sizes in one graph per EM chunk (RegistrationBatch) against
 the same pairs registered one by one: the same iteration counts and final positions within 1e-4
-voxels (the joint histograms' FP32 atomics may add in another order, so theta can differ in its
-last bits)."""
+voxels (the batch's E-steps run on 16 CTAs, whose fixed-point histogram scale differs from the
+default grid's, so theta can differ in its last bits)."""
 import numpy as np
 import pytest
 
