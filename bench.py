@@ -240,6 +240,70 @@ def run_batch(core, rank, em_iters, dist):
             "iterations": sorted(set(int(i) for i in its)), "autotune": table}
 
 
+INITNET_CKPT = os.path.join(ROOT, "binder_b200", "data", "initnet_seeded_64.npz")
+LEARNED_PAIRS = 8
+
+
+def run_learned(core, rank, dist):
+    """The metric's comparison with the learned initialiser (64^3 held-out pairs, seeds
+    900000.., the reference CLI's convergence rule): the plain FP32 method from the identity
+    against the committed EM-seeded network + BF16-split passes (16 plain iterations, the
+    network, then EM to convergence).  Device time of every EM call (CUDA events) plus the
+    network's inference (CUDA events around it); the two arms' iterations, final
+    min-log-posterior per voxel and negative Jacobians."""
+    import torch
+    from binder_b200 import initnet as I
+    from binder_b200 import phantoms
+    if not os.path.exists(INITNET_CKPT):
+        return None
+    net = I.InitNet(1, I.SIZE, 0, in_channels=5)
+    net.load(INITNET_CKPT)
+    pairs = I.make_pairs(range(900000 + 1000 * rank, 900000 + 1000 * rank + LEARNED_PAIRS))
+    # warm-up of both paths
+    I.refine(core, pairs[0], precision=0, max_iter=8)
+    I.learned_registration(core, net, pairs[0])
+    plain_ms = learned_ms = 0.0
+    its0, its1, mlp0, mlp1, neg0, neg1 = [], [], [], [], [], []
+    for pair in pairs:
+        shape = pair.u.shape
+        grid = phantoms.identity_positions(shape)
+        it, d, mlp, reg = I.refine(core, pair, precision=0)
+        plain_ms += reg.last_elapsed_ms()
+        its0.append(it), mlp0.append(mlp)
+        neg0.append(int((core.compute_jacobian_determinant_3D(grid + d, *shape, 1, 1, 1) < 0).sum()))
+        # learned: early EM, network, EM to convergence, each device-timed
+        reg_e, early = I.early_em(core, pair)
+        ms = reg_e.last_elapsed_ms()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        init = early + I.predict_displacement(net, pair, early)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        it, d, mlp, reg = I.refine(core, pair, init_displacement=init, precision=3)
+        ms += reg.last_elapsed_ms()
+        learned_ms += ms
+        its1.append(I.EARLY_EM + it), mlp1.append(mlp)
+        neg1.append(int((core.compute_jacobian_determinant_3D(grid + d, *shape, 1, 1, 1) < 0).sum()))
+    plain_ms = max_over_ranks(plain_ms, dist)
+    learned_ms = max_over_ranks(learned_ms, dist)
+    n = len(pairs)
+    return {"metric": "64^3 registrations/s to convergence (held-out pairs): learned init + BF16 "
+                      "against plain FP32 from the identity",
+            "plain_fp32": {"registrations_per_s": n / (plain_ms / 1e3),
+                           "mean_iterations": float(np.mean(its0)),
+                           "mean_final_mlp_per_voxel": float(np.mean(mlp0)),
+                           "negative_jacobians": int(sum(neg0))},
+            "learned_bf16": {"registrations_per_s": n / (learned_ms / 1e3),
+                             "mean_iterations": float(np.mean(its1)),
+                             "mean_final_mlp_per_voxel": float(np.mean(mlp1)),
+                             "negative_jacobians": int(sum(neg1))},
+            "speedup": plain_ms / learned_ms, "pairs": n,
+            "note": "inference time of the network included in the learned arm; the network "
+                    "input includes the displacement after 16 plain EM iterations"}
+
+
 C1_SHAPE = (128, 128)
 C1_BINS = 32
 C1_SEED = 12345
@@ -647,6 +711,7 @@ def run_b200(args, rank, world, local, dist):
             "speedup_vs_plain_fp32": plain_ms / (ms / args.steps)}
 
     topology = run_topology(core, rank, dist)
+    learned = run_learned(core, rank, dist)
     # Gibbs sampling throughput on the 96^3 pair (every rank runs its own chains)
     gibbs = run_gibbs(core, rank, args.gibbs_chains, dist)
     # 64 pairs of uneven sizes in one batch
@@ -678,6 +743,7 @@ def run_b200(args, rank, world, local, dist):
                      "topology_stats": topo_stats},
         "em_iterations_per_s": world * args.em_iters / ((em_ms or 1) / 1e3),
         "precision_arms": arms,
+        "learned_init": learned,
         "topology_c2": topology,
         "gibbs": gibbs,
         "batch_c4": batched,

@@ -129,7 +129,7 @@ def _declare(lib):
                                                    C.POINTER(_d), C.POINTER(C.c_longlong)],
         "binder_topology_correct_3d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _i, _f64, _P],
         "binder_topology_correct_2d": [_f64, _d, _d, _i, _i, _i, _f64, _i, _i, _f64, _P],
-        "binder_initnet_create": [C.POINTER(_P), _i, _i, _u64],
+        "binder_initnet_create": [C.POINTER(_P), _i, _i, _i, _u64],
         "binder_initnet_destroy": [_P],
         "binder_initnet_parameter_count": [_P, C.POINTER(C.c_longlong)],
         "binder_initnet_get_parameters": [_P, _P],

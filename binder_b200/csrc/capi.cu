@@ -771,13 +771,14 @@ int binder_gemm_bf16(const uint16_t *A, const uint16_t *B, float *C, int M, int 
     });
 }
 
-int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed) {
+int binder_initnet_create(binder_initnet **out, int batch, int size, int in_channels,
+                          uint64_t seed) {
     return guard([&] {
         NEED(out);
         *out = nullptr;
         auto *h = new binder_initnet{nullptr};
         try {
-            h->impl = new binder::InitNet(batch, size, seed);
+            h->impl = new binder::InitNet(batch, size, seed, in_channels);
         } catch (...) {
             delete h;
             throw;

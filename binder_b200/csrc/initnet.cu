@@ -515,7 +515,8 @@ __global__ void add_f32_kernel(float *dst, const float *src, long n) {
 }
 }  // namespace
 
-InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(batch), S_(size) {
+InitNet::InitNet(int batch, int size, uint64_t seed, int in_channels)
+    : impl_(new Impl()), B_(batch), S_(size), Cin_(in_channels) {
     BINDER_CHECK(batch >= 1 && batch <= 64, "batch must be in [1, 64]");
     BINDER_CHECK(size >= 8 && size % 8 == 0 && size <= 256,
                  "the input size must be a multiple of 8 in [8, 256]");
@@ -525,7 +526,8 @@ InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(bat
     BINDER_CUDA(cudaMemsetAsync(m.err, 0, sizeof(int), m.s));
     const int S0 = size, S1 = size / 2, S2 = size / 4, S3 = size / 8;
     // encoder (channels 16-32-64-128, two convolutions per level), decoder to the 4-voxel grid
-    const int spec[11][4] = {{2, 16, S0, 1},   {16, 16, S0, 1},   {16, 32, S1, 1},
+    BINDER_CHECK(in_channels >= 1 && in_channels <= 16, "input channels must be in [1, 16]");
+    const int spec[11][4] = {{in_channels, 16, S0, 1},   {16, 16, S0, 1},   {16, 32, S1, 1},
                              {32, 32, S1, 1},  {32, 64, S2, 1},   {64, 64, S2, 1},
                              {64, 128, S3, 1}, {128, 128, S3, 1}, {128, 64, S2, 1},
                              {64, 64, S2, 1},  {64, 3, S2, 0}};
@@ -564,8 +566,8 @@ InitNet::InitNet(int batch, int size, uint64_t seed) : impl_(new Impl()), B_(bat
         l.dy = m.alloc<float>((size_t)M * l.cout);
     }
     auto vox = [&](int S) { return (size_t)batch * S * S * S; };
-    m.x0 = m.alloc<uint16_t>(vox(S0) * 2);
-    m.in_f = m.alloc<float>(vox(S0) * 2);
+    m.x0 = m.alloc<uint16_t>(vox(S0) * in_channels);
+    m.in_f = m.alloc<float>(vox(S0) * in_channels);
     m.tgt = m.alloc<float>(vox(S2) * 3);
     m.p0 = m.alloc<uint16_t>(vox(S1) * 16);
     m.p1 = m.alloc<uint16_t>(vox(S2) * 32);
@@ -677,8 +679,9 @@ double InitNet::forward_backward(const float *in, const float *target, bool back
     std::vector<Layer> &L = m.L;
     const int S0 = S_, S1 = S_ / 2, S2 = S_ / 4, S3 = S_ / 8;
 
-    BINDER_CUDA(cudaMemcpyAsync(m.in_f, in, sizeof(float) * vox(S0) * 2, cudaMemcpyDefault, s));
-    count_launch(), to_bf16_kernel<<<grid_for_n(vox(S0) * 2), 256, 0, s>>>(m.in_f, vox(S0) * 2, m.x0);
+    BINDER_CUDA(cudaMemcpyAsync(m.in_f, in, sizeof(float) * vox(S0) * Cin_, cudaMemcpyDefault, s));
+    count_launch(), to_bf16_kernel<<<grid_for_n(vox(S0) * Cin_), 256, 0, s>>>(m.in_f, vox(S0) * Cin_,
+                                                                              m.x0);
     forward(L[0], m.x0);
     forward(L[1], L[0].y);
     count_launch(), avgpool2_kernel<<<grid_for_n(vox(S1) * 16), 256, 0, s>>>(L[1].y, B, S0, 16, m.p0);

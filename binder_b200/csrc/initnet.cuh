@@ -29,17 +29,12 @@ void launch_gemm_bf16(const GemmArgs &g, cudaStream_t s);
 // the same on host arrays (row-major, leading dimensions K, K, N), through device copies
 void gemm_bf16_host(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K);
 
-// the network's shape: input [B][S][S][S][2] (moving, fixed intensities), output the coarse
-// displacement [B][S/4][S/4][S/4][3] in voxels of the input grid; S a multiple of 8
-struct InitNetShape {
-    int B, S;
-};
-
 class InitNet {
   public:
-    explicit InitNet(int batch, int size, uint64_t seed);
+    // in_channels: input channels per voxel (2: moving and fixed intensities)
+    InitNet(int batch, int size, uint64_t seed, int in_channels = 2);
     ~InitNet();
-    // forward pass of `in` (device or host memory, FP32 [B][S^3][2]) into out (FP32
+    // forward pass of `in` (device or host memory, FP32 [B][S^3][in_channels]) into out (FP32
     // [B][(S/4)^3][3], host or device)
     void predict(const float *in, float *out);
     // one Adam step on the mean squared error against `target` ([B][(S/4)^3][3]); returns the
@@ -52,13 +47,14 @@ class InitNet {
     void get_parameters(float *out) const;  // FP32 master copy, layer by layer: W [Cout][27 Cin], b [Cout]
     void set_parameters(const float *in);
     int batch() const { return B_; }
+    int in_channels() const { return Cin_; }
     int size() const { return S_; }
 
   private:
     struct Layer;
     struct Impl;
     Impl *impl_;
-    int B_, S_;
+    int B_, S_, Cin_;
     long nparam_;
     double forward_backward(const float *in, const float *target, bool backward);
 };

@@ -38,10 +38,11 @@ class InitNet:
     """ctypes front of binder_initnet_*: batch x size^3 x 2 FP32 input (moving, fixed), batch x
     (size/4)^3 x 3 FP32 output (displacement in voxels)."""
 
-    def __init__(self, batch=4, size=SIZE, seed=0):
-        self.batch, self.size = int(batch), int(size)
+    def __init__(self, batch=4, size=SIZE, seed=0, in_channels=2):
+        self.batch, self.size, self.in_channels = int(batch), int(size), int(in_channels)
         self._h = C.c_void_p()
-        check(lib().binder_initnet_create(C.byref(self._h), self.batch, self.size, int(seed)))
+        check(lib().binder_initnet_create(C.byref(self._h), self.batch, self.size,
+                                          self.in_channels, int(seed)))
         n = C.c_longlong(0)
         check(lib().binder_initnet_parameter_count(self._h, C.byref(n)))
         self.nparam = int(n.value)
@@ -57,8 +58,9 @@ class InitNet:
 
     def _in(self, x):
         x = np.ascontiguousarray(x, np.float32)
-        if x.size != self.batch * self.size ** 3 * 2:
-            raise ValueError(f"input must hold {self.batch} x {self.size}^3 x 2 values")
+        if x.size != self.batch * self.size ** 3 * self.in_channels:
+            raise ValueError(f"input must hold {self.batch} x {self.size}^3 x "
+                             f"{self.in_channels} values")
         return x
 
     def _tgt(self, t):
@@ -101,14 +103,41 @@ class InitNet:
                                              C.byref(loss), g.ctypes.data))
         return loss.value, g
 
-    def save(self, path):
-        np.savez_compressed(path, params=self.get_parameters(), size=self.size)
+    def _weight_mask(self):
+        """True at the parameters that are convolution weights (False at the biases)"""
+        from .initnet_layers import layer_table
+        mask = np.zeros(self.nparam, bool)
+        o = 0
+        for cin, cout in layer_table(self.in_channels):
+            mask[o:o + 27 * cin * cout] = True
+            o += 27 * cin * cout + cout
+        return mask
+
+    def save(self, path, bf16_weights=False):
+        """an .npz checkpoint; bf16_weights stores the convolution weights as BF16 -- exactly the
+        operands the kernels use, so inference is unchanged -- at half the size"""
+        p = self.get_parameters()
+        meta = dict(size=self.size, in_channels=self.in_channels)
+        if bf16_weights:
+            m = self._weight_mask()
+            u = p.view(np.uint32).astype(np.uint64)
+            bits = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+            np.savez_compressed(path, weights_bf16=bits[m], biases=p[~m], **meta)
+        else:
+            np.savez_compressed(path, params=p, **meta)
 
     def load(self, path):
         z = np.load(path)
-        if int(z["size"]) != self.size:
-            raise ValueError("checkpoint was trained for another grid size")
-        self.set_parameters(z["params"])
+        if int(z["size"]) != self.size or int(z["in_channels"]) != self.in_channels:
+            raise ValueError("checkpoint was trained for another grid size or input")
+        if "params" in z.files:
+            self.set_parameters(z["params"])
+            return
+        m = self._weight_mask()
+        p = np.empty(self.nparam, np.float32)
+        p[m] = (z["weights_bf16"].astype(np.uint32) << 16).view(np.float32)
+        p[~m] = z["biases"]
+        self.set_parameters(p)
 
 
 # ---- data ---------------------------------------------------------------------------------------
@@ -190,19 +219,65 @@ def make_pairs(seeds, size=SIZE, workers=None):
         return pool.map(_pair_job, jobs, chunksize=max(1, len(jobs) // (4 * n)))
 
 
-def training_set(core, seeds, size=SIZE):
-    """inputs [n, S, S, S, 2] and targets [n, S/4, S/4, S/4, 3]: phantom pairs of this package's
-    generator, targets the plain method's converged displacements"""
+EARLY_EM = 16  # EM iterations before the network, for the EM-seeded input
+
+
+def early_em(core, pair, n=EARLY_EM):
+    """the plain method's first n iterations from the identity: (Registration, displacement)"""
+    from . import phantoms
+    reg = registration(core, pair, None, 0)
+    reg.EM(n, -1e300, 1, 0)
+    fin = reg.get_final_locations_as_numpy_array().astype(np.float64)
+    return reg, fin - phantoms.identity_positions(pair.u.shape)
+
+
+def make_input(pair, early=None):
+    """the network input of a pair: [S, S, S, 2] intensities, or [S, S, S, 5] with the early EM
+    displacement appended (the EM-seeded form)"""
+    x = network_input(pair)
+    if early is None:
+        return x
+    return np.concatenate([x, np.asarray(early, np.float32)], -1)
+
+
+def training_set(core, seeds, size=SIZE, seeded=False):
+    """inputs and targets for the seeds' phantom pairs.  Plain form: input the two intensities,
+    target the plain method's converged displacement (4^3 block means).  EM-seeded form: input
+    also the displacement after EARLY_EM iterations, target the rest of the way (converged minus
+    early)."""
     xs, ts = [], []
     for pair in make_pairs(seeds, size):
-        _, disp, _, _ = refine(core, pair)
-        xs.append(network_input(pair))
-        ts.append(coarse_target(disp))
+        if seeded:
+            reg, early = early_em(core, pair)
+            reg.EM(MAX_EM, CONVERGENCE, 1, 0)  # the same run, on to convergence
+            from . import phantoms
+            fin = reg.get_final_locations_as_numpy_array().astype(np.float64) - \
+                phantoms.identity_positions(pair.u.shape)
+            xs.append(make_input(pair, early))
+            ts.append(coarse_target(fin - early))
+        else:
+            _, disp, _, _ = refine(core, pair)
+            xs.append(make_input(pair))
+            ts.append(coarse_target(disp))
     return np.stack(xs), np.stack(ts)
 
 
-def train(net, xs, ts, steps, lr=1e-3, seed=0, log=None):
-    """Adam on random mini-batches of the training set; returns the loss history"""
+def learned_registration(core, net, pair, precision=3):
+    """registration seeded by the network: (total EM iterations, final displacement, final
+    min-log-posterior per voxel, Registration).  EM-seeded networks (5 input channels) run
+    EARLY_EM plain iterations first, whose count is included."""
+    if net.in_channels == 5:
+        _, early = early_em(core, pair)
+        init = early + predict_displacement(net, pair, early)
+        it, disp, mlp, reg = refine(core, pair, init_displacement=init, precision=precision)
+        return EARLY_EM + it, disp, mlp, reg
+    init = predict_displacement(net, pair)
+    return refine(core, pair, init_displacement=init, precision=precision)
+
+
+def train(net, xs, ts, steps, lr=1e-3, seed=0, log=None, warmup=200):
+    """Adam on random mini-batches of the training set, the learning rate ramped up linearly over
+    the first `warmup` steps and cosine-decayed after; returns the loss history"""
     rng = np.random.default_rng(seed)
     n = len(xs)
     hist = []
@@ -216,16 +291,19 @@ def train(net, xs, ts, steps, lr=1e-3, seed=0, log=None):
                 t = np.flip(t, axis=1 + a)
                 t[..., a] = -t[..., a]
         cur = lr * (0.5 * (1 + np.cos(np.pi * step / max(1, steps))))  # cosine decay
+        if step < warmup:
+            cur *= (step + 1) / warmup
         hist.append(net.train_step(np.ascontiguousarray(x), np.ascontiguousarray(t), cur))
         if log and (step % 100 == 0 or step == steps - 1):
             log(f"step {step}: loss {hist[-1]:.5f}")
     return hist
 
 
-def predict_displacement(net, pair):
+def predict_displacement(net, pair, early=None):
     """the network's displacement for one pair, up-sampled to the full grid"""
-    x = np.zeros((net.batch,) + network_input(pair).shape, np.float32)
-    x[0] = network_input(pair)
+    x1 = make_input(pair, early)
+    x = np.zeros((net.batch,) + x1.shape, np.float32)
+    x[0] = x1
     coarse = net.predict(x)[0]
     return upsample_displacement(coarse, pair.u.shape)
 
@@ -239,15 +317,37 @@ def main():
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--seeded", action="store_true",
+                    help="EM-seeded form: the input includes the displacement after EARLY_EM "
+                         "iterations")
+    ap.add_argument("--evaluate", type=int, default=0,
+                    help="held-out pairs (seeds from 900000) to compare against zero "
+                         "initialisation after training")
     a = ap.parse_args()
     t0 = time.time()
-    xs, ts = training_set(core, range(a.seed, a.seed + a.pairs))
+    xs, ts = training_set(core, range(a.seed, a.seed + a.pairs), seeded=a.seeded)
     print(f"{a.pairs} training pairs in {time.time() - t0:.1f} s", flush=True)
-    net = InitNet(a.batch, SIZE, a.seed)
+    net = InitNet(a.batch, SIZE, a.seed, in_channels=xs.shape[-1])
     t0 = time.time()
-    train(net, xs, ts, a.steps, a.lr, a.seed, log=lambda s: print(s, flush=True))
-    print(f"{a.steps} steps in {time.time() - t0:.1f} s", flush=True)
-    net.save(a.out)
+    hist = train(net, xs, ts, a.steps, a.lr, a.seed, log=lambda s: print(s, flush=True),
+                 warmup=a.warmup)
+    print(f"{a.steps} steps in {time.time() - t0:.1f} s; mean loss of the first / last 200 "
+          f"steps {np.mean(hist[:200]):.5f} / {np.mean(hist[-200:]):.5f}", flush=True)
+    net.save(a.out, bf16_weights=True)
+    if a.evaluate:
+        ev = InitNet(1, SIZE, 0, in_channels=xs.shape[-1])
+        ev.load(a.out)
+        rows = []
+        for pair in make_pairs(range(900000, 900000 + a.evaluate)):
+            it0, _, mlp0, _ = refine(core, pair, precision=0)
+            it1, _, mlp1, _ = learned_registration(core, ev, pair)
+            rows.append((it0, it1, mlp0, mlp1))
+        r = np.array(rows)
+        print("held-out: EM iterations %.1f (zero initialisation, FP32 passes) -> %.1f (learned, "
+              "BF16 passes); final min-log-posterior per voxel %.5f -> %.5f" % tuple(r.mean(0)),
+              flush=True)
+        print("per pair (zero, learned):", r[:, :2].astype(int).tolist(), flush=True)
 
 
 if __name__ == "__main__":

@@ -392,8 +392,9 @@ int binder_registration_set_estep_grid(binder_registration *h, int ctas);
  * A 3D convolutional encoder-decoder (channels 16-32-64-128, 3x3x3 convolutions with leaky ReLU,
  * 2x2x2 average pooling, a skip connection at the 4-voxel level) whose prediction seeds the
  * positions a registration starts from (the reference's hook is the final_locations argument of
- * Registration, FastRegistration.py:443-450).  Input: batch x S^3 voxels x 2 channels (moving and
- * fixed intensities in [0, 1]), FP32, channels last; S a multiple of 8.  Output: the displacement
+ * Registration, FastRegistration.py:443-450).  Input: batch x S^3 voxels x in_channels channels
+ * (moving and fixed intensities in [0, 1], optionally followed by a displacement field), FP32,
+ * channels last; S a multiple of 8.  Output: the displacement
  * on the grid of every 4th voxel, batch x (S/4)^3 x 3, FP32, in voxels.  Every layer runs on
  * hand-written sm_100a kernels: im2col gathers into BF16 operands, a tcgen05 BF16 GEMM with FP32
  * accumulation in TMEM, FP32 master weights and Adam.  Pointers may be host or device memory. */
@@ -401,7 +402,8 @@ int binder_registration_set_estep_grid(binder_registration *h, int ctas);
  * BF16 operands (raw bits, row-major, K contiguous), K a multiple of 64, on the tcgen05 kernel
  * every convolution runs on (FP32 accumulation in TMEM; K split over CTAs above 4096). */
 int binder_gemm_bf16(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K);
-int binder_initnet_create(binder_initnet **out, int batch, int size, uint64_t seed);
+int binder_initnet_create(binder_initnet **out, int batch, int size, int in_channels,
+                          uint64_t seed);
 int binder_initnet_destroy(binder_initnet *h);
 int binder_initnet_parameter_count(const binder_initnet *h, long long *out);
 /* FP32 parameters layer by layer: W [Cout][27 Cin] (tap-major: tap = (dx*3+dy)*3+dz, then Cin),

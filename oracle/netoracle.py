@@ -28,10 +28,15 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def unpack(params):
+def layers(in_channels=2):
+    """the layer table for a network with `in_channels` input channels"""
+    return [(in_channels,) + LAYERS[0][1:]] + LAYERS[1:]
+
+
+def unpack(params, in_channels=2):
     """[(W [Cout, 27 Cin], b [Cout]), ...] from the flat parameter vector"""
     out, o = [], 0
-    for cin, cout, _, _ in LAYERS:
+    for cin, cout, _, _ in layers(in_channels):
         W = np.asarray(params[o:o + 27 * cin * cout], np.float64).reshape(cout, 27 * cin)
         o += 27 * cin * cout
         b = np.asarray(params[o:o + cout], np.float64)
@@ -84,7 +89,7 @@ def forward_backward(params, x, target=None, round=True):
     """(output [B, S/4, S/4, S/4, 3], loss, gradient [n params]) of the network on input x
     [B, S, S, S, 2]; loss and gradient are None without a target"""
     R = bf16 if round else (lambda a: np.asarray(a, np.float64))
-    lay = unpack(params)
+    lay = unpack(params, x.shape[-1])
     cache = []
 
     def conv(i, xin):
