@@ -202,6 +202,16 @@ def refine(core, pair, init_displacement=None, precision=0, max_iter=MAX_EM, th=
     return it, disp, mlp, reg
 
 
+def negative_jacobians(core, reg, shape, correct=False):
+    """negative Jacobian determinants of a registration's field; with correct=True after the
+    topology correction the reference pipeline applies once EM is done (FastRegistration.py:
+    527-546, its defaults e1 = 0.01, e2 = 100, 10 outer and 10 inner iterations), in place"""
+    if correct:
+        reg.correct_topology(0.01, 100.0, 10, 10, (1.0, 1.0, 1.0))
+    pos = reg.get_final_locations_as_numpy_array().astype(np.float64)
+    return int((core.compute_jacobian_determinant_3D(pos, *shape, 1, 1, 1) < 0).sum())
+
+
 def _pair_job(args):
     """one phantom pair (module level, so a spawn pool can run it)"""
     return make_pair(*args)

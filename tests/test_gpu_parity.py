@@ -97,13 +97,21 @@ def test_em_convergence_rule(core, oracle):
     assert 1 <= n < 200 and abs(n - it) <= 1
 
 
-def test_smoothing_matches_reference_golden(core):
+# DCT operand format -> bound on the smoothed field against the reference's output: FP32-level
+# for the TF32 split (about 22 significant bits per operand); the BF16 split (the default) keeps
+# about 16 bits per operand, so its per-element bound is five times wider
+SMOOTHING_BOUNDS = {1: 2e-6, 3: 1e-5}
+
+
+@pytest.mark.parametrize("precision", sorted(SMOOTHING_BOUNDS))
+def test_smoothing_matches_reference_golden(core, precision):
     g = golden("smoothing_ref.npz")
     shape = g["field"].shape[:3]
     t = core.NonLinearTransformation(*g["gamma"], 1, 1, 1, 1, 1, 1, g["D"], *shape, 1,
                                      float(g["sigma"]), 0.0)
+    t.set_precision(precision)
     cost, out = t.smooth_deformation(g["field"])
-    np.testing.assert_allclose(out, g["out"], rtol=0, atol=2e-6)   # FP32 GEMM-DCT
+    np.testing.assert_allclose(out, g["out"], rtol=0, atol=SMOOTHING_BOUNDS[precision])
     assert cost == pytest.approx(float(g["cost"]), rel=1e-5)
 
 

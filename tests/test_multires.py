@@ -124,10 +124,14 @@ def test_next_level_matches_move_resolution(core, oracle, shape, freq):
 
 
 @pytest.mark.gpu
-def test_device_loop_matches_host_loop(core, oracle):
+def test_device_loop_matches_host_loop(core, oracle, monkeypatch):
     """multires.run (device hand-offs) against FastRegistration.run's loop through host arrays
-    and the _core mirror (positions after [4, 2, 1] with topology correction)."""
+    and the _core mirror (positions after [4, 2, 1] with topology correction).  Both loops run
+    their DCT passes in the TF32 split, so what is compared is the hand-off between levels (FP32
+    on the device, FP64 through the host) and not the operand format: the EM trajectories
+    amplify differences at the passes' rounding level, and the BF16 split's is larger."""
     from binder_b200 import multires as mr
+    monkeypatch.setenv("BINDER_B200_PRECISION", "1")
     full = _full((48, 40, 36), seed=2)
     K = full["K"]
     theta = np.full((K, K), 1.0 / K, np.float32)
