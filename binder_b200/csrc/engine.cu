@@ -340,6 +340,9 @@ Registration::Registration(const float *final_locations, const float *voxel_pos,
     // dream locations start at zero: r = 0 - x
     launch_aos_minus_to_soa(nullptr, x_, g, r_, s);
     mstep_.init(nx, ny, nz, s);
+    BINDER_CUDA(cudaStreamCreate(&lk_stream_));
+    BINDER_CUDA(cudaEventCreateWithFlags(&lk_fork_, cudaEventDisableTiming));
+    BINDER_CUDA(cudaEventCreateWithFlags(&lk_join_, cudaEventDisableTiming));
     BINDER_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -347,6 +350,9 @@ Registration::~Registration() {
     // nothing of this object may still run when its buffers go back to the pool
     if (stream_ != own_stream_) cudaStreamSynchronize(stream_);
     cudaStreamSynchronize(own_stream_);
+    if (lk_stream_) cudaStreamSynchronize(lk_stream_), cudaStreamDestroy(lk_stream_);
+    if (lk_fork_) cudaEventDestroy(lk_fork_);
+    if (lk_join_) cudaEventDestroy(lk_join_);
     em_graph_.clear();
     const cudaStream_t s = own_stream_;
     dfree(d_, s); dfree(x_, s); dfree(r_, s); dfree(D_, s); dfree(theta_, s); dfree(hist_, s);
@@ -511,6 +517,7 @@ void Registration::set_ssd_likelihood(int bins, double sigma2, int shift_scale, 
     BINDER_CUDA(cudaStreamSynchronize(s));  // `h` goes out of scope
     lk_ = 1;
     egrid_e_ = estep_grid(false, bins, bins, V_, N_, true);
+    egrid_s_ = estep_grid(true, bins, bins, V_, N_, true);
 }
 
 // The SSD filter likelihood (SSDLikelihoodFilter.cpp): continuous features, EM in log space.
@@ -656,15 +663,21 @@ EStepArgs Registration::estep_args(const int *skip) const {
 void Registration::enqueue_em_iteration(int max_iter, double th, int update, cudaStream_t s) {
     const int grid = estep_grid_override_ > 0 ? estep_grid_override_ : egrid_e_;
     launch_estep(estep_args(&st_->done), false, grid, s);
+    // the likelihood update (one CTA) reads the E-step's histogram or statistics and the M-step
+    // the dream locations: the two run side by side and join before the bookkeeping
+    BINDER_CUDA(cudaEventRecord(lk_fork_, s));
+    BINDER_CUDA(cudaStreamWaitEvent(lk_stream_, lk_fork_, 0));
     if (lk_ == 1)
-        launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, s);
+        launch_ssd_update(theta_, colmax_, hist_, K_, L_, update, ssd_, st_, lk_stream_);
     else if (lk_ == 3)
-        launch_ssdf_update(fst_, fstats_, update, st_, s);
+        launch_ssdf_update(fst_, fstats_, update, st_, lk_stream_);
     else
-        launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, s);
+        launch_theta_update(theta_, hist_, M_ * K_, L_, alpha_, update, st_, lk_stream_);
+    BINDER_CUDA(cudaEventRecord(lk_join_, lk_stream_));
     const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 0, 0, 1, seed_, chain_,
                    rho_[0] * rho_[1] * rho_[2], eta2, &st_->done, s);
+    BINDER_CUDA(cudaStreamWaitEvent(s, lk_join_, 0));
     launch_em_finish(st_, stats_, max_iter, th, nzv_, s);
 }
 
@@ -792,8 +805,6 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     if (sample_posteriors || sample_likelihood_parameters) {
         if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
     }
-    if (lk_ == 1)
-        throw Error(kUnsupported, "the sampler with the SSD likelihood is not built (EM only)");
     if (lk_ == 2 || lk_ == 3)
         throw Error(kUnsupported,
                     "the sampler with a filter (feature) likelihood is not built (EM only)");
@@ -824,9 +835,14 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
                 if (sample_posteriors) {
                     launch_estep(estep_args(&st_->done), true, egrid_s_, stream_);
                 }
-                if (sample_likelihood_parameters)
-                    launch_dirichlet_sample(theta_, hcnt_, K_, L_, alpha_, seed_, chain_, st_,
-                                            stream_);
+                if (sample_likelihood_parameters) {
+                    if (lk_ == 1)  // SSDLikelihood::sample_parameters from the sweep's counts
+                        launch_ssd_sample(theta_, colmax_, hcnt_, K_, L_, ssd_, st_, seed_,
+                                          chain_, stream_);
+                    else
+                        launch_dirichlet_sample(theta_, hcnt_, K_, L_, alpha_, seed_, chain_,
+                                                st_, stream_);
+                }
                 if (sample_transformation_parameters) {
                     mstep_.enqueue(r_, d_, x_, D_, st_, sigma2_, 1, sample_gamma, every, seed_,
                                    chain_, rho_p, eta2, &st_->done, stream_);

@@ -175,6 +175,9 @@ class Registration {
     // own_stream_ owns the buffers (pool allocations and frees); stream_ (own_stream_ unless the
     // caller set one) carries the copies and kernels
     cudaStream_t stream_ = 0, own_stream_ = 0;
+    // the likelihood update of an EM iteration runs on lk_stream_, beside the M-step
+    cudaStream_t lk_stream_ = nullptr;
+    cudaEvent_t lk_fork_ = nullptr, lk_join_ = nullptr;
     uint32_t chain_ = 0;
     // device buffers
     float *d_ = nullptr, *x_ = nullptr, *r_ = nullptr, *D_ = nullptr, *theta_ = nullptr,

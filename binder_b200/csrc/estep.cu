@@ -796,7 +796,7 @@ __global__ void features_to_soa_kernel(const double *in, long n, int C, double *
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
 // for the Gibbs draw and for EM with K > 64.
-template <bool SAMPLE, int DIM>
+template <bool SAMPLE, int DIM, bool LOGT = false>
 __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs args) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     constexpr int R = 4 * Q;  // node rows of 4 packed nodes
@@ -843,6 +843,29 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
         gather_bins<DIM>(a, ix, iy, iz, pk);
         const float *thc = th + a.u[i];  // theta column of this voxel's bin: thc[k * L]
         const int L = a.L;
+        // LOGT (the SSD likelihood, sampling): thc holds log2 likelihoods, the spline weights
+        // enter as log2 (-inf for a zero tap) and every neighbour's weight is exp2 of its term
+        // minus the voxel's largest term (Registration.cpp:331-470)
+        float lx[4], ly[4] = {0.f, 0.f, 0.f, 0.f}, lz[4], lm = 0.0f;
+        if (LOGT) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                lx[t] = log2f(bx[t]);
+                if (DIM == 3) ly[t] = log2f(by[t]);
+                lz[t] = log2f(bz[t]);
+            }
+            lm = -INFINITY;
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const uint32_t word = pk[p * Q + q];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        lm = fmaxf(lm, __fadd_rn(__fadd_rn(__fadd_rn(lx[p], ly[q]), lz[c]),
+                                                 thc[((word >> (8 * c)) & 0xff) * L]));
+                }
+        }
 
         // pass 1: normaliser and the posterior-weighted node offsets
         float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f;
@@ -855,7 +878,10 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
                     const int k = (word >> (8 * c)) & 0xff;
-                    const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
+                    const float w =
+                        LOGT ? exp2f(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(lx[p], ly[q]),
+                                                                   lz[c]), thc[k * L]), -lm))
+                             : __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
                     S = __fadd_rn(S, w);
                     Sx = fmaf((float)(p - 1), w, Sx);
                     if (DIM == 3) Sy = fmaf((float)(q - 1), w, Sy);
@@ -918,12 +944,20 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs arg
             const float bxp = p == 0 ? bx[0] : (p == 1 ? bx[1] : (p == 2 ? bx[2] : bx[3]));
             const float byq = q == 0 ? by[0] : (q == 1 ? by[1] : (q == 2 ? by[2] : by[3]));
             const float bxy = DIM == 3 ? __fmul_rn(bxp, byq) : bxp;
+            float lxy = 0.0f;
+            if (LOGT) {
+                const float lxp = p == 0 ? lx[0] : (p == 1 ? lx[1] : (p == 2 ? lx[2] : lx[3]));
+                const float lyq = q == 0 ? ly[0] : (q == 1 ? ly[1] : (q == 2 ? ly[2] : ly[3]));
+                lxy = __fadd_rn(lxp, lyq);
+            }
             const uint32_t word = gather_word<DIM>(a, a.vpad, ix, iy, iz, p, q);
             int pick = -1, kp = 0;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int k = (word >> (8 * c)) & 0xff;
-                const float w = __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
+                const float w =
+                    LOGT ? exp2f(__fadd_rn(__fadd_rn(__fadd_rn(lxy, lz[c]), thc[k * L]), -lm))
+                         : __fmul_rn(__fmul_rn(bxy, bz[c]), thc[k * L]);
                 cdf = __fadd_rn(cdf, w);
                 if (pick < 0 && cdf >= t) {
                     pick = row * 4 + c;
@@ -1149,6 +1183,7 @@ size_t estep_smem(bool sample, int K, int L, bool logt = false) {
 namespace {
 template <int DIM>
 const void *estep_fn(bool sample, int K, bool logt) {
+    if (logt && sample) return (const void *)estep_kernel<true, DIM, true>;
     if (logt) return (const void *)estep_em_fast_kernel<kFastThreads, DIM, true>;
     return sample ? (const void *)estep_kernel<true, DIM>
                   : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads, DIM, false>
@@ -1184,6 +1219,8 @@ void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cu
         launch_ssdf_dim<DIM>(a, grid, smem, s);
     else if (a.filter)
         count_launch(), estep_filter_kernel<DIM><<<grid, kEThreads, smem, s>>>(a);
+    else if (a.logt && sample)
+        count_launch(), estep_kernel<true, DIM, true><<<grid, kEThreads, smem, s>>>(a);
     else if (a.logt)
         count_launch(), estep_em_fast_kernel<kFastThreads, DIM, true>
                             <<<grid, kFastThreads, smem, s>>>(a);
@@ -1199,14 +1236,14 @@ void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cu
 
 int estep_grid(bool sample, int K, int L, long V, int dim, bool logt) {
     BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
-    BINDER_CHECK(!logt || (!sample && K <= kSmallK && K <= kLogMaxBins),
-                 "the log-space E-step supports EM with at most 64 bins");
+    BINDER_CHECK(!logt || (K <= kSmallK && K <= kLogMaxBins),
+                 "the log-space E-step supports at most 64 bins");
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t smem = estep_smem(sample, K, L, logt);
     const void *fn = dim == 3 ? estep_fn<3>(sample, K, logt) : estep_fn<2>(sample, K, logt);
-    const int tpb = (logt || (!sample && K <= kSmallK)) ? kFastThreads : kEThreads;
+    const int tpb = (!sample && (logt || K <= kSmallK)) ? kFastThreads : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // all of the unified L1 / shared array as shared memory, so the CTAs the occupancy query
     // counts are the CTAs that become resident (the default carveout may be smaller)
@@ -1283,8 +1320,8 @@ void launch_features_to_soa(const double *in, long n, int C, double *out, cudaSt
 }
 
 void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, int chains) {
-    BINDER_CHECK(!args.logt || (!sample && args.K <= kSmallK && args.colmax),
-                 "the log-space E-step runs EM only, with at most 64 bins");
+    BINDER_CHECK(!args.logt || (args.K <= kSmallK && (sample || args.colmax)),
+                 "the log-space E-step supports at most 64 bins");
     BINDER_CHECK(!args.filter || (!sample && !args.logt && args.M >= 1 &&
                                   args.M <= kMaxChannels &&
                                   (long)args.M * args.K * args.L <= kFilterMaxCells),
@@ -1308,8 +1345,8 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
     a.hscale = (float)std::ldexp(1.0, e);
     a.hinv = (float)std::ldexp(1.0, -e);
     BINDER_CHECK(a.dim == 2 || a.dim == 3, "dimension must be 2 or 3");
-    BINDER_CHECK(chains >= 1 && chains <= 65535 && (chains == 1 || sample),
-                 "a batch of chains runs the sampling E-step only");
+    BINDER_CHECK(chains >= 1 && chains <= 65535 && (chains == 1 || (sample && !a.logt)),
+                 "a batch of chains runs the sampling E-step of the MI likelihood only");
     if (chains > 1) {
         // the single-chain grid shared out over the chains (every CTA still loops over voxels)
         const int gx = (grid + chains - 1) / chains;
@@ -1425,12 +1462,113 @@ __global__ void ssd_update_kernel(float *table, float *colmax, float *hist, int 
         for (int q = threadIdx.x; q < K * L; q += blockDim.x) hist[q] = 0.0f;
     }
 }
+
+// SSDLikelihood::sample_parameters (:284-302) with update_shift_and_scale / update_sigma run with
+// sample = 1 (:167-285), from the sweep's counts hcnt[k][l] (the drawn node's bin k at voxel bin
+// l; bin 0 also holds the nodes outside the grid): shiftScale 0: sigmaSq = 1 / g with g ~
+// Gamma(shape den / 2, scale 2 den / num), the reference's parameterisation as written;
+// shiftScale 1: (shift, scale) = A^-1 b + chol(A^-1) z with z two standard normals, then sigmaSq
+// the same way from the drawn shift and scale.  Philox ctr {0, sweep, 6, chain} gives z by
+// Box-Muller on words 0 and 1; the gamma uses tag 7.  Then the next sweep's log2 table, and the
+// counts cleared.  One CTA.
+__global__ void ssd_sample_kernel(float *table, float *colmax, unsigned *hcnt, int K, int L,
+                                  SsdState *ps, DevState *st, uint64_t seed, uint32_t chain) {
+    if (st->done) return;
+    __shared__ double G[kLogMaxBins], S1[kLogMaxBins], S2[kLogMaxBins], D2[kLogMaxBins];
+    __shared__ SsdState p;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) p = *ps;
+    for (int k = wid; k < K; k += nw) {
+        double g = 0.0, s1 = 0.0, s2 = 0.0, d2 = 0.0;
+        for (int l = lane; l < L; l += 32) {
+            const double h = (double)hcnt[k * L + l], df = (double)l - (double)k;
+            g += h;
+            s1 += h * (double)l;
+            s2 += h * (double)l * (double)l;
+            d2 += h * df * df;
+        }
+        g = warp_sum(g);
+        s1 = warp_sum(s1);
+        s2 = warp_sum(s2);
+        d2 = warp_sum(d2);
+        if (lane == 0) {
+            G[k] = g;
+            S1[k] = s1;
+            S2[k] = s2;
+            D2[k] = d2;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t sweep = (uint32_t)st->sweep;
+        double num = 0.0, den = 0.0;
+        if (!p.shift_scale) {
+            for (int k = 0; k < K; ++k) {
+                num += D2[k];
+                den += G[k];
+            }
+        } else {
+            double A00 = 0.0, A01 = 0.0, A11 = 0.0, b0 = 0.0, b1 = 0.0;
+            for (int k = 0; k < K; ++k) {
+                A00 += G[k];
+                A01 += G[k] * (double)k;
+                A11 += G[k] * (double)k * (double)k;
+                b0 += S1[k];
+                b1 += S1[k] * (double)k;
+            }
+            const double det = A00 * A11 - A01 * A01;
+            if (det > 0.0 && isfinite(det)) {
+                const double x0 = (b0 * A11 - A01 * b1) / det, x1 = (A00 * b1 - A01 * b0) / det;
+                const double c00 = A11 / det, c01 = -A01 / det, c11 = A00 / det;
+                const double l00 = sqrt(c00), l10 = c01 / l00, l11 = sqrt(c11 - l10 * l10);
+                const u32x4 r = philox_draw(seed, 0u, sweep, 6u, chain);
+                const double rad = sqrt(-2.0 * log(u01_d32(r.x))), t = 2.0 * u01_d32(r.y);
+                const double z0 = rad * cospi(t), z1 = rad * sinpi(t);
+                p.shift = x0 + l00 * z0;
+                p.scale = x1 + l10 * z0 + l11 * z1;
+            }
+            for (int k = 0; k < K; ++k) {
+                const double t1 = p.shift + p.scale * (double)k;
+                num += S2[k] + -2.0 * S1[k] * t1 + G[k] * (t1 * t1);
+                den += G[k];
+            }
+        }
+        num += p.alpha0 * p.beta0;
+        den += p.alpha0;
+        bool capped = false;
+        const double g = gamma_mt(den * 0.5, seed, 0u, sweep, 7u, chain, &capped) *
+                         (2.0 * den / num);
+        p.sigma2 = 1.0 / g;
+        if (capped) atomicOr(&st->flags, (unsigned)kFlagGammaCapped);
+        if (!isfinite(p.sigma2) || !(p.sigma2 > 0.0)) atomicOr(&st->flags, (unsigned)kFlagNonFinite);
+        *ps = p;
+        const double a = p.alpha0, b = p.alpha0 * p.beta0, x = p.sigma2;
+        st->lp_lik = -(a * log(b) - lgamma(a) + (-a - 1.0) * log(x) - b / x);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        double m = -INFINITY;
+        for (int k = 0; k < K; ++k) m = fmax(m, ssd_loglik(k, l, p));
+        colmax[l] = (float)m;
+        for (int k = 0; k < K; ++k)
+            table[k * L + l] = (float)((ssd_loglik(k, l, p) - m) * 1.4426950408889634);
+    }
+    for (int q = threadIdx.x; q < K * L; q += blockDim.x) hcnt[q] = 0u;
+}
 }  // namespace
 
 void launch_ssd_update(float *table, float *colmax, float *hist, int K, int L, int update,
                        SsdState *p, DevState *st, cudaStream_t s) {
     BINDER_CHECK(K >= 1 && K <= kLogMaxBins && L >= 1, "SSD bins must be in [1, 64]");
     count_launch(), ssd_update_kernel<<<1, 256, 0, s>>>(table, colmax, hist, K, L, update, p, st);
+    BINDER_CUDA(cudaGetLastError());
+}
+
+void launch_ssd_sample(float *table, float *colmax, unsigned *hcnt, int K, int L, SsdState *p,
+                       DevState *st, uint64_t seed, uint32_t chain, cudaStream_t s) {
+    BINDER_CHECK(K >= 1 && K <= kLogMaxBins && L >= 1, "SSD bins must be in [1, 64]");
+    count_launch(), ssd_sample_kernel<<<1, 256, 0, s>>>(table, colmax, hcnt, K, L, p, st, seed,
+                                                        chain);
     BINDER_CUDA(cudaGetLastError());
 }
 

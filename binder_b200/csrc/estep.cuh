@@ -109,6 +109,12 @@ struct SsdState {
 void launch_ssd_update(float *table, float *colmax, float *hist, int K, int L, int update,
                        SsdState *p, DevState *st, cudaStream_t s);
 
+// the sampler's draw of the SSD likelihood's parameters (SSDLikelihood.cpp:284-302) from the
+// sweep's counts hcnt [K][L] (Philox ctr {0, st->sweep, 6 / 7, chain}), the log2 table and its
+// column maxima rebuilt, the counts cleared; the prior cost into st->lp_lik.  One CTA.
+void launch_ssd_sample(float *table, float *colmax, unsigned *hcnt, int K, int L, SsdState *p,
+                       DevState *st, uint64_t seed, uint32_t chain, cudaStream_t s);
+
 // theta <- (hist + alpha - 1)/rowsum (if update), Dirichlet prior cost into st->lp_lik,
 // hist zeroed for the next iteration.  One CTA.
 void launch_theta_update(float *theta, float *hist, int K, int L, double alpha, int update,

@@ -86,7 +86,8 @@ int binder_registration_set_mi_likelihood_filter(binder_registration *h, double 
 /* setSSDLikelihood(bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
  *                  binned_voxels, alpha_0, beta_0)                  cpu/bindings.cpp:120-152
  * The CPU backend's SSD likelihood (SSDLikelihood.cpp): the bins are the intensities, bins <= 64;
- * scale_shift 0 fits sigma^2 only, 1 also shift and scale.  EM only (the sampler rejects it).
+ * scale_shift 0 fits sigma^2 only, 1 also shift and scale.  EM and the sampler (its draws of
+ * sigma^2, shift and scale: SSDLikelihood.cpp:167-302 with sample = 1; not in sampler_chains).
  * get_likelihood_parameters then returns (scale, shift). */
 int binder_registration_set_ssd_likelihood(binder_registration *h, int bins, int threads,
                                            double sigma_sq, int scale_shift, double scale,
@@ -132,7 +133,9 @@ int binder_registration_em(binder_registration *h, int max_iterations, double co
 /* sampler(seed, N_b, N_s, sample_gamma, sample_gamma_every, sample_posteriors,
  *         sample_likelihood_parameters, sample_transformation_parameters) -> (mean, cov)
  *                                                               gpu/bindings.cpp:105-131
- * mean_out [V*3] and cov_out [V*3*3] (M2 / (N_s - 1)) in FP64 (FP64 Welford accumulators). */
+ * mean_out [V*3] and cov_out [V*3*3] (M2 / (N_s - 1)) in FP64 (FP64 Welford accumulators).
+ * Likelihoods: MI and SSD (cpu/Registration.cpp:515-642 drives both); the filter likelihoods
+ * are rejected. */
 int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, int N_s,
                                 int sample_gamma, int sample_gamma_every, int sample_posteriors,
                                 int sample_likelihood_parameters,

@@ -724,6 +724,68 @@ double orc_ssd_update(const double *hist, int K, int L, orc_ssd *p, int update) 
     return -(a * log(b) - lgamma(a) + (-a - 1.0) * log(x) - b / x);
 }
 
+/* SSDLikelihood::sample_parameters (:284-302), update_shift_and_scale and update_sigma with
+ * sample = 1 (:167-285), from the sweep's counts hist[k][l] (the drawn node's bin k at voxel bin
+ * l).  shiftScale 0: sigmaSq = 1 / g with g ~ Gamma(shape den / 2, scale 2 den / num), the
+ * reference's parameterisation as written (num = sum h (l - k)^2 + alpha_0 beta_0, den = sum h +
+ * alpha_0).  shiftScale 1: (shift, scale) = A^-1 b + chol(A^-1) z, z two standard normals, then
+ * sigmaSq the same way with the drawn shift and scale.  Random numbers: Philox ctr {0, sweep, 6,
+ * chain} gives z by Box-Muller on words 0 and 1 (cos, sin); the gamma uses tag 7, index 0.
+ * Returns 1 when the gamma draw hit its attempt cap. */
+int orc_ssd_sample(const double *hist, int K, int L, orc_ssd *p, uint64_t seed, uint32_t sweep,
+                   uint32_t chain) {
+    double G[256], S1[256], S2[256];
+    for (int k = 0; k < K; ++k) {
+        G[k] = S1[k] = S2[k] = 0.0;
+        for (int l = 0; l < L; ++l) {
+            const double h = hist[(long)k * L + l];
+            G[k] += h;
+            S1[k] += h * (double)l;
+            S2[k] += h * (double)l * (double)l;
+        }
+    }
+    double num = 0.0, den = 0.0;
+    if (!p->shift_scale) {
+        for (int k = 0; k < K; ++k)
+            for (int l = 0; l < L; ++l) {
+                const double df = (double)l - (double)k;
+                num += hist[(long)k * L + l] * df * df;
+            }
+        for (int k = 0; k < K; ++k) den += G[k];
+    } else {
+        double A00 = 0, A01 = 0, A11 = 0, b0 = 0, b1 = 0;
+        for (int k = 0; k < K; ++k) {
+            A00 += G[k];
+            A01 += G[k] * (double)k;
+            A11 += G[k] * (double)k * (double)k;
+            b0 += S1[k];
+            b1 += S1[k] * (double)k;
+        }
+        const double det = A00 * A11 - A01 * A01;
+        const double x0 = (b0 * A11 - A01 * b1) / det, x1 = (A00 * b1 - A01 * b0) / det;
+        const double c00 = A11 / det, c01 = -A01 / det, c11 = A00 / det;
+        const double l00 = sqrt(c00), l10 = c01 / l00, l11 = sqrt(c11 - l10 * l10);
+        uint32_t r[4];
+        philox_draw(seed, 0u, sweep, 6u, chain, r);
+        const double rad = sqrt(-2.0 * log(u01_d32(r[0]))), ang = 2.0 * PI_D * u01_d32(r[1]);
+        const double z0 = rad * cos(ang), z1 = rad * sin(ang);
+        p->shift = x0 + l00 * z0;
+        p->scale = x1 + l10 * z0 + l11 * z1;
+        for (int k = 0; k < K; ++k) {
+            const double t1 = p->shift + p->scale * (double)k;
+            num += S2[k] + -2.0 * S1[k] * t1 + G[k] * (t1 * t1);
+            den += G[k];
+        }
+    }
+    num += p->alpha0 * p->beta0;
+    den += p->alpha0;
+    int capped = 0;
+    const double g = orc_gamma_sample(den * 0.5, seed, 0u, sweep, 7u, chain, &capped) *
+                     (2.0 * den / num);
+    p->sigma2 = 1.0 / g;
+    return capped;
+}
+
 /* Registration.cpp:122-217 with the SSD likelihood */
 int orc_ssd_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
                orc_ssd *p, const double *D, const double gamma[3], double sigma, int nx, int ny,

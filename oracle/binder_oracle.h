@@ -116,6 +116,10 @@ double orc_ssd_estep(const double *d, const int *u, const int *v, const orc_ssd 
                      double *hist);
 /* update_parameters (:143-285) from the joint histogram, then compute_cost (:314-326) */
 double orc_ssd_update(const double *hist, int K, int L, orc_ssd *p, int update);
+/* sample_parameters (:284-302) from the sweep's counts, Philox-driven; 1 if the gamma draw hit
+ * its attempt cap */
+int orc_ssd_sample(const double *hist, int K, int L, orc_ssd *p, uint64_t seed, uint32_t sweep,
+                   uint32_t chain);
 int orc_ssd_em(double *final_locations, const double *voxel_pos, const int *u, const int *v,
                orc_ssd *p, const double *D, const double gamma[3], double sigma, int nx, int ny,
                int nz, int nxn, int nyn, int nzn, int K, int L, double non_zero_voxels,

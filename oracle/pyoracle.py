@@ -44,6 +44,8 @@ def _load_oracle():
     lib.orc_ssd_estep.restype = d
     lib.orc_ssd_update.argtypes = [_dp, i, i, C.c_void_p, i]
     lib.orc_ssd_update.restype = d
+    lib.orc_ssd_sample.argtypes = [_dp, i, i, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32]
+    lib.orc_ssd_sample.restype = i
     lib.orc_ssd_em.argtypes = [_dp, _dp, _ip, _ip, C.c_void_p, _dp, _dp, d] + [i] * 8 + \
         [d, i, d, i, C.c_void_p]
     lib.orc_ssd_em.restype = i
@@ -149,6 +151,9 @@ def ref_lib():
     r.ref_sampler.argtypes = [_dp, _dp, i, i, i, _dp, _dp, d, _dp, i, i, _ip, _ip] + \
         [i] * 9 + [_dp, _dp]
     r.ref_sampler.restype = d
+    r.ref_sampler_ssd.argtypes = [_dp, _dp, i, i, i, _dp, _dp, i, _dp, _ip, _ip] + \
+        [i] * 9 + [_dp, _dp, _dp]
+    r.ref_sampler_ssd.restype = d
     r.ref_em_filter.argtypes = [_dp, _dp] + [i] * 7 + [d, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
                                                        _dp, _dp, _dp, _dp, i, d, d, i, i, d, i,
                                                        _dp, _dp]
@@ -405,6 +410,13 @@ def ssd_update(hist, K, L, params, update=True):
     return lib().orc_ssd_update(_c64(hist).ravel(), K, L, C.addressof(params), int(update))
 
 
+def ssd_sample(hist, K, L, params, seed, sweep, chain=0):
+    """the sampler's parameter draw from the sweep's counts (params updated in place); returns
+    1 if the gamma draw hit its attempt cap"""
+    return lib().orc_ssd_sample(_c64(hist).ravel(), K, L, C.addressof(params), int(seed),
+                                int(sweep), int(chain))
+
+
 def ssd_em(final_locations, voxel_pos, u, v, params, D, gamma, sigma, vshape, nshape, K, L,
            non_zero_voxels, max_iter, convergence_th, update=True):
     """Full EM with the SSD likelihood. Returns (iterations, final[V*N], stats[iters, 4]);
@@ -562,6 +574,23 @@ def ref_sampler(R, final_locations, voxel_pos, D, gamma, shape, nodes, voxels, a
                         int(seed), int(N_b), int(N_s), int(sample_gamma), int(every),
                         int(posteriors), int(lik), int(transf), int(threads), mean, cov)
     return mean, cov, sec
+
+
+def ref_sampler_ssd(R, final_locations, voxel_pos, D, gamma, shape, nodes, voxels, bins, ssd,
+                    seed, N_b, N_s, sample_gamma=1, every=1, posteriors=1, lik=1, transf=1,
+                    threads=1):
+    """The reference's Registration::sampler with the SSD likelihood, ssd = (sigmaSq, shiftScale,
+    scale, shift, alpha_0, beta_0).  Returns (mean [V*3], cov [V*9], (scale, shift), seconds)."""
+    nx, ny, nz = shape
+    V = nx * ny * nz
+    mean, cov, par = np.zeros(V * 3), np.zeros(V * 9), np.zeros(2)
+    sec = R.ref_sampler_ssd(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz,
+                            _c64(np.asarray(gamma, np.float64)), _c64(D).ravel(), int(bins),
+                            _c64(np.asarray(ssd, np.float64)), _c32i(nodes).ravel(),
+                            _c32i(voxels).ravel(), int(seed), int(N_b), int(N_s),
+                            int(sample_gamma), int(every), int(posteriors), int(lik), int(transf),
+                            int(threads), mean, cov, par)
+    return mean, cov, (par[0], par[1]), sec
 
 
 def ref_em_filter(R, final_locations, voxel_pos, D, gamma, vshape, max_iter, mi=None, ssd=None,

@@ -255,6 +255,35 @@ double ref_sampler(const double *final_locations, const double *voxel_pos, int n
     return sec;
 }
 
+// Registration::sampler with the SSD likelihood (setSSDLikelihood(bins, threads, sigmaSq,
+// shiftScale, scale, shift, nodes, voxels, alpha_0, beta_0), ssd = {sigmaSq, shiftScale, scale,
+// shift, alpha_0, beta_0}); mean_out / cov_out as ref_sampler; params_out = {scale, shift} after
+// the last sweep (get_likelihood_parameters); returns the wall seconds of the sampler call.
+double ref_sampler_ssd(const double *final_locations, const double *voxel_pos, int nx, int ny,
+                       int nz, const double gamma[3], const double *D, int bins,
+                       const double *ssd, const int *nodes, const int *voxels, int seed, int N_b,
+                       int N_s, int sample_gamma, int every, int posteriors, int lik_params,
+                       int transf_params, int threads, double *mean_out, double *cov_out,
+                       double *params_out) {
+    Registration r(final_locations, threads, voxel_pos, voxel_pos, nx, ny, nz, nx, ny, nz, 3,
+                   (double)nx * ny * nz);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], 1, 1, 1, 1, 1, 1, D);
+    r.setSSDLikelihood(bins, threads, ssd[0], (int)ssd[1], ssd[2], ssd[3], nodes, voxels, ssd[4],
+                       ssd[5]);
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto res = r.sampler(seed, N_b, N_s, sample_gamma, every, posteriors, lik_params,
+                               transf_params);
+    const double sec =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (mean_out) std::memcpy(mean_out, res.first.data(), sizeof(double) * res.first.size());
+    if (cov_out) std::memcpy(cov_out, res.second.data(), sizeof(double) * res.second.size());
+    if (params_out) {
+        const auto p = r.get_likelihood_parameters();
+        std::memcpy(params_out, p.data(), sizeof(double) * p.size());
+    }
+    return sec;
+}
+
 // the same, the wall seconds alone
 double ref_sampler_seconds(const double *final_locations, const double *voxel_pos, int nx, int ny,
                            int nz, const double gamma[3], const double *D, double alpha,

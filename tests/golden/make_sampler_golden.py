@@ -9,7 +9,8 @@ kernel from the same start has the same expected chain mean and covariance whate
 numbers, so the difference of the two across-chain means divided by its standard error is a
 z-score per voxel (tests/test_oracle.py and tests/test_gpu_sampler_reference.py).
 
-Run from the repository root:  python tests/golden/make_sampler_golden.py
+Run from the repository root:  python tests/golden/make_sampler_golden.py        (MI)
+                               python tests/golden/make_sampler_golden.py ssd    (SSD)
 """
 from __future__ import annotations
 
@@ -79,5 +80,53 @@ def main():
     print("sampler_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
 
 
+# the SSD likelihood's case: the same positions, prior and field as case(), both images in 16
+# intensity bins (the SSD likelihood compares bin values), (sigmaSq, shiftScale, scale, shift,
+# alpha_0, beta_0) = (4, 1, 1, 0, 1, 1) (run_BINDER's alpha_0 = beta_0 = 1)
+SSD_BINS = 16
+SSD_PARAMS = (4.0, 1, 1.0, 0.0, 1.0, 1.0)
+
+
+def case_ssd():
+    c = case()
+    pair = phantoms.make_pair(SHAPE, 7, bins=SSD_BINS, n_objects=10, axes=(2.0, 6.0), rms=1.0,
+                              spacing=3.0)
+    v, _ = bin_signal_robust(pair.moving, SSD_BINS)
+    c.update(u=pair.u.astype(np.int32), v=v.astype(np.int32))
+    return c
+
+
+def main_ssd():
+    """sampler_ssd_ref.npz: the reference's sampler with the SSD likelihood (SSDLikelihood.cpp:
+    147-300), 32 chains from case_ssd(), every switch on; also each chain's final (scale, shift)"""
+    R = pyoracle.ref_lib()
+    assert R is not None, "oracle/_ref/libbinder_ref.so is needed (make -C oracle)"
+    c = case_ssd()
+    V = int(np.prod(SHAPE))
+    means, covs, pars = [], [], []
+    saved = os.dup(1)
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    try:
+        for ch in range(CHAINS):
+            m, cv, par, _ = pyoracle.ref_sampler_ssd(R, c["d0"], c["grid"], c["D"], c["gamma"],
+                                                     SHAPE, c["v"], c["u"], SSD_BINS, SSD_PARAMS,
+                                                     SEED0 + ch, N_B, N_S)
+            means.append(m.reshape(V, 3))
+            covs.append(cv.reshape(V, 9)[:, UPPER])
+            pars.append(par)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    mm, mv, cm, cvv = chain_stats(means, covs)
+    pars = np.asarray(pars)
+    np.savez_compressed(os.path.join(HERE, "sampler_ssd_ref.npz"), shape=np.array(SHAPE),
+                        bins=SSD_BINS, ssd=np.array(SSD_PARAMS), chains=CHAINS, N_b=N_B, N_s=N_S,
+                        d0=c["d0"], u=c["u"], v=c["v"], D=c["D"], gamma=c["gamma"],
+                        mean_mean=mm, mean_var=mv, cov_mean=cm, cov_var=cvv,
+                        params_mean=pars.mean(0), params_var=pars.var(0, ddof=1))
+    print("sampler_ssd_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
+
+
 if __name__ == "__main__":
-    main()
+    # no argument: the MI fixture; "ssd": the SSD likelihood's
+    main_ssd() if sys.argv[1:] == ["ssd"] else main()

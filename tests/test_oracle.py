@@ -351,3 +351,58 @@ def test_sampler_parity_check_has_power(oracle):
     g = fixture()
     zm, zc = zscores(g, *_oracle_chains(oracle, g, 3.0 * g["gamma"], chains=8))
     assert not agrees(zm) or not agrees(zc), (summary(zm), summary(zc))
+
+
+def _ssd_counts(K=16, L=16, seed=5):
+    """a joint count histogram with a linear bin relation l ~ 0.9 k + 1 plus noise"""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(0, K, 4000)
+    l = np.clip(np.rint(0.9 * k + 1 + rng.normal(0, 1.2, k.size)), 0, L - 1).astype(int)
+    h = np.zeros((K, L))
+    np.add.at(h, (k, l), 1.0)
+    return h
+
+
+@pytest.mark.parametrize("shift_scale", [0, 1])
+def test_ssd_sample_distribution(oracle, shift_scale):
+    """The SSD likelihood's parameter draw (SSDLikelihood.cpp:167-302 with sample = 1), restated
+    with Philox: over 4000 sweeps, (shift, scale) has the mean A^-1 b and covariance A^-1 of the
+    reference's bivariate normal, and 1 / sigmaSq the mean den^2 / num of its gamma draw
+    (shape den / 2, scale 2 den / num, the reference's parameterisation); with shiftScale 1 the
+    num of each draw depends on the drawn shift and scale, so there the gamma is checked through
+    its shape: the coefficient of variation of g * num / den^2 is sqrt(2 / den)."""
+    K = L = 16
+    h = _ssd_counts(K, L)
+    n = 4000
+    draws = []
+    for sweep in range(n):
+        p = oracle.SSDParams(shift_scale, 4.0, 0.0, 1.0, 1.0, 1.0)
+        assert oracle.ssd_sample(h, K, L, p, 77, sweep) == 0
+        draws.append((p.shift, p.scale, p.sigma2))
+    d = np.array(draws)
+    kk = np.arange(K, dtype=float)
+    ll = np.arange(L, dtype=float)
+    G = h.sum(1)
+    S1 = h @ ll
+    S2 = h @ (ll * ll)
+    den = G.sum() + 1.0
+    if shift_scale == 0:
+        num = (h * (ll[None, :] - kk[:, None]) ** 2).sum() + 1.0
+        g = 1.0 / d[:, 2]
+        want = den * den / num
+        assert abs(g.mean() - want) < 4 * want * np.sqrt(2.0 / den) / np.sqrt(n)
+        assert np.all(d[:, 0] == 0.0) and np.all(d[:, 1] == 1.0)
+        return
+    A = np.array([[G.sum(), G @ kk], [G @ kk, G @ (kk * kk)]])
+    b = np.array([S1.sum(), S1 @ kk])
+    x = np.linalg.solve(A, b)
+    cov = np.linalg.inv(A)
+    sd = np.sqrt(np.diag(cov))
+    assert np.all(np.abs(d[:, :2].mean(0) - x) < 4 * sd / np.sqrt(n))
+    emp = np.cov(d[:, :2].T)
+    np.testing.assert_allclose(emp, cov, rtol=0.12)
+    num = np.array([S2.sum() - 2 * (S1 @ (s + c * kk)) + G @ (s + c * kk) ** 2 + 1.0
+                    for s, c, _ in d])
+    ratio = (1.0 / d[:, 2]) * num / (den * den)
+    assert abs(ratio.mean() - 1.0) < 4 * np.sqrt(2.0 / den) / np.sqrt(n)
+    assert ratio.std() == pytest.approx(np.sqrt(2.0 / den), rel=0.1)
