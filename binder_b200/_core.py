@@ -122,7 +122,7 @@ class Registration:
         """``setMILikelihoodFilter`` of the CPU module (cpu/bindings.cpp:90-115): M channels,
         theta [M][K][L]; channel m of voxel (node) i is read at [i + m] as MILikelihoodFilter.cpp
         reads it, so the bin arrays need at least V + M - 1 (Vn + M - 1) entries (the usual
-        [..., M] arrays have more).  EM only."""
+        [..., M] arrays have more).  EM and the sampler (M * K * L up to about 22000 there)."""
         K, L, M = int(K), int(L), int(M)
         Vn = int(np.prod(self._nshape))
         nodes = _i32(binned_nodes)

@@ -391,7 +391,8 @@ void Registration::set_mi_filter_likelihood(double alpha, const float *theta, in
     load_bins(alpha, theta, K, L, M, binned_nodes, binned_voxels);
     lk_ = 2;
     egrid_e_ = estep_filter_grid(K, L, M, V_, N_);
-    egrid_s_ = 0;
+    // the sampler's draw keeps a running-sum table per thread next to theta and the counts
+    egrid_s_ = filter_sampling_fits(K, L, M) ? estep_filter_grid(K, L, M, V_, N_, true) : 0;
     have_mi_ = true;
 }
 
@@ -805,9 +806,13 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     if (sample_posteriors || sample_likelihood_parameters) {
         if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
     }
-    if (lk_ == 2 || lk_ == 3)
+    if (lk_ == 3)
         throw Error(kUnsupported,
-                    "the sampler with a filter (feature) likelihood is not built (EM only)");
+                    "the sampler with the SSD filter (feature) likelihood is not built (EM only)");
+    if (lk_ == 2 && sample_posteriors && egrid_s_ == 0)
+        throw Error(kUnsupported,
+                    "the sampler with the MI filter likelihood needs M * K * L small enough for "
+                    "its theta, counts and draw table in shared memory (about 22000 cells)");
     if (!have_tr_) throw Error(kNotReady, "setNonLinearTransformation has not been called");
     BINDER_CHECK(N_b >= 0 && N_s >= 0, "N_b and N_s must be non-negative");
     BINDER_CHECK(sample_gamma_every >= 1 || !sample_gamma, "sample_gamma_every must be >= 1");
@@ -839,8 +844,8 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
                     if (lk_ == 1)  // SSDLikelihood::sample_parameters from the sweep's counts
                         launch_ssd_sample(theta_, colmax_, hcnt_, K_, L_, ssd_, st_, seed_,
                                           chain_, stream_);
-                    else
-                        launch_dirichlet_sample(theta_, hcnt_, K_, L_, alpha_, seed_, chain_,
+                    else  // MI: K rows; MI filter: M * K rows (MILikelihoodFilter.cpp:152-175)
+                        launch_dirichlet_sample(theta_, hcnt_, M_ * K_, L_, alpha_, seed_, chain_,
                                                 st_, stream_);
                 }
                 if (sample_transformation_parameters) {

@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
 // channel's histogram.  theta [M][L][KP] (transposed per channel) and the histograms [M][K][LP]
 // live in shared memory; the second pass recomputes the weights and adds p = w / S with one
 // shared atomic per channel and neighbour.
-template <int DIM>
+template <int DIM, bool SAMPLE = false>
 __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepArgs a) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     if (a.skip && *a.skip) return;
@@ -428,14 +428,18 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepA
     const int KP = theta_pitch(K), LP = theta_pitch(L);
     const int KL = K * L;
     float *thT = sm;                        // [M][L][KP]
-    float *hs = sm + (size_t)M * L * KP;    // [M][K][LP]
+    float *hs = sm + (size_t)M * L * KP;    // [M][K][LP] EM histogram
+    unsigned *hc = reinterpret_cast<unsigned *>(hs);  // sampling: counts
+    // sampling: the running sum at the end of node row r, cps[r * kEThreads]
+    float *cps = hs + (size_t)M * K * LP + threadIdx.x;
     for (int q = threadIdx.x; q < M * KL; q += blockDim.x) {
         const int m = q / KL, r = q - m * KL, k = r / L, l = r - k * L;
         thT[(m * L + l) * KP + k] = a.theta[q];
-        hs[(m * K + k) * LP + l] = 0.0f;
+        if (SAMPLE) hc[(m * K + k) * LP + l] = 0u; else hs[(m * K + k) * LP + l] = 0.0f;
     }
     __syncthreads();
 
+    const uint32_t sweep = SAMPLE ? (uint32_t)a.st->sweep : 0u;
     double mll = 0.0;
     unsigned deg = 0;
     const unsigned V = (unsigned)a.V, nz = (unsigned)a.nz, ny = (unsigned)a.ny;
@@ -470,6 +474,13 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepA
 #pragma unroll
                     for (int c = 0; c < 4; ++c) t[c] *= th[(w >> (8 * c)) & 0xff];
                 }
+                if (SAMPLE) {
+                    // node by node, so the draw below can re-add one row in the same order
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) S = __fadd_rn(S, t[c]);
+                    cps[(p * Q + q) * kEThreads] = S;
+                    continue;
+                }
                 const float s4 = (t[0] + t[1]) + (t[2] + t[3]);
                 S += s4;
                 Sx += (float)(p - 1) * s4;
@@ -479,6 +490,54 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepA
         if (!(S > 0.0f)) {
             vp.store_r(a, i, V, fx, fy, fz);
             ++deg;
+            continue;
+        }
+        if (SAMPLE) {
+            // categorical draw of one neighbour (Registration.cpp:219-330 with sample): the first
+            // whose running sum reaches u * S; every channel counts the drawn node's bin
+            // (MILikelihoodFilter.cpp:102-115 with posterior 1)
+            const u32x4 rr = philox_draw(a.seed, i, sweep, 1u, a.chain);
+            const float tgt = u01_f24(rr.x) * S;
+            int row = 4 * Q - 1;
+            float cdf = 0.0f;
+            for (int r = 0; r < 4 * Q; ++r) {
+                const float e = cps[r * kEThreads];
+                if (e >= tgt) {
+                    row = r;
+                    break;
+                }
+                cdf = e;
+            }
+            const int p = row / Q, q = row % Q;
+            const float bxp = p == 0 ? bx[0] : (p == 1 ? bx[1] : (p == 2 ? bx[2] : bx[3]));
+            const float byq = q == 0 ? by[0] : (q == 1 ? by[1] : (q == 2 ? by[2] : by[3]));
+            const float bxy = Q == 4 ? bxp * byq : bxp;
+            float t[4] = {bxy * bz[0], bxy * bz[1], bxy * bz[2], bxy * bz[3]};
+            uint32_t wd[kMaxChannels];
+#pragma unroll
+            for (int m = 0; m < kMaxChannels; ++m) {
+                if (m >= M) break;
+                wd[m] = gather_word<DIM>(a, a.vpad + m * a.vch, ix, iy, iz, p, q);
+                const float *th = thT + (m * L + um[m]) * KP;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) t[c] *= th[(wd[m] >> (8 * c)) & 0xff];
+            }
+            int pc = 3;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                cdf = __fadd_rn(cdf, t[c]);
+                if (cdf >= tgt) {
+                    pc = c;
+                    break;
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kMaxChannels; ++m) {
+                if (m >= M) break;
+                const int k = (wd[m] >> (8 * pc)) & 0xff;
+                atomicAdd(&hc[(m * K + k) * LP + um[m]], 1u);
+            }
+            vp.store_r(a, i, V, fx + (float)(p - 1), fy + (float)(q - 1), fz + (float)(pc - 1));
             continue;
         }
         const float inv = 1.0f / S;
@@ -516,12 +575,17 @@ __global__ void __launch_bounds__(kEThreads, 2) estep_filter_kernel(const EStepA
     __syncthreads();
     for (int q = threadIdx.x; q < M * KL; q += blockDim.x) {
         const int m = q / KL, r = q - m * KL, k = r / L, l = r - k * L;
+        if (SAMPLE) {
+            const unsigned v = hc[(m * K + k) * LP + l];
+            if (v) atomicAdd(&a.hcnt[q], v);
+            continue;
+        }
         const float v = hs[(m * K + k) * LP + l];
         if (v != 0.0f) atomicAdd(&a.hist[q], v);
     }
     __shared__ double red[32];
     const double ms = block_sum(mll, red);
-    if (threadIdx.x == 0) atomicAdd(&a.st->mll, ms);
+    if (threadIdx.x == 0 && !SAMPLE) atomicAdd(&a.st->mll, ms);
     const double dg = block_sum((double)deg, red);
     if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
 }
@@ -1190,8 +1254,9 @@ const void *estep_fn(bool sample, int K, bool logt) {
                                   : (const void *)estep_kernel<false, DIM>);
 }
 
-size_t filter_smem(int K, int L, int M) {
-    return (size_t)M * (L * theta_pitch(K) + K * theta_pitch(L)) * sizeof(float);
+size_t filter_smem(int K, int L, int M, bool sample = false) {
+    return ((size_t)M * (L * theta_pitch(K) + K * theta_pitch(L)) + (sample ? 16 * kEThreads : 0)) *
+           sizeof(float);
 }
 
 size_t ssdf_smem(int M, int Fn) { return (size_t)ssdf_nstats(M, Fn) * kSsdfThreads * 8; }
@@ -1217,6 +1282,8 @@ template <int DIM>
 void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
     if (a.ssdf)
         launch_ssdf_dim<DIM>(a, grid, smem, s);
+    else if (a.filter && sample)
+        count_launch(), estep_filter_kernel<DIM, true><<<grid, kEThreads, smem, s>>>(a);
     else if (a.filter)
         count_launch(), estep_filter_kernel<DIM><<<grid, kEThreads, smem, s>>>(a);
     else if (a.logt && sample)
@@ -1257,18 +1324,27 @@ int estep_grid(bool sample, int K, int L, long V, int dim, bool logt) {
     return (int)g;
 }
 
-int estep_filter_grid(int K, int L, int M, long V, int dim) {
+bool filter_sampling_fits(int K, int L, int M) {
+    return filter_smem(K, L, M, true) <= 227 * 1024;
+}
+
+int estep_filter_grid(int K, int L, int M, long V, int dim, bool sample) {
     BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
     BINDER_CHECK(M >= 1 && M <= kMaxChannels && (long)M * K * L <= kFilterMaxCells,
                  "the MI filter likelihood needs 1 <= M <= 8 and M * K * L <= 24576");
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = filter_smem(K, L, M);
+    const size_t smem = filter_smem(K, L, M, sample);
     BINDER_CHECK(smem <= 227 * 1024,
-                 "the MI filter likelihood's theta and histograms do not fit in shared memory");
-    const void *fn = dim == 3 ? (const void *)estep_filter_kernel<3>
-                              : (const void *)estep_filter_kernel<2>;
+                 sample ? "the MI filter likelihood's theta, counts and draw table do not fit in "
+                          "shared memory (the sampler needs M * K * L below about 22000)"
+                        : "the MI filter likelihood's theta and histograms do not fit in shared "
+                          "memory");
+    const void *fn = sample ? (dim == 3 ? (const void *)estep_filter_kernel<3, true>
+                                        : (const void *)estep_filter_kernel<2, true>)
+                            : (dim == 3 ? (const void *)estep_filter_kernel<3>
+                                        : (const void *)estep_filter_kernel<2>);
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared));
@@ -1322,15 +1398,15 @@ void launch_features_to_soa(const double *in, long n, int C, double *out, cudaSt
 void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, int chains) {
     BINDER_CHECK(!args.logt || (args.K <= kSmallK && (sample || args.colmax)),
                  "the log-space E-step supports at most 64 bins");
-    BINDER_CHECK(!args.filter || (!sample && !args.logt && args.M >= 1 &&
+    BINDER_CHECK(!args.filter || (!args.logt && args.M >= 1 &&
                                   args.M <= kMaxChannels &&
                                   (long)args.M * args.K * args.L <= kFilterMaxCells),
-                 "the MI filter E-step runs EM only, with 1 <= M <= 8 and M * K * L <= 24576");
+                 "the MI filter E-step needs 1 <= M <= 8 and M * K * L <= 24576");
     BINDER_CHECK(!args.ssdf || (!sample && args.fstate && args.fstats && args.M >= 1 &&
                                 args.M <= kSsdfMax && args.Fn >= 1 && args.Fn <= kSsdfMax),
                  "the SSD filter E-step runs EM only, with 1 <= M, F <= 8");
     const size_t smem = args.ssdf     ? ssdf_smem(args.M, args.Fn)
-                        : args.filter ? filter_smem(args.K, args.L, args.M)
+                        : args.filter ? filter_smem(args.K, args.L, args.M, sample)
                                       : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
     // the order-independent merge of the single-pass EM kernel keeps one partial per CTA

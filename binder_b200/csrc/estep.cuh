@@ -68,7 +68,10 @@ constexpr int kLogMaxBins = 64;
 // theta and histograms)
 constexpr int kMaxChannels = 8;
 constexpr long kFilterMaxCells = 24576;
-int estep_filter_grid(int K, int L, int M, long V, int dim);
+int estep_filter_grid(int K, int L, int M, long V, int dim, bool sample = false);
+// whether the sampling E-step of the MI filter likelihood fits in shared memory (theta, counts
+// and its per-thread draw table)
+bool filter_sampling_fits(int K, int L, int M);
 
 // State of the SSD filter likelihood (BINDER/src/cpu/SSDLikelihoodFilter.cpp): M fixed-image
 // channels, F moving-image features (Fn = F, or M with reg_across_features, whose prediction of

@@ -154,6 +154,9 @@ def ref_lib():
     r.ref_sampler_ssd.argtypes = [_dp, _dp, i, i, i, _dp, _dp, i, _dp, _ip, _ip] + \
         [i] * 9 + [_dp, _dp, _dp]
     r.ref_sampler_ssd.restype = d
+    r.ref_sampler_filter.argtypes = [_dp, _dp, i, i, i, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
+                                     _dp, _dp, _dp, _dp, i, d, d, i] + [i] * 8 + \
+        [_dp, _dp, _dp]
     r.ref_em_filter.argtypes = [_dp, _dp] + [i] * 7 + [d, _dp, _dp, i, d, _dp, i, i, i, _ip, _ip,
                                                        _dp, _dp, _dp, _dp, i, d, d, i, i, d, i,
                                                        _dp, _dp]
@@ -591,6 +594,39 @@ def ref_sampler_ssd(R, final_locations, voxel_pos, D, gamma, shape, nodes, voxel
                             int(sample_gamma), int(every), int(posteriors), int(lik), int(transf),
                             int(threads), mean, cov, par)
     return mean, cov, (par[0], par[1]), sec
+
+
+def ref_sampler_filter(R, final_locations, voxel_pos, D, gamma, shape, seed, N_b, N_s, mi=None,
+                       ssd=None, sample_gamma=1, every=1, posteriors=1, lik=1, transf=1):
+    """The reference's Registration::sampler with setMILikelihoodFilter (mi = (alpha,
+    theta[M][K][L], nodes, voxels)) or setSSDLikelihoodFilter (ssd = (coeff[M][F], sigma[M],
+    fnodes, fvoxels, rfa, alpha_0, beta_0)).  Returns (mean [V*3], cov [V*9], parameters)."""
+    nx, ny, nz = shape
+    V = nx * ny * nz
+    mean, cov = np.zeros(V * 3), np.zeros(V * 9)
+    g = np.zeros(3)
+    g[:len(gamma)] = gamma
+    z, zi = np.zeros(1), np.zeros(1, np.int32)
+    if mi is not None:
+        alpha, theta, nodes, voxels = mi
+        M, K, L = np.asarray(theta).shape
+        params = np.zeros(M * K * L)
+        R.ref_sampler_filter(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz,
+                             g, _c64(D).ravel(), 2, float(alpha), _c64(theta).ravel(), K, L, M,
+                             _c32i(nodes).ravel(), _c32i(voxels).ravel(), z, z, z, z, 0, 1.0,
+                             1.0, 1, int(seed), int(N_b), int(N_s), int(sample_gamma),
+                             int(every), int(posteriors), int(lik), int(transf), mean, cov, params)
+    else:
+        coeff, sigma, fnodes, fvoxels, rfa, a0, b0 = ssd
+        M, F = np.asarray(coeff).shape
+        params = np.zeros(M * F)
+        R.ref_sampler_filter(_c64(final_locations).ravel(), _c64(voxel_pos).ravel(), nx, ny, nz,
+                             g, _c64(D).ravel(), 3, 0.0, z, 1, 1, M, zi, zi,
+                             _c64(coeff).ravel(), _c64(sigma).ravel(), _c64(fnodes).ravel(),
+                             _c64(fvoxels).ravel(), int(rfa), float(a0), float(b0), F, int(seed),
+                             int(N_b), int(N_s), int(sample_gamma), int(every), int(posteriors),
+                             int(lik), int(transf), mean, cov, params)
+    return mean, cov, params
 
 
 def ref_em_filter(R, final_locations, voxel_pos, D, gamma, vshape, max_iter, mi=None, ssd=None,

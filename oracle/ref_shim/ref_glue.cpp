@@ -284,6 +284,35 @@ double ref_sampler_ssd(const double *final_locations, const double *voxel_pos, i
     return sec;
 }
 
+// Registration::sampler with a filter likelihood, set up as ref_em_filter does (lk 2: the MI
+// filter likelihood, lk 3: the SSD filter likelihood); mean_out / cov_out as ref_sampler;
+// params_out receives get_likelihood_parameters after the last sweep (theta [M][K][L] or
+// coeff [M][F]).
+void ref_sampler_filter(const double *final_locations, const double *voxel_pos, int nx, int ny,
+                        int nz, const double gamma[3], const double *D, int lk, double alpha,
+                        const double *theta, int K, int L, int M, const int *nodes,
+                        const int *voxels, const double *coeff, const double *sigma,
+                        const double *fnodes, const double *fvoxels, int rfa, double alpha0,
+                        double beta0, int F, int seed, int N_b, int N_s, int sample_gamma,
+                        int every, int posteriors, int lik_params, int transf_params,
+                        double *mean_out, double *cov_out, double *params_out) {
+    Registration r(final_locations, 1, voxel_pos, voxel_pos, nx, ny, nz, nx, ny, nz, 3,
+                   (double)nx * ny * nz);
+    r.setNonLinearTransformation(gamma[0], gamma[1], gamma[2], 1, 1, 1, 1, 1, 1, D);
+    if (lk == 2)
+        r.setMILikelihoodFilter(alpha, theta, 1, nodes, voxels, K, L, M);
+    else
+        r.setSSDLikelihoodFilter(coeff, 1, sigma, fnodes, fvoxels, rfa, alpha0, beta0, M, F);
+    const auto res = r.sampler(seed, N_b, N_s, sample_gamma, every, posteriors, lik_params,
+                               transf_params);
+    if (mean_out) std::memcpy(mean_out, res.first.data(), sizeof(double) * res.first.size());
+    if (cov_out) std::memcpy(cov_out, res.second.data(), sizeof(double) * res.second.size());
+    if (params_out) {
+        const auto p = r.get_likelihood_parameters();
+        std::memcpy(params_out, p.data(), sizeof(double) * p.size());
+    }
+}
+
 // the same, the wall seconds alone
 double ref_sampler_seconds(const double *final_locations, const double *voxel_pos, int nx, int ny,
                            int nz, const double gamma[3], const double *D, double alpha,

@@ -11,6 +11,7 @@ z-score per voxel (tests/test_oracle.py and tests/test_gpu_sampler_reference.py)
 
 Run from the repository root:  python tests/golden/make_sampler_golden.py        (MI)
                                python tests/golden/make_sampler_golden.py ssd    (SSD)
+                               python tests/golden/make_sampler_golden.py mi_filter
 """
 from __future__ import annotations
 
@@ -127,6 +128,56 @@ def main_ssd():
     print("sampler_ssd_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
 
 
+# the MI filter likelihood's case: M = 2 channels of 8 bins, channel m of voxel (node) i read
+# at [i + m] (MILikelihoodFilter.cpp:46-68), one bin array each with one extra entry
+FILTER_M, FILTER_BINS = 2, 8
+
+
+def case_mi_filter():
+    c = case()
+    rng = np.random.default_rng(20261205)
+    pair = phantoms.make_pair(SHAPE, 7, bins=FILTER_BINS, n_objects=10, axes=(2.0, 6.0),
+                              rms=1.0, spacing=3.0)
+    v, _ = bin_signal_robust(pair.moving, FILTER_BINS)
+    c["v"] = np.append(v.astype(np.int32).ravel(), 0)
+    c["u"] = np.append(pair.u.astype(np.int32).ravel(), 0)
+    theta = rng.random((FILTER_M, FILTER_BINS, FILTER_BINS)) + 0.05
+    c["theta"] = theta / theta.sum(2, keepdims=True)
+    return c
+
+
+def main_mi_filter():
+    """sampler_mi_filter_ref.npz: the reference's sampler with the MI filter likelihood
+    (MILikelihoodFilter.cpp:102-175), 32 chains from case_mi_filter(), every switch on; also
+    each chain's final theta"""
+    R = pyoracle.ref_lib()
+    assert R is not None, "oracle/_ref/libbinder_ref.so is needed (make -C oracle)"
+    c = case_mi_filter()
+    V = int(np.prod(SHAPE))
+    means, covs, pars = [], [], []
+    saved = os.dup(1)
+    os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+    try:
+        for ch in range(CHAINS):
+            m, cv, par = pyoracle.ref_sampler_filter(
+                R, c["d0"], c["grid"], c["D"], c["gamma"], SHAPE, SEED0 + ch, N_B, N_S,
+                mi=(2.0, c["theta"], c["v"], c["u"]))
+            means.append(m.reshape(V, 3))
+            covs.append(cv.reshape(V, 9)[:, UPPER])
+            pars.append(par)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    mm, mv, cm, cvv = chain_stats(means, covs)
+    pars = np.asarray(pars)
+    np.savez_compressed(os.path.join(HERE, "sampler_mi_filter_ref.npz"), shape=np.array(SHAPE),
+                        M=FILTER_M, K=FILTER_BINS, L=FILTER_BINS, alpha=2.0, chains=CHAINS,
+                        N_b=N_B, N_s=N_S, d0=c["d0"], u=c["u"], v=c["v"], theta=c["theta"],
+                        D=c["D"], gamma=c["gamma"], mean_mean=mm, mean_var=mv, cov_mean=cm,
+                        cov_var=cvv, params_mean=pars.mean(0), params_var=pars.var(0, ddof=1))
+    print("sampler_mi_filter_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
+
+
 if __name__ == "__main__":
-    # no argument: the MI fixture; "ssd": the SSD likelihood's
-    main_ssd() if sys.argv[1:] == ["ssd"] else main()
+    # no argument: the MI fixture; "ssd" / "mi_filter": the SSD / MI filter likelihood's
+    {"ssd": main_ssd, "mi_filter": main_mi_filter}.get((sys.argv[1:] or [""])[0], main)()
