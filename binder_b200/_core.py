@@ -141,7 +141,7 @@ class Registration:
                                reg_across_features, alpha_0, beta_0, M, F):
         """``setSSDLikelihoodFilter`` of the CPU module (cpu/bindings.cpp:154-189): M fixed-image
         channels ([V][M] features), F moving-image features ([Vn][F], or [Vn][M] with
-        reg_across_features), coeff [M][F], sigma [M].  EM only."""
+        reg_across_features), coeff [M][F], sigma [M].  EM and the sampler."""
         M, F = int(M), int(F)
         Fn = M if reg_across_features else F
         Vn = int(np.prod(self._nshape))
@@ -164,7 +164,8 @@ class Registration:
 
     def setSSDLikelihood(self, bins, threads, sigma_sq, scale_shift, scale, shift, binned_nodes,
                          binned_voxels, alpha_0, beta_0):
-        """``setSSDLikelihood`` of the CPU module (cpu/bindings.cpp:120-152); EM only."""
+        """``setSSDLikelihood`` of the CPU module (cpu/bindings.cpp:120-152); EM and the
+        sampler."""
         bins = int(bins)
         Vn = int(np.prod(self._nshape))
         check(lib().binder_registration_set_ssd_likelihood(

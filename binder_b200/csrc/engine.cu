@@ -572,7 +572,7 @@ void Registration::set_ssd_filter_likelihood(const double *coeff, const double *
     fFn_ = Fn;
     lk_ = 3;
     egrid_e_ = estep_ssdf_grid(M, Fn, V_, N_);
-    egrid_s_ = 0;
+    egrid_s_ = estep_ssdf_grid(M, Fn, V_, N_, true);
     have_mi_ = true;
 }
 
@@ -806,9 +806,6 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     if (sample_posteriors || sample_likelihood_parameters) {
         if (!have_mi_) throw Error(kNotReady, "setMILikelihood has not been called");
     }
-    if (lk_ == 3)
-        throw Error(kUnsupported,
-                    "the sampler with the SSD filter (feature) likelihood is not built (EM only)");
     if (lk_ == 2 && sample_posteriors && egrid_s_ == 0)
         throw Error(kUnsupported,
                     "the sampler with the MI filter likelihood needs M * K * L small enough for "
@@ -844,6 +841,8 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
                     if (lk_ == 1)  // SSDLikelihood::sample_parameters from the sweep's counts
                         launch_ssd_sample(theta_, colmax_, hcnt_, K_, L_, ssd_, st_, seed_,
                                           chain_, stream_);
+                    else if (lk_ == 3)  // SSDLikelihoodFilter::sample_parameters
+                        launch_ssdf_sample(fst_, fstats_, st_, seed_, chain_, stream_);
                     else  // MI: K rows; MI filter: M * K rows (MILikelihoodFilter.cpp:152-175)
                         launch_dirichlet_sample(theta_, hcnt_, M_ * K_, L_, alpha_, seed_, chain_,
                                                 st_, stream_);

@@ -606,7 +606,7 @@ __host__ __device__ constexpr int ssdf_nstats(int M, int Fn) {
 // whose sigma numerator is S2_m - 2 c_m . b_m + c_m^T A c_m for the new coefficients c_m), so
 // each voxel adds its posterior moments of n to per-thread FP64 columns in shared memory, reduced
 // once per CTA.  Two passes over the neighbours: the largest term, then exp(term - max).
-template <int DIM, int FM>
+template <int DIM, int FM, bool SAMPLE = false>
 __global__ void __launch_bounds__(kSsdfThreads) estep_ssdf_kernel(const EStepArgs a) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     constexpr int NA = FM * (FM + 1) / 2;
@@ -622,6 +622,9 @@ __global__ void __launch_bounds__(kSsdfThreads) estep_ssdf_kernel(const EStepArg
     const double lc = ps->lc;
     double *my = cols + threadIdx.x;  // my[s * kSsdfThreads]
     for (int s = 0; s < nst; ++s) my[s * kSsdfThreads] = 0.0;
+    // sampling: the running sum at the end of node row r, cps[r * kSsdfThreads]
+    float *cps = reinterpret_cast<float *>(cols + (size_t)nst * kSsdfThreads) + threadIdx.x;
+    const uint32_t sweep = SAMPLE ? (uint32_t)a.st->sweep : 0u;
     __syncthreads();
 
     const long Vn = (long)a.nxn * a.nyn * a.nzn;
@@ -680,6 +683,75 @@ __global__ void __launch_bounds__(kSsdfThreads) estep_ssdf_kernel(const EStepArg
                     double n[FM];
                     mx = fmax(mx, term_of(p, q, c, n));
                 }
+        if (SAMPLE) {
+            // categorical draw of one neighbour (Registration.cpp:331-470 with sample): the
+            // first whose running sum of exp(term - max) reaches u * S; its statistics enter
+            // with posterior 1 (SSDLikelihoodFilter.cpp:168-198)
+            float S = 0.0f;
+#pragma unroll 1
+            for (int p = 0; p < 4; ++p)
+#pragma unroll 1
+                for (int q = 0; q < Q; ++q) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        double nd[FM];
+                        S = __fadd_rn(S, expf((float)(term_of(p, q, c, nd) - mx)));
+                    }
+                    cps[(p * Q + q) * kSsdfThreads] = S;
+                }
+            if (!(S > 0.0f)) {
+                vp.store_r(a, i, V, (float)ix, (float)iy, (float)iz);
+                ++deg;
+                continue;
+            }
+            const u32x4 rr = philox_draw(a.seed, i, sweep, 1u, a.chain);
+            const float tgt = u01_f24(rr.x) * S;
+            int row = 4 * Q - 1;
+            float cdf = 0.0f;
+            for (int r = 0; r < 4 * Q; ++r) {
+                const float e = cps[r * kSsdfThreads];
+                if (e >= tgt) {
+                    row = r;
+                    break;
+                }
+                cdf = e;
+            }
+            const int p = row / Q, q = row % Q;
+            int pc = 3;
+            double nd[FM], pick[FM];
+#pragma unroll
+            for (int f = 0; f < FM; ++f) pick[f] = 0.0;
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+                cdf = __fadd_rn(cdf, expf((float)(term_of(p, q, c, nd) - mx)));
+                pc = c;
+#pragma unroll
+                for (int f = 0; f < FM; ++f) pick[f] = nd[f];
+                if (cdf >= tgt) break;
+            }
+            int s = 0;
+#pragma unroll
+            for (int f = 0; f < FM; ++f)
+#pragma unroll
+                for (int g = f; g < FM; ++g)
+                    if (g < Fn) my[(s++) * kSsdfThreads] += pick[f] * pick[g];
+#pragma unroll
+            for (int m = 0; m < kSsdfMax; ++m) {
+                if (m >= M) break;
+#pragma unroll
+                for (int f = 0; f < FM; ++f)
+                    if (f < Fn) my[(s++) * kSsdfThreads] += xv[m] * pick[f];
+            }
+#pragma unroll
+            for (int m = 0; m < kSsdfMax; ++m) {
+                if (m >= M) break;
+                my[(s++) * kSsdfThreads] += xv[m] * xv[m];
+            }
+            my[s * kSsdfThreads] += 1.0;
+            vp.store_r(a, i, V, (float)(ix - 1 + p), (float)(DIM == 3 ? iy - 1 + q : 0),
+                       (float)(iz - 1 + pc));
+            continue;
+        }
         float S = 0.0f, Sx = 0.0f, Sy = 0.0f, Sz = 0.0f, Bn[FM], A[NA];
 #pragma unroll
         for (int f = 0; f < FM; ++f) Bn[f] = 0.0f;
@@ -755,7 +827,7 @@ __global__ void __launch_bounds__(kSsdfThreads) estep_ssdf_kernel(const EStepArg
         }
     }
     const double ms = block_sum(mll, red);
-    if (threadIdx.x == 0) atomicAdd(&a.st->mll, ms);
+    if (threadIdx.x == 0 && !SAMPLE) atomicAdd(&a.st->mll, ms);
     const double dg = block_sum((double)deg, red);
     if (threadIdx.x == 0 && dg > 0.0) atomicAdd(&a.st->degenerate, (unsigned long long)dg);
 }
@@ -843,6 +915,86 @@ __global__ void ssdf_update_kernel(SsdfState *ps, double *stats, int update, Dev
             cost += -(a * log(bb) - lgamma(a) + (-a - 1.0) * log(x) - bb / x);
         }
         if (st) st->lp_lik = cost;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kSsdfStats; q += blockDim.x) stats[q] = 0.0;
+}
+
+// SSDLikelihoodFilter::sample_parameters (:459-463): update_coefficients and update_sigma with
+// sample = true, from the sweep's statistics (the drawn nodes, posterior 1).  Coefficients
+// (reg_across_features 0): x = solve(A, b_m), then sample_multivariate_normal(x, A) as written
+// (:392-427): L = chol(A) -- A itself as the covariance -- and coefficient i = x_i + sum_{j<=i}
+// L_ij z_ij with a fresh standard normal z_ij per term (Philox ctr {(m * 8 + i) * 8 + j, sweep,
+// 8, chain}, Box-Muller on words 0 and 1).  sigma_m = 1 / g, g ~ Gamma(shape den / 2, scale
+// 2 / num_m) (sample_inverse_gamma(den / 2, num_m / 2), :429-432; tag 9, index m) with num_m from
+// the drawn coefficients.  One thread.
+__device__ double gamma_mt(double shape, uint64_t seed, uint32_t index, uint32_t sweep,
+                           uint32_t tag, uint32_t chain, bool *capped);
+
+__global__ void ssdf_sample_kernel(SsdfState *ps, double *stats, DevState *st, uint64_t seed,
+                                   uint32_t chain) {
+    if (st->done) return;
+    if (threadIdx.x == 0) {
+        SsdfState &p = *ps;
+        const int M = p.M, Fn = p.Fn;
+        const uint32_t sweep = (uint32_t)st->sweep;
+        const double *A = stats + kSsdfA, *b = stats + kSsdfB;
+        double c[kSsdfMax * kSsdfMax];
+        if (p.rfa) {
+            for (int m = 0; m < M; ++m)
+                for (int f = 0; f < Fn; ++f) c[m * Fn + f] = m == f ? 1.0 : 0.0;
+        } else {
+            double Lc[kSsdfMax * kSsdfMax];
+            for (int i = 0; i < Fn; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    double sum = 0.0;
+                    for (int k = 0; k < j; ++k) sum += Lc[i * Fn + k] * Lc[j * Fn + k];
+                    Lc[i * Fn + j] = i == j ? sqrt(A[j * Fn + j] - sum)
+                                            : (A[i * Fn + j] - sum) / Lc[j * Fn + j];
+                }
+            for (int m = 0; m < M; ++m) {
+                double x[kSsdfMax];
+                ssdf_solve(Fn, A, b + m * Fn, x);
+                for (int i = 0; i < Fn; ++i) {
+                    double v = x[i];
+                    for (int j = 0; j <= i; ++j) {
+                        const u32x4 r = philox_draw(seed, (uint32_t)((m * 8 + i) * 8 + j), sweep,
+                                                    8u, chain);
+                        const double z = sqrt(-2.0 * log(u01_d32(r.x))) * cospi(2.0 * u01_d32(r.y));
+                        v += Lc[i * Fn + j] * z;
+                    }
+                    c[m * Fn + i] = v;
+                    p.coeff[m * p.F + i] = v;
+                }
+            }
+        }
+        const double den = stats[kSsdfEff] + 2.0 * p.alpha0;
+        bool capped = false;
+        for (int m = 0; m < M; ++m) {
+            const double *cm = c + m * Fn;
+            double cb = 0.0, cac = 0.0;
+            for (int f = 0; f < Fn; ++f) {
+                cb += cm[f] * b[m * Fn + f];
+                double af = 0.0;
+                for (int g = 0; g < Fn; ++g) af += A[f * Fn + g] * cm[g];
+                cac += cm[f] * af;
+            }
+            const double num = stats[kSsdfS2 + m] - 2.0 * cb + cac + 2.0 * p.alpha0 * p.beta0;
+            const double g = gamma_mt(0.5 * den, seed, (uint32_t)m, sweep, 9u, chain, &capped) *
+                             (2.0 / num);
+            p.sigma[m] = 1.0 / g;
+            if (!isfinite(p.sigma[m]) || !(p.sigma[m] > 0.0))
+                atomicOr(&st->flags, (unsigned)kFlagNonFinite);
+        }
+        if (capped) atomicOr(&st->flags, (unsigned)kFlagGammaCapped);
+        ssdf_refresh(p);
+        const double a = p.alpha0, bb = p.alpha0 * p.beta0;
+        double cost = 0.0;
+        for (int m = 0; m < M; ++m) {
+            const double x = p.sigma[m];
+            cost += -(a * log(bb) - lgamma(a) + (-a - 1.0) * log(x) - bb / x);
+        }
+        st->lp_lik = cost;
     }
     __syncthreads();
     for (int q = threadIdx.x; q < kSsdfStats; q += blockDim.x) stats[q] = 0.0;
@@ -1259,29 +1411,45 @@ size_t filter_smem(int K, int L, int M, bool sample = false) {
            sizeof(float);
 }
 
-size_t ssdf_smem(int M, int Fn) { return (size_t)ssdf_nstats(M, Fn) * kSsdfThreads * 8; }
+// the per-thread statistics columns, and for sampling the per-thread draw table (16 rows)
+size_t ssdf_smem(int M, int Fn, bool sample = false) {
+    return (size_t)ssdf_nstats(M, Fn) * kSsdfThreads * 8 + (sample ? 16 * kSsdfThreads * 4 : 0);
+}
 
-template <int DIM>
-const void *ssdf_fn(int Fn) {
-    if (Fn <= 2) return (const void *)estep_ssdf_kernel<DIM, 2>;
-    if (Fn <= 4) return (const void *)estep_ssdf_kernel<DIM, 4>;
-    return (const void *)estep_ssdf_kernel<DIM, 8>;
+template <int DIM, bool SAMPLE>
+const void *ssdf_fn_s(int Fn) {
+    if (Fn <= 2) return (const void *)estep_ssdf_kernel<DIM, 2, SAMPLE>;
+    if (Fn <= 4) return (const void *)estep_ssdf_kernel<DIM, 4, SAMPLE>;
+    return (const void *)estep_ssdf_kernel<DIM, 8, SAMPLE>;
 }
 
 template <int DIM>
-void launch_ssdf_dim(const EStepArgs &a, int grid, size_t smem, cudaStream_t s) {
+const void *ssdf_fn(int Fn, bool sample = false) {
+    return sample ? ssdf_fn_s<DIM, true>(Fn) : ssdf_fn_s<DIM, false>(Fn);
+}
+
+template <int DIM, bool SAMPLE>
+void launch_ssdf_dim_s(const EStepArgs &a, int grid, size_t smem, cudaStream_t s) {
     if (a.Fn <= 2)
-        count_launch(), estep_ssdf_kernel<DIM, 2><<<grid, kSsdfThreads, smem, s>>>(a);
+        count_launch(), estep_ssdf_kernel<DIM, 2, SAMPLE><<<grid, kSsdfThreads, smem, s>>>(a);
     else if (a.Fn <= 4)
-        count_launch(), estep_ssdf_kernel<DIM, 4><<<grid, kSsdfThreads, smem, s>>>(a);
+        count_launch(), estep_ssdf_kernel<DIM, 4, SAMPLE><<<grid, kSsdfThreads, smem, s>>>(a);
     else
-        count_launch(), estep_ssdf_kernel<DIM, 8><<<grid, kSsdfThreads, smem, s>>>(a);
+        count_launch(), estep_ssdf_kernel<DIM, 8, SAMPLE><<<grid, kSsdfThreads, smem, s>>>(a);
+}
+
+template <int DIM>
+void launch_ssdf_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
+    if (sample)
+        launch_ssdf_dim_s<DIM, true>(a, grid, smem, s);
+    else
+        launch_ssdf_dim_s<DIM, false>(a, grid, smem, s);
 }
 
 template <int DIM>
 void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
     if (a.ssdf)
-        launch_ssdf_dim<DIM>(a, grid, smem, s);
+        launch_ssdf_dim<DIM>(a, sample, grid, smem, s);
     else if (a.filter && sample)
         count_launch(), estep_filter_kernel<DIM, true><<<grid, kEThreads, smem, s>>>(a);
     else if (a.filter)
@@ -1356,16 +1524,16 @@ int estep_filter_grid(int K, int L, int M, long V, int dim, bool sample) {
     return (int)g;
 }
 
-int estep_ssdf_grid(int M, int Fn, long V, int dim) {
+int estep_ssdf_grid(int M, int Fn, long V, int dim, bool sample) {
     BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
     BINDER_CHECK(M >= 1 && M <= kSsdfMax && Fn >= 1 && Fn <= kSsdfMax,
                  "the SSD filter likelihood needs 1 <= M, F <= 8");
     int dev = 0, sms = 148, per_sm = 1;
     BINDER_CUDA(cudaGetDevice(&dev));
     BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = ssdf_smem(M, Fn);
+    const size_t smem = ssdf_smem(M, Fn, sample);
     // both dimensions' kernels for this feature count
-    const void *fns[2] = {ssdf_fn<2>(Fn), ssdf_fn<3>(Fn)};
+    const void *fns[2] = {ssdf_fn<2>(Fn, sample), ssdf_fn<3>(Fn, sample)};
     for (const void *f : fns) {
         BINDER_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
@@ -1382,6 +1550,12 @@ int estep_ssdf_grid(int M, int Fn, long V, int dim) {
 }
 
 void ssdf_refresh_host(SsdfState &p) { ssdf_refresh(p); }
+
+void launch_ssdf_sample(SsdfState *p, double *stats, DevState *st, uint64_t seed,
+                        uint32_t chain, cudaStream_t s) {
+    count_launch(), ssdf_sample_kernel<<<1, 160, 0, s>>>(p, stats, st, seed, chain);
+    BINDER_CUDA(cudaGetLastError());
+}
 
 void launch_ssdf_update(SsdfState *p, double *stats, int update, DevState *st, cudaStream_t s) {
     count_launch(), ssdf_update_kernel<<<1, 160, 0, s>>>(p, stats, update, st);
@@ -1402,10 +1576,10 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
                                   args.M <= kMaxChannels &&
                                   (long)args.M * args.K * args.L <= kFilterMaxCells),
                  "the MI filter E-step needs 1 <= M <= 8 and M * K * L <= 24576");
-    BINDER_CHECK(!args.ssdf || (!sample && args.fstate && args.fstats && args.M >= 1 &&
+    BINDER_CHECK(!args.ssdf || (args.fstate && args.fstats && args.M >= 1 &&
                                 args.M <= kSsdfMax && args.Fn >= 1 && args.Fn <= kSsdfMax),
-                 "the SSD filter E-step runs EM only, with 1 <= M, F <= 8");
-    const size_t smem = args.ssdf     ? ssdf_smem(args.M, args.Fn)
+                 "the SSD filter E-step needs 1 <= M, F <= 8");
+    const size_t smem = args.ssdf     ? ssdf_smem(args.M, args.Fn, sample)
                         : args.filter ? filter_smem(args.K, args.L, args.M, sample)
                                       : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;

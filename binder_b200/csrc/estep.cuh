@@ -91,10 +91,15 @@ struct SsdfState {
 // eff = sum p (n the node's features, 0 outside the grid)
 constexpr int kSsdfA = 0, kSsdfB = 64, kSsdfS2 = 128, kSsdfEff = 136, kSsdfStats = 137;
 void ssdf_refresh_host(SsdfState &p);  // cf, h, lc from coeff, sigma
-int estep_ssdf_grid(int M, int Fn, long V, int dim);
+int estep_ssdf_grid(int M, int Fn, long V, int dim, bool sample = false);
 // update_parameters (when update) and compute_cost of the SSD filter likelihood from stats,
 // which it clears; the cost goes to st->lp_lik
 void launch_ssdf_update(SsdfState *p, double *stats, int update, DevState *st, cudaStream_t s);
+// the sampler's draw of the SSD filter likelihood's coefficients and sigmas
+// (SSDLikelihoodFilter.cpp:459-463) from the sweep's statistics, which it clears; Philox ctr
+// {index, st->sweep, 8 / 9, chain}; the prior cost into st->lp_lik.  One CTA.
+void launch_ssdf_sample(SsdfState *p, double *stats, DevState *st, uint64_t seed,
+                        uint32_t chain, cudaStream_t s);
 // [n][C] features (device memory) to SoA [C][n]
 void launch_features_to_soa(const double *in, long n, int C, double *out, cudaStream_t s);
 

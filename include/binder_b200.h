@@ -75,7 +75,7 @@ int binder_registration_set_mi_likelihood(binder_registration *h, double alpha, 
  * The CPU backend's multi-channel MI likelihood (MILikelihoodFilter.cpp): theta [M][K][L]; the
  * bins of channel m are read at [index + m] as the reference reads them, so binned_nodes holds
  * at least Nx_n*Ny_n*Nz_n + M - 1 bins in [0, K) and binned_voxels Nx_v*Ny_v*Nz_v + M - 1 in
- * [0, L).  1 <= M <= 8, M*K*L <= 24576.  EM only (the sampler rejects it);
+ * [0, L).  1 <= M <= 8, M*K*L <= 24576.  EM and the sampler (M*K*L up to about 22000 there);
  * get_likelihood_parameters then returns M*K*L values. */
 int binder_registration_set_mi_likelihood_filter(binder_registration *h, double alpha,
                                                  const float *theta, int threads,
@@ -103,8 +103,9 @@ int binder_registration_get_ssd_parameters(const binder_registration *h, double 
  * (features_voxels [Nx_v*Ny_v*Nz_v][M]), F moving-image features (features_nodes
  * [Nx_n*Ny_n*Nz_n][F], or [..][M] with reg_across_features, which then predicts channel m by
  * feature m and fits no coefficients), coeff [M][F] and sigma [M] in host memory; 1 <= M, F <= 8.
- * EM in log space only (the sampler rejects it); get_likelihood_parameters then returns the M*F
- * coefficients. */
+ * EM in log space and the sampler (its draws of the coefficients and sigmas, :459-463, with
+ * sample_multivariate_normal and sample_inverse_gamma as written; not in sampler_chains);
+ * get_likelihood_parameters then returns the M*F coefficients. */
 int binder_registration_set_ssd_likelihood_filter(binder_registration *h, const double *coeff,
                                                   int threads, const double *sigma,
                                                   const double *features_nodes,
@@ -134,8 +135,8 @@ int binder_registration_em(binder_registration *h, int max_iterations, double co
  *         sample_likelihood_parameters, sample_transformation_parameters) -> (mean, cov)
  *                                                               gpu/bindings.cpp:105-131
  * mean_out [V*3] and cov_out [V*3*3] (M2 / (N_s - 1)) in FP64 (FP64 Welford accumulators).
- * Likelihoods: MI and SSD (cpu/Registration.cpp:515-642 drives both); the filter likelihoods
- * are rejected. */
+ * Every likelihood: MI, SSD, MI filter and SSD filter (cpu/Registration.cpp:515-642 drives
+ * each through its sample_parameters). */
 int binder_registration_sampler(binder_registration *h, uint64_t seed, int N_b, int N_s,
                                 int sample_gamma, int sample_gamma_every, int sample_posteriors,
                                 int sample_likelihood_parameters,

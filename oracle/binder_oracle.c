@@ -1533,6 +1533,66 @@ static void ssdf_solve(int n, const double *A, const double *b, double *x) {
 /* update_parameters (:200-203): update_coefficients (:205-290, EM branch) then update_sigma
  * (:292-346), from the accumulators of orc_ssdf_estep; then compute_cost (:72-89).  With
  * update == 0 only the cost. */
+/* sample_parameters (:459-463): update_coefficients and update_sigma with sample = true.
+ * Coefficients (reg_across_features 0): x = solve(A, b_m), then sample_multivariate_normal(x, A)
+ * as written (:392-427): L = chol(A) and coefficient i = x_i + sum_{j<=i} L_ij z_ij, a fresh
+ * standard normal per term (Philox ctr {(m * 8 + i) * 8 + j, sweep, 8, chain}, Box-Muller on
+ * words 0 and 1).  sigma_m = 1 / g, g ~ Gamma(shape den / 2, scale 2 / num_m)
+ * (sample_inverse_gamma(den / 2, num_m / 2), :429-432; tag 9, index m), num_m with the drawn
+ * coefficients.  Returns 1 when a gamma draw hit its attempt cap. */
+int orc_ssdf_sample(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
+                    const double *gamma, const double *s1, const double *s2,
+                    const double *outside, uint64_t seed, uint32_t sweep, uint32_t chain) {
+    const int M = p->M, F = p->F;
+    const long Vn = (long)nxn * nyn * nzn;
+    double eff = outside[0];
+    for (long j = 0; j < Vn; ++j) eff += gamma[j];
+    if (!p->rfa) {
+        double A[64] = {0}, b[64] = {0}, x[8], Lc[64] = {0};
+        for (long j = 0; j < Vn; ++j)
+            for (int f1 = 0; f1 < F; ++f1)
+                for (int f2 = 0; f2 < F; ++f2)
+                    A[f1 * F + f2] += nodes[j * F + f1] * nodes[j * F + f2] * gamma[j];
+        for (int m = 0; m < M; ++m)
+            for (long j = 0; j < Vn; ++j)
+                for (int f = 0; f < F; ++f) b[m * F + f] += s1[m * Vn + j] * nodes[j * F + f];
+        for (int i = 0; i < F; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double sum = 0.0;
+                for (int k = 0; k < j; ++k) sum += Lc[i * F + k] * Lc[j * F + k];
+                Lc[i * F + j] = i == j ? sqrt(A[j * F + j] - sum) : (A[i * F + j] - sum) / Lc[j * F + j];
+            }
+        for (int m = 0; m < M; ++m) {
+            ssdf_solve(F, A, b + m * F, x);
+            for (int i = 0; i < F; ++i) {
+                double v = x[i];
+                for (int j = 0; j <= i; ++j) {
+                    uint32_t r[4];
+                    philox_draw(seed, (uint32_t)((m * 8 + i) * 8 + j), sweep, 8u, chain, r);
+                    v += Lc[i * F + j] * sqrt(-2.0 * log(u01_d32(r[0]))) *
+                         cos(2.0 * PI_D * u01_d32(r[1]));
+                }
+                p->coeff[m * F + i] = v;
+            }
+        }
+    }
+    int capped = 0;
+    for (int m = 0; m < M; ++m) {
+        double num = 0.0;
+        for (long j = 0; j < Vn; ++j) {
+            const double t = ssdf_pred(p, nodes, j, m);
+            num += s2[m * Vn + j] + (-2.0 * s1[m * Vn + j] * t) + gamma[j] * t * t;
+        }
+        num += outside[1 + M + m];
+        num += 2.0 * p->alpha0 * p->beta0;
+        const double den = eff + 2.0 * p->alpha0;
+        const double g = orc_gamma_sample(0.5 * den, seed, (uint32_t)m, sweep, 9u, chain, &capped) *
+                         (2.0 / num);
+        p->sigma[m] = 1.0 / g;
+    }
+    return capped;
+}
+
 double orc_ssdf_update(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
                        const double *gamma, const double *s1, const double *s2,
                        const double *outside, int update) {

@@ -142,6 +142,10 @@ double orc_ssdf_estep(const double *d, const double *nodes, const double *voxels
 double orc_ssdf_update(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
                        const double *gamma, const double *s1, const double *s2,
                        const double *outside, int update);
+/* sample_parameters (:459-463), Philox-driven; 1 if a gamma draw hit its attempt cap */
+int orc_ssdf_sample(orc_ssdf *p, const double *nodes, int nxn, int nyn, int nzn,
+                    const double *gamma, const double *s1, const double *s2,
+                    const double *outside, uint64_t seed, uint32_t sweep, uint32_t chain);
 
 /* ---- Gibbs sampler driver: BINDER/src/cpu/Registration.cpp:515-642 ----------------------------
  * mean_out [V*N], cov_out [V*N*N] (M2 / (N_s - 1)).  dream is the working dream-location buffer

@@ -63,6 +63,8 @@ def _load_oracle():
     lib.orc_ssdf_estep.restype = d
     lib.orc_ssdf_update.argtypes = [C.c_void_p, _dp, i, i, i, _dp, _dp, _dp, _dp, i]
     lib.orc_ssdf_update.restype = d
+    lib.orc_ssdf_sample.argtypes = [C.c_void_p, _dp, i, i, i, _dp, _dp, _dp, _dp, u64, u32, u32]
+    lib.orc_ssdf_sample.restype = i
     lib.orc_estep_sample.argtypes = [_dp, _ip, _ip, _dp] + [i] * 8 + [u64, u32, u32, _dp, _dp]
     lib.orc_estep_sample.restype = d
     lib.orc_theta_map.argtypes = [_dp, i, i, d]
@@ -526,6 +528,13 @@ def ssdf_update(params, nodes, nshape, acc, update=True):
     """update_parameters (when update) and compute_cost; params is updated in place."""
     return lib().orc_ssdf_update(C.addressof(params), _c64(nodes).ravel(), *nshape, *acc,
                                  int(update))
+
+
+def ssdf_sample(params, nodes, nshape, acc, seed, sweep, chain=0):
+    """sample_parameters from the accumulators acc = (gamma, s1, s2, outside); params is
+    updated in place; returns 1 if a gamma draw hit its attempt cap"""
+    return lib().orc_ssdf_sample(C.addressof(params), _c64(nodes).ravel(), *nshape, *acc,
+                                 int(seed), int(sweep), int(chain))
 
 
 def ref_em(R, final_locations, voxel_pos, D, gamma, vshape, nshape, nodes, voxels, max_iter,

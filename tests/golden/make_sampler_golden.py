@@ -12,6 +12,7 @@ z-score per voxel (tests/test_oracle.py and tests/test_gpu_sampler_reference.py)
 Run from the repository root:  python tests/golden/make_sampler_golden.py        (MI)
                                python tests/golden/make_sampler_golden.py ssd    (SSD)
                                python tests/golden/make_sampler_golden.py mi_filter
+                               python tests/golden/make_sampler_golden.py ssd_filter
 """
 from __future__ import annotations
 
@@ -178,6 +179,57 @@ def main_mi_filter():
     print("sampler_mi_filter_ref.npz:", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
 
 
+def case_ssd_filter():
+    """the SSD filter likelihood's case: F = 2 node features (the moving image and its Gaussian
+    smoothing, sigma 1) and M = 2 voxel channels (the same of the fixed image), identity
+    coefficients, sigma 0.05 per channel, alpha_0 = beta_0 = 1"""
+    from scipy import ndimage
+    c = case()
+    pair = phantoms.make_pair(SHAPE, 7, bins=16, n_objects=10, axes=(2.0, 6.0), rms=1.0,
+                              spacing=3.0)
+    mv, fx = pair.moving.astype(np.float64), pair.fixed.astype(np.float64)
+    c["fn"] = np.stack([mv, ndimage.gaussian_filter(mv, 1.0)], -1).reshape(-1, 2)
+    c["fv"] = np.stack([fx, ndimage.gaussian_filter(fx, 1.0)], -1).reshape(-1, 2)
+    c["coeff"] = np.eye(2)
+    c["sigma"] = np.array([0.05, 0.05])
+    return c
+
+
+def main_ssd_filter():
+    """sampler_ssd_filter_ref.npz: the reference's sampler with the SSD filter likelihood
+    (SSDLikelihoodFilter.cpp:168-463), 32 chains each with reg_across_features 1 (sigma drawn)
+    and 0 (coefficients drawn too), every switch on; also each chain's final coefficients"""
+    R = pyoracle.ref_lib()
+    assert R is not None, "oracle/_ref/libbinder_ref.so is needed (make -C oracle)"
+    c = case_ssd_filter()
+    V = int(np.prod(SHAPE))
+    out = dict(shape=np.array(SHAPE), chains=CHAINS, N_b=N_B, N_s=N_S, d0=c["d0"], fn=c["fn"],
+               fv=c["fv"], coeff=c["coeff"], sigma=c["sigma"], D=c["D"], gamma=c["gamma"])
+    for rfa in (1, 0):
+        means, covs, pars = [], [], []
+        saved = os.dup(1)
+        os.dup2(os.open(os.devnull, os.O_WRONLY), 1)
+        try:
+            for ch in range(CHAINS):
+                m, cv, par = pyoracle.ref_sampler_filter(
+                    R, c["d0"], c["grid"], c["D"], c["gamma"], SHAPE, SEED0 + ch, N_B, N_S,
+                    ssd=(c["coeff"], c["sigma"], c["fn"], c["fv"], rfa, 1.0, 1.0))
+                means.append(m.reshape(V, 3))
+                covs.append(cv.reshape(V, 9)[:, UPPER])
+                pars.append(par)
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        mm, mv, cm, cvv = chain_stats(means, covs)
+        pars = np.asarray(pars)
+        out.update({f"r{rfa}_mean_mean": mm, f"r{rfa}_mean_var": mv, f"r{rfa}_cov_mean": cm,
+                    f"r{rfa}_cov_var": cvv, f"r{rfa}_params_mean": pars.mean(0),
+                    f"r{rfa}_params_var": pars.var(0, ddof=1)})
+    np.savez_compressed(os.path.join(HERE, "sampler_ssd_filter_ref.npz"), **out)
+    print("sampler_ssd_filter_ref.npz: 2 x", CHAINS, "chains of", N_B + N_S, "sweeps on", SHAPE)
+
+
 if __name__ == "__main__":
-    # no argument: the MI fixture; "ssd" / "mi_filter": the SSD / MI filter likelihood's
-    {"ssd": main_ssd, "mi_filter": main_mi_filter}.get((sys.argv[1:] or [""])[0], main)()
+    # no argument: the MI fixture; "ssd" / "mi_filter" / "ssd_filter": the other likelihoods'
+    {"ssd": main_ssd, "mi_filter": main_mi_filter,
+     "ssd_filter": main_ssd_filter}.get((sys.argv[1:] or [""])[0], main)()

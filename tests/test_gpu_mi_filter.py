@@ -134,8 +134,9 @@ def test_reset_and_errors(core):
     assert not np.array_equal(reg.get_likelihood_parameters(), th0)
     reg.reset()
     np.testing.assert_array_equal(reg.get_likelihood_parameters(), th0)
-    with pytest.raises(BinderError, match="unsupported"):
-        reg.sampler(1, 1, 1, 0, 1, 1, 1, 1)
+    # the sampler runs with this likelihood (its checks: tests/test_gpu_filter_sampler.py)
+    m, cv = reg.sampler(1, 1, 2, 0, 1, 1, 1, 1)
+    assert np.all(np.isfinite(m)) and np.all(np.isfinite(cv))
     bad = c["uf"].copy()
     bad[17] = c["L"]
     with pytest.raises(BinderError, match="binned_voxels value 6 outside"):

@@ -105,8 +105,8 @@ def test_reset_and_rejections(core):
     reg.EM(3, -1e30, 1, 0)
     # the same run again; the cross-CTA FP32 histogram sums are atomics, so equal to round-off
     np.testing.assert_allclose(reg.get_final_locations_as_numpy_array(), a, rtol=0, atol=1e-5)
-    with pytest.raises(core.BinderError) as e:
-        reg.sampler(1, 1, 2, 0, 1, 1, 1, 1)
-    assert e.value.status == 3
+    # the sampler runs with this likelihood (its checks: tests/test_gpu_ssd_sampler.py)
+    m, cv = reg.sampler(1, 1, 2, 0, 1, 1, 1, 1)
+    assert np.all(np.isfinite(m)) and np.all(np.isfinite(cv))
     with pytest.raises(core.BinderError):
         new_reg(core, ssd_case(seed=62, bins=80), 0)

@@ -156,8 +156,9 @@ def test_reset_and_errors(core):
     coeff, sigma = reg.ssd_filter_parameters()
     np.testing.assert_array_equal(coeff, c["coeff"])
     np.testing.assert_array_equal(sigma, c["sigma"])
-    with pytest.raises(BinderError, match="unsupported"):
-        reg.sampler(1, 1, 1, 0, 1, 1, 1, 1)
+    # the sampler runs with this likelihood (its checks: tests/test_gpu_filter_sampler.py)
+    m, cv = reg.sampler(1, 1, 2, 0, 1, 1, 1, 1)
+    assert np.all(np.isfinite(m)) and np.all(np.isfinite(cv))
     with pytest.raises(BinderError, match="sigma must be positive"):
         reg.setSSDLikelihoodFilter(c["coeff"], 1, [1.0, -1.0], c["nodes"], c["voxels"], 0, 2.0,
                                    0.5, 2, 3)
