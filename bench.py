@@ -330,13 +330,11 @@ def run_target(core, rank, dist):
     import torch
     from binder_b200 import autotune
     from binder_b200 import initnet as I
-    from binder_b200 import phantoms
     if not os.path.exists(INITNET_CKPT):
         return None
     seeds = range(TARGET_SEED0 + 1000 * rank, TARGET_SEED0 + 1000 * rank + TARGET_PAIRS)
     pairs = I.make_pairs(seeds)
-    shape = pairs[0].u.shape
-    grid = phantoms.identity_positions(shape)
+    shape = tuple(int(x) for x in pairs[0].u.shape)
     nb = 8
     net = I.InitNet(nb, I.SIZE, 0, in_channels=5)
     net.load(INITNET_CKPT)
@@ -350,16 +348,18 @@ def run_target(core, rank, dist):
             out.append((it, r))
         return out
 
+    grid32 = I.grid_and_prior(shape)[0]  # the identity grid, shared by both arms
+    xs = np.zeros((nb,) + shape + (5,), np.float32)
+
     def learned():
         regs = [I.registration(core, p, None, 3) for p in pairs]
         autotune.tune(core, regs, [shape] * len(regs), cache=cache)
         core.RegistrationBatch(regs).EM(I.EARLY_EM, -1e300, 1)
-        early = [r.get_final_locations_as_numpy_array().astype(np.float64) - grid for r in regs]
+        early = [r.get_final_locations_as_numpy_array() - grid32 for r in regs]
         init = []
         for b in range(0, len(pairs), nb):
-            xs = np.zeros((nb,) + shape + (5,), np.float32)
             for j, (p, e) in enumerate(zip(pairs[b:b + nb], early[b:b + nb])):
-                xs[j] = I.make_input(p, e)
+                I.fill_input(xs[j], p, e)
             pred = net.predict(xs)
             for j, e in enumerate(early[b:b + nb]):
                 init.append(e + I.upsample_displacement(pred[j], shape))

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 
 #include "engine.cuh"
 #include "layout.cuh"
@@ -1214,6 +1215,8 @@ RegistrationBatch::RegistrationBatch(const std::vector<Registration *> &regs) : 
     BINDER_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
     branch_.resize(regs.size(), nullptr);
     join_.resize(regs.size(), nullptr);
+    BINDER_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&done_host_), sizeof(int) * regs.size(),
+                              cudaHostAllocDefault));
     for (size_t i = 0; i < regs.size(); ++i) {
         BINDER_CUDA(cudaStreamCreateWithFlags(&branch_[i], cudaStreamNonBlocking));
         BINDER_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
@@ -1228,6 +1231,7 @@ RegistrationBatch::~RegistrationBatch() {
     }
     if (fork_) cudaEventDestroy(fork_);
     if (master_) cudaStreamDestroy(master_);
+    if (done_host_) cudaFreeHost(done_host_);
 }
 
 void RegistrationBatch::em(int max_iterations, double th, int update, int *its_out) {
@@ -1236,7 +1240,14 @@ void RegistrationBatch::em(int max_iterations, double th, int update, int *its_o
         return;
     }
     for (auto *r : regs_) r->em_prepare(max_iterations);
-    const int chunk = max_iterations < 8 ? max_iterations : 8;
+    // iterations per graph: capturing and instantiating a graph costs host time per node, so a
+    // large batch captures fewer iterations per chunk (at most about 32 pair-iterations per graph;
+    // a pair whose rule has fired turns its remaining kernels into no-ops)
+    const int n = (int)regs_.size();
+    int chunk = n <= 4 ? 8 : (n <= 8 ? 4 : (n <= 16 ? 2 : 1));
+    if (chunk > max_iterations) chunk = max_iterations;
+    std::vector<size_t> active(regs_.size());
+    for (size_t i = 0; i < active.size(); ++i) active[i] = i;
     Graph graph;
     const long long kernels = capture_graph(master_, graph, [&] {
         BINDER_CUDA(cudaEventRecord(fork_, master_));
@@ -1255,15 +1266,17 @@ void RegistrationBatch::em(int max_iterations, double th, int update, int *its_o
     while (true) {
         replay(graph, kernels, master_);
         launched += chunk;
-        BINDER_CUDA(cudaStreamSynchronize(master_));
         if (launched >= max_iterations) break;
-        bool all = true;
-        for (auto *r : regs_)
-            if (!r->em_done()) {
-                all = false;
-                break;
-            }
-        if (all) break;
+        // the done flags of the pairs still iterating, in one round trip
+        for (size_t i : active)
+            BINDER_CUDA(cudaMemcpyAsync(&done_host_[i], regs_[i]->done_flag(), sizeof(int),
+                                        cudaMemcpyDeviceToHost, master_));
+        BINDER_CUDA(cudaStreamSynchronize(master_));
+        std::vector<size_t> left;
+        for (size_t i : active)
+            if (!done_host_[i]) left.push_back(i);
+        if (left.empty()) break;
+        active.swap(left);
     }
     BINDER_CUDA(cudaEventRecord(t1, master_));
     BINDER_CUDA(cudaEventSynchronize(t1));

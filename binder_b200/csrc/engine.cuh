@@ -143,6 +143,8 @@ class Registration {
     void set_precision(int p);
     double last_elapsed_ms() const { return last_ms_; }
     cudaStream_t stream() const { return stream_; }
+    // the device flag the EM bookkeeping sets once this object's convergence rule fires
+    const int *done_flag() const { return &st_->done; }
     // average ms per launch of stage 0 (E-step), 1 (M-step) or 2 (theta update), n eager launches
     double profile_stage(int stage, int n);
 
@@ -249,6 +251,7 @@ class RegistrationBatch {
     std::vector<cudaStream_t> branch_;
     cudaEvent_t fork_ = nullptr;
     std::vector<cudaEvent_t> join_;
+    int *done_host_ = nullptr;  // page-locked copies of the pairs' done flags
     double last_ms_ = 0.0;
 };
 

@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import functools
 import time
 
 import numpy as np
@@ -169,16 +170,24 @@ def make_pair(seed, size=SIZE):
     return phantoms.make_pair((size,) * 3, seed, bins=BINS)
 
 
-def registration(core, pair, init_displacement=None, precision=None):
-    """a Registration of the pair from the identity grid, or from identity + init_displacement"""
+@functools.lru_cache(maxsize=8)
+def grid_and_prior(shape):
+    """the identity grid [*shape, 3] and the prior's DCT-domain field of a shape (FP32; callers
+    do not modify them), computed once per shape: a batch of pairs of one size shares them"""
     from . import phantoms
     from .utils import initialize_fourier_domain_smoothing
-    shape = pair.u.shape
-    V = int(np.prod(shape))
     grid = phantoms.identity_positions(shape).astype(np.float32)
+    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
+    return grid, D
+
+
+def registration(core, pair, init_displacement=None, precision=None):
+    """a Registration of the pair from the identity grid, or from identity + init_displacement"""
+    shape = tuple(int(s) for s in pair.u.shape)
+    V = int(np.prod(shape))
+    grid, D = grid_and_prior(shape)
     start = grid if init_displacement is None else \
         (grid + np.asarray(init_displacement, np.float32)).astype(np.float32)
-    D = initialize_fourier_domain_smoothing(shape, True, 2, 3).astype(np.float32)
     g = GAMMA_INIT * V
     reg = core.Registration(start, 1, grid, grid, *shape, *shape, 3,
                             float(np.count_nonzero(pair.u)))
@@ -248,6 +257,19 @@ def make_input(pair, early=None):
     if early is None:
         return x
     return np.concatenate([x, np.asarray(early, np.float32)], -1)
+
+
+def fill_input(out, pair, early):
+    """make_input(pair, early) of the EM-seeded form written into out [S, S, S, 5] (a slot of a
+    batch buffer), without the intermediate arrays"""
+    mv = pair.moving
+    fx = pair.fixed
+    out[..., 0] = mv
+    out[..., 0] /= max(float(mv.max()), 1e-6)
+    np.clip(fx, 0.0, None, out=out[..., 1])
+    out[..., 1] /= max(float(fx.max()), 1e-6)
+    out[..., 2:] = early
+    return out
 
 
 def training_set(core, seeds, size=SIZE, seeded=False):
