@@ -254,6 +254,23 @@ class Registration:
         check(lib().binder_registration_set_dream_locations(
             self._h, _f32(dream_locations, self._V * self._N, "dream_locations")))
 
+    def add_displacement(self, field, shape=None):
+        """Positions += the order-1 resize of a displacement field [fx, fy, fz, N] (numpy, FP32)
+        to the voxel grid (no counterpart in the reference); a device buffer can be given as an
+        integer address with its `shape` (fx, fy, fz).  Theta and the other state are kept."""
+        if isinstance(field, int):
+            fx, fy, fz = (int(v) for v in shape)
+            ptr = C.c_void_p(field)
+        else:
+            f = np.ascontiguousarray(field, np.float32)
+            if f.ndim == 3 and self._N == 2:
+                f = f[:, :, None, :]
+            if f.ndim != 4 or f.shape[-1] != self._N:
+                raise ValueError(f"field must be [fx, fy, fz, {self._N}]")
+            fx, fy, fz = f.shape[:3]
+            ptr = f.ctypes.data_as(C.c_void_p)
+        check(lib().binder_registration_add_displacement(self._h, ptr, int(fx), int(fy), int(fz)))
+
     def get_likelihood_parameters(self):
         if self._K is None:
             raise BinderError(4, "setMILikelihood has not been called")

@@ -25,8 +25,8 @@ EXPORTS = [
     "binder_registration_set_ssd_likelihood_filter", "binder_registration_get_ssd_filter_parameters",
     "binder_registration_em", "binder_registration_sampler", "binder_registration_sampler_chains",
     "binder_registration_get_final_locations", "binder_registration_get_dream_locations",
-    "binder_registration_set_dream_locations", "binder_registration_get_likelihood_parameters",
-    "binder_registration_get_shape", "binder_registration_get_iteration_stats",
+    "binder_registration_set_dream_locations", "binder_registration_add_displacement",
+    "binder_registration_get_likelihood_parameters", "binder_registration_get_shape", "binder_registration_get_iteration_stats",
     "binder_registration_get_state", "binder_registration_last_elapsed_ms",
     "binder_registration_set_stream", "binder_registration_set_chain",
     "binder_registration_reset", "binder_registration_correct_topology",
@@ -88,6 +88,7 @@ def _declare(lib):
         "binder_registration_get_final_locations": [_P, _f32],
         "binder_registration_get_dream_locations": [_P, _f32],
         "binder_registration_set_dream_locations": [_P, _f32],
+        "binder_registration_add_displacement": [_P, _P, _i, _i, _i],
         "binder_registration_get_likelihood_parameters": [_P, _f32],
         "binder_registration_get_shape": [_P, _i32],
         "binder_registration_get_iteration_stats": [_P, _f64, _i, C.POINTER(_i)],

@@ -247,6 +247,15 @@ int binder_registration_set_dream_locations(binder_registration *h, const float 
     });
 }
 
+int binder_registration_add_displacement(binder_registration *h, const float *field, int Nx_f,
+                                         int Ny_f, int Nz_f) {
+    return guard([&] {
+        NEED(h);
+        NEED(field);
+        h->impl->add_displacement(field, Nx_f, Ny_f, Nz_f);
+    });
+}
+
 int binder_registration_get_likelihood_parameters(const binder_registration *h, float *out) {
     return guard([&] {
         NEED(h);

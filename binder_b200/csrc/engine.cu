@@ -10,6 +10,7 @@
 #include "engine.cuh"
 #include "layout.cuh"
 #include "mstep2d.cuh"
+#include "resample.cuh"
 
 namespace binder {
 
@@ -1159,6 +1160,11 @@ void Registration::set_dream_locations(const float *in) {
                                 stream_));
     launch_aos_minus_to_soa(mstep_.t1, x_, grid_dims(), r_, stream_);
     BINDER_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Registration::add_displacement(const float *field, int fx, int fy, int fz) {
+    BINDER_CHECK((N_ == 2) == (fz == 1), "a 2D registration takes a 2D field (fz == 1)");
+    add_resized_displacement(field, fx, fy, fz, N_, nx_, ny_, nz_, d_, stream_);
 }
 
 void Registration::get_likelihood_parameters(float *out) const {

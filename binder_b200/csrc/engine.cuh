@@ -133,6 +133,9 @@ class Registration {
     void set_final_locations(const float *in);
     void get_dream_locations(float *out) const;      // AoS [V][3]
     void set_dream_locations(const float *in);
+    // positions += the order-1 resize of a displacement field on an fx x fy x fz grid (AoS FP32
+    // [fx][fy][fz][N], host or device memory); theta and the other state are kept
+    void add_displacement(const float *field, int fx, int fy, int fz);
     void get_likelihood_parameters(float *out) const;  // [K*L]
     void get_shape(int out[4]) const;
     int get_iteration_stats(double *out, int max_n) const;  // [n][4]: mll, lp_lik, lp_tr, mlp

@@ -230,6 +230,40 @@ void host_resample(Resampler::Kind kind, const double *field, const int in[3], c
 }
 }  // namespace
 
+namespace {
+__global__ void f32_to_f64_kernel(const float *in, double *out, long n) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (long)gridDim.x * blockDim.x)
+        out[q] = (double)in[q];
+}
+
+__global__ void add_aos_to_soa_kernel(const double *aos, long V, int N, float *soa) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
+         i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < N; ++c) soa[c * V + i] += (float)aos[i * N + c];
+}
+}  // namespace
+
+void add_resized_displacement(const float *field, int fx, int fy, int fz, int N, int nx, int ny,
+                              int nz, float *soa, cudaStream_t s) {
+    BINDER_CHECK(fx >= 1 && fy >= 1 && fz >= 1, "the field's dimensions must be positive");
+    BINDER_CHECK(N >= 1 && N <= 3, "fields have 1 to 3 components");
+    const long Vf = (long)fx * fy * fz, V = (long)nx * ny * nz;
+    const int in[3] = {fx, fy, fz}, o[3] = {nx, ny, nz};
+    DBuf<float> f32(Vf * N, s);
+    DBuf<double> f64(Vf * N, s), up(V * N, s);
+    BINDER_CUDA(cudaMemcpyAsync(f32.p, field, sizeof(float) * Vf * N, cudaMemcpyDefault, s));
+    count_launch(), f32_to_f64_kernel<<<blocks_for(Vf * N), 256, 0, s>>>(f32.p, f64.p, Vf * N);
+    BINDER_CUDA(cudaGetLastError());
+    {
+        Resampler rs(Resampler::kLinear, in, o, N, s);
+        rs.apply(f64.p, up.p, s);
+        count_launch(), add_aos_to_soa_kernel<<<blocks_for(V), 256, 0, s>>>(up.p, V, N, soa);
+        BINDER_CUDA(cudaGetLastError());
+        BINDER_CUDA(cudaStreamSynchronize(s));  // the resampler's matrices go with it
+    }
+}
+
 void up_sample(const double *field, int nx, int ny, int nz, int mx, int my, int mz, double *out) {
     BINDER_CHECK(nx >= 1 && ny >= 1 && nz >= 1, "input dimensions must be positive");
     BINDER_CHECK(mx >= nx && my >= ny && mz >= nz,

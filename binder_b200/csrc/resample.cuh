@@ -52,6 +52,12 @@ class Resampler {
     cudaStream_t s_;
 };
 
+// soa [N][nx*ny*nz] (FP32, device) += the order-1 resize (resize_linear, scale 1) of the AoS FP32
+// displacement field [fx][fy][fz][N] (host or device memory) to the nx x ny x nz grid; stream s
+// (synchronised before returning)
+void add_resized_displacement(const float *field, int fx, int fy, int fz, int N, int nx, int ny,
+                              int nz, float *soa, cudaStream_t s);
+
 // Host-to-host entry points (own stream, device buffers from the pool).
 // NonLinearTransformation.up_sample: N = 2 when mz == 1
 void up_sample(const double *field, int nx, int ny, int nz, int mx, int my, int mz, double *out);

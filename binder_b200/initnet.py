@@ -12,8 +12,10 @@ benchmark's phantoms are: random-ellipsoid phantoms warped by prior-sampled defo
 registered by the plain method (FP32 DCT passes, from the identity, to convergence) -- the
 network learns the field the method itself converges to.
 
-Recipe (a checkpoint is an .npz of the FP32 parameters):
-    python -m binder_b200.initnet --out initnet.npz --pairs 512 --steps 1500
+Recipe of the shipped checkpoint (binder_b200/data/initnet_seeded_64.npz: BF16 convolution
+weights, FP32 biases):
+    python -m binder_b200.initnet --seeded --pairs 512 --steps 3000 --lr 5e-4 --warmup 300 \
+        --evaluate 16 --out initnet_seeded_64.npz
 """
 from __future__ import annotations
 
@@ -294,14 +296,31 @@ def training_set(core, seeds, size=SIZE, seeded=False):
     return np.stack(xs), np.stack(ts)
 
 
-def learned_registration(core, net, pair, precision=3):
+def predict_coarse(net, pair, early):
+    """the network's coarse displacement [S/4, S/4, S/4, 3] for one pair (EM-seeded form)"""
+    x = np.zeros((net.batch,) + tuple(pair.u.shape) + (net.in_channels,), np.float32)
+    fill_input(x[0], pair, early)
+    return net.predict(x)[0]
+
+
+def learned_registration(core, net, pair, precision=3, max_iter=MAX_EM, th=CONVERGENCE):
     """registration seeded by the network: (total EM iterations, final displacement, final
-    min-log-posterior per voxel, Registration).  EM-seeded networks (5 input channels) run
-    EARLY_EM plain iterations first, whose count is included."""
+    min-log-posterior per voxel, Registration).  EM-seeded networks (5 input channels): EARLY_EM
+    plain iterations from the identity, the network's coarse prediction added to the positions
+    of the same registration (add_displacement, order-1 resize), then EM to convergence with
+    `precision` passes, theta carried on -- the run the training targets come from; the early
+    iterations are counted."""
     if net.in_channels == 5:
-        _, early = early_em(core, pair)
-        init = early + predict_displacement(net, pair, early)
-        it, disp, mlp, reg = refine(core, pair, init_displacement=init, precision=precision)
+        shape = tuple(int(s) for s in pair.u.shape)
+        grid = grid_and_prior(shape)[0]
+        reg = registration(core, pair, None, 0)
+        reg.EM(EARLY_EM, -1e300, 1, 0)
+        early = reg.get_final_locations_as_numpy_array() - grid
+        reg.add_displacement(predict_coarse(net, pair, early))
+        reg.set_precision(precision)
+        it = reg.EM(max_iter, th, 1, 0)
+        disp = reg.get_final_locations_as_numpy_array().astype(np.float64) - grid
+        mlp = float(reg.iteration_stats()[-1, 3] / np.count_nonzero(pair.u))
         return EARLY_EM + it, disp, mlp, reg
     init = predict_displacement(net, pair)
     return refine(core, pair, init_displacement=init, precision=precision)

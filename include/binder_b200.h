@@ -165,6 +165,14 @@ int binder_registration_get_final_locations(const binder_registration *h, float 
 /* get_dream_locations() / set_dream_locations(arr)              gpu/bindings.cpp:133-140 */
 int binder_registration_get_dream_locations(const binder_registration *h, float *out);
 int binder_registration_set_dream_locations(binder_registration *h, const float *in);
+/* No counterpart in the reference: adds to the current positions a displacement field given on
+ * an Nx_f x Ny_f x Nz_f grid (AoS FP32 [Nx_f][Ny_f][Nz_f][N], host or device memory), resampled
+ * to the voxel grid by the order-1 resize of binder_resize_linear (Nz_f == 1 for a 2D
+ * registration).  Theta, the likelihood and prior state are kept, so EM continues from the
+ * moved positions (the learned initialiser's coarse prediction; reset() still restores the
+ * creation-time positions). */
+int binder_registration_add_displacement(binder_registration *h, const float *field, int Nx_f,
+                                         int Ny_f, int Nz_f);
 /* get_likelihood_parameters() -> K*L (M*K*L with the filter likelihood, (scale, shift) with
  * SSD)                                                                 gpu/bindings.cpp:97 */
 int binder_registration_get_likelihood_parameters(const binder_registration *h, float *out);

@@ -72,3 +72,33 @@ def test_resize_linear_matches_restatement(core, oracle, shape, oshape, scale):
     ref = oracle.resize_linear(f, oshape, scale)
     assert out.shape == ref.shape
     np.testing.assert_allclose(out, ref, rtol=0, atol=1e-11 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,fshape", [((20, 24, 16), (5, 6, 4)), ((18, 14, 1), (6, 7, 1))])
+def test_add_displacement_equals_resized_start(core, shape, fshape):
+    """Registration.add_displacement (the positions moved by the order-1 resize of a coarse
+    field, on the device) equals a registration created at identity + resize_linear(field), and
+    keeps theta; a 2D registration takes a field with fz == 1."""
+    rng = np.random.default_rng(3)
+    N = 2 if shape[2] == 1 else 3
+    grid = np.stack(np.indices(shape), -1).astype(np.float32)[..., :N]
+    field = rng.normal(0.0, 1.5, fshape + (N,)).astype(np.float32)
+    up = core.resize_linear(field.reshape(fshape[:N] + (N,)).astype(np.float64), shape[:N])
+    up = up.reshape(shape + (N,))
+    V = int(np.prod(shape))
+    K = 8
+    bins = rng.integers(0, K, V).astype(np.int32)
+
+    def make(start):
+        r = core.Registration(start, 1, grid, grid, *shape, *shape, 3, float(V))
+        r.setMILikelihood(2.0, np.full((K, K), 1.0 / K, np.float32), K, K, 1, bins, bins)
+        return r
+
+    a = make(grid)
+    a.add_displacement(field)
+    b = make((grid + up.astype(np.float32)).astype(np.float32))
+    np.testing.assert_allclose(a.get_final_locations_as_numpy_array(),
+                               b.get_final_locations_as_numpy_array(), rtol=0, atol=2e-5)
+    np.testing.assert_array_equal(a.get_likelihood_parameters(), np.full(K * K, 1.0 / K,
+                                                                         np.float32))
