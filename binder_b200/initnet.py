@@ -14,8 +14,8 @@ network learns the field the method itself converges to.
 
 Recipe of the shipped checkpoint (binder_b200/data/initnet_seeded_64.npz: BF16 convolution
 weights, FP32 biases):
-    python -m binder_b200.initnet --seeded --pairs 512 --steps 3000 --lr 5e-4 --warmup 300 \
-        --evaluate 16 --out initnet_seeded_64.npz
+    python -m binder_b200.initnet --seeded --pairs 2048 --steps 8000 --batch 8 --lr 5e-4 \
+        --warmup 500 --evaluate 16 --out initnet_seeded_64.npz
 """
 from __future__ import annotations
 

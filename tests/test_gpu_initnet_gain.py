@@ -2,15 +2,16 @@
 
 The committed checkpoint (binder_b200/data/initnet_seeded_64.npz, from the recipe in
 binder_b200/initnet.py) is the EM-seeded network: it sees the moving and fixed images and the
-displacement after 16 plain iterations, and predicts the rest of the way.  On 8 held-out 64^3
+displacement after 16 plain iterations, and predicts the rest of the way, which is added to the
+same registration's positions before its EM continues.  On 8 held-out 64^3
 pairs (seeds 900000..900007, never trained on) the registration seeded by it is compared with the
 plain method from the identity, both run to the reference CLI's convergence rule: fewer EM
 iterations in total (the 16 early ones included), a final mutual information (FP64, soft joint
 histogram) no lower than 1e-3 relative below the plain method's, and no more negative Jacobians
 in the pipeline's output, i.e. after the topology correction the reference's FastRegistration
 applies once EM is done (its defaults).  Before that correction the learned arm's fields fold in
-more voxels than the plain method's (a higher-MI optimum; measured: 29,492 against 27,205 voxels
-over the 8 pairs); the counts are printed."""
+a few percent more voxels than the plain method's (a higher-MI optimum); the counts are
+printed."""
 import os
 
 import numpy as np
