@@ -741,16 +741,17 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
     cudaEvent_t t0, t1;
     BINDER_CUDA(cudaEventCreate(&t0));
     BINDER_CUDA(cudaEventCreate(&t1));
+    // iterations between two reads of the device state; the graph holds ONE iteration, replayed
+    // chunk times (capturing and instantiating costs host time per node, and a new object's
+    // first EM call pays it), and is kept for the next call with the same parameters and buffers
     const int chunk = max_iterations < 8 ? max_iterations : 8;
-    // the captured chunk is kept for the next call with the same parameters and buffers
     EmGraphCache &gc = em_graph_;
-    if (!gc.e || gc.chunk != chunk || gc.max_iter != max_iterations || gc.update != update ||
+    if (!gc.e || gc.max_iter != max_iterations || gc.update != update ||
         gc.th != convergence_th || gc.stream != stream_ || gc.stats != stats_) {
         gc.clear();
         Graph graph;
         gc.kernels = capture_graph(stream_, graph, [&] {
-            for (int c = 0; c < chunk; ++c)
-                enqueue_em_iteration(max_iterations, convergence_th, update, stream_);
+            enqueue_em_iteration(max_iterations, convergence_th, update, stream_);
         });
         gc.g = graph.g;
         gc.e = graph.e;
@@ -769,9 +770,12 @@ int Registration::em(int max_iterations, double convergence_th, int update, int 
     DevState h{};
     int launched = 0;
     while (true) {
-        BINDER_CUDA(cudaGraphLaunch(gc.e, stream_));
-        count_launch(kernels);
-        launched += chunk;
+        const int n = max_iterations - launched < chunk ? max_iterations - launched : chunk;
+        for (int c = 0; c < n; ++c) {
+            BINDER_CUDA(cudaGraphLaunch(gc.e, stream_));
+            count_launch(kernels);
+        }
+        launched += n;
         BINDER_CUDA(cudaMemcpyAsync(&h, st_, sizeof(DevState), cudaMemcpyDeviceToHost, stream_));
         BINDER_CUDA(cudaStreamSynchronize(stream_));
         if (h.done || launched >= max_iterations) break;
@@ -832,7 +836,8 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
         const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
         const double rho_p = rho_[0] * rho_[1] * rho_[2];
         const int every = sample_gamma_every < 1 ? 1 : sample_gamma_every;
-        const int chunk = total < 16 ? total : 16;
+        // one sweep per graph, replayed `total` times (capture costs host time per node)
+        const int chunk = 1;
         Graph graph;
         const long long kernels = capture_graph(stream_, graph, [&] {
             for (int c = 0; c < chunk; ++c) {
@@ -968,7 +973,7 @@ void Registration::sampler_chains(uint64_t seed, int chains, int N_b, int N_s, i
         const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
         const double rho_p = rho_[0] * rho_[1] * rho_[2];
         const int every = sample_gamma_every < 1 ? 1 : sample_gamma_every;
-        const int chunk = total < 16 ? total : 16;
+        const int chunk = 1;  // one sweep of every chain per graph, replayed `total` times
         EStepArgs e = estep_args(&b.st->done);
         e.d = b.d; e.r = b.r; e.theta = b.theta; e.hcnt = b.hcnt; e.st = b.st; e.seed = seed;
         Graph graph;
@@ -1246,12 +1251,10 @@ void RegistrationBatch::em(int max_iterations, double th, int update, int *its_o
         return;
     }
     for (auto *r : regs_) r->em_prepare(max_iterations);
-    // iterations per graph: capturing and instantiating a graph costs host time per node, so a
-    // large batch captures fewer iterations per chunk (at most about 32 pair-iterations per graph;
-    // a pair whose rule has fired turns its remaining kernels into no-ops)
-    const int n = (int)regs_.size();
-    int chunk = n <= 4 ? 8 : (n <= 8 ? 4 : (n <= 16 ? 2 : 1));
-    if (chunk > max_iterations) chunk = max_iterations;
+    // the graph holds ONE iteration of every pair (capturing and instantiating costs host time
+    // per node), replayed up to 8 times between two reads of the pairs' done flags; a pair whose
+    // rule has fired turns its remaining kernels into no-ops
+    const int chunk = 8;
     std::vector<size_t> active(regs_.size());
     for (size_t i = 0; i < active.size(); ++i) active[i] = i;
     Graph graph;
@@ -1259,7 +1262,7 @@ void RegistrationBatch::em(int max_iterations, double th, int update, int *its_o
         BINDER_CUDA(cudaEventRecord(fork_, master_));
         for (size_t i = 0; i < regs_.size(); ++i) {
             BINDER_CUDA(cudaStreamWaitEvent(branch_[i], fork_, 0));
-            regs_[i]->enqueue_em(chunk, max_iterations, th, update, branch_[i]);
+            regs_[i]->enqueue_em(1, max_iterations, th, update, branch_[i]);
             BINDER_CUDA(cudaEventRecord(join_[i], branch_[i]));
             BINDER_CUDA(cudaStreamWaitEvent(master_, join_[i], 0));
         }
@@ -1270,8 +1273,9 @@ void RegistrationBatch::em(int max_iterations, double th, int update, int *its_o
     BINDER_CUDA(cudaEventRecord(t0, master_));
     int launched = 0;
     while (true) {
-        replay(graph, kernels, master_);
-        launched += chunk;
+        const int n = max_iterations - launched < chunk ? max_iterations - launched : chunk;
+        for (int c = 0; c < n; ++c) replay(graph, kernels, master_);
+        launched += n;
         if (launched >= max_iterations) break;
         // the done flags of the pairs still iterating, in one round trip
         for (size_t i : active)
