@@ -907,79 +907,6 @@ class captured_stdout:
         sys.stderr.write(self.text[-4000:])
 
 
-REF_GPU_NOTE = ("the reference's CUDA backend (BINDER/src/gpu: its five .cu files and pybind11 "
-                "bindings compiled unmodified for sm_100a in oracle/_ref/gpu)")
-
-
-def ref_gpu_module():
-    """the reference's CUDA backend module built in oracle/_ref/gpu, or None"""
-    import glob
-    import importlib.util
-    paths = glob.glob(os.path.join(ROOT, "oracle", "_ref", "gpu", "_core*.so"))
-    if not paths:
-        return None
-    spec = importlib.util.spec_from_file_location("_core", paths[0])
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod
-
-
-def run_reference_gpu(inp, em_iters, dist, reps=2):
-    """The reference's own CUDA backend on this B200 and the same C2 inputs, through its own
-    pybind11 API in FastRegistration.run's order: Registration, setMILikelihood,
-    setNonLinearTransformation, EM (em_iters iterations, convergence off), the final positions,
-    its GPU topology correction.  Wall time per registration after one warm-up (its EM
-    synchronises and prints every iteration, so the time is its implementation's), and the E-step
-    and M-step milliseconds it prints per iteration (means of iterations 2..)."""
-    import re
-
-    import torch
-    ref = ref_gpu_module()
-    if ref is None:
-        return None
-    pair, grid, D = inp["pair"], inp["grid"].ravel(), inp["D"].ravel()
-    v, u = pair.v.ravel().astype(np.int32), pair.u.ravel().astype(np.int32)
-    vs = np.ones(3, np.float32)
-    walls, em_walls, es, ms = [], [], [], []
-    for rep in range(reps + 1):
-        torch.cuda.synchronize()
-        barrier(dist)
-        with captured_stdout() as c:
-            t0 = time.perf_counter()
-            r = ref.Registration(grid, 1, grid, grid, *SHAPE, *SHAPE, 3, inp["nzv"])
-            r.setMILikelihood(ALPHA, inp["theta"].ravel(), BINS, BINS, 1, v, u)
-            r.setNonLinearTransformation(*inp["gamma"], 1, 1, 1, 1, 1, 1, D)
-            t1 = time.perf_counter()
-            r.EM(em_iters, -1e30, 1, 0)
-            fin = np.asarray(r.get_final_locations_as_numpy_array(), np.float32)
-            t2 = time.perf_counter()
-            out = ref.topology_correction_3D().correct_topology(
-                fin.ravel(), TOPO["e1"], TOPO["e2"], TOPO["max_outer"], TOPO["max_inner"], 1, vs,
-                *SHAPE)
-            np.asarray(out)
-            torch.cuda.synchronize()
-            t3 = time.perf_counter()
-        del r
-        if rep == 0:
-            continue
-        walls.append(t3 - t0)
-        em_walls.append(t2 - t1)
-        es += [float(x) for x in re.findall(
-            r"Time estimating posterior and updating likelihood \(ms\): ([0-9.eE+-]+)", c.text)][1:]
-        ms += [float(x) for x in re.findall(
-            r"Time updating transformation \(ms\): ([0-9.eE+-]+)", c.text)][1:]
-    wall = max_over_ranks(float(np.mean(walls)), dist)
-    world = dist.get_world_size() if dist is not None else 1
-    return {"metric": metric(em_iters) + " by the reference's own CUDA backend on this GPU",
-            "value": world / wall, "unit": "registrations/s", "ms_per_registration": 1e3 * wall,
-            "em_ms": 1e3 * float(np.mean(em_walls)),
-            "estep_ms_per_iteration": float(np.mean(es)) if es else None,
-            "mstep_ms_per_iteration": float(np.mean(ms)) if ms else None,
-            "kind": "reference", "repeats": reps,
-            "note": REF_GPU_NOTE + "; wall time of set-up, EM, read-back and topology correction "
-                    "through its Python API (FP32 throughout; its sigma_spline 0.6)"}
-
-
 def cpu_em_phases(inp, threads, iters):
     """The reference's own EM driver on the C2 pair for `iters` iterations (all host cores): the
     EM call's wall seconds and the per-iteration E-step ("Time updating theta and dream
