@@ -170,10 +170,15 @@ int default_precision() {
     return kPrecBF16x3;
 }
 
+void MStep::prepare_sampling(cudaStream_t s) {
+    if (!noise) noise = dalloc<float>((size_t)V * 3 * chains, s);
+}
+
 void MStep::release(cudaStream_t s) {
     dct.release(s);
     dfree(t1, s);
     dfree(t2, s);
+    dfree(noise, s);
     for (int i = 0; i < 2; ++i) {
         if (side[i]) cudaStreamSynchronize(side[i]), cudaStreamDestroy(side[i]);
         if (join[i]) cudaEventDestroy(join[i]);
@@ -210,6 +215,14 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     for (int n = 0; n < 3; ++n) a.eta2[n] = eta2[n];
     const bool tc = precision != kPrecFP32Simt;
     const int planes = (precision == kPrecTF32 || precision == kPrecBF16) ? 1 : 2;
+    const bool bf16 = precision == kPrecBF16x3 || precision == kPrecBF16;
+    // the per-tile tensor-core passes read the prior noise drawn beforehand (the persistent and
+    // CUDA-core passes draw it per element)
+    if (sample && tc && noise && !(persistent && !bf16)) {
+        launch_prior_noise(noise, V, ncomp * chains, chains > 1 ? ncomp : 0, seed, chain, st, skip,
+                           s);
+        a.noise = noise;
+    }
     if (chains > 1) {
         // chains x components per launch: enough tiles to fill the GPU without stream branches
         a.chain_comps = ncomp;
@@ -832,6 +845,10 @@ void Registration::sampler(uint64_t seed, int N_b, int N_s, int sample_gamma,
     BINDER_CUDA(cudaMemsetAsync(m2_, 0, sizeof(double) * V_ * NM2, stream_));
     reset_state(true);
     const int total = N_b + N_s;
+    if (total > 0 && sample_transformation_parameters) {
+        mstep_.prepare_sampling(own_stream_);
+        BINDER_CUDA(cudaStreamSynchronize(own_stream_));
+    }
     if (total > 0) {
         const double eta2[3] = {eta_[0] * eta_[0], eta_[1] * eta_[1], eta_[2] * eta_[2]};
         const double rho_p = rho_[0] * rho_[1] * rho_[2];
@@ -943,6 +960,10 @@ void Registration::sampler_chains(uint64_t seed, int chains, int N_b, int N_s, i
         BINDER_CUDA(cudaStreamSynchronize(so));
     }
     cb_->mstep.precision = mstep_.precision;
+    if (sample_transformation_parameters) {
+        cb_->mstep.prepare_sampling(own_stream_);
+        BINDER_CUDA(cudaStreamSynchronize(own_stream_));
+    }
     ChainBatch &b = *cb_;
     // every chain starts from the object's positions, dream locations, theta and gammas
     for (int c = 0; c < C; ++c) {

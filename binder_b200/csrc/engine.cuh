@@ -40,8 +40,13 @@ struct MStep {
     // a batch of chains: every pass runs over chains x components in one launch (per-tile
     // tensor-core passes or the SIMT passes), the scratch holds [chains][3][V]
     int chains = 1;
+    // the sampler's prior noise of every coefficient, [chains][3][V] (prepare_sampling; null
+    // until a sampler call needs it): drawn by one fully occupied kernel before the passes, so
+    // the tensor-core epilogue only reads it
+    float *noise = nullptr;
     // buffers from the stream-ordered pool on stream s
     void init(int nx, int ny, int nz, cudaStream_t s, int chains = 1);
+    void prepare_sampling(cudaStream_t s);
     void release(cudaStream_t s);
     void enqueue(const float *r, float *d, const float *xpos, const float *D, DevState *st,
                  double sigma2, int sample, int want_raw, int every, uint64_t seed, uint32_t chain,

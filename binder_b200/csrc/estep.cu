@@ -1598,8 +1598,9 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
     BINDER_CHECK(chains >= 1 && chains <= 65535 && (chains == 1 || (sample && !a.logt)),
                  "a batch of chains runs the sampling E-step of the MI likelihood only");
     if (chains > 1) {
-        // the single-chain grid shared out over the chains (every CTA still loops over voxels)
-        const int gx = (grid + chains - 1) / chains;
+        // the single-chain grid (one wave of CTAs) shared out over the chains, rounded down so all
+        // of them are resident at once (every CTA loops over its chain's voxels)
+        const int gx = grid / chains > 0 ? grid / chains : 1;
         const dim3 g2((unsigned)gx, (unsigned)chains, 1);
         if (a.dim == 3)
             count_launch(), estep_kernel<true, 3><<<g2, kEThreads, smem, s>>>(a);

@@ -344,4 +344,42 @@ void hartley_matrix(int n, double *out) {
         }
 }
 
+namespace {
+__global__ void prior_noise_kernel(float *noise, long V, int ncomp, int chain_comps,
+                                   uint64_t seed, uint32_t chain0, const DevState *st,
+                                   const int *skip) {
+    if (skip && *skip) return;
+    const int per = chain_comps ? chain_comps : ncomp;  // components per chain
+    const int chains = ncomp / per;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < V * chains;
+         q += (long)gridDim.x * blockDim.x) {
+        const int ch = (int)(q / V);
+        const uint32_t i = (uint32_t)(q - (long)ch * V);
+        const uint32_t sweep = (uint32_t)st[chain_comps ? ch : 0].sweep;
+        const uint32_t chain = chain0 + (uint32_t)(chain_comps ? ch : 0);
+        float *out = noise + (long)ch * per * V + i;
+        // components 0 and 1: the cosine and the sine of one Box-Muller pair (tag 2)
+        const u32x4 r = philox_draw(seed, i, sweep, 2u, chain);
+        const float u1 = u01_f24(r.x), u2 = u01_f24(r.y);
+        const float rad = sqrtf(-2.0f * logf(u1));
+        float sn, cs;
+        sincospif(2.0f * u2, &sn, &cs);
+        out[0] = rad * cs;
+        if (per > 1) out[V] = rad * sn;
+        if (per > 2) out[2 * V] = dct_prior_normal(seed, i, sweep, chain, 2);
+    }
+}
+}  // namespace
+
+void launch_prior_noise(float *noise, long V, int ncomp, int chain_comps, uint64_t seed,
+                        uint32_t chain, const DevState *st, const int *skip, cudaStream_t s) {
+    const int per = chain_comps ? chain_comps : ncomp;
+    BINDER_CHECK(per >= 1 && per <= 3 && ncomp % per == 0, "noise components");
+    long b = (V * (ncomp / per) + 255) / 256;
+    b = b < 1 ? 1 : (b > 148L * 16 ? 148L * 16 : b);
+    count_launch(), prior_noise_kernel<<<(int)b, 256, 0, s>>>(noise, V, ncomp, chain_comps, seed,
+                                                             chain, st, skip);
+    BINDER_CUDA(cudaGetLastError());
+}
+
 }  // namespace binder

@@ -52,6 +52,9 @@ struct AxisArgs {
     DevState *st;
     double sigma2;
     int sample;            // add prior-sampling noise (Philox counter sweep = st->sweep)
+    // the noise precomputed by launch_prior_noise ([components][V], the launch's component
+    // index), or null: the pass then draws it per element
+    const float *noise;
     int want_raw;          // accumulate the raw regulariser when st->sweep % every == 0
     int every;
     uint64_t seed;
@@ -71,6 +74,14 @@ struct AxisArgs {
     // st[chain] and Philox chain indices chain + chain; 0 for one chain
     int chain_comps;
 };
+
+// The prior-sampling normals of every coefficient: noise[c * V + i] = dct_prior_normal(seed, i,
+// st[c / chain_comps].sweep, chain + c / chain_comps, c % chain_comps) for the ncomp components
+// of a launch (chain_comps 0: one chain, ncomp components); components 0 and 1 share one Philox
+// draw (the cosine and the sine of one Box-Muller pair), as dct_prior_normal draws them.  A no-op
+// when *skip.
+void launch_prior_noise(float *noise, long V, int ncomp, int chain_comps, uint64_t seed,
+                        uint32_t chain, const DevState *st, const int *skip, cudaStream_t s);
 
 // Launch one pass over `ncomp` components (blockIdx.z = component).
 template <typename T>

@@ -42,6 +42,7 @@ struct UArgs {
     DevState *st;
     double sigma2;
     int sample, want_raw, every;
+    const float *noise;  // precomputed prior-sampling normals [components][V], or null
     uint64_t seed;
     uint32_t chain;
     double rho_p;
@@ -748,8 +749,10 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                             val *= f;
                             if (a.sample)
                                 val += sqrtf((float)a.sigma2 * f) *
-                                       prior_normal_tc(a.seed, (uint32_t)((long)k * a.s + t), sweep,
-                                                       chain, cn);
+                                       (a.noise ? __ldg(a.noise + comp * a.V + (long)k * a.s + t)
+                                                : prior_normal_tc(a.seed,
+                                                                  (uint32_t)((long)k * a.s + t),
+                                                                  sweep, chain, cn));
                             ccost += Dv * val * val;
                         }
                         op[(long)k * a.s] = val;
@@ -1390,6 +1393,7 @@ void launch_axis_pass_tc(const AxisArgs<float> &b, const UmmaMatrix &M1, const U
     a.B1 = bf16 ? reinterpret_cast<const float *>(M1.dev16) : M1.dev;
     a.B2 = M2 ? M2->dev : nullptr;
     a.D = b.D; a.st = b.st; a.sigma2 = b.sigma2; a.sample = b.sample; a.want_raw = b.want_raw;
+    a.noise = b.noise;
     a.every = b.every < 1 ? 1 : b.every; a.seed = b.seed; a.chain = b.chain; a.rho_p = b.rho_p;
     for (int i = 0; i < 3; ++i) a.eta2[i] = b.eta2[i];
     a.xpos = b.xpos; a.ny = b.ny; a.nz = b.nz; a.dims = b.dims; a.comp0 = b.comp0; a.skip = b.skip;

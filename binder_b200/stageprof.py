@@ -8,7 +8,8 @@ The pair is the benchmark's 3D MI workload by default (160x192x160, 64 bins, see
 3-voxel-RMS prior-sampled warp; ``binder_b200/phantoms.py``); a profiler such as ncu captures the
 stage's kernels of one run (``-k`` with the kernel's name, ``-s`` past the warm-up).  Stages:
 ``estep`` (the E-step kernel), ``mstep`` (the DCT M-step's passes), ``em`` (whole EM iterations,
-captured as CUDA graphs).  No counterpart in the reference.
+captured as CUDA graphs), ``sampler`` (Gibbs sweeps of a batch of chains, every sampling switch on,
+after 10 EM iterations; ``--chains``).  No counterpart in the reference.
 """
 from __future__ import annotations
 
@@ -38,7 +39,8 @@ def make_registration(core, shape, bins, seed):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--stage", choices=["estep", "mstep", "em"], default="estep")
+    ap.add_argument("--stage", choices=["estep", "mstep", "em", "sampler"], default="estep")
+    ap.add_argument("--chains", type=int, default=32, help="chains of the sampler stage")
     ap.add_argument("--shape", type=int, nargs=3, default=[160, 192, 160])
     ap.add_argument("--bins", type=int, default=64)
     ap.add_argument("--seed", type=int, default=20260001)
@@ -51,6 +53,14 @@ def main(argv=None):
     reg = make_registration(core, tuple(a.shape), a.bins, a.seed)
     if a.precision is not None:
         reg.set_precision(a.precision)
+    if a.stage == "sampler":
+        reg.EM(10, -1e300, 1, 0)
+        reg.sampler_chains(1, a.chains, 1, 1, 1, 1, 1, 1, 1, per_chain=False)  # warm-up
+        for _ in range(a.n):
+            reg.sampler_chains(7, a.chains, 4, 16, 1, 1, 1, 1, 1, per_chain=False)
+            ms = reg.last_elapsed_ms()
+            print(f"sampler: {ms / 20:.4f} ms per sweep of {a.chains} chains", flush=True)
+        return
     if a.stage == "em":
         reg.EM(a.warmup, -1e300, 1, 0)
         for _ in range(a.n):
