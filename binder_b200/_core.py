@@ -316,6 +316,11 @@ class Registration:
         3 tensor-core BF16 split (three products), 4 tensor-core BF16."""
         check(lib().binder_registration_set_precision(self._h, int(precision)))
 
+    def set_histogram_precision(self, precision):
+        """E-step bin columns of the MI likelihood: 0 FP32 (the default), 1 FP16 (each voxel's
+        per-bin posterior mass rounded to FP16; three CTAs per SM instead of two)."""
+        check(lib().binder_registration_set_histogram_precision(self._h, int(precision)))
+
     def set_estep_grid(self, ctas):
         """CTAs of the EM E-step launch (0: the default, every SM times its occupancy)."""
         check(lib().binder_registration_set_estep_grid(self._h, int(ctas)))

@@ -32,6 +32,7 @@ EXPORTS = [
     "binder_registration_reset", "binder_registration_correct_topology",
     "binder_kernel_launch_count", "binder_registration_get_stream",
     "binder_registration_profile_stage", "binder_registration_set_precision",
+    "binder_registration_set_histogram_precision",
     "binder_transform_set_precision",
     "binder_transform_create", "binder_transform_destroy",
     "binder_transform_smooth_deformation", "binder_transform_sample_deformation_field",
@@ -99,6 +100,7 @@ def _declare(lib):
         "binder_registration_set_chain": [_P, _u32],
         "binder_registration_reset": [_P],
         "binder_registration_set_precision": [_P, _i],
+        "binder_registration_set_histogram_precision": [_P, _i],
         "binder_transform_set_precision": [_P, _i],
         "binder_registration_get_stream": [_P, C.POINTER(_P)],
         "binder_registration_profile_stage": [_P, _i, _i, C.POINTER(_d)],

@@ -345,6 +345,13 @@ int binder_registration_set_precision(binder_registration *h, int precision) {
     });
 }
 
+int binder_registration_set_histogram_precision(binder_registration *h, int precision) {
+    return guard([&] {
+        NEED(h);
+        h->impl->set_histogram_precision(precision);
+    });
+}
+
 int binder_transform_set_precision(binder_transform *h, int precision) {
     return guard([&] {
         NEED(h);

@@ -388,9 +388,17 @@ void Registration::set_mi_likelihood(double alpha, const float *theta, int K, in
     BINDER_CHECK((long)K * L <= 24576, "K * L must be at most 24576 (shared-memory histogram)");
     load_bins(alpha, theta, K, L, 1, binned_nodes, binned_voxels);
     lk_ = 0;
-    egrid_e_ = estep_grid(false, K, L, V_, N_);
+    egrid_e_ = estep_grid(false, K, L, V_, N_, false, hist_prec_ == 1);
     egrid_s_ = estep_grid(true, K, L, V_, N_);
     have_mi_ = true;
+}
+
+void Registration::set_histogram_precision(int h) {
+    BINDER_CHECK(h == 0 || h == 1,
+                 "histogram precision must be 0 (FP32 bin columns) or 1 (FP16 bin columns)");
+    hist_prec_ = h;
+    if (lk_ == 0 && K_ > 0) egrid_e_ = estep_grid(false, K_, L_, V_, N_, false, h == 1);
+    em_graph_.clear();
 }
 
 // The MI filter likelihood (BINDER/src/cpu/Registration.cpp:466-470, MILikelihoodFilter.cpp):
@@ -671,6 +679,7 @@ EStepArgs Registration::estep_args(const int *skip) const {
     e.P = P_; e.PZ = PZ_; e.pyn = pyn_; e.zp = zp_; e.K = K_; e.L = L_; e.dim = N_;
     e.seed = seed_; e.chain = chain_; e.order = order_;
     e.logt = lk_ == 1; e.colmax = colmax_;
+    e.halfcol = lk_ == 0 ? hist_prec_ : 0;
     e.M = lk_ == 3 ? fM_ : M_; e.filter = lk_ == 2; e.uch = 1; e.vch = vch_;
     e.ssdf = lk_ == 3; e.Fn = fFn_; e.fx = fx_; e.fn = fn_; e.fstate = fst_; e.fstats = fstats_;
     return e;

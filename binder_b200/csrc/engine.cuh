@@ -149,6 +149,9 @@ class Registration {
     void set_stream(cudaStream_t s);
     void set_chain(uint32_t c);
     void set_precision(int p);
+    // E-step bin columns of the MI likelihood: 0 FP32 (the default), 1 FP16
+    void set_histogram_precision(int h);
+    int histogram_precision() const { return hist_prec_; }
     double last_elapsed_ms() const { return last_ms_; }
     cudaStream_t stream() const { return stream_; }
     // the device flag the EM bookkeeping sets once this object's convergence rule fires
@@ -226,6 +229,7 @@ class Registration {
     double sigma2_ = 0.0;
     int P_ = 8, PZ_ = 8, pyn_ = 0, zp_ = 0;
     int egrid_e_ = 0, egrid_s_ = 0;
+    int hist_prec_ = 0;  // set_histogram_precision
     uint64_t seed_ = 12345;
     int iters_done_ = 0;
     int order_ = 3;  // B-spline order of the E-step

@@ -1,6 +1,9 @@
 // E-step kernels (EM soft assignment and Gibbs categorical draw), theta updates, Dirichlet and
 // gamma-prior sampling, EM bookkeeping and FP64 Welford moments.
+#include <cuda_fp16.h>
+
 #include <cmath>
+#include <type_traits>
 
 #include "estep.cuh"
 
@@ -167,6 +170,14 @@ __host__ __device__ constexpr int theta_pitch(int K) { return K + ((9 - K % 32) 
 
 constexpr int kSmallK = 64;  // the single-pass EM kernel keeps a K-bin column per thread
 constexpr int kFastThreads = 256;
+// the single-pass EM kernel's wide form: one CTA of 24 warps per SM (FP32 columns for 768 threads
+// and the tables fill the SM's shared memory, with the tables' rows 5 banks apart so they fit)
+constexpr int kWideThreads = 768;
+__host__ __device__ constexpr int wide_pitch(int K) { return K + ((5 - K % 32) + 32) % 32; }
+template <int TPB>
+__host__ __device__ constexpr int fast_pitch(int K) {
+    return TPB > kFastThreads ? wide_pitch(K) : theta_pitch(K);
+}
 
 // The node pass of one EM voxel (4 x Q rows of 4 packed nodes; Q = 4 in 3D, 1 in 2D): weights
 // w = bx[p] by[q] bz[c] theta[k] added to the thread's private bin column col[k * TPB], their sum
@@ -174,9 +185,46 @@ constexpr int kFastThreads = 256;
 // touched.  theta and the column are disjoint regions of shared memory; the __restrict__
 // qualifiers let the compiler hoist the theta loads of later nodes above earlier column updates.
 // Products and sums run on paired FP32 lanes (nodes c = 0,1 and c = 2,3 of each packed word).
-template <int TPB, int Q>
+// FP16 bin columns (EStepArgs::halfcol): [K][TPB] halves, the thread's entry for bin k at
+// col[k * TPB], the same indexing as the FP32 columns (one shift and add per neighbour).  Lanes 2j
+// and 2j + 1 share a 32-bit word, so two such lanes updating different bins in one instruction
+// meet in a bank (a two-way conflict); a layout pairing bins 2j, 2j + 1 of one thread in a word
+// avoids that but costs more integer instructions per neighbour than the conflicts cost.  Each
+// mass is rounded to FP16 before it is added, and the sum is held in FP16.
+template <int TPB>
+__device__ __forceinline__ __half *half_slot(__half *col, int k) {
+    return col + k * TPB;
+}
+// masses w.x, w.y of two neighbours with bins ka, kb (one FP32 to FP16 pair conversion)
+template <int TPB>
+__device__ __forceinline__ void col_add2(float *__restrict__ col, int ka, int kb, float2 w) {
+    col[ka * TPB] += w.x;
+    col[kb * TPB] += w.y;
+}
+template <int TPB>
+__device__ __forceinline__ void col_add2(__half *__restrict__ col, int ka, int kb, float2 w) {
+    const __half2 h = __float22half2_rn(w);
+    __half *p = half_slot<TPB>(col, ka);
+    *p = __hadd(*p, __low2half(h));
+    __half *q = half_slot<TPB>(col, kb);
+    *q = __hadd(*q, __high2half(h));
+}
+template <int TPB>
+__device__ __forceinline__ float col_get(const float *col, int k) { return col[k * TPB]; }
+template <int TPB>
+__device__ __forceinline__ float col_get(__half *col, int k) {
+    return __half2float(*half_slot<TPB>(col, k));
+}
+template <int TPB>
+__device__ __forceinline__ void col_clear(float *col, int k) { col[k * TPB] = 0.0f; }
+template <int TPB>
+__device__ __forceinline__ void col_clear(__half *col, int k) {
+    *half_slot<TPB>(col, k) = __float2half_rn(0.0f);
+}
+
+template <int TPB, int Q, typename CT>
 __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
-                                              float *__restrict__ col, const uint32_t (&pk)[4 * Q],
+                                              CT *__restrict__ col, const uint32_t (&pk)[4 * Q],
                                               const float (&bx)[4], const float (&by)[4],
                                               const float (&bz)[4], float &S, float &Sx, float &Sy,
                                               float &Sz, int &kmin, int &kmax) {
@@ -198,10 +246,8 @@ __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
                       k3 = word >> 24;
             const float2 w01 = __fmul2_rn(b01, make_float2(thu[k0], thu[k1]));
             const float2 w23 = __fmul2_rn(b23, make_float2(thu[k2], thu[k3]));
-            col[k0 * TPB] += w01.x;
-            col[k1 * TPB] += w01.y;
-            col[k2 * TPB] += w23.x;
-            col[k3 * TPB] += w23.y;
+            col_add2<TPB>(col, k0, k1, w01);
+            col_add2<TPB>(col, k2, k3, w23);
             a01 = __fadd2_rn(a01, w01);
             a23 = __fadd2_rn(a23, w23);
             if (p == 0) { x01 = __ffma2_rn(m1, w01, x01); x23 = __ffma2_rn(m1, w23, x23); }
@@ -295,29 +341,41 @@ __device__ __forceinline__ void em_accumulate_log(const float *__restrict__ thu,
 // each addition relative to the running sum instead.  theta is staged transposed (thT[u][k]); it
 // and the histogram use a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ by
 // small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the host).
-template <int TPB, int DIM, bool LOGT>
-__global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a) {
+//
+// HC (EStepArgs::halfcol): the columns hold FP16 (half the shared memory, so three CTAs fit on an SM
+// instead of two), theta is staged multiplied by kHalfColScale so that the masses stay well inside
+// FP16's normal range, and the log-likelihood takes the scale back out.  S, the moments and the CTA
+// histogram stay FP32 / fixed point; only the per-voxel bin sums are rounded to FP16.
+constexpr float kHalfColScale = 4096.0f;
+constexpr double kLnHalfColScale = 8.317766166719343;  // ln 4096
+
+template <int TPB, int DIM, bool LOGT, bool HC = false>
+__global__ void __launch_bounds__(TPB, HC ? 3 : (TPB > kFastThreads ? 1 : 2))
+    estep_em_fast_kernel(const EStepArgs a) {
     constexpr int Q = DIM == 3 ? 4 : 1;
+    using CT = typename std::conditional<HC, __half, float>::type;
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) float sm[];
     const int K = a.K, L = a.L, KL = K * L;
-    const int KP = theta_pitch(K), LP = theta_pitch(L);
+    const int KP = fast_pitch<TPB>(K), LP = fast_pitch<TPB>(L);
     float *thT = sm;                                             // [L][KP]
     unsigned *hs = reinterpret_cast<unsigned *>(sm + L * KP);    // [K][LP] CTA histogram (fixed)
-    float *hk = sm + L * KP + K * LP;                            // [K][TPB] per-thread bin masses
-    float *cmx = hk + K * TPB;                                   // [L] log-space column maxima
+    float *hkw = sm + L * KP + K * LP;  // per-thread bin masses: [K][TPB] FP32 or FP16
+    const int hk_words = HC ? ((K + 1) / 2) * TPB : K * TPB;
+    float *cmx = hkw + hk_words;                                 // [L] log-space column maxima
     __shared__ double red[32];
     if (LOGT)
         for (int l = threadIdx.x; l < L; l += TPB) cmx[l] = a.colmax[l];
+    const float tscale = HC ? kHalfColScale : 1.0f;
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const int k = q / L, l = q - k * L;
-        thT[l * KP + k] = a.theta[q];
+        thT[l * KP + k] = a.theta[q] * tscale;
         hs[k * LP + l] = 0u;
     }
-    for (int q = threadIdx.x; q < K * TPB; q += TPB) hk[q] = 0.0f;
+    for (int q = threadIdx.x; q < hk_words; q += TPB) hkw[q] = 0.0f;
     __syncthreads();
 
-    float *my = hk + threadIdx.x;  // my[k * TPB]
+    CT *my = reinterpret_cast<CT *>(hkw) + threadIdx.x;  // my[k * TPB]
     double mll = 0.0;
     unsigned deg = 0;
     // unsigned: i + stride stays below 2^32 for any V < 2^31
@@ -340,7 +398,7 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
         float S, Sx, Sy, Sz;
         int kmin, kmax;
         float mlog = 0.0f;
-        if (LOGT)
+        if constexpr (LOGT)
             em_accumulate_log<TPB, Q>(thT + ui * KP, my, pk, bx, by, bz, S, Sx, Sy, Sz, kmin,
                                       kmax, mlog);
         else
@@ -350,10 +408,10 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
         const float invs = inv * a.hscale;
         unsigned *hcol = hs + ui;  // hcol[k * LP]
         for (int k = kmin; k <= kmax; ++k) {
-            const float m = my[k * TPB];
+            const float m = col_get<TPB>(my, k);
             if (m != 0.0f) {
                 if (ok) atomicAdd(&hcol[k * LP], __float2uint_rn(m * invs));
-                my[k * TPB] = 0.0f;
+                col_clear<TPB>(my, k);
             }
         }
         if (!ok) {
@@ -362,6 +420,7 @@ __global__ void __launch_bounds__(TPB, 2) estep_em_fast_kernel(const EStepArgs a
             continue;
         }
         mll -= (double)logf(S);  // FP32 log, FP64 accumulation
+        if (HC) mll += kLnHalfColScale;
         if (LOGT) mll -= (double)mlog * 0.6931471805599453 + (double)cmx[ui];
         vp.store_r(a, i, V, fx + Sx * inv, fy + Sy * inv, fz + Sz * inv);
     }
@@ -1388,19 +1447,46 @@ __global__ void sweep_advance_kernel(DevState *st, int total) {
 }  // namespace
 
 namespace {
-size_t estep_smem(bool sample, int K, int L, bool logt = false) {
-    if (!sample && K <= kSmallK)
-        return (size_t)(L * theta_pitch(K) + K * theta_pitch(L) + K * kFastThreads +
-                        (logt ? L : 0)) * sizeof(float);
+// shared memory of the single-pass EM kernel with tpb threads
+size_t fast_smem(int K, int L, int tpb, bool logt, bool half) {
+    const bool w = tpb > kFastThreads;
+    const int KP = w ? wide_pitch(K) : theta_pitch(K), LP = w ? wide_pitch(L) : theta_pitch(L);
+    return (size_t)(L * KP + K * LP + (half ? ((K + 1) / 2) * tpb : K * tpb) + (logt ? L : 0)) *
+           sizeof(float);
+}
+
+int device_sms() {
+    int dev = 0, sms = 148;
+    BINDER_CUDA(cudaGetDevice(&dev));
+    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+// threads per CTA of the single-pass EM kernel (MI likelihood, FP32 columns): the wide form when
+// its tables fit and one wave of it gives every thread a voxel at least, else 256 (two CTAs/SM)
+int fast_threads(long V, int K, int L, bool logt, bool half) {
+    if (logt || half || K > kSmallK) return kFastThreads;
+    if (fast_smem(K, L, kWideThreads, false, false) + 512 > 227 * 1024) return kFastThreads;
+    if (V < (long)device_sms() * kWideThreads) return kFastThreads;
+    return kWideThreads;
+}
+
+size_t estep_smem(bool sample, int K, int L, bool logt = false, bool half = false,
+                  int tpb = kFastThreads) {
+    if (!sample && K <= kSmallK) return fast_smem(K, L, tpb, logt, half);
     return (size_t)(2 * K * L + (sample ? 16 * kEThreads : 0)) * sizeof(float);
 }
 }  // namespace
 
 namespace {
 template <int DIM>
-const void *estep_fn(bool sample, int K, bool logt) {
+const void *estep_fn(bool sample, int K, bool logt, bool half, bool wide) {
     if (logt && sample) return (const void *)estep_kernel<true, DIM, true>;
     if (logt) return (const void *)estep_em_fast_kernel<kFastThreads, DIM, true>;
+    if (half && !sample && K <= kSmallK)
+        return (const void *)estep_em_fast_kernel<kFastThreads, DIM, false, true>;
+    if (wide && !sample && K <= kSmallK)
+        return (const void *)estep_em_fast_kernel<kWideThreads, DIM, false>;
     return sample ? (const void *)estep_kernel<true, DIM>
                   : (K <= kSmallK ? (const void *)estep_em_fast_kernel<kFastThreads, DIM, false>
                                   : (const void *)estep_kernel<false, DIM>);
@@ -1447,7 +1533,8 @@ void launch_ssdf_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cud
 }
 
 template <int DIM>
-void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s) {
+void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cudaStream_t s,
+                      int ftpb) {
     if (a.ssdf)
         launch_ssdf_dim<DIM>(a, sample, grid, smem, s);
     else if (a.filter && sample)
@@ -1461,6 +1548,12 @@ void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cu
                             <<<grid, kFastThreads, smem, s>>>(a);
     else if (sample)
         count_launch(), estep_kernel<true, DIM><<<grid, kEThreads, smem, s>>>(a);
+    else if (a.K <= kSmallK && a.halfcol)
+        count_launch(), estep_em_fast_kernel<kFastThreads, DIM, false, true>
+                            <<<grid, kFastThreads, smem, s>>>(a);
+    else if (a.K <= kSmallK && ftpb == kWideThreads)
+        count_launch(), estep_em_fast_kernel<kWideThreads, DIM, false>
+                            <<<grid, kWideThreads, smem, s>>>(a);
     else if (a.K <= kSmallK)
         count_launch(), estep_em_fast_kernel<kFastThreads, DIM, false>
                             <<<grid, kFastThreads, smem, s>>>(a);
@@ -1469,16 +1562,19 @@ void launch_estep_dim(const EStepArgs &a, bool sample, int grid, size_t smem, cu
 }
 }  // namespace
 
-int estep_grid(bool sample, int K, int L, long V, int dim, bool logt) {
+int estep_grid(bool sample, int K, int L, long V, int dim, bool logt, bool half) {
     BINDER_CHECK(dim == 2 || dim == 3, "dimension must be 2 or 3");
     BINDER_CHECK(!logt || (K <= kSmallK && K <= kLogMaxBins),
                  "the log-space E-step supports at most 64 bins");
-    int dev = 0, sms = 148, per_sm = 1;
-    BINDER_CUDA(cudaGetDevice(&dev));
-    BINDER_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = estep_smem(sample, K, L, logt);
-    const void *fn = dim == 3 ? estep_fn<3>(sample, K, logt) : estep_fn<2>(sample, K, logt);
-    const int tpb = (!sample && (logt || K <= kSmallK)) ? kFastThreads : kEThreads;
+    int per_sm = 1;
+    const int sms = device_sms();
+    const bool hc = half && !sample && !logt && K <= kSmallK;
+    const int ftpb = sample ? kFastThreads : fast_threads(V, K, L, logt, hc);
+    const bool wide = ftpb == kWideThreads;
+    const size_t smem = estep_smem(sample, K, L, logt, hc, ftpb);
+    const void *fn = dim == 3 ? estep_fn<3>(sample, K, logt, hc, wide)
+                              : estep_fn<2>(sample, K, logt, hc, wide);
+    const int tpb = (!sample && (logt || K <= kSmallK)) ? ftpb : kEThreads;
     BINDER_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // all of the unified L1 / shared array as shared memory, so the CTAs the occupancy query
     // counts are the CTAs that become resident (the default carveout may be smaller)
@@ -1579,17 +1675,22 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
     BINDER_CHECK(!args.ssdf || (args.fstate && args.fstats && args.M >= 1 &&
                                 args.M <= kSsdfMax && args.Fn >= 1 && args.Fn <= kSsdfMax),
                  "the SSD filter E-step needs 1 <= M, F <= 8");
-    const size_t smem = args.ssdf     ? ssdf_smem(args.M, args.Fn, sample)
-                        : args.filter ? filter_smem(args.K, args.L, args.M, sample)
-                                      : estep_smem(sample, args.K, args.L, args.logt != 0);
     EStepArgs a = args;
+    if (sample || a.logt || a.filter || a.ssdf) a.halfcol = 0;  // FP32 columns only there
+    // threads per CTA of the single-pass EM kernel (the same choice as estep_grid's)
+    const int ftpb = (sample || a.filter || a.ssdf)
+                         ? kFastThreads
+                         : fast_threads(a.V, a.K, a.L, a.logt != 0, a.halfcol != 0);
+    const size_t smem = a.ssdf     ? ssdf_smem(a.M, a.Fn, sample)
+                        : a.filter ? filter_smem(a.K, a.L, a.M, sample)
+                                   : estep_smem(sample, a.K, a.L, a.logt != 0, a.halfcol != 0,
+                                                ftpb);
     // the order-independent merge of the single-pass EM kernel keeps one partial per CTA
     if (a.hfix && grid > kMaxEmCtas) grid = kMaxEmCtas;
     // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
     // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a
     // cell, fit in 32 bits
-    const long per_cta = ((a.V + (long)grid * kFastThreads - 1) / ((long)grid * kFastThreads)) *
-                         kFastThreads;
+    const long per_cta = ((a.V + (long)grid * ftpb - 1) / ((long)grid * ftpb)) * ftpb;
     int e = 30;
     while (e > 0 && (double)per_cta * (std::ldexp(1.0, e) + 1.0) >= 4294967295.0) --e;
     a.hscale = (float)std::ldexp(1.0, e);
@@ -1607,9 +1708,9 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
         else
             count_launch(), estep_kernel<true, 2><<<g2, kEThreads, smem, s>>>(a);
     } else if (a.dim == 3) {
-        launch_estep_dim<3>(a, sample, grid, smem, s);
+        launch_estep_dim<3>(a, sample, grid, smem, s, ftpb);
     } else {
-        launch_estep_dim<2>(a, sample, grid, smem, s);
+        launch_estep_dim<2>(a, sample, grid, smem, s, ftpb);
     }
     BINDER_CUDA(cudaGetLastError());
 }

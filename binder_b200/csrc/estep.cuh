@@ -52,6 +52,9 @@ struct EStepArgs {
     double *fstats;
     uint64_t seed;
     uint32_t chain;
+    // the single-pass EM kernel of the MI likelihood (K <= 64): 1 = FP16 per-thread bin columns
+    // (three CTAs per SM; each voxel's per-bin posterior mass rounded to FP16), 0 = FP32
+    int halfcol;
     // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
     float hscale, hinv;
 };
@@ -61,7 +64,8 @@ constexpr int kMaxEmCtas = 2048;
 // chains > 1: a batch of chains, the sampling E-step only (chain = blockIdx.y; buffers
 // [chains][dim][V] positions / dream locations, [chains][K][L] theta / counts, [chains] states)
 void launch_estep(const EStepArgs &a, bool sample, int grid, cudaStream_t s, int chains = 1);
-int estep_grid(bool sample, int K, int L, long V, int dim, bool logt = false);
+// grid of one wave; half: for the FP16-column EM kernel (EStepArgs::halfcol)
+int estep_grid(bool sample, int K, int L, long V, int dim, bool logt = false, bool half = false);
 // largest number of bins of the log-space (SSD) E-step
 constexpr int kLogMaxBins = 64;
 // largest number of channels of the MI filter likelihood, and of M * K * L (its shared-memory

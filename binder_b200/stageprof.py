@@ -46,6 +46,8 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=20260001)
     ap.add_argument("--precision", type=int, default=None,
                     help="DCT pass format (0 FP32, 1 3xTF32, 2 TF32, 3 BF16 split, 4 BF16)")
+    ap.add_argument("--hist-precision", type=int, default=0,
+                    help="E-step bin columns (0 FP32, 1 FP16)")
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--n", type=int, default=3, help="timed runs of the stage")
     a = ap.parse_args(argv)
@@ -53,6 +55,7 @@ def main(argv=None):
     reg = make_registration(core, tuple(a.shape), a.bins, a.seed)
     if a.precision is not None:
         reg.set_precision(a.precision)
+    reg.set_histogram_precision(a.hist_precision)
     if a.stage == "sampler":
         reg.EM(10, -1e300, 1, 0)
         reg.sampler_chains(1, a.chains, 1, 1, 1, 1, 1, 1, 1, per_chain=False)  # warm-up

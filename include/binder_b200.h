@@ -223,6 +223,17 @@ int binder_registration_correct_topology(binder_registration *h, double e1, doub
 int binder_registration_set_precision(binder_registration *h, int precision);
 int binder_transform_set_precision(binder_transform *h, int precision);
 
+/* No counterpart in the reference (its E-step accumulates the joint histogram in FP32): the
+ * per-thread bin columns of the MI likelihood's EM E-step (K <= 64), where each voxel's posterior
+ * mass is summed per moving bin before it enters the histogram.  BINDER_HISTOGRAM_FP32 (the
+ * default) or BINDER_HISTOGRAM_FP16: FP16 columns use half the shared memory, so three CTAs fit
+ * on an SM instead of two; each voxel's per-bin mass is rounded to FP16 (about 11 bits), while
+ * the normaliser, the dream location, the log-likelihood and the histogram itself stay FP32 /
+ * fixed point.  Other likelihoods and the sampler ignore the setting. */
+#define BINDER_HISTOGRAM_FP32 0
+#define BINDER_HISTOGRAM_FP16 1
+int binder_registration_set_histogram_precision(binder_registration *h, int precision);
+
 /* No counterpart in the reference: the cudaStream_t the object's work runs on (for events). */
 int binder_registration_get_stream(const binder_registration *h, void **stream_out);
 

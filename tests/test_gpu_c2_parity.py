@@ -98,8 +98,10 @@ def test_c2_topology_matches_reference(core, c2):
 # FP32, 3xTF32 and the BF16 split meet the bar of the FP32 path (MI within 1e-3 relative,
 # positions within 2e-3 voxels); one TF32 or one BF16 product per pass is reported with looser
 # bounds (MI within 1e-2 relative).
-MODES = {0: ("FP32", 1e-3, 2e-3), 1: ("3xTF32", 1e-3, 2e-3), 2: ("TF32", 1e-2, 5e-2),
-         3: ("BF16x3", 1e-3, 2e-3), 4: ("BF16", 1e-2, 5e-2)}
+# (DCT pass precision, E-step bin columns): (name, bound on the relative MI error, on positions)
+MODES = {(0, 0): ("FP32", 1e-3, 2e-3), (1, 0): ("3xTF32", 1e-3, 2e-3), (2, 0): ("TF32", 1e-2, 5e-2),
+         (3, 0): ("BF16x3", 1e-3, 2e-3), (4, 0): ("BF16", 1e-2, 5e-2),
+         (3, 1): ("BF16x3 + FP16 columns", 1e-3, 2e-3)}
 
 
 def test_c2_precision_error_table(core, oracle, c2):
@@ -115,9 +117,10 @@ def test_c2_precision_error_table(core, oracle, c2):
     oracle.set_threads(os.cpu_count() or 1)
     reg = bench.setup_registration(core, inp)
     rows = []
-    for prec, (name, mi_bound, pos_bound) in MODES.items():
+    for (prec, hp), (name, mi_bound, pos_bound) in MODES.items():
         reg.reset()
         reg.set_precision(prec)
+        reg.set_histogram_precision(hp)
         assert reg.EM(its, -1e300, 1, 0) == its
         final = reg.get_final_locations_as_numpy_array().reshape(V, 3).astype(np.float64)
         theta = reg.get_likelihood_parameters()[: bench.BINS ** 2].reshape(bench.BINS,
@@ -137,3 +140,4 @@ def test_c2_precision_error_table(core, oracle, c2):
         assert row["mi_rel"] < mi_bound, row
         assert row["pos_max"] < pos_bound, row
     reg.set_precision(1)
+    reg.set_histogram_precision(0)

@@ -64,6 +64,26 @@ def test_one_em_iteration_matches_oracle(core, oracle):
     np.testing.assert_allclose(final_g, final, rtol=0, atol=2e-4)      # FP32 DCT M-step
 
 
+@pytest.mark.parametrize("shape,K,L", [((50, 48, 48), 64, 64), ((52, 50, 46), 40, 56)])
+def test_one_em_iteration_wide_form_matches_oracle(core, oracle, shape, K, L):
+    """Grids of at least one voxel per thread of a full wave of 768-thread CTAs run the E-step's
+    wide form (one CTA of 24 warps per SM, theta rows 5 banks apart); the same bounds as the
+    small case above."""
+    c = make_case(shape=shape, K=K, L=L, seed=7, disp=1.2)
+    reg = new_reg(core, c)
+    assert reg.EM(1, -1e30, 1, 0) == 1
+    dream_g = reg.get_dream_locations()
+    theta_g = reg.get_likelihood_parameters()
+    st = reg.iteration_stats()[0]
+    mll, dream, hist, deg = oracle.estep(c["d0"].astype(np.float64), c["u"], c["v"],
+                                         c["theta"].astype(np.float64), shape, shape, K, L)
+    theta = oracle.theta_map(hist, K, L, 2.0)
+    assert deg == 0
+    np.testing.assert_allclose(dream_g, dream, rtol=0, atol=5e-5)
+    np.testing.assert_allclose(theta_g, theta, rtol=1e-4, atol=1e-7)
+    assert st[0] == pytest.approx(mll, rel=1e-6)
+
+
 def test_em_run_matches_oracle_and_mi(core, oracle):
     c = make_case(shape=(14, 12, 16), seed=1)
     shape, K, L = c["shape"], c["K"], c["L"]
