@@ -1070,9 +1070,11 @@ __global__ void features_to_soa_kernel(const double *in, long n, int C, double *
 
 // BINDER/src/cpu/Registration.cpp:219-330 (EM and sampling branches), restated per voxel with the
 // histogram kept in shared memory and neighbouring equal bins combined before the atomics.  Used
-// for the Gibbs draw and for EM with K > 64.
+// for the Gibbs draw and for EM with K > 64.  The MI draw fits in 80 registers (three CTAs, 24
+// warps per SM); the log-space draw and EM keep 128 (two CTAs).
 template <bool SAMPLE, int DIM, bool LOGT = false>
-__global__ void __launch_bounds__(kEThreads, 2) estep_kernel(const EStepArgs args) {
+__global__ void __launch_bounds__(kEThreads, (SAMPLE && !LOGT) ? 3 : 2)
+    estep_kernel(const EStepArgs args) {
     constexpr int Q = DIM == 3 ? 4 : 1;
     constexpr int R = 4 * Q;  // node rows of 4 packed nodes
     if (args.skip && *args.skip) return;
