@@ -337,10 +337,11 @@ __device__ __forceinline__ void em_accumulate_log(const float *__restrict__ thu,
 // neighbourhood is a handful of bins in smooth images).  The CTA histogram is 32-bit fixed point
 // (scale a.hscale, chosen by the host so that a cell cannot overflow), which makes every flush a
 // native integer shared atomic, and is converted to FP32 once per CTA.  Each contribution is
-// rounded to within 0.5 / hscale (4e-6 at 2^17); FP32 accumulation of the same sums would round
-// each addition relative to the running sum instead.  theta is staged transposed (thT[u][k]); it
-// and the histogram use a row pitch of 9 (mod 32) banks, so lanes whose (u, k) pairs differ by
-// small amounts hit different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the host).
+// rounded to within 0.5 / hscale (3.9e-6 at 127,097, the wide form's scale at 160 x 192 x 160);
+// FP32 accumulation of the same sums would round each addition relative to the running sum
+// instead.  theta is staged transposed (thT[u][k]); it and the histogram use a row pitch of 9
+// (mod 32) banks (5 in the wide form), so lanes whose (u, k) pairs differ by small amounts hit
+// different banks.  Voxel indices are 32-bit (V < 2^31 is checked by the host).
 //
 // HC (EStepArgs::halfcol): the columns hold FP16 (half the shared memory, so three CTAs fit on an SM
 // instead of two), theta is staged multiplied by kHalfColScale so that the masses stay well inside
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(TPB, HC ? 3 : (TPB > kFastThreads ? 1 : 2))
         for (int q = threadIdx.x; q < KL; q += TPB) {
             const int k = q / L;
             const unsigned v = hs[k * LP + (q - k * L)];
-            if (v) atomicAdd(&a.hist[q], (float)v * a.hinv);
+            if (v) atomicAdd(&a.hist[q], (float)((double)v * a.hinv));
         }
         if (threadIdx.x == 0) atomicAdd(&a.st->mll, m);
         return;
@@ -454,7 +455,7 @@ __global__ void __launch_bounds__(TPB, HC ? 3 : (TPB > kFastThreads ? 1 : 2))
     __syncthreads();
     if (!last) return;
     __threadfence();
-    const double hinv = (double)a.hinv;
+    const double hinv = a.hinv;
     for (int q = threadIdx.x; q < KL; q += TPB) {
         const unsigned long long v = __ldcg(a.hfix + q);
         if (v) {
@@ -1465,11 +1466,14 @@ int device_sms() {
 }
 
 // threads per CTA of the single-pass EM kernel (MI likelihood, FP32 columns): the wide form when
-// its tables fit and one wave of it gives every thread a voxel at least, else 256 (two CTAs/SM)
+// its tables fit and one wave of it gives every thread 8 voxels at least, else 256 (two CTAs/SM).
+// With fewer voxels per thread the last pass over the grid leaves more of the wide CTAs idle, and
+// registrations run side by side (a batch) overlap better in the smaller CTAs.
+constexpr int kWideMinVoxelsPerThread = 8;
 int fast_threads(long V, int K, int L, bool logt, bool half) {
     if (logt || half || K > kSmallK) return kFastThreads;
     if (fast_smem(K, L, kWideThreads, false, false) + 512 > 227 * 1024) return kFastThreads;
-    if (V < (long)device_sms() * kWideThreads) return kFastThreads;
+    if (V < (long)device_sms() * kWideThreads * kWideMinVoxelsPerThread) return kFastThreads;
     return kWideThreads;
 }
 
@@ -1689,14 +1693,17 @@ void launch_estep(const EStepArgs &args, bool sample, int grid, cudaStream_t s, 
                                                 ftpb);
     // the order-independent merge of the single-pass EM kernel keeps one partial per CTA
     if (a.hfix && grid > kMaxEmCtas) grid = kMaxEmCtas;
-    // fixed-point scale of the EM histogram: the largest power of two (at most 2^30) for which
-    // the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded) to a
+    // fixed-point scale of the EM histogram: the largest scale (at most 2^30, exact in FP32) for
+    // which the voxels one CTA visits, each adding at most scale + 1/2 (a posterior of 1, rounded;
+    // FP32 rounding of m / S can exceed 1 by a few ulps, covered by the factor 1 + 2^-16) to a
     // cell, fit in 32 bits
     const long per_cta = ((a.V + (long)grid * ftpb - 1) / ((long)grid * ftpb)) * ftpb;
-    int e = 30;
-    while (e > 0 && (double)per_cta * (std::ldexp(1.0, e) + 1.0) >= 4294967295.0) --e;
-    a.hscale = (float)std::ldexp(1.0, e);
-    a.hinv = (float)std::ldexp(1.0, -e);
+    double sc = std::floor(4294967295.0 / ((double)per_cta * (1.0 + 1.0 / 65536.0)) - 1.0);
+    sc = sc < 1.0 ? 1.0 : (sc > 1073741824.0 ? 1073741824.0 : sc);
+    float fsc = (float)sc;
+    if ((double)fsc > sc) fsc = std::nextafter(fsc, 0.0f);  // round down into FP32
+    a.hscale = fsc;
+    a.hinv = 1.0 / (double)fsc;
     BINDER_CHECK(a.dim == 2 || a.dim == 3, "dimension must be 2 or 3");
     BINDER_CHECK(chains >= 1 && chains <= 65535 && (chains == 1 || (sample && !a.logt)),
                  "a batch of chains runs the sampling E-step of the MI likelihood only");

@@ -55,8 +55,11 @@ struct EStepArgs {
     // the single-pass EM kernel of the MI likelihood (K <= 64): 1 = FP16 per-thread bin columns
     // (three CTAs per SM; each voxel's per-bin posterior mass rounded to FP16), 0 = FP32
     int halfcol;
-    // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram (power of two)
-    float hscale, hinv;
+    // set by launch_estep: fixed-point scale of the EM kernel's per-CTA histogram and its inverse
+    // (FP64, so that the kernel multiplies: an FP64 division in the kernel's tail measured twice as
+    // slow a whole launch)
+    float hscale;
+    double hinv;
 };
 
 // CTAs of the single-pass EM kernel at most when it merges in fixed order (EStepArgs::mpart)
