@@ -216,9 +216,10 @@ void MStep::enqueue(const float *r, float *d, const float *xpos, const float *D,
     const bool tc = precision != kPrecFP32Simt;
     const int planes = (precision == kPrecTF32 || precision == kPrecBF16) ? 1 : 2;
     const bool bf16 = precision == kPrecBF16x3 || precision == kPrecBF16;
-    // the per-tile tensor-core passes read the prior noise drawn beforehand (the persistent and
-    // CUDA-core passes draw it per element)
-    if (sample && tc && noise && !(persistent && !bf16)) {
+    // the per-tile tensor-core passes read the prior noise drawn beforehand by one fully occupied
+    // kernel (the persistent and CUDA-core passes draw it per element)
+    if (sample && tc && !(persistent && !bf16)) {
+        BINDER_CHECK(noise, "sampling on the tensor-core passes needs MStep::prepare_sampling first");
         launch_prior_noise(noise, V, ncomp * chains, chains > 1 ? ncomp : 0, seed, chain, st, skip,
                            s);
         a.noise = noise;
@@ -1392,6 +1393,8 @@ void PriorTransform::sample(const float *field, int n, float *out) {
     BINDER_CHECK(n >= 0, "number_of_samples must be non-negative");
     if (n == 0) return;
     BINDER_CUDA(cudaStreamSynchronize(stream_));
+    mstep_.prepare_sampling(own_stream_);
+    BINDER_CUDA(cudaStreamSynchronize(own_stream_));
     BINDER_CUDA(cudaMemcpyAsync(mstep_.t1, field, sizeof(float) * V_ * N_,
                                 cudaMemcpyHostToDevice, stream_));
     launch_aos_to_soa(mstep_.t1, r_, V_, N_, stream_);

@@ -503,11 +503,11 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
 
     const int comp = a.comp0 + (int)blockIdx.z;
     // components of a batch of chains are numbered chain * chain_comps + component: the chain
-    // picks the state and the Philox chain index, the component within it everything else
+    // picks the state (and, in the noise buffer, its block of components), the component within
+    // it everything else
     const int bch = a.chain_comps ? comp / a.chain_comps : 0;
     const int cn = comp - bch * a.chain_comps;
     DevState *const st = a.st ? a.st + bch : nullptr;
-    const uint32_t chain = a.chain + (uint32_t)bch;
     const float *in = a.in + comp * a.V;
     float *out = a.out + comp * a.V;
     const long nlines = a.outer * a.s;
@@ -678,7 +678,6 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
     umma::fence_after_sync();
 
     double part_cost = 0.0, part_raw = 0.0;
-    const uint32_t sweep = (MODE == kEpiSpectralOut && a.sample) ? (uint32_t)st->sweep : 0u;
     const bool want_raw = MODE == kEpiSpectralOut && a.want_raw && (st->sweep % a.every == 0);
     const double gamma = MODE == kEpiSpectralOut ? st->gamma[cn] : 0.0;
     const float gs2 = (float)(gamma * a.sigma2);
@@ -728,7 +727,18 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
 #pragma unroll
                 for (int m = 0; m < 32; ++m) dnext[m] = dfirst[m];
             for (int cc = 0; cc < nchunks; ++cc) {
-                float v[32], dcur[32];
+                float v[32], dcur[32], nz[32];
+                // the chunk's prior noise, all 32 loads in flight before the first is used (read
+                // one element at a time between the stores, each waited a full memory latency)
+                if (MODE == kEpiSpectralOut && a.sample) {
+#pragma unroll
+                    for (int m = 0; m < 32; ++m) {
+                        const int k = cc * 32 + m;
+                        nz[m] = (valid && k < n)
+                                    ? __ldg(a.noise + comp * a.V + (long)k * a.s + t)
+                                    : 0.0f;
+                    }
+                }
                 umma::tmem_ld32(tmem + tlane + (uint32_t)(cc * 32), v);
                 if (MODE == kEpiSpectralOut) {
 #pragma unroll
@@ -747,12 +757,7 @@ __global__ void __launch_bounds__(kWsThreads, 2) umma_ws_kernel(const UArgs a) {
                             const float Dv = dcur[m];
                             const float f = __fdividef(1.0f, fmaf(gs2, Dv, 1.0f));
                             val *= f;
-                            if (a.sample)
-                                val += sqrtf((float)a.sigma2 * f) *
-                                       (a.noise ? __ldg(a.noise + comp * a.V + (long)k * a.s + t)
-                                                : prior_normal_tc(a.seed,
-                                                                  (uint32_t)((long)k * a.s + t),
-                                                                  sweep, chain, cn));
+                            if (a.sample) val += sqrtf((float)a.sigma2 * f) * nz[m];
                             ccost += Dv * val * val;
                         }
                         op[(long)k * a.s] = val;
