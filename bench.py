@@ -778,7 +778,9 @@ def run_b200(args, rank, world, local, dist):
               dict(grid=inp["grid"], D=inp["D"], theta=inp["theta"], u=inp["pair"].u,
                    v=inp["pair"].v).items()}
     V = inp["V"]
-    h2d = (pinned["grid"].nbytes * 2 + pinned["D"].nbytes + pinned["theta"].nbytes +
+    # the starting positions and the voxel grid are the same host array, which the library
+    # copies to the device once
+    h2d = (pinned["grid"].nbytes + pinned["D"].nbytes + pinned["theta"].nbytes +
            pinned["u"].nbytes + pinned["v"].nbytes)
     d2h = V * 3 * 4
 
