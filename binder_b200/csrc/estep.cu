@@ -179,12 +179,6 @@ __host__ __device__ constexpr int fast_pitch(int K) {
     return TPB > kFastThreads ? wide_pitch(K) : theta_pitch(K);
 }
 
-// The node pass of one EM voxel (4 x Q rows of 4 packed nodes; Q = 4 in 3D, 1 in 2D): weights
-// w = bx[p] by[q] bz[c] theta[k] added to the thread's private bin column col[k * TPB], their sum
-// S, their first moments along each axis (node offset -1 .. 2 times w) and the range of bins
-// touched.  theta and the column are disjoint regions of shared memory; the __restrict__
-// qualifiers let the compiler hoist the theta loads of later nodes above earlier column updates.
-// Products and sums run on paired FP32 lanes (nodes c = 0,1 and c = 2,3 of each packed word).
 // FP16 bin columns (EStepArgs::halfcol): [K][TPB] halves, the thread's entry for bin k at
 // col[k * TPB], the same indexing as the FP32 columns (one shift and add per neighbour).  Lanes 2j
 // and 2j + 1 share a 32-bit word, so two such lanes updating different bins in one instruction
@@ -222,6 +216,12 @@ __device__ __forceinline__ void col_clear(__half *col, int k) {
     *half_slot<TPB>(col, k) = __float2half_rn(0.0f);
 }
 
+// The node pass of one EM voxel (4 x Q rows of 4 packed nodes; Q = 4 in 3D, 1 in 2D): weights
+// w = bx[p] by[q] bz[c] theta[k] added to the thread's private bin column col[k * TPB], their sum
+// S, their first moments along each axis (node offset -1 .. 2 times w) and the range of bins
+// touched.  theta and the column are disjoint regions of shared memory; the __restrict__
+// qualifiers let the compiler hoist the theta loads of later nodes above earlier column updates.
+// Products and sums run on paired FP32 lanes (nodes c = 0,1 and c = 2,3 of each packed word).
 template <int TPB, int Q, typename CT>
 __device__ __forceinline__ void em_accumulate(const float *__restrict__ thu,
                                               CT *__restrict__ col, const uint32_t (&pk)[4 * Q],
