@@ -15,8 +15,11 @@ import os
 
 import numpy as np
 
-# E-step CTAs (0: every SM times its occupancy) x DCT operand format (3 BF16 split, 1 TF32 split)
+# E-step CTAs (0: every SM times its occupancy) x DCT operand format (3 BF16 split, 1 TF32 split);
+# the first is the default, which another candidate must beat by MARGIN to be chosen
 CANDIDATES = [dict(estep_ctas=c, precision=p) for c in (0, 148, 74, 37) for p in (3, 1)]
+MARGIN = 0.03
+REPEATS = 2  # timed runs per candidate, the fastest kept
 CLASS_EDGES = (64 ** 3, 112 ** 3)  # voxel counts separating the small / medium / large classes
 
 
@@ -51,20 +54,26 @@ def tune(core, regs, shapes, cache=None, iterations=6, retune=False):
         if cls in table:
             continue
         sub = members[:8]
-        best = None
+        times = []
         for cand in CANDIDATES:
             for r in sub:
                 apply(r, cand)
                 r.reset()
             b = core.RegistrationBatch(sub)
             b.EM(iterations, -1e300, 1)  # warm-up (graph capture, first launches)
-            for r in sub:
-                r.reset()
-            b.EM(iterations, -1e300, 1)
-            ms = b.last_ms
-            if best is None or ms < best[0]:
-                best = (ms, cand)
-        table[cls] = dict(best[1], ms_per_iteration=best[0] / iterations, pairs=len(sub))
+            ms = float("inf")
+            for _ in range(REPEATS):
+                for r in sub:
+                    r.reset()
+                b.EM(iterations, -1e300, 1)
+                ms = min(ms, b.last_ms)
+            times.append(ms)
+        # a single timing of a few iterations is noisy: keep the default unless another
+        # candidate is clearly faster
+        k = int(np.argmin(times))
+        if times[k] > (1.0 - MARGIN) * times[0]:
+            k = 0
+        table[cls] = dict(CANDIDATES[k], ms_per_iteration=times[k] / iterations, pairs=len(sub))
     for r, s in zip(regs, shapes):
         apply(r, table[size_class(s)])
         r.reset()
