@@ -44,6 +44,8 @@ def test_null_arguments_are_rejected(core):
     assert st == 1 and b"NULL" in lib().binder_last_error()
     assert lib().binder_registration_destroy(None) == 0
     assert lib().binder_transform_destroy(None) == 0
+    for fn in ("binder_registration_set_precision", "binder_registration_set_histogram_precision"):
+        assert getattr(lib(), fn)(None, 0) == 1 and b"NULL" in lib().binder_last_error(), fn
     del h
 
 
