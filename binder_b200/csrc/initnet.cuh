@@ -1,7 +1,7 @@
 // Learned initialiser of the registration: a 3D convolutional encoder-decoder that predicts a
 // coarse displacement field from a moving / fixed image pair, trained and run on hand-written
 // sm_100a kernels (BF16 operands on tcgen05 with FP32 accumulation in TMEM, FP32 master weights
-// and Adam).  The registration itself stays the judge: the prediction only seeds the positions
+// and Adam).  The registration itself has the last word: the prediction only seeds the positions
 // the EM starts from (the final_locations argument of Registration).
 #pragma once
 

@@ -4,7 +4,7 @@ A 3D convolutional encoder-decoder (channels 16-32-64-128) predicts, from a movi
 pair, the displacement on the grid of every 4th voxel; up-sampled to the full grid it seeds the
 positions the EM starts from -- the reference's own hook for an initial deformation is the
 final_locations argument of Registration (BINDER/FastRegistration.py:443-450).  The registration
-stays the judge: it runs to convergence from the seeded positions exactly as from the identity.
+has the last word: it runs to convergence from the seeded positions exactly as from the identity.
 
 The network trains and runs on the library's hand-written kernels (binder_initnet_* in
 include/binder_b200.h).  Training pairs are generated by this package itself, the way the
